@@ -1,0 +1,830 @@
+// mk_api.cu — C ABI of libmechanic_b200: the GpuPhysics replacement
+// (crates/mechanic-gpu/src/device.rs:369-1663) over CUDA streams and graphs.
+//
+// One handle = one scene on one device: a single device arena holds every
+// buffer, one stream orders all work, and each tick is one CUDA graph launch
+// (two graphs, one per contact-buffer parity, because the previous tick's
+// contact list is the manifold cache of the next).
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "mk_device.cuh"
+#include "mk_internal.h"
+#include "mk_mechanism.h"
+
+namespace {
+
+thread_local std::string g_last_error;
+
+constexpr uint32_t kTickRing = 64;       // pinned tick-config slots in flight
+constexpr uint32_t kStageEvents = 8;
+
+struct DeviceGuard {
+    int prev = -1;
+    explicit DeviceGuard(int dev) {
+        cudaGetDevice(&prev);
+        if (prev != dev) cudaSetDevice(dev);
+    }
+    ~DeviceGuard() {
+        int cur = -1;
+        cudaGetDevice(&cur);
+        if (prev >= 0 && cur != prev) cudaSetDevice(prev);
+    }
+};
+
+void set_error(MkError* err, int code, const char* fmt, ...) {
+    char buf[256];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    g_last_error = buf;
+    if (err) {
+        std::memset(err, 0, sizeof(*err));
+        err->code = code;
+        std::snprintf(err->message, sizeof(err->message), "%s", buf);
+    }
+}
+
+}  // namespace
+
+struct MkHandle {
+    int device = 0;
+    int sm_count = 148;
+    cudaStream_t stream = nullptr;
+    MkConfig config{};
+    mk::StepParams params{};
+    mk::StepLaunch launch{};
+    mk::StepBuffers buf{};
+    mk::MechBuffers mech{};
+    mk::MechParams mech_params{};
+    uint32_t B = 0, C = 0, J = 0, S = 0, Q = 0, max_depth = 0, closure_count = 0;
+    uint32_t pair_capacity = 0;
+    bool mechanism_active = false;
+    bool collisions = false;
+    // memory
+    void* arena = nullptr;
+    size_t arena_bytes = 0;
+    float4* staging = nullptr;          // 2 x float4 per body (interleaved transforms)
+    // host
+    mk::DevTick* h_tick = nullptr;      // pinned ring
+    GpuDiagnostics* h_diag = nullptr;   // pinned, written at the end of every tick
+    cudaEvent_t tick_done[kTickRing] = {};
+    uint64_t tick_sub[kTickRing] = {};
+    cudaEvent_t stage[kStageEvents] = {};
+    cudaGraphExec_t graph[2] = {nullptr, nullptr};
+    int parity = 0;                     // parity of the next tick's contact buffer
+    uint64_t submissions = 0;
+    uint64_t last_submission = 0;
+    bool any_tick = false;
+};
+
+namespace {
+
+bool check(cudaError_t e, MkError* err, const char* what) {
+    if (e == cudaSuccess) return true;
+    set_error(err, MK_ERR_DEVICE_FAILURE, "%s: %s", what, cudaGetErrorString(e));
+    return false;
+}
+
+// Bump allocator over one device arena.
+struct Carver {
+    char* base = nullptr;
+    uint64_t off = 0;
+    template <class T>
+    T* take(uint64_t count) {
+        T* p = base ? reinterpret_cast<T*>(base + off) : nullptr;
+        off += mk::align256(count * sizeof(T) + (count == 0 ? 16 : 0));
+        return p;
+    }
+};
+
+uint32_t pick(uint32_t v, uint32_t fallback) { return v ? v : fallback; }
+
+// Lays out every buffer of the handle; with base == nullptr it only sizes.
+uint64_t carve(MkHandle* h, char* base) {
+    Carver c{base, 0};
+    const uint32_t B = std::max(h->B, 1u), C = std::max(h->C, 1u);
+    const uint64_t P = h->pair_capacity;
+    mk::StepBuffers& b = h->buf;
+    b.pos = c.take<float4>(B);
+    b.rot = c.take<float4>(B);
+    b.lin = c.take<float4>(B);
+    b.ang = c.take<float4>(B);
+    b.inv_mass = c.take<float>(B);
+    b.mass = c.take<float4>(4ull * B);
+    b.world_mass = c.take<float4>(3ull * B);
+    b.root_flags = c.take<uint32_t>(B);
+    b.components = nullptr;
+    b.deltas = c.take<int32_t>(6ull * B);
+    b.snap_pos = c.take<float4>(3ull * B);
+    b.snap_rot = c.take<float4>(3ull * B);
+    b.colliders = c.take<float4>(4ull * C);
+    b.boxes = c.take<float4>(3ull * C);
+    b.aabbs = c.take<float4>(2ull * C);
+    b.keys = c.take<uint64_t>(C);
+    b.values = c.take<uint32_t>(C);
+    b.skeys = c.take<uint64_t>(C);
+    b.svals = c.take<uint32_t>(C);
+    b.children = c.take<uint2>(C);
+    b.parents = c.take<uint32_t>(2ull * C);
+    b.visits = c.take<uint32_t>(C);
+    b.node_aabbs = c.take<float4>(4ull * C);
+    b.suppressed = c.take<uint2>(std::max(h->S, 1u));
+    b.pair_offsets = c.take<uint32_t>(C + 1ull);
+    b.pairs = c.take<uint2>(P);
+    for (int k = 0; k < 2; ++k) {
+        b.contacts[k] = c.take<GpuContact>(P);
+        b.contact_keys[k] = c.take<uint64_t>(P);
+        b.features[k] = c.take<uint32_t>(P);
+    }
+    b.active = c.take<uint32_t>(P);
+    b.lookback_words = std::max<uint64_t>(P / 256 + 2, C / 256 + 2);
+    b.lookback = c.take<uint64_t>(4 * b.lookback_words);
+    b.tickets = c.take<uint32_t>(16);
+    b.diag = c.take<GpuDiagnostics>(1);
+    b.tick = c.take<mk::DevTick>(1);
+    b.counts = c.take<mk::DevCounts>(1);
+    b.sort_scratch_bytes = mk::sort_scratch_bytes(C, 63);
+    b.sort_scratch = c.take<char>(b.sort_scratch_bytes);
+    h->staging = c.take<float4>(2ull * B);
+    // mechanism buffers
+    if (h->mechanism_active || h->J > 0) {
+        mk::carve_mechanism(h->mech, h->B, h->J, h->Q, [&](uint64_t bytes) { return c.take<char>(bytes); });
+    }
+    if (h->config.mechanism_self_collisions == 0) b.components = c.take<uint32_t>(B);
+    return c.off;
+}
+
+// The full tick on `stream` (captured into a graph or launched directly).
+cudaError_t enqueue_tick(MkHandle* h, int parity, bool capturing) {
+    cudaStream_t s = h->stream;
+    mk::StepBuffers& b = h->buf;
+    // Stage boundaries: external event-record nodes inside a graph, plain
+    // records when launched directly.
+    auto mark = [&](int i) -> cudaError_t {
+        return capturing ? cudaEventRecordWithFlags(h->stage[i], s, cudaEventRecordExternal)
+                         : cudaEventRecord(h->stage[i], s);
+    };
+    cudaError_t e;
+    if ((e = mark(0)) != cudaSuccess) return e;
+    cudaMemsetAsync(b.diag, 0, sizeof(GpuDiagnostics), s);
+    cudaMemsetAsync(b.counts, 0, 4 * sizeof(uint32_t), s);
+    cudaMemsetAsync(b.tickets, 0, 16 * sizeof(uint32_t), s);
+    if (h->collisions) {
+        cudaMemsetAsync(b.visits, 0, sizeof(uint32_t) * std::max(h->C, 1u), s);
+        cudaMemsetAsync(b.deltas, 0, sizeof(int32_t) * 6ull * std::max(h->B, 1u), s);
+        cudaMemsetAsync(b.lookback, 0, sizeof(uint64_t) * 4 * b.lookback_words, s);
+    }
+    if (h->mechanism_active) mk::enqueue_mechanism_prelude(h->mech, b, h->mech_params, s);
+    const bool fuse = !h->mechanism_active;
+    mk::StepLaunch l = h->launch;
+    l.fuse_world_mass = fuse;
+    if ((e = mk::launch_integrate(b, h->params, l, s)) != cudaSuccess) return e;
+    if ((e = mark(1)) != cudaSuccess) return e;
+    if (h->mechanism_active) {
+        if ((e = mk::enqueue_mechanism(h->mech, b, h->mech_params, s)) != cudaSuccess) return e;
+    }
+    if ((e = mark(2)) != cudaSuccess) return e;
+    if (h->collisions) {
+        if (!fuse && (e = mk::launch_world_masses(b, h->params, s)) != cudaSuccess) return e;
+        if ((e = mk::launch_broadphase(b, h->params, l, parity, s)) != cudaSuccess) return e;
+        if ((e = mark(3)) != cudaSuccess) return e;
+        if ((e = mk::launch_narrowphase(b, h->params, l, parity, s)) != cudaSuccess) return e;
+        if ((e = mark(4)) != cudaSuccess) return e;
+        if (h->mechanism_active && h->mech_params.has_dynamic_root) {
+            if ((e = mk::enqueue_contact_solver_with_bearings(h->mech, b, h->params, h->mech_params, l, parity, s)) !=
+                cudaSuccess)
+                return e;
+        } else {
+            if ((e = mk::launch_contact_solver(b, h->params, l, parity, s)) != cudaSuccess) return e;
+        }
+        if (h->mechanism_active) {
+            if ((e = mk::enqueue_post_contact(h->mech, b, h->mech_params, s)) != cudaSuccess) return e;
+        }
+    } else {
+        if ((e = mark(3)) != cudaSuccess) return e;
+        if ((e = mark(4)) != cudaSuccess) return e;
+    }
+    if ((e = mark(5)) != cudaSuccess) return e;
+    if (h->mechanism_active) mk::enqueue_validate_state(h->mech, b, h->mech_params, s);
+    if (h->J > 0) mk::enqueue_validate_bearings(h->mech, b, h->mech_params, h->mechanism_active, s);
+    if ((e = mark(6)) != cudaSuccess) return e;
+    if (!fuse && (e = mk::launch_snapshot(b, h->params, s)) != cudaSuccess) return e;
+    if (h->collisions && (e = mk::launch_finish_tick(b, h->params, parity, s)) != cudaSuccess) return e;
+    cudaMemcpyAsync(h->h_diag, b.diag, sizeof(GpuDiagnostics), cudaMemcpyDeviceToHost, s);
+    if ((e = mark(7)) != cudaSuccess) return e;
+    return cudaGetLastError();
+}
+
+bool build_graphs(MkHandle* h, MkError* err) {
+    for (int p = 0; p < 2; ++p) {
+        cudaGraph_t g = nullptr;
+        if (!check(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal), err, "begin capture"))
+            return false;
+        cudaError_t e = enqueue_tick(h, p, true);
+        cudaError_t e2 = cudaStreamEndCapture(h->stream, &g);
+        if (!check(e, err, "capture tick") || !check(e2, err, "end capture")) {
+            if (g) cudaGraphDestroy(g);
+            return false;
+        }
+        cudaGraphExec_t exec = nullptr;
+        e = cudaGraphInstantiate(&exec, g, 0);
+        cudaGraphDestroy(g);
+        if (!check(e, err, "instantiate tick graph")) return false;
+        h->graph[p] = exec;
+    }
+    return true;
+}
+
+template <class T>
+cudaError_t upload(T* dst, const void* src, uint64_t count, cudaStream_t s) {
+    if (!src || count == 0) return cudaSuccess;
+    return cudaMemcpyAsync(dst, src, count * sizeof(T), cudaMemcpyHostToDevice, s);
+}
+
+// Interleaves float4 pos/rot rows into GpuTransform rows on the device.
+__global__ void k_interleave(const float4* a, const float4* b, float4* out, uint32_t n) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    out[2ull * i] = a[i];
+    out[2ull * i + 1] = b[i];
+}
+__global__ void k_deinterleave(const float4* in, float4* a, float4* b, uint32_t n) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    a[i] = in[2ull * i];
+    b[i] = in[2ull * i + 1];
+}
+
+void destroy_handle(MkHandle* h) {
+    if (!h) return;
+    DeviceGuard g(h->device);
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    for (auto& gx : h->graph)
+        if (gx) cudaGraphExecDestroy(gx);
+    for (auto& e : h->tick_done)
+        if (e) cudaEventDestroy(e);
+    for (auto& e : h->stage)
+        if (e) cudaEventDestroy(e);
+    if (h->arena) cudaFree(h->arena);
+    if (h->h_tick) cudaFreeHost(h->h_tick);
+    if (h->h_diag) cudaFreeHost(h->h_diag);
+    if (h->stream) cudaStreamDestroy(h->stream);
+    delete h;
+}
+
+}  // namespace
+
+extern "C" {
+
+void mk_config_default(MkConfig* c) {
+    if (!c) return;
+    std::memset(c, 0, sizeof(*c));
+    c->collisions_enabled = 1;
+    c->mechanism_self_collisions = 1;
+    c->solver_iterations = 8;
+    c->morton_mode = MK_MORTON_63;
+    c->closure_mode = MK_CLOSURE_REFERENCE;
+    c->use_graph = 1;
+}
+
+const char* mk_version(void) { return "mechanic_b200 0.1.0 sm_100a"; }
+
+const char* mk_last_error(void) { return g_last_error.c_str(); }
+
+int mk_create(const MkCreation* cr, const MkConfig* config, const MkCapacities* caps, MkHandle** out, MkError* err) {
+    if (err) std::memset(err, 0, sizeof(*err));
+    if (!cr || !out) {
+        set_error(err, MK_ERR_INVALID_ARGUMENT, "creation and out must be non-null");
+        return MK_ERR_INVALID_ARGUMENT;
+    }
+    *out = nullptr;
+    // Capacity checks (device.rs:405-422).
+    const uint32_t max_bodies = caps ? pick(caps->max_bodies, cr->body_count) : MK_DEFAULT_MAX_BODIES;
+    const uint32_t max_bearings = caps ? pick(caps->max_bearings, cr->bearing_count) : MK_DEFAULT_MAX_BEARINGS;
+    const uint32_t max_colliders = caps ? pick(caps->max_colliders, cr->collider_count) : MK_DEFAULT_MAX_COLLIDERS;
+    const uint32_t pair_capacity = caps ? pick(caps->pair_capacity, MK_DEFAULT_MAX_CONTACT_PAIRS)
+                                        : MK_DEFAULT_MAX_CONTACT_PAIRS;
+    if (cr->body_count > max_bodies) {
+        set_error(err, MK_ERR_BODY_CAPACITY, "scene requires %u bodies but capacity is %u", cr->body_count, max_bodies);
+        err ? (err->required = cr->body_count, err->capacity = max_bodies) : 0;
+        return MK_ERR_BODY_CAPACITY;
+    }
+    if (cr->bearing_count > max_bearings) {
+        set_error(err, MK_ERR_BEARING_CAPACITY, "scene requires %u bearings but capacity is %u", cr->bearing_count,
+                  max_bearings);
+        err ? (err->required = cr->bearing_count, err->capacity = max_bearings) : 0;
+        return MK_ERR_BEARING_CAPACITY;
+    }
+    if (cr->collider_count > max_colliders) {
+        set_error(err, MK_ERR_COLLIDER_CAPACITY, "scene requires %u colliders but capacity is %u", cr->collider_count,
+                  max_colliders);
+        err ? (err->required = cr->collider_count, err->capacity = max_colliders) : 0;
+        return MK_ERR_COLLIDER_CAPACITY;
+    }
+    if (cr->body_count == 0 || !cr->transforms || !cr->masses ||
+        (cr->collider_count && !cr->colliders) || (cr->bearing_count && !cr->bearings) ||
+        (cr->suppression_count && !cr->suppressed_pairs) ||
+        (cr->max_depth > 0 && (!cr->mechanism_bodies || !cr->preorder))) {
+        set_error(err, MK_ERR_INVALID_ARGUMENT, "creation arrays missing for the given counts");
+        return MK_ERR_INVALID_ARGUMENT;
+    }
+    if (pair_capacity == 0 || pair_capacity > (1u << 30)) {
+        set_error(err, MK_ERR_PAIR_CAPACITY, "pair capacity %u outside 1..2^30", pair_capacity);
+        return MK_ERR_PAIR_CAPACITY;
+    }
+    MkHandle* h = new MkHandle();
+    if (config) h->config = *config;
+    else mk_config_default(&h->config);
+    h->device = h->config.device;
+    DeviceGuard guard(h->device);
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || h->device < 0 || h->device >= ndev) {
+        set_error(err, MK_ERR_DEVICE_FAILURE, "CUDA device %d unavailable", h->device);
+        delete h;
+        return MK_ERR_DEVICE_FAILURE;
+    }
+    cudaSetDevice(h->device);
+    cudaDeviceGetAttribute(&h->sm_count, cudaDevAttrMultiProcessorCount, h->device);
+    h->B = cr->body_count;
+    h->C = cr->collider_count;
+    h->J = cr->bearing_count;
+    h->S = cr->suppression_count;
+    h->Q = cr->coordinate_count;
+    h->max_depth = cr->max_depth;
+    h->closure_count = cr->closure_count;
+    h->pair_capacity = pair_capacity;
+    h->mechanism_active = cr->max_depth > 0;
+    h->collisions = h->config.collisions_enabled && h->C > 0;
+    const MkConfig& c = h->config;
+    h->params.dt = c.delta_seconds != 0.0f ? c.delta_seconds : 1.0f / 60.0f;
+    h->params.gravity = c.gravity_y != 0.0f ? c.gravity_y : -9.81f;
+    h->params.lin_damp = c.linear_damping != 0.0f ? c.linear_damping : 0.999f;
+    h->params.ang_damp = c.angular_damping != 0.0f ? c.angular_damping : 0.98f;
+    h->params.body_count = h->B;
+    h->params.collider_count = h->C;
+    h->params.pair_capacity = pair_capacity;
+    h->params.suppression_count = h->S;
+    h->launch.sm_count = h->sm_count;
+    h->launch.morton_mode = c.morton_mode;
+    h->launch.iterations = std::max(1u, c.solver_iterations ? c.solver_iterations : 8u);
+    h->launch.collisions = h->collisions;
+    h->mech_params = mk::make_mech_params(cr, h->params, h->launch.iterations, c.closure_mode);
+
+    bool ok = check(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking), err, "stream");
+    const uint64_t bytes = ok ? carve(h, nullptr) : 0;
+    ok = ok && check(cudaMalloc(&h->arena, bytes), err, "device arena");
+    if (ok) {
+        h->arena_bytes = bytes;
+        carve(h, (char*)h->arena);
+        ok = check(cudaMemsetAsync(h->arena, 0, bytes, h->stream), err, "clear arena");
+    }
+    ok = ok && check(cudaMallocHost(&h->h_tick, sizeof(mk::DevTick) * kTickRing), err, "pinned tick ring");
+    ok = ok && check(cudaMallocHost(&h->h_diag, sizeof(GpuDiagnostics)), err, "pinned diagnostics");
+    for (uint32_t i = 0; ok && i < kTickRing; ++i)
+        ok = check(cudaEventCreateWithFlags(&h->tick_done[i], cudaEventDisableTiming), err, "event");
+    for (uint32_t i = 0; ok && i < kStageEvents; ++i) ok = check(cudaEventCreate(&h->stage[i]), err, "event");
+    if (!ok) {
+        destroy_handle(h);
+        return MK_ERR_DEVICE_FAILURE;
+    }
+    std::memset(h->h_diag, 0, sizeof(GpuDiagnostics));
+    // Upload rows (device.rs:429-523): transforms de-interleaved into SoA.
+    mk::StepBuffers& b = h->buf;
+    cudaStream_t s = h->stream;
+    std::vector<float4> tmp(2ull * h->B);
+    std::memcpy(tmp.data(), cr->transforms, sizeof(GpuTransform) * h->B);
+    ok = check(upload<float4>(h->staging, tmp.data(), 2ull * h->B, s), err, "upload transforms");
+    if (ok) k_deinterleave<<<(h->B + 255) / 256, 256, 0, s>>>(h->staging, b.pos, b.rot, h->B);
+    if (ok && cr->velocities) {
+        std::memcpy(tmp.data(), cr->velocities, sizeof(GpuVelocity) * h->B);
+        ok = check(cudaStreamSynchronize(s), err, "sync");
+        ok = ok && check(upload<float4>(h->staging, tmp.data(), 2ull * h->B, s), err, "upload velocities");
+        if (ok) k_deinterleave<<<(h->B + 255) / 256, 256, 0, s>>>(h->staging, b.lin, b.ang, h->B);
+    }
+    std::vector<float> inv(h->B);
+    std::vector<uint32_t> roots(h->B, 1u);
+    for (uint32_t i = 0; i < h->B; ++i) inv[i] = cr->masses[i].inverse_mass[0];
+    if (cr->root_flags) std::memcpy(roots.data(), cr->root_flags, 4ull * h->B);
+    ok = ok && check(upload<float>(const_cast<float*>(b.inv_mass), inv.data(), h->B, s), err, "upload inverse masses");
+    ok = ok && check(upload<float4>(const_cast<float4*>(b.mass), cr->masses, 4ull * h->B, s), err, "upload masses");
+    ok = ok && check(upload<uint32_t>(const_cast<uint32_t*>(b.root_flags), roots.data(), h->B, s), err, "upload roots");
+    ok = ok && check(upload<float4>(const_cast<float4*>(b.colliders), cr->colliders, 4ull * h->C, s), err,
+                     "upload colliders");
+    ok = ok && check(upload<uint2>(const_cast<uint2*>(b.suppressed), cr->suppressed_pairs, h->S, s), err,
+                     "upload suppression");
+    if (ok && b.components) {
+        std::vector<uint32_t> comp(h->B);
+        for (uint32_t i = 0; i < h->B; ++i) comp[i] = cr->body_components ? cr->body_components[i] : i;
+        ok = check(upload<uint32_t>(const_cast<uint32_t*>(b.components), comp.data(), h->B, s), err, "components");
+        ok = ok && check(cudaStreamSynchronize(s), err, "sync");
+    }
+    if (ok && (h->mechanism_active || h->J > 0)) ok = mk::upload_mechanism(h->mech, cr, s, err);
+    ok = ok && check(cudaStreamSynchronize(s), err, "upload sync");
+    // Snapshot ring starts as the initial pose (device.rs:666-684).
+    for (uint32_t slot = 0; ok && slot < 3; ++slot) {
+        ok = check(cudaMemcpyAsync(b.snap_pos + (size_t)slot * h->B, b.pos, 16ull * h->B, cudaMemcpyDeviceToDevice, s),
+                   err, "snapshot init");
+        ok = ok && check(cudaMemcpyAsync(b.snap_rot + (size_t)slot * h->B, b.rot, 16ull * h->B,
+                                         cudaMemcpyDeviceToDevice, s), err, "snapshot init");
+    }
+    ok = ok && check(cudaStreamSynchronize(s), err, "create sync");
+    if (ok && h->config.use_graph) ok = build_graphs(h, err);
+    if (!ok) {
+        destroy_handle(h);
+        return err ? err->code : MK_ERR_DEVICE_FAILURE;
+    }
+    *out = h;
+    return MK_OK;
+}
+
+void mk_destroy(MkHandle* h) { destroy_handle(h); }
+
+int mk_dispatch_tick(MkHandle* h, uint64_t tick_index, MkSubmission* out) {
+    if (!h) return MK_ERR_INVALID_ARGUMENT;
+    DeviceGuard guard(h->device);
+    const uint64_t sub = ++h->submissions;
+    const uint32_t slot = (uint32_t)(sub % kTickRing);
+    if (h->tick_sub[slot]) cudaEventSynchronize(h->tick_done[slot]);
+    mk::DevTick& t = h->h_tick[slot];
+    std::memset(&t, 0, sizeof(t));
+    t.tick_index = (uint32_t)tick_index;    // wrapping_u32 (device.rs:868)
+    t.snapshot_slot = (uint32_t)(tick_index % 3);
+    cudaError_t e = cudaMemcpyAsync(h->buf.tick, &t, sizeof(t), cudaMemcpyHostToDevice, h->stream);
+    const int parity = h->parity;
+    if (e == cudaSuccess) {
+        if (h->graph[parity]) e = cudaGraphLaunch(h->graph[parity], h->stream);
+        else e = enqueue_tick(h, parity, false);
+    }
+    if (e == cudaSuccess) e = cudaEventRecord(h->tick_done[slot], h->stream);
+    if (e != cudaSuccess) {
+        set_error(nullptr, MK_ERR_DEVICE_FAILURE, "dispatch_tick: %s", cudaGetErrorString(e));
+        return MK_ERR_DEVICE_FAILURE;
+    }
+    h->tick_sub[slot] = sub;
+    h->last_submission = sub;
+    h->parity ^= (h->collisions ? 1 : 0);
+    h->any_tick = true;
+    if (out) {
+        std::memset(out, 0, sizeof(*out));
+        out->tick_index = tick_index;
+        out->snapshot_slot = (uint8_t)(tick_index % 3);
+        out->submission_index = sub;
+    }
+    return MK_OK;
+}
+
+int mk_wait(MkHandle* h, uint64_t submission) {
+    if (!h) return MK_ERR_INVALID_ARGUMENT;
+    DeviceGuard guard(h->device);
+    cudaError_t e = cudaSuccess;
+    if (submission == 0 || submission >= h->last_submission) {
+        e = cudaStreamSynchronize(h->stream);
+    } else {
+        const uint32_t slot = (uint32_t)(submission % kTickRing);
+        if (h->tick_sub[slot] == submission) e = cudaEventSynchronize(h->tick_done[slot]);
+    }
+    if (e != cudaSuccess) {
+        set_error(nullptr, MK_ERR_DEVICE_FAILURE, "wait: %s", cudaGetErrorString(e));
+        return MK_ERR_DEVICE_FAILURE;
+    }
+    return MK_OK;
+}
+
+int mk_read_last_tick(MkHandle* h, MkTickReadback* out) {
+    if (!h || !out) return MK_ERR_INVALID_ARGUMENT;
+    DeviceGuard guard(h->device);
+    cudaError_t e = cudaStreamSynchronize(h->stream);
+    if (e != cudaSuccess) {
+        set_error(nullptr, MK_ERR_DEVICE_FAILURE, "read_last_tick: %s", cudaGetErrorString(e));
+        return MK_ERR_DEVICE_FAILURE;
+    }
+    std::memset(out, 0, sizeof(*out));
+    const GpuDiagnostics d = *h->h_diag;
+    out->has_timestamps = 1;
+    out->error_flags = d.error_flags;
+    out->pair_count = d.pair_count;
+    out->contact_count = d.contact_count;
+    out->active_contact_count = d.active_contact_count;
+    // diagnostic_units: micro-units to units (device.rs:1520-1521).
+    out->anchor_residual_meters = (float)((double)d.max_anchor_micrometers / 1.0e6);
+    out->axis_residual_degrees = (float)((double)d.max_axis_microdegrees / 1.0e6);
+    if (h->any_tick) {
+        float ms[kStageEvents - 1] = {};
+        for (uint32_t i = 0; i + 1 < kStageEvents; ++i)
+            if (cudaEventElapsedTime(&ms[i], h->stage[i], h->stage[i + 1]) != cudaSuccess) ms[i] = 0.0f;
+        cudaGetLastError();
+        out->kernel_timings.integration_ms = ms[0];
+        out->kernel_timings.mechanism_ms = ms[1];
+        out->kernel_timings.broadphase_ms = ms[2];
+        out->kernel_timings.narrowphase_ms = ms[3];
+        out->kernel_timings.contact_solver_ms = ms[4];
+        out->kernel_timings.bearings_ms = ms[5];
+        out->kernel_timings.snapshot_ms = ms[6];
+        double total = 0;
+        for (float m : ms) total += m;
+        out->gpu_tick_ms = total;
+    }
+    mk::read_mechanism_readback(h->mech, out);
+    return MK_OK;
+}
+
+int mk_read_snapshot(MkHandle* h, uint8_t slot, GpuTransform* out, uint32_t capacity, MkError* err) {
+    if (!h) return MK_ERR_INVALID_ARGUMENT;
+    if (slot >= 3) {
+        set_error(err, MK_ERR_INVALID_SNAPSHOT_SLOT, "snapshot slot %u is outside the published ring", slot);
+        if (err) err->slot = slot;
+        return MK_ERR_INVALID_SNAPSHOT_SLOT;
+    }
+    if (!out || capacity < h->B) {
+        set_error(err, MK_ERR_INVALID_ARGUMENT, "output holds %u rows, %u needed", capacity, h->B);
+        return MK_ERR_INVALID_ARGUMENT;
+    }
+    DeviceGuard guard(h->device);
+    cudaStream_t s = h->stream;
+    k_interleave<<<(h->B + 255) / 256, 256, 0, s>>>(h->buf.snap_pos + (size_t)slot * h->B,
+                                                     h->buf.snap_rot + (size_t)slot * h->B, h->staging, h->B);
+    cudaError_t e = cudaMemcpyAsync(out, h->staging, sizeof(GpuTransform) * h->B, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (!check(e, err, "read_snapshot")) return MK_ERR_DEVICE_FAILURE;
+    return MK_OK;
+}
+
+int mk_snapshot_buffers(MkHandle* h, uint8_t slot, void** positions, void** rotations, MkError* err) {
+    if (!h) return MK_ERR_INVALID_ARGUMENT;
+    if (slot >= 3) {
+        set_error(err, MK_ERR_INVALID_SNAPSHOT_SLOT, "snapshot slot %u is outside the published ring", slot);
+        if (err) err->slot = slot;
+        return MK_ERR_INVALID_SNAPSHOT_SLOT;
+    }
+    if (positions) *positions = h->buf.snap_pos + (size_t)slot * h->B;
+    if (rotations) *rotations = h->buf.snap_rot + (size_t)slot * h->B;
+    return MK_OK;
+}
+
+int mk_apply_impulse(MkHandle* h, uint32_t body, const float p[3], const float J[3], MkError* err) {
+    if (!h || !p || !J) return MK_ERR_INVALID_ARGUMENT;
+    if (body >= h->B) {
+        set_error(err, MK_ERR_BODY_INDEX_OUT_OF_RANGE, "body index %u is outside the uploaded body count %u", body, h->B);
+        if (err) { err->body_index = body; err->body_count = h->B; }
+        return MK_ERR_BODY_INDEX_OUT_OF_RANGE;
+    }
+    for (int k = 0; k < 3; ++k)
+        if (!std::isfinite(p[k]) || !std::isfinite(J[k])) {
+            set_error(err, MK_ERR_NON_FINITE, "external impulse point and vector must be finite");
+            return MK_ERR_NON_FINITE;
+        }
+    DeviceGuard guard(h->device);
+    cudaError_t e = mk::launch_apply_impulse(h->buf, body, make_float3(p[0], p[1], p[2]), make_float3(J[0], J[1], J[2]),
+                                             h->stream);
+    return check(e, err, "apply_impulse") ? MK_OK : MK_ERR_DEVICE_FAILURE;
+}
+
+int mk_write_drives(MkHandle* h, const GpuMechanismDrive* drives, uint32_t count, MkError* err) {
+    if (!h) return MK_ERR_INVALID_ARGUMENT;
+    if (count != h->Q) {
+        set_error(err, MK_ERR_DRIVE_STATE_COUNT, "drive state has %u rows but scene requires %u", count, h->Q);
+        if (err) { err->provided = count; err->required = h->Q; }
+        return MK_ERR_DRIVE_STATE_COUNT;
+    }
+    if (count == 0) return MK_OK;
+    DeviceGuard guard(h->device);
+    cudaError_t e = cudaMemcpyAsync(h->mech.drives, drives, sizeof(GpuMechanismDrive) * count, cudaMemcpyHostToDevice,
+                                    h->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    return check(e, err, "write_drives") ? MK_OK : MK_ERR_DEVICE_FAILURE;
+}
+
+int mk_init_coordinates(MkHandle* h, const GpuMechanismCoordinate* coords, uint32_t count, MkError* err) {
+    if (!h) return MK_ERR_INVALID_ARGUMENT;
+    if (count != h->Q) {
+        set_error(err, MK_ERR_COORDINATE_STATE_COUNT, "coordinate state has %u rows but scene requires %u", count,
+                  h->Q);
+        if (err) { err->provided = count; err->required = h->Q; }
+        return MK_ERR_COORDINATE_STATE_COUNT;
+    }
+    if (count == 0) return MK_OK;
+    DeviceGuard guard(h->device);
+    cudaError_t e = cudaMemcpyAsync(h->mech.coords, coords, sizeof(GpuMechanismCoordinate) * count,
+                                    cudaMemcpyHostToDevice, h->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    return check(e, err, "init_coordinates") ? MK_OK : MK_ERR_DEVICE_FAILURE;
+}
+
+uint32_t mk_body_count(const MkHandle* h) { return h ? h->B : 0u; }
+
+int mk_has_gpu_timestamps(const MkHandle* h) { return h ? 1 : 0; }
+
+int mk_state_buffers(MkHandle* h, MkDeviceState* out) {
+    if (!h || !out) return MK_ERR_INVALID_ARGUMENT;
+    out->positions = h->buf.pos;
+    out->rotations = h->buf.rot;
+    out->linear_velocities = h->buf.lin;
+    out->angular_velocities = h->buf.ang;
+    out->inverse_masses = const_cast<float*>(h->buf.inv_mass);
+    out->coordinates = h->mech.coords;
+    out->diagnostics = h->buf.diag;
+    out->stream = h->stream;
+    return MK_OK;
+}
+
+int mk_save_state(MkHandle* h, MkHostState* st, MkError* err) {
+    if (!h || !st) return MK_ERR_INVALID_ARGUMENT;
+    DeviceGuard guard(h->device);
+    cudaStream_t s = h->stream;
+    cudaError_t e = cudaStreamSynchronize(s);
+    const uint32_t B = h->B;
+    if (e == cudaSuccess && st->transforms) {
+        k_interleave<<<(B + 255) / 256, 256, 0, s>>>(h->buf.pos, h->buf.rot, h->staging, B);
+        e = cudaMemcpyAsync(st->transforms, h->staging, 32ull * B, cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    }
+    if (e == cudaSuccess && st->velocities) {
+        k_interleave<<<(B + 255) / 256, 256, 0, s>>>(h->buf.lin, h->buf.ang, h->staging, B);
+        e = cudaMemcpyAsync(st->velocities, h->staging, 32ull * B, cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    }
+    if (e == cudaSuccess && st->coordinates && h->Q)
+        e = cudaMemcpy(st->coordinates, h->mech.coords, sizeof(GpuMechanismCoordinate) * h->Q, cudaMemcpyDeviceToHost);
+    st->manifold_count = 0;
+    st->manifold_tick = 0;
+    if (e == cudaSuccess && h->collisions) {
+        mk::DevCounts counts;
+        e = cudaMemcpy(&counts, h->buf.counts, sizeof(counts), cudaMemcpyDeviceToHost);
+        const int prev = h->parity ^ 1;   // buffer written by the last completed tick
+        if (e == cudaSuccess && counts.prev_valid) {
+            const uint32_t n = counts.prev_contacts;
+            std::vector<GpuContact> rows(n);
+            std::vector<uint64_t> keys(n);
+            std::vector<uint32_t> feat(n);
+            e = cudaMemcpy(rows.data(), h->buf.contacts[prev], sizeof(GpuContact) * n, cudaMemcpyDeviceToHost);
+            if (e == cudaSuccess)
+                e = cudaMemcpy(keys.data(), h->buf.contact_keys[prev], 8ull * n, cudaMemcpyDeviceToHost);
+            if (e == cudaSuccess) e = cudaMemcpy(feat.data(), h->buf.features[prev], 4ull * n, cudaMemcpyDeviceToHost);
+            std::vector<uint32_t> order;
+            for (uint32_t k = 0; k < n; ++k)
+                if (feat[k] & (1u << 24)) order.push_back(k);
+            std::sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b2) { return keys[a] < keys[b2]; });
+            uint32_t m = 0;
+            for (uint32_t k : order) {
+                if (st->manifold_contacts && m < st->manifold_capacity) {
+                    GpuContact c = rows[k];
+                    c.metadata[2] = (uint32_t)(keys[k] >> 32);
+                    c.metadata[3] = (uint32_t)keys[k];
+                    std::memset(c.arm_b, 0, sizeof(c.arm_b));
+                    st->manifold_contacts[m] = c;
+                }
+                ++m;
+            }
+            st->manifold_count = m;
+            st->manifold_tick = counts.prev_tick;
+        }
+    }
+    return check(e, err, "save_state") ? MK_OK : MK_ERR_DEVICE_FAILURE;
+}
+
+int mk_load_state(MkHandle* h, const MkHostState* st, MkError* err) {
+    if (!h || !st) return MK_ERR_INVALID_ARGUMENT;
+    DeviceGuard guard(h->device);
+    cudaStream_t s = h->stream;
+    cudaError_t e = cudaStreamSynchronize(s);
+    const uint32_t B = h->B;
+    if (e == cudaSuccess && st->transforms) {
+        e = cudaMemcpyAsync(h->staging, st->transforms, 32ull * B, cudaMemcpyHostToDevice, s);
+        k_deinterleave<<<(B + 255) / 256, 256, 0, s>>>(h->staging, h->buf.pos, h->buf.rot, B);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    }
+    if (e == cudaSuccess && st->velocities) {
+        e = cudaMemcpyAsync(h->staging, st->velocities, 32ull * B, cudaMemcpyHostToDevice, s);
+        k_deinterleave<<<(B + 255) / 256, 256, 0, s>>>(h->staging, h->buf.lin, h->buf.ang, B);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    }
+    if (e == cudaSuccess && st->coordinates && h->Q)
+        e = cudaMemcpy(h->mech.coords, st->coordinates, sizeof(GpuMechanismCoordinate) * h->Q, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess && h->collisions) {
+        // The next tick reads the buffer of parity ^ 1 as its manifold.
+        const int prev = h->parity ^ 1;
+        const uint32_t n = st->manifold_contacts ? st->manifold_count : 0u;
+        if (n > h->pair_capacity) {
+            set_error(err, MK_ERR_INVALID_ARGUMENT, "manifold rows %u exceed pair capacity %u", n, h->pair_capacity);
+            return MK_ERR_INVALID_ARGUMENT;
+        }
+        std::vector<uint32_t> order(n);
+        std::vector<uint64_t> key(n);
+        for (uint32_t k = 0; k < n; ++k) {
+            order[k] = k;
+            key[k] = ((uint64_t)st->manifold_contacts[k].metadata[2] << 32) | st->manifold_contacts[k].metadata[3];
+        }
+        // narrowphase rows first, then ground rows, each sorted by key
+        std::sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b2) {
+            const bool ga = (uint32_t)key[a] == 0xffffffffu, gb = (uint32_t)key[b2] == 0xffffffffu;
+            if (ga != gb) return !ga;
+            return key[a] < key[b2];
+        });
+        std::vector<GpuContact> rows(n);
+        std::vector<uint64_t> keys(n);
+        std::vector<uint32_t> feat(n, 1u << 24);
+        uint32_t narrow = 0;
+        for (uint32_t k = 0; k < n; ++k) {
+            rows[k] = st->manifold_contacts[order[k]];
+            keys[k] = key[order[k]];
+            rows[k].metadata[2] = k;
+            rows[k].metadata[3] = 1;
+            if ((uint32_t)keys[k] != 0xffffffffu) ++narrow;
+        }
+        if (n) {
+            e = cudaMemcpy(h->buf.contacts[prev], rows.data(), sizeof(GpuContact) * n, cudaMemcpyHostToDevice);
+            if (e == cudaSuccess) e = cudaMemcpy(h->buf.contact_keys[prev], keys.data(), 8ull * n, cudaMemcpyHostToDevice);
+            if (e == cudaSuccess) e = cudaMemcpy(h->buf.features[prev], feat.data(), 4ull * n, cudaMemcpyHostToDevice);
+        }
+        mk::DevCounts counts;
+        if (e == cudaSuccess) e = cudaMemcpy(&counts, h->buf.counts, sizeof(counts), cudaMemcpyDeviceToHost);
+        counts.prev_narrow = narrow;
+        counts.prev_contacts = n;
+        counts.prev_tick = (uint32_t)st->manifold_tick;
+        counts.prev_valid = st->manifold_contacts ? 1u : 0u;
+        if (e == cudaSuccess) e = cudaMemcpy(h->buf.counts, &counts, sizeof(counts), cudaMemcpyHostToDevice);
+    }
+    return check(e, err, "load_state") ? MK_OK : MK_ERR_DEVICE_FAILURE;
+}
+
+int mk_read_buffer(MkHandle* h, uint32_t id, void* host, uint64_t cap_bytes, uint64_t* count, MkError* err) {
+    if (!h) return MK_ERR_INVALID_ARGUMENT;
+    DeviceGuard guard(h->device);
+    cudaError_t e = cudaStreamSynchronize(h->stream);
+    if (!check(e, err, "read_buffer sync")) return MK_ERR_DEVICE_FAILURE;
+    mk::DevCounts counts{};
+    e = cudaMemcpy(&counts, h->buf.counts, sizeof(counts), cudaMemcpyDeviceToHost);
+    const int last = h->parity ^ (h->collisions ? 1 : 0);   // parity written by the last tick
+    const void* src = nullptr;
+    uint64_t n = 0, row = 0;
+    const mk::StepBuffers& b = h->buf;
+    switch (id) {
+        case MK_BUF_SORTED_KEYS: src = b.skeys; n = h->C; row = 8; break;
+        case MK_BUF_SORTED_VALUES: src = b.svals; n = h->C; row = 4; break;
+        case MK_BUF_COLLIDER_AABBS: src = b.aabbs; n = h->C; row = 32; break;
+        case MK_BUF_NODE_CHILDREN: src = b.children; n = h->C ? h->C - 1 : 0; row = 8; break;
+        case MK_BUF_NODE_AABBS: src = b.node_aabbs; n = h->C ? 2ull * h->C - 1 : 0; row = 32; break;
+        case MK_BUF_PAIRS: src = b.pairs; n = counts.pairs; row = 8; break;
+        case MK_BUF_CONTACTS: src = b.contacts[last]; n = counts.contacts; row = 64; break;
+        case MK_BUF_ACTIVE: src = b.active; n = counts.active; row = 4; break;
+        case MK_BUF_COLLIDER_KEYS: src = b.keys; n = h->C; row = 8; break;
+        case MK_BUF_CONTACT_FEATURES: src = b.features[last]; n = counts.contacts; row = 4; break;
+        case MK_BUF_WORLD_MASSES: src = b.world_mass; n = h->B; row = 48; break;
+        case MK_BUF_LINKS: src = h->mech.links_final; n = h->mech.links_final ? h->B : 0; row = 48; break;
+        default:
+            set_error(err, MK_ERR_INVALID_ARGUMENT, "unknown buffer id %u", id);
+            return MK_ERR_INVALID_ARGUMENT;
+    }
+    if (count) *count = n;
+    if (!host) return MK_OK;
+    const uint64_t bytes = std::min<uint64_t>(n * row, cap_bytes);
+    if (e == cudaSuccess && bytes && src) e = cudaMemcpy(host, src, bytes, cudaMemcpyDeviceToHost);
+    return check(e, err, "read_buffer") ? MK_OK : MK_ERR_DEVICE_FAILURE;
+}
+
+uint64_t mk_op_sort_scratch_bytes(uint32_t n) { return mk::sort_scratch_bytes(n, 63); }
+
+int mk_op_sort_keys(const uint64_t* keys_in, const uint32_t* values_in, uint64_t* keys_out, uint32_t* values_out,
+                    uint32_t n, uint32_t key_bits, void* scratch, uint64_t scratch_bytes, void* stream) {
+    if (n == 0) return MK_OK;
+    if (!keys_in || !values_in || !keys_out || !values_out || !scratch || key_bits == 0 || key_bits > 64) {
+        set_error(nullptr, MK_ERR_INVALID_ARGUMENT, "sort: null pointer or key_bits outside 1..64");
+        return MK_ERR_INVALID_ARGUMENT;
+    }
+    if (scratch_bytes < mk::sort_scratch_bytes(n, key_bits) || ((uintptr_t)scratch & 255u)) {
+        set_error(nullptr, MK_ERR_INVALID_ARGUMENT, "sort: scratch too small or not 256-byte aligned");
+        return MK_ERR_INVALID_ARGUMENT;
+    }
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    // The error word lives at the end of the caller's scratch (inside the size).
+    uint32_t* flags = nullptr;
+    cudaError_t e = mk::launch_sort(keys_in, values_in, keys_out, values_out, n, nullptr, key_bits, scratch,
+                                    scratch_bytes, flags, (cudaStream_t)stream, sms);
+    if (e != cudaSuccess) {
+        set_error(nullptr, MK_ERR_DEVICE_FAILURE, "sort: %s", cudaGetErrorString(e));
+        return MK_ERR_DEVICE_FAILURE;
+    }
+    return MK_OK;
+}
+
+int mk_op_obb_sat(const float* boxes_a, const float* boxes_b, uint32_t count, float* np, uint32_t* features,
+                  void* stream) {
+    if (count == 0) return MK_OK;
+    if (!boxes_a || !boxes_b || !np || !features) return MK_ERR_INVALID_ARGUMENT;
+    cudaError_t e = mk::launch_obb_sat(boxes_a, boxes_b, count, np, features, (cudaStream_t)stream);
+    if (e != cudaSuccess) {
+        set_error(nullptr, MK_ERR_DEVICE_FAILURE, "obb_sat: %s", cudaGetErrorString(e));
+        return MK_ERR_DEVICE_FAILURE;
+    }
+    return MK_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,111 @@
+// mk_internal.h — host/device shared declarations of libmechanic_b200.
+#pragma once
+
+#include <algorithm>
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "../../include/mechanic_b200.h"
+
+namespace mk {
+
+inline uint64_t align256(uint64_t b) { return (b + 255) & ~255ull; }
+
+// Per-tick values the host writes before each graph launch (64 bytes).
+struct DevTick {
+    uint32_t tick_index;
+    uint32_t snapshot_slot;
+    uint32_t pad[14];
+};
+
+// Counts produced on the device during a tick.  `prev_*` describe the
+// contact list of the previous tick, which doubles as the manifold cache.
+struct DevCounts {
+    uint32_t pairs;            // candidate pairs stored (clamped to capacity)
+    uint32_t narrow;           // narrowphase contacts stored
+    uint32_t contacts;         // narrowphase + ground contacts stored
+    uint32_t active;           // active contacts
+    uint32_t prev_narrow;      // previous tick: narrowphase contacts
+    uint32_t prev_contacts;    // previous tick: all contacts
+    uint32_t prev_tick;        // previous tick index
+    uint32_t prev_valid;       // 1 when the previous list may be matched
+    uint32_t requested_contacts;
+    uint32_t pad[7];
+};
+
+// Solver-side constants of a handle.
+struct StepParams {
+    float dt, gravity, lin_damp, ang_damp;
+    uint32_t body_count, collider_count, pair_capacity, suppression_count;
+};
+
+// Launches implemented in mk_sort.cu.
+uint32_t sort_passes(uint32_t key_bits);
+uint64_t sort_scratch_bytes(uint32_t n, uint32_t key_bits);
+cudaError_t launch_sort(const uint64_t* keys_in, const uint32_t* vals_in, uint64_t* keys_out, uint32_t* vals_out,
+                        uint32_t n, const uint32_t* n_dev, uint32_t key_bits, void* scratch,
+                        uint64_t scratch_bytes, uint32_t* error_flags, cudaStream_t stream, int sm_count);
+
+// Device buffers of one handle's step (all device pointers).
+struct StepBuffers {
+    float4 *pos, *rot, *lin, *ang;
+    const float* inv_mass;
+    const float4* mass;          // GpuMass rows (4 x float4)
+    float4* world_mass;          // 3 x float4 per body
+    const uint32_t* root_flags;
+    const uint32_t* components;  // null unless mechanism self-collisions are disabled
+    int32_t* deltas;             // 6 per body
+    float4 *snap_pos, *snap_rot; // ring base, slot-major
+    const float4* colliders;     // GpuCollider rows (4 x float4)
+    float4* boxes;               // 3 x float4 per collider (world box)
+    float4* aabbs;               // 2 x float4 per collider
+    uint64_t* keys;              // per collider
+    uint32_t* values;            // identity
+    uint64_t* skeys;             // sorted
+    uint32_t* svals;
+    uint2* children;             // C-1
+    uint32_t* parents;           // 2C-1
+    uint32_t* visits;            // C-1
+    float4* node_aabbs;          // 2 x float4 per node
+    const uint2* suppressed;
+    uint32_t* pair_offsets;      // C + 1
+    uint2* pairs;                // pair_capacity
+    GpuContact* contacts[2];     // ping-pong, pair_capacity rows each
+    uint64_t* contact_keys[2];
+    uint32_t* features[2];
+    uint32_t* active;            // pair_capacity
+    uint64_t* lookback;          // look-back words for ordered compaction
+    uint64_t lookback_words;     // per site
+    uint32_t* tickets;           // 8 tile tickets
+    GpuDiagnostics* diag;
+    DevTick* tick;
+    DevCounts* counts;
+    void* sort_scratch;
+    uint64_t sort_scratch_bytes;
+};
+
+struct StepLaunch {
+    int sm_count;
+    uint32_t morton_mode;     // MK_MORTON_*
+    uint32_t iterations;
+    bool fuse_world_mass;     // no mechanism: integrate also writes world masses + snapshot
+    bool collisions;
+};
+
+// mk_step.cu
+cudaError_t launch_integrate(const StepBuffers& b, const StepParams& p, const StepLaunch& l, cudaStream_t s);
+cudaError_t launch_world_masses(const StepBuffers& b, const StepParams& p, cudaStream_t s);
+cudaError_t launch_snapshot(const StepBuffers& b, const StepParams& p, cudaStream_t s);
+cudaError_t launch_broadphase(const StepBuffers& b, const StepParams& p, const StepLaunch& l, int parity,
+                              cudaStream_t s);
+cudaError_t launch_narrowphase(const StepBuffers& b, const StepParams& p, const StepLaunch& l, int parity,
+                               cudaStream_t s);
+cudaError_t launch_contact_solver(const StepBuffers& b, const StepParams& p, const StepLaunch& l, int parity,
+                                  cudaStream_t s);
+cudaError_t launch_finish_tick(const StepBuffers& b, const StepParams& p, int parity, cudaStream_t s);
+cudaError_t launch_apply_impulse(const StepBuffers& b, uint32_t body, float3 point, float3 impulse,
+                                 cudaStream_t s);
+cudaError_t launch_obb_sat(const float* boxes_a, const float* boxes_b, uint32_t count, float* np,
+                           uint32_t* features, cudaStream_t s);
+
+}  // namespace mk

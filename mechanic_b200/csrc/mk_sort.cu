@@ -1,0 +1,225 @@
+// mk_sort.cu — stable LSD onesweep radix sort of (63-bit key, 32-bit value).
+//
+// Replaces the reference's bitonic network (lbvh.wgsl:132-217, 54-77
+// full-buffer passes per tick) with one histogram pass over the keys plus one
+// single-pass "onesweep" scatter per 8-bit digit: each tile ranks its keys
+// with warp match-any, publishes per-digit counts, and learns its global
+// offsets by decoupled look-back over the preceding tiles.  Stability
+// (equal keys keep input order) gives the reference's (code, index)
+// tie-break when the values are collider indices in ascending order.
+#include "mk_device.cuh"
+#include "mk_internal.h"
+
+namespace mk {
+
+constexpr uint32_t kSortThreads = 256;
+constexpr uint32_t kSortItems = 8;
+constexpr uint32_t kSortTile = kSortThreads * kSortItems;   // 2048 keys per tile
+constexpr uint32_t kRadixBins = 256;
+
+// 30-bit digit look-back words: bits 30-31 status, 0-29 count.
+constexpr uint32_t kDigitAggregate = 1u << 30;
+constexpr uint32_t kDigitInclusive = 2u << 30;
+constexpr uint32_t kDigitCountMask = (1u << 30) - 1;
+
+__global__ void __launch_bounds__(kSortThreads)
+k_radix_histogram(const uint64_t* __restrict__ keys, const uint32_t* __restrict__ n_ptr, uint32_t n_fixed,
+                  uint32_t passes, uint32_t* __restrict__ hist /* passes x 256 */) {
+    __shared__ uint32_t s_hist[8][kRadixBins];
+    const uint32_t n = n_ptr ? *n_ptr : n_fixed;
+    for (uint32_t i = threadIdx.x; i < 8 * kRadixBins; i += blockDim.x) (&s_hist[0][0])[i] = 0;
+    __syncthreads();
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        uint64_t k = keys[i];
+        for (uint32_t p = 0; p < passes; ++p) atomicAdd(&s_hist[p][(k >> (8 * p)) & 0xffu], 1u);
+    }
+    __syncthreads();
+    for (uint32_t i = threadIdx.x; i < passes * kRadixBins; i += blockDim.x) {
+        uint32_t v = (&s_hist[0][0])[i];
+        if (v) atomicAdd(&hist[i], v);
+    }
+}
+
+// Exclusive scan of each pass's 256-bin histogram (one block per pass).
+__global__ void __launch_bounds__(kRadixBins) k_radix_offsets(uint32_t* __restrict__ hist) {
+    __shared__ uint32_t scratch[33];
+    uint32_t* h = hist + blockIdx.x * kRadixBins;
+    uint32_t total;
+    uint32_t v = h[threadIdx.x];
+    uint32_t e = block_exclusive_scan(v, scratch, &total);
+    h[threadIdx.x] = e;
+}
+
+__device__ __forceinline__ uint32_t lanemask_lt() {
+    uint32_t m;
+    asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+    return m;
+}
+
+__global__ void __launch_bounds__(kSortThreads)
+k_radix_onesweep(const uint64_t* __restrict__ keys_in, const uint32_t* __restrict__ vals_in,
+                 uint64_t* __restrict__ keys_out, uint32_t* __restrict__ vals_out,
+                 const uint32_t* __restrict__ n_ptr, uint32_t n_fixed, uint32_t shift,
+                 const uint32_t* __restrict__ digit_offsets /* 256 */, uint32_t* __restrict__ lookback,
+                 uint32_t* __restrict__ ticket, uint32_t* __restrict__ error_flags) {
+    __shared__ uint64_t s_keys[kSortTile];
+    __shared__ uint32_t s_vals[kSortTile];
+    __shared__ uint32_t s_warp[kSortThreads / 32][kRadixBins];
+    __shared__ uint32_t s_local_start[kRadixBins];
+    __shared__ uint32_t s_global_base[kRadixBins];
+    __shared__ uint32_t s_scan[33];
+    __shared__ uint32_t s_tile;
+
+    const uint32_t n = n_ptr ? *n_ptr : n_fixed;
+    const uint32_t tiles = (n + kSortTile - 1) / kSortTile;
+    const uint32_t lane = lane_id(), w = warp_id();
+
+    for (;;) {
+        if (threadIdx.x == 0) s_tile = atomicAdd(ticket, 1u);
+        for (uint32_t i = threadIdx.x; i < (kSortThreads / 32) * kRadixBins; i += kSortThreads)
+            (&s_warp[0][0])[i] = 0;
+        __syncthreads();
+        const uint32_t tile = s_tile;
+        if (tile >= tiles) break;
+        const uint32_t tile_base = tile * kSortTile;
+
+        // ---- load (warp-striped) and rank within each warp, item by item
+        uint64_t k[kSortItems];
+        uint32_t v[kSortItems];
+        uint32_t rank[kSortItems];
+        uint32_t dig[kSortItems];
+#pragma unroll
+        for (uint32_t i = 0; i < kSortItems; ++i) {
+            uint32_t idx = tile_base + w * 32 * kSortItems + i * 32 + lane;
+            bool valid = idx < n;
+            k[i] = valid ? keys_in[idx] : 0ull;
+            v[i] = valid ? vals_in[idx] : 0u;
+            uint32_t d = valid ? (uint32_t)((k[i] >> shift) & 0xffu) : kRadixBins;
+            dig[i] = d;
+            uint32_t peers = __match_any_sync(0xffffffffu, d);
+            uint32_t leader = __ffs(peers) - 1;
+            uint32_t base = 0;
+            if (lane == leader && valid) base = s_warp[w][d];
+            base = __shfl_sync(0xffffffffu, base, leader);
+            rank[i] = base + __popc(peers & lanemask_lt());
+            if (lane == leader && valid) s_warp[w][d] = base + __popc(peers);
+            __syncwarp();
+        }
+        __syncthreads();
+
+        // ---- per digit: prefix over warps, tile count, tile-local start
+        const uint32_t d = threadIdx.x;   // kSortThreads == kRadixBins
+        uint32_t count = 0;
+#pragma unroll
+        for (uint32_t ww = 0; ww < kSortThreads / 32; ++ww) {
+            uint32_t c = s_warp[ww][d];
+            s_warp[ww][d] = count;
+            count += c;
+        }
+        uint32_t total;
+        uint32_t local_start = block_exclusive_scan(count, s_scan, &total);
+        s_local_start[d] = local_start;
+
+        // ---- decoupled look-back for digit d (one thread per digit)
+        uint32_t* lb = lookback + (size_t)tile * kRadixBins + d;
+        uint32_t prefix = 0;
+        if (tile == 0) {
+            st_release_u32(lb, kDigitInclusive | count);
+        } else {
+            st_release_u32(lb, kDigitAggregate | count);
+            int64_t t = (int64_t)tile - 1;
+            uint32_t spins = 0;
+            while (t >= 0) {
+                uint32_t s = ld_acquire_u32(lookback + (size_t)t * kRadixBins + d);
+                uint32_t status = s >> 30;
+                if (status == 0) {
+                    if (++spins > kSpinLimit) { if (error_flags) atomicOr(error_flags, MK_DEVICE_WAIT_TIMEOUT_FLAG); break; }
+                    continue;
+                }
+                prefix += s & kDigitCountMask;
+                if (status == 2) break;
+                --t;
+            }
+            st_release_u32(lb, kDigitInclusive | (prefix + count));
+        }
+        s_global_base[d] = digit_offsets[d] + prefix - local_start;
+        __syncthreads();
+
+        // ---- reorder through shared memory, then scatter by digit runs
+#pragma unroll
+        for (uint32_t i = 0; i < kSortItems; ++i) {
+            if (dig[i] < kRadixBins) {
+                uint32_t r = s_local_start[dig[i]] + s_warp[w][dig[i]] + rank[i];
+                s_keys[r] = k[i];
+                s_vals[r] = v[i];
+            }
+        }
+        __syncthreads();
+        for (uint32_t j = threadIdx.x; j < total; j += kSortThreads) {
+            uint64_t kk = s_keys[j];
+            uint32_t dd = (uint32_t)((kk >> shift) & 0xffu);
+            uint32_t dst = s_global_base[dd] + j;
+            keys_out[dst] = kk;
+            vals_out[dst] = s_vals[j];
+        }
+        __syncthreads();
+    }
+}
+
+uint32_t sort_passes(uint32_t key_bits) { return (key_bits + 7) / 8; }
+
+uint64_t sort_scratch_bytes(uint32_t n, uint32_t key_bits) {
+    uint32_t passes = sort_passes(key_bits);
+    uint64_t tiles = (n + kSortTile - 1) / kSortTile;
+    uint64_t b = 0;
+    b += align256((uint64_t)n * 8);                       // ping-pong keys
+    b += align256((uint64_t)n * 4);                       // ping-pong values
+    b += align256((uint64_t)passes * kRadixBins * 4);     // histograms / offsets
+    b += align256((uint64_t)passes * (tiles ? tiles : 1) * kRadixBins * 4);   // look-back words
+    b += align256((uint64_t)passes * 4);                  // tile tickets
+    return b;
+}
+
+// Stream-ordered sort.  `n_dev` (device count) may be null, then n is used;
+// with a device count, n is the capacity that sizes the grid and scratch.
+cudaError_t launch_sort(const uint64_t* keys_in, const uint32_t* vals_in, uint64_t* keys_out, uint32_t* vals_out,
+                        uint32_t n, const uint32_t* n_dev, uint32_t key_bits, void* scratch,
+                        uint64_t scratch_bytes, uint32_t* error_flags, cudaStream_t stream, int sm_count) {
+    if (n == 0) return cudaSuccess;
+    uint32_t passes = sort_passes(key_bits);
+    if (passes == 0 || passes > 8) return cudaErrorInvalidValue;
+    if (scratch_bytes < sort_scratch_bytes(n, key_bits)) return cudaErrorInvalidValue;
+    uint64_t tiles = (n + kSortTile - 1) / kSortTile;
+    char* p = (char*)scratch;
+    uint64_t* tmp_keys = (uint64_t*)p; p += align256((uint64_t)n * 8);
+    uint32_t* tmp_vals = (uint32_t*)p; p += align256((uint64_t)n * 4);
+    uint32_t* hist = (uint32_t*)p; p += align256((uint64_t)passes * kRadixBins * 4);
+    uint32_t* lookback = (uint32_t*)p; p += align256((uint64_t)passes * tiles * kRadixBins * 4);
+    uint32_t* tickets = (uint32_t*)p;
+    uint64_t zero_bytes = (uint64_t)((char*)tickets - (char*)hist) + passes * 4;
+    cudaError_t e = cudaMemsetAsync(hist, 0, zero_bytes, stream);
+    if (e != cudaSuccess) return e;
+    uint32_t hist_blocks = (uint32_t)std::min<uint64_t>((n + 4095) / 4096, (uint64_t)sm_count * 4);
+    if (hist_blocks == 0) hist_blocks = 1;
+    k_radix_histogram<<<hist_blocks, 256, 0, stream>>>(keys_in, n_dev, n, passes, hist);
+    k_radix_offsets<<<passes, kRadixBins, 0, stream>>>(hist);
+    uint32_t grid = (uint32_t)std::min<uint64_t>(tiles, (uint64_t)sm_count * 3);
+    if (grid == 0) grid = 1;
+    // passes alternate between (tmp, out) so that the last pass writes `out`.
+    const uint64_t* src_k = keys_in;
+    const uint32_t* src_v = vals_in;
+    for (uint32_t pass = 0; pass < passes; ++pass) {
+        bool to_out = ((passes - 1 - pass) % 2) == 0;
+        uint64_t* dk = to_out ? keys_out : tmp_keys;
+        uint32_t* dv = to_out ? vals_out : tmp_vals;
+        k_radix_onesweep<<<grid, kSortThreads, 0, stream>>>(src_k, src_v, dk, dv, n_dev, n, 8 * pass,
+                                                             hist + pass * kRadixBins,
+                                                             lookback + (size_t)pass * tiles * kRadixBins,
+                                                             tickets + pass, error_flags);
+        src_k = dk;
+        src_v = dv;
+    }
+    return cudaGetLastError();
+}
+
+}  // namespace mk

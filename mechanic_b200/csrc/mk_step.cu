@@ -1,0 +1,1065 @@
+// mk_step.cu — the plain rigid-body tick on sm_100a.
+//
+// Stage map (reference kernel -> this file):
+//   physics.wgsl integrate :92-132 + collision.wgsl update_world_masses
+//     :144-162 + snapshot.wgsl publish_snapshot :6-14       -> k_integrate
+//   lbvh.wgsl compute_morton :108-130                        -> k_collider_bounds
+//   lbvh.wgsl sort_* :132-217                                -> mk_sort.cu (onesweep)
+//   lbvh.wgsl build_topology :233-278                        -> k_karras
+//   lbvh.wgsl prepare_leaves + build_bounds :280-319         -> k_refit
+//   lbvh.wgsl traverse :361-398                              -> k_traverse<count|write> + k_scan_offsets
+//   collision.wgsl narrowphase :570-603                      -> k_narrowphase
+//   collision.wgsl generate_ground_contacts :622-664         -> k_ground
+//   collision.wgsl prepare_contacts :674-736                 -> k_prepare
+//   collision.wgsl warm_start / solve_accumulate :774-906    -> k_solve<warm>
+//   collision.wgsl solve_apply :1050-1069                    -> k_apply
+//   collision.wgsl persist_contacts :1071-1088               -> the contact list itself (ping-pong)
+//
+// Variable-size stages (pairs, contacts, active contacts) run as persistent
+// grids that take tiles in ticket order and append their output in
+// canonical order through a decoupled look-back, so the whole tick is a
+// fixed launch sequence (CUDA-graph friendly) with deterministic output.
+#include <cstdio>
+
+#include "mk_device.cuh"
+#include "mk_internal.h"
+
+namespace mk {
+
+constexpr uint32_t kBlock = 256;
+constexpr uint32_t kScanItems = 4;
+constexpr uint32_t kScanTile = kBlock * kScanItems;
+constexpr uint32_t kFixedScale = 1048576;   // FIXED_VELOCITY_SCALE (collision.wgsl:63)
+
+// ---------------------------------------------------------------- integrate
+// physics.wgsl:92-132, then (no mechanism) world inverse inertia
+// (collision.wgsl:134-162) and the snapshot ring copy (snapshot.wgsl:6-14):
+// positions do not change again during a plain tick.
+__device__ __forceinline__ f3 world_inverse_inertia_column(float4 r, const float4* m, f3 axis) {
+    f3 local = quat_rotate(conjq(r), axis);
+    f3 lr = xyz(m[1]) * local.x + xyz(m[2]) * local.y + xyz(m[3]) * local.z;
+    return quat_rotate(r, lr);
+}
+
+__device__ __forceinline__ void write_world_mass(float4* wm, float4 r, const float4* m) {
+    wm[0] = f4(world_inverse_inertia_column(r, m, mkf3(1, 0, 0)), m[0].x);
+    wm[1] = f4(world_inverse_inertia_column(r, m, mkf3(0, 1, 0)), 0.0f);
+    wm[2] = f4(world_inverse_inertia_column(r, m, mkf3(0, 0, 1)), 0.0f);
+}
+
+template <bool kFuse>
+__global__ void __launch_bounds__(kBlock) k_integrate(StepBuffers b, StepParams p) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= p.body_count) return;
+    float4 pos = b.pos[i], q = b.rot[i], l = b.lin[i], a = b.ang[i];
+    const float inv = b.inv_mass[i];
+    if (inv > 0.0f) {
+        l.y += p.gravity * p.dt;
+        f3 lv = xyz(l) * p.lin_damp;
+        l = f4(lv, l.w);
+        f3 av = xyz(a) * p.ang_damp;
+        a = f4(av, a.w);
+        if (b.root_flags[i] != 0u) {
+            f3 pv = xyz(pos) + xyz(l) * p.dt;
+            pos = f4(pv, pos.w);
+            float4 spin = f4(xyz(a), 0.0f);
+            float4 d = quat_multiply(spin, q);
+            const float h = 0.5f * p.dt;
+            q = make_float4(q.x + d.x * h, q.y + d.y * h, q.z + d.z * h, q.w + d.w * h);
+            float ns = dot4(q, q);
+            if (ns > 1.0e-20f) {
+                float s = rsqrt_ieee(ns);
+                q = make_float4(q.x * s, q.y * s, q.z * s, q.w * s);
+            } else {
+                q = make_float4(0.0f, 0.0f, 0.0f, 1.0f);
+                atomicOr(&b.diag->error_flags, MK_INVALID_NUMERIC_FLAG);
+            }
+        }
+    }
+    bool ok = finite4(pos) && finite4(q) && finite4(l) && finite4(a);
+    if (!ok) {
+        atomicOr(&b.diag->error_flags, MK_INVALID_NUMERIC_FLAG);
+        pos = b.pos[i];
+        q = b.rot[i];
+    } else {
+        b.pos[i] = pos;
+        b.rot[i] = q;
+        b.lin[i] = l;
+        b.ang[i] = a;
+    }
+    if (kFuse) {
+        const float4* m = b.mass + 4ull * i;
+        float4 mr[4] = {__ldg(m), __ldg(m + 1), __ldg(m + 2), __ldg(m + 3)};
+        write_world_mass(b.world_mass + 3ull * i, q, mr);
+        const uint32_t slot = b.tick->snapshot_slot;
+        b.snap_pos[(size_t)slot * p.body_count + i] = pos;
+        b.snap_rot[(size_t)slot * p.body_count + i] = q;
+    }
+}
+
+__global__ void __launch_bounds__(kBlock) k_world_masses(StepBuffers b, StepParams p) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= p.body_count) return;
+    const float4* m = b.mass + 4ull * i;
+    float4 mr[4] = {__ldg(m), __ldg(m + 1), __ldg(m + 2), __ldg(m + 3)};
+    write_world_mass(b.world_mass + 3ull * i, b.rot[i], mr);
+}
+
+__global__ void __launch_bounds__(kBlock) k_snapshot(StepBuffers b, StepParams p) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= p.body_count) return;
+    const uint32_t slot = b.tick->snapshot_slot;
+    b.snap_pos[(size_t)slot * p.body_count + i] = b.pos[i];
+    b.snap_rot[(size_t)slot * p.body_count + i] = b.rot[i];
+}
+
+// ------------------------------------------------------------ bounds/Morton
+__device__ __forceinline__ uint32_t expand10(uint32_t v) {
+    v &= 0x3ffu;
+    v = (v | (v << 16)) & 0x030000ffu;
+    v = (v | (v << 8)) & 0x0300f00fu;
+    v = (v | (v << 4)) & 0x030c30c3u;
+    v = (v | (v << 2)) & 0x09249249u;
+    return v;
+}
+__device__ __forceinline__ uint64_t expand21(uint64_t v) {
+    v &= 0x1fffffull;
+    v = (v | (v << 32)) & 0x1f00000000ffffull;
+    v = (v | (v << 16)) & 0x1f0000ff0000ffull;
+    v = (v | (v << 8)) & 0x100f00f00f00f00full;
+    v = (v | (v << 4)) & 0x10c30c30c30c30c3ull;
+    v = (v | (v << 2)) & 0x1249249249249249ull;
+    return v;
+}
+// lbvh.wgsl:93-98: 10 bits per axis over 1 m cells in [-512, 512).
+__device__ __forceinline__ uint32_t morton30(f3 c) {
+    uint32_t qx = (uint32_t)clampf(floorf(c.x + 512.0f), 0.0f, 1023.0f);
+    uint32_t qy = (uint32_t)clampf(floorf(c.y + 512.0f), 0.0f, 1023.0f);
+    uint32_t qz = (uint32_t)clampf(floorf(c.z + 512.0f), 0.0f, 1023.0f);
+    return expand10(qx) | (expand10(qy) << 1) | (expand10(qz) << 2);
+}
+// 21 bits per axis over the same [-512, 512) box: 2048 cells per metre.
+__device__ __forceinline__ uint64_t morton63(f3 c) {
+    uint64_t qx = (uint64_t)clampf(floorf((c.x + 512.0f) * 2048.0f), 0.0f, 2097151.0f);
+    uint64_t qy = (uint64_t)clampf(floorf((c.y + 512.0f) * 2048.0f), 0.0f, 2097151.0f);
+    uint64_t qz = (uint64_t)clampf(floorf((c.z + 512.0f) * 2048.0f), 0.0f, 2097151.0f);
+    return expand21(qx) | (expand21(qy) << 1) | (expand21(qz) << 2);
+}
+
+// lbvh.wgsl:108-130 plus the world box row the narrowphase reads:
+// box r0 = {center, half.x}, r1 = world rotation, r2 = {half.y, half.z, body, role}.
+__global__ void __launch_bounds__(kBlock) k_collider_bounds(StepBuffers b, StepParams p, uint32_t morton_mode) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= p.collider_count) return;
+    const float4* c = b.colliders + 4ull * i;
+    const float4 lc = __ldg(c), lr = __ldg(c + 1), he = __ldg(c + 2);
+    const uint4 meta = __ldg(reinterpret_cast<const uint4*>(c + 3));
+    const uint32_t body = meta.x;
+    const float4 bq = b.rot[body];
+    const f3 center = xyz(b.pos[body]) + quat_rotate(bq, xyz(lc));
+    const float4 r = quat_multiply(bq, lr);
+    const f3 ax = quat_rotate(r, mkf3(1, 0, 0));
+    const f3 ay = quat_rotate(r, mkf3(0, 1, 0));
+    const f3 az = quat_rotate(r, mkf3(0, 0, 1));
+    const f3 e = absf3(ax) * he.x + absf3(ay) * he.y + absf3(az) * he.z;
+    b.aabbs[2ull * i] = f4(center - e, 0.0f);
+    b.aabbs[2ull * i + 1] = f4(center + e, 0.0f);
+    float4* box = b.boxes + 3ull * i;
+    box[0] = f4(center, he.x);
+    box[1] = r;
+    box[2] = make_float4(he.y, he.z, __uint_as_float(body), __uint_as_float(meta.w));
+    b.keys[i] = morton_mode == MK_MORTON_REFERENCE_30 ? (uint64_t)morton30(center) : morton63(center);
+    b.values[i] = i;
+}
+
+// ------------------------------------------------------------- Karras tree
+__device__ __forceinline__ int common_prefix(const uint64_t* __restrict__ k, const uint32_t* __restrict__ v,
+                                             int n, int i, int j) {
+    if (j < 0 || j >= n) return -1;
+    uint64_t d = k[i] ^ k[j];
+    if (d != 0) return __clzll((long long)d);
+    return 64 + __clz((int)(v[i] ^ v[j]));
+}
+
+// lbvh.wgsl:219-278 (Karras 2012) over (key, index) entries.
+__global__ void __launch_bounds__(kBlock) k_karras(StepBuffers b, StepParams p) {
+    const int n = (int)p.collider_count;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i == 0) b.parents[0] = 0u;
+    if (n <= 1 || i >= n - 1) return;
+    const uint64_t* k = b.skeys;
+    const uint32_t* v = b.svals;
+    const int dir = common_prefix(k, v, n, i, i + 1) > common_prefix(k, v, n, i, i - 1) ? 1 : -1;
+    const int min_prefix = common_prefix(k, v, n, i, i - dir);
+    int max_len = 2;
+    while (common_prefix(k, v, n, i, i + max_len * dir) > min_prefix) max_len *= 2;
+    int len = 0;
+    for (int step = max_len / 2; step >= 1; step /= 2)
+        if (common_prefix(k, v, n, i, i + (len + step) * dir) > min_prefix) len += step;
+    const int other = i + len * dir;
+    const int node_prefix = common_prefix(k, v, n, i, other);
+    int split_off = 0;
+    int step = (len + 1) / 2;
+    while (step >= 1) {
+        if (common_prefix(k, v, n, i, i + (split_off + step) * dir) > node_prefix) split_off += step;
+        if (step == 1) break;
+        step = (step + 1) / 2;
+    }
+    const int split = i + split_off * dir + min(dir, 0);
+    const int first = min(i, other), last = max(i, other);
+    const uint32_t leaf_base = (uint32_t)(n - 1);
+    const uint32_t left = split == first ? leaf_base + (uint32_t)split : (uint32_t)split;
+    const uint32_t right = split + 1 == last ? leaf_base + (uint32_t)(split + 1) : (uint32_t)(split + 1);
+    b.children[i] = make_uint2(left, right);
+    b.parents[left] = (uint32_t)i + 1u;
+    b.parents[right] = (uint32_t)i + 1u;
+}
+
+// lbvh.wgsl:280-319: leaf boxes in sorted order, then a bottom-up climb where
+// the second arrival at a node writes the union.  min.w carries the largest
+// collider index below the node (prunes the j > i query).
+__global__ void __launch_bounds__(kBlock) k_refit(StepBuffers b, StepParams p) {
+    const uint32_t n = p.collider_count;
+    const uint32_t leaf = blockIdx.x * blockDim.x + threadIdx.x;
+    if (leaf >= n) return;
+    const uint32_t leaf_base = n - 1;
+    const uint32_t j = b.svals[leaf];
+    float4 mn = b.aabbs[2ull * j], mx = b.aabbs[2ull * j + 1];
+    mn.w = __uint_as_float(j);
+    uint32_t cur = leaf_base + leaf;
+    b.node_aabbs[2ull * cur] = mn;
+    b.node_aabbs[2ull * cur + 1] = mx;
+    if (n <= 1) return;
+    __threadfence();
+    for (uint32_t guard = 0; guard < 2 * n; ++guard) {
+        const uint32_t ep = b.parents[cur];
+        if (ep == 0u) return;
+        const uint32_t parent = ep - 1u;
+        const uint32_t arrival = atomicAdd(&b.visits[parent], 1u);
+        if (arrival == 0u) return;
+        if (arrival > 1u) {
+            atomicOr(&b.diag->error_flags, MK_PAIR_OVERFLOW_FLAG);
+            return;
+        }
+        const uint2 ch = b.children[parent];
+        const float4 lmn = __ldcg(b.node_aabbs + 2ull * ch.x), lmx = __ldcg(b.node_aabbs + 2ull * ch.x + 1);
+        const float4 rmn = __ldcg(b.node_aabbs + 2ull * ch.y), rmx = __ldcg(b.node_aabbs + 2ull * ch.y + 1);
+        float4 pm = make_float4(mnf(lmn.x, rmn.x), mnf(lmn.y, rmn.y), mnf(lmn.z, rmn.z),
+                                __uint_as_float(max(__float_as_uint(lmn.w), __float_as_uint(rmn.w))));
+        float4 px = make_float4(mxf(lmx.x, rmx.x), mxf(lmx.y, rmx.y), mxf(lmx.z, rmx.z), 0.0f);
+        b.node_aabbs[2ull * parent] = pm;
+        b.node_aabbs[2ull * parent + 1] = px;
+        __threadfence();
+        cur = parent;
+    }
+}
+
+// ---------------------------------------------------------------- traverse
+__device__ __forceinline__ bool overlaps(float4 amin, float4 amax, float4 bmin, float4 bmax) {
+    return amin.x <= bmax.x && amin.y <= bmax.y && amin.z <= bmax.z && bmin.x <= amax.x && bmin.y <= amax.y &&
+           bmin.z <= amax.z;
+}
+
+// lbvh.wgsl:325-345 (binary search over sorted suppressed body pairs).
+__device__ __forceinline__ bool pair_is_suppressed(const uint2* __restrict__ sup, uint32_t count, uint32_t a,
+                                                   uint32_t c) {
+    const uint32_t low = min(a, c), high = max(a, c);
+    uint32_t left = 0, right = count;
+    while (left < right) {
+        const uint32_t mid = left + (right - left) / 2u;
+        const uint2 cand = __ldg(sup + mid);
+        if (cand.x < low || (cand.x == low && cand.y < high)) left = mid + 1u;
+        else right = mid;
+    }
+    if (left >= count) return false;
+    const uint2 hit = __ldg(sup + left);
+    return hit.x == low && hit.y == high;
+}
+
+constexpr uint32_t kStack = 64;
+constexpr uint32_t kLocalPairs = 48;
+
+// One query per collider index i: every leaf j > i of another, unsuppressed
+// body whose box overlaps i's box (the pair set of lbvh.wgsl:361-398, with
+// (i, j) ordered as the reference emits them).  kWrite=false counts,
+// kWrite=true writes at the scanned offset and sorts the segment by j.
+template <bool kWrite>
+__global__ void __launch_bounds__(128) k_traverse(StepBuffers b, StepParams p) {
+    const uint32_t n = p.collider_count;
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float4 qmin = b.aabbs[2ull * i], qmax = b.aabbs[2ull * i + 1];
+    const uint32_t body_i = __float_as_uint(b.boxes[3ull * i + 2].z);
+    const uint32_t leaf_base = n - 1;
+    uint32_t stack[kStack];
+    uint32_t sp = 1;
+    stack[0] = n > 1 ? 0u : leaf_base;
+    uint32_t count = 0;
+    uint32_t base = 0, cap_left = 0;
+    uint32_t local[kLocalPairs];
+    if (kWrite) {
+        base = b.pair_offsets[i];
+        cap_left = base < p.pair_capacity ? p.pair_capacity - base : 0u;
+    }
+    while (sp > 0) {
+        const uint32_t node = stack[--sp];
+        const float4 nmin = __ldg(b.node_aabbs + 2ull * node);
+        if (__float_as_uint(nmin.w) <= i) continue;   // no collider index above i below this node
+        const float4 nmax = __ldg(b.node_aabbs + 2ull * node + 1);
+        if (!overlaps(qmin, qmax, nmin, nmax)) continue;
+        if (node >= leaf_base) {
+            const uint32_t j = __float_as_uint(nmin.w);
+            const uint32_t body_j = __float_as_uint(__ldg(b.boxes + 3ull * j + 2).z);
+            if (body_i == body_j) continue;
+            if (p.suppression_count && pair_is_suppressed(b.suppressed, p.suppression_count, body_i, body_j)) continue;
+            if (kWrite) {
+                if (count < kLocalPairs) local[count] = j;
+                else if (count < cap_left) b.pairs[base + count] = make_uint2(i, j);
+            }
+            ++count;
+            continue;
+        }
+        if (sp > kStack - 3) {   // lbvh.wgsl:389-392
+            atomicOr(&b.diag->error_flags, MK_PAIR_OVERFLOW_FLAG);
+            break;
+        }
+        const uint2 ch = __ldg(b.children + node);
+        stack[sp] = ch.x;
+        stack[sp + 1] = ch.y;
+        sp += 2;
+    }
+    if (!kWrite) {
+        b.pair_offsets[i] = count;
+        return;
+    }
+    const uint32_t stored = min(count, cap_left);
+    if (count <= kLocalPairs) {
+        // insertion sort in registers/local memory, then one write pass
+        for (uint32_t x = 1; x < count; ++x) {
+            uint32_t v = local[x];
+            int y = (int)x - 1;
+            while (y >= 0 && local[y] > v) { local[y + 1] = local[y]; --y; }
+            local[y + 1] = v;
+        }
+        for (uint32_t x = 0; x < stored; ++x) b.pairs[base + x] = make_uint2(i, local[x]);
+    } else {
+        uint2* seg = b.pairs + base;
+        for (uint32_t x = 0; x < kLocalPairs && x < stored; ++x) seg[x] = make_uint2(i, local[x]);
+        for (uint32_t x = 1; x < stored; ++x) {
+            uint2 v = seg[x];
+            int y = (int)x - 1;
+            while (y >= 0 && seg[y].y > v.y) { seg[y + 1] = seg[y]; --y; }
+            seg[y + 1] = v;
+        }
+    }
+}
+
+// Exclusive scan of the per-collider pair counts (single pass, look-back).
+__global__ void __launch_bounds__(kBlock) k_scan_offsets(StepBuffers b, StepParams p) {
+    __shared__ uint32_t s_scan[33];
+    __shared__ uint32_t s_tile;
+    __shared__ uint64_t s_prefix;
+    const uint32_t n = p.collider_count;
+    const uint32_t tiles = (n + kScanTile - 1) / kScanTile;
+    uint64_t* states = b.lookback;
+    for (;;) {
+        if (threadIdx.x == 0) s_tile = atomicAdd(&b.tickets[0], 1u);
+        __syncthreads();
+        const uint32_t tile = s_tile;
+        if (tile >= tiles) break;
+        const uint32_t base = tile * kScanTile + threadIdx.x * kScanItems;
+        uint32_t v[kScanItems];
+        uint32_t sum = 0;
+#pragma unroll
+        for (uint32_t k = 0; k < kScanItems; ++k) {
+            v[k] = base + k < n ? b.pair_offsets[base + k] : 0u;
+            sum += v[k];
+        }
+        uint32_t total;
+        const uint32_t ex = block_exclusive_scan(sum, s_scan, &total);
+        if (warp_id() == 0) {
+            uint64_t pre = tile_lookback(states, tile, total, &b.diag->error_flags);
+            if (lane_id() == 0) s_prefix = pre;
+        }
+        __syncthreads();
+        const uint64_t pre = s_prefix;
+        uint64_t run = pre + ex;
+#pragma unroll
+        for (uint32_t k = 0; k < kScanItems; ++k) {
+            if (base + k < n) b.pair_offsets[base + k] = (uint32_t)umin64(run, 0xffffffffull);
+            run += v[k];
+        }
+        if (tile == tiles - 1 && threadIdx.x == 0) {
+            const uint64_t all = pre + total;
+            b.pair_offsets[n] = (uint32_t)umin64(all, 0xffffffffull);
+            b.diag->pair_count = (uint32_t)umin64(all, 0xffffffffull);
+            b.counts->pairs = (uint32_t)umin64(all, p.pair_capacity);
+            if (all > p.pair_capacity) atomicOr(&b.diag->error_flags, MK_PAIR_OVERFLOW_FLAG);
+        }
+        __syncthreads();
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0 && tiles == 0) {
+        b.pair_offsets[n] = 0;
+        b.diag->pair_count = 0;
+        b.counts->pairs = 0;
+    }
+}
+
+// ------------------------------------------------------------- narrowphase
+struct Box {
+    f3 c;
+    float4 q;
+    f3 ax[3];
+    float h[3];
+};
+
+__device__ __forceinline__ Box make_box(const float4* boxes, uint32_t i) {
+    const float4* p = boxes + 3ull * i;
+    const float4 r0 = __ldg(p), r1 = __ldg(p + 1), r2 = __ldg(p + 2);
+    Box o;
+    o.c = xyz(r0);
+    o.q = r1;
+    o.h[0] = r0.w;
+    o.h[1] = r2.x;
+    o.h[2] = r2.y;
+    o.ax[0] = quat_rotate(r1, mkf3(1, 0, 0));
+    o.ax[1] = quat_rotate(r1, mkf3(0, 1, 0));
+    o.ax[2] = quat_rotate(r1, mkf3(0, 0, 1));
+    return o;
+}
+
+struct Sat { f3 n; float pen; uint32_t near; uint32_t axis; uint32_t early; };
+
+__device__ __forceinline__ float projection_radius(const Box& o, f3 axis) {
+    return fabsf(dot(o.ax[0], axis)) * o.h[0] + fabsf(dot(o.ax[1], axis)) * o.h[1] + fabsf(dot(o.ax[2], axis)) * o.h[2];
+}
+
+// collision.wgsl:399-420
+__device__ __forceinline__ Sat test_axis(f3 delta, const Box& a, const Box& b, f3 raw, uint32_t idx) {
+    const float l2 = dot(raw, raw);
+    if (l2 < 1.0e-10f) return {mkf3(1, 0, 0), kFloatMax, 0u, idx, 0u};
+    f3 axis = raw * rsqrt_ieee(l2);
+    const float sd = dot(delta, axis);
+    const float pen = projection_radius(a, axis) + projection_radius(b, axis) - fabsf(sd);
+    if (sd < 0.0f) axis = -axis;
+    return {axis, pen, 0u, idx, 0u};
+}
+
+// collision.wgsl:422-486: axes A0 B0 A1 B1 A2 B2 then Ai x Bj, first negative
+// penetration returns immediately.
+__device__ Sat obb_sat(const Box& a, const Box& b) {
+    const f3 delta = b.c - a.c;
+    Sat best = {mkf3(1, 0, 0), kFloatMax, 0u, 0u, 0u};
+    uint32_t near = 0;
+#pragma unroll
+    for (uint32_t i = 0; i < 3; ++i) {
+        Sat ra = test_axis(delta, a, b, a.ax[i], 2 * i);
+        if (ra.pen < 0.0f) { ra.early = 1; return ra; }
+        if (ra.pen <= 1.0e-4f) near += 1;
+        if (ra.pen < best.pen) best = ra;
+        Sat rb = test_axis(delta, a, b, b.ax[i], 2 * i + 1);
+        if (rb.pen < 0.0f) { rb.early = 1; return rb; }
+        if (rb.pen <= 1.0e-4f) near += 1;
+        if (rb.pen < best.pen) best = rb;
+    }
+#pragma unroll
+    for (uint32_t i = 0; i < 3; ++i)
+#pragma unroll
+        for (uint32_t j = 0; j < 3; ++j) {
+            Sat r = test_axis(delta, a, b, cross(a.ax[i], b.ax[j]), 6 + 3 * i + j);
+            if (r.pen < 0.0f) { r.early = 1; return r; }
+            if (r.pen < best.pen) best = r;
+        }
+    best.near = near;
+    return best;
+}
+
+// collision.wgsl:175-191 (box support) and :240-287 (averaged contact point).
+__device__ __forceinline__ f3 support_point(const Box& o, f3 dir) {
+    f3 p = o.c;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        const float proj = dot(o.ax[a], dir);
+        if (fabsf(proj) > 1.0e-5f) p = p + o.ax[a] * o.h[a] * sgnf(proj);
+    }
+    return p;
+}
+__device__ __forceinline__ f3 vertex(const Box& o, uint32_t v) {
+    f3 p = o.c;
+#pragma unroll
+    for (uint32_t a = 0; a < 3; ++a) {
+        const float d = (v & (1u << a)) ? 1.0f : -1.0f;
+        p = p + o.ax[a] * o.h[a] * d;
+    }
+    return p;
+}
+__device__ __forceinline__ bool contains(const Box& o, f3 pt) {
+    const f3 l = quat_rotate(conjq(o.q), pt - o.c);
+    return fabsf(l.x) <= o.h[0] + 1.0e-5f && fabsf(l.y) <= o.h[1] + 1.0e-5f && fabsf(l.z) <= o.h[2] + 1.0e-5f;
+}
+__device__ f3 contact_point(const Box& a, const Box& b, f3 n) {
+    f3 sum = mkf3(0, 0, 0);
+    float count = 0.0f;
+#pragma unroll 1
+    for (uint32_t v = 0; v < 8; ++v) {
+        const f3 pa = vertex(a, v);
+        if (contains(b, pa)) { sum = sum + pa; count += 1.0f; }
+        const f3 pb = vertex(b, v);
+        if (contains(a, pb)) { sum = sum + pb; count += 1.0f; }
+    }
+    if (count > 0.0f) return sum / count;
+    const f3 pa = support_point(a, n), pb = support_point(b, -n);
+    return (pa + pb) * 0.5f;
+}
+
+__device__ __forceinline__ void store_contact(GpuContact* dst, uint32_t ba, uint32_t bb, uint32_t ca, uint32_t cb,
+                                              float4 np, float4 aa, float4 ab) {
+    float4* d = reinterpret_cast<float4*>(dst);
+    d[0] = make_float4(__uint_as_float(ba), __uint_as_float(bb), __uint_as_float(ca), __uint_as_float(cb));
+    d[1] = np;
+    d[2] = aa;
+    d[3] = ab;
+}
+
+// Persistent ordered append over tiles of kBlock items.  The functor decides
+// per item whether it emits; emitted items are written in item order.
+struct AppendSite {
+    uint64_t* states;
+    uint32_t* ticket;
+};
+
+__device__ __forceinline__ uint32_t take_tile(uint32_t* ticket, uint32_t* s_tile) {
+    if (threadIdx.x == 0) *s_tile = atomicAdd(ticket, 1u);
+    __syncthreads();
+    uint32_t t = *s_tile;
+    __syncthreads();
+    return t;
+}
+
+// collision.wgsl:570-620 (narrowphase with the optional self-collision filter).
+__global__ void __launch_bounds__(kBlock) k_narrowphase(StepBuffers b, StepParams p, AppendSite site,
+                                                        GpuContact* out, uint64_t* out_keys, uint32_t* out_feat) {
+    __shared__ uint32_t s_scan[33];
+    __shared__ uint32_t s_tile;
+    __shared__ uint64_t s_prefix;
+    const uint32_t n = b.counts->pairs;
+    const uint32_t tiles = (n + kBlock - 1) / kBlock;
+    for (;;) {
+        const uint32_t tile = take_tile(site.ticket, &s_tile);
+        if (tile >= tiles) break;
+        const uint32_t idx = tile * kBlock + threadIdx.x;
+        bool emit = false;
+        uint2 pr = make_uint2(0, 0);
+        Sat s;
+        f3 pt = mkf3(0, 0, 0);
+        uint32_t ba = 0, bb = 0;
+        if (idx < n) {
+            pr = b.pairs[idx];
+            const Box A = make_box(b.boxes, pr.x), Bx = make_box(b.boxes, pr.y);
+            ba = __float_as_uint(__ldg(b.boxes + 3ull * pr.x + 2).z);
+            bb = __float_as_uint(__ldg(b.boxes + 3ull * pr.y + 2).z);
+            bool skip = b.components && __ldg(b.components + ba) == __ldg(b.components + bb);
+            if (!skip) {
+                s = obb_sat(A, Bx);
+                if (!(s.pen < -1.0e-5f)) {
+                    pt = contact_point(A, Bx, s.n);
+                    emit = true;
+                }
+            }
+        }
+        uint32_t total;
+        const uint32_t ex = block_exclusive_scan(emit ? 1u : 0u, s_scan, &total);
+        if (warp_id() == 0) {
+            uint64_t pre = tile_lookback(site.states, tile, total, &b.diag->error_flags);
+            if (lane_id() == 0) s_prefix = pre;
+        }
+        __syncthreads();
+        const uint64_t pre = s_prefix;
+        if (emit) {
+            const uint64_t o = pre + ex;
+            if (o < p.pair_capacity) {
+                const f3 xa = xyz(b.pos[ba]), xb = xyz(b.pos[bb]);
+                store_contact(out + o, ba, bb, pr.x, pr.y, f4(s.n, mxf(s.pen, 0.0f)), f4(pt - xa, 0.0f),
+                              f4(pt - xb, (float)s.near));
+                out_keys[o] = ((uint64_t)pr.x << 32) | pr.y;
+                out_feat[o] = s.axis | (s.near << 8) | (s.early << 16);
+            }
+        }
+        if (tile == tiles - 1 && threadIdx.x == 0) {
+            const uint64_t all = pre + total;
+            b.counts->narrow = (uint32_t)umin64(all, p.pair_capacity);
+            b.counts->requested_contacts = (uint32_t)umin64(all, 0xffffffffull);
+        }
+        __syncthreads();
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0 && tiles == 0) {
+        b.counts->narrow = 0;
+        b.counts->requested_contacts = 0;
+    }
+}
+
+// collision.wgsl:175-238 and :622-664: analytic contact with the y = 0 plane.
+__global__ void __launch_bounds__(kBlock) k_ground(StepBuffers b, StepParams p, AppendSite site, GpuContact* out,
+                                                   uint64_t* out_keys, uint32_t* out_feat) {
+    __shared__ uint32_t s_scan[33];
+    __shared__ uint32_t s_tile;
+    __shared__ uint64_t s_prefix;
+    const uint32_t n = p.collider_count;
+    const uint32_t tiles = (n + kBlock - 1) / kBlock;
+    const uint32_t narrow = b.counts->narrow;
+    const uint32_t requested_narrow = b.counts->requested_contacts;
+    for (;;) {
+        const uint32_t tile = take_tile(site.ticket, &s_tile);
+        if (tile >= tiles) break;
+        const uint32_t i = tile * kBlock + threadIdx.x;
+        bool emit = false;
+        f3 sp = mkf3(0, 0, 0);
+        uint32_t body = 0, role = 0;
+        if (i < n) {
+            const Box o = make_box(b.boxes, i);
+            const float4 r2 = __ldg(b.boxes + 3ull * i + 2);
+            body = __float_as_uint(r2.z);
+            role = __float_as_uint(r2.w);
+            const f3 down = mkf3(0, -1, 0);
+            sp = support_point(o, down);
+            bool skip = false;
+            if (role != 0u) {
+                const float center_radius = __ldg(b.colliders + 4ull * i).w;
+                const float outer_radius = __ldg(b.colliders + 4ull * i + 2).w;
+                const f3 caxis = o.ax[1];
+                const float ap = dot(caxis, down);
+                const f3 radial = down - caxis * ap;
+                const float rl = length(radial);
+                const uint32_t cc = rl < 0.05f ? 4u : 1u;
+                if (role > cc) {
+                    skip = true;
+                } else {
+                    f3 q = o.c - o.ax[0] * center_radius;
+                    if (rl < 0.05f) {
+                        q = q + caxis * sgnf(ap) * o.h[1];
+                        const f3 ta = normalize(mkf3(1, 0, 0) - caxis * caxis.x);
+                        const f3 tb = normalize(cross(caxis, ta));
+                        if (role == 1u) q = q + ta * outer_radius;
+                        else if (role == 2u) q = q - ta * outer_radius;
+                        else if (role == 3u) q = q + tb * outer_radius;
+                        else q = q - tb * outer_radius;
+                    } else {
+                        q = q + radial * (outer_radius / rl);
+                        if (fabsf(ap) >= 0.05f) q = q + caxis * sgnf(ap) * o.h[1];
+                    }
+                    sp = q;
+                }
+            }
+            emit = !skip && !(sp.y > 1.0e-5f);
+        }
+        uint32_t total;
+        const uint32_t ex = block_exclusive_scan(emit ? 1u : 0u, s_scan, &total);
+        if (warp_id() == 0) {
+            uint64_t pre = tile_lookback(site.states, tile, total, &b.diag->error_flags);
+            if (lane_id() == 0) s_prefix = pre;
+        }
+        __syncthreads();
+        const uint64_t pre = s_prefix;
+        if (emit) {
+            const uint64_t o = (uint64_t)narrow + pre + ex;
+            if (o < p.pair_capacity) {
+                store_contact(out + o, body, kInvalid, i, kInvalid, make_float4(0.0f, -1.0f, 0.0f, mxf(-sp.y, 0.0f)),
+                              f4(sp - xyz(b.pos[body]), 0.0f), make_float4(0.0f, 0.0f, 0.0f, role != 0u ? -1.0f : 0.0f));
+                out_keys[o] = ((uint64_t)i << 32) | kInvalid;
+                out_feat[o] = 0xffffu;
+            }
+        }
+        if (tile == tiles - 1 && threadIdx.x == 0) {
+            const uint64_t all = (uint64_t)requested_narrow + pre + total;
+            const uint64_t stored = (uint64_t)narrow + pre + total;
+            b.counts->contacts = (uint32_t)umin64(stored, p.pair_capacity);
+            b.diag->contact_count = (uint32_t)umin64(all, 0xffffffffull);
+            if (all > p.pair_capacity) atomicOr(&b.diag->error_flags, MK_PAIR_OVERFLOW_FLAG);
+        }
+        __syncthreads();
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0 && tiles == 0) {
+        b.counts->contacts = narrow;
+        b.diag->contact_count = requested_narrow;
+    }
+}
+
+// ------------------------------------------------------------ contact solve
+__device__ __forceinline__ f3 contact_velocity(const StepBuffers& b, uint32_t body, f3 arm) {
+    return xyz(b.lin[body]) + cross(xyz(b.ang[body]), arm);
+}
+
+// Manifold lookup: the previous tick's contact list is sorted by
+// (collider_a, collider_b) within its narrowphase part and its ground part.
+__device__ __forceinline__ int64_t find_previous(const uint64_t* __restrict__ keys, uint32_t lo, uint32_t end,
+                                                 uint64_t key) {
+    uint32_t hi = end;
+    while (lo < hi) {
+        const uint32_t mid = lo + (hi - lo) / 2u;
+        const uint64_t k = __ldg(keys + mid);
+        if (k < key) lo = mid + 1u;
+        else hi = mid;
+    }
+    return (lo < end && __ldg(keys + lo) == key) ? (int64_t)lo : -1;
+}
+
+// collision.wgsl:674-736 with the persistent manifold of the previous tick
+// read from its contact list (acquired rows carry feature bit 24).
+__global__ void __launch_bounds__(kBlock) k_prepare(StepBuffers b, StepParams p, AppendSite site, GpuContact* cur,
+                                                    uint64_t* cur_keys, uint32_t* cur_feat, const GpuContact* prev,
+                                                    const uint64_t* prev_keys, const uint32_t* prev_feat) {
+    __shared__ uint32_t s_scan[33];
+    __shared__ uint32_t s_tile;
+    __shared__ uint64_t s_prefix;
+    const uint32_t n = b.counts->contacts;
+    const uint32_t tiles = (n + kBlock - 1) / kBlock;
+    const uint32_t tick = b.tick->tick_index;
+    const bool prev_ok = b.counts->prev_valid != 0u && b.counts->prev_tick == tick - 1u;
+    const uint32_t prev_narrow = b.counts->prev_narrow, prev_all = b.counts->prev_contacts;
+    for (;;) {
+        const uint32_t tile = take_tile(site.ticket, &s_tile);
+        if (tile >= tiles) break;
+        const uint32_t k = tile * kBlock + threadIdx.x;
+        bool act = false;
+        if (k < n) {
+            float4* row = reinterpret_cast<float4*>(cur + k);
+            const float4 r0 = row[0], np = row[1], aa = row[2], ab = row[3];
+            const uint32_t a = __float_as_uint(r0.x), bb = __float_as_uint(r0.y);
+            const f3 arm_a = xyz(aa), arm_b = xyz(ab);
+            float inv_b = 0.0f;
+            f3 vb = mkf3(0, 0, 0);
+            if (bb != kInvalid) {
+                inv_b = b.world_mass[3ull * bb].w;
+                vb = contact_velocity(b, bb, arm_b);
+            }
+            if (!(b.world_mass[3ull * a].w + inv_b <= 0.0f)) {
+                const f3 rel = vb - contact_velocity(b, a, arm_a);
+                const f3 nrm = xyz(np);
+                const float vn = dot(rel, nrm);
+                if (np.w <= 1.0e-6f && vn >= 0.0f) {
+                    row[0] = make_float4(r0.x, r0.y, __uint_as_float(kInvalid), __uint_as_float(0u));
+                } else {
+                    float cached = 0.0f;
+                    if (prev_ok) {
+                        const uint64_t key = cur_keys[k];
+                        const bool ground = (uint32_t)key == kInvalid;
+                        const int64_t m = ground ? find_previous(prev_keys, prev_narrow, prev_all, key)
+                                                 : find_previous(prev_keys, 0u, prev_narrow, key);
+                        if (m >= 0 && (__ldg(prev_feat + m) & (1u << 24))) {
+                            const float4* pr = reinterpret_cast<const float4*>(prev + m);
+                            const float4 pn = __ldg(pr + 1), pa = __ldg(pr + 2);
+                            const bool match = dot(xyz(pn), nrm) >= 0.98f && length(xyz(pa) - arm_a) <= 0.02f;
+                            if (match) cached = pa.w;
+                        }
+                    }
+                    row[0] = make_float4(r0.x, r0.y, __uint_as_float(k), __uint_as_float(1u));
+                    row[2] = f4(arm_a, cached);
+                    cur_feat[k] |= 1u << 24;
+                    act = np.w > 1.0e-5f || vn < -1.0e-5f || cached > 1.0e-6f;
+                }
+            }
+        }
+        uint32_t total;
+        const uint32_t ex = block_exclusive_scan(act ? 1u : 0u, s_scan, &total);
+        if (warp_id() == 0) {
+            uint64_t pre = tile_lookback(site.states, tile, total, &b.diag->error_flags);
+            if (lane_id() == 0) s_prefix = pre;
+        }
+        __syncthreads();
+        const uint64_t pre = s_prefix;
+        if (act) b.active[pre + ex] = k;
+        if (tile == tiles - 1 && threadIdx.x == 0) {
+            b.counts->active = (uint32_t)(pre + total);
+            b.diag->active_contact_count = (uint32_t)(pre + total);
+        }
+        __syncthreads();
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0 && tiles == 0) {
+        b.counts->active = 0;
+        b.diag->active_contact_count = 0;
+    }
+}
+
+__device__ __forceinline__ f3 inverse_inertia(const float4* wm, f3 v) {
+    return xyz(wm[0]) * v.x + xyz(wm[1]) * v.y + xyz(wm[2]) * v.z;
+}
+
+// collision.wgsl:116-132
+__device__ __forceinline__ float impulse_denominator(const float4* wa, const float4* wb, f3 arm_a, f3 arm_b, f3 d) {
+    float r = wa[0].w;
+    const f3 ang_a = cross(inverse_inertia(wa, cross(arm_a, d)), arm_a);
+    r += dot(ang_a, d);
+    if (wb) {
+        r += wb[0].w;
+        const f3 ang_b = cross(inverse_inertia(wb, cross(arm_b, d)), arm_b);
+        r += dot(ang_b, d);
+    }
+    return r;
+}
+
+// Segmented sum over runs of equal `key` in consecutive lanes; the last lane
+// of each run returns the run total (others return garbage) in *v.
+__device__ __forceinline__ bool run_tail_sum(uint32_t key, int32_t* v, int n) {
+    const uint32_t lane = lane_id();
+    const uint32_t prev = __shfl_up_sync(0xffffffffu, key, 1);
+    const uint32_t next = __shfl_down_sync(0xffffffffu, key, 1);
+    const bool head = lane == 0 || prev != key;
+    const bool tail = lane == 31 || next != key;
+    const uint32_t heads = __ballot_sync(0xffffffffu, head);
+    // distance to the run head
+    const uint32_t below = heads & ((2u << lane) - 1u);
+    const uint32_t head_lane = 31u - __clz(below);
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+#pragma unroll
+        for (int c = 0; c < 6; ++c) {
+            if (c >= n) break;
+            const int32_t u = __shfl_up_sync(0xffffffffu, v[c], o);
+            if (lane >= head_lane + (uint32_t)o) v[c] = (int32_t)((uint32_t)v[c] + (uint32_t)u);
+        }
+    }
+    return tail;
+}
+
+// collision.wgsl:774-906.  kWarm: warm_start (iteration 0), else solve_accumulate.
+template <bool kWarm>
+__global__ void __launch_bounds__(kBlock) k_solve(StepBuffers b, StepParams p, GpuContact* cur) {
+    const uint32_t A = b.counts->active;
+    const uint32_t stride = gridDim.x * blockDim.x;
+    const float scale = (float)kFixedScale;
+    for (uint32_t base = blockIdx.x * blockDim.x; base < A; base += stride) {
+        const uint32_t t = base + threadIdx.x;
+        bool live = false;
+        uint32_t a = kInvalid, bb = kInvalid;
+        int32_t da[6] = {0, 0, 0, 0, 0, 0}, db[6] = {0, 0, 0, 0, 0, 0};
+        if (t < A) {
+            const uint32_t k = b.active[t];
+            float4* row = reinterpret_cast<float4*>(cur + k);
+            const float4 r0 = row[0], np = row[1], aa = row[2], ab = row[3];
+            a = __float_as_uint(r0.x);
+            bb = __float_as_uint(r0.y);
+            const f3 arm_a = xyz(aa), arm_b = xyz(ab);
+            const float4* wa = b.world_mass + 3ull * a;
+            const float4* wb = bb != kInvalid ? b.world_mass + 3ull * bb : nullptr;
+            f3 vb = mkf3(0, 0, 0);
+            if (bb != kInvalid) vb = contact_velocity(b, bb, arm_b);
+            const f3 nrm = xyz(np);
+            const float den = impulse_denominator(wa, wb, arm_a, arm_b, nrm);
+            if (!(den <= 0.0f)) {
+                const f3 rel = vb - contact_velocity(b, a, arm_a);
+                const float vn = dot(rel, nrm);
+                if (np.w <= 1.0e-5f && vn >= -1.0e-5f && aa.w <= 1.0e-6f) {
+                    row[2] = f4(arm_a, 0.0f);
+                } else {
+                    const bool cyl = ab.w < 0.0f;
+                    const float recovery = cyl ? 1.0f : 0.2f;
+                    const float bias = mnf(mxf(np.w - 0.001f, 0.0f) * recovery / p.dt, 1.0f);
+                    float acc, delta;
+                    if (kWarm) {
+                        const float warmed = aa.w * (cyl ? 1.0f : 0.5f);
+                        acc = mxf(warmed + 0.125f * (-vn + bias) / den, 0.0f);
+                        delta = acc;
+                    } else {
+                        const float prev = mxf(aa.w, 0.0f);
+                        acc = mxf(prev + 0.125f * (-vn + bias) / den, 0.0f);
+                        delta = acc - prev;
+                    }
+                    row[2] = f4(arm_a, acc);
+                    f3 imp = nrm * delta;
+                    const f3 tv = rel - nrm * vn;
+                    const float ts = length(tv);
+                    if (ts > 1.0e-6f) {
+                        const f3 tg = tv / ts;
+                        const float tden = impulse_denominator(wa, wb, arm_a, arm_b, tg);
+                        const float fr = mnf(ts / tden, (kWarm ? acc : fabsf(delta)) * 0.05f);
+                        imp = imp - tg * fr;
+                    }
+                    const f3 la = -imp * wa[0].w;
+                    const f3 ga = inverse_inertia(wa, cross(arm_a, -imp));
+                    da[0] = fixed_i32(la.x * scale); da[1] = fixed_i32(la.y * scale); da[2] = fixed_i32(la.z * scale);
+                    da[3] = fixed_i32(ga.x * scale); da[4] = fixed_i32(ga.y * scale); da[5] = fixed_i32(ga.z * scale);
+                    live = true;
+                    if (wb) {
+                        const f3 lb = imp * wb[0].w;
+                        const f3 gb = inverse_inertia(wb, cross(arm_b, imp));
+                        db[0] = fixed_i32(lb.x * scale); db[1] = fixed_i32(lb.y * scale); db[2] = fixed_i32(lb.z * scale);
+                        db[3] = fixed_i32(gb.x * scale); db[4] = fixed_i32(gb.y * scale); db[5] = fixed_i32(gb.z * scale);
+                    }
+                }
+            }
+        }
+        // body A: contacts arrive grouped by collider A, so sum runs of equal
+        // bodies across the warp first (integer sums are order-free).
+        const uint32_t key_a = live ? a : kInvalid;
+        const bool tail = run_tail_sum(key_a, da, 6);
+        if (tail && key_a != kInvalid) {
+            int32_t* d = b.deltas + 6ull * key_a;
+#pragma unroll
+            for (int c = 0; c < 6; ++c)
+                if (da[c]) atomicAdd(d + c, da[c]);
+        }
+        if (live && bb != kInvalid) {
+            int32_t* d = b.deltas + 6ull * bb;
+#pragma unroll
+            for (int c = 0; c < 6; ++c)
+                if (db[c]) atomicAdd(d + c, db[c]);
+        }
+    }
+}
+
+// collision.wgsl:1050-1069 (only dispatched with active contacts, :744).
+__global__ void __launch_bounds__(kBlock) k_apply(StepBuffers b, StepParams p) {
+    if (b.counts->active == 0u) return;
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= p.body_count) return;
+    // 6 ints per body: 24-byte rows are 8-byte aligned
+    int2* d2 = reinterpret_cast<int2*>(b.deltas + 6ull * i);
+    const int2 x0 = d2[0], x1 = d2[1], x2 = d2[2];
+    d2[0] = make_int2(0, 0);
+    d2[1] = make_int2(0, 0);
+    d2[2] = make_int2(0, 0);
+    const float s = (float)kFixedScale;
+    const f3 ld = mkf3((float)x0.x, (float)x0.y, (float)x1.x) / s;
+    const f3 ad = mkf3((float)x1.y, (float)x2.x, (float)x2.y) / s;
+    b.lin[i] = f4(xyz(b.lin[i]) + ld, 0.0f);
+    b.ang[i] = f4(xyz(b.ang[i]) + ad, 0.0f);
+}
+
+// Bookkeeping at the end of a tick: this tick's contact list becomes the
+// manifold cache of the next one.
+__global__ void k_finish_tick(StepBuffers b) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    DevCounts* c = b.counts;
+    c->prev_narrow = c->narrow;
+    c->prev_contacts = c->contacts;
+    c->prev_tick = b.tick->tick_index;
+    c->prev_valid = 1u;
+}
+
+// physics.wgsl:73-90
+__global__ void k_apply_impulse(StepBuffers b, uint32_t body, float3 point, float3 impulse) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    const float4* m = b.mass + 4ull * body;
+    const float inv = m[0].x;
+    if (inv <= 0.0f) return;
+    const f3 J = mkf3(impulse.x, impulse.y, impulse.z);
+    const f3 arm = mkf3(point.x, point.y, point.z) - xyz(b.pos[body]);
+    b.lin[body] = f4(xyz(b.lin[body]) + J * inv, 0.0f);
+    const float4 r = b.rot[body];
+    const f3 v = cross(arm, J);
+    const f3 local = quat_rotate(conjq(r), v);
+    const f3 lr = xyz(m[1]) * local.x + xyz(m[2]) * local.y + xyz(m[3]) * local.z;
+    b.ang[body] = f4(xyz(b.ang[body]) + quat_rotate(r, lr), 0.0f);
+}
+
+// Standalone batched SAT (mk_op_obb_sat): boxes as 4 float4 rows
+// {center, hx}, {axis_x, hy}, {axis_y, hz}, {axis_z, -}.
+__global__ void __launch_bounds__(kBlock) k_obb_sat_op(const float4* __restrict__ ba, const float4* __restrict__ bb,
+                                                       uint32_t count, float4* __restrict__ np, uint32_t* __restrict__ feat) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= count) return;
+    auto load = [](const float4* p) {
+        Box o;
+        const float4 r0 = __ldg(p), r1 = __ldg(p + 1), r2 = __ldg(p + 2), r3 = __ldg(p + 3);
+        o.c = xyz(r0);
+        o.h[0] = r0.w; o.h[1] = r1.w; o.h[2] = r2.w;
+        o.ax[0] = xyz(r1); o.ax[1] = xyz(r2); o.ax[2] = xyz(r3);
+        o.q = make_float4(0, 0, 0, 1);
+        return o;
+    };
+    const Box A = load(ba + 4ull * i), B = load(bb + 4ull * i);
+    const Sat s = obb_sat(A, B);
+    np[i] = f4(s.n, s.pen);
+    feat[i] = s.axis | (s.near << 8) | (s.early << 16);
+}
+
+// ------------------------------------------------------------------ launch
+static inline uint32_t blocks_for(uint32_t n, uint32_t t) { return (n + t - 1) / t; }
+
+cudaError_t launch_integrate(const StepBuffers& b, const StepParams& p, const StepLaunch& l, cudaStream_t s) {
+    if (p.body_count == 0) return cudaSuccess;
+    if (l.fuse_world_mass) k_integrate<true><<<blocks_for(p.body_count, kBlock), kBlock, 0, s>>>(b, p);
+    else k_integrate<false><<<blocks_for(p.body_count, kBlock), kBlock, 0, s>>>(b, p);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_world_masses(const StepBuffers& b, const StepParams& p, cudaStream_t s) {
+    if (p.body_count == 0) return cudaSuccess;
+    k_world_masses<<<blocks_for(p.body_count, kBlock), kBlock, 0, s>>>(b, p);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_snapshot(const StepBuffers& b, const StepParams& p, cudaStream_t s) {
+    if (p.body_count == 0) return cudaSuccess;
+    k_snapshot<<<blocks_for(p.body_count, kBlock), kBlock, 0, s>>>(b, p);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_broadphase(const StepBuffers& b, const StepParams& p, const StepLaunch& l, int parity,
+                              cudaStream_t s) {
+    (void)parity;
+    const uint32_t C = p.collider_count;
+    if (C == 0) return cudaSuccess;
+    k_collider_bounds<<<blocks_for(C, kBlock), kBlock, 0, s>>>(b, p, l.morton_mode);
+    const uint32_t key_bits = l.morton_mode == MK_MORTON_REFERENCE_30 ? 30u : 63u;
+    cudaError_t e = launch_sort(b.keys, b.values, b.skeys, b.svals, C, nullptr, key_bits, b.sort_scratch,
+                                b.sort_scratch_bytes, &b.diag->error_flags, s, l.sm_count);
+    if (e != cudaSuccess) return e;
+    k_karras<<<blocks_for(C, kBlock), kBlock, 0, s>>>(b, p);
+    k_refit<<<blocks_for(C, kBlock), kBlock, 0, s>>>(b, p);
+    k_traverse<false><<<blocks_for(C, 128), 128, 0, s>>>(b, p);
+    const uint32_t tiles = blocks_for(C, kScanTile);
+    k_scan_offsets<<<std::min<uint32_t>(tiles, (uint32_t)l.sm_count * 2), kBlock, 0, s>>>(b, p);
+    k_traverse<true><<<blocks_for(C, 128), 128, 0, s>>>(b, p);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_narrowphase(const StepBuffers& b, const StepParams& p, const StepLaunch& l, int parity,
+                               cudaStream_t s) {
+    const uint32_t grid = (uint32_t)l.sm_count * 8;
+    AppendSite narrow{b.lookback + 1 * b.lookback_words, b.tickets + 1};
+    AppendSite ground{b.lookback + 2 * b.lookback_words, b.tickets + 2};
+    k_narrowphase<<<grid, kBlock, 0, s>>>(b, p, narrow, b.contacts[parity], b.contact_keys[parity], b.features[parity]);
+    k_ground<<<std::min<uint32_t>(grid, blocks_for(p.collider_count, kBlock) + 1), kBlock, 0, s>>>(
+        b, p, ground, b.contacts[parity], b.contact_keys[parity], b.features[parity]);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_contact_solver(const StepBuffers& b, const StepParams& p, const StepLaunch& l, int parity,
+                                  cudaStream_t s) {
+    const uint32_t grid = (uint32_t)l.sm_count * 8;
+    AppendSite prep{b.lookback + 3 * b.lookback_words, b.tickets + 3};
+    const int prev = parity ^ 1;
+    k_prepare<<<grid, kBlock, 0, s>>>(b, p, prep, b.contacts[parity], b.contact_keys[parity], b.features[parity],
+                                       b.contacts[prev], b.contact_keys[prev], b.features[prev]);
+    const uint32_t iters = std::max<uint32_t>(1u, l.iterations);
+    for (uint32_t it = 0; it < iters; ++it) {
+        if (it == 0) k_solve<true><<<grid, kBlock, 0, s>>>(b, p, b.contacts[parity]);
+        else k_solve<false><<<grid, kBlock, 0, s>>>(b, p, b.contacts[parity]);
+        k_apply<<<blocks_for(p.body_count, kBlock), kBlock, 0, s>>>(b, p);
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_finish_tick(const StepBuffers& b, const StepParams& p, int parity, cudaStream_t s) {
+    (void)p;
+    (void)parity;
+    k_finish_tick<<<1, 32, 0, s>>>(b);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_apply_impulse(const StepBuffers& b, uint32_t body, float3 point, float3 impulse, cudaStream_t s) {
+    k_apply_impulse<<<1, 32, 0, s>>>(b, body, point, impulse);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_obb_sat(const float* boxes_a, const float* boxes_b, uint32_t count, float* np, uint32_t* features,
+                           cudaStream_t s) {
+    if (count == 0) return cudaSuccess;
+    k_obb_sat_op<<<blocks_for(count, kBlock), kBlock, 0, s>>>(reinterpret_cast<const float4*>(boxes_a),
+                                                               reinterpret_cast<const float4*>(boxes_b), count,
+                                                               reinterpret_cast<float4*>(np), features);
+    return cudaGetLastError();
+}
+
+}  // namespace mk

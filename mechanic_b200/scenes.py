@@ -1,0 +1,408 @@
+"""Seeded synthetic scenes written directly as mechanic-gpu ABI rows.
+
+The reference builds rows from a ``CompiledCreation`` (compile.rs:256-609,
+device.rs:429-523).  These generators write the same rows without the
+construction graph, following the reference's own rules:
+
+* part mass and inertia: compile.rs:839-879 (cuboid and cylinder sector);
+* compound aggregation at the centre of mass with identity root rotation:
+  compile.rs:768-821, :330-337;
+* 16 cuboid colliders per cylinder: compile.rs:881-929;
+* analytic cylinder ground roles: device.rs:3008-3045.
+
+Randomness is a counter-based SplitMix64 (one stream per field, seeded with
+``seed ^ scene_index``), so the GPU library and the CPU oracle see identical
+rows.  All row arithmetic is float32, as in the reference.
+"""
+from __future__ import annotations
+
+import dataclasses
+import math
+
+import numpy as np
+
+from . import abi
+
+CUBOID_DENSITY = np.float32(1000.0)   # the reference hard-codes 500 (mechanic-core lib.rs:35); the
+                                      # benchmark scenes ask for 1000 kg/m^3
+CYLINDER_COLLIDER_COUNT = 16          # compile.rs:15
+
+_GOLDEN = np.uint64(0x9E3779B97F4A7C15)
+_M1 = np.uint64(0xBF58476D1CE4E5B9)
+_M2 = np.uint64(0x94D049BB133111EB)
+
+
+def splitmix64(seed: int, index: np.ndarray) -> np.ndarray:
+    """SplitMix64 output for counter ``index`` of stream ``seed`` (vectorised)."""
+    with np.errstate(over="ignore"):
+        z = np.uint64(seed & 0xFFFFFFFFFFFFFFFF) + (index.astype(np.uint64) + np.uint64(1)) * _GOLDEN
+        z = (z ^ (z >> np.uint64(30))) * _M1
+        z = (z ^ (z >> np.uint64(27))) * _M2
+        return z ^ (z >> np.uint64(31))
+
+
+class Rng:
+    """Independent named streams over one seed."""
+
+    def __init__(self, seed: int):
+        self.seed = seed
+
+    def _stream(self, name: str) -> int:
+        h = 1469598103934665603
+        for ch in name.encode():
+            h = ((h ^ ch) * 1099511628211) & 0xFFFFFFFFFFFFFFFF
+        return (self.seed * 0x2545F4914F6CDD1D ^ h) & 0xFFFFFFFFFFFFFFFF
+
+    def uniform(self, name: str, n: int, lo: float = 0.0, hi: float = 1.0) -> np.ndarray:
+        u = (splitmix64(self._stream(name), np.arange(n)) >> np.uint64(11)).astype(np.float64)
+        u *= 2.0 ** -53
+        return lo + (hi - lo) * u
+
+    def normal(self, name: str, n: int) -> np.ndarray:
+        u1 = self.uniform(name + ".u1", n)
+        u2 = self.uniform(name + ".u2", n)
+        return np.sqrt(-2.0 * np.log1p(-u1)) * np.cos(2.0 * np.pi * u2)
+
+    def unit_quaternions(self, name: str, n: int) -> np.ndarray:
+        """Uniform rotations (Shoemake 1992), xyzw."""
+        u1, u2, u3 = (self.uniform(f"{name}.{k}", n) for k in range(3))
+        a, b = np.sqrt(1.0 - u1), np.sqrt(u1)
+        q = np.stack([a * np.sin(2 * np.pi * u2), a * np.cos(2 * np.pi * u2),
+                      b * np.sin(2 * np.pi * u3), b * np.cos(2 * np.pi * u3)], axis=1)
+        return q
+
+
+# ------------------------------------------------------------------ quats
+def quat_yaw(angle: np.ndarray) -> np.ndarray:
+    """``Quat::from_rotation_y`` (xyzw)."""
+    h = np.asarray(angle, np.float64) * 0.5
+    z = np.zeros_like(h)
+    return np.stack([z, np.sin(h), z, np.cos(h)], axis=-1)
+
+
+def quat_mul(a: np.ndarray, b: np.ndarray) -> np.ndarray:
+    ax, ay, az, aw = np.moveaxis(a, -1, 0)
+    bx, by, bz, bw = np.moveaxis(b, -1, 0)
+    return np.stack([aw * bx + ax * bw + ay * bz - az * by,
+                     aw * by - ax * bz + ay * bw + az * bx,
+                     aw * bz + ax * by - ay * bx + az * bw,
+                     aw * bw - ax * bx - ay * by - az * bz], axis=-1)
+
+
+def quat_rotate(q: np.ndarray, v: np.ndarray) -> np.ndarray:
+    u = q[..., :3]
+    t = 2.0 * np.cross(u, v)
+    return v + q[..., 3:4] * t + np.cross(u, t)
+
+
+def quat_matrix(q: np.ndarray) -> np.ndarray:
+    """Rotation matrices (..., 3, 3) with columns R*e_i."""
+    eye = np.eye(3)
+    cols = [quat_rotate(q, np.broadcast_to(eye[i], q.shape[:-1] + (3,))) for i in range(3)]
+    return np.stack(cols, axis=-1)
+
+
+# ------------------------------------------------------------- part rules
+def cuboid_mass_properties(size: np.ndarray, density=CUBOID_DENSITY):
+    """compile.rs:841-852: mass, local centre (0) and principal inertia."""
+    size = np.asarray(size, np.float32)
+    sx, sy, sz = size[..., 0], size[..., 1], size[..., 2]
+    mass = (density * sx * sy * sz).astype(np.float32)
+    twelve = np.float32(12.0)
+    inertia = np.stack([mass * (sy * sy + sz * sz) / twelve,
+                        mass * (sx * sx + sz * sz) / twelve,
+                        mass * (sx * sx + sy * sy) / twelve], axis=-1).astype(np.float32)
+    return mass, np.zeros(size.shape, np.float32), inertia
+
+
+def cylinder_mass_properties(outer_diameter, inner_diameter, length, sweep_degrees=360.0,
+                             density=CUBOID_DENSITY):
+    """compile.rs:853-876: hollow cylinder sector about local Y, centroid on +X."""
+    f = np.float32
+    outer = f(np.asarray(outer_diameter, np.float32) * f(0.5))
+    inner = f(np.asarray(inner_diameter, np.float32) * f(0.5))
+    length = np.asarray(length, np.float32)
+    sweep = np.float32(np.deg2rad(np.float32(sweep_degrees)))
+    sweep = np.broadcast_to(sweep, outer.shape).astype(np.float32)
+    radial_squared = outer * outer + inner * inner
+    mass = (density * sweep * (outer * outer - inner * inner) * length * f(0.5)).astype(np.float32)
+    sin_half = np.sin(sweep * f(0.5)).astype(np.float32)
+    center_x = (f(4.0) * sin_half * (outer ** 3 - inner ** 3)
+                / (f(3.0) * sweep * (outer * outer - inner * inner))).astype(np.float32)
+    sin_sweep = np.sin(sweep).astype(np.float32)
+    radial_parallel = radial_squared * (sweep + sin_sweep) / (f(4.0) * sweep)
+    radial_perpendicular = radial_squared * (sweep - sin_sweep) / (f(4.0) * sweep)
+    axial_variance = length * length / f(12.0)
+    inertia = np.stack([
+        mass * (axial_variance + radial_perpendicular),
+        mass * (radial_parallel + radial_perpendicular - center_x * center_x),
+        mass * (radial_parallel + axial_variance - center_x * center_x),
+    ], axis=-1).astype(np.float32)
+    local_center = np.stack([center_x, np.zeros_like(center_x), np.zeros_like(center_x)], axis=-1)
+    return mass, local_center.astype(np.float32), inertia
+
+
+def world_inertia(rotation: np.ndarray, principal: np.ndarray) -> np.ndarray:
+    """R diag(I) R^T of one single-part compound (compile.rs:784-794, offset 0)."""
+    r = quat_matrix(np.asarray(rotation, np.float64)).astype(np.float32)
+    d = np.asarray(principal, np.float32)
+    return np.einsum("...ij,...j,...kj->...ik", r, d, r).astype(np.float32)
+
+
+def cylinder_segments(outer_diameter, inner_diameter, length, sweep_degrees=360.0):
+    """compile.rs:896-926: per segment (local centre offset in part frame, yaw angle,
+    half extents).  Returns arrays of shape (..., 16, 3), (..., 16), (..., 3)."""
+    f = np.float32
+    outer = np.asarray(outer_diameter, np.float32) * f(0.5)
+    inner = np.asarray(inner_diameter, np.float32) * f(0.5)
+    half_radial = (outer - inner) * f(0.5)
+    center_radius = (outer + inner) * f(0.5)
+    sweep = f(np.deg2rad(np.float32(sweep_degrees)))
+    segment_angle = f(sweep / f(16.0))
+    half_tangent = (outer * f(np.tan(segment_angle * f(0.5)))).astype(np.float32)
+    start = f(-segment_angle * f(0.5)) if float(sweep_degrees) == 360.0 else f(-sweep * f(0.5))
+    seg = np.arange(16, dtype=np.float32)
+    angle = (start + segment_angle * (seg + f(0.5))).astype(np.float32)
+    radial = np.stack([np.cos(angle), np.zeros_like(angle), np.sin(angle)], axis=-1).astype(np.float32)
+    offset = radial * center_radius[..., None, None]
+    half = np.stack([half_radial, np.asarray(length, np.float32) * f(0.5), half_tangent], axis=-1)
+    return offset.astype(np.float32), angle, half.astype(np.float32), center_radius
+
+
+# ------------------------------------------------------------------ scene
+@dataclasses.dataclass
+class Scene:
+    """Flattened creation: exactly the arrays ``mk_create`` receives."""
+
+    transforms: np.ndarray
+    velocities: np.ndarray
+    masses: np.ndarray
+    spatial_inertias: np.ndarray
+    colliders: np.ndarray
+    bearings: np.ndarray = dataclasses.field(default_factory=lambda: np.zeros(0, abi.BEARING))
+    suppressed_pairs: np.ndarray = dataclasses.field(default_factory=lambda: np.zeros(0, abi.PAIR))
+    mechanism_bodies: np.ndarray | None = None
+    root_flags: np.ndarray | None = None
+    preorder: np.ndarray | None = None
+    body_components: np.ndarray | None = None
+    drives: np.ndarray | None = None
+    coordinate_count: int = 0
+    max_depth: int = 0
+    closure_count: int = 0
+    has_dynamic_root: int = 0
+    name: str = "scene"
+    scene_offsets: np.ndarray | None = None   # batched scenes: body offset per scene (+ total)
+
+    @property
+    def body_count(self) -> int:
+        return int(self.transforms.shape[0])
+
+    @property
+    def collider_count(self) -> int:
+        return int(self.colliders.shape[0])
+
+    @property
+    def bearing_count(self) -> int:
+        return int(self.bearings.shape[0])
+
+    def creation(self) -> abi.MkCreation:
+        """ctypes view; the arrays must outlive the returned structure."""
+        c = abi.MkCreation()
+        c.body_count = self.body_count
+        c.collider_count = self.collider_count
+        c.bearing_count = self.bearing_count
+        c.suppression_count = int(self.suppressed_pairs.shape[0])
+        c.coordinate_count = int(self.coordinate_count)
+        c.max_depth = int(self.max_depth)
+        c.transforms = abi.ptr(self.transforms)
+        c.velocities = abi.ptr(self.velocities)
+        c.masses = abi.ptr(self.masses)
+        c.spatial_inertias = abi.ptr(self.spatial_inertias)
+        c.colliders = abi.ptr(self.colliders)
+        c.bearings = abi.ptr(self.bearings) if self.bearing_count else None
+        c.suppressed_pairs = abi.ptr(self.suppressed_pairs) if len(self.suppressed_pairs) else None
+        c.mechanism_bodies = abi.ptr(self.mechanism_bodies)
+        c.root_flags = abi.ptr(self.root_flags)
+        c.preorder = abi.ptr(self.preorder)
+        c.body_components = abi.ptr(self.body_components)
+        c.drives = abi.ptr(self.drives)
+        c.closure_count = int(self.closure_count)
+        c.has_dynamic_root = int(self.has_dynamic_root)
+        return c
+
+
+def _body_rows(translation, inverse_inertia, inertia, mass, dynamic=True):
+    """Mass rows of device.rs:449-477 for single-part compounds."""
+    n = translation.shape[0]
+    transforms = np.zeros(n, abi.TRANSFORM)
+    transforms["position"][:, :3] = translation
+    transforms["rotation"][:, 3] = 1.0                      # root_rotation = IDENTITY (compile.rs:333)
+    masses = np.zeros(n, abi.MASS)
+    inv_m = np.where(dynamic, np.float32(1.0) / mass, np.float32(0.0)).astype(np.float32)
+    masses["inverse_mass"][:, 0] = inv_m
+    masses["inverse_inertia_x"][:, :3] = inverse_inertia[:, :, 0]
+    masses["inverse_inertia_y"][:, :3] = inverse_inertia[:, :, 1]
+    masses["inverse_inertia_z"][:, :3] = inverse_inertia[:, :, 2]
+    spatial = np.zeros(n, abi.SPATIAL_INERTIA)
+    spatial["mass"][:, 0] = mass
+    spatial["inertia_x"][:, :3] = inertia[:, :, 0]
+    spatial["inertia_y"][:, :3] = inertia[:, :, 1]
+    spatial["inertia_z"][:, :3] = inertia[:, :, 2]
+    return transforms, masses, spatial
+
+
+def _invert(m: np.ndarray) -> np.ndarray:
+    return np.linalg.inv(m.astype(np.float64)).astype(np.float32)
+
+
+def _assemble(translation, part_rotation, is_cylinder, outer_d, inner_d, length, cube_size,
+              name, velocities=None, density=CUBOID_DENSITY):
+    """Rows for single-part bodies: cuboids (cube_size) or full cylinders."""
+    n = translation.shape[0]
+    translation = np.asarray(translation, np.float32)
+    part_rotation = np.asarray(part_rotation, np.float64)
+    cube_idx = np.nonzero(~is_cylinder)[0]
+    cyl_idx = np.nonzero(is_cylinder)[0]
+    mass = np.zeros(n, np.float32)
+    principal = np.zeros((n, 3), np.float32)
+    local_c = np.zeros((n, 3), np.float32)
+    size = np.broadcast_to(np.asarray(cube_size, np.float32), (len(cube_idx), 3))
+    m, lc, pi = cuboid_mass_properties(size, density)
+    mass[cube_idx], local_c[cube_idx], principal[cube_idx] = m, lc, pi
+    if len(cyl_idx):
+        m, lc, pi = cylinder_mass_properties(outer_d[cyl_idx], inner_d[cyl_idx], length[cyl_idx],
+                                             360.0, density)
+        mass[cyl_idx], local_c[cyl_idx], principal[cyl_idx] = m, lc, pi
+    rot_f = part_rotation.astype(np.float32)
+    com = (translation + quat_rotate(part_rotation, local_c.astype(np.float64))).astype(np.float32)
+    inertia = world_inertia(part_rotation, principal)
+    inverse = _invert(inertia)
+    transforms, masses, spatial = _body_rows(com, inverse, inertia, mass)
+
+    counts = np.where(is_cylinder, CYLINDER_COLLIDER_COUNT, 1).astype(np.int64)
+    starts = np.concatenate([[0], np.cumsum(counts)[:-1]])
+    total = int(counts.sum())
+    colliders = np.zeros(total, abi.COLLIDER)
+    body_of = np.repeat(np.arange(n, dtype=np.uint32), counts)
+    colliders["metadata"][:, 0] = body_of
+    colliders["metadata"][:, 1] = body_of          # source part slot (one part per body)
+    colliders["metadata"][:, 2] = 0                # source generation
+    # cuboids
+    cs = starts[cube_idx]
+    colliders["local_center"][cs, :3] = (translation[cube_idx] - com[cube_idx])
+    colliders["local_rotation"][cs] = rot_f[cube_idx]
+    colliders["half_extents"][cs, :3] = size * np.float32(0.5)
+    # cylinders (compile.rs:896-926; ground data device.rs:3008-3045)
+    if len(cyl_idx):
+        offset, angle, half, center_radius = cylinder_segments(outer_d[cyl_idx], inner_d[cyl_idx],
+                                                               length[cyl_idx])
+        rq = part_rotation[cyl_idx]
+        seg_rot = quat_mul(rq[:, None, :], quat_yaw(-angle.astype(np.float64))[None, :, :])
+        seg_center = (translation[cyl_idx, None, :] - com[cyl_idx, None, :]
+                      + quat_rotate(np.broadcast_to(rq[:, None, :], offset.shape[:-1] + (4,)),
+                                    offset.astype(np.float64))).astype(np.float32)
+        rows = starts[cyl_idx][:, None] + np.arange(16)[None, :]
+        colliders["local_center"][rows, :3] = seg_center
+        colliders["local_rotation"][rows] = seg_rot.astype(np.float32)
+        colliders["half_extents"][rows, :3] = half[:, None, :]
+        mean_center = seg_center.astype(np.float64).mean(axis=1, keepdims=True)
+        cr = np.linalg.norm(seg_center[:, :1].astype(np.float64) - mean_center, axis=-1).astype(np.float32)
+        outer_r = (cr[:, 0] + half[:, 0]).astype(np.float32)
+        colliders["local_center"][rows, 3] = cr
+        colliders["half_extents"][rows, 3] = outer_r[:, None]
+        colliders["metadata"][rows, 3] = np.arange(1, 17, dtype=np.uint32)[None, :]
+    vel = np.zeros(n, abi.VELOCITY) if velocities is None else velocities
+    return Scene(transforms=transforms, velocities=vel, masses=masses, spatial_inertias=spatial,
+                 colliders=colliders, root_flags=np.ones(n, np.uint32),
+                 body_components=np.arange(n, dtype=np.uint32), name=name)
+
+
+# -------------------------------------------------------------- configs
+def falling_cubes(n: int = 1000, seed: int = 0, box: float = 10.0) -> Scene:
+    """Plain method, small: n 0.25 m cubes, centres uniform in a box x z in
+    [-box/2, box/2), y in [0.25, box + 0.25), uniform orientations, N(0, 1)
+    linear and angular velocity per axis."""
+    rng = Rng(seed)
+    x = rng.uniform("x", n, -box / 2, box / 2)
+    y = rng.uniform("y", n, 0.25, box + 0.25)
+    z = rng.uniform("z", n, -box / 2, box / 2)
+    translation = np.stack([x, y, z], 1).astype(np.float32)
+    rotation = rng.unit_quaternions("q", n)
+    vel = np.zeros(n, abi.VELOCITY)
+    vel["linear"][:, 0] = rng.normal("vx", n)
+    vel["linear"][:, 1] = rng.normal("vy", n)
+    vel["linear"][:, 2] = rng.normal("vz", n)
+    vel["angular"][:, 0] = rng.normal("wx", n)
+    vel["angular"][:, 1] = rng.normal("wy", n)
+    vel["angular"][:, 2] = rng.normal("wz", n)
+    zeros = np.zeros(n)
+    return _assemble(translation, rotation, np.zeros(n, bool), zeros, zeros, zeros,
+                     (0.25, 0.25, 0.25), f"falling_cubes_{n}", vel)
+
+
+def stack_grid(nx: int = 50, ny: int = 40, nz: int = 50, seed: int = 0, spacing: float = 0.26,
+               cylinder_fraction: float = 0.2, jitter: float = 0.005) -> Scene:
+    """Plain method at scale: bodies on an nx*ny*nz grid (spacing 0.26 m) above the
+    ground, jitter U(-0.005, 0.005) m, yaw U(0, 2 pi); 80% 0.25 m cubes, 20% hollow
+    cylinders (outer diameter U(0.25, 1), inner U(0, outer - 0.05), length
+    U(0.25, 2), 360 degrees) with 16 OBB segments each, density 1000 kg/m^3."""
+    rng = Rng(seed)
+    n = nx * ny * nz
+    idx = np.arange(n)
+    ix, iy, iz = idx % nx, (idx // nx) % ny, idx // (nx * ny)
+    x = (ix - (nx - 1) * 0.5) * spacing + rng.uniform("jx", n, -jitter, jitter)
+    y = spacing * 0.5 + iy * spacing + rng.uniform("jy", n, -jitter, jitter)
+    z = (iz - (nz - 1) * 0.5) * spacing + rng.uniform("jz", n, -jitter, jitter)
+    translation = np.stack([x, y, z], 1).astype(np.float32)
+    rotation = quat_yaw(rng.uniform("yaw", n, 0.0, 2.0 * math.pi))
+    is_cyl = rng.uniform("kind", n) < cylinder_fraction
+    outer = rng.uniform("outer", n, 0.25, 1.0).astype(np.float32)
+    inner = (rng.uniform("inner", n) * (outer - 0.05)).astype(np.float32)
+    length = rng.uniform("length", n, 0.25, 2.0).astype(np.float32)
+    return _assemble(translation, rotation, is_cyl, outer, inner, length, (0.25, 0.25, 0.25),
+                     f"stack_grid_{nx}x{ny}x{nz}")
+
+
+def config_plain_small(seed: int = 0) -> Scene:
+    """1,000 falling cubes (the reference's CPU-runnable case)."""
+    return falling_cubes(1000, seed)
+
+
+def config_plain_scale(seed: int = 0) -> Scene:
+    """100,000 bodies on a 50x40x50 grid, 20% cylinders."""
+    return stack_grid(50, 40, 50, seed)
+
+
+def with_suppression(scene: Scene, body_pairs: np.ndarray) -> Scene:
+    """Adds sorted, de-duplicated suppressed body pairs (compile.rs:373, ordered_pair)."""
+    p = np.sort(np.asarray(body_pairs, np.uint32).reshape(-1, 2), axis=1)
+    p = np.unique(p, axis=0)
+    rows = np.zeros(len(p), abi.PAIR)
+    rows["collider_a"], rows["collider_b"] = p[:, 0], p[:, 1]
+    return dataclasses.replace(scene, suppressed_pairs=rows)
+
+
+def compound_mass_properties(parts, density=CUBOID_DENSITY):
+    """compile.rs:768-821 for a weld group: parts are (kind, translation, rotation xyzw,
+    size) with kind "cuboid" (size = edge lengths) or "cylinder" (size = outer diameter,
+    inner diameter, length; 360 degrees).  Returns (mass, centre of mass, inertia 3x3)
+    about the centre of mass in world axes."""
+    props = []
+    for kind, translation, rotation, size in parts:
+        rotation = np.asarray(rotation, np.float64)
+        if kind == "cuboid":
+            m, lc, pi = cuboid_mass_properties(np.asarray(size, np.float32)[None, :], density)
+        else:
+            m, lc, pi = cylinder_mass_properties(*(np.float32(s) for s in size), 360.0, density)
+            m, lc, pi = np.atleast_1d(m), np.atleast_2d(lc), np.atleast_2d(pi)
+        center = np.asarray(translation, np.float64) + quat_rotate(rotation, lc[0].astype(np.float64))
+        props.append((float(m[0]), center, rotation, pi[0].astype(np.float64)))
+    total = sum(p[0] for p in props)
+    com = sum(p[0] * p[1] for p in props) / total
+    inertia = np.zeros((3, 3))
+    for m, center, rotation, principal in props:
+        r = quat_matrix(rotation)
+        own = r @ np.diag(principal) @ r.T
+        off = center - com
+        inertia += own + m * (np.eye(3) * off.dot(off) - np.outer(off, off))
+    return np.float32(total), com.astype(np.float32), inertia.astype(np.float32)

@@ -1,0 +1,1205 @@
+// oracle.cpp — CPU restatement of Mechanic's rigid-body step.
+//
+// TEST INFRASTRUCTURE ONLY: the checker for the CUDA library, never linked
+// into it.  Each function names the reference file:line it restates (paths
+// are relative to the jens-hj/mechanic project).  Operation order follows the
+// WGSL source left to right; the FP32 build uses -ffp-contract=off so that
+// every add/mul/div/sqrt is one IEEE-754 operation, exactly as the CUDA
+// kernels compiled with --fmad=false.  Parity is unpinned against the
+// reference's own kernels (none can run here); see oracle.h.
+
+#include "oracle.h"
+
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <unordered_map>
+#include <vector>
+
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+namespace orc {
+
+static const uint32_t INVALID = 0xffffffffu;
+static int g_threads = 0;
+
+// ---------------------------------------------------------------- math ----
+template <class T> struct V3 { T x, y, z; };
+template <class T> struct V4 { T x, y, z, w; };
+
+template <class T> static inline V3<T> v3(T x, T y, T z) { return {x, y, z}; }
+template <class T> static inline V3<T> xyz(const V4<T>& a) { return {a.x, a.y, a.z}; }
+template <class T> static inline V4<T> v4(const V3<T>& a, T w) { return {a.x, a.y, a.z, w}; }
+template <class T> static inline V3<T> operator+(V3<T> a, V3<T> b) { return {a.x + b.x, a.y + b.y, a.z + b.z}; }
+template <class T> static inline V3<T> operator-(V3<T> a, V3<T> b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
+template <class T> static inline V3<T> operator-(V3<T> a) { return {-a.x, -a.y, -a.z}; }
+template <class T> static inline V3<T> operator*(V3<T> a, T s) { return {a.x * s, a.y * s, a.z * s}; }
+template <class T> static inline V3<T> operator*(T s, V3<T> a) { return {s * a.x, s * a.y, s * a.z}; }
+template <class T> static inline V3<T> operator/(V3<T> a, T s) { return {a.x / s, a.y / s, a.z / s}; }
+template <class T> static inline T dot(V3<T> a, V3<T> b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+template <class T> static inline T dot4(V4<T> a, V4<T> b) { return a.x * b.x + a.y * b.y + a.z * b.z + a.w * b.w; }
+template <class T> static inline V3<T> cross(V3<T> a, V3<T> b) {
+    return {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x};
+}
+template <class T> static inline T length(V3<T> a) { return std::sqrt(dot(a, a)); }
+// normalize(v) = v * inverseSqrt(dot(v, v)); inverseSqrt taken as 1 / sqrt.
+template <class T> static inline V3<T> normalize(V3<T> a) { return a * (T(1) / std::sqrt(dot(a, a))); }
+template <class T> static inline V4<T> normalize4(V4<T> a) {
+    T s = T(1) / std::sqrt(dot4(a, a));
+    return {a.x * s, a.y * s, a.z * s, a.w * s};
+}
+// WGSL min/max/clamp with a fixed answer for equal operands.
+template <class T> static inline T mx(T a, T b) { return a > b ? a : b; }
+template <class T> static inline T mn(T a, T b) { return a < b ? a : b; }
+template <class T> static inline T clampv(T x, T lo, T hi) { return mn(mx(x, lo), hi); }
+template <class T> static inline T sgn(T x) { return x > T(0) ? T(1) : (x < T(0) ? T(-1) : T(0)); }
+template <class T> static inline V3<T> absv(V3<T> a) { return {std::fabs(a.x), std::fabs(a.y), std::fabs(a.z)}; }
+
+// Transcendentals evaluated in double and rounded once, so the FP32 result
+// is the correctly rounded value on both the CPU and the GPU.
+template <class T> static inline T tsin(T x) { return T(std::sin(double(x))); }
+template <class T> static inline T tcos(T x) { return T(std::cos(double(x))); }
+template <class T> static inline T tacos(T x) { return T(std::acos(double(x))); }
+template <class T> static inline T tatan2(T y, T x) { return T(std::atan2(double(y), double(x))); }
+
+// physics.wgsl:46-56, collision.wgsl:97-107 (identical in every kernel file).
+template <class T> static inline V4<T> quat_multiply(V4<T> a, V4<T> b) {
+    V3<T> av = xyz(a), bv = xyz(b);
+    V3<T> v = a.w * bv + b.w * av + cross(av, bv);
+    return {v.x, v.y, v.z, a.w * b.w - dot(av, bv)};
+}
+template <class T> static inline V3<T> quat_rotate(V4<T> q, V3<T> v) {
+    V3<T> t = T(2) * cross(xyz(q), v);
+    return v + q.w * t + cross(xyz(q), t);
+}
+template <class T> static inline V4<T> conj(V4<T> q) { return {-q.x, -q.y, -q.z, q.w}; }
+
+template <class T> static inline bool finite4(V4<T> v) {
+    const T lim = T(3.402823e+38f);
+    return v.x == v.x && v.y == v.y && v.z == v.z && v.w == v.w &&
+           std::fabs(v.x) < lim && std::fabs(v.y) < lim && std::fabs(v.z) < lim && std::fabs(v.w) < lim;
+}
+
+// i32(round(x)): WGSL round is half-to-even; the conversion saturates and
+// sends NaN to 0 (as the GPU's cvt.rni.s32.f32 does).
+template <class T> static inline int32_t fixed_i32(T x) {
+    T r = std::nearbyint(x);
+    if (r != r) return 0;
+    if (r >= T(2147483647.0)) return INT32_MAX;
+    if (r <= T(-2147483648.0)) return INT32_MIN;
+    return (int32_t)r;
+}
+template <class T> static inline uint32_t round_u32(T x) {
+    T r = std::nearbyint(x);
+    if (!(r > T(0))) return 0;
+    if (r >= T(4294967295.0)) return 0xffffffffu;
+    return (uint32_t)r;
+}
+
+template <class T> static inline V4<T> load4(const float* p) { return {T(p[0]), T(p[1]), T(p[2]), T(p[3])}; }
+
+// ------------------------------------------------------------- world -----
+template <class T> struct Collider { V4<T> center, rot, half; uint32_t meta[4]; };
+template <class T> struct Mass { T inv_mass; V3<T> ix, iy, iz; };
+template <class T> struct WorldMass { V4<T> x, y, z; };  // x.w = inverse mass
+template <class T> struct Contact {
+    uint32_t meta[4];
+    V4<T> np;   // normal, penetration
+    V4<T> aa;   // arm a, impulse
+    V4<T> ab;   // arm b, near-face axes / -1
+};
+template <class T> struct Manifold { uint32_t tick, count; V4<T> np; V4<T> pi; };
+template <class T> struct Bearing { V4<T> aa, ab, xa, xb; uint32_t meta[4]; };
+template <class T> struct MechBody { uint32_t meta[4]; uint32_t trav[4]; V4<T> bpos, brot; };
+template <class T> struct Link { V4<T> pos, rot; uint32_t meta[4]; };
+struct Drive { uint32_t mode; float max_acc, max_speed, target_speed, target_angle, min_angle, max_angle; };
+
+struct SatResult32 { uint32_t axis; };
+
+template <class T> struct Sat { V3<T> normal; T pen; uint32_t near; uint32_t axis; uint32_t early; };
+
+template <class T> struct Obb { V3<T> c; V3<T> ax[3]; V3<T> h; };
+
+struct WorldBase {
+    virtual ~WorldBase() {}
+    virtual int step(uint64_t tick) = 0;
+    int precision = 32;
+};
+
+template <class T> struct World : WorldBase {
+    // configuration
+    uint32_t B = 0, C = 0, J = 0, S = 0, Q = 0, max_depth = 0, closure_count = 0;
+    T dt, gravity, lin_damp, ang_damp;
+    uint32_t iterations = 8, morton_mode = 0, collisions = 1, self_collisions = 1, pair_capacity = 0;
+    uint32_t has_dynamic_root = 0;
+    // rows
+    std::vector<V4<T>> pos, rot, lin, ang;
+    std::vector<T> inv_mass;
+    std::vector<Mass<T>> mass;
+    std::vector<Collider<T>> col;
+    std::vector<uint32_t> sup;  // 2*S
+    std::vector<uint32_t> root;
+    std::vector<uint32_t> components;
+    std::vector<Bearing<T>> bear;
+    std::vector<MechBody<T>> mech;
+    std::vector<uint32_t> preorder;
+    std::vector<Drive> drives;
+    std::vector<V4<T>> coords;  // x angle, y angular velocity
+    // per tick
+    std::vector<WorldMass<T>> wm;
+    std::vector<uint32_t> deltas;  // 6 per body, i32 bit patterns with wrap-around
+    std::vector<V4<T>> aabb_min, aabb_max;
+    std::vector<uint64_t> keys, skeys;
+    std::vector<uint32_t> svals;
+    std::vector<uint32_t> pairs;    // 2 per pair
+    std::vector<Contact<T>> contacts;
+    std::vector<uint64_t> contact_keys;
+    std::vector<uint32_t> features;
+    std::vector<uint32_t> active;
+    std::unordered_map<uint64_t, Manifold<T>> manifold;
+    std::vector<V4<T>> snap_pos[3], snap_rot[3];
+    std::vector<Link<T>> links;
+    GpuDiagnostics diag{};
+    uint32_t tick32 = 0;
+
+    // ---------------------------------------------------------- helpers
+    V3<T> collider_center(uint32_t i) const {
+        const Collider<T>& c = col[i];
+        uint32_t b = c.meta[0];
+        return xyz(pos[b]) + quat_rotate(rot[b], xyz(c.center));
+    }
+    V4<T> collider_rotation(uint32_t i) const { return quat_multiply(rot[col[i].meta[0]], col[i].rot); }
+    Obb<T> obb(uint32_t i) const {
+        Obb<T> o;
+        V4<T> r = collider_rotation(i);
+        o.c = collider_center(i);
+        o.ax[0] = quat_rotate(r, v3<T>(1, 0, 0));
+        o.ax[1] = quat_rotate(r, v3<T>(0, 1, 0));
+        o.ax[2] = quat_rotate(r, v3<T>(0, 0, 1));
+        o.h = xyz(col[i].half);
+        return o;
+    }
+
+    bool pair_is_suppressed(uint32_t a, uint32_t b) const {  // lbvh.wgsl:325-345
+        uint32_t low = std::min(a, b), high = std::max(a, b);
+        uint32_t left = 0, right = S;
+        while (left < right) {
+            uint32_t mid = left + (right - left) / 2;
+            uint32_t cx = sup[2 * mid], cy = sup[2 * mid + 1];
+            if (cx < low || (cx == low && cy < high)) left = mid + 1; else right = mid;
+        }
+        return left < S && sup[2 * left] == low && sup[2 * left + 1] == high;
+    }
+
+    // ------------------------------------------------- physics.wgsl:92-132
+    void integrate() {
+        const T gdt = gravity * dt;
+        const T half_dt = T(0.5) * dt;
+        std::atomic<uint32_t> flag{0};
+#pragma omp parallel for schedule(static)
+        for (int64_t ii = 0; ii < (int64_t)B; ++ii) {
+            uint32_t i = (uint32_t)ii;
+            V4<T> p = pos[i], q = rot[i], l = lin[i], a = ang[i];
+            if (inv_mass[i] > T(0)) {
+                l.y += gdt;
+                V3<T> lv = xyz(l) * lin_damp; l = v4(lv, l.w);
+                V3<T> av = xyz(a) * ang_damp; a = v4(av, a.w);
+                if (root[i] != 0) {
+                    V3<T> pv = xyz(p) + xyz(l) * dt; p = v4(pv, p.w);
+                    V4<T> spin = v4(xyz(a), T(0));
+                    V4<T> d = quat_multiply(spin, q);
+                    q = {q.x + d.x * half_dt, q.y + d.y * half_dt, q.z + d.z * half_dt, q.w + d.w * half_dt};
+                    T ns = dot4(q, q);
+                    if (ns > T(1.0e-20f)) {
+                        T s = T(1) / std::sqrt(ns);
+                        q = {q.x * s, q.y * s, q.z * s, q.w * s};
+                    } else {
+                        q = {0, 0, 0, 1};
+                        flag |= MK_INVALID_NUMERIC_FLAG;
+                    }
+                }
+            }
+            if (!(finite4(p) && finite4(q) && finite4(l) && finite4(a))) {
+                flag |= MK_INVALID_NUMERIC_FLAG;
+                continue;
+            }
+            pos[i] = p; rot[i] = q; lin[i] = l; ang[i] = a;
+        }
+        diag.error_flags |= flag.load();
+    }
+
+    // --------------------------------------------- collision.wgsl:134-162
+    V3<T> world_inverse_inertia_column(uint32_t b, V3<T> axis) const {
+        V4<T> r = rot[b];
+        V3<T> local = quat_rotate(conj(r), axis);
+        const Mass<T>& m = mass[b];
+        V3<T> lr = m.ix * local.x + m.iy * local.y + m.iz * local.z;
+        return quat_rotate(r, lr);
+    }
+    void update_world_masses() {
+#pragma omp parallel for schedule(static)
+        for (int64_t ii = 0; ii < (int64_t)B; ++ii) {
+            uint32_t b = (uint32_t)ii;
+            wm[b].x = v4(world_inverse_inertia_column(b, v3<T>(1, 0, 0)), mass[b].inv_mass);
+            wm[b].y = v4(world_inverse_inertia_column(b, v3<T>(0, 1, 0)), T(0));
+            wm[b].z = v4(world_inverse_inertia_column(b, v3<T>(0, 0, 1)), T(0));
+        }
+    }
+
+    // ------------------------------------------------ lbvh.wgsl:84-130
+    static uint32_t expand10(uint32_t v) {
+        v &= 0x3ffu;
+        v = (v | (v << 16)) & 0x030000ffu;
+        v = (v | (v << 8)) & 0x0300f00fu;
+        v = (v | (v << 4)) & 0x030c30c3u;
+        v = (v | (v << 2)) & 0x09249249u;
+        return v;
+    }
+    static uint64_t expand21(uint64_t v) {
+        v &= 0x1fffffull;
+        v = (v | (v << 32)) & 0x1f00000000ffffull;
+        v = (v | (v << 16)) & 0x1f0000ff0000ffull;
+        v = (v | (v << 8)) & 0x100f00f00f00f00full;
+        v = (v | (v << 4)) & 0x10c30c30c30c30c3ull;
+        v = (v | (v << 2)) & 0x1249249249249249ull;
+        return v;
+    }
+    static uint32_t morton30(V3<T> c) {
+        auto q = [](T x) -> uint32_t {
+            T f = clampv(std::floor(x + T(512)), T(0), T(1023));
+            return (uint32_t)f;
+        };
+        return expand10(q(c.x)) | (expand10(q(c.y)) << 1) | (expand10(q(c.z)) << 2);
+    }
+    static uint64_t morton63(V3<T> c) {
+        auto q = [](T x) -> uint64_t {
+            T f = clampv(std::floor((x + T(512)) * T(2048)), T(0), T(2097151));
+            return (uint64_t)f;
+        };
+        return expand21(q(c.x)) | (expand21(q(c.y)) << 1) | (expand21(q(c.z)) << 2);
+    }
+    void compute_bounds() {
+#pragma omp parallel for schedule(static)
+        for (int64_t ii = 0; ii < (int64_t)C; ++ii) {
+            uint32_t i = (uint32_t)ii;
+            V3<T> c = collider_center(i);
+            V4<T> r = collider_rotation(i);
+            V3<T> ax = quat_rotate(r, v3<T>(1, 0, 0));
+            V3<T> ay = quat_rotate(r, v3<T>(0, 1, 0));
+            V3<T> az = quat_rotate(r, v3<T>(0, 0, 1));
+            const V4<T>& h = col[i].half;
+            V3<T> e = absv(ax) * h.x + absv(ay) * h.y + absv(az) * h.z;
+            aabb_min[i] = v4(c - e, T(0));
+            aabb_max[i] = v4(c + e, T(0));
+            keys[i] = morton_mode == MK_MORTON_REFERENCE_30 ? (uint64_t)morton30(c) : morton63(c);
+        }
+        // Stable sort by key == ascending (key, index) order.
+        std::vector<uint32_t> perm(C);
+        for (uint32_t i = 0; i < C; ++i) perm[i] = i;
+        std::stable_sort(perm.begin(), perm.end(), [&](uint32_t a, uint32_t b) { return keys[a] < keys[b]; });
+        for (uint32_t i = 0; i < C; ++i) { skeys[i] = keys[perm[i]]; svals[i] = perm[i]; }
+    }
+
+    static bool overlaps(const V4<T>& amin, const V4<T>& amax, const V4<T>& bmin, const V4<T>& bmax) {
+        return amin.x <= bmax.x && amin.y <= bmax.y && amin.z <= bmax.z &&
+               bmin.x <= amax.x && bmin.y <= amax.y && bmin.z <= amax.z;
+    }
+
+    // Pair set of lbvh.wgsl:321-398: every collider pair (i < j) of different,
+    // non-suppressed bodies whose closed AABBs overlap.  Found here with a
+    // uniform grid (an independent method) and emitted in canonical order.
+    void broadphase() {
+        pairs.clear();
+        if (C < 2) return;
+        if (C <= 2048) {
+            for (uint32_t i = 0; i < C; ++i)
+                for (uint32_t j = i + 1; j < C; ++j) consider_pair(i, j, pairs);
+        } else {
+            grid_pairs();
+        }
+        uint64_t count = pairs.size() / 2;
+        if (count > pair_capacity) {
+            diag.error_flags |= MK_PAIR_OVERFLOW_FLAG;
+            pairs.resize(2ull * pair_capacity);
+        }
+        diag.pair_count = (uint32_t)std::min<uint64_t>(count, 0xffffffffull);
+    }
+    void consider_pair(uint32_t i, uint32_t j, std::vector<uint32_t>& out) const {
+        uint32_t a = col[i].meta[0], b = col[j].meta[0];
+        if (a == b) return;
+        if (!overlaps(aabb_min[i], aabb_max[i], aabb_min[j], aabb_max[j])) return;
+        if (pair_is_suppressed(a, b)) return;
+        out.push_back(i);
+        out.push_back(j);
+    }
+    void grid_pairs() {
+        // Cell size: twice the median AABB extent, at least 0.05 m.
+        std::vector<T> ext(C);
+        for (uint32_t i = 0; i < C; ++i)
+            ext[i] = mx(mx(aabb_max[i].x - aabb_min[i].x, aabb_max[i].y - aabb_min[i].y), aabb_max[i].z - aabb_min[i].z);
+        std::nth_element(ext.begin(), ext.begin() + C / 2, ext.end());
+        double cell = std::max(0.05, 2.0 * double(ext[C / 2]));
+        double lo[3] = {1e300, 1e300, 1e300};
+        for (uint32_t i = 0; i < C; ++i) {
+            lo[0] = std::min(lo[0], double(aabb_min[i].x));
+            lo[1] = std::min(lo[1], double(aabb_min[i].y));
+            lo[2] = std::min(lo[2], double(aabb_min[i].z));
+        }
+        auto cidx = [&](double v, int d) -> int64_t { return (int64_t)std::floor((v - lo[d]) / cell); };
+        // cell key -> colliders; a pair is reported only in the cell holding
+        // the max of the two AABB minima, so each pair appears once.
+        std::unordered_map<uint64_t, std::vector<uint32_t>> grid;
+        grid.reserve(C * 2);
+        auto key3 = [](int64_t x, int64_t y, int64_t z) -> uint64_t {
+            return ((uint64_t)(x & 0x1fffff) << 42) | ((uint64_t)(y & 0x1fffff) << 21) | (uint64_t)(z & 0x1fffff);
+        };
+        for (uint32_t i = 0; i < C; ++i) {
+            int64_t x0 = cidx(aabb_min[i].x, 0), x1 = cidx(aabb_max[i].x, 0);
+            int64_t y0 = cidx(aabb_min[i].y, 1), y1 = cidx(aabb_max[i].y, 1);
+            int64_t z0 = cidx(aabb_min[i].z, 2), z1 = cidx(aabb_max[i].z, 2);
+            for (int64_t x = x0; x <= x1; ++x)
+                for (int64_t y = y0; y <= y1; ++y)
+                    for (int64_t z = z0; z <= z1; ++z) grid[key3(x, y, z)].push_back(i);
+        }
+        std::vector<const std::vector<uint32_t>*> cells;
+        std::vector<uint64_t> cell_keys;
+        cells.reserve(grid.size());
+        for (auto& kv : grid) { cells.push_back(&kv.second); cell_keys.push_back(kv.first); }
+        int nt = 1;
+#ifdef _OPENMP
+        nt = omp_get_max_threads();
+#endif
+        std::vector<std::vector<uint32_t>> local(nt);
+#pragma omp parallel
+        {
+            int t = 0;
+#ifdef _OPENMP
+            t = omp_get_thread_num();
+#endif
+            std::vector<uint32_t>& out = local[t];
+#pragma omp for schedule(dynamic, 64)
+            for (int64_t ci = 0; ci < (int64_t)cells.size(); ++ci) {
+                const std::vector<uint32_t>& v = *cells[ci];
+                uint64_t k = cell_keys[ci];
+                for (size_t a = 0; a < v.size(); ++a)
+                    for (size_t b = a + 1; b < v.size(); ++b) {
+                        uint32_t i = v[a], j = v[b];
+                        // owning cell = cell of the componentwise max of minima
+                        double mxv[3] = {std::max(double(aabb_min[i].x), double(aabb_min[j].x)),
+                                         std::max(double(aabb_min[i].y), double(aabb_min[j].y)),
+                                         std::max(double(aabb_min[i].z), double(aabb_min[j].z))};
+                        if (key3(cidx(mxv[0], 0), cidx(mxv[1], 1), cidx(mxv[2], 2)) != k) continue;
+                        uint32_t lo_i = std::min(i, j), hi_i = std::max(i, j);
+                        consider_pair(lo_i, hi_i, out);
+                    }
+            }
+        }
+        std::vector<uint64_t> all;
+        for (auto& l : local)
+            for (size_t p = 0; p < l.size(); p += 2) all.push_back(((uint64_t)l[p] << 32) | l[p + 1]);
+        std::sort(all.begin(), all.end());
+        pairs.resize(all.size() * 2);
+        for (size_t p = 0; p < all.size(); ++p) {
+            pairs[2 * p] = (uint32_t)(all[p] >> 32);
+            pairs[2 * p + 1] = (uint32_t)all[p];
+        }
+    }
+
+    // ----------------------------------------- collision.wgsl:175-287
+    V3<T> support_point(const Obb<T>& o, V3<T> dir) const {
+        V3<T> p = o.c;
+        const T he[3] = {o.h.x, o.h.y, o.h.z};
+        for (int a = 0; a < 3; ++a) {
+            T proj = dot(o.ax[a], dir);
+            if (std::fabs(proj) > T(1.0e-5f)) p = p + o.ax[a] * he[a] * sgn(proj);
+        }
+        return p;
+    }
+    static V3<T> vertex(const Obb<T>& o, uint32_t v) {
+        V3<T> p = o.c;
+        const T he[3] = {o.h.x, o.h.y, o.h.z};
+        for (uint32_t a = 0; a < 3; ++a) {
+            T d = (v & (1u << a)) ? T(1) : T(-1);
+            p = p + o.ax[a] * he[a] * d;
+        }
+        return p;
+    }
+    static bool contains(const Obb<T>& o, V4<T> r, V3<T> p) {
+        V3<T> local = quat_rotate(conj(r), p - o.c);
+        return std::fabs(local.x) <= o.h.x + T(1.0e-5f) && std::fabs(local.y) <= o.h.y + T(1.0e-5f) &&
+               std::fabs(local.z) <= o.h.z + T(1.0e-5f);
+    }
+    // contains() in collision.wgsl:256-264 rotates by the conjugate collider
+    // rotation; boxes given only by axes use the transposed basis instead.
+    static bool contains_axes(const Obb<T>& o, V3<T> p) {
+        V3<T> d = p - o.c;
+        V3<T> local = v3<T>(dot(o.ax[0], d), dot(o.ax[1], d), dot(o.ax[2], d));
+        return std::fabs(local.x) <= o.h.x + T(1.0e-5f) && std::fabs(local.y) <= o.h.y + T(1.0e-5f) &&
+               std::fabs(local.z) <= o.h.z + T(1.0e-5f);
+    }
+    V3<T> contact_point(const Obb<T>& a, V4<T> ra, const Obb<T>& b, V4<T> rb, V3<T> n, bool by_axes) const {
+        V3<T> sum = v3<T>(0, 0, 0);
+        T count = T(0);
+        for (uint32_t v = 0; v < 8; ++v) {
+            V3<T> pa = vertex(a, v);
+            if (by_axes ? contains_axes(b, pa) : contains(b, rb, pa)) { sum = sum + pa; count += T(1); }
+            V3<T> pb = vertex(b, v);
+            if (by_axes ? contains_axes(a, pb) : contains(a, ra, pb)) { sum = sum + pb; count += T(1); }
+        }
+        if (count > T(0)) return sum / count;
+        V3<T> pa = support_point(a, n), pb = support_point(b, -n);
+        return (pa + pb) * T(0.5);
+    }
+
+    // ----------------------------------------- collision.wgsl:393-486
+    static T projection_radius(const V3<T>* ax, V3<T> e, V3<T> axis) {
+        return std::fabs(dot(ax[0], axis)) * e.x + std::fabs(dot(ax[1], axis)) * e.y + std::fabs(dot(ax[2], axis)) * e.z;
+    }
+    static Sat<T> test_axis(V3<T> delta, const Obb<T>& a, const Obb<T>& b, V3<T> raw, uint32_t idx) {
+        T l2 = dot(raw, raw);
+        if (l2 < T(1.0e-10f)) return {v3<T>(1, 0, 0), T(3.402823e+38f), 0, idx, 0};
+        V3<T> axis = raw * (T(1) / std::sqrt(l2));
+        T sd = dot(delta, axis);
+        T pen = projection_radius(a.ax, a.h, axis) + projection_radius(b.ax, b.h, axis) - std::fabs(sd);
+        if (sd < T(0)) axis = -axis;
+        return {axis, pen, 0, idx, 0};
+    }
+    static Sat<T> obb_sat(const Obb<T>& a, const Obb<T>& b) {
+        V3<T> delta = b.c - a.c;
+        Sat<T> mn_r = {v3<T>(1, 0, 0), T(3.402823e+38f), 0, 0, 0};
+        uint32_t near = 0;
+        for (uint32_t i = 0; i < 3; ++i) {
+            Sat<T> ra = test_axis(delta, a, b, a.ax[i], 2 * i);
+            if (ra.pen < T(0)) { ra.early = 1; return ra; }
+            if (ra.pen <= T(1.0e-4f)) near += 1;
+            if (ra.pen < mn_r.pen) mn_r = ra;
+            Sat<T> rb = test_axis(delta, a, b, b.ax[i], 2 * i + 1);
+            if (rb.pen < T(0)) { rb.early = 1; return rb; }
+            if (rb.pen <= T(1.0e-4f)) near += 1;
+            if (rb.pen < mn_r.pen) mn_r = rb;
+        }
+        for (uint32_t i = 0; i < 3; ++i)
+            for (uint32_t j = 0; j < 3; ++j) {
+                Sat<T> r = test_axis(delta, a, b, cross(a.ax[i], b.ax[j]), 6 + 3 * i + j);
+                if (r.pen < T(0)) { r.early = 1; return r; }
+                if (r.pen < mn_r.pen) mn_r = r;
+            }
+        mn_r.near = near;
+        return mn_r;
+    }
+
+    // ----------------------------------------- collision.wgsl:570-603
+    void narrowphase() {
+        uint64_t np = pairs.size() / 2;
+        std::vector<Contact<T>> out(np);
+        std::vector<uint32_t> feat(np);
+        std::vector<uint8_t> emit(np);
+#pragma omp parallel for schedule(dynamic, 256)
+        for (int64_t pp = 0; pp < (int64_t)np; ++pp) {
+            uint32_t ia = pairs[2 * pp], ib = pairs[2 * pp + 1];
+            Obb<T> a = obb(ia), b = obb(ib);
+            Sat<T> s = obb_sat(a, b);
+            emit[pp] = 0;
+            if (s.pen < T(-1.0e-5f)) continue;
+            V3<T> p = contact_point(a, collider_rotation(ia), b, collider_rotation(ib), s.normal, false);
+            uint32_t ba = col[ia].meta[0], bb = col[ib].meta[0];
+            Contact<T>& c = out[pp];
+            c.meta[0] = ba; c.meta[1] = bb; c.meta[2] = ia; c.meta[3] = ib;
+            c.np = v4(s.normal, mx(s.pen, T(0)));
+            c.aa = v4(p - xyz(pos[ba]), T(0));
+            c.ab = v4(p - xyz(pos[bb]), T(s.near));
+            feat[pp] = s.axis | (s.near << 8) | (s.early << 16);
+            emit[pp] = 1;
+        }
+        contacts.clear(); contact_keys.clear(); features.clear();
+        for (uint64_t pp = 0; pp < np; ++pp) {
+            if (!emit[pp]) continue;
+            contacts.push_back(out[pp]);
+            contact_keys.push_back(((uint64_t)pairs[2 * pp] << 32) | pairs[2 * pp + 1]);
+            features.push_back(feat[pp]);
+        }
+    }
+
+    // ----------------------------------------- collision.wgsl:193-238, 622-664
+    void ground_contacts() {
+        std::vector<Contact<T>> out(C);
+        std::vector<uint8_t> emit(C);
+#pragma omp parallel for schedule(static)
+        for (int64_t ii = 0; ii < (int64_t)C; ++ii) {
+            uint32_t i = (uint32_t)ii;
+            emit[i] = 0;
+            const Collider<T>& c = col[i];
+            Obb<T> o = obb(i);
+            V3<T> down = v3<T>(0, -1, 0);
+            V3<T> sp = support_point(o, down);
+            uint32_t role = c.meta[3];
+            if (role != 0) {
+                V3<T> caxis = o.ax[1];
+                T ap = dot(caxis, down);
+                V3<T> radial = down - caxis * ap;
+                T rl = length(radial);
+                uint32_t cc = rl < T(0.05f) ? 4u : 1u;
+                if (role > cc) continue;
+                V3<T> p = o.c - o.ax[0] * c.center.w;
+                if (rl < T(0.05f)) {
+                    p = p + caxis * sgn(ap) * c.half.y;
+                    V3<T> ta = normalize(v3<T>(1, 0, 0) - caxis * caxis.x);
+                    V3<T> tb = normalize(cross(caxis, ta));
+                    if (role == 1) p = p + ta * c.half.w;
+                    else if (role == 2) p = p - ta * c.half.w;
+                    else if (role == 3) p = p + tb * c.half.w;
+                    else p = p - tb * c.half.w;
+                } else {
+                    p = p + radial * (c.half.w / rl);
+                    if (std::fabs(ap) >= T(0.05f)) p = p + caxis * sgn(ap) * c.half.y;
+                }
+                sp = p;
+            }
+            T bottom = sp.y;
+            if (bottom > T(1.0e-5f)) continue;
+            uint32_t b = c.meta[0];
+            Contact<T>& k = out[i];
+            k.meta[0] = b; k.meta[1] = INVALID; k.meta[2] = i; k.meta[3] = INVALID;
+            k.np = {T(0), T(-1), T(0), mx(-bottom, T(0))};
+            k.aa = v4(sp - xyz(pos[b]), T(0));
+            k.ab = {T(0), T(0), T(0), role != 0 ? T(-1) : T(0)};
+            emit[i] = 1;
+        }
+        for (uint32_t i = 0; i < C; ++i) {
+            if (!emit[i]) continue;
+            contacts.push_back(out[i]);
+            contact_keys.push_back(((uint64_t)i << 32) | INVALID);
+            features.push_back(0xffffu);
+        }
+    }
+
+    // ----------------------------------------- collision.wgsl:674-736, 752
+    V3<T> contact_velocity(uint32_t b, V3<T> arm) const { return xyz(lin[b]) + cross(xyz(ang[b]), arm); }
+
+    void prepare_contacts() {
+        uint64_t K = contacts.size();
+        diag.contact_count = (uint32_t)std::min<uint64_t>(K, 0xffffffffull);
+        if (K > pair_capacity) {
+            diag.error_flags |= MK_PAIR_OVERFLOW_FLAG;
+            contacts.resize(pair_capacity); contact_keys.resize(pair_capacity); features.resize(pair_capacity);
+            K = pair_capacity;
+        }
+        std::vector<uint8_t> act(K);
+        std::vector<uint8_t> acq(K);
+#pragma omp parallel for schedule(static)
+        for (int64_t kk = 0; kk < (int64_t)K; ++kk) {
+            Contact<T>& c = contacts[kk];
+            act[kk] = 0; acq[kk] = 0;
+            uint32_t a = c.meta[0], b = c.meta[1];
+            V3<T> arm_a = xyz(c.aa), arm_b = xyz(c.ab);
+            T inv_b = T(0);
+            V3<T> vb = v3<T>(0, 0, 0);
+            if (b != INVALID) { inv_b = wm[b].x.w; vb = contact_velocity(b, arm_b); }
+            if (wm[a].x.w + inv_b <= T(0)) continue;
+            V3<T> rel = vb - contact_velocity(a, arm_a);
+            V3<T> n = xyz(c.np);
+            T vn = dot(rel, n);
+            if (c.np.w <= T(1.0e-6f) && vn >= T(0)) { c.meta[2] = INVALID; c.meta[3] = 0; continue; }
+            // acquire_manifold (collision.wgsl:499-538) as a map keyed by the
+            // ordered collider pair; the hash slot is not part of parity.
+            uint64_t key = contact_keys[kk];
+            T cached_impulse = T(0);
+            auto it = manifold.find(key);
+            if (it != manifold.end()) {
+                const Manifold<T>& m = it->second;
+                bool match = m.tick == tick32 - 1u && dot(xyz(m.np), n) >= T(0.98f) &&
+                             length(xyz(m.pi) - arm_a) <= T(0.02f);
+                if (match) cached_impulse = m.pi.w;
+            }
+            c.meta[2] = (uint32_t)kk;
+            c.meta[3] = 1;
+            c.aa.w = cached_impulse;
+            acq[kk] = 1;
+            if (c.np.w > T(1.0e-5f) || vn < T(-1.0e-5f) || cached_impulse > T(1.0e-6f)) act[kk] = 1;
+        }
+        active.clear();
+        for (uint64_t kk = 0; kk < K; ++kk)
+            if (act[kk]) active.push_back((uint32_t)kk);
+        acquired_flags.swap(acq);
+        diag.active_contact_count = (uint32_t)active.size();
+    }
+    std::vector<uint8_t> acquired_flags;
+
+    // ----------------------------------------- collision.wgsl:109-132
+    V3<T> inverse_inertia(uint32_t b, V3<T> v) const {
+        const WorldMass<T>& m = wm[b];
+        return xyz(m.x) * v.x + xyz(m.y) * v.y + xyz(m.z) * v.z;
+    }
+    T impulse_denominator(uint32_t a, uint32_t b, V3<T> arm_a, V3<T> arm_b, V3<T> d) const {
+        T r = wm[a].x.w;
+        V3<T> ang_a = cross(inverse_inertia(a, cross(arm_a, d)), arm_a);
+        r += dot(ang_a, d);
+        if (b != INVALID) {
+            r += wm[b].x.w;
+            V3<T> ang_b = cross(inverse_inertia(b, cross(arm_b, d)), arm_b);
+            r += dot(ang_b, d);
+        }
+        return r;
+    }
+    T penetration_bias(T pen, bool cyl) const {
+        T recovery = cyl ? T(1) : T(0.2f);
+        return mn(mx(pen - T(0.001f), T(0)) * recovery / dt, T(1));
+    }
+    void add_delta(uint32_t b, V3<T> l, V3<T> a) {
+        const T s = T(1048576.0f);
+        uint32_t* d = &deltas[6 * (size_t)b];
+        int32_t v[6] = {fixed_i32(l.x * s), fixed_i32(l.y * s), fixed_i32(l.z * s),
+                        fixed_i32(a.x * s), fixed_i32(a.y * s), fixed_i32(a.z * s)};
+        for (int k = 0; k < 6; ++k) {
+            std::atomic_ref<uint32_t> r(d[k]);
+            r.fetch_add((uint32_t)v[k], std::memory_order_relaxed);
+        }
+    }
+    // warm_start (collision.wgsl:774-839) when warm, solve_accumulate (:841-906) otherwise.
+    void solve_contact(uint32_t ci, bool warm) {
+        Contact<T>& c = contacts[ci];
+        uint32_t a = c.meta[0], b = c.meta[1];
+        V3<T> arm_a = xyz(c.aa), arm_b = xyz(c.ab);
+        V3<T> vb = v3<T>(0, 0, 0);
+        if (b != INVALID) vb = contact_velocity(b, arm_b);
+        V3<T> n = xyz(c.np);
+        T den = impulse_denominator(a, b, arm_a, arm_b, n);
+        if (den <= T(0)) return;
+        V3<T> rel = vb - contact_velocity(a, arm_a);
+        T vn = dot(rel, n);
+        if (c.np.w <= T(1.0e-5f) && vn >= T(-1.0e-5f) && c.aa.w <= T(1.0e-6f)) { c.aa.w = T(0); return; }
+        bool cyl = c.ab.w < T(0);
+        T bias = penetration_bias(c.np.w, cyl);
+        T acc, delta;
+        if (warm) {
+            T ws = cyl ? T(1) : T(0.5f);
+            T warmed = c.aa.w * ws;
+            acc = mx(warmed + T(0.125f) * (-vn + bias) / den, T(0));
+            delta = acc;
+        } else {
+            T prev = mx(c.aa.w, T(0));
+            acc = mx(prev + T(0.125f) * (-vn + bias) / den, T(0));
+            delta = acc - prev;
+        }
+        c.aa.w = acc;
+        V3<T> imp = n * delta;
+        V3<T> tv = rel - n * vn;
+        T ts = length(tv);
+        if (ts > T(1.0e-6f)) {
+            V3<T> t = tv / ts;
+            T dt_den = impulse_denominator(a, b, arm_a, arm_b, t);
+            T fr = mn(ts / dt_den, (warm ? acc : std::fabs(delta)) * T(0.05f));
+            imp = imp - t * fr;
+        }
+        add_delta(a, -imp * wm[a].x.w, inverse_inertia(a, cross(arm_a, -imp)));
+        if (b != INVALID) add_delta(b, imp * wm[b].x.w, inverse_inertia(b, cross(arm_b, imp)));
+    }
+    // solve_apply (collision.wgsl:1050-1069)
+    void solve_apply() {
+        const T s = T(1048576.0f);
+#pragma omp parallel for schedule(static)
+        for (int64_t bb = 0; bb < (int64_t)B; ++bb) {
+            uint32_t* d = &deltas[6 * bb];
+            V3<T> ld = v3<T>(T((int32_t)d[0]), T((int32_t)d[1]), T((int32_t)d[2])) / s;
+            V3<T> ad = v3<T>(T((int32_t)d[3]), T((int32_t)d[4]), T((int32_t)d[5])) / s;
+            for (int k = 0; k < 6; ++k) d[k] = 0;
+            lin[bb] = v4(xyz(lin[bb]) + ld, T(0));
+            ang[bb] = v4(xyz(ang[bb]) + ad, T(0));
+        }
+    }
+    void solve() {
+        uint32_t A = (uint32_t)active.size();
+        for (uint32_t it = 0; it < std::max(1u, iterations); ++it) {
+#pragma omp parallel for schedule(static)
+            for (int64_t k = 0; k < (int64_t)A; ++k) solve_contact(active[k], it == 0);
+            if (A > 0) solve_apply();
+        }
+    }
+    // persist_contacts (collision.wgsl:1071-1088) + the prepare-time writes:
+    // every acquired contact's manifold entry holds this tick's values.
+    void persist() {
+        for (size_t k = 0; k < contacts.size(); ++k) {
+            if (acquired_flags.size() <= k || !acquired_flags[k]) continue;
+            const Contact<T>& c = contacts[k];
+            Manifold<T> m;
+            m.tick = tick32;
+            m.count = 1;
+            m.np = c.np;
+            m.pi = c.aa;
+            manifold[contact_keys[k]] = m;
+        }
+        last_tick = tick32;
+    }
+    uint32_t last_tick = 0;
+
+    // ----------------------------------------------- snapshot.wgsl:6-14
+    void snapshot(uint32_t slot) {
+        snap_pos[slot] = pos;
+        snap_rot[slot] = rot;
+    }
+
+    void collision_passes() {
+        update_world_masses();
+        compute_bounds();
+        broadphase();
+        narrowphase();
+        ground_contacts();
+        prepare_contacts();
+        solve();
+        persist();
+    }
+
+    int step(uint64_t tick) override {
+        diag = GpuDiagnostics{};
+        tick32 = (uint32_t)tick;
+        uint32_t slot = (uint32_t)(tick % 3);
+        std::fill(deltas.begin(), deltas.end(), 0u);
+        integrate();
+        bool run_collisions = collisions && C > 0;
+        if (run_collisions) collision_passes();
+        snapshot(slot);
+        return 0;
+    }
+};
+
+}  // namespace orc
+
+using namespace orc;
+
+struct OrWorld {
+    WorldBase* w = nullptr;
+    World<float>* f = nullptr;
+    World<double>* d = nullptr;
+};
+
+template <class T>
+static World<T>* build_world(const MkCreation* cr, const MkConfig* cfg, uint32_t pair_capacity) {
+    World<T>* w = new World<T>();
+    w->precision = sizeof(T) == 4 ? 32 : 64;
+    w->B = cr->body_count; w->C = cr->collider_count; w->J = cr->bearing_count;
+    w->S = cr->suppression_count; w->Q = cr->coordinate_count; w->max_depth = cr->max_depth;
+    w->closure_count = cr->closure_count; w->has_dynamic_root = cr->has_dynamic_root;
+    MkConfig c;
+    if (cfg) c = *cfg; else { std::memset(&c, 0, sizeof(c)); c.collisions_enabled = 1; c.mechanism_self_collisions = 1; c.solver_iterations = 8; }
+    w->dt = T(c.delta_seconds != 0.0f ? c.delta_seconds : 1.0f / 60.0f);
+    w->gravity = T(c.gravity_y != 0.0f ? c.gravity_y : -9.81f);
+    w->lin_damp = T(c.linear_damping != 0.0f ? c.linear_damping : 0.999f);
+    w->ang_damp = T(c.angular_damping != 0.0f ? c.angular_damping : 0.98f);
+    w->iterations = c.solver_iterations ? c.solver_iterations : 8;
+    w->morton_mode = c.morton_mode;
+    w->collisions = c.collisions_enabled;
+    w->self_collisions = c.mechanism_self_collisions;
+    w->pair_capacity = pair_capacity ? pair_capacity : MK_DEFAULT_MAX_CONTACT_PAIRS;
+    uint32_t B = w->B, C = w->C;
+    w->pos.resize(B); w->rot.resize(B); w->lin.resize(B); w->ang.resize(B);
+    w->inv_mass.resize(B); w->mass.resize(B); w->root.resize(B); w->components.resize(B);
+    for (uint32_t i = 0; i < B; ++i) {
+        w->pos[i] = load4<T>(cr->transforms[i].position);
+        w->rot[i] = load4<T>(cr->transforms[i].rotation);
+        if (cr->velocities) {
+            w->lin[i] = load4<T>(cr->velocities[i].linear);
+            w->ang[i] = load4<T>(cr->velocities[i].angular);
+        } else {
+            w->lin[i] = {0, 0, 0, 0}; w->ang[i] = {0, 0, 0, 0};
+        }
+        const GpuMass& m = cr->masses[i];
+        w->inv_mass[i] = T(m.inverse_mass[0]);
+        w->mass[i].inv_mass = T(m.inverse_mass[0]);
+        w->mass[i].ix = xyz(load4<T>(m.inverse_inertia_x));
+        w->mass[i].iy = xyz(load4<T>(m.inverse_inertia_y));
+        w->mass[i].iz = xyz(load4<T>(m.inverse_inertia_z));
+        w->root[i] = cr->root_flags ? cr->root_flags[i] : 1u;
+        w->components[i] = cr->body_components ? cr->body_components[i] : i;
+    }
+    w->col.resize(C);
+    for (uint32_t i = 0; i < C; ++i) {
+        const GpuCollider& g = cr->colliders[i];
+        w->col[i].center = load4<T>(g.local_center);
+        w->col[i].rot = load4<T>(g.local_rotation);
+        w->col[i].half = load4<T>(g.half_extents);
+        for (int k = 0; k < 4; ++k) w->col[i].meta[k] = g.metadata[k];
+    }
+    w->sup.resize(2 * (size_t)w->S);
+    for (uint32_t i = 0; i < w->S; ++i) {
+        w->sup[2 * i] = cr->suppressed_pairs[i].collider_a;
+        w->sup[2 * i + 1] = cr->suppressed_pairs[i].collider_b;
+    }
+    w->wm.resize(B);
+    w->deltas.assign(6 * (size_t)B, 0u);
+    w->aabb_min.resize(C); w->aabb_max.resize(C);
+    w->keys.resize(C); w->skeys.resize(C); w->svals.resize(C);
+    for (int s = 0; s < 3; ++s) { w->snap_pos[s] = w->pos; w->snap_rot[s] = w->rot; }
+    w->coords.assign(w->Q, V4<T>{0, 0, 0, 0});
+    return w;
+}
+
+template <class T> static void put4(float* d, const V4<T>& v) { d[0] = float(v.x); d[1] = float(v.y); d[2] = float(v.z); d[3] = float(v.w); }
+template <class T> static void put4d(double* d, const V4<T>& v) { d[0] = double(v.x); d[1] = double(v.y); d[2] = double(v.z); d[3] = double(v.w); }
+
+extern "C" {
+
+OrWorld* or_create(const MkCreation* creation, const MkConfig* config, int precision, uint32_t pair_capacity) {
+    if (!creation) return nullptr;
+    OrWorld* o = new OrWorld();
+    if (precision == 64) { o->d = build_world<double>(creation, config, pair_capacity); o->w = o->d; }
+    else { o->f = build_world<float>(creation, config, pair_capacity); o->w = o->f; }
+    return o;
+}
+
+void or_destroy(OrWorld* o) {
+    if (!o) return;
+    delete o->w;
+    delete o;
+}
+
+void or_set_threads(int threads) {
+    g_threads = threads;
+#ifdef _OPENMP
+    if (threads > 0) omp_set_num_threads(threads);
+#endif
+}
+
+int or_get_threads(void) {
+#ifdef _OPENMP
+    return omp_get_max_threads();
+#else
+    return 1;
+#endif
+}
+
+int or_step(OrWorld* o, uint64_t tick) { return o->w->step(tick); }
+
+#define DISPATCH(expr_f, expr_d) do { if (o->f) { auto* w = o->f; expr_f; } else { auto* w = o->d; expr_d; } } while (0)
+#define BOTH(...) do { if (o->f) { auto* w = o->f; __VA_ARGS__; } else { auto* w = o->d; __VA_ARGS__; } } while (0)
+
+uint64_t or_count(const OrWorld* o, int what) {
+    uint64_t r = 0;
+    BOTH({
+        switch (what) {
+            case OR_COUNT_PAIRS: r = w->pairs.size() / 2; break;
+            case OR_COUNT_CONTACTS: r = w->contacts.size(); break;
+            case OR_COUNT_ACTIVE: r = w->active.size(); break;
+            case OR_COUNT_BODIES: r = w->B; break;
+            case OR_COUNT_COLLIDERS: r = w->C; break;
+            case OR_COUNT_MANIFOLD: {
+                uint64_t n = 0;
+                for (auto& kv : w->manifold) if (kv.second.tick == w->last_tick) ++n;
+                r = n; break;
+            }
+            case OR_COUNT_COORDINATES: r = w->Q; break;
+            case OR_COUNT_BEARINGS: r = w->J; break;
+        }
+    });
+    return r;
+}
+
+
+void or_get_state(const OrWorld* o, GpuTransform* tr, GpuVelocity* vel) {
+    BOTH({
+        for (uint32_t i = 0; i < w->B; ++i) {
+            if (tr) { put4(tr[i].position, w->pos[i]); put4(tr[i].rotation, w->rot[i]); }
+            if (vel) { put4(vel[i].linear, w->lin[i]); put4(vel[i].angular, w->ang[i]); }
+        }
+    });
+}
+
+void or_get_state_f64(const OrWorld* o, double* p, double* r, double* l, double* a) {
+    BOTH({
+        for (uint32_t i = 0; i < w->B; ++i) {
+            if (p) put4d(p + 4 * i, w->pos[i]);
+            if (r) put4d(r + 4 * i, w->rot[i]);
+            if (l) put4d(l + 4 * i, w->lin[i]);
+            if (a) put4d(a + 4 * i, w->ang[i]);
+        }
+    });
+}
+
+void or_set_state(OrWorld* o, const GpuTransform* tr, const GpuVelocity* vel) {
+    DISPATCH({
+        for (uint32_t i = 0; i < w->B; ++i) {
+            if (tr) { w->pos[i] = load4<float>(tr[i].position); w->rot[i] = load4<float>(tr[i].rotation); }
+            if (vel) { w->lin[i] = load4<float>(vel[i].linear); w->ang[i] = load4<float>(vel[i].angular); }
+        }
+    }, {
+        for (uint32_t i = 0; i < w->B; ++i) {
+            if (tr) { w->pos[i] = load4<double>(tr[i].position); w->rot[i] = load4<double>(tr[i].rotation); }
+            if (vel) { w->lin[i] = load4<double>(vel[i].linear); w->ang[i] = load4<double>(vel[i].angular); }
+        }
+    });
+}
+
+void or_get_diagnostics(const OrWorld* o, GpuDiagnostics* out) { BOTH(*out = w->diag); }
+
+void or_get_pairs(const OrWorld* o, GpuPair* out) {
+    BOTH({ for (size_t p = 0; p < w->pairs.size() / 2; ++p) { out[p].collider_a = w->pairs[2 * p]; out[p].collider_b = w->pairs[2 * p + 1]; } });
+}
+
+void or_get_contacts(const OrWorld* o, GpuContact* out) {
+    BOTH({
+        for (size_t k = 0; k < w->contacts.size(); ++k) {
+            const auto& c = w->contacts[k];
+            for (int j = 0; j < 4; ++j) out[k].metadata[j] = c.meta[j];
+            put4(out[k].normal_penetration, c.np); put4(out[k].arm_a_impulse, c.aa); put4(out[k].arm_b, c.ab);
+        }
+    });
+}
+
+void or_get_contacts_f64(const OrWorld* o, double* rows) {
+    BOTH({
+        for (size_t k = 0; k < w->contacts.size(); ++k) {
+            const auto& c = w->contacts[k];
+            for (int j = 0; j < 4; ++j) rows[16 * k + j] = double(c.meta[j]);
+            put4d(rows + 16 * k + 4, c.np); put4d(rows + 16 * k + 8, c.aa); put4d(rows + 16 * k + 12, c.ab);
+        }
+    });
+}
+
+void or_get_contact_keys(const OrWorld* o, uint64_t* out) { BOTH(std::copy(w->contact_keys.begin(), w->contact_keys.end(), out)); }
+void or_get_features(const OrWorld* o, uint32_t* out) { BOTH(std::copy(w->features.begin(), w->features.end(), out)); }
+void or_get_active(const OrWorld* o, uint32_t* out) { BOTH(std::copy(w->active.begin(), w->active.end(), out)); }
+void or_get_collider_keys(const OrWorld* o, uint64_t* out) { BOTH(std::copy(w->keys.begin(), w->keys.end(), out)); }
+
+void or_get_sorted(const OrWorld* o, uint64_t* keys, uint32_t* values) {
+    BOTH({
+        if (keys) std::copy(w->skeys.begin(), w->skeys.end(), keys);
+        if (values) std::copy(w->svals.begin(), w->svals.end(), values);
+    });
+}
+
+void or_get_aabbs(const OrWorld* o, float* out8) {
+    BOTH({ for (uint32_t i = 0; i < w->C; ++i) { put4(out8 + 8 * i, w->aabb_min[i]); put4(out8 + 8 * i + 4, w->aabb_max[i]); } });
+}
+
+void or_get_world_masses(const OrWorld* o, float* out12) {
+    BOTH({ for (uint32_t i = 0; i < w->B; ++i) { put4(out12 + 12 * i, w->wm[i].x); put4(out12 + 12 * i + 4, w->wm[i].y); put4(out12 + 12 * i + 8, w->wm[i].z); } });
+}
+
+void or_get_snapshot(const OrWorld* o, uint32_t slot, GpuTransform* out) {
+    if (slot > 2) return;
+    BOTH({ for (uint32_t i = 0; i < w->B; ++i) { put4(out[i].position, w->snap_pos[slot][i]); put4(out[i].rotation, w->snap_rot[slot][i]); } });
+}
+
+void or_get_coordinates(const OrWorld* o, GpuMechanismCoordinate* out) {
+    BOTH({ for (uint32_t i = 0; i < w->Q; ++i) { out[i].angle = float(w->coords[i].x); out[i].angular_velocity = float(w->coords[i].y); } });
+}
+
+void or_set_coordinates(OrWorld* o, const GpuMechanismCoordinate* in) {
+    BOTH({ for (uint32_t i = 0; i < w->Q; ++i) { w->coords[i].x = in[i].angle; w->coords[i].y = in[i].angular_velocity; } });
+}
+
+void or_get_links(const OrWorld* o, GpuLinkState* out) {
+    BOTH({
+        for (size_t i = 0; i < w->links.size(); ++i) {
+            put4(out[i].position, w->links[i].pos); put4(out[i].rotation, w->links[i].rot);
+            for (int k = 0; k < 4; ++k) out[i].metadata[k] = w->links[i].meta[k];
+        }
+    });
+}
+
+uint32_t or_get_manifold(const OrWorld* o, GpuContact* out, uint32_t capacity) {
+    uint32_t n = 0;
+    BOTH({
+        std::vector<uint64_t> ks;
+        for (auto& kv : w->manifold) if (kv.second.tick == w->last_tick) ks.push_back(kv.first);
+        std::sort(ks.begin(), ks.end());
+        for (uint64_t k : ks) {
+            if (n >= capacity) break;
+            const auto& m = w->manifold.at(k);
+            GpuContact& c = out[n++];
+            c.metadata[0] = 0; c.metadata[1] = 0; c.metadata[2] = (uint32_t)(k >> 32); c.metadata[3] = (uint32_t)k;
+            put4(c.normal_penetration, m.np); put4(c.arm_a_impulse, m.pi);
+            c.arm_b[0] = c.arm_b[1] = c.arm_b[2] = c.arm_b[3] = 0.0f;
+        }
+    });
+    return n;
+}
+
+void or_set_manifold(OrWorld* o, const GpuContact* rows, uint32_t count, uint64_t last_tick) {
+    DISPATCH({
+        w->manifold.clear();
+        for (uint32_t i = 0; i < count; ++i) {
+            Manifold<float> m; m.tick = (uint32_t)last_tick; m.count = 1;
+            m.np = load4<float>(rows[i].normal_penetration); m.pi = load4<float>(rows[i].arm_a_impulse);
+            w->manifold[((uint64_t)rows[i].metadata[2] << 32) | rows[i].metadata[3]] = m;
+        }
+        w->last_tick = (uint32_t)last_tick;
+    }, {
+        w->manifold.clear();
+        for (uint32_t i = 0; i < count; ++i) {
+            Manifold<double> m; m.tick = (uint32_t)last_tick; m.count = 1;
+            m.np = load4<double>(rows[i].normal_penetration); m.pi = load4<double>(rows[i].arm_a_impulse);
+            w->manifold[((uint64_t)rows[i].metadata[2] << 32) | rows[i].metadata[3]] = m;
+        }
+        w->last_tick = (uint32_t)last_tick;
+    });
+}
+
+// lbvh.wgsl:219-278 over (key, value) entries.
+static int common_prefix(const uint64_t* k, const uint32_t* v, int64_t n, int64_t i, int64_t j) {
+    if (j < 0 || j >= n) return -1;
+    uint64_t d = k[i] ^ k[j];
+    if (d != 0) return __builtin_clzll(d);
+    uint32_t e = v[i] ^ v[j];
+    return 64 + (e ? __builtin_clz(e) : 32);
+}
+
+void or_get_karras(const OrWorld* o, uint32_t* children) {
+    BOTH({
+        const uint64_t* k = w->skeys.data();
+        const uint32_t* v = w->svals.data();
+        int64_t n = w->C;
+        for (int64_t i = 0; i + 1 < n; ++i) {
+            int dir = common_prefix(k, v, n, i, i + 1) > common_prefix(k, v, n, i, i - 1) ? 1 : -1;
+            int min_prefix = common_prefix(k, v, n, i, i - dir);
+            int64_t max_len = 2;
+            while (common_prefix(k, v, n, i, i + max_len * dir) > min_prefix) max_len *= 2;
+            int64_t len = 0;
+            for (int64_t step = max_len / 2; step >= 1; step /= 2)
+                if (common_prefix(k, v, n, i, i + (len + step) * dir) > min_prefix) len += step;
+            int64_t other = i + len * dir;
+            int node_prefix = common_prefix(k, v, n, i, other);
+            int64_t split_off = 0;
+            int64_t step = (len + 1) / 2;
+            while (step >= 1) {
+                if (common_prefix(k, v, n, i, i + (split_off + step) * dir) > node_prefix) split_off += step;
+                if (step == 1) break;
+                step = (step + 1) / 2;
+            }
+            int64_t split = i + split_off * dir + std::min(dir, 0);
+            int64_t first = std::min(i, other), last = std::max(i, other);
+            uint32_t leaf_base = (uint32_t)(n - 1);
+            children[2 * i] = split == first ? leaf_base + (uint32_t)split : (uint32_t)split;
+            children[2 * i + 1] = split + 1 == last ? leaf_base + (uint32_t)(split + 1) : (uint32_t)(split + 1);
+        }
+    });
+}
+
+static Obb<float> box_from(const float* b) {
+    Obb<float> o;
+    o.c = v3<float>(b[0], b[1], b[2]);
+    o.h = v3<float>(b[3], b[7], b[11]);
+    o.ax[0] = v3<float>(b[4], b[5], b[6]);
+    o.ax[1] = v3<float>(b[8], b[9], b[10]);
+    o.ax[2] = v3<float>(b[12], b[13], b[14]);
+    return o;
+}
+
+uint32_t or_obb_sat_f32(const float* box_a, const float* box_b, float* np) {
+    Obb<float> a = box_from(box_a), b = box_from(box_b);
+    Sat<float> s = World<float>::obb_sat(a, b);
+    np[0] = s.normal.x; np[1] = s.normal.y; np[2] = s.normal.z; np[3] = s.pen;
+    return s.axis | (s.near << 8) | (s.early << 16);
+}
+
+void or_contact_point_f32(const float* box_a, const float* box_b, const float* n, float* p3) {
+    Obb<float> a = box_from(box_a), b = box_from(box_b);
+    World<float> tmp;
+    V3<float> p = tmp.contact_point(a, V4<float>{0, 0, 0, 1}, b, V4<float>{0, 0, 0, 1}, v3<float>(n[0], n[1], n[2]), true);
+    p3[0] = p.x; p3[1] = p.y; p3[2] = p.z;
+}
+
+// collision.rs:43-183 (CPU reference narrowphase; glam operation order is
+// approximated with the same vector helpers).
+static Obb<float> cpu_obb(const float* c, const float* q, const float* h) {
+    Obb<float> o;
+    V4<float> r = {q[0], q[1], q[2], q[3]};
+    o.c = v3<float>(c[0], c[1], c[2]);
+    o.h = v3<float>(h[0], h[1], h[2]);
+    o.ax[0] = quat_rotate(r, v3<float>(1, 0, 0));
+    o.ax[1] = quat_rotate(r, v3<float>(0, 1, 0));
+    o.ax[2] = quat_rotate(r, v3<float>(0, 0, 1));
+    return o;
+}
+
+static bool cpu_sat(const Obb<float>& a, const Obb<float>& b, V3<float>& normal, float& pen) {
+    V3<float> delta = b.c - a.c;
+    normal = v3<float>(1, 0, 0);
+    pen = INFINITY;
+    auto test = [&](V3<float> axis) -> bool {
+        float ra = World<float>::projection_radius(a.ax, a.h, axis);
+        float rb = World<float>::projection_radius(b.ax, b.h, axis);
+        float sd = dot(delta, axis);
+        float p = ra + rb - std::fabs(sd);
+        if (p < -1.0e-6f) return false;
+        if (p < pen) { pen = mx(p, 0.0f); normal = sd < 0.0f ? -axis : axis; }
+        return true;
+    };
+    for (int i = 0; i < 3; ++i) if (!test(a.ax[i])) return false;
+    for (int i = 0; i < 3; ++i) if (!test(b.ax[i])) return false;
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) {
+            V3<float> c = cross(a.ax[i], b.ax[j]);
+            if (dot(c, c) > 1.0e-10f)
+                if (!test(normalize(c))) return false;
+        }
+    return true;
+}
+
+int or_cpu_obb_sat(const float* ca, const float* qa, const float* ha, const float* cb, const float* qb,
+                   const float* hb, float* np) {
+    Obb<float> a = cpu_obb(ca, qa, ha), b = cpu_obb(cb, qb, hb);
+    V3<float> n; float p;
+    if (!cpu_sat(a, b, n, p)) return 0;
+    np[0] = n.x; np[1] = n.y; np[2] = n.z; np[3] = p;
+    return 1;
+}
+
+int or_cpu_contact_manifold(const float* ca, const float* qa, const float* ha, const float* cb, const float* qb,
+                            const float* hb, float* np, float* points) {
+    Obb<float> a = cpu_obb(ca, qa, ha), b = cpu_obb(cb, qb, hb);
+    V3<float> n; float p;
+    if (!cpu_sat(a, b, n, p)) return 0;
+    auto verts = [](const Obb<float>& o, V3<float>* out) {
+        V3<float> x = o.ax[0] * o.h.x, y = o.ax[1] * o.h.y, z = o.ax[2] * o.h.z;
+        int k = 0;
+        for (int sx = -1; sx <= 1; sx += 2)
+            for (int sy = -1; sy <= 1; sy += 2)
+                for (int sz = -1; sz <= 1; sz += 2)
+                    out[k++] = o.c + x * float(sx) + y * float(sy) + z * float(sz);
+    };
+    auto contains = [](const Obb<float>& o, V3<float> pt) {
+        V3<float> d = pt - o.c;
+        return std::fabs(dot(o.ax[0], d)) <= o.h.x + 1.0e-5f && std::fabs(dot(o.ax[1], d)) <= o.h.y + 1.0e-5f &&
+               std::fabs(dot(o.ax[2], d)) <= o.h.z + 1.0e-5f;
+    };
+    std::vector<V3<float>> cand;
+    auto push_unique = [&](V3<float> c) {
+        for (auto& q : cand) { V3<float> d = q - c; if (!(dot(d, d) > 1.0e-10f)) return; }
+        cand.push_back(c);
+    };
+    V3<float> va[8], vb[8];
+    verts(a, va); verts(b, vb);
+    for (auto& v : va) if (contains(b, v)) push_unique(v);
+    for (auto& v : vb) if (contains(a, v)) push_unique(v);
+    if (cand.empty()) {
+        auto support = [](const Obb<float>& o, V3<float> dir) {
+            V3<float> pt = o.c;
+            const float he[3] = {o.h.x, o.h.y, o.h.z};
+            for (int k = 0; k < 3; ++k) {
+                float s = dot(o.ax[k], dir);
+                float sg = s > 0.0f ? 1.0f : (s < 0.0f ? -1.0f : (std::signbit(s) ? -1.0f : 1.0f));
+                pt = pt + o.ax[k] * he[k] * sg;
+            }
+            return pt;
+        };
+        cand.push_back((support(a, n) + support(b, -n)) * 0.5f);
+    }
+    std::sort(cand.begin(), cand.end(), [](const V3<float>& l, const V3<float>& r) {
+        if (l.x != r.x) return l.x < r.x;
+        if (l.y != r.y) return l.y < r.y;
+        return l.z < r.z;
+    });
+    if (cand.size() > 4) cand.resize(4);
+    np[0] = n.x; np[1] = n.y; np[2] = n.z; np[3] = p;
+    for (size_t i = 0; i < cand.size(); ++i) { points[3 * i] = cand[i].x; points[3 * i + 1] = cand[i].y; points[3 * i + 2] = cand[i].z; }
+    return (int)cand.size();
+}
+
+uint32_t or_morton30(float x, float y, float z) { return World<float>::morton30(v3<float>(x, y, z)); }
+uint64_t or_morton63(float x, float y, float z) { return World<float>::morton63(v3<float>(x, y, z)); }
+
+}  // extern "C"

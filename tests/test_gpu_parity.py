@@ -1,0 +1,242 @@
+"""GPU parity: libmechanic_b200 (through the C ABI) against the CPU oracle.
+
+Bit-exact targets: collider Morton keys, the sort permutation, Karras
+topology, AABBs, the canonical pair list, contact rows (points, depths,
+normals, impulses), SAT feature words, the active list and the body state
+after each tick.  The oracle's FP32 build and the CUDA build both evaluate
+every float operation as one IEEE-754 operation in the reference's order, so
+the tolerance for all of these is zero ULP.
+"""
+import numpy as np
+import pytest
+
+import oracle
+from mechanic_b200 import abi, scenes
+from mechanic_b200.physics import (BodyIndexOutOfRange, GpuPhysics, GpuPhysicsConfig,
+                                   InvalidSnapshotSlot, NonFinite)
+
+pytestmark = pytest.mark.gpu
+
+
+def _bits(a):
+    a = np.ascontiguousarray(a)
+    return a.view(np.uint8)
+
+
+def assert_bitwise(a, b, what):
+    a = np.ascontiguousarray(a)
+    b = np.ascontiguousarray(b)
+    assert a.shape == b.shape, f"{what}: shape {a.shape} vs {b.shape}"
+    if not np.array_equal(_bits(a), _bits(b)):
+        fa = a.view(np.float32).reshape(len(a), -1) if a.dtype.names else a
+        fb = b.view(np.float32).reshape(len(b), -1) if b.dtype.names else b
+        bad = np.nonzero((_bits(a).reshape(len(a), -1) != _bits(b).reshape(len(b), -1)).any(axis=1))[0]
+        raise AssertionError(f"{what}: {len(bad)} rows differ, first {bad[:5]}: {fa[bad[:2]]} vs {fb[bad[:2]]}")
+
+
+def make_pair(scene, config=None, pair_capacity=1 << 22):
+    cfg = config or GpuPhysicsConfig()
+    gpu = GpuPhysics(scene, cfg, capacities={"pair_capacity": pair_capacity})
+    orc = oracle.OracleWorld(scene, cfg.to_c(), precision=32, pair_capacity=pair_capacity)
+    return gpu, orc
+
+
+def compare_tick(gpu, orc, tick, check_tree=True):
+    gpu.dispatch_tick(tick)
+    rb = gpu.read_last_tick()
+    orc.step(tick)
+    d = orc.diagnostics()
+    assert rb.error_flags == int(d["error_flags"]), f"tick {tick} flags"
+    assert rb.pair_count == int(d["pair_count"]), f"tick {tick} pair count"
+    assert rb.contact_count == int(d["contact_count"]), f"tick {tick} contact count"
+    assert rb.active_contact_count == int(d["active_contact_count"]), f"tick {tick} active count"
+    if check_tree:
+        assert np.array_equal(gpu.collider_keys(), orc.collider_keys()), "Morton keys"
+        gk, gv = gpu.sorted_entries()
+        ok, ov = orc.sorted_entries()
+        assert np.array_equal(gk, ok) and np.array_equal(gv, ov), "sort permutation"
+        assert np.array_equal(gpu.node_children(), orc.karras()), "Karras topology"
+        assert_bitwise(gpu.aabbs(), orc.aabbs(), "collider AABBs")
+        assert_bitwise(gpu.world_masses(), orc.world_masses(), "world inverse inertia")
+    assert np.array_equal(gpu.pairs(), orc.pairs()), f"tick {tick} canonical pair list"
+    assert_bitwise(gpu.contacts(), orc.contacts(), f"tick {tick} contacts")
+    assert np.array_equal(gpu.features() & 0xFFFFFF, orc.features()), f"tick {tick} SAT features"
+    assert np.array_equal(gpu.active(), orc.active()), f"tick {tick} active list"
+    st = gpu.save_state(manifold_capacity=0)
+    tr, vel = orc.state()
+    assert_bitwise(st["transforms"], tr, f"tick {tick} transforms")
+    assert_bitwise(st["velocities"], vel, f"tick {tick} velocities")
+
+
+def test_falling_cubes_one_tick_bitexact(cuda_lib):
+    scene = scenes.falling_cubes(1000, seed=0)
+    gpu, orc = make_pair(scene)
+    compare_tick(gpu, orc, 1)
+
+
+def test_falling_cubes_sixty_ticks_bitexact(cuda_lib):
+    """Config 1 (1,000 cubes, 8 iterations, 60 steps) with warm starting."""
+    scene = scenes.falling_cubes(1000, seed=0)
+    gpu, orc = make_pair(scene)
+    for tick in range(1, 61):
+        compare_tick(gpu, orc, tick, check_tree=(tick % 20 == 0))
+    slot = 60 % 3
+    snap = gpu.read_snapshot_transforms(slot)
+    assert_bitwise(snap, orc.snapshot(slot), "snapshot ring slot")
+
+
+def test_stack_grid_small_bitexact(cuda_lib):
+    """Config 2's mix (cubes + 16-segment cylinders) on a 12x8x12 grid."""
+    scene = scenes.stack_grid(12, 8, 12, seed=3)
+    gpu, orc = make_pair(scene)
+    for tick in range(1, 6):
+        compare_tick(gpu, orc, tick)
+
+
+def test_reference_morton_mode_same_pairs(cuda_lib):
+    """30-bit keys of lbvh.wgsl:93-98 build another tree; the pair set is the same."""
+    scene = scenes.stack_grid(10, 6, 10, seed=5)
+    cfg = GpuPhysicsConfig(morton_mode=abi.MORTON_REFERENCE_30)
+    gpu, orc = make_pair(scene, cfg)
+    for tick in range(1, 4):
+        compare_tick(gpu, orc, tick)
+
+
+def test_graph_and_direct_launch_agree(cuda_lib):
+    scene = scenes.stack_grid(8, 6, 8, seed=1)
+    a = GpuPhysics(scene, GpuPhysicsConfig(use_graph=True))
+    b = GpuPhysics(scene, GpuPhysicsConfig(use_graph=False))
+    for tick in range(1, 8):
+        a.dispatch_tick(tick)
+        b.dispatch_tick(tick)
+    sa, sb = a.save_state(), b.save_state()
+    assert_bitwise(sa["transforms"], sb["transforms"], "graph vs direct transforms")
+    assert_bitwise(sa["velocities"], sb["velocities"], "graph vs direct velocities")
+
+
+def test_one_step_from_identical_state(cuda_lib):
+    """Load the oracle's state (pose, velocity, manifold) into the GPU and step once."""
+    scene = scenes.stack_grid(10, 6, 10, seed=7)
+    orc = oracle.OracleWorld(scene, GpuPhysicsConfig().to_c(), pair_capacity=1 << 22)
+    for tick in range(1, 5):
+        orc.step(tick)
+    tr, vel = orc.state()
+    man = orc.manifold()
+    gpu = GpuPhysics(scene, GpuPhysicsConfig(), capacities={"pair_capacity": 1 << 22})
+    gpu.load_state(tr, vel, manifold=man, manifold_tick=4)
+    compare_tick(gpu, orc, 5)
+    saved = gpu.save_state()
+    assert saved["manifold_tick"] == 5
+    assert np.array_equal(saved["manifold"]["metadata"][:, 2:], orc.manifold()["metadata"][:, 2:])
+    assert_bitwise(saved["manifold"]["normal_penetration"], orc.manifold()["normal_penetration"], "manifold")
+    assert_bitwise(saved["manifold"]["arm_a_impulse"], orc.manifold()["arm_a_impulse"], "manifold impulses")
+
+
+def test_error_variants(cuda_lib):
+    scene = scenes.falling_cubes(16, seed=2)
+    gpu = GpuPhysics(scene)
+    with pytest.raises(InvalidSnapshotSlot):
+        gpu.read_snapshot_transforms(3)
+    with pytest.raises(BodyIndexOutOfRange) as e:
+        gpu.apply_impulse(16, (0, 0, 0), (1, 0, 0))
+    assert e.value.body_index == 16 and e.value.body_count == 16
+    with pytest.raises(NonFinite):
+        gpu.apply_impulse(0, (np.nan, 0, 0), (1, 0, 0))
+    assert gpu.snapshot(3) is None and gpu.snapshot(0) is not None
+
+
+def test_apply_impulse_matches_formula(cuda_lib):
+    """physics.wgsl:73-90 on a resting cube: dv = J/m, dw = I^-1 (r x J)."""
+    scene = scenes.falling_cubes(1, seed=4)
+    scene.velocities[:] = 0
+    gpu = GpuPhysics(scene, GpuPhysicsConfig(collisions_enabled=False))
+    pos = scene.transforms["position"][0, :3].astype(np.float64)
+    gpu.apply_impulse(0, pos + np.array([0.0, 0.125, 0.0]), (1.0, 0.0, 0.0))
+    st = gpu.save_state()
+    inv_m = float(scene.masses["inverse_mass"][0, 0])
+    assert st["velocities"]["linear"][0, 0] == pytest.approx(inv_m, rel=1e-6)
+    inv_i = float(scene.masses["inverse_inertia_z"][0, 2])
+    assert st["velocities"]["angular"][0, 2] == pytest.approx(-0.125 * inv_i, rel=1e-5)
+
+
+def test_pair_overflow_sets_flag_without_overrun(cuda_lib):
+    scene = scenes.stack_grid(10, 6, 10, seed=9)
+    gpu = GpuPhysics(scene, GpuPhysicsConfig(), capacities={"pair_capacity": 64})
+    gpu.dispatch_tick(1)
+    rb = gpu.read_last_tick()
+    assert rb.error_flags & abi.PAIR_OVERFLOW_FLAG
+    assert rb.pair_count > 64
+    assert len(gpu.pairs()) == 64
+    orc = oracle.OracleWorld(scene, GpuPhysicsConfig().to_c(), pair_capacity=64)
+    orc.step(1)
+    assert np.array_equal(gpu.pairs(), orc.pairs())
+
+
+def test_nan_input_sets_invalid_numeric(cuda_lib):
+    scene = scenes.falling_cubes(32, seed=6)
+    scene.velocities["linear"][5, 1] = np.nan
+    gpu = GpuPhysics(scene)
+    gpu.dispatch_tick(1)
+    assert gpu.read_last_tick().error_flags & abi.INVALID_NUMERIC_FLAG
+
+
+def test_capacity_errors(cuda_lib):
+    from mechanic_b200.physics import BodyCapacity, ColliderCapacity
+    scene = scenes.falling_cubes(64, seed=1)
+    with pytest.raises(BodyCapacity) as e:
+        GpuPhysics(scene, capacities={"max_bodies": 32})
+    assert e.value.required == 64 and e.value.capacity == 32
+    with pytest.raises(ColliderCapacity):
+        GpuPhysics(scene, capacities={"max_colliders": 10})
+
+
+def test_timings_and_determinism(cuda_lib):
+    scene = scenes.stack_grid(16, 8, 16, seed=11)
+    runs = []
+    for _ in range(2):
+        gpu = GpuPhysics(scene)
+        for tick in range(1, 4):
+            gpu.dispatch_tick(tick)
+        rb = gpu.read_last_tick()
+        assert rb.gpu_tick_ms is not None and rb.gpu_tick_ms > 0
+        runs.append(gpu.save_state())
+    assert_bitwise(runs[0]["transforms"], runs[1]["transforms"], "run-to-run transforms")
+    assert_bitwise(runs[0]["velocities"], runs[1]["velocities"], "run-to-run velocities")
+
+
+def test_standalone_sort_matches_stable_sort(cuda_lib):
+    import torch
+    from mechanic_b200 import ops
+    rng = np.random.default_rng(0)
+    for n in (1, 1000, 2048, 2049, 300_001):
+        keys = rng.integers(0, 1 << 63, n, dtype=np.uint64)
+        keys[: n // 3] = keys[0]                       # many ties
+        vals = np.arange(n, dtype=np.uint32)
+        k_out, v_out = ops.sort_keys(torch.from_numpy(keys.view(np.int64)).cuda(),
+                                     torch.from_numpy(vals.view(np.int32)).cuda())
+        order = np.argsort(keys, kind="stable")
+        assert np.array_equal(k_out.cpu().numpy().view(np.uint64), keys[order])
+        assert np.array_equal(v_out.cpu().numpy().view(np.uint32), vals[order])
+
+
+def test_standalone_sat_matches_oracle(cuda_lib):
+    import torch
+    from mechanic_b200 import ops
+    rng = np.random.default_rng(1)
+    n = 4096
+    def boxes(seed_shift):
+        q = scenes.Rng(seed_shift).unit_quaternions("q", n)
+        axes = scenes.quat_matrix(q).astype(np.float32)
+        b = np.zeros((n, 4, 4), np.float32)
+        b[:, 0, :3] = rng.uniform(-0.4, 0.4, (n, 3))
+        half = rng.uniform(0.05, 0.3, (n, 3)).astype(np.float32)
+        b[:, 0, 3], b[:, 1, 3], b[:, 2, 3] = half[:, 0], half[:, 1], half[:, 2]
+        b[:, 1, :3], b[:, 2, :3], b[:, 3, :3] = axes[:, :, 0], axes[:, :, 1], axes[:, :, 2]
+        return b
+    a, b = boxes(1), boxes(2)
+    np_out, feat = ops.obb_sat(torch.from_numpy(a).cuda(), torch.from_numpy(b).cuda())
+    np_out, feat = np_out.cpu().numpy(), feat.cpu().numpy().view(np.uint32)
+    for i in range(n):
+        ref, f = oracle.obb_sat(a[i].reshape(-1), b[i].reshape(-1))
+        assert f == feat[i]
+        assert np.array_equal(ref.view(np.uint32), np_out[i].view(np.uint32)), i
