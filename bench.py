@@ -1,0 +1,334 @@
+"""Benchmark: body-steps/s of the plain rigid-body step at 100,000 bodies.
+
+Workload (N=1): the 100,000-body stack (50x40x50 grid at 0.26 m, 20% hollow
+cylinders with 16 OBB segments each, 400,855 colliders, 8 PGS iterations),
+stepped K ticks from its generated state; a step is one tick of the whole
+scene.  Warm-up ticks run from the same state, which is then reloaded, so
+the timed ticks are ticks 1..K of the configuration's trajectory whatever W
+is.  With torchrun (N>1) every rank steps its own replica (a single scene
+does not shard) and the slowest rank's device time sets the throughput.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Prints one JSON line.  Device time comes from CUDA events around each tick's
+graph launch on the handle's stream, with L2 flushed between ticks; `e2e`
+repeats the run through the C ABI with a per-tick host readback of the
+snapshot ring (what a renderer consumes) and the diagnostics, wall-clocked.
+The reference arm times the CPU restatement of the same tick on all host
+cores (the reference's own wgpu pipeline needs a graphics stack, which this
+machine does not have).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+import numpy as np  # noqa: E402
+
+METRIC = "body-steps/s at 100k bodies, plain vs learned+batched, at equal 1e-5 residual"
+UNIT = "body-steps/s"
+WORKLOAD = "plain step, 100,000 bodies (50x40x50 grid, 0.26 m, 20% hollow cylinders), 8 PGS iterations"
+PAIR_CAPACITY = 1 << 24
+# Algorithmic bytes (minimal compulsory traffic) per unit, FP32 rows as in the ABI.
+BYTES_SOLVE_PER_CONTACT_ITER = 284     # contact 64 + idx 4 + 2 x (v 16 + w 16 + world mass 48) + lambda 4 + 2 x 24 deltas
+BYTES_APPLY_PER_BODY_ITER = 112        # deltas 24 + velocities 32 read, velocities 32 + deltas 24 written
+BYTES_PREPARE_PER_CONTACT = 340        # contact 64 + 2 x (v/w 32 + world mass 48) + manifold 96, 16 + 48 + 4 written
+# broadphase per collider: AABB + Morton 140 (collider 64 + pose 32 read, AABB 32 + key/value 12 written),
+# onesweep sort 204 (2 x 12 x 8 digit passes + 12), Karras 24, refit 96 + 32, traversal 32
+BYTES_BROADPHASE_PER_COLLIDER = 140 + 204 + 24 + 96 + 32 + 32
+# per candidate pair: traversal output 8 + pair-key sort (5 digit passes x 16 + 8)
+BYTES_BROADPHASE_PER_PAIR = 8 + 88
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=120)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+# ----------------------------------------------------------------- clocks
+class ClockSampler:
+    """nvidia-smi samples during the timed region (clocks and throttle reasons)."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.device_index = device_index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.device_index}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except (OSError, ValueError):
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if self.proc is None or not self.path or not os.path.exists(self.path):
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        rows = []
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                rows.append({"sm": float(parts[1]), "max": float(parts[2]), "power": float(parts[3]),
+                             "hw": parts[5], "hw_thermal": parts[6], "sw_thermal": parts[7],
+                             "power_cap": parts[8]})
+            except ValueError:
+                continue
+        os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        loaded = [r for r in rows if r["power"] > 200.0] or rows
+        reasons = []
+        for key, name in (("hw", "hw_slowdown"), ("hw_thermal", "hw_thermal_slowdown"),
+                          ("sw_thermal", "sw_thermal_slowdown"), ("power_cap", "sw_power_cap")):
+            if any(r[key].lower() == "active" for r in rows):
+                reasons.append(name)
+        return {"sm_mhz": statistics.median(r["sm"] for r in loaded), "sm_max_mhz": max(r["max"] for r in rows),
+                "samples": len(rows), "samples_under_load": len(loaded), "reasons": reasons}
+
+
+# ------------------------------------------------------------- cpu legs
+def cpu_trajectory(scene, ticks: int, budget_s: float, threads: int):
+    """Steps the CPU oracle along ticks 1..ticks, stopping early once budget_s has passed."""
+    import oracle
+    oracle.set_threads(threads)
+    w = oracle.OracleWorld(scene, pair_capacity=PAIR_CAPACITY)
+    t0 = time.perf_counter()
+    done = 0
+    for tick in range(1, ticks + 1):
+        w.step(tick)
+        done += 1
+        if time.perf_counter() - t0 > budget_s:
+            break
+    return done, time.perf_counter() - t0, oracle.threads()
+
+
+def run_reference(args, scene):
+    """The CPU restatement on all host cores (reference arm)."""
+    threads = os.cpu_count() or 1
+    import oracle
+    oracle.build()
+    oracle.set_threads(threads)
+    warm = oracle.OracleWorld(scene, pair_capacity=PAIR_CAPACITY)
+    for tick in range(1, args.warmup + 1):
+        warm.step(tick)
+    del warm
+    done, elapsed, used = cpu_trajectory(scene, args.steps, 150.0, threads)
+    value = scene.body_count * done / elapsed
+    sample = (f"ticks 1..{done} of the {args.steps}-tick trajectory of the same scene, CPU restatement "
+              f"(oracle, FP32) on {used} threads")
+    return {
+        "metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": 0,
+        "steps": done, "warmup": args.warmup, "ms_per_step": 1e3 * elapsed / done, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded generator)",
+        "config": {"workload": WORKLOAD, "bodies": scene.body_count, "colliders": scene.collider_count,
+                   "ticks": args.steps, "seed": args.seed},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": used, "kind": "port", "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "note": "the reference's wgpu pipeline needs a graphics stack that is unavailable on this box; "
+                "this arm times the CPU restatement of the same tick",
+    }
+
+
+# ------------------------------------------------------------------ ours
+def main():
+    args = parse()
+    rank, world, local = dist_env()
+    from mechanic_b200 import scenes
+    scene = scenes.stack_grid(50, 40, 50, seed=args.seed)
+
+    if args.impl == "reference":
+        if rank == 0:
+            print(json.dumps(run_reference(args, scene)), flush=True)
+        return
+
+    import torch
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=torch.device("cuda", local))
+    from mechanic_b200 import abi
+    from mechanic_b200.physics import GpuPhysics, GpuPhysicsConfig
+
+    gpu = GpuPhysics(scene, GpuPhysicsConfig(device=local), capacities={"pair_capacity": PAIR_CAPACITY})
+    initial = {"transforms": scene.transforms.copy(), "velocities": scene.velocities.copy()}
+    st = gpu.state_buffers()
+    stream = torch.cuda.ExternalStream(st.stream, device=torch.device("cuda", local))
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{local}")   # > 126 MB L2
+
+    def reset():
+        gpu.load_state(initial["transforms"], initial["velocities"], manifold=np.zeros(0, abi.CONTACT),
+                       manifold_tick=0)
+
+    # warm-up from the initial state, then reload it
+    for tick in range(1, args.warmup + 1):
+        gpu.dispatch_tick(tick)
+    gpu.wait()
+    reset()
+    torch.cuda.synchronize()
+
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    stage_ms = {"broadphase": 0.0, "narrowphase": 0.0, "contact_solver": 0.0, "integration": 0.0}
+    solve_bytes = 0.0
+    broad_bytes = 0.0
+    counts = []
+    flags = 0
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clocks:
+        with torch.cuda.stream(stream):
+            for k in range(args.steps):
+                flush.zero_()
+                starts[k].record(stream)
+                gpu.dispatch_tick(k + 1)
+                ends[k].record(stream)
+                rb = gpu.read_last_tick()   # stage events of this tick (synchronizes)
+                flags |= rb.error_flags
+                kt = rb.kernel_timings
+                stage_ms["integration"] += kt.integration_ms
+                stage_ms["broadphase"] += kt.broadphase_ms
+                stage_ms["narrowphase"] += kt.narrowphase_ms
+                stage_ms["contact_solver"] += kt.contact_solver_ms
+                counts.append((rb.pair_count, rb.contact_count, rb.active_contact_count))
+                broad_bytes += (BYTES_BROADPHASE_PER_COLLIDER * scene.collider_count
+                                + BYTES_BROADPHASE_PER_PAIR * rb.pair_count)
+                solve_bytes += (8 * (BYTES_SOLVE_PER_CONTACT_ITER * rb.active_contact_count
+                                     + (BYTES_APPLY_PER_BODY_ITER * scene.body_count
+                                        if rb.active_contact_count else 0))
+                                + BYTES_PREPARE_PER_CONTACT * rb.contact_count)
+        torch.cuda.synchronize()
+    per_tick = [s.elapsed_time(e) for s, e in zip(starts, ends)]
+    total_ms = float(sum(per_tick))
+    if world > 1:
+        t = torch.tensor([total_ms], device=f"cuda:{local}", dtype=torch.float64)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        total_ms = float(t.item())
+    value = world * scene.body_count * args.steps / (total_ms / 1e3)
+
+    # ---- end to end through the C ABI with host buffers
+    reset()
+    pinned = torch.empty(scene.body_count * abi.TRANSFORM.itemsize, dtype=torch.uint8, pin_memory=True)
+    rows = np.frombuffer(pinned.numpy().data, dtype=abi.TRANSFORM, count=scene.body_count)
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for k in range(args.steps):
+        sub = gpu.dispatch_tick(k + 1)             # H2D: the 64-byte tick row
+        gpu.read_last_tick()                       # D2H: 32-byte diagnostics
+        gpu.read_snapshot_transforms(sub.snapshot_slot, rows)   # D2H: snapshot ring slot
+    e2e_s = time.perf_counter() - t0
+    if world > 1:
+        t = torch.tensor([e2e_s], device=f"cuda:{local}", dtype=torch.float64)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e_value = world * scene.body_count * args.steps / e2e_s
+
+    kernels_per_tick = gpu.tick_kernel_count()
+    solve_ms = stage_ms["contact_solver"]
+    broad_ms = stage_ms["broadphase"]
+    peaks = {}
+    peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(peaks_path):
+        peaks = json.load(open(peaks_path))
+    peak = peaks.get("hbm_gbs")
+    peak_note = "measured" if peak else "fallback"
+    peak = peak or 6650.0
+    solve_gbs = solve_bytes / (solve_ms / 1e3) / 1e9 if solve_ms > 0 else 0.0
+    broad_gbs = broad_bytes / (broad_ms / 1e3) / 1e9 if broad_ms > 0 else 0.0
+    stages = {
+        "broadphase": {"kernel": "broadphase stage (bounds + Morton, onesweep sort, Karras, refit, traversal, "
+                                 "pair-key sort)", "achieved": broad_gbs, "ms": broad_ms,
+                       "bytes_per_step": broad_bytes / args.steps},
+        "contact_solve": {"kernel": "contact solve stage (k_prepare + k_solve_all: 8 x (solve + apply))",
+                          "achieved": solve_gbs, "ms": solve_ms, "bytes_per_step": solve_bytes / args.steps},
+    }
+    dominant = max(stages, key=lambda k: stages[k]["ms"])
+    other = "contact_solve" if dominant == "broadphase" else "broadphase"
+
+    if rank == 0:
+        cpu = None
+        if not args.no_cpu_baseline and world == 1:
+            done, elapsed, used = cpu_trajectory(scene, args.steps, 30.0, os.cpu_count() or 1)
+            cpu = {"value": scene.body_count * done / elapsed, "unit": UNIT, "cores": used, "kind": "port",
+                   "sample": f"ticks 1..{done} of the same trajectory on the CPU restatement (FP32), {used} threads, "
+                             f"{elapsed:.1f} s"}
+        tick1 = counts[0] if counts else (0, 0, 0)
+        out = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded generator)",
+            "config": {"workload": WORKLOAD, "bodies": scene.body_count, "colliders": scene.collider_count,
+                       "ticks": f"1..{args.steps} from the generated state (warm-up state reloaded)",
+                       "parallelism": "replicas" if world > 1 else "single", "l2": "flushed between ticks",
+                       "pair_capacity": PAIR_CAPACITY, "tick1_pairs_contacts_active": list(tick1),
+                       "seed": args.seed},
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 64,
+                    "d2h_bytes_per_step": 32 + scene.body_count * abi.TRANSFORM.itemsize},
+            "roofline": {"bound": "hbm", "kernel": stages[dominant]["kernel"],
+                         "achieved": stages[dominant]["achieved"], "peak": peak, "unit": "GB/s",
+                         "frac": stages[dominant]["achieved"] / peak, "peak_source": peak_note, "traffic": None,
+                         "algorithmic_bytes_per_step": stages[dominant]["bytes_per_step"],
+                         "secondary": {"kernel": stages[other]["kernel"], "achieved": stages[other]["achieved"],
+                                       "frac": stages[other]["achieved"] / peak,
+                                       "algorithmic_bytes_per_step": stages[other]["bytes_per_step"]},
+                         "stage_ms_per_step": {k: v / args.steps for k, v in stage_ms.items()}},
+            "cpu_baseline": cpu,
+            "clocks": clocks.summary(),
+            "gpu_launches": kernels_per_tick * args.steps,
+            "error_flags": flags,
+        }
+        print(json.dumps(out), flush=True)
+    gpu.close()
+    if world > 1:
+        torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -412,6 +412,17 @@ MK_API int mk_load_state(MkHandle* handle, const MkHostState* in, MkError* err);
 MK_API int mk_read_buffer(MkHandle* handle, uint32_t buffer_id, void* host,
                    uint64_t capacity_bytes, uint64_t* count, MkError* err);
 
+/* Number of this library's kernels one tick launches (kernel nodes of the
+ * captured tick graph; 0 before the first capture or without a graph). */
+MK_API uint32_t mk_tick_kernel_count(const MkHandle* handle);
+
+/* Process-wide tuning knobs read when a tick is captured (mk_create) or an
+ * operation is launched.  Keys: MK_TUNE_SORT_ITEMS (keys per thread of a
+ * radix-sort tile: 2, 4 or 8; 0 = size-based default).  Returns the previous
+ * value, or -1 for an unknown key. */
+#define MK_TUNE_SORT_ITEMS 1u
+MK_API int mk_set_tuning(uint32_t key, uint32_t value);
+
 /* Library identity: returns "mechanic_b200 <version> sm_100a". */
 MK_API const char* mk_version(void);
 

@@ -81,6 +81,7 @@ struct MkHandle {
     uint64_t submissions = 0;
     uint64_t last_submission = 0;
     bool any_tick = false;
+    uint32_t kernels_per_tick = 0;
 };
 
 namespace {
@@ -115,6 +116,7 @@ uint64_t carve(MkHandle* h, char* base) {
     b.rot = c.take<float4>(B);
     b.lin = c.take<float4>(B);
     b.ang = c.take<float4>(B);
+    b.vel_iter = c.take<float4>(2ull * B * std::max(1u, h->launch.iterations - 1));
     b.inv_mass = c.take<float>(B);
     b.mass = c.take<float4>(4ull * B);
     b.world_mass = c.take<float4>(3ull * B);
@@ -134,9 +136,12 @@ uint64_t carve(MkHandle* h, char* base) {
     b.parents = c.take<uint32_t>(2ull * C);
     b.visits = c.take<uint32_t>(C);
     b.node_aabbs = c.take<float4>(4ull * C);
+    b.node_records = c.take<float4>(4ull * C);
     b.suppressed = c.take<uint2>(std::max(h->S, 1u));
-    b.pair_offsets = c.take<uint32_t>(C + 1ull);
-    b.pairs = c.take<uint2>(P);
+    b.pair_stage = c.take<uint64_t>(P);
+    b.pair_keys = c.take<uint64_t>(P);
+    b.pair_sort_scratch_bytes = mk::sort_scratch_bytes((uint32_t)P, 2 * h->params.pair_shift, false);
+    b.pair_sort_scratch = c.take<char>(b.pair_sort_scratch_bytes);
     for (int k = 0; k < 2; ++k) {
         b.contacts[k] = c.take<GpuContact>(P);
         b.contact_keys[k] = c.take<uint64_t>(P);
@@ -146,6 +151,7 @@ uint64_t carve(MkHandle* h, char* base) {
     b.lookback_words = std::max<uint64_t>(P / 256 + 2, C / 256 + 2);
     b.lookback = c.take<uint64_t>(4 * b.lookback_words);
     b.tickets = c.take<uint32_t>(16);
+    b.grid_barrier = c.take<uint32_t>(64);
     b.diag = c.take<GpuDiagnostics>(1);
     b.tick = c.take<mk::DevTick>(1);
     b.counts = c.take<mk::DevCounts>(1);
@@ -173,7 +179,7 @@ cudaError_t enqueue_tick(MkHandle* h, int parity, bool capturing) {
     cudaError_t e;
     if ((e = mark(0)) != cudaSuccess) return e;
     cudaMemsetAsync(b.diag, 0, sizeof(GpuDiagnostics), s);
-    cudaMemsetAsync(b.counts, 0, 4 * sizeof(uint32_t), s);
+    cudaMemsetAsync(b.counts, 0, mk::kCountResetBytes, s);
     cudaMemsetAsync(b.tickets, 0, 16 * sizeof(uint32_t), s);
     if (h->collisions) {
         cudaMemsetAsync(b.visits, 0, sizeof(uint32_t) * std::max(h->C, 1u), s);
@@ -232,6 +238,16 @@ bool build_graphs(MkHandle* h, MkError* err) {
             if (g) cudaGraphDestroy(g);
             return false;
         }
+        size_t nodes = 0;
+        cudaGraphGetNodes(g, nullptr, &nodes);
+        std::vector<cudaGraphNode_t> list(nodes);
+        cudaGraphGetNodes(g, list.data(), &nodes);
+        uint32_t kernels = 0;
+        for (cudaGraphNode_t n : list) {
+            cudaGraphNodeType t;
+            if (cudaGraphNodeGetType(n, &t) == cudaSuccess && t == cudaGraphNodeTypeKernel) ++kernels;
+        }
+        h->kernels_per_tick = kernels;
         cudaGraphExec_t exec = nullptr;
         e = cudaGraphInstantiate(&exec, g, 0);
         cudaGraphDestroy(g);
@@ -294,6 +310,17 @@ void mk_config_default(MkConfig* c) {
 }
 
 const char* mk_version(void) { return "mechanic_b200 0.1.0 sm_100a"; }
+
+int mk_set_tuning(uint32_t key, uint32_t value) {
+    static uint32_t sort_items = 0;
+    if (key == MK_TUNE_SORT_ITEMS) {
+        const uint32_t prev = sort_items;
+        sort_items = value;
+        mk::set_sort_items(value);
+        return (int)prev;
+    }
+    return -1;
+}
 
 const char* mk_last_error(void) { return g_last_error.c_str(); }
 
@@ -370,6 +397,11 @@ int mk_create(const MkCreation* cr, const MkConfig* config, const MkCapacities* 
     h->params.collider_count = h->C;
     h->params.pair_capacity = pair_capacity;
     h->params.suppression_count = h->S;
+    {
+        uint32_t shift = 1;
+        while (shift < 31 && (1ull << shift) < (uint64_t)h->C) ++shift;
+        h->params.pair_shift = shift;
+    }
     h->launch.sm_count = h->sm_count;
     h->launch.morton_mode = c.morton_mode;
     h->launch.iterations = std::max(1u, c.solver_iterations ? c.solver_iterations : 8u);
@@ -618,6 +650,8 @@ int mk_init_coordinates(MkHandle* h, const GpuMechanismCoordinate* coords, uint3
 
 uint32_t mk_body_count(const MkHandle* h) { return h ? h->B : 0u; }
 
+uint32_t mk_tick_kernel_count(const MkHandle* h) { return h ? h->kernels_per_tick : 0u; }
+
 int mk_has_gpu_timestamps(const MkHandle* h) { return h ? 1 : 0; }
 
 int mk_state_buffers(MkHandle* h, MkDeviceState* out) {
@@ -770,7 +804,7 @@ int mk_read_buffer(MkHandle* h, uint32_t id, void* host, uint64_t cap_bytes, uin
         case MK_BUF_COLLIDER_AABBS: src = b.aabbs; n = h->C; row = 32; break;
         case MK_BUF_NODE_CHILDREN: src = b.children; n = h->C ? h->C - 1 : 0; row = 8; break;
         case MK_BUF_NODE_AABBS: src = b.node_aabbs; n = h->C ? 2ull * h->C - 1 : 0; row = 32; break;
-        case MK_BUF_PAIRS: src = b.pairs; n = counts.pairs; row = 8; break;
+        case MK_BUF_PAIRS: src = b.pair_keys; n = counts.pairs; row = 8; break;
         case MK_BUF_CONTACTS: src = b.contacts[last]; n = counts.contacts; row = 64; break;
         case MK_BUF_ACTIVE: src = b.active; n = counts.active; row = 4; break;
         case MK_BUF_COLLIDER_KEYS: src = b.keys; n = h->C; row = 8; break;
@@ -785,6 +819,16 @@ int mk_read_buffer(MkHandle* h, uint32_t id, void* host, uint64_t cap_bytes, uin
     if (!host) return MK_OK;
     const uint64_t bytes = std::min<uint64_t>(n * row, cap_bytes);
     if (e == cudaSuccess && bytes && src) e = cudaMemcpy(host, src, bytes, cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess && id == MK_BUF_PAIRS) {
+        // pair keys (a << shift | b) to GpuPair rows
+        const uint32_t shift = h->params.pair_shift;
+        uint64_t* k = reinterpret_cast<uint64_t*>(host);
+        for (uint64_t r = 0; r < bytes / 8; ++r) {
+            const uint64_t key = k[r];
+            GpuPair pr{(uint32_t)(key >> shift), (uint32_t)(key & ((1ull << shift) - 1))};
+            std::memcpy(&k[r], &pr, sizeof(pr));
+        }
+    }
     return check(e, err, "read_buffer") ? MK_OK : MK_ERR_DEVICE_FAILURE;
 }
 

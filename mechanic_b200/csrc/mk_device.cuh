@@ -168,6 +168,15 @@ __device__ __forceinline__ void st_release_u32(uint32_t* p, uint32_t v) {
     asm volatile("st.release.gpu.global.u32 [%0], %1;" :: "l"(p), "r"(v) : "memory");
 }
 
+// Fetch-add with acquire-release semantics at GPU scope: orders this thread's
+// earlier writes before the add and makes writes released by earlier adds on
+// the same word visible after it (the bottom-up refit's arrival counter).
+__device__ __forceinline__ uint32_t atomic_add_acq_rel(uint32_t* p, uint32_t v) {
+    uint32_t old;
+    asm volatile("atom.acq_rel.gpu.global.add.u32 %0, [%1], %2;" : "=r"(old) : "l"(p), "r"(v) : "memory");
+    return old;
+}
+
 // Called by warp 0 of a block (all 32 lanes).  Returns the exclusive prefix
 // of `tile` and publishes its inclusive prefix.
 __device__ __forceinline__ uint64_t tile_lookback(uint64_t* states, uint32_t tile, uint64_t aggregate,

@@ -21,27 +21,35 @@ struct DevTick {
 // Counts produced on the device during a tick.  `prev_*` describe the
 // contact list of the previous tick, which doubles as the manifold cache.
 struct DevCounts {
+    // reset at the start of every tick (first kResetWords words)
     uint32_t pairs;            // candidate pairs stored (clamped to capacity)
     uint32_t narrow;           // narrowphase contacts stored
     uint32_t contacts;         // narrowphase + ground contacts stored
     uint32_t active;           // active contacts
+    uint32_t pairs_found;      // candidate pairs found by the traversal
+    uint32_t requested_contacts;
+    uint32_t reset_pad[2];
+    // carried across ticks
     uint32_t prev_narrow;      // previous tick: narrowphase contacts
     uint32_t prev_contacts;    // previous tick: all contacts
     uint32_t prev_tick;        // previous tick index
     uint32_t prev_valid;       // 1 when the previous list may be matched
-    uint32_t requested_contacts;
-    uint32_t pad[7];
+    uint32_t pad[4];
 };
+constexpr uint32_t kCountResetBytes = 8 * sizeof(uint32_t);
 
 // Solver-side constants of a handle.
 struct StepParams {
     float dt, gravity, lin_damp, ang_damp;
     uint32_t body_count, collider_count, pair_capacity, suppression_count;
+    uint32_t pair_shift;       // bits of a collider index inside a pair key
 };
 
 // Launches implemented in mk_sort.cu.
 uint32_t sort_passes(uint32_t key_bits);
-uint64_t sort_scratch_bytes(uint32_t n, uint32_t key_bits);
+void set_sort_items(uint32_t items);
+uint32_t sort_items_for(uint32_t n);
+uint64_t sort_scratch_bytes(uint32_t n, uint32_t key_bits, bool values = true);
 cudaError_t launch_sort(const uint64_t* keys_in, const uint32_t* vals_in, uint64_t* keys_out, uint32_t* vals_out,
                         uint32_t n, const uint32_t* n_dev, uint32_t key_bits, void* scratch,
                         uint64_t scratch_bytes, uint32_t* error_flags, cudaStream_t stream, int sm_count);
@@ -49,6 +57,7 @@ cudaError_t launch_sort(const uint64_t* keys_in, const uint32_t* vals_in, uint64
 // Device buffers of one handle's step (all device pointers).
 struct StepBuffers {
     float4 *pos, *rot, *lin, *ang;
+    float4* vel_iter;            // (iterations - 1) x {lin, ang} x body_count: per-iteration velocities
     const float* inv_mass;
     const float4* mass;          // GpuMass rows (4 x float4)
     float4* world_mass;          // 3 x float4 per body
@@ -66,10 +75,13 @@ struct StepBuffers {
     uint2* children;             // C-1
     uint32_t* parents;           // 2C-1
     uint32_t* visits;            // C-1
-    float4* node_aabbs;          // 2 x float4 per node
+    float4* node_aabbs;          // 2 x float4 per node (union boxes)
+    float4* node_records;        // 4 x float4 per internal node (both children's boxes)
     const uint2* suppressed;
-    uint32_t* pair_offsets;      // C + 1
-    uint2* pairs;                // pair_capacity
+    uint64_t* pair_stage;        // pair keys as found (pair_capacity)
+    uint64_t* pair_keys;         // pair keys sorted: canonical pair list
+    void* pair_sort_scratch;
+    uint64_t pair_sort_scratch_bytes;
     GpuContact* contacts[2];     // ping-pong, pair_capacity rows each
     uint64_t* contact_keys[2];
     uint32_t* features[2];
@@ -77,6 +89,7 @@ struct StepBuffers {
     uint64_t* lookback;          // look-back words for ordered compaction
     uint64_t lookback_words;     // per site
     uint32_t* tickets;           // 8 tile tickets
+    uint32_t* grid_barrier;      // count + generation of the cooperative solver's barrier
     GpuDiagnostics* diag;
     DevTick* tick;
     DevCounts* counts;

@@ -13,8 +13,6 @@
 namespace mk {
 
 constexpr uint32_t kSortThreads = 256;
-constexpr uint32_t kSortItems = 8;
-constexpr uint32_t kSortTile = kSortThreads * kSortItems;   // 2048 keys per tile
 constexpr uint32_t kRadixBins = 256;
 
 // 30-bit digit look-back words: bits 30-31 status, 0-29 count.
@@ -24,9 +22,17 @@ constexpr uint32_t kDigitCountMask = (1u << 30) - 1;
 
 __global__ void __launch_bounds__(kSortThreads)
 k_radix_histogram(const uint64_t* __restrict__ keys, const uint32_t* __restrict__ n_ptr, uint32_t n_fixed,
-                  uint32_t passes, uint32_t* __restrict__ hist /* passes x 256 */) {
+                  uint32_t passes, uint32_t* __restrict__ hist /* passes x 256 */,
+                  uint32_t* __restrict__ lookback, uint64_t lookback_pass_words, uint32_t tile_keys) {
     __shared__ uint32_t s_hist[8][kRadixBins];
     const uint32_t n = n_ptr ? *n_ptr : n_fixed;
+    // clear the look-back words the onesweep passes will use for this n only
+    const uint64_t used = (uint64_t)((n + tile_keys - 1) / tile_keys) * kRadixBins;
+    for (uint64_t w = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; w < used * passes;
+         w += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t pass = w / used, off = w % used;
+        lookback[pass * lookback_pass_words + off] = 0u;
+    }
     for (uint32_t i = threadIdx.x; i < 8 * kRadixBins; i += blockDim.x) (&s_hist[0][0])[i] = 0;
     __syncthreads();
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
@@ -56,14 +62,16 @@ __device__ __forceinline__ uint32_t lanemask_lt() {
     return m;
 }
 
+template <uint32_t kSortItems>
 __global__ void __launch_bounds__(kSortThreads)
 k_radix_onesweep(const uint64_t* __restrict__ keys_in, const uint32_t* __restrict__ vals_in,
                  uint64_t* __restrict__ keys_out, uint32_t* __restrict__ vals_out,
                  const uint32_t* __restrict__ n_ptr, uint32_t n_fixed, uint32_t shift,
                  const uint32_t* __restrict__ digit_offsets /* 256 */, uint32_t* __restrict__ lookback,
                  uint32_t* __restrict__ ticket, uint32_t* __restrict__ error_flags) {
-    __shared__ uint64_t s_keys[kSortTile];
-    __shared__ uint32_t s_vals[kSortTile];
+    constexpr uint32_t kTile = kSortThreads * kSortItems;
+    __shared__ uint64_t s_keys[kTile];
+    __shared__ uint32_t s_vals[kTile];
     __shared__ uint32_t s_warp[kSortThreads / 32][kRadixBins];
     __shared__ uint32_t s_local_start[kRadixBins];
     __shared__ uint32_t s_global_base[kRadixBins];
@@ -71,7 +79,7 @@ k_radix_onesweep(const uint64_t* __restrict__ keys_in, const uint32_t* __restric
     __shared__ uint32_t s_tile;
 
     const uint32_t n = n_ptr ? *n_ptr : n_fixed;
-    const uint32_t tiles = (n + kSortTile - 1) / kSortTile;
+    const uint32_t tiles = (n + kTile - 1) / kTile;
     const uint32_t lane = lane_id(), w = warp_id();
 
     for (;;) {
@@ -81,7 +89,7 @@ k_radix_onesweep(const uint64_t* __restrict__ keys_in, const uint32_t* __restric
         __syncthreads();
         const uint32_t tile = s_tile;
         if (tile >= tiles) break;
-        const uint32_t tile_base = tile * kSortTile;
+        const uint32_t tile_base = tile * kTile;
 
         // ---- load (warp-striped) and rank within each warp, item by item
         uint64_t k[kSortItems];
@@ -93,7 +101,7 @@ k_radix_onesweep(const uint64_t* __restrict__ keys_in, const uint32_t* __restric
             uint32_t idx = tile_base + w * 32 * kSortItems + i * 32 + lane;
             bool valid = idx < n;
             k[i] = valid ? keys_in[idx] : 0ull;
-            v[i] = valid ? vals_in[idx] : 0u;
+            v[i] = (valid && vals_in) ? vals_in[idx] : 0u;
             uint32_t d = valid ? (uint32_t)((k[i] >> shift) & 0xffu) : kRadixBins;
             dig[i] = d;
             uint32_t peers = __match_any_sync(0xffffffffu, d);
@@ -151,7 +159,7 @@ k_radix_onesweep(const uint64_t* __restrict__ keys_in, const uint32_t* __restric
             if (dig[i] < kRadixBins) {
                 uint32_t r = s_local_start[dig[i]] + s_warp[w][dig[i]] + rank[i];
                 s_keys[r] = k[i];
-                s_vals[r] = v[i];
+                if (vals_out) s_vals[r] = v[i];
             }
         }
         __syncthreads();
@@ -160,7 +168,7 @@ k_radix_onesweep(const uint64_t* __restrict__ keys_in, const uint32_t* __restric
             uint32_t dd = (uint32_t)((kk >> shift) & 0xffu);
             uint32_t dst = s_global_base[dd] + j;
             keys_out[dst] = kk;
-            vals_out[dst] = s_vals[j];
+            if (vals_out) vals_out[dst] = s_vals[j];
         }
         __syncthreads();
     }
@@ -168,16 +176,36 @@ k_radix_onesweep(const uint64_t* __restrict__ keys_in, const uint32_t* __restric
 
 uint32_t sort_passes(uint32_t key_bits) { return (key_bits + 7) / 8; }
 
-uint64_t sort_scratch_bytes(uint32_t n, uint32_t key_bits) {
+// Keys per thread of the onesweep tile: smaller tiles spread small sorts over
+// more SMs, larger tiles amortise the look-back on large ones.  The choice is
+// a tuning parameter (set_sort_items overrides the size-based default).
+static uint32_t g_sort_items_override = 0;
+void set_sort_items(uint32_t items) { g_sort_items_override = items; }
+uint32_t sort_items_for(uint32_t n) {
+    if (g_sort_items_override == 2 || g_sort_items_override == 4 || g_sort_items_override == 8)
+        return g_sort_items_override;
+    (void)n;
+    return 8u;   // measured fastest for 0.4M-14M keys on B200 (look-back chains dominate small tiles)
+}
+
+uint64_t sort_scratch_bytes(uint32_t n, uint32_t key_bits, bool values) {
     uint32_t passes = sort_passes(key_bits);
-    uint64_t tiles = (n + kSortTile - 1) / kSortTile;
+    uint64_t tiles = (n + 2 * kSortThreads - 1) / (2 * kSortThreads);   // smallest tile: 512 keys
     uint64_t b = 0;
     b += align256((uint64_t)n * 8);                       // ping-pong keys
-    b += align256((uint64_t)n * 4);                       // ping-pong values
+    b += align256((uint64_t)(values ? n : 0) * 4);        // ping-pong values
     b += align256((uint64_t)passes * kRadixBins * 4);     // histograms / offsets
-    b += align256((uint64_t)passes * (tiles ? tiles : 1) * kRadixBins * 4);   // look-back words
     b += align256((uint64_t)passes * 4);                  // tile tickets
+    b += align256((uint64_t)passes * (tiles ? tiles : 1) * kRadixBins * 4);   // look-back words
     return b;
+}
+
+template <uint32_t kItems>
+static void launch_pass(const uint64_t* sk, const uint32_t* sv, uint64_t* dk, uint32_t* dv, const uint32_t* n_dev,
+                        uint32_t n, uint32_t shift, const uint32_t* offsets, uint32_t* lookback, uint32_t* ticket,
+                        uint32_t* error_flags, uint32_t grid, cudaStream_t stream) {
+    k_radix_onesweep<kItems><<<grid, kSortThreads, 0, stream>>>(sk, sv, dk, dv, n_dev, n, shift, offsets, lookback,
+                                                                ticket, error_flags);
 }
 
 // Stream-ordered sort.  `n_dev` (device count) may be null, then n is used;
@@ -188,22 +216,28 @@ cudaError_t launch_sort(const uint64_t* keys_in, const uint32_t* vals_in, uint64
     if (n == 0) return cudaSuccess;
     uint32_t passes = sort_passes(key_bits);
     if (passes == 0 || passes > 8) return cudaErrorInvalidValue;
-    if (scratch_bytes < sort_scratch_bytes(n, key_bits)) return cudaErrorInvalidValue;
-    uint64_t tiles = (n + kSortTile - 1) / kSortTile;
+    const bool values = vals_in != nullptr;
+    if (scratch_bytes < sort_scratch_bytes(n, key_bits, values)) return cudaErrorInvalidValue;
+    const uint32_t items = sort_items_for(n);
+    const uint32_t tile_keys = kSortThreads * items;
+    const uint64_t tiles = (n + tile_keys - 1) / tile_keys;
+    const uint64_t tiles_max = (n + 2 * kSortThreads - 1) / (2 * kSortThreads);
     char* p = (char*)scratch;
     uint64_t* tmp_keys = (uint64_t*)p; p += align256((uint64_t)n * 8);
-    uint32_t* tmp_vals = (uint32_t*)p; p += align256((uint64_t)n * 4);
+    uint32_t* tmp_vals = values ? (uint32_t*)p : nullptr; p += align256((uint64_t)(values ? n : 0) * 4);
     uint32_t* hist = (uint32_t*)p; p += align256((uint64_t)passes * kRadixBins * 4);
-    uint32_t* lookback = (uint32_t*)p; p += align256((uint64_t)passes * tiles * kRadixBins * 4);
-    uint32_t* tickets = (uint32_t*)p;
-    uint64_t zero_bytes = (uint64_t)((char*)tickets - (char*)hist) + passes * 4;
-    cudaError_t e = cudaMemsetAsync(hist, 0, zero_bytes, stream);
+    uint32_t* tickets = (uint32_t*)p; p += align256((uint64_t)passes * 4);
+    uint32_t* lookback = (uint32_t*)p;
+    // histogram bins and tile tickets are cleared here; look-back words by the
+    // histogram kernel, only as many as the device-side count needs
+    cudaError_t e = cudaMemsetAsync(hist, 0, (uint64_t)((char*)tickets - (char*)hist) + passes * 4, stream);
     if (e != cudaSuccess) return e;
     uint32_t hist_blocks = (uint32_t)std::min<uint64_t>((n + 4095) / 4096, (uint64_t)sm_count * 4);
     if (hist_blocks == 0) hist_blocks = 1;
-    k_radix_histogram<<<hist_blocks, 256, 0, stream>>>(keys_in, n_dev, n, passes, hist);
+    k_radix_histogram<<<hist_blocks, 256, 0, stream>>>(keys_in, n_dev, n, passes, hist, lookback,
+                                                       tiles_max * kRadixBins, tile_keys);
     k_radix_offsets<<<passes, kRadixBins, 0, stream>>>(hist);
-    uint32_t grid = (uint32_t)std::min<uint64_t>(tiles, (uint64_t)sm_count * 3);
+    uint32_t grid = (uint32_t)std::min<uint64_t>(tiles, (uint64_t)sm_count * (items == 8 ? 3 : 6));
     if (grid == 0) grid = 1;
     // passes alternate between (tmp, out) so that the last pass writes `out`.
     const uint64_t* src_k = keys_in;
@@ -211,11 +245,17 @@ cudaError_t launch_sort(const uint64_t* keys_in, const uint32_t* vals_in, uint64
     for (uint32_t pass = 0; pass < passes; ++pass) {
         bool to_out = ((passes - 1 - pass) % 2) == 0;
         uint64_t* dk = to_out ? keys_out : tmp_keys;
-        uint32_t* dv = to_out ? vals_out : tmp_vals;
-        k_radix_onesweep<<<grid, kSortThreads, 0, stream>>>(src_k, src_v, dk, dv, n_dev, n, 8 * pass,
-                                                             hist + pass * kRadixBins,
-                                                             lookback + (size_t)pass * tiles * kRadixBins,
-                                                             tickets + pass, error_flags);
+        uint32_t* dv = values ? (to_out ? vals_out : tmp_vals) : nullptr;
+        uint32_t* lb = lookback + (size_t)pass * tiles_max * kRadixBins;
+        if (items == 2)
+            launch_pass<2>(src_k, src_v, dk, dv, n_dev, n, 8 * pass, hist + pass * kRadixBins, lb, tickets + pass,
+                           error_flags, grid, stream);
+        else if (items == 4)
+            launch_pass<4>(src_k, src_v, dk, dv, n_dev, n, 8 * pass, hist + pass * kRadixBins, lb, tickets + pass,
+                           error_flags, grid, stream);
+        else
+            launch_pass<8>(src_k, src_v, dk, dv, n_dev, n, 8 * pass, hist + pass * kRadixBins, lb, tickets + pass,
+                           error_flags, grid, stream);
         src_k = dk;
         src_v = dv;
     }

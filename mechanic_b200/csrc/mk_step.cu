@@ -7,12 +7,12 @@
 //   lbvh.wgsl sort_* :132-217                                -> mk_sort.cu (onesweep)
 //   lbvh.wgsl build_topology :233-278                        -> k_karras
 //   lbvh.wgsl prepare_leaves + build_bounds :280-319         -> k_refit
-//   lbvh.wgsl traverse :361-398                              -> k_traverse<count|write> + k_scan_offsets
+//   lbvh.wgsl traverse :361-398                              -> k_traverse + pair-key radix sort
 //   collision.wgsl narrowphase :570-603                      -> k_narrowphase
 //   collision.wgsl generate_ground_contacts :622-664         -> k_ground
 //   collision.wgsl prepare_contacts :674-736                 -> k_prepare
-//   collision.wgsl warm_start / solve_accumulate :774-906    -> k_solve<warm>
-//   collision.wgsl solve_apply :1050-1069                    -> k_apply
+//   collision.wgsl warm_start / solve_accumulate :774-906 and
+//   solve_apply :1050-1069 (8 iterations)                    -> k_solve_all (cooperative, grid barriers)
 //   collision.wgsl persist_contacts :1071-1088               -> the contact list itself (ping-pong)
 //
 // Variable-size stages (pairs, contacts, active contacts) run as persistent
@@ -27,8 +27,6 @@
 namespace mk {
 
 constexpr uint32_t kBlock = 256;
-constexpr uint32_t kScanItems = 4;
-constexpr uint32_t kScanTile = kBlock * kScanItems;
 constexpr uint32_t kFixedScale = 1048576;   // FIXED_VELOCITY_SCALE (collision.wgsl:63)
 
 // ---------------------------------------------------------------- integrate
@@ -216,8 +214,14 @@ __global__ void __launch_bounds__(kBlock) k_karras(StepBuffers b, StepParams p) 
 }
 
 // lbvh.wgsl:280-319: leaf boxes in sorted order, then a bottom-up climb where
-// the second arrival at a node writes the union.  min.w carries the largest
-// collider index below the node (prunes the j > i query).
+// the second arrival at a node writes the union.  Besides the union (kept for
+// the climb, min.w = last sorted leaf position below the node) each internal
+// node gets a 64-byte traversal record with both children's boxes:
+// {lmin, left code}, {lmax, left last}, {rmin, right code}, {rmax, right last}.
+// A child code is the internal node index, or 0x80000000 | collider index
+// for a leaf; "last" is the largest sorted leaf position below the child.
+constexpr uint32_t kLeafCode = 0x80000000u;
+
 __global__ void __launch_bounds__(kBlock) k_refit(StepBuffers b, StepParams p) {
     const uint32_t n = p.collider_count;
     const uint32_t leaf = blockIdx.x * blockDim.x + threadIdx.x;
@@ -225,17 +229,18 @@ __global__ void __launch_bounds__(kBlock) k_refit(StepBuffers b, StepParams p) {
     const uint32_t leaf_base = n - 1;
     const uint32_t j = b.svals[leaf];
     float4 mn = b.aabbs[2ull * j], mx = b.aabbs[2ull * j + 1];
-    mn.w = __uint_as_float(j);
+    mn.w = __uint_as_float(leaf);
     uint32_t cur = leaf_base + leaf;
     b.node_aabbs[2ull * cur] = mn;
     b.node_aabbs[2ull * cur + 1] = mx;
     if (n <= 1) return;
-    __threadfence();
     for (uint32_t guard = 0; guard < 2 * n; ++guard) {
         const uint32_t ep = b.parents[cur];
         if (ep == 0u) return;
         const uint32_t parent = ep - 1u;
-        const uint32_t arrival = atomicAdd(&b.visits[parent], 1u);
+        // release: this node's box is visible to whoever arrives second;
+        // acquire: the sibling's box (released by its add) is visible to us
+        const uint32_t arrival = atomic_add_acq_rel(&b.visits[parent], 1u);
         if (arrival == 0u) return;
         if (arrival > 1u) {
             atomicOr(&b.diag->error_flags, MK_PAIR_OVERFLOW_FLAG);
@@ -244,12 +249,18 @@ __global__ void __launch_bounds__(kBlock) k_refit(StepBuffers b, StepParams p) {
         const uint2 ch = b.children[parent];
         const float4 lmn = __ldcg(b.node_aabbs + 2ull * ch.x), lmx = __ldcg(b.node_aabbs + 2ull * ch.x + 1);
         const float4 rmn = __ldcg(b.node_aabbs + 2ull * ch.y), rmx = __ldcg(b.node_aabbs + 2ull * ch.y + 1);
+        const uint32_t lcode = ch.x >= leaf_base ? (kLeafCode | b.svals[ch.x - leaf_base]) : ch.x;
+        const uint32_t rcode = ch.y >= leaf_base ? (kLeafCode | b.svals[ch.y - leaf_base]) : ch.y;
+        float4* rec = b.node_records + 4ull * parent;
+        rec[0] = make_float4(lmn.x, lmn.y, lmn.z, __uint_as_float(lcode));
+        rec[1] = make_float4(lmx.x, lmx.y, lmx.z, lmn.w);
+        rec[2] = make_float4(rmn.x, rmn.y, rmn.z, __uint_as_float(rcode));
+        rec[3] = make_float4(rmx.x, rmx.y, rmx.z, rmn.w);
         float4 pm = make_float4(mnf(lmn.x, rmn.x), mnf(lmn.y, rmn.y), mnf(lmn.z, rmn.z),
                                 __uint_as_float(max(__float_as_uint(lmn.w), __float_as_uint(rmn.w))));
         float4 px = make_float4(mxf(lmx.x, rmx.x), mxf(lmx.y, rmx.y), mxf(lmx.z, rmx.z), 0.0f);
         b.node_aabbs[2ull * parent] = pm;
         b.node_aabbs[2ull * parent + 1] = px;
-        __threadfence();
         cur = parent;
     }
 }
@@ -277,132 +288,86 @@ __device__ __forceinline__ bool pair_is_suppressed(const uint2* __restrict__ sup
 }
 
 constexpr uint32_t kStack = 64;
-constexpr uint32_t kLocalPairs = 48;
+constexpr uint32_t kTravThreads = 128;
+constexpr uint32_t kStage = 512;   // pair keys staged per warp in shared memory
 
-// One query per collider index i: every leaf j > i of another, unsuppressed
-// body whose box overlaps i's box (the pair set of lbvh.wgsl:361-398, with
-// (i, j) ordered as the reference emits them).  kWrite=false counts,
-// kWrite=true writes at the scanned offset and sorts the segment by j.
-template <bool kWrite>
-__global__ void __launch_bounds__(128) k_traverse(StepBuffers b, StepParams p) {
+// The pair set of lbvh.wgsl:361-398: every collider pair of different,
+// unsuppressed bodies whose closed boxes overlap.  Threads take sorted leaves
+// in order (neighbouring boxes in a warp walk the same nodes) and look only
+// at leaves further right in Morton order, so whole left subtrees are cut off
+// and each pair is found once.  A pair is emitted as the key
+// (min index << shift) | max index into a per-warp shared-memory stage that
+// is flushed with one global reservation; the keys are radix-sorted next,
+// which yields the canonical (collider_a, collider_b) order.
+__global__ void __launch_bounds__(kTravThreads) k_traverse(StepBuffers b, StepParams p) {
+    __shared__ uint64_t s_stage[kTravThreads / 32][kStage];
+    __shared__ uint32_t s_count[kTravThreads / 32];
     const uint32_t n = p.collider_count;
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    const float4 qmin = b.aabbs[2ull * i], qmax = b.aabbs[2ull * i + 1];
-    const uint32_t body_i = __float_as_uint(b.boxes[3ull * i + 2].z);
-    const uint32_t leaf_base = n - 1;
-    uint32_t stack[kStack];
-    uint32_t sp = 1;
-    stack[0] = n > 1 ? 0u : leaf_base;
-    uint32_t count = 0;
-    uint32_t base = 0, cap_left = 0;
-    uint32_t local[kLocalPairs];
-    if (kWrite) {
-        base = b.pair_offsets[i];
-        cap_left = base < p.pair_capacity ? p.pair_capacity - base : 0u;
-    }
-    while (sp > 0) {
-        const uint32_t node = stack[--sp];
-        const float4 nmin = __ldg(b.node_aabbs + 2ull * node);
-        if (__float_as_uint(nmin.w) <= i) continue;   // no collider index above i below this node
-        const float4 nmax = __ldg(b.node_aabbs + 2ull * node + 1);
-        if (!overlaps(qmin, qmax, nmin, nmax)) continue;
-        if (node >= leaf_base) {
-            const uint32_t j = __float_as_uint(nmin.w);
-            const uint32_t body_j = __float_as_uint(__ldg(b.boxes + 3ull * j + 2).z);
-            if (body_i == body_j) continue;
-            if (p.suppression_count && pair_is_suppressed(b.suppressed, p.suppression_count, body_i, body_j)) continue;
-            if (kWrite) {
-                if (count < kLocalPairs) local[count] = j;
-                else if (count < cap_left) b.pairs[base + count] = make_uint2(i, j);
+    const uint32_t w = warp_id(), lane = lane_id();
+    if (lane == 0) s_count[w] = 0;
+    __syncwarp();
+    uint32_t* found = &b.counts->pairs_found;
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < n && n > 1) {
+        const uint32_t leaf_base = n - 1;
+        const uint32_t i = b.svals[t];
+        const float4 qmin = b.node_aabbs[2ull * (leaf_base + t)], qmax = b.node_aabbs[2ull * (leaf_base + t) + 1];
+        const uint32_t body_i = __float_as_uint(b.boxes[3ull * i + 2].z);
+        uint32_t stack[kStack];
+        uint32_t sp = 0;
+        uint32_t node = 0;
+        for (;;) {
+            const float4* rec = b.node_records + 4ull * node;
+#pragma unroll
+            for (int side = 0; side < 2; ++side) {
+                const float4 cmax = __ldg(rec + 2 * side + 1);
+                if (__float_as_uint(cmax.w) <= t) continue;     // nothing to the right of this leaf below
+                const float4 cmin = __ldg(rec + 2 * side);
+                if (!overlaps(qmin, qmax, cmin, cmax)) continue;
+                const uint32_t code = __float_as_uint(cmin.w);
+                if (code & kLeafCode) {
+                    const uint32_t j = code & ~kLeafCode;
+                    const uint32_t body_j = __float_as_uint(__ldg(b.boxes + 3ull * j + 2).z);
+                    if (body_i == body_j) continue;
+                    if (p.suppression_count && pair_is_suppressed(b.suppressed, p.suppression_count, body_i, body_j))
+                        continue;
+                    const uint64_t key = ((uint64_t)min(i, j) << p.pair_shift) | max(i, j);
+                    const uint32_t k = atomicAdd(&s_count[w], 1u);
+                    if (k < kStage) {
+                        s_stage[w][k] = key;
+                    } else {
+                        const uint32_t g = atomicAdd(found, 1u);
+                        if (g < p.pair_capacity) b.pair_stage[g] = key;
+                    }
+                } else {
+                    if (sp >= kStack) {   // lbvh.wgsl:389-392
+                        atomicOr(&b.diag->error_flags, MK_PAIR_OVERFLOW_FLAG);
+                        sp = 0;
+                        break;
+                    }
+                    stack[sp++] = code;
+                }
             }
-            ++count;
-            continue;
-        }
-        if (sp > kStack - 3) {   // lbvh.wgsl:389-392
-            atomicOr(&b.diag->error_flags, MK_PAIR_OVERFLOW_FLAG);
-            break;
-        }
-        const uint2 ch = __ldg(b.children + node);
-        stack[sp] = ch.x;
-        stack[sp + 1] = ch.y;
-        sp += 2;
-    }
-    if (!kWrite) {
-        b.pair_offsets[i] = count;
-        return;
-    }
-    const uint32_t stored = min(count, cap_left);
-    if (count <= kLocalPairs) {
-        // insertion sort in registers/local memory, then one write pass
-        for (uint32_t x = 1; x < count; ++x) {
-            uint32_t v = local[x];
-            int y = (int)x - 1;
-            while (y >= 0 && local[y] > v) { local[y + 1] = local[y]; --y; }
-            local[y + 1] = v;
-        }
-        for (uint32_t x = 0; x < stored; ++x) b.pairs[base + x] = make_uint2(i, local[x]);
-    } else {
-        uint2* seg = b.pairs + base;
-        for (uint32_t x = 0; x < kLocalPairs && x < stored; ++x) seg[x] = make_uint2(i, local[x]);
-        for (uint32_t x = 1; x < stored; ++x) {
-            uint2 v = seg[x];
-            int y = (int)x - 1;
-            while (y >= 0 && seg[y].y > v.y) { seg[y + 1] = seg[y]; --y; }
-            seg[y + 1] = v;
+            if (sp == 0) break;
+            node = stack[--sp];
         }
     }
+    __syncwarp();
+    const uint32_t staged = min(s_count[w], kStage);
+    uint32_t base = 0;
+    if (lane == 0 && staged) base = atomicAdd(found, staged);
+    base = __shfl_sync(0xffffffffu, base, 0);
+    for (uint32_t k = lane; k < staged; k += 32)
+        if (base + k < p.pair_capacity) b.pair_stage[base + k] = s_stage[w][k];
 }
 
-// Exclusive scan of the per-collider pair counts (single pass, look-back).
-__global__ void __launch_bounds__(kBlock) k_scan_offsets(StepBuffers b, StepParams p) {
-    __shared__ uint32_t s_scan[33];
-    __shared__ uint32_t s_tile;
-    __shared__ uint64_t s_prefix;
-    const uint32_t n = p.collider_count;
-    const uint32_t tiles = (n + kScanTile - 1) / kScanTile;
-    uint64_t* states = b.lookback;
-    for (;;) {
-        if (threadIdx.x == 0) s_tile = atomicAdd(&b.tickets[0], 1u);
-        __syncthreads();
-        const uint32_t tile = s_tile;
-        if (tile >= tiles) break;
-        const uint32_t base = tile * kScanTile + threadIdx.x * kScanItems;
-        uint32_t v[kScanItems];
-        uint32_t sum = 0;
-#pragma unroll
-        for (uint32_t k = 0; k < kScanItems; ++k) {
-            v[k] = base + k < n ? b.pair_offsets[base + k] : 0u;
-            sum += v[k];
-        }
-        uint32_t total;
-        const uint32_t ex = block_exclusive_scan(sum, s_scan, &total);
-        if (warp_id() == 0) {
-            uint64_t pre = tile_lookback(states, tile, total, &b.diag->error_flags);
-            if (lane_id() == 0) s_prefix = pre;
-        }
-        __syncthreads();
-        const uint64_t pre = s_prefix;
-        uint64_t run = pre + ex;
-#pragma unroll
-        for (uint32_t k = 0; k < kScanItems; ++k) {
-            if (base + k < n) b.pair_offsets[base + k] = (uint32_t)umin64(run, 0xffffffffull);
-            run += v[k];
-        }
-        if (tile == tiles - 1 && threadIdx.x == 0) {
-            const uint64_t all = pre + total;
-            b.pair_offsets[n] = (uint32_t)umin64(all, 0xffffffffull);
-            b.diag->pair_count = (uint32_t)umin64(all, 0xffffffffull);
-            b.counts->pairs = (uint32_t)umin64(all, p.pair_capacity);
-            if (all > p.pair_capacity) atomicOr(&b.diag->error_flags, MK_PAIR_OVERFLOW_FLAG);
-        }
-        __syncthreads();
-    }
-    if (blockIdx.x == 0 && threadIdx.x == 0 && tiles == 0) {
-        b.pair_offsets[n] = 0;
-        b.diag->pair_count = 0;
-        b.counts->pairs = 0;
-    }
+// Pair count of the tick (diag[1] keeps the requested count, lbvh.wgsl:353-358).
+__global__ void k_pairs_finalize(StepBuffers b, StepParams p) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    const uint32_t found = b.counts->pairs_found;
+    b.diag->pair_count = found;
+    b.counts->pairs = min(found, p.pair_capacity);
+    if (found > p.pair_capacity) atomicOr(&b.diag->error_flags, MK_PAIR_OVERFLOW_FLAG);
 }
 
 // ------------------------------------------------------------- narrowphase
@@ -554,7 +519,8 @@ __global__ void __launch_bounds__(kBlock) k_narrowphase(StepBuffers b, StepParam
         f3 pt = mkf3(0, 0, 0);
         uint32_t ba = 0, bb = 0;
         if (idx < n) {
-            pr = b.pairs[idx];
+            const uint64_t key = b.pair_keys[idx];
+            pr = make_uint2((uint32_t)(key >> p.pair_shift), (uint32_t)(key & ((1ull << p.pair_shift) - 1)));
             const Box A = make_box(b.boxes, pr.x), Bx = make_box(b.boxes, pr.y);
             ba = __float_as_uint(__ldg(b.boxes + 3ull * pr.x + 2).z);
             bb = __float_as_uint(__ldg(b.boxes + 3ull * pr.y + 2).z);
@@ -821,32 +787,40 @@ __device__ __forceinline__ bool run_tail_sum(uint32_t key, int32_t* v, int n) {
     return tail;
 }
 
-// collision.wgsl:774-906.  kWarm: warm_start (iteration 0), else solve_accumulate.
+// collision.wgsl:774-906 for the active contacts [first, A) in strides of
+// `stride`.  kWarm: warm_start (iteration 0), else solve_accumulate.  The
+// velocities of iteration k live in their own buffer pair (vl, va), written
+// by the previous phase and never written again in this launch, so they are
+// read through the L1/texture path; contact rows and deltas change between
+// phases of the launch and are read through L2 (ld.cg).
+__device__ __forceinline__ f3 contact_velocity_it(const float4* vl, const float4* va, uint32_t body, f3 arm) {
+    return xyz(__ldg(vl + body)) + cross(xyz(__ldg(va + body)), arm);
+}
+
 template <bool kWarm>
-__global__ void __launch_bounds__(kBlock) k_solve(StepBuffers b, StepParams p, GpuContact* cur) {
-    const uint32_t A = b.counts->active;
-    const uint32_t stride = gridDim.x * blockDim.x;
+__device__ __forceinline__ void solve_span(const StepBuffers& b, const StepParams& p, GpuContact* cur, uint32_t A,
+                                           uint32_t first, uint32_t stride, const float4* vl, const float4* va) {
     const float scale = (float)kFixedScale;
-    for (uint32_t base = blockIdx.x * blockDim.x; base < A; base += stride) {
+    for (uint32_t base = first; base < A; base += stride) {
         const uint32_t t = base + threadIdx.x;
         bool live = false;
         uint32_t a = kInvalid, bb = kInvalid;
         int32_t da[6] = {0, 0, 0, 0, 0, 0}, db[6] = {0, 0, 0, 0, 0, 0};
         if (t < A) {
-            const uint32_t k = b.active[t];
+            const uint32_t k = __ldcg(b.active + t);
             float4* row = reinterpret_cast<float4*>(cur + k);
-            const float4 r0 = row[0], np = row[1], aa = row[2], ab = row[3];
+            const float4 r0 = __ldcg(row), np = __ldcg(row + 1), aa = __ldcg(row + 2), ab = __ldcg(row + 3);
             a = __float_as_uint(r0.x);
             bb = __float_as_uint(r0.y);
             const f3 arm_a = xyz(aa), arm_b = xyz(ab);
             const float4* wa = b.world_mass + 3ull * a;
             const float4* wb = bb != kInvalid ? b.world_mass + 3ull * bb : nullptr;
             f3 vb = mkf3(0, 0, 0);
-            if (bb != kInvalid) vb = contact_velocity(b, bb, arm_b);
+            if (bb != kInvalid) vb = contact_velocity_it(vl, va, bb, arm_b);
             const f3 nrm = xyz(np);
             const float den = impulse_denominator(wa, wb, arm_a, arm_b, nrm);
             if (!(den <= 0.0f)) {
-                const f3 rel = vb - contact_velocity(b, a, arm_a);
+                const f3 rel = vb - contact_velocity_it(vl, va, a, arm_a);
                 const float vn = dot(rel, nrm);
                 if (np.w <= 1.0e-5f && vn >= -1.0e-5f && aa.w <= 1.0e-6f) {
                     row[2] = f4(arm_a, 0.0f);
@@ -907,22 +881,81 @@ __global__ void __launch_bounds__(kBlock) k_solve(StepBuffers b, StepParams p, G
     }
 }
 
-// collision.wgsl:1050-1069 (only dispatched with active contacts, :744).
-__global__ void __launch_bounds__(kBlock) k_apply(StepBuffers b, StepParams p) {
-    if (b.counts->active == 0u) return;
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= p.body_count) return;
-    // 6 ints per body: 24-byte rows are 8-byte aligned
-    int2* d2 = reinterpret_cast<int2*>(b.deltas + 6ull * i);
-    const int2 x0 = d2[0], x1 = d2[1], x2 = d2[2];
-    d2[0] = make_int2(0, 0);
-    d2[1] = make_int2(0, 0);
-    d2[2] = make_int2(0, 0);
+// collision.wgsl:1050-1069: v += delta / 2^20 (from the iteration's buffer
+// into the next one), then clear the delta.
+__device__ __forceinline__ void apply_span(const StepBuffers& b, const StepParams& p, uint32_t first,
+                                           uint32_t stride, const float4* sl, const float4* sa, float4* dl,
+                                           float4* da) {
     const float s = (float)kFixedScale;
-    const f3 ld = mkf3((float)x0.x, (float)x0.y, (float)x1.x) / s;
-    const f3 ad = mkf3((float)x1.y, (float)x2.x, (float)x2.y) / s;
-    b.lin[i] = f4(xyz(b.lin[i]) + ld, 0.0f);
-    b.ang[i] = f4(xyz(b.ang[i]) + ad, 0.0f);
+    for (uint32_t i = first; i < p.body_count; i += stride) {
+        int2* d2 = reinterpret_cast<int2*>(b.deltas + 6ull * i);   // 24-byte rows are 8-byte aligned
+        const int2 x0 = __ldcg(d2), x1 = __ldcg(d2 + 1), x2 = __ldcg(d2 + 2);
+        if ((x0.x | x0.y | x1.x | x1.y | x2.x | x2.y) != 0) {
+            d2[0] = make_int2(0, 0);
+            d2[1] = make_int2(0, 0);
+            d2[2] = make_int2(0, 0);
+        }
+        const f3 ld = mkf3((float)x0.x, (float)x0.y, (float)x1.x) / s;
+        const f3 ad = mkf3((float)x1.y, (float)x2.x, (float)x2.y) / s;
+        dl[i] = f4(xyz(__ldg(sl + i)) + ld, 0.0f);
+        da[i] = f4(xyz(__ldg(sa + i)) + ad, 0.0f);
+    }
+}
+
+// Grid-wide barrier for a cooperative launch.  The wait is bounded: a block
+// that gives up raises MK_DEVICE_WAIT_TIMEOUT_FLAG and carries on.
+__device__ __forceinline__ void grid_barrier(uint32_t* state, uint32_t* error_flags) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint32_t* count = state;
+        uint32_t* generation = state + 1;
+        const uint32_t gen = ld_acquire_u32(generation);
+        __threadfence();
+        const uint32_t arrived = atomicAdd(count, 1u);
+        if (arrived == gridDim.x - 1) {
+            atomicExch(count, 0u);
+            __threadfence();
+            st_release_u32(generation, gen + 1u);
+        } else {
+            uint32_t spins = 0;
+            while (ld_acquire_u32(generation) == gen) {
+                __nanosleep(20);
+                if (++spins > kSpinLimit) {
+                    atomicOr(error_flags, MK_DEVICE_WAIT_TIMEOUT_FLAG);
+                    break;
+                }
+            }
+        }
+        __threadfence();
+    }
+    __syncthreads();
+}
+
+// All solver iterations in one cooperative launch: warm start, then
+// (iterations - 1) projections, each followed by the velocity apply
+// (device.rs:1343-1416 dispatch order), separated by grid barriers.
+constexpr uint32_t kSolveThreads = 1024;   // one block per SM: 148 barrier participants
+
+__global__ void __launch_bounds__(kSolveThreads) k_solve_all(StepBuffers b, StepParams p, GpuContact* cur,
+                                                      uint32_t iterations, uint32_t* barrier) {
+    const uint32_t A = b.counts->active;
+    if (A == 0u) return;   // collision.wgsl:744-747: no solve and no apply dispatch
+    const uint32_t first = blockIdx.x * blockDim.x;
+    const uint32_t stride = gridDim.x * blockDim.x;
+    const size_t B = p.body_count;
+    for (uint32_t it = 0; it < iterations; ++it) {
+        // iteration `it` reads buffer it (0 = the integrated velocities) and
+        // its apply writes buffer it + 1 (the last one back into lin/ang)
+        const float4* sl = it == 0 ? b.lin : b.vel_iter + (2 * (it - 1)) * B;
+        const float4* sa = it == 0 ? b.ang : b.vel_iter + (2 * (it - 1) + 1) * B;
+        float4* dl = it + 1 == iterations ? b.lin : b.vel_iter + (2 * it) * B;
+        float4* da = it + 1 == iterations ? b.ang : b.vel_iter + (2 * it + 1) * B;
+        if (it == 0) solve_span<true>(b, p, cur, A, first, stride, sl, sa);
+        else solve_span<false>(b, p, cur, A, first, stride, sl, sa);
+        grid_barrier(barrier, &b.diag->error_flags);
+        apply_span(b, p, first + threadIdx.x, stride, sl, sa, dl, da);
+        grid_barrier(barrier, &b.diag->error_flags);
+    }
 }
 
 // Bookkeeping at the end of a tick: this tick's contact list becomes the
@@ -1007,10 +1040,12 @@ cudaError_t launch_broadphase(const StepBuffers& b, const StepParams& p, const S
     if (e != cudaSuccess) return e;
     k_karras<<<blocks_for(C, kBlock), kBlock, 0, s>>>(b, p);
     k_refit<<<blocks_for(C, kBlock), kBlock, 0, s>>>(b, p);
-    k_traverse<false><<<blocks_for(C, 128), 128, 0, s>>>(b, p);
-    const uint32_t tiles = blocks_for(C, kScanTile);
-    k_scan_offsets<<<std::min<uint32_t>(tiles, (uint32_t)l.sm_count * 2), kBlock, 0, s>>>(b, p);
-    k_traverse<true><<<blocks_for(C, 128), 128, 0, s>>>(b, p);
+    k_traverse<<<blocks_for(C, kTravThreads), kTravThreads, 0, s>>>(b, p);
+    k_pairs_finalize<<<1, 32, 0, s>>>(b, p);
+    e = launch_sort(b.pair_stage, nullptr, b.pair_keys, nullptr, p.pair_capacity, &b.counts->pairs,
+                    2 * p.pair_shift, b.pair_sort_scratch, b.pair_sort_scratch_bytes, &b.diag->error_flags, s,
+                    l.sm_count);
+    if (e != cudaSuccess) return e;
     return cudaGetLastError();
 }
 
@@ -1032,12 +1067,29 @@ cudaError_t launch_contact_solver(const StepBuffers& b, const StepParams& p, con
     const int prev = parity ^ 1;
     k_prepare<<<grid, kBlock, 0, s>>>(b, p, prep, b.contacts[parity], b.contact_keys[parity], b.features[parity],
                                        b.contacts[prev], b.contact_keys[prev], b.features[prev]);
+    // one co-resident grid for every iteration (cooperative launch)
+    int per_sm = 0;
+    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_solve_all, kSolveThreads, 0);
+    if (e != cudaSuccess) return e;
+    if (per_sm < 1) return cudaErrorInvalidConfiguration;
+    const uint32_t blocks = (uint32_t)l.sm_count;
     const uint32_t iters = std::max<uint32_t>(1u, l.iterations);
-    for (uint32_t it = 0; it < iters; ++it) {
-        if (it == 0) k_solve<true><<<grid, kBlock, 0, s>>>(b, p, b.contacts[parity]);
-        else k_solve<false><<<grid, kBlock, 0, s>>>(b, p, b.contacts[parity]);
-        k_apply<<<blocks_for(p.body_count, kBlock), kBlock, 0, s>>>(b, p);
-    }
+    GpuContact* cur = b.contacts[parity];
+    uint32_t* barrier = b.grid_barrier;
+    StepBuffers bb = b;
+    StepParams pp = p;
+    void* args[] = {&bb, &pp, &cur, (void*)&iters, &barrier};
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(blocks);
+    cfg.blockDim = dim3(kSolveThreads);
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    e = cudaLaunchKernelExC(&cfg, (const void*)k_solve_all, args);
+    if (e != cudaSuccess) return e;
     return cudaGetLastError();
 }
 

@@ -24,6 +24,7 @@ EXPORTS = [
     "mk_write_drives", "mk_init_coordinates", "mk_body_count", "mk_has_gpu_timestamps",
     "mk_state_buffers", "mk_save_state", "mk_load_state", "mk_read_buffer", "mk_version",
     "mk_last_error", "mk_op_sort_scratch_bytes", "mk_op_sort_keys", "mk_op_obb_sat",
+    "mk_tick_kernel_count", "mk_set_tuning",
 ]
 
 _lib = None
@@ -62,6 +63,8 @@ def library(path: str | None = None):
         "mk_op_sort_scratch_bytes": (u64, [u32]),
         "mk_op_sort_keys": (i32, [vp, vp, vp, vp, u32, u32, vp, u64, vp]),
         "mk_op_obb_sat": (i32, [vp, vp, u32, vp, vp, vp]),
+        "mk_tick_kernel_count": (u32, [vp]),
+        "mk_set_tuning": (i32, [u32, u32]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -276,6 +279,9 @@ class GpuPhysics:
     def body_count(self) -> int:
         return int(library().mk_body_count(self._h))
 
+    def tick_kernel_count(self) -> int:
+        return int(library().mk_tick_kernel_count(self._h))
+
     def has_gpu_timestamps(self) -> bool:
         return bool(library().mk_has_gpu_timestamps(self._h))
 
@@ -361,6 +367,14 @@ class GpuPhysics:
 
     def links(self):
         return self.read_buffer(abi.BUF_LINKS, abi.LINK_STATE, 48)
+
+
+TUNE_SORT_ITEMS = 1
+
+
+def set_tuning(key: int, value: int) -> int:
+    """Process-wide tuning knob (mk_set_tuning); applies to handles created afterwards."""
+    return int(library().mk_set_tuning(int(key), int(value)))
 
 
 def version() -> str:

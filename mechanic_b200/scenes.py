@@ -406,3 +406,22 @@ def compound_mass_properties(parts, density=CUBOID_DENSITY):
         off = center - com
         inertia += own + m * (np.eye(3) * off.dot(off) - np.outer(off, off))
     return np.float32(total), com.astype(np.float32), inertia.astype(np.float32)
+
+
+REFERENCE_DENSITY = np.float32(500.0)   # CUBOID_DENSITY_KG_M3 (mechanic-core lib.rs:35)
+
+
+def dense_grid(count: int = 100_000) -> Scene:
+    """mechanic-bench's dense scene (crates/mechanic-bench/src/main.rs:442-454): `count`
+    one-metre cubes on a 50 x 40 x z grid of 1 m pitch, centres at (x, y + 0.5, z), resting
+    and touching, reference density 500 kg/m^3, zero velocity."""
+    idx = np.arange(count)
+    x = (idx % 50).astype(np.float32)
+    y = ((idx // 50) % 40).astype(np.float32) + np.float32(0.5)
+    z = (idx // 2000).astype(np.float32)
+    translation = np.stack([x, y, z], 1).astype(np.float32)
+    rotation = np.zeros((count, 4))
+    rotation[:, 3] = 1.0
+    zeros = np.zeros(count)
+    return _assemble(translation, rotation, np.zeros(count, bool), zeros, zeros, zeros, (1.0, 1.0, 1.0),
+                     f"dense_{count}", density=REFERENCE_DENSITY)

@@ -166,10 +166,16 @@ def test_pair_overflow_sets_flag_without_overrun(cuda_lib):
     rb = gpu.read_last_tick()
     assert rb.error_flags & abi.PAIR_OVERFLOW_FLAG
     assert rb.pair_count > 64
-    assert len(gpu.pairs()) == 64
-    orc = oracle.OracleWorld(scene, GpuPhysicsConfig().to_c(), pair_capacity=64)
+    pairs = gpu.pairs()
+    assert len(pairs) == 64
+    # which pairs survive an overflow depends on arrival order (as in the
+    # reference, lbvh.wgsl:353-358); they are still real pairs, in canonical order
+    orc = oracle.OracleWorld(scene, GpuPhysicsConfig().to_c(), pair_capacity=1 << 22)
     orc.step(1)
-    assert np.array_equal(gpu.pairs(), orc.pairs())
+    assert rb.pair_count == orc.pair_count
+    ref = {(int(a), int(b)) for a, b in orc.pairs()[["collider_a", "collider_b"]].tolist()}
+    got = [(int(a), int(b)) for a, b in pairs[["collider_a", "collider_b"]].tolist()]
+    assert got == sorted(got) and set(got) <= ref
 
 
 def test_nan_input_sets_invalid_numeric(cuda_lib):
