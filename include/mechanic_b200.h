@@ -449,6 +449,21 @@ MK_API int mk_op_sort_keys(const uint64_t* keys_in, const uint32_t* values_in,
                     uint32_t key_bits, void* scratch, uint64_t scratch_bytes,
                     void* stream);
 
+/* The same sort for callers that cannot allocate device memory when they
+ * need it (code inside host callbacks or allocator hooks, embedders with a
+ * fixed memory budget).  No counterpart in the reference.  Its scratch is a
+ * static device array owned by the library (about 14 MB on every GPU that
+ * loads it, kept until exit), so only inputs and outputs are passed and
+ * nothing is allocated.  At most MK_STATIC_SORT_MAX_KEYS keys; larger n
+ * returns MK_ERR_INVALID_ARGUMENT with the reason in mk_last_error().  The
+ * first call on each device (with it current) looks up the array's device
+ * address: make it before any stream capture.  All calls share the array, so
+ * calls that overlap on the GPU race and must be ordered by the caller. */
+#define MK_STATIC_SORT_MAX_KEYS 524288u
+MK_API int mk_op_sort_keys_static(const uint64_t* keys_in, const uint32_t* values_in,
+                                  uint64_t* keys_out, uint32_t* values_out, uint32_t n,
+                                  uint32_t key_bits, void* stream);
+
 /* Batched OBB separating-axis test of collision.wgsl:393-486 for `count`
  * pairs of world boxes.  Each box is four float4 rows:
  * {center.xyz, half_x}, {axis_x.xyz, half_y}, {axis_y.xyz, half_z},

@@ -52,6 +52,8 @@ void set_error(MkError* err, int code, const char* fmt, ...) {
 
 }  // namespace
 
+void mk::set_last_error(const char* msg) { g_last_error = msg ? msg : ""; }
+
 struct MkHandle {
     int device = 0;
     int sm_count = 148;

@@ -11,6 +11,9 @@ namespace mk {
 
 inline uint64_t align256(uint64_t b) { return (b + 255) & ~255ull; }
 
+// Records the text mk_last_error() returns on this thread.
+void set_last_error(const char* msg);
+
 // Per-tick values the host writes before each graph launch (64 bytes).
 struct DevTick {
     uint32_t tick_index;

@@ -24,7 +24,7 @@ EXPORTS = [
     "mk_write_drives", "mk_init_coordinates", "mk_body_count", "mk_has_gpu_timestamps",
     "mk_state_buffers", "mk_save_state", "mk_load_state", "mk_read_buffer", "mk_version",
     "mk_last_error", "mk_op_sort_scratch_bytes", "mk_op_sort_keys", "mk_op_obb_sat",
-    "mk_tick_kernel_count", "mk_set_tuning",
+    "mk_tick_kernel_count", "mk_set_tuning", "mk_op_sort_keys_static",
 ]
 
 _lib = None
@@ -65,6 +65,7 @@ def library(path: str | None = None):
         "mk_op_obb_sat": (i32, [vp, vp, u32, vp, vp, vp]),
         "mk_tick_kernel_count": (u32, [vp]),
         "mk_set_tuning": (i32, [u32, u32]),
+        "mk_op_sort_keys_static": (i32, [vp, vp, vp, vp, u32, u32, vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
