@@ -84,6 +84,7 @@ struct MkHandle {
     uint64_t last_submission = 0;
     bool any_tick = false;
     uint32_t kernels_per_tick = 0;
+    std::vector<uint32_t> mech_level_offsets;   // host side of MechBuffers::level_offsets
 };
 
 namespace {
@@ -162,7 +163,8 @@ uint64_t carve(MkHandle* h, char* base) {
     h->staging = c.take<float4>(2ull * B);
     // mechanism buffers
     if (h->mechanism_active || h->J > 0) {
-        mk::carve_mechanism(h->mech, h->B, h->J, h->Q, [&](uint64_t bytes) { return c.take<char>(bytes); });
+        mk::carve_mechanism(h->mech, h->mech_params, h->B, h->J, h->Q,
+                            [&](uint64_t bytes) { return c.take<char>(bytes); });
     }
     if (h->config.mechanism_self_collisions == 0) b.components = c.take<uint32_t>(B);
     return c.off;
@@ -409,6 +411,7 @@ int mk_create(const MkCreation* cr, const MkConfig* config, const MkCapacities* 
     h->launch.iterations = std::max(1u, c.solver_iterations ? c.solver_iterations : 8u);
     h->launch.collisions = h->collisions;
     h->mech_params = mk::make_mech_params(cr, h->params, h->launch.iterations, c.closure_mode);
+    const mk::MechTopology topo = mk::derive_topology(cr, h->mech_params);
 
     bool ok = check(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking), err, "stream");
     const uint64_t bytes = ok ? carve(h, nullptr) : 0;
@@ -458,7 +461,10 @@ int mk_create(const MkCreation* cr, const MkConfig* config, const MkCapacities* 
         ok = check(upload<uint32_t>(const_cast<uint32_t*>(b.components), comp.data(), h->B, s), err, "components");
         ok = ok && check(cudaStreamSynchronize(s), err, "sync");
     }
-    if (ok && (h->mechanism_active || h->J > 0)) ok = mk::upload_mechanism(h->mech, cr, s, err);
+    if (ok && (h->mechanism_active || h->J > 0)) ok = mk::upload_mechanism(h->mech, h->mech_params, topo, cr, s, err);
+    h->mech_level_offsets = topo.level_offsets;
+    h->mech.level_offsets = h->mech_level_offsets.data();
+    h->mech.level_count = h->mech_level_offsets.empty() ? 0u : (uint32_t)h->mech_level_offsets.size() - 1u;
     ok = ok && check(cudaStreamSynchronize(s), err, "upload sync");
     // Snapshot ring starts as the initial pose (device.rs:666-684).
     for (uint32_t slot = 0; ok && slot < 3; ++slot) {
@@ -564,7 +570,7 @@ int mk_read_last_tick(MkHandle* h, MkTickReadback* out) {
         for (float m : ms) total += m;
         out->gpu_tick_ms = total;
     }
-    mk::read_mechanism_readback(h->mech, out);
+    mk::read_mechanism_readback(h->mech, d, out);
     return MK_OK;
 }
 

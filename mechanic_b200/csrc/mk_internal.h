@@ -3,6 +3,7 @@
 
 #include <algorithm>
 #include <cstdint>
+#include <functional>
 #include <cuda_runtime.h>
 
 #include "../../include/mechanic_b200.h"
@@ -119,6 +120,11 @@ cudaError_t launch_narrowphase(const StepBuffers& b, const StepParams& p, const 
 cudaError_t launch_contact_solver(const StepBuffers& b, const StepParams& p, const StepLaunch& l, int parity,
                                   cudaStream_t s);
 cudaError_t launch_finish_tick(const StepBuffers& b, const StepParams& p, int parity, cudaStream_t s);
+// Contact iterations as separate launches with a hook after each velocity
+// apply (bearing projection of mechanisms with a dynamic root).
+cudaError_t launch_contact_solver_stepwise(const StepBuffers& b, const StepParams& p, const StepLaunch& l, int parity,
+                                           bool serial, const std::function<cudaError_t(bool)>& after_apply,
+                                           cudaStream_t s);
 cudaError_t launch_apply_impulse(const StepBuffers& b, uint32_t body, float3 point, float3 impulse,
                                  cudaStream_t s);
 cudaError_t launch_obb_sat(const float* boxes_a, const float* boxes_b, uint32_t count, float* np,

@@ -1,11 +1,27 @@
 // mk_mechanism.cu — articulated passes of the tick.
 //
-// bearings.wgsl:48-102 (residual validation) is implemented here; the
-// articulated solver passes (articulated.wgsl, mechanism.wgsl, closure.wgsl)
-// report cudaErrorNotSupported until they land, so a creation with a
-// mechanism fails loudly at mk_create instead of stepping without joints.
+// Stage map (reference kernel -> this file), in the dispatch order of
+// device.rs:963-1155:
+//   articulated.wgsl project_bearing_velocities :287-316   -> k_project_bearings
+//   articulated.wgsl apply_velocity_deltas :318-337        -> k_apply_mdeltas
+//   articulated.wgsl advance_coordinates :366-415          -> k_advance_coordinates
+//   mechanism.wgsl prepare_links / jump_* :72-149          -> k_prepare_links / k_jump (list-restricted)
+//   closure.wgsl evaluate / finalize / solve_closure_pcg   -> k_closure_loop (one block, all 12 Newton steps)
+//   mechanism.wgsl publish_* :151-185                      -> k_publish
+//   articulated.wgsl reconstruct_body_velocities :431-456  -> k_reconstruct_level (one launch per depth)
+//   articulated.wgsl capture_coordinates :417-429          -> k_capture_coordinates
+//   articulated.wgsl validate_articulated_state :458-484   -> k_validate_state
+//   bearings.wgsl validate_* :68-102                       -> k_validate_bearings
+//   articulated.wgsl project_bearing_velocities_serial     -> k_project_bearings_serial
+//
+// The serial reconstruction becomes level-synchronous (every body of depth
+// d after all of depth d-1: the same arithmetic per body, so the same bits).
+// The closure accumulators are gathered per coordinate from per-joint slots
+// in the serial accumulation order instead of float atomics.
+#include <algorithm>
 #include <cstdio>
 #include <cstring>
+#include <map>
 #include <vector>
 
 #include "mk_device.cuh"
@@ -13,6 +29,12 @@
 
 namespace mk {
 
+constexpr uint32_t kMBlock = 256;
+constexpr uint32_t kClosureThreads = 1024;
+constexpr uint32_t kClosureSteps = 12;     // device.rs:974
+constexpr uint32_t kClosureRounds = 8;     // closure.wgsl:356
+
+// ----------------------------------------------------------------- host side
 MechParams make_mech_params(const MkCreation* cr, const StepParams& p, uint32_t iterations, uint32_t closure_mode) {
     MechParams m;
     m.body_count = cr->body_count;
@@ -28,27 +50,108 @@ MechParams make_mech_params(const MkCreation* cr, const StepParams& p, uint32_t 
     m.iterations = iterations;
     m.closure_mode = closure_mode;
     m.has_dynamic_root = cr->has_dynamic_root;
-    m.serial_contacts = (cr->has_dynamic_root && cr->bearing_count <= 64) ? 1u : 0u;
+    m.serial_contacts = (cr->max_depth > 0 && cr->has_dynamic_root && cr->bearing_count <= 64) ? 1u : 0u;
     m.dt = p.dt;
     m.ang_damp = p.ang_damp;
     return m;
 }
 
-void carve_mechanism(MechBuffers& m, uint32_t B, uint32_t J, uint32_t Q, const std::function<char*(uint64_t)>& take) {
+MechTopology derive_topology(const MkCreation* cr, MechParams& p) {
+    MechTopology t;
+    const uint32_t B = cr->body_count;
+    if (cr->max_depth == 0 || !cr->mechanism_bodies) return t;
+    const GpuMechanismBody* mb = cr->mechanism_bodies;
+    // depth levels 1..max_depth (roots are skipped by the reconstruction)
+    t.level_offsets.assign(cr->max_depth + 2, 0);
+    for (uint32_t i = 0; i < B; ++i)
+        if (!mb[i].metadata[3] && mb[i].traversal[1] <= cr->max_depth) ++t.level_offsets[mb[i].traversal[1] + 1];
+    for (size_t l = 1; l < t.level_offsets.size(); ++l) t.level_offsets[l] += t.level_offsets[l - 1];
+    t.level_bodies.resize(t.level_offsets.back());
+    std::vector<uint32_t> fill(t.level_offsets.begin(), t.level_offsets.end() - 1);
+    for (uint32_t i = 0; i < B; ++i)
+        if (!mb[i].metadata[3] && mb[i].traversal[1] <= cr->max_depth) t.level_bodies[fill[mb[i].traversal[1]]++] = i;
+    // closure branches: walk each endpoint to its root (closure.wgsl:154-192)
+    std::map<uint32_t, std::vector<uint32_t>> coord_slots;
+    std::vector<uint8_t> closure_root(B, 0);
+    t.cl_slot_off.push_back(0);
+    for (uint32_t j = 0; j < cr->bearing_count; ++j) {
+        const GpuBearing& br = cr->bearings[j];
+        if (br.metadata[3] == 0) continue;
+        t.cl_bearings.push_back(j);
+        for (int side = 0; side < 2; ++side) {
+            if (side == 1) t.cl_split.push_back((uint32_t)t.slot_body.size());
+            uint32_t body = br.metadata[side];
+            for (uint32_t guard = 0; guard <= B && body < B; ++guard) {
+                if (mb[body].metadata[3] != 0) { closure_root[body] = 1; break; }
+                const uint32_t coord = cr->bearings[mb[body].metadata[1]].metadata[2];
+                coord_slots[coord].push_back((uint32_t)t.slot_body.size());
+                t.slot_body.push_back(body);
+                body = mb[body].metadata[0];
+            }
+        }
+        t.cl_slot_off.push_back((uint32_t)t.slot_body.size());
+    }
+    t.cq_off.push_back(0);
+    for (auto& kv : coord_slots) {
+        t.cq_coords.push_back(kv.first);
+        for (uint32_t sl : kv.second) t.cq_slots.push_back(sl);
+        t.cq_off.push_back((uint32_t)t.cq_slots.size());
+    }
+    // bodies whose root carries a closure: the only links the closure loop changes
+    if (!t.cl_bearings.empty()) {
+        for (uint32_t i = 0; i < B; ++i) {
+            uint32_t body = i;
+            for (uint32_t guard = 0; guard <= B && mb[body].metadata[3] == 0; ++guard) body = mb[body].metadata[0];
+            if (closure_root[body]) t.cb_bodies.push_back(i);
+        }
+    }
+    p.closures = (uint32_t)t.cl_bearings.size();
+    p.slots = (uint32_t)t.slot_body.size();
+    p.closure_coords = (uint32_t)t.cq_coords.size();
+    p.closure_bodies = (uint32_t)t.cb_bodies.size();
+    return t;
+}
+
+void carve_mechanism(MechBuffers& m, const MechParams& p, uint32_t B, uint32_t J, uint32_t Q,
+                     const std::function<char*(uint64_t)>& take) {
     B = B ? B : 1;
     J = J ? J : 1;
     Q = Q ? Q : 1;
+    auto u32 = [&](uint64_t n) { return reinterpret_cast<uint32_t*>(take(4ull * (n ? n : 1))); };
+    auto f32 = [&](uint64_t n) { return reinterpret_cast<float*>(take(4ull * (n ? n : 1))); };
     m.bearings = reinterpret_cast<GpuBearing*>(take(sizeof(GpuBearing) * (uint64_t)J));
     m.bodies = reinterpret_cast<GpuMechanismBody*>(take(sizeof(GpuMechanismBody) * (uint64_t)B));
     m.coords = reinterpret_cast<GpuMechanismCoordinate*>(take(sizeof(GpuMechanismCoordinate) * (uint64_t)Q));
     m.drives = reinterpret_cast<GpuMechanismDrive*>(take(sizeof(GpuMechanismDrive) * (uint64_t)Q));
-    m.preorder = reinterpret_cast<uint32_t*>(take(4ull * B));
+    m.preorder = u32(B);
     m.links_a = reinterpret_cast<GpuLinkState*>(take(sizeof(GpuLinkState) * (uint64_t)B));
     m.links_b = reinterpret_cast<GpuLinkState*>(take(sizeof(GpuLinkState) * (uint64_t)B));
     m.deltas = reinterpret_cast<int32_t*>(take(24ull * B));
+    m.level_bodies = u32(B);
+    m.cl_bearings = u32(p.closures);
+    m.cl_slot_off = u32(p.closures + 1);
+    m.cl_split = u32(p.closures);
+    m.slot_body = u32(p.slots);
+    m.cq_coords = u32(p.closure_coords);
+    m.cq_off = u32(p.closure_coords + 1);
+    m.cq_slots = u32(p.slots);
+    m.cb_bodies = u32(p.closure_bodies);
+    m.slot_g = f32(p.slots);
+    m.slot_d = f32(p.slots);
+    m.grad = f32(Q);
+    m.diag = f32(Q);
+    m.pcg = f32(5ull * Q);
+    m.links_final = p.final_is_a ? m.links_a : m.links_b;
 }
 
-bool upload_mechanism(MechBuffers& m, const MkCreation* cr, cudaStream_t s, MkError* err) {
+template <class T>
+static cudaError_t put(T* dst, const std::vector<T>& v, cudaStream_t s) {
+    if (v.empty()) return cudaSuccess;
+    return cudaMemcpyAsync(dst, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice, s);
+}
+
+bool upload_mechanism(MechBuffers& m, const MechParams& p, const MechTopology& t, const MkCreation* cr,
+                      cudaStream_t s, MkError* err) {
     cudaError_t e = cudaSuccess;
     if (cr->bearing_count)
         e = cudaMemcpyAsync(m.bearings, cr->bearings, sizeof(GpuBearing) * cr->bearing_count, cudaMemcpyHostToDevice, s);
@@ -57,8 +160,8 @@ bool upload_mechanism(MechBuffers& m, const MkCreation* cr, cudaStream_t s, MkEr
                             cudaMemcpyHostToDevice, s);
     if (e == cudaSuccess && cr->preorder)
         e = cudaMemcpyAsync(m.preorder, cr->preorder, 4ull * cr->body_count, cudaMemcpyHostToDevice, s);
-    if (e == cudaSuccess && cr->coordinate_count) {
-        std::vector<GpuMechanismDrive> d(cr->coordinate_count);
+    std::vector<GpuMechanismDrive> d(cr->coordinate_count);
+    if (cr->coordinate_count) {
         if (cr->drives) {
             std::memcpy(d.data(), cr->drives, sizeof(GpuMechanismDrive) * cr->coordinate_count);
         } else {
@@ -68,9 +171,19 @@ bool upload_mechanism(MechBuffers& m, const MkCreation* cr, cudaStream_t s, MkEr
                 r.max_angle = INFINITY;
             }
         }
-        e = cudaMemcpyAsync(m.drives, d.data(), sizeof(GpuMechanismDrive) * d.size(), cudaMemcpyHostToDevice, s);
-        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        if (e == cudaSuccess) e = put(m.drives, d, s);
     }
+    if (e == cudaSuccess) e = put(m.level_bodies, t.level_bodies, s);
+    if (e == cudaSuccess) e = put(m.cl_bearings, t.cl_bearings, s);
+    if (e == cudaSuccess) e = put(m.cl_slot_off, t.cl_slot_off, s);
+    if (e == cudaSuccess) e = put(m.cl_split, t.cl_split, s);
+    if (e == cudaSuccess) e = put(m.slot_body, t.slot_body, s);
+    if (e == cudaSuccess) e = put(m.cq_coords, t.cq_coords, s);
+    if (e == cudaSuccess) e = put(m.cq_off, t.cq_off, s);
+    if (e == cudaSuccess) e = put(m.cq_slots, t.cq_slots, s);
+    if (e == cudaSuccess) e = put(m.cb_bodies, t.cb_bodies, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    (void)p;
     if (e != cudaSuccess) {
         if (err) {
             std::memset(err, 0, sizeof(*err));
@@ -79,29 +192,325 @@ bool upload_mechanism(MechBuffers& m, const MkCreation* cr, cudaStream_t s, MkEr
         }
         return false;
     }
-    m.links_final = nullptr;
     return true;
 }
 
-void enqueue_mechanism_prelude(MechBuffers& m, const StepBuffers& b, const MechParams& p, cudaStream_t s) {
-    (void)b;
-    cudaMemsetAsync(m.deltas, 0, 24ull * (p.body_count ? p.body_count : 1), s);
+// --------------------------------------------------------------- device math
+__device__ __forceinline__ f3 r3(const float* v) { return mkf3(v[0], v[1], v[2]); }
+__device__ __forceinline__ float4 r4(const float* v) { return make_float4(v[0], v[1], v[2], v[3]); }
+
+// articulated.wgsl:94-102: world inverse inertia from the body-frame rows.
+__device__ __forceinline__ f3 wii(const StepBuffers& b, uint32_t body, f3 v) {
+    const float4 r = b.rot[body];
+    const f3 l = quat_rotate(conjq(r), v);
+    const float4* m = b.mass + 4ull * body;
+    const f3 lr = xyz(m[1]) * l.x + xyz(m[2]) * l.y + xyz(m[3]) * l.z;
+    return quat_rotate(r, lr);
+}
+__device__ __forceinline__ float inv_mass(const StepBuffers& b, uint32_t body) { return b.mass[4ull * body].x; }
+
+__device__ __forceinline__ void add_mdelta(int32_t* deltas, uint32_t body, f3 l, f3 a) {   // :104-112
+    const float s = 1048576.0f;
+    int32_t* d = deltas + 6ull * body;
+    atomicAdd(d + 0, fixed_i32(l.x * s));
+    atomicAdd(d + 1, fixed_i32(l.y * s));
+    atomicAdd(d + 2, fixed_i32(l.z * s));
+    atomicAdd(d + 3, fixed_i32(a.x * s));
+    atomicAdd(d + 4, fixed_i32(a.y * s));
+    atomicAdd(d + 5, fixed_i32(a.z * s));
 }
 
-cudaError_t enqueue_mechanism(MechBuffers&, const StepBuffers&, const MechParams&, cudaStream_t) {
-    return cudaErrorNotSupported;
+__device__ __forceinline__ void hinge_tangents(const StepBuffers& b, uint32_t a, uint32_t c, const GpuBearing& br,
+                                               f3& ta, f3& tb) {
+    const f3 axa = normalize(quat_rotate(b.rot[a], r3(br.local_axis_a)));
+    const f3 axb = normalize(quat_rotate(b.rot[c], r3(br.local_axis_b)));
+    const f3 hinge = normalize(axa + axb);
+    const f3 helper = fabsf(hinge.x) > 0.8f ? mkf3(0, 1, 0) : mkf3(1, 0, 0);
+    ta = normalize(cross(hinge, helper));
+    tb = cross(hinge, ta);
 }
 
-cudaError_t enqueue_contact_solver_with_bearings(MechBuffers&, const StepBuffers&, const StepParams&,
-                                                 const MechParams&, const StepLaunch&, int, cudaStream_t) {
-    return cudaErrorNotSupported;
+// articulated.wgsl:114-155, 287-316
+__global__ void __launch_bounds__(kMBlock) k_project_bearings(StepBuffers b, MechBuffers m, MechParams p) {
+    const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= p.bearing_count) return;
+    const GpuBearing br = m.bearings[j];
+    const uint32_t a = br.metadata[0], c = br.metadata[1];
+    const f3 arm_a = quat_rotate(b.rot[a], r3(br.local_anchor_a)), arm_b = quat_rotate(b.rot[c], r3(br.local_anchor_b));
+    const f3 va = xyz(b.lin[a]) + cross(xyz(b.ang[a]), arm_a);
+    const f3 vb = xyz(b.lin[c]) + cross(xyz(b.ang[c]), arm_b);
+    const f3 rel = vb - va;
+    const float ima = inv_mass(b, a), imb = inv_mass(b, c);
+    const f3 dirs[3] = {mkf3(1, 0, 0), mkf3(0, 1, 0), mkf3(0, 0, 1)};
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        const f3 d = dirs[k];
+        const f3 ang_a = cross(arm_a, d), ang_b = cross(arm_b, d);
+        const float den = ima + imb + dot(ang_a, wii(b, a, ang_a)) + dot(ang_b, wii(b, c, ang_b));
+        if (den <= 1.0e-12f) continue;
+        const f3 imp = d * (0.5f * dot(rel, d) / den);
+        add_mdelta(m.deltas, a, imp * ima, wii(b, a, cross(arm_a, imp)));
+        add_mdelta(m.deltas, c, -imp * imb, wii(b, c, cross(arm_b, -imp)));
+    }
+    f3 ta, tb;
+    hinge_tangents(b, a, c, br, ta, tb);
+    const f3 rang = xyz(b.ang[c]) - xyz(b.ang[a]);
+    const f3 tangents[2] = {ta, tb};
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {
+        const f3 axis = tangents[k];
+        const f3 ia = wii(b, a, axis), ib = wii(b, c, axis);
+        const float den = dot(axis, ia + ib);
+        if (den <= 1.0e-12f) continue;
+        const float imp = 0.5f * dot(rang, axis) / den;
+        add_mdelta(m.deltas, a, mkf3(0, 0, 0), ia * imp);
+        add_mdelta(m.deltas, c, mkf3(0, 0, 0), -ib * imp);
+    }
 }
 
-cudaError_t enqueue_post_contact(MechBuffers&, const StepBuffers&, const MechParams&, cudaStream_t) {
-    return cudaErrorNotSupported;
+// articulated.wgsl:318-337
+__global__ void __launch_bounds__(kMBlock) k_apply_mdeltas(StepBuffers b, MechBuffers m, MechParams p) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= p.body_count) return;
+    int2* d2 = reinterpret_cast<int2*>(m.deltas + 6ull * i);
+    const int2 x0 = d2[0], x1 = d2[1], x2 = d2[2];
+    d2[0] = make_int2(0, 0);
+    d2[1] = make_int2(0, 0);
+    d2[2] = make_int2(0, 0);
+    const float s = 1048576.0f;
+    const f3 ld = mkf3((float)x0.x, (float)x0.y, (float)x1.x) / s;
+    const f3 ad = mkf3((float)x1.y, (float)x2.x, (float)x2.y) / s;
+    b.lin[i] = f4(xyz(b.lin[i]) + ld, 0.0f);
+    b.ang[i] = f4(xyz(b.ang[i]) + ad, 0.0f);
 }
 
-void enqueue_validate_state(MechBuffers&, const StepBuffers&, const MechParams&, cudaStream_t) {}
+// articulated.wgsl:157-285: forward then backward sweeps with immediate updates.
+__device__ void project_row_immediate(const StepBuffers& b, const MechBuffers& m, uint32_t j) {
+    const GpuBearing br = m.bearings[j];
+    const uint32_t a = br.metadata[0], c = br.metadata[1];
+    const f3 arm_a = quat_rotate(b.rot[a], r3(br.local_anchor_a)), arm_b = quat_rotate(b.rot[c], r3(br.local_anchor_b));
+    const float ima = inv_mass(b, a), imb = inv_mass(b, c);
+    const f3 dirs[3] = {mkf3(1, 0, 0), mkf3(0, 1, 0), mkf3(0, 0, 1)};
+    for (int k = 0; k < 3; ++k) {
+        const f3 va = xyz(b.lin[a]) + cross(xyz(b.ang[a]), arm_a);
+        const f3 vb = xyz(b.lin[c]) + cross(xyz(b.ang[c]), arm_b);
+        const f3 rel = vb - va, d = dirs[k];
+        const f3 ang_a = cross(arm_a, d), ang_b = cross(arm_b, d);
+        const float den = ima + imb + dot(ang_a, wii(b, a, ang_a)) + dot(ang_b, wii(b, c, ang_b));
+        if (den <= 1.0e-12f) continue;
+        const f3 imp = d * (dot(rel, d) / den);
+        b.lin[a] = f4(xyz(b.lin[a]) + imp * ima, 0.0f);
+        b.ang[a] = f4(xyz(b.ang[a]) + wii(b, a, cross(arm_a, imp)), 0.0f);
+        b.lin[c] = f4(xyz(b.lin[c]) - imp * imb, 0.0f);
+        b.ang[c] = f4(xyz(b.ang[c]) + wii(b, c, cross(arm_b, -imp)), 0.0f);
+    }
+    f3 ta, tb;
+    hinge_tangents(b, a, c, br, ta, tb);
+    const f3 tangents[2] = {ta, tb};
+    for (int k = 0; k < 2; ++k) {
+        const f3 rang = xyz(b.ang[c]) - xyz(b.ang[a]);
+        const f3 axis = tangents[k];
+        const f3 ia = wii(b, a, axis), ib = wii(b, c, axis);
+        const float den = dot(axis, ia + ib);
+        if (den <= 1.0e-12f) continue;
+        const float imp = dot(rang, axis) / den;
+        b.ang[a] = f4(xyz(b.ang[a]) + ia * imp, 0.0f);
+        b.ang[c] = f4(xyz(b.ang[c]) - ib * imp, 0.0f);
+    }
+}
+
+// Dispatched through indirect args that are zero without active contacts
+// (collision.wgsl:747-749, device.rs:1101-1110).
+__global__ void k_project_bearings_serial(StepBuffers b, MechBuffers m, MechParams p) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    if (b.counts->active == 0u) return;
+    for (uint32_t j = 0; j < p.bearing_count; ++j) project_row_immediate(b, m, j);
+    for (uint32_t j = p.bearing_count; j > 0; --j) project_row_immediate(b, m, j - 1);
+}
+
+// articulated.wgsl:339-364
+__device__ __forceinline__ f3 permitted_axis(const StepBuffers& b, const MechBuffers& m, uint32_t body) {
+    const GpuMechanismBody mb = m.bodies[body];
+    const uint32_t parent = mb.metadata[0];
+    const GpuBearing& br = m.bearings[mb.metadata[1]];
+    f3 axis = normalize(quat_rotate(b.rot[parent], r3(br.local_axis_a)));
+    if (mb.metadata[2] != 0u) axis = -normalize(quat_rotate(b.rot[parent], r3(br.local_axis_b)));
+    return axis;
+}
+__device__ __forceinline__ float permitted_speed(const StepBuffers& b, const MechBuffers& m, uint32_t body) {
+    const uint32_t parent = m.bodies[body].metadata[0];
+    return dot(xyz(b.ang[body]) - xyz(b.ang[parent]), permitted_axis(b, m, body));
+}
+__device__ __forceinline__ float stabilized_speed(const StepBuffers& b, const MechBuffers& m, uint32_t body,
+                                                  float speed) {
+    const bool aligned = fabsf(permitted_axis(b, m, body).y) > 0.999f;
+    return (aligned && fabsf(speed) < 0.005f) ? 0.0f : speed;
+}
+
+// articulated.wgsl:366-415
+__global__ void __launch_bounds__(kMBlock) k_advance_coordinates(StepBuffers b, MechBuffers m, MechParams p) {
+    const uint32_t body = blockIdx.x * blockDim.x + threadIdx.x;
+    if (body >= p.body_count || m.bodies[body].metadata[3] != 0u) return;
+    const uint32_t c = m.bearings[m.bodies[body].metadata[1]].metadata[2];
+    if (c == kInvalid) return;
+    const float measured = permitted_speed(b, m, body) * p.ang_damp;
+    const GpuMechanismDrive dr = m.drives[c];
+    float speed = 0.0f;
+    if (dr.mode == MK_DRIVE_MODE_PASSIVE) {
+        speed = stabilized_speed(b, m, body, measured);
+    } else {
+        float desired = clampf(dr.target_speed, -dr.max_speed, dr.max_speed);
+        if (dr.mode == MK_DRIVE_MODE_ANGLE) {
+            const float err = dr.target_angle - m.coords[c].angle;
+            const float brake = sqrtf(2.0f * dr.max_acceleration * fabsf(err));
+            desired = sgnf(err) * mnf(brake, dr.max_speed);
+            if (fabsf(err) < 0.0005f) desired = 0.0f;
+        }
+        const float budget = dr.max_acceleration * p.dt;
+        speed = measured + clampf(desired - measured, -budget, budget);
+    }
+    float angle = m.coords[c].angle + speed * p.dt;
+    if (angle < dr.min_angle) {
+        angle = dr.min_angle;
+        speed = 0.0f;
+    } else if (angle > dr.max_angle) {
+        angle = dr.max_angle;
+        speed = 0.0f;
+    }
+    m.coords[c].angular_velocity = speed;
+    m.coords[c].angle = angle;
+}
+
+// articulated.wgsl:417-429
+__global__ void __launch_bounds__(kMBlock) k_capture_coordinates(StepBuffers b, MechBuffers m, MechParams p) {
+    const uint32_t body = blockIdx.x * blockDim.x + threadIdx.x;
+    if (body >= p.body_count || m.bodies[body].metadata[3] != 0u) return;
+    const uint32_t c = m.bearings[m.bodies[body].metadata[1]].metadata[2];
+    if (c != kInvalid) m.coords[c].angular_velocity = stabilized_speed(b, m, body, permitted_speed(b, m, body));
+}
+
+// ------------------------------------------------------ forward kinematics
+struct Link { float4 pos, rot; uint4 meta; };
+__device__ __forceinline__ Link ld_link(const GpuLinkState* L, uint32_t i) {
+    const float4* p = reinterpret_cast<const float4*>(L + i);
+    const float4 m = p[2];
+    return {p[0], p[1], make_uint4(__float_as_uint(m.x), __float_as_uint(m.y), __float_as_uint(m.z), __float_as_uint(m.w))};
+}
+__device__ __forceinline__ void st_link(GpuLinkState* L, uint32_t i, const Link& v) {
+    float4* p = reinterpret_cast<float4*>(L + i);
+    p[0] = v.pos;
+    p[1] = v.rot;
+    p[2] = make_float4(__uint_as_float(v.meta.x), __uint_as_float(v.meta.y), __uint_as_float(v.meta.z),
+                       __uint_as_float(v.meta.w));
+}
+
+// mechanism.wgsl:67-70
+__device__ __forceinline__ float4 axis_rotation(f3 axis, float angle) {
+    const float h = angle * 0.5f;
+    const f3 v = normalize(axis) * sin_cr(h);
+    return make_float4(v.x, v.y, v.z, cos_cr(h));
+}
+
+// mechanism.wgsl:72-108
+__device__ __forceinline__ void prepare_link(const MechBuffers& m, uint32_t body) {
+    const GpuMechanismBody mb = m.bodies[body];
+    if (mb.metadata[3] != 0u) {
+        st_link(m.links_a, body, {make_float4(0, 0, 0, 0), make_float4(0, 0, 0, 1), make_uint4(body, 1, 0, 0)});
+        return;
+    }
+    const GpuBearing& br = m.bearings[mb.metadata[1]];
+    const float angle = m.coords[br.metadata[2]].angle;
+    const float4 bind = r4(mb.bind_relative_rotation);
+    float4 rr;
+    f3 rp;
+    if (mb.metadata[2] == 0u) {
+        rr = quat_multiply(axis_rotation(r3(br.local_axis_a), angle), bind);
+        rp = r3(br.local_anchor_a) - quat_rotate(rr, r3(br.local_anchor_b));
+    } else {
+        rr = quat_multiply(axis_rotation(r3(br.local_axis_b), -angle), bind);
+        rp = r3(br.local_anchor_b) - quat_rotate(rr, r3(br.local_anchor_a));
+    }
+    st_link(m.links_a, body, {f4(rp, 0.0f), rr, make_uint4(mb.metadata[0], 0, 0, 0)});
+}
+
+// mechanism.wgsl:110-149
+__device__ __forceinline__ void jump_link(const GpuLinkState* src, GpuLinkState* dst, uint32_t body) {
+    const Link child = ld_link(src, body);
+    if (child.meta.y != 0u) {
+        st_link(dst, body, child);
+        return;
+    }
+    const Link par = ld_link(src, child.meta.x);
+    Link r;
+    r.pos = f4(xyz(par.pos) + quat_rotate(par.rot, xyz(child.pos)), 0.0f);
+    r.rot = normalize4(quat_multiply(par.rot, child.rot));
+    r.meta = make_uint4(par.meta.x, par.meta.y, 0, 0);
+    st_link(dst, body, r);
+}
+
+__global__ void __launch_bounds__(kMBlock) k_prepare_links(MechBuffers m, MechParams p) {
+    const uint32_t body = blockIdx.x * blockDim.x + threadIdx.x;
+    if (body < p.body_count) prepare_link(m, body);
+}
+__global__ void __launch_bounds__(kMBlock) k_jump(const GpuLinkState* src, GpuLinkState* dst, MechParams p) {
+    const uint32_t body = blockIdx.x * blockDim.x + threadIdx.x;
+    if (body < p.body_count) jump_link(src, dst, body);
+}
+
+// mechanism.wgsl:151-185
+__global__ void __launch_bounds__(kMBlock) k_publish(StepBuffers b, MechBuffers m, MechParams p) {
+    const uint32_t body = blockIdx.x * blockDim.x + threadIdx.x;
+    if (body >= p.body_count) return;
+    const Link L = ld_link(m.links_final, body);
+    const uint32_t root = L.meta.x;
+    if (body == root) return;
+    const float4 rq = b.rot[root];
+    b.pos[body] = f4(xyz(b.pos[root]) + quat_rotate(rq, xyz(L.pos)), 0.0f);
+    b.rot[body] = normalize4(quat_multiply(rq, L.rot));
+}
+
+// articulated.wgsl:431-456 for the bodies of one depth level.
+__global__ void __launch_bounds__(kMBlock) k_reconstruct_level(StepBuffers b, MechBuffers m, uint32_t begin,
+                                                               uint32_t end) {
+    const uint32_t t = begin + blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= end) return;
+    const uint32_t body = m.level_bodies[t];
+    const GpuMechanismBody mb = m.bodies[body];
+    const uint32_t parent = mb.metadata[0];
+    const GpuBearing& br = m.bearings[mb.metadata[1]];
+    const float4 rp = b.rot[parent], rb = b.rot[body];
+    f3 axis = normalize(quat_rotate(rp, r3(br.local_axis_a)));
+    f3 pa = quat_rotate(rp, r3(br.local_anchor_a));
+    f3 ca = quat_rotate(rb, r3(br.local_anchor_b));
+    if (mb.metadata[2] != 0u) {
+        axis = -normalize(quat_rotate(rp, r3(br.local_axis_b)));
+        pa = quat_rotate(rp, r3(br.local_anchor_b));
+        ca = quat_rotate(rb, r3(br.local_anchor_a));
+    }
+    const float speed = m.coords[br.metadata[2]].angular_velocity;
+    const f3 wp = xyz(b.ang[parent]);
+    const f3 angular = wp + axis * speed;
+    const f3 av = xyz(b.lin[parent]) + cross(wp, pa);
+    b.lin[body] = f4(av - cross(angular, ca), 0.0f);
+    b.ang[body] = f4(angular, 0.0f);
+}
+
+// articulated.wgsl:458-484
+__global__ void __launch_bounds__(kMBlock) k_validate_state(StepBuffers b, MechBuffers m, MechParams p) {
+    const uint32_t body = blockIdx.x * blockDim.x + threadIdx.x;
+    if (body >= p.body_count) return;
+    const float4 q = b.rot[body];
+    const float rl = dot4(q, q);
+    bool valid = finite4(b.pos[body]) && finite4(q) && finite4(b.lin[body]) && finite4(b.ang[body]) && rl > 0.5f &&
+                 rl < 1.5f;
+    const GpuMechanismBody mb = m.bodies[body];
+    if (mb.metadata[3] == 0u) {
+        const GpuMechanismCoordinate st = m.coords[m.bearings[mb.metadata[1]].metadata[2]];
+        valid = valid && st.angle == st.angle && fabsf(st.angle) < kFloatMax && st.angular_velocity == st.angular_velocity &&
+                fabsf(st.angular_velocity) < kFloatMax;
+    }
+    if (!valid) atomicOr(&b.diag->error_flags, MK_INVALID_NUMERIC_FLAG);
+}
 
 // bearings.wgsl:48-66
 __device__ __forceinline__ void record_residual(GpuDiagnostics* d, f3 anchor_a, f3 anchor_b, f3 axis_a, f3 axis_b,
@@ -123,31 +532,374 @@ __global__ void k_validate_bearings(const GpuBearing* __restrict__ bearings, uin
     const uint32_t a = br.metadata[0], c = br.metadata[1];
     float4 pa, qa, pc, qc;
     if (links) {
-        pa = *reinterpret_cast<const float4*>(links[a].position);
-        qa = *reinterpret_cast<const float4*>(links[a].rotation);
-        pc = *reinterpret_cast<const float4*>(links[c].position);
-        qc = *reinterpret_cast<const float4*>(links[c].rotation);
+        const Link la = ld_link(links, a), lc = ld_link(links, c);
+        pa = la.pos; qa = la.rot; pc = lc.pos; qc = lc.rot;
     } else {
         pa = pos[a]; qa = rot[a]; pc = pos[c]; qc = rot[c];
     }
-    const f3 anchor_a = xyz(pa) + quat_rotate(qa, mkf3(br.local_anchor_a[0], br.local_anchor_a[1], br.local_anchor_a[2]));
-    const f3 anchor_b = xyz(pc) + quat_rotate(qc, mkf3(br.local_anchor_b[0], br.local_anchor_b[1], br.local_anchor_b[2]));
-    const f3 axis_a = normalize(quat_rotate(qa, mkf3(br.local_axis_a[0], br.local_axis_a[1], br.local_axis_a[2])));
-    const f3 axis_b = normalize(quat_rotate(qc, mkf3(br.local_axis_b[0], br.local_axis_b[1], br.local_axis_b[2])));
+    const f3 anchor_a = xyz(pa) + quat_rotate(qa, r3(br.local_anchor_a));
+    const f3 anchor_b = xyz(pc) + quat_rotate(qc, r3(br.local_anchor_b));
+    const f3 axis_a = normalize(quat_rotate(qa, r3(br.local_axis_a)));
+    const f3 axis_b = normalize(quat_rotate(qc, r3(br.local_axis_b)));
     record_residual(diag, anchor_a, anchor_b, axis_a, axis_b, br.metadata[3] != 0u);
+}
+
+// ------------------------------------------------------------- closure loop
+__device__ __forceinline__ float block_sum(float v, float* scratch) {
+    // fixed tree order: warp shuffles, then warp 0 over the warp partials
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    const uint32_t w = threadIdx.x >> 5, lane = threadIdx.x & 31u;
+    __syncthreads();
+    if (lane == 0) scratch[w] = v;
+    __syncthreads();
+    float r = 0.0f;
+    if (w == 0) {
+        r = lane < (blockDim.x >> 5) ? scratch[lane] : 0.0f;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) r += __shfl_down_sync(0xffffffffu, r, o);
+        if (lane == 0) scratch[32] = r;
+    }
+    __syncthreads();
+    return scratch[32];
+}
+
+// Dot product over the closure coordinates.  Up to kSerialDot coordinates it
+// is summed by one thread in ascending coordinate order (the serial order of
+// closure.wgsl:339-414, so small systems reproduce it bit for bit); larger
+// systems use the fixed-order block tree of the per-thread partials.
+constexpr uint32_t kSerialDot = 512;
+enum DotKind { kDotRZ, kDotDirOp };
+__device__ __forceinline__ float closure_dot(DotKind kind, float partial, const MechBuffers& m, uint32_t nq,
+                                             const float* a, const float* bvec, float* scratch) {
+    if (nq > kSerialDot) return block_sum(partial, scratch);
+    (void)kind;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        float acc = 0.0f;
+        for (uint32_t q = 0; q < nq; ++q) {
+            const uint32_t c = m.cq_coords[q];
+            acc += a[c] * bvec[c];
+        }
+        scratch[32] = acc;
+    }
+    __syncthreads();
+    return scratch[32];
+}
+
+// Joint frame of `body` in its root's frame (closure.wgsl:168-181).
+__device__ __forceinline__ void joint_frame(const MechBuffers& m, uint32_t body, f3& axis, f3& anchor, uint32_t& coord) {
+    const GpuMechanismBody mb = m.bodies[body];
+    const GpuBearing& tb = m.bearings[mb.metadata[1]];
+    const Link pp = ld_link(m.links_final, mb.metadata[0]);
+    if (mb.metadata[2] == 0u) {
+        axis = normalize(quat_rotate(pp.rot, r3(tb.local_axis_a)));
+        anchor = xyz(pp.pos) + quat_rotate(pp.rot, r3(tb.local_anchor_a));
+    } else {
+        axis = -normalize(quat_rotate(pp.rot, r3(tb.local_axis_b)));
+        anchor = xyz(pp.pos) + quat_rotate(pp.rot, r3(tb.local_anchor_b));
+    }
+    coord = tb.metadata[2];
+}
+
+__device__ __forceinline__ void closure_frames(const MechBuffers& m, const GpuBearing& br, f3& anc_a, f3& anc_b,
+                                               f3& ax_a, f3& ax_b) {
+    const Link pa = ld_link(m.links_final, br.metadata[0]), pb = ld_link(m.links_final, br.metadata[1]);
+    anc_a = xyz(pa.pos) + quat_rotate(pa.rot, r3(br.local_anchor_a));
+    anc_b = xyz(pb.pos) + quat_rotate(pb.rot, r3(br.local_anchor_b));
+    ax_a = normalize(quat_rotate(pa.rot, r3(br.local_axis_a)));
+    ax_b = normalize(quat_rotate(pb.rot, r3(br.local_axis_b)));
+}
+
+__device__ __forceinline__ bool finite3(f3 v) {
+    return v.x == v.x && v.y == v.y && v.z == v.z && fabsf(v.x) < kFloatMax && fabsf(v.y) < kFloatMax &&
+           fabsf(v.z) < kFloatMax;
+}
+
+// The closure loop of device.rs:973-1020 in one block: 12 Newton steps of
+// closure.wgsl:268-427 (evaluate, finalize, 8-round diagonal PCG, step the
+// coordinates), each followed by forward kinematics of the closure
+// components.  Accumulations go through per-joint slots summed per
+// coordinate in the serial order; dot products are fixed-order block sums.
+__global__ void __launch_bounds__(kClosureThreads) k_closure_loop(StepBuffers b, MechBuffers m, MechParams p) {
+    __shared__ float s_red[33];
+    __shared__ uint32_t s_state[2];
+    __shared__ uint32_t s_unconverged, s_converged_prev;
+    __shared__ uint32_t s_steps, s_rounds;
+    const uint32_t tid = threadIdx.x, nt = blockDim.x;
+    const uint32_t NC = p.closures, NQ = p.closure_coords, NB = p.closure_bodies, Q = p.coordinate_count;
+    float* sol = m.pcg;
+    float* res = m.pcg + Q;
+    float* pre = m.pcg + 2ull * Q;
+    float* dir = m.pcg + 3ull * Q;
+    float* op = m.pcg + 4ull * Q;
+    if (tid == 0) { s_converged_prev = 0; s_steps = 0; s_rounds = 0; }
+    __syncthreads();
+    for (uint32_t step = 0; step < kClosureSteps; ++step) {
+        if (tid == 0) { s_state[0] = 0; s_state[1] = 0; }
+        __syncthreads();
+        const bool evaluate = step == 0 || !s_converged_prev;
+        // evaluate_closures (closure.wgsl:268-319): slot contributions
+        if (evaluate) {
+            for (uint32_t k = tid; k < NC; k += nt) {
+                const GpuBearing br = m.bearings[m.cl_bearings[k]];
+                f3 aa, ab, xa, xb;
+                closure_frames(m, br, aa, ab, xa, xb);
+                const f3 rp = aa - ab, ra = xa - xb;
+                const uint32_t s0 = m.cl_slot_off[k], s1 = m.cl_slot_off[k + 1], split = m.cl_split[k];
+                bool active = true;
+                if (!finite3(rp) || !finite3(ra)) {
+                    atomicOr(&b.diag->error_flags, MK_INVALID_NUMERIC_FLAG);
+                    atomicMax(&s_state[0], 0xffffffffu);
+                    atomicMax(&s_state[1], 0xffffffffu);
+                    active = false;
+                } else {
+                    const uint32_t um = round_u32(length(rp) * 1000000.0f);
+                    // axis error as atan2(|a x b|, a . b): FP32 acos (closure.wgsl:295) reads 0
+                    // below ~3.5e-4 rad, blind to the 1000 micro-degree tolerance
+                    const float deg =
+                        atan2_cr(length(cross(xa, xb)), clampf(dot(xa, xb), -1.0f, 1.0f)) * 57.295779513f;
+                    const uint32_t ud = round_u32(deg * 1000000.0f);
+                    atomicMax(&s_state[0], um);
+                    atomicMax(&s_state[1], ud);
+                    active = !(um <= 10u && ud <= 1000u);
+                }
+                for (uint32_t sl = s0; sl < s1; ++sl) {
+                    float g = 0.0f, d = 0.0f;
+                    uint32_t valid = 0;
+                    if (active) {
+                        const bool side_a = sl < split;
+                        const f3 ea = side_a ? aa : ab, ex = side_a ? xa : xb;
+                        const float sign = side_a ? 1.0f : -1.0f;
+                        f3 axis, anchor;
+                        uint32_t coord;
+                        joint_frame(m, m.slot_body[sl], axis, anchor, coord);
+                        if (coord >= Q) {
+                            atomicOr(&b.diag->error_flags, MK_INVALID_NUMERIC_FLAG);
+                        } else {
+                            const f3 pd = cross(axis, ea - anchor) * sign;
+                            const f3 ad = cross(axis, ex) * sign;
+                            g = dot(rp, pd) + 1.0f * dot(ra, ad);
+                            d = dot(pd, pd) + 1.0f * dot(ad, ad);
+                            if (g == g && d == d) valid = 1;
+                            else atomicOr(&b.diag->error_flags, MK_INVALID_NUMERIC_FLAG);
+                        }
+                    }
+                    // NaN marks "no contribution" so the gather skips it
+                    m.slot_g[sl] = valid ? g : __int_as_float(0x7fffffff);
+                    m.slot_d[sl] = valid ? d : 0.0f;
+                }
+            }
+        }
+        __syncthreads();
+        // gather per coordinate in the serial accumulation order
+        for (uint32_t q = tid; q < NQ; q += nt) {
+            float g = 0.0f, d = 0.0f;
+            if (evaluate) {
+                for (uint32_t i = m.cq_off[q]; i < m.cq_off[q + 1]; ++i) {
+                    const uint32_t sl = m.cq_slots[i];
+                    const float sg = m.slot_g[sl];
+                    if (sg == sg) { g += sg; d += m.slot_d[sl]; }
+                }
+            }
+            const uint32_t c = m.cq_coords[q];
+            m.grad[c] = g;
+            m.diag[c] = d;
+        }
+        if (tid == 0) {
+            s_unconverged = (s_state[0] > 10u || s_state[1] > 1000u) ? 1u : 0u;
+            if (s_unconverged) ++s_steps;
+        }
+        __syncthreads();
+        const bool unconverged = s_unconverged != 0u;
+        if (unconverged) {
+            // solve_closure_pcg (closure.wgsl:333-427)
+            float part = 0.0f;
+            for (uint32_t q = tid; q < NQ; q += nt) {
+                const uint32_t c = m.cq_coords[q];
+                const float g = m.grad[c], d = m.diag[c];
+                float r = 0.0f, z = 0.0f;
+                if (d > 1.0e-12f) { r = -g; z = r / d; }
+                sol[c] = 0.0f; res[c] = r; pre[c] = z; dir[c] = z; op[c] = 0.0f;
+                part += r * z;
+            }
+            float rz = closure_dot(kDotRZ, part, m, NQ, res, pre, s_red);
+            for (uint32_t round = 0; round < kClosureRounds; ++round) {
+                // J^T J dir per closure: branch products then transposes (closure.wgsl:194-266)
+                for (uint32_t k = tid; k < NC; k += nt) {
+                    const GpuBearing br = m.bearings[m.cl_bearings[k]];
+                    f3 aa, ab, xa, xb;
+                    closure_frames(m, br, aa, ab, xa, xb);
+                    const uint32_t s0 = m.cl_slot_off[k], s1 = m.cl_slot_off[k + 1], split = m.cl_split[k];
+                    f3 prod_p[2] = {mkf3(0, 0, 0), mkf3(0, 0, 0)}, prod_a[2] = {mkf3(0, 0, 0), mkf3(0, 0, 0)};
+                    for (uint32_t sl = s0; sl < s1; ++sl) {
+                        const int side = sl < split ? 0 : 1;
+                        const f3 ea = side == 0 ? aa : ab, ex = side == 0 ? xa : xb;
+                        const float sign = side == 0 ? 1.0f : -1.0f;
+                        f3 axis, anchor;
+                        uint32_t coord;
+                        joint_frame(m, m.slot_body[sl], axis, anchor, coord);
+                        const float dv = dir[coord];
+                        prod_p[side] = prod_p[side] + sign * cross(axis, ea - anchor) * dv;
+                        prod_a[side] = prod_a[side] + sign * cross(axis, ex) * dv;
+                    }
+                    const f3 pp = prod_p[0] + prod_p[1], pa = prod_a[0] + prod_a[1];
+                    for (uint32_t sl = s0; sl < s1; ++sl) {
+                        const bool side_a = sl < split;
+                        const f3 ea = side_a ? aa : ab, ex = side_a ? xa : xb;
+                        const float sign = side_a ? 1.0f : -1.0f;
+                        f3 axis, anchor;
+                        uint32_t coord;
+                        joint_frame(m, m.slot_body[sl], axis, anchor, coord);
+                        const f3 pd = sign * cross(axis, ea - anchor);
+                        const f3 ad = sign * cross(axis, ex);
+                        m.slot_g[sl] = dot(pd, pp) + 1.0f * dot(ad, pa);
+                    }
+                }
+                __syncthreads();
+                float dpart = 0.0f;
+                for (uint32_t q = tid; q < NQ; q += nt) {
+                    float o = 0.0f;
+                    for (uint32_t i = m.cq_off[q]; i < m.cq_off[q + 1]; ++i) o += m.slot_g[m.cq_slots[i]];
+                    const uint32_t c = m.cq_coords[q];
+                    op[c] = o;
+                    dpart += dir[c] * o;
+                }
+                const float dop = closure_dot(kDotDirOp, dpart, m, NQ, dir, op, s_red);
+                const float alpha = fabsf(dop) > 1.0e-20f ? rz / dop : 0.0f;
+                float npart = 0.0f;
+                for (uint32_t q = tid; q < NQ; q += nt) {
+                    const uint32_t c = m.cq_coords[q];
+                    sol[c] += alpha * dir[c];
+                    res[c] -= alpha * op[c];
+                    const float d = m.diag[c];
+                    pre[c] = 0.0f;
+                    if (d > 1.0e-12f) pre[c] = res[c] / d;
+                    npart += res[c] * pre[c];
+                }
+                const float nrz = closure_dot(kDotRZ, npart, m, NQ, res, pre, s_red);
+                const float beta = fabsf(rz) > 1.0e-20f ? nrz / rz : 0.0f;
+                for (uint32_t q = tid; q < NQ; q += nt) {
+                    const uint32_t c = m.cq_coords[q];
+                    dir[c] = pre[c] + beta * dir[c];
+                }
+                rz = nrz;
+                if (tid == 0) ++s_rounds;
+                __syncthreads();
+            }
+            // step every coordinate (coordinates off the closure branches add 0)
+            for (uint32_t c = tid; c < Q; c += nt) {
+                const float stp = clampf(0.35f * sol[c], -0.2f, 0.2f);
+                if (stp == stp) m.coords[c].angle += stp;
+                else atomicOr(&b.diag->error_flags, MK_INVALID_NUMERIC_FLAG);
+            }
+            __syncthreads();
+            // forward kinematics of the closure components (mechanism.wgsl:72-149)
+            for (uint32_t i = tid; i < NB; i += nt) prepare_link(m, m.cb_bodies[i]);
+            __syncthreads();
+            bool a_src = true;
+            for (uint32_t r = 0; r < p.jump_rounds; ++r) {
+                for (uint32_t i = tid; i < NB; i += nt)
+                    jump_link(a_src ? m.links_a : m.links_b, a_src ? m.links_b : m.links_a, m.cb_bodies[i]);
+                __syncthreads();
+                a_src = !a_src;
+            }
+        }
+        if (tid == 0) s_converged_prev = unconverged ? 0u : 1u;
+        __syncthreads();
+    }
+    if (tid == 0) {
+        atomicAdd(&b.diag->reserved_b, s_steps);
+        atomicAdd(&b.diag->reserved_c, s_rounds);
+    }
+}
+
+// --------------------------------------------------------------- launches
+static inline uint32_t nblocks(uint32_t n) { return (n + kMBlock - 1) / kMBlock; }
+
+void enqueue_mechanism_prelude(MechBuffers& m, const StepBuffers& b, const MechParams& p, cudaStream_t s) {
+    (void)b;
+    cudaMemsetAsync(m.deltas, 0, 24ull * (p.body_count ? p.body_count : 1), s);
+}
+
+static cudaError_t bearing_projection_iteration(MechBuffers& m, const StepBuffers& b, const MechParams& p,
+                                                cudaStream_t s) {
+    if (p.bearing_count) k_project_bearings<<<nblocks(p.bearing_count), kMBlock, 0, s>>>(b, m, p);
+    k_apply_mdeltas<<<nblocks(p.body_count), kMBlock, 0, s>>>(b, m, p);
+    return cudaGetLastError();
+}
+
+static cudaError_t forward_kinematics(MechBuffers& m, const MechParams& p, cudaStream_t s) {
+    k_prepare_links<<<nblocks(p.body_count), kMBlock, 0, s>>>(m, p);
+    bool a_src = true;
+    for (uint32_t r = 0; r < p.jump_rounds; ++r) {
+        k_jump<<<nblocks(p.body_count), kMBlock, 0, s>>>(a_src ? m.links_a : m.links_b, a_src ? m.links_b : m.links_a,
+                                                         p);
+        a_src = !a_src;
+    }
+    return cudaGetLastError();
+}
+
+static cudaError_t reconstruct(MechBuffers& m, const StepBuffers& b, cudaStream_t s) {
+    for (uint32_t l = 1; l < m.level_count; ++l) {
+        const uint32_t begin = m.level_offsets[l], end = m.level_offsets[l + 1];
+        if (end > begin) k_reconstruct_level<<<nblocks(end - begin), kMBlock, 0, s>>>(b, m, begin, end);
+    }
+    return cudaGetLastError();
+}
+
+// device.rs:963-1048
+cudaError_t enqueue_mechanism(MechBuffers& m, const StepBuffers& b, const MechParams& p, cudaStream_t s) {
+    cudaError_t e;
+    for (uint32_t it = 0; it < std::max(1u, p.iterations); ++it)
+        if ((e = bearing_projection_iteration(m, b, p, s)) != cudaSuccess) return e;
+    k_advance_coordinates<<<nblocks(p.body_count), kMBlock, 0, s>>>(b, m, p);
+    if ((e = forward_kinematics(m, p, s)) != cudaSuccess) return e;
+    if (p.closures > 0) k_closure_loop<<<1, kClosureThreads, 0, s>>>(b, m, p);
+    k_publish<<<nblocks(p.body_count), kMBlock, 0, s>>>(b, m, p);
+    return reconstruct(m, b, s);
+}
+
+// device.rs:1343-1416 with a dynamic mechanism root
+cudaError_t enqueue_contact_solver_with_bearings(MechBuffers& m, const StepBuffers& b, const StepParams& sp,
+                                                 const MechParams& p, const StepLaunch& l, int parity,
+                                                 cudaStream_t s) {
+    return launch_contact_solver_stepwise(b, sp, l, parity, p.serial_contacts != 0u, [&](bool serial) {
+        if (serial) {
+            k_project_bearings_serial<<<1, 32, 0, s>>>(b, m, p);
+            return cudaGetLastError();
+        }
+        return bearing_projection_iteration(m, b, p, s);
+    }, s);
+}
+
+// device.rs:1128-1155
+cudaError_t enqueue_post_contact(MechBuffers& m, const StepBuffers& b, const MechParams& p, cudaStream_t s) {
+    cudaError_t e;
+    if (!p.has_dynamic_root)
+        for (uint32_t it = 0; it < std::max(1u, p.iterations); ++it)
+            if ((e = bearing_projection_iteration(m, b, p, s)) != cudaSuccess) return e;
+    k_capture_coordinates<<<nblocks(p.body_count), kMBlock, 0, s>>>(b, m, p);
+    if (!p.has_dynamic_root) return reconstruct(m, b, s);
+    return cudaGetLastError();
+}
+
+void enqueue_validate_state(MechBuffers& m, const StepBuffers& b, const MechParams& p, cudaStream_t s) {
+    k_validate_state<<<nblocks(p.body_count), kMBlock, 0, s>>>(b, m, p);
 }
 
 void enqueue_validate_bearings(MechBuffers& m, const StepBuffers& b, const MechParams& p, bool mechanism_active,
                                cudaStream_t s) {
     if (p.bearing_count == 0) return;
-    k_validate_bearings<<<(p.bearing_count + 255) / 256, 256, 0, s>>>(m.bearings, p.bearing_count, b.pos, b.rot,
-                                                                       mechanism_active ? m.links_final : nullptr,
-                                                                       b.diag);
+    k_validate_bearings<<<nblocks(p.bearing_count), kMBlock, 0, s>>>(m.bearings, p.bearing_count, b.pos, b.rot,
+                                                                      mechanism_active ? m.links_final : nullptr,
+                                                                      b.diag);
 }
 
-void read_mechanism_readback(const MechBuffers& m, MkTickReadback* out) {
-    out->closure_iterations = m.readback_iterations;
-    out->closure_relative_residual = m.readback_residual;
+void read_mechanism_readback(const MechBuffers& m, const GpuDiagnostics& d, MkTickReadback* out) {
+    (void)m;
+    out->closure_iterations = d.reserved_c;
+    out->closure_relative_residual = 0.0;
 }
 
 }  // namespace mk

@@ -5,6 +5,7 @@
 
 #include <cstdint>
 #include <functional>
+#include <vector>
 
 #include "mk_internal.h"
 
@@ -19,6 +20,11 @@ struct MechParams {
     uint32_t has_dynamic_root = 0;
     uint32_t serial_contacts = 0;    // dynamic root and <= 64 bearings (device.rs:1370-1373)
     float dt = 1.0f / 60.0f, ang_damp = 0.98f;
+    // closure topology (host-derived, static)
+    uint32_t closures = 0;           // closure bearings
+    uint32_t slots = 0;              // joints on closure branches, over all closures
+    uint32_t closure_coords = 0;     // distinct coordinates on closure branches
+    uint32_t closure_bodies = 0;     // bodies of components that contain a closure
 };
 
 struct MechBuffers {
@@ -27,26 +33,43 @@ struct MechBuffers {
     GpuMechanismCoordinate* coords = nullptr;   // Q
     GpuMechanismDrive* drives = nullptr;        // Q
     uint32_t* preorder = nullptr;               // B
-    uint32_t* level_offsets = nullptr;          // depth levels of the preorder (max_depth + 2)
-    uint32_t* level_bodies = nullptr;           // bodies grouped by depth
     GpuLinkState* links_a = nullptr;            // B
     GpuLinkState* links_b = nullptr;            // B
     GpuLinkState* links_final = nullptr;        // alias of a or b
     int32_t* deltas = nullptr;                  // 6 per body (bearing projection)
-    float* closure_grad = nullptr;              // Q (float CAS accumulators, closure.wgsl:46-49)
-    float* closure_diag = nullptr;              // Q
-    uint32_t* closure_state = nullptr;          // 2 words + flags
-    float* pcg = nullptr;                       // Q x 8 (PcgRow, closure.wgsl:51-60)
-    double* reduce = nullptr;                   // FP64 reduction scratch
-    uint32_t* closure_bearings = nullptr;       // indices of closure bearings
-    uint32_t* readback = nullptr;               // host-visible iteration count / residual bits
+    // reconstruct_body_velocities by depth level (level l: bodies [off[l], off[l+1]))
+    uint32_t* level_bodies = nullptr;
+    const uint32_t* level_offsets = nullptr;    // host memory owned by the handle, level_count + 1 entries
+    uint32_t level_count = 0;
+    // closure loop
+    uint32_t* cl_bearings = nullptr;            // closure bearing rows
+    uint32_t* cl_slot_off = nullptr;            // closures + 1: slots of closure k (branch a, then branch b)
+    uint32_t* cl_split = nullptr;               // first branch-b slot of closure k
+    uint32_t* slot_body = nullptr;              // child body of the joint of each slot
+    uint32_t* cq_coords = nullptr;              // coordinates on closure branches (ascending)
+    uint32_t* cq_off = nullptr;                 // closure_coords + 1: CSR into cq_slots
+    uint32_t* cq_slots = nullptr;               // slots of each coordinate, in serial accumulation order
+    uint32_t* cb_bodies = nullptr;              // bodies of closure components
+    float* slot_g = nullptr;                    // per-slot gradient / operator contributions
+    float* slot_d = nullptr;
+    float* grad = nullptr;                      // Q (closure.wgsl:46-49 accumulators)
+    float* diag = nullptr;                      // Q
+    float* pcg = nullptr;                       // 5 x Q: sol, res, pre, dir, op (closure.wgsl:51-60)
     uint32_t readback_iterations = 0;
     double readback_residual = 0.0;
 };
 
 MechParams make_mech_params(const MkCreation* cr, const StepParams& p, uint32_t iterations, uint32_t closure_mode);
-void carve_mechanism(MechBuffers& m, uint32_t B, uint32_t J, uint32_t Q, const std::function<char*(uint64_t)>& take);
-bool upload_mechanism(MechBuffers& m, const MkCreation* cr, cudaStream_t s, MkError* err);
+// Host-side closure topology and depth levels; fills the counts in `p`.
+struct MechTopology {
+    std::vector<uint32_t> level_bodies, level_offsets;
+    std::vector<uint32_t> cl_bearings, cl_slot_off, cl_split, slot_body, cq_coords, cq_off, cq_slots, cb_bodies;
+};
+MechTopology derive_topology(const MkCreation* cr, MechParams& p);
+void carve_mechanism(MechBuffers& m, const MechParams& p, uint32_t B, uint32_t J, uint32_t Q,
+                     const std::function<char*(uint64_t)>& take);
+bool upload_mechanism(MechBuffers& m, const MechParams& p, const MechTopology& topo, const MkCreation* cr,
+                      cudaStream_t s, MkError* err);
 void enqueue_mechanism_prelude(MechBuffers& m, const StepBuffers& b, const MechParams& p, cudaStream_t s);
 cudaError_t enqueue_mechanism(MechBuffers& m, const StepBuffers& b, const MechParams& p, cudaStream_t s);
 cudaError_t enqueue_contact_solver_with_bearings(MechBuffers& m, const StepBuffers& b, const StepParams& sp,
@@ -55,6 +78,6 @@ cudaError_t enqueue_post_contact(MechBuffers& m, const StepBuffers& b, const Mec
 void enqueue_validate_state(MechBuffers& m, const StepBuffers& b, const MechParams& p, cudaStream_t s);
 void enqueue_validate_bearings(MechBuffers& m, const StepBuffers& b, const MechParams& p, bool mechanism_active,
                                cudaStream_t s);
-void read_mechanism_readback(const MechBuffers& m, MkTickReadback* out);
+void read_mechanism_readback(const MechBuffers& m, const GpuDiagnostics& d, MkTickReadback* out);
 
 }  // namespace mk

@@ -20,6 +20,7 @@
 // canonical order through a decoupled look-back, so the whole tick is a
 // fixed launch sequence (CUDA-graph friendly) with deterministic output.
 #include <cstdio>
+#include <functional>
 
 #include "mk_device.cuh"
 #include "mk_internal.h"
@@ -958,6 +959,105 @@ __global__ void __launch_bounds__(kSolveThreads) k_solve_all(StepBuffers b, Step
     }
 }
 
+// Per-iteration kernels for ticks that interleave bearing projection with
+// the contact iterations (device.rs:1363-1416): velocities are updated in
+// place, so each phase is its own launch.
+template <bool kWarm>
+__global__ void __launch_bounds__(kBlock) k_solve_iter(StepBuffers b, StepParams p, GpuContact* cur) {
+    const uint32_t A = b.counts->active;
+    solve_span<kWarm>(b, p, cur, A, blockIdx.x * blockDim.x, gridDim.x * blockDim.x, b.lin, b.ang);
+}
+
+__global__ void __launch_bounds__(kBlock) k_apply_iter(StepBuffers b, StepParams p) {
+    if (b.counts->active == 0u) return;   // collision.wgsl:744 (no apply dispatch without active contacts)
+    const uint32_t first = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t stride = gridDim.x * blockDim.x;
+    const float s = (float)kFixedScale;
+    for (uint32_t i = first; i < p.body_count; i += stride) {
+        int2* d2 = reinterpret_cast<int2*>(b.deltas + 6ull * i);
+        const int2 x0 = d2[0], x1 = d2[1], x2 = d2[2];
+        d2[0] = make_int2(0, 0);
+        d2[1] = make_int2(0, 0);
+        d2[2] = make_int2(0, 0);
+        const f3 ld = mkf3((float)x0.x, (float)x0.y, (float)x1.x) / s;
+        const f3 ad = mkf3((float)x1.y, (float)x2.x, (float)x2.y) / s;
+        b.lin[i] = f4(xyz(b.lin[i]) + ld, 0.0f);
+        b.ang[i] = f4(xyz(b.ang[i]) + ad, 0.0f);
+    }
+}
+
+// collision.wgsl:908-977: one contact, velocities updated immediately.
+__device__ void solve_contact_immediate(const StepBuffers& b, const StepParams& p, GpuContact* cur, uint32_t k) {
+    float4* row = reinterpret_cast<float4*>(cur + k);
+    const float4 r0 = row[0], np = row[1], aa = row[2], ab = row[3];
+    const uint32_t a = __float_as_uint(r0.x), bb = __float_as_uint(r0.y);
+    const f3 arm_a = xyz(aa), arm_b = xyz(ab);
+    const float4* wa = b.world_mass + 3ull * a;
+    const float4* wb = bb != kInvalid ? b.world_mass + 3ull * bb : nullptr;
+    f3 vb = mkf3(0, 0, 0);
+    if (bb != kInvalid) vb = contact_velocity(b, bb, arm_b);
+    const f3 nrm = xyz(np);
+    const float den = impulse_denominator(wa, wb, arm_a, arm_b, nrm);
+    if (den <= 0.0f) return;
+    const f3 rel = vb - contact_velocity(b, a, arm_a);
+    const float vn = dot(rel, nrm);
+    if (np.w <= 1.0e-5f && vn >= -1.0e-5f && aa.w <= 1.0e-6f) {
+        row[2] = f4(arm_a, 0.0f);
+        return;
+    }
+    const bool cyl = ab.w < 0.0f;
+    const float bias = mnf(mxf(np.w - 0.001f, 0.0f) * (cyl ? 1.0f : 0.2f) / p.dt, 1.0f);
+    const float prev = mxf(aa.w, 0.0f);
+    const float acc = mxf(prev + (-vn + bias) / den, 0.0f);
+    const float delta = acc - prev;
+    row[2] = f4(arm_a, acc);
+    f3 imp = nrm * delta;
+    const f3 tv = rel - nrm * vn;
+    const float ts = length(tv);
+    if (ts > 1.0e-6f) {
+        const f3 tg = tv / ts;
+        const float tden = impulse_denominator(wa, wb, arm_a, arm_b, tg);
+        const float fr = mnf(ts / tden, fabsf(delta) * 0.05f);
+        imp = imp - tg * fr;
+    }
+    b.lin[a] = f4(xyz(b.lin[a]) - imp * wa[0].w, 0.0f);
+    b.ang[a] = f4(xyz(b.ang[a]) + inverse_inertia(wa, cross(arm_a, -imp)), 0.0f);
+    if (wb) {
+        b.lin[bb] = f4(xyz(b.lin[bb]) + imp * wb[0].w, 0.0f);
+        b.ang[bb] = f4(xyz(b.ang[bb]) + inverse_inertia(wb, cross(arm_b, imp)), 0.0f);
+    }
+}
+
+// collision.wgsl:979-1048: forward then backward Gauss-Seidel sweeps, one
+// thread; at most 64 active contacts are visited in (body a, body b,
+// manifold slot) order, more in active-list order.
+__global__ void k_solve_serial(StepBuffers b, StepParams p, GpuContact* cur) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    const uint32_t A = b.counts->active;
+    if (A > 64u) {
+        for (uint32_t k = 0; k < A; ++k) solve_contact_immediate(b, p, cur, b.active[k]);
+        for (uint32_t k = A; k > 0; --k) solve_contact_immediate(b, p, cur, b.active[k - 1]);
+        return;
+    }
+    uint32_t order[64];
+    for (uint32_t k = 0; k < A; ++k) order[k] = b.active[k];
+    for (uint32_t x = 1; x < A; ++x) {   // sort by (body a, body b, manifold slot)
+        const uint32_t v = order[x];
+        const uint4 kv = *reinterpret_cast<const uint4*>(cur[v].metadata);
+        int y = (int)x - 1;
+        while (y >= 0) {
+            const uint4 ky = *reinterpret_cast<const uint4*>(cur[order[y]].metadata);
+            const bool greater = ky.x > kv.x || (ky.x == kv.x && (ky.y > kv.y || (ky.y == kv.y && ky.z > kv.z)));
+            if (!greater) break;
+            order[y + 1] = order[y];
+            --y;
+        }
+        order[y + 1] = v;
+    }
+    for (uint32_t k = 0; k < A; ++k) solve_contact_immediate(b, p, cur, order[k]);
+    for (uint32_t k = A; k > 0; --k) solve_contact_immediate(b, p, cur, order[k - 1]);
+}
+
 // Bookkeeping at the end of a tick: this tick's contact list becomes the
 // manifold cache of the next one.
 __global__ void k_finish_tick(StepBuffers b) {
@@ -1090,6 +1190,33 @@ cudaError_t launch_contact_solver(const StepBuffers& b, const StepParams& p, con
     cfg.numAttrs = 1;
     e = cudaLaunchKernelExC(&cfg, (const void*)k_solve_all, args);
     if (e != cudaSuccess) return e;
+    return cudaGetLastError();
+}
+
+cudaError_t launch_contact_solver_stepwise(const StepBuffers& b, const StepParams& p, const StepLaunch& l, int parity,
+                                           bool serial, const std::function<cudaError_t(bool)>& after_apply,
+                                           cudaStream_t s) {
+    const uint32_t grid = (uint32_t)l.sm_count * 8;
+    AppendSite prep{b.lookback + 3 * b.lookback_words, b.tickets + 3};
+    const int prev = parity ^ 1;
+    GpuContact* cur = b.contacts[parity];
+    k_prepare<<<grid, kBlock, 0, s>>>(b, p, prep, cur, b.contact_keys[parity], b.features[parity], b.contacts[prev],
+                                       b.contact_keys[prev], b.features[prev]);
+    const uint32_t body_blocks = std::max<uint32_t>(1u, std::min<uint32_t>(blocks_for(p.body_count, kBlock), grid));
+    k_solve_iter<true><<<grid, kBlock, 0, s>>>(b, p, cur);
+    k_apply_iter<<<body_blocks, kBlock, 0, s>>>(b, p);
+    cudaError_t e = after_apply(serial);
+    if (e != cudaSuccess) return e;
+    const uint32_t iters = serial ? std::max<uint32_t>(1u, l.iterations) * 12u : std::max<uint32_t>(1u, l.iterations);
+    for (uint32_t it = 1; it < iters; ++it) {
+        if (serial) {
+            k_solve_serial<<<1, 32, 0, s>>>(b, p, cur);
+        } else {
+            k_solve_iter<false><<<grid, kBlock, 0, s>>>(b, p, cur);
+            k_apply_iter<<<body_blocks, kBlock, 0, s>>>(b, p);
+        }
+        if ((e = after_apply(serial)) != cudaSuccess) return e;
+    }
     return cudaGetLastError();
 }
 

@@ -425,3 +425,160 @@ def dense_grid(count: int = 100_000) -> Scene:
     zeros = np.zeros(count)
     return _assemble(translation, rotation, np.zeros(count, bool), zeros, zeros, zeros, (1.0, 1.0, 1.0),
                      f"dense_{count}", density=REFERENCE_DENSITY)
+
+
+def _unit_vectors(rng: Rng, name: str, n: int) -> np.ndarray:
+    """Uniform directions on the sphere."""
+    z = rng.uniform(name + ".z", n, -1.0, 1.0)
+    phi = rng.uniform(name + ".phi", n, 0.0, 2.0 * math.pi)
+    r = np.sqrt(np.maximum(0.0, 1.0 - z * z))
+    return np.stack([r * np.cos(phi), r * np.sin(phi), z], axis=1)
+
+
+def _mechanism_rows(scene: Scene, parents: np.ndarray, tree_bearing: np.ndarray, components: np.ndarray,
+                    depth: np.ndarray, preorder_pos: np.ndarray, postorder_pos: np.ndarray) -> None:
+    """GpuMechanismBody rows (device.rs:1699-1760) for identity root rotations."""
+    n = scene.body_count
+    rows = np.zeros(n, abi.MECHANISM_BODY)
+    root = parents < 0
+    idx = np.arange(n, dtype=np.uint32)
+    rows["metadata"][:, 0] = np.where(root, idx, parents.astype(np.int64)).astype(np.uint32)
+    rows["metadata"][:, 1] = np.where(root, abi.INVALID_INDEX, tree_bearing.astype(np.int64)).astype(np.uint32)
+    rows["metadata"][:, 2] = 0                       # bearing.compound_a is the parent
+    rows["metadata"][:, 3] = root.astype(np.uint32)
+    rows["traversal"][:, 0] = components
+    rows["traversal"][:, 1] = depth
+    rows["traversal"][:, 2] = preorder_pos
+    rows["traversal"][:, 3] = postorder_pos
+    p = scene.transforms["position"][:, :3]
+    rel = np.where(root[:, None], 0.0, p - p[np.maximum(parents, 0)])
+    rows["bind_relative_position"][:, :3] = rel.astype(np.float32)
+    rows["bind_relative_rotation"][:, 3] = 1.0
+    scene.mechanism_bodies = rows
+    scene.root_flags = root.astype(np.uint32)
+    order = np.argsort(preorder_pos, kind="stable")
+    scene.preorder = order.astype(np.uint32)
+    scene.body_components = components.astype(np.uint32)
+
+
+def bearing_chains(chains: int = 4000, links: int = 5, seed: int = 0, closure_fraction: float = 0.1,
+                   driven_fraction: float = 0.5, size: float = 0.25, height: float = 1.0,
+                   columns: int = 40, pitch_x: float = 1.5, pitch_z: float = 0.5) -> Scene:
+    """Articulated config: `chains` serial chains of `links` 0.25 m cubes (density 1000)
+    joined face to face by revolute bearings with random unit axes, travel limits
+    U(+-30, +-180) degrees, half of them driven at U(-3, 3) rad/s (max speed 3 rad/s,
+    unlimited torque, the DriveLimits defaults of mechanic-core drive.rs:534, 650-651),
+    and a loop-closure bearing between the first and last body of `closure_fraction`
+    of the chains.  Chains lie along x at `height` on a grid; roots are dynamic."""
+    rng = Rng(seed)
+    n = chains * links
+    c = np.arange(chains)
+    cx, cz = c % columns, c // columns
+    x0 = (cx - (columns - 1) * 0.5) * pitch_x
+    z0 = (cz - (chains // columns - 1) * 0.5) * pitch_z
+    k = np.arange(links)
+    x = (x0[:, None] + (k[None, :] - (links - 1) * 0.5) * size).reshape(-1)
+    translation = np.stack([x, np.full(n, height), np.repeat(z0, links)], 1).astype(np.float32)
+    rotation = np.zeros((n, 4))
+    rotation[:, 3] = 1.0
+    zeros = np.zeros(n)
+    scene = _assemble(translation, rotation, np.zeros(n, bool), zeros, zeros, zeros, (size, size, size),
+                      f"chains_{chains}x{links}")
+    has_closure = rng.uniform("closure", chains) < closure_fraction
+    tree_axes = _unit_vectors(rng, "axis", chains * (links - 1)).reshape(chains, links - 1, 3)
+    closure_axes = _unit_vectors(rng, "closure_axis", chains)
+    # bearing rows: per chain its links-1 tree bearings, then its closure (if any)
+    per_chain = (links - 1) + has_closure.astype(np.int64)
+    first_row = np.concatenate([[0], np.cumsum(per_chain)[:-1]])
+    J = int(per_chain.sum())
+    bearings = np.zeros(J, abi.BEARING)
+    coord_of_row = np.full(J, abi.INVALID_INDEX, np.uint32)
+    parents = np.full(n, -1, np.int64)
+    tree_bearing = np.full(n, -1, np.int64)
+    depth = np.tile(k, chains).astype(np.uint32)
+    pos = translation.astype(np.float64)
+    for j in range(links - 1):
+        rows = first_row + j
+        a = c * links + j
+        b = a + 1
+        anchor = pos[a] + np.array([size * 0.5, 0.0, 0.0])
+        bearings["local_anchor_a"][rows, :3] = anchor - pos[a]
+        bearings["local_anchor_b"][rows, :3] = anchor - pos[b]
+        bearings["local_axis_a"][rows, :3] = tree_axes[:, j]
+        bearings["local_axis_b"][rows, :3] = tree_axes[:, j]
+        bearings["metadata"][rows, 0] = a
+        bearings["metadata"][rows, 1] = b
+        coords = c * (links - 1) + j
+        bearings["metadata"][rows, 2] = coords
+        coord_of_row[rows] = coords
+        parents[b] = a
+        tree_bearing[b] = rows
+    closed = np.nonzero(has_closure)[0]
+    rows = first_row[closed] + (links - 1)
+    a = closed * links
+    b = a + links - 1
+    anchor = 0.5 * (pos[a] + pos[b])
+    bearings["local_anchor_a"][rows, :3] = anchor - pos[a]
+    bearings["local_anchor_b"][rows, :3] = anchor - pos[b]
+    bearings["local_axis_a"][rows, :3] = closure_axes[closed]
+    bearings["local_axis_b"][rows, :3] = closure_axes[closed]
+    bearings["metadata"][rows, 0] = a
+    bearings["metadata"][rows, 1] = b
+    bearings["metadata"][rows, 2] = abi.INVALID_INDEX
+    bearings["metadata"][rows, 3] = 1
+    scene.bearings = bearings
+    Q = chains * (links - 1)
+    limit = np.deg2rad(rng.uniform("limit", Q, 30.0, 180.0)).astype(np.float32)
+    drives = np.zeros(Q, abi.MECHANISM_DRIVE)
+    driven = rng.uniform("driven", Q) < driven_fraction
+    drives["mode"] = np.where(driven, abi.DRIVE_MODE_SPEED, abi.DRIVE_MODE_PASSIVE)
+    drives["max_acceleration"] = np.where(driven, np.inf, 0.0)
+    drives["max_speed"] = np.where(driven, 3.0, 0.0)
+    drives["target_speed"] = np.where(driven, rng.uniform("target", Q, -3.0, 3.0), 0.0)
+    drives["min_angle"] = -limit
+    drives["max_angle"] = limit
+    scene.drives = drives
+    scene.coordinate_count = Q
+    scene.max_depth = links - 1
+    scene.closure_count = int(len(closed))
+    scene.has_dynamic_root = 1
+    comp = np.repeat(c, links).astype(np.uint32)
+    _mechanism_rows(scene, parents, tree_bearing, comp, depth, np.arange(n, dtype=np.uint32),
+                    np.arange(n, dtype=np.uint32))
+    pairs = np.stack([bearings["metadata"][:, 0], bearings["metadata"][:, 1]], 1)
+    return with_suppression(scene, pairs)
+
+
+def four_bar(invalid: bool = False) -> Scene:
+    """mechanic-bench's four_bar / invalid_loop (crates/mechanic-bench/src/main.rs:372-440):
+    four 1 m cubes at (0,0,0), (1,0,0), (1,1,0), (0,1,0) joined by bearings about X, Y, -X, -Y
+    at the shared face centres; the last edge closes the loop.  `invalid` moves the closure's
+    anchor on body b by (0.2, 0.13, 0.07) m (main.rs:431-438)."""
+    translation = np.array([[0, 0, 0], [1, 0, 0], [1, 1, 0], [0, 1, 0]], np.float32)
+    rotation = np.zeros((4, 4))
+    rotation[:, 3] = 1.0
+    zeros = np.zeros(4)
+    scene = _assemble(translation, rotation, np.zeros(4, bool), zeros, zeros, zeros, (1.0, 1.0, 1.0),
+                      "invalid_loop" if invalid else "four_bar", density=REFERENCE_DENSITY)
+    edges = [(0, 1, (0.5, 0, 0), (1, 0, 0)), (1, 2, (1, 0.5, 0), (0, 1, 0)),
+             (2, 3, (0.5, 1, 0), (-1, 0, 0)), (3, 0, (0, 0.5, 0), (0, -1, 0))]
+    bearings = np.zeros(4, abi.BEARING)
+    for r, (a, b, anchor, axis) in enumerate(edges):
+        anchor = np.array(anchor, np.float32)
+        bearings["local_anchor_a"][r, :3] = anchor - translation[a]
+        bearings["local_anchor_b"][r, :3] = anchor - translation[b]
+        bearings["local_axis_a"][r, :3] = axis
+        bearings["local_axis_b"][r, :3] = axis
+        bearings["metadata"][r] = (a, b, r if r < 3 else abi.INVALID_INDEX, 0 if r < 3 else 1)
+    if invalid:
+        bearings["local_anchor_b"][3, :3] += np.array([0.2, 0.13, 0.07], np.float32)
+    scene.bearings = bearings
+    scene.drives = abi.passive_drive_rows(3)
+    scene.coordinate_count = 3
+    scene.max_depth = 3
+    scene.closure_count = 1
+    scene.has_dynamic_root = 1
+    _mechanism_rows(scene, np.array([-1, 0, 1, 2]), np.array([-1, 0, 1, 2]), np.zeros(4, np.uint32),
+                    np.arange(4, dtype=np.uint32), np.arange(4, dtype=np.uint32),
+                    np.array([3, 2, 1, 0], np.uint32))
+    return with_suppression(scene, [(0, 1), (1, 2), (2, 3), (3, 0)])

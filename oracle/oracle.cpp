@@ -162,7 +162,6 @@ template <class T> struct World : WorldBase {
     std::vector<uint32_t> active;
     std::unordered_map<uint64_t, Manifold<T>> manifold;
     std::vector<V4<T>> snap_pos[3], snap_rot[3];
-    std::vector<Link<T>> links;
     GpuDiagnostics diag{};
     uint32_t tick32 = 0;
 
@@ -501,6 +500,8 @@ template <class T> struct World : WorldBase {
 #pragma omp parallel for schedule(dynamic, 256)
         for (int64_t pp = 0; pp < (int64_t)np; ++pp) {
             uint32_t ia = pairs[2 * pp], ib = pairs[2 * pp + 1];
+            emit[pp] = 0;
+            if (!self_collisions && components[col[ia].meta[0]] == components[col[ib].meta[0]]) continue;
             Obb<T> a = obb(ia), b = obb(ib);
             Sat<T> s = obb_sat(a, b);
             emit[pp] = 0;
@@ -742,6 +743,557 @@ template <class T> struct World : WorldBase {
         snap_rot[slot] = rot;
     }
 
+
+    // ================================================= articulated passes
+    // mechanism.wgsl:67-185, articulated.wgsl:94-484, closure.wgsl:94-427,
+    // bearings.wgsl:48-102, in the dispatch order of device.rs:963-1155.
+    std::vector<Link<T>> links_a, links_b;
+    std::vector<uint32_t> mdeltas;     // bearing-projection fixed-point deltas (6 per body)
+    std::vector<T> grad, dgl;          // closure accumulators
+    uint32_t closure_state[2] = {0, 0};
+    struct Pcg { T sol, res, pre, dir, op; };
+    std::vector<Pcg> pcg;
+    uint32_t jump_rounds = 0;
+    bool final_is_a = true;
+    std::vector<Link<T>>& final_links() { return final_is_a ? links_a : links_b; }
+
+    V3<T> wii(uint32_t b, V3<T> v) const {   // articulated.wgsl:94-102 (body-frame mass rows)
+        V4<T> r = rot[b];
+        V3<T> l = quat_rotate(conj(r), v);
+        const Mass<T>& m = mass[b];
+        V3<T> lr = m.ix * l.x + m.iy * l.y + m.iz * l.z;
+        return quat_rotate(r, lr);
+    }
+    void add_mdelta(uint32_t b, V3<T> l, V3<T> a) {   // articulated.wgsl:104-112
+        const T s = T(1048576.0f);
+        uint32_t* d = &mdeltas[6 * (size_t)b];
+        int32_t v[6] = {fixed_i32(l.x * s), fixed_i32(l.y * s), fixed_i32(l.z * s),
+                        fixed_i32(a.x * s), fixed_i32(a.y * s), fixed_i32(a.z * s)};
+        for (int k = 0; k < 6; ++k) {
+            std::atomic_ref<uint32_t> r(d[k]);
+            r.fetch_add((uint32_t)v[k], std::memory_order_relaxed);
+        }
+    }
+    void solve_linear_axis(uint32_t a, uint32_t b, V3<T> arm_a, V3<T> arm_b, V3<T> rel, V3<T> d) {   // :114-143
+        V3<T> ang_a = cross(arm_a, d), ang_b = cross(arm_b, d);
+        T den = mass[a].inv_mass + mass[b].inv_mass + dot(ang_a, wii(a, ang_a)) + dot(ang_b, wii(b, ang_b));
+        if (den <= T(1.0e-12f)) return;
+        V3<T> imp = d * (T(0.5f) * dot(rel, d) / den);
+        add_mdelta(a, imp * mass[a].inv_mass, wii(a, cross(arm_a, imp)));
+        add_mdelta(b, -imp * mass[b].inv_mass, wii(b, cross(arm_b, -imp)));
+    }
+    void solve_angular_axis(uint32_t a, uint32_t b, V3<T> rel, V3<T> axis) {   // :145-155
+        V3<T> ia = wii(a, axis), ib = wii(b, axis);
+        T den = dot(axis, ia + ib);
+        if (den <= T(1.0e-12f)) return;
+        T imp = T(0.5f) * dot(rel, axis) / den;
+        add_mdelta(a, v3<T>(0, 0, 0), ia * imp);
+        add_mdelta(b, v3<T>(0, 0, 0), -ib * imp);
+    }
+    void hinge_tangents(uint32_t a, uint32_t b, const Bearing<T>& br, V3<T>& ta, V3<T>& tb) const {
+        V3<T> axa = normalize(quat_rotate(rot[a], xyz(br.xa)));
+        V3<T> axb = normalize(quat_rotate(rot[b], xyz(br.xb)));
+        V3<T> hinge = normalize(axa + axb);
+        V3<T> helper = std::fabs(hinge.x) > T(0.8f) ? v3<T>(0, 1, 0) : v3<T>(1, 0, 0);
+        ta = normalize(cross(hinge, helper));
+        tb = cross(hinge, ta);
+    }
+    void project_bearing_velocities() {   // articulated.wgsl:287-316 (relaxed Jacobi)
+#pragma omp parallel for schedule(static)
+        for (int64_t jj = 0; jj < (int64_t)J; ++jj) {
+            const Bearing<T>& br = bear[jj];
+            uint32_t a = br.meta[0], b = br.meta[1];
+            V3<T> arm_a = quat_rotate(rot[a], xyz(br.aa)), arm_b = quat_rotate(rot[b], xyz(br.ab));
+            V3<T> va = xyz(lin[a]) + cross(xyz(ang[a]), arm_a);
+            V3<T> vb = xyz(lin[b]) + cross(xyz(ang[b]), arm_b);
+            V3<T> rel = vb - va;
+            solve_linear_axis(a, b, arm_a, arm_b, rel, v3<T>(1, 0, 0));
+            solve_linear_axis(a, b, arm_a, arm_b, rel, v3<T>(0, 1, 0));
+            solve_linear_axis(a, b, arm_a, arm_b, rel, v3<T>(0, 0, 1));
+            V3<T> ta, tb;
+            hinge_tangents(a, b, br, ta, tb);
+            V3<T> rang = xyz(ang[b]) - xyz(ang[a]);
+            solve_angular_axis(a, b, rang, ta);
+            solve_angular_axis(a, b, rang, tb);
+        }
+    }
+    void apply_mdeltas() {   // articulated.wgsl:318-337
+        const T s = T(1048576.0f);
+#pragma omp parallel for schedule(static)
+        for (int64_t bb = 0; bb < (int64_t)B; ++bb) {
+            uint32_t* d = &mdeltas[6 * bb];
+            V3<T> ld = v3<T>(T((int32_t)d[0]), T((int32_t)d[1]), T((int32_t)d[2])) / s;
+            V3<T> ad = v3<T>(T((int32_t)d[3]), T((int32_t)d[4]), T((int32_t)d[5])) / s;
+            for (int k = 0; k < 6; ++k) d[k] = 0;
+            lin[bb] = v4(xyz(lin[bb]) + ld, T(0));
+            ang[bb] = v4(xyz(ang[bb]) + ad, T(0));
+        }
+    }
+    void bearing_projection_iteration() { project_bearing_velocities(); apply_mdeltas(); }
+
+    // serial Gauss-Seidel variants (articulated.wgsl:157-285)
+    void linear_axis_immediate(uint32_t a, uint32_t b, V3<T> arm_a, V3<T> arm_b, V3<T> rel, V3<T> d) {
+        V3<T> ang_a = cross(arm_a, d), ang_b = cross(arm_b, d);
+        T den = mass[a].inv_mass + mass[b].inv_mass + dot(ang_a, wii(a, ang_a)) + dot(ang_b, wii(b, ang_b));
+        if (den <= T(1.0e-12f)) return;
+        V3<T> imp = d * (dot(rel, d) / den);
+        lin[a] = v4(xyz(lin[a]) + imp * mass[a].inv_mass, T(0));
+        ang[a] = v4(xyz(ang[a]) + wii(a, cross(arm_a, imp)), T(0));
+        lin[b] = v4(xyz(lin[b]) - imp * mass[b].inv_mass, T(0));
+        ang[b] = v4(xyz(ang[b]) + wii(b, cross(arm_b, -imp)), T(0));
+    }
+    void angular_axis_immediate(uint32_t a, uint32_t b, V3<T> rel, V3<T> axis) {
+        V3<T> ia = wii(a, axis), ib = wii(b, axis);
+        T den = dot(axis, ia + ib);
+        if (den <= T(1.0e-12f)) return;
+        T imp = dot(rel, axis) / den;
+        ang[a] = v4(xyz(ang[a]) + ia * imp, T(0));
+        ang[b] = v4(xyz(ang[b]) - ib * imp, T(0));
+    }
+    void project_bearing_row_immediate(uint32_t j) {
+        const Bearing<T>& br = bear[j];
+        uint32_t a = br.meta[0], b = br.meta[1];
+        V3<T> arm_a = quat_rotate(rot[a], xyz(br.aa)), arm_b = quat_rotate(rot[b], xyz(br.ab));
+        const V3<T> dirs[3] = {v3<T>(1, 0, 0), v3<T>(0, 1, 0), v3<T>(0, 0, 1)};
+        for (int k = 0; k < 3; ++k) {
+            V3<T> va = xyz(lin[a]) + cross(xyz(ang[a]), arm_a);
+            V3<T> vb = xyz(lin[b]) + cross(xyz(ang[b]), arm_b);
+            linear_axis_immediate(a, b, arm_a, arm_b, vb - va, dirs[k]);
+        }
+        V3<T> ta, tb;
+        hinge_tangents(a, b, br, ta, tb);
+        V3<T> rang = xyz(ang[b]) - xyz(ang[a]);
+        angular_axis_immediate(a, b, rang, ta);
+        rang = xyz(ang[b]) - xyz(ang[a]);
+        angular_axis_immediate(a, b, rang, tb);
+    }
+    void project_bearing_velocities_serial() {
+        for (uint32_t j = 0; j < J; ++j) project_bearing_row_immediate(j);
+        for (uint32_t j = J; j > 0; --j) project_bearing_row_immediate(j - 1);
+    }
+
+    V3<T> permitted_axis(uint32_t body) const {   // articulated.wgsl:339-348
+        const MechBody<T>& m = mech[body];
+        uint32_t parent = m.meta[0];
+        const Bearing<T>& br = bear[m.meta[1]];
+        V3<T> axis = normalize(quat_rotate(rot[parent], xyz(br.xa)));
+        if (m.meta[2] != 0) axis = -normalize(quat_rotate(rot[parent], xyz(br.xb)));
+        return axis;
+    }
+    T permitted_speed(uint32_t body) const {
+        uint32_t parent = mech[body].meta[0];
+        return dot(xyz(ang[body]) - xyz(ang[parent]), permitted_axis(body));
+    }
+    T stabilized_speed(uint32_t body, T speed) const {
+        bool aligned = std::fabs(permitted_axis(body).y) > T(0.999f);
+        return (aligned && std::fabs(speed) < T(0.005f)) ? T(0) : speed;
+    }
+    void advance_coordinates() {   // articulated.wgsl:366-415
+#pragma omp parallel for schedule(static)
+        for (int64_t bb = 0; bb < (int64_t)B; ++bb) {
+            uint32_t body = (uint32_t)bb;
+            if (mech[body].meta[3] != 0) continue;
+            const Bearing<T>& br = bear[mech[body].meta[1]];
+            uint32_t c = br.meta[2];
+            if (c == INVALID) continue;
+            T measured = permitted_speed(body) * ang_damp;
+            const Drive& dr = drives[c];
+            T speed = T(0);
+            if (dr.mode == MK_DRIVE_MODE_PASSIVE) {
+                speed = stabilized_speed(body, measured);
+            } else {
+                T desired = clampv(T(dr.target_speed), T(-dr.max_speed), T(dr.max_speed));
+                if (dr.mode == MK_DRIVE_MODE_ANGLE) {
+                    T err = T(dr.target_angle) - coords[c].x;
+                    T brake = std::sqrt(T(2) * T(dr.max_acc) * std::fabs(err));
+                    desired = sgn(err) * mn(brake, T(dr.max_speed));
+                    if (std::fabs(err) < T(0.0005f)) desired = T(0);
+                }
+                T budget = T(dr.max_acc) * dt;
+                speed = measured + clampv(desired - measured, -budget, budget);
+            }
+            T angle = coords[c].x + speed * dt;
+            if (angle < T(dr.min_angle)) { angle = T(dr.min_angle); speed = T(0); }
+            else if (angle > T(dr.max_angle)) { angle = T(dr.max_angle); speed = T(0); }
+            coords[c].y = speed;
+            coords[c].x = angle;
+        }
+    }
+    void capture_coordinates() {   // articulated.wgsl:417-429
+#pragma omp parallel for schedule(static)
+        for (int64_t bb = 0; bb < (int64_t)B; ++bb) {
+            uint32_t body = (uint32_t)bb;
+            if (mech[body].meta[3] != 0) continue;
+            uint32_t c = bear[mech[body].meta[1]].meta[2];
+            if (c != INVALID) coords[c].y = stabilized_speed(body, permitted_speed(body));
+        }
+    }
+    void reconstruct_body_velocities() {   // articulated.wgsl:431-456 (serial preorder)
+        for (uint32_t t = 0; t < B; ++t) {
+            uint32_t body = preorder[t];
+            const MechBody<T>& m = mech[body];
+            if (m.meta[3] != 0) continue;
+            uint32_t parent = m.meta[0];
+            const Bearing<T>& br = bear[m.meta[1]];
+            V3<T> axis = normalize(quat_rotate(rot[parent], xyz(br.xa)));
+            V3<T> pa = quat_rotate(rot[parent], xyz(br.aa));
+            V3<T> ca = quat_rotate(rot[body], xyz(br.ab));
+            if (m.meta[2] != 0) {
+                axis = -normalize(quat_rotate(rot[parent], xyz(br.xb)));
+                pa = quat_rotate(rot[parent], xyz(br.ab));
+                ca = quat_rotate(rot[body], xyz(br.aa));
+            }
+            T speed = coords[br.meta[2]].y;
+            V3<T> angular = xyz(ang[parent]) + axis * speed;
+            V3<T> av = xyz(lin[parent]) + cross(xyz(ang[parent]), pa);
+            lin[body] = v4(av - cross(angular, ca), T(0));
+            ang[body] = v4(angular, T(0));
+        }
+    }
+    void validate_articulated_state() {   // articulated.wgsl:458-484
+        std::atomic<uint32_t> bad{0};
+#pragma omp parallel for schedule(static)
+        for (int64_t bb = 0; bb < (int64_t)B; ++bb) {
+            uint32_t body = (uint32_t)bb;
+            T rl = dot4(rot[body], rot[body]);
+            bool valid = finite4(pos[body]) && finite4(rot[body]) && finite4(lin[body]) && finite4(ang[body]) &&
+                         rl > T(0.5f) && rl < T(1.5f);
+            const MechBody<T>& m = mech[body];
+            if (m.meta[3] == 0) {
+                uint32_t c = bear[m.meta[1]].meta[2];
+                const V4<T>& st = coords[c];
+                const T lim = T(3.402823e+38f);
+                valid = valid && st.x == st.x && std::fabs(st.x) < lim && st.y == st.y && std::fabs(st.y) < lim;
+            }
+            if (!valid) bad = 1;
+        }
+        if (bad.load()) diag.error_flags |= MK_INVALID_NUMERIC_FLAG;
+    }
+
+    // ---------------------------------------------- forward kinematics
+    static V4<T> axis_rotation(V3<T> axis, T angle) {   // mechanism.wgsl:67-70
+        T h = angle * T(0.5f);
+        V3<T> v = normalize(axis) * tsin(h);
+        return {v.x, v.y, v.z, tcos(h)};
+    }
+    void prepare_links() {   // mechanism.wgsl:72-108
+#pragma omp parallel for schedule(static)
+        for (int64_t bb = 0; bb < (int64_t)B; ++bb) {
+            uint32_t body = (uint32_t)bb;
+            const MechBody<T>& m = mech[body];
+            Link<T>& L = links_a[body];
+            if (m.meta[3] != 0) {
+                L.pos = {0, 0, 0, 0}; L.rot = {0, 0, 0, 1};
+                L.meta[0] = body; L.meta[1] = 1; L.meta[2] = 0; L.meta[3] = 0;
+                continue;
+            }
+            const Bearing<T>& br = bear[m.meta[1]];
+            T angle = coords[br.meta[2]].x;
+            V4<T> rr;
+            V3<T> rp;
+            if (m.meta[2] == 0) {
+                rr = quat_multiply(axis_rotation(xyz(br.xa), angle), m.brot);
+                rp = xyz(br.aa) - quat_rotate(rr, xyz(br.ab));
+            } else {
+                rr = quat_multiply(axis_rotation(xyz(br.xb), -angle), m.brot);
+                rp = xyz(br.ab) - quat_rotate(rr, xyz(br.aa));
+            }
+            L.pos = v4(rp, T(0)); L.rot = rr;
+            L.meta[0] = m.meta[0]; L.meta[1] = 0; L.meta[2] = 0; L.meta[3] = 0;
+        }
+    }
+    static Link<T> compose(const Link<T>& child, const Link<T>& parent) {   // mechanism.wgsl:110-119
+        Link<T> r;
+        r.pos = v4(xyz(parent.pos) + quat_rotate(parent.rot, xyz(child.pos)), T(0));
+        r.rot = normalize4(quat_multiply(parent.rot, child.rot));
+        r.meta[0] = parent.meta[0]; r.meta[1] = 0; r.meta[2] = 0; r.meta[3] = 0;
+        return r;
+    }
+    void jump(const std::vector<Link<T>>& src, std::vector<Link<T>>& dst) {   // mechanism.wgsl:121-149
+#pragma omp parallel for schedule(static)
+        for (int64_t bb = 0; bb < (int64_t)B; ++bb) {
+            const Link<T>& child = src[bb];
+            if (child.meta[1] != 0) { dst[bb] = child; continue; }
+            const Link<T>& par = src[child.meta[0]];
+            dst[bb] = compose(child, par);
+            dst[bb].meta[1] = par.meta[1];
+        }
+    }
+    void forward_kinematics() {
+        prepare_links();
+        bool a_final = true;
+        for (uint32_t r = 0; r < jump_rounds; ++r) {
+            if (a_final) jump(links_a, links_b); else jump(links_b, links_a);
+            a_final = !a_final;
+        }
+    }
+    void publish() {   // mechanism.wgsl:151-185
+        const std::vector<Link<T>>& L = final_links();
+#pragma omp parallel for schedule(static)
+        for (int64_t bb = 0; bb < (int64_t)B; ++bb) {
+            uint32_t root_body = L[bb].meta[0];
+            if ((uint32_t)bb == root_body) continue;
+            pos[bb] = v4(xyz(pos[root_body]) + quat_rotate(rot[root_body], xyz(L[bb].pos)), T(0));
+            rot[bb] = normalize4(quat_multiply(rot[root_body], L[bb].rot));
+        }
+    }
+
+    // ------------------------------------------------------ closures
+    struct Vec2 { V3<T> p, a; };
+    void joint_frame(uint32_t body, V3<T>& axis, V3<T>& anchor, uint32_t& coord, uint32_t& parent) const {
+        const MechBody<T>& m = mech[body];
+        parent = m.meta[0];
+        const Bearing<T>& tb = bear[m.meta[1]];
+        const Link<T>& pp = links_final_const()[parent];
+        if (m.meta[2] == 0) {
+            axis = normalize(quat_rotate(pp.rot, xyz(tb.xa)));
+            anchor = xyz(pp.pos) + quat_rotate(pp.rot, xyz(tb.aa));
+        } else {
+            axis = -normalize(quat_rotate(pp.rot, xyz(tb.xb)));
+            anchor = xyz(pp.pos) + quat_rotate(pp.rot, xyz(tb.ab));
+        }
+        coord = tb.meta[2];
+    }
+    const std::vector<Link<T>>& links_final_const() const { return final_is_a ? links_a : links_b; }
+    void closure_frames(const Bearing<T>& br, V3<T>& anc_a, V3<T>& anc_b, V3<T>& ax_a, V3<T>& ax_b) const {
+        const std::vector<Link<T>>& L = links_final_const();
+        const Link<T>& pa = L[br.meta[0]];
+        const Link<T>& pb = L[br.meta[1]];
+        anc_a = xyz(pa.pos) + quat_rotate(pa.rot, xyz(br.aa));
+        anc_b = xyz(pb.pos) + quat_rotate(pb.rot, xyz(br.ab));
+        ax_a = normalize(quat_rotate(pa.rot, xyz(br.xa)));
+        ax_b = normalize(quat_rotate(pb.rot, xyz(br.xb)));
+    }
+    void accumulate_branch(uint32_t start, V3<T> ea, V3<T> ex, V3<T> rp, V3<T> ra, T sign) {   // closure.wgsl:128-192
+        uint32_t body = start;
+        for (uint32_t guard = 0; guard <= B; ++guard) {
+            if (mech[body].meta[3] != 0) break;
+            V3<T> axis, anchor; uint32_t c, parent;
+            joint_frame(body, axis, anchor, c, parent);
+            if (c >= Q) { diag.error_flags |= MK_INVALID_NUMERIC_FLAG; }
+            else {
+                V3<T> pd = cross(axis, ea - anchor) * sign;
+                V3<T> ad = cross(axis, ex) * sign;
+                T g = dot(rp, pd) + T(1) * dot(ra, ad);
+                T d = dot(pd, pd) + T(1) * dot(ad, ad);
+                if (g == g && d == d) { grad[c] += g; dgl[c] += d; }
+                else diag.error_flags |= MK_INVALID_NUMERIC_FLAG;
+            }
+            body = parent;
+        }
+    }
+    void evaluate_closures() {   // closure.wgsl:268-319 (sequential in bearing order)
+        for (uint32_t j = 0; j < J; ++j) {
+            const Bearing<T>& br = bear[j];
+            if (br.meta[3] == 0) continue;
+            V3<T> aa, ab, xa, xb;
+            closure_frames(br, aa, ab, xa, xb);
+            V3<T> rp = aa - ab, ra = xa - xb;
+            auto finite3 = [](V3<T> v) {
+                const T lim = T(3.402823e+38f);
+                return v.x == v.x && v.y == v.y && v.z == v.z && std::fabs(v.x) < lim && std::fabs(v.y) < lim &&
+                       std::fabs(v.z) < lim;
+            };
+            if (!finite3(rp) || !finite3(ra)) {   // per-bearing return in the kernel
+                diag.error_flags |= MK_INVALID_NUMERIC_FLAG;
+                closure_state[0] = closure_state[1] = 0xffffffffu;
+                continue;
+            }
+            uint32_t um = round_u32(length(rp) * T(1000000.0f));
+            // closure.wgsl:295 measures the axis error as acos(dot); in FP32 that
+            // reads 0 below ~3.5e-4 rad (dot rounds to 1), blind to its own
+            // 1000 micro-degree tolerance.  The angle is taken as
+            // atan2(|a x b|, a . b), the form bearings.wgsl:56-59 validates with.
+            T deg = tatan2(length(cross(xa, xb)), clampv(dot(xa, xb), T(-1), T(1))) * T(57.295779513f);
+            uint32_t ud = round_u32(deg * T(1000000.0f));
+            closure_state[0] = std::max(closure_state[0], um);
+            closure_state[1] = std::max(closure_state[1], ud);
+            if (um <= 10u && ud <= 1000u) continue;
+            accumulate_branch(br.meta[0], aa, xa, rp, ra, T(1));
+            accumulate_branch(br.meta[1], ab, xb, rp, ra, T(-1));
+        }
+    }
+    Vec2 branch_product(uint32_t start, V3<T> ea, V3<T> ex, T sign) const {   // closure.wgsl:194-230
+        Vec2 prod{v3<T>(0, 0, 0), v3<T>(0, 0, 0)};
+        uint32_t body = start;
+        for (uint32_t guard = 0; guard <= B; ++guard) {
+            if (mech[body].meta[3] != 0) break;
+            V3<T> axis, anchor; uint32_t c, parent;
+            joint_frame(body, axis, anchor, c, parent);
+            T d = pcg[c].dir;
+            prod.p = prod.p + sign * cross(axis, ea - anchor) * d;
+            prod.a = prod.a + sign * cross(axis, ex) * d;
+            body = parent;
+        }
+        return prod;
+    }
+    void branch_transpose(uint32_t start, V3<T> ea, V3<T> ex, const Vec2& prod, T sign) {   // closure.wgsl:232-266
+        uint32_t body = start;
+        for (uint32_t guard = 0; guard <= B; ++guard) {
+            if (mech[body].meta[3] != 0) break;
+            V3<T> axis, anchor; uint32_t c, parent;
+            joint_frame(body, axis, anchor, c, parent);
+            V3<T> pd = sign * cross(axis, ea - anchor);
+            V3<T> ad = sign * cross(axis, ex);
+            pcg[c].op += dot(pd, prod.p) + T(1) * dot(ad, prod.a);
+            body = parent;
+        }
+    }
+    uint32_t closure_pcg_rounds = 8;
+    void solve_closure_pcg() {   // closure.wgsl:333-427 (one Newton step, 8 diagonal-PCG rounds)
+        T rz = T(0);
+        for (uint32_t c = 0; c < Q; ++c) {
+            T g = grad[c], d = dgl[c], r = T(0), z = T(0);
+            if (d > T(1.0e-12f)) { r = -g; z = r / d; }
+            pcg[c] = {T(0), r, z, z, T(0)};
+            rz += r * z;
+        }
+        for (uint32_t it = 0; it < closure_pcg_rounds; ++it) {
+            for (uint32_t c = 0; c < Q; ++c) pcg[c].op = T(0);
+            for (uint32_t j = 0; j < J; ++j) {
+                const Bearing<T>& br = bear[j];
+                if (br.meta[3] == 0) continue;
+                V3<T> aa, ab, xa, xb;
+                closure_frames(br, aa, ab, xa, xb);
+                Vec2 pa = branch_product(br.meta[0], aa, xa, T(1));
+                Vec2 pb = branch_product(br.meta[1], ab, xb, T(-1));
+                Vec2 prod{pa.p + pb.p, pa.a + pb.a};
+                branch_transpose(br.meta[0], aa, xa, prod, T(1));
+                branch_transpose(br.meta[1], ab, xb, prod, T(-1));
+            }
+            T dop = T(0);
+            for (uint32_t c = 0; c < Q; ++c) dop += pcg[c].dir * pcg[c].op;
+            T alpha = std::fabs(dop) > T(1.0e-20f) ? rz / dop : T(0);
+            T nrz = T(0);
+            for (uint32_t c = 0; c < Q; ++c) {
+                pcg[c].sol += alpha * pcg[c].dir;
+                pcg[c].res -= alpha * pcg[c].op;
+                T d = dgl[c];
+                pcg[c].pre = T(0);
+                if (d > T(1.0e-12f)) pcg[c].pre = pcg[c].res / d;
+                nrz += pcg[c].res * pcg[c].pre;
+            }
+            T beta = std::fabs(rz) > T(1.0e-20f) ? nrz / rz : T(0);
+            for (uint32_t c = 0; c < Q; ++c) pcg[c].dir = pcg[c].pre + beta * pcg[c].dir;
+            rz = nrz;
+        }
+        for (uint32_t c = 0; c < Q; ++c) {
+            T st = clampv(T(0.35f) * pcg[c].sol, T(-0.2f), T(0.2f));
+            if (st == st) coords[c].x += st;
+            else diag.error_flags |= MK_INVALID_NUMERIC_FLAG;
+        }
+    }
+    void closure_loop() {   // device.rs:973-1020
+        bool converged_prev = false;
+        for (uint32_t step = 0; step < 12; ++step) {
+            std::fill(grad.begin(), grad.end(), T(0));
+            std::fill(dgl.begin(), dgl.end(), T(0));
+            closure_state[0] = closure_state[1] = 0;
+            if (step == 0 || !converged_prev) evaluate_closures();
+            bool unconverged = closure_state[0] > 10u || closure_state[1] > 1000u;
+            if (unconverged) {
+                solve_closure_pcg();
+                forward_kinematics();
+            }
+            converged_prev = !unconverged;
+        }
+    }
+
+    void mechanism_passes() {   // device.rs:963-1048
+        for (uint32_t it = 0; it < std::max(1u, iterations); ++it) bearing_projection_iteration();
+        advance_coordinates();
+        forward_kinematics();
+        if (closure_count > 0) closure_loop();
+        publish();
+        reconstruct_body_velocities();
+    }
+    void post_contact_mechanism() {   // device.rs:1128-1155
+        if (!has_dynamic_root)
+            for (uint32_t it = 0; it < std::max(1u, iterations); ++it) bearing_projection_iteration();
+        capture_coordinates();
+        if (!has_dynamic_root) reconstruct_body_velocities();
+    }
+    void validate_bearings(bool use_links) {   // bearings.wgsl:48-102
+        for (uint32_t j = 0; j < J; ++j) {
+            const Bearing<T>& br = bear[j];
+            uint32_t a = br.meta[0], b = br.meta[1];
+            V4<T> pa, qa, pb, qb;
+            if (use_links) {
+                const std::vector<Link<T>>& L = links_final_const();
+                pa = L[a].pos; qa = L[a].rot; pb = L[b].pos; qb = L[b].rot;
+            } else {
+                pa = pos[a]; qa = rot[a]; pb = pos[b]; qb = rot[b];
+            }
+            V3<T> anc_a = xyz(pa) + quat_rotate(qa, xyz(br.aa));
+            V3<T> anc_b = xyz(pb) + quat_rotate(qb, xyz(br.ab));
+            V3<T> axa = normalize(quat_rotate(qa, xyz(br.xa)));
+            V3<T> axb = normalize(quat_rotate(qb, xyz(br.xb)));
+            uint32_t um = round_u32(length(anc_a - anc_b) * T(1000000.0f));
+            T deg = tatan2(length(cross(axa, axb)), clampv(dot(axa, axb), T(-1), T(1))) * T(57.295779513f);
+            uint32_t ud = round_u32(deg * T(1000000.0f));
+            diag.max_anchor_micrometers = std::max(diag.max_anchor_micrometers, um);
+            diag.max_axis_microdegrees = std::max(diag.max_axis_microdegrees, ud);
+            if (br.meta[3] != 0 && (um > 10u || ud > 1000u)) diag.error_flags |= MK_CONSTRAINT_NON_CONVERGENCE_FLAG;
+        }
+    }
+
+    // serial contact Gauss-Seidel (collision.wgsl:908-1048), mechanisms with a
+    // dynamic root and at most 64 bearings (device.rs:1370-1417)
+    void solve_contact_immediate(uint32_t ci) {
+        Contact<T>& c = contacts[ci];
+        uint32_t a = c.meta[0], b = c.meta[1];
+        V3<T> arm_a = xyz(c.aa), arm_b = xyz(c.ab);
+        V3<T> vb = v3<T>(0, 0, 0);
+        if (b != INVALID) vb = contact_velocity(b, arm_b);
+        V3<T> n = xyz(c.np);
+        T den = impulse_denominator(a, b, arm_a, arm_b, n);
+        if (den <= T(0)) return;
+        V3<T> rel = vb - contact_velocity(a, arm_a);
+        T vn = dot(rel, n);
+        if (c.np.w <= T(1.0e-5f) && vn >= T(-1.0e-5f) && c.aa.w <= T(1.0e-6f)) { c.aa.w = T(0); return; }
+        T prev = mx(c.aa.w, T(0));
+        T acc = mx(prev + (-vn + penetration_bias(c.np.w, c.ab.w < T(0))) / den, T(0));
+        T delta = acc - prev;
+        c.aa.w = acc;
+        V3<T> imp = n * delta;
+        V3<T> tv = rel - n * vn;
+        T ts = length(tv);
+        if (ts > T(1.0e-6f)) {
+            V3<T> t = tv / ts;
+            T tden = impulse_denominator(a, b, arm_a, arm_b, t);
+            T fr = mn(ts / tden, std::fabs(delta) * T(0.05f));
+            imp = imp - t * fr;
+        }
+        lin[a] = v4(xyz(lin[a]) - imp * wm[a].x.w, T(0));
+        ang[a] = v4(xyz(ang[a]) + inverse_inertia(a, cross(arm_a, -imp)), T(0));
+        if (b != INVALID) {
+            lin[b] = v4(xyz(lin[b]) + imp * wm[b].x.w, T(0));
+            ang[b] = v4(xyz(ang[b]) + inverse_inertia(b, cross(arm_b, imp)), T(0));
+        }
+    }
+    void solve_serial_pass() {
+        uint32_t A = (uint32_t)active.size();
+        if (A > 64) {
+            for (uint32_t k = 0; k < A; ++k) solve_contact_immediate(active[k]);
+            for (uint32_t k = A; k > 0; --k) solve_contact_immediate(active[k - 1]);
+            return;
+        }
+        std::vector<uint32_t> order(active.begin(), active.end());
+        std::sort(order.begin(), order.end(), [&](uint32_t x, uint32_t y) {
+            const Contact<T>& cx = contacts[x]; const Contact<T>& cy = contacts[y];
+            if (cx.meta[0] != cy.meta[0]) return cx.meta[0] < cy.meta[0];
+            if (cx.meta[1] != cy.meta[1]) return cx.meta[1] < cy.meta[1];
+            return cx.meta[2] < cy.meta[2];
+        });
+        for (uint32_t k = 0; k < A; ++k) solve_contact_immediate(order[k]);
+        for (uint32_t k = A; k > 0; --k) solve_contact_immediate(order[k - 1]);
+    }
+
+    bool mechanism_active() const { return max_depth > 0; }
+    bool serial_mechanism() const { return mechanism_active() && has_dynamic_root && J <= 64; }
+
+    // device.rs:1219-1431, with bearing projection interleaved when a
+    // mechanism root is dynamic (:1363-1416)
     void collision_passes() {
         update_world_masses();
         compute_bounds();
@@ -749,7 +1301,31 @@ template <class T> struct World : WorldBase {
         narrowphase();
         ground_contacts();
         prepare_contacts();
-        solve();
+        const bool interleave = mechanism_active() && has_dynamic_root;
+        const bool serial = serial_mechanism();
+        const uint32_t A = (uint32_t)active.size();
+        // warm start + apply
+#pragma omp parallel for schedule(static)
+        for (int64_t k = 0; k < (int64_t)A; ++k) solve_contact(active[k], true);
+        if (A > 0) solve_apply();
+        if (interleave) {
+            if (serial) { if (A > 0) project_bearing_velocities_serial(); }
+            else bearing_projection_iteration();
+        }
+        const uint32_t iters = serial ? std::max(1u, iterations) * 12u : std::max(1u, iterations);
+        for (uint32_t it = 1; it < iters; ++it) {
+            if (serial) {
+                solve_serial_pass();
+            } else {
+#pragma omp parallel for schedule(static)
+                for (int64_t k = 0; k < (int64_t)A; ++k) solve_contact(active[k], false);
+                if (A > 0) solve_apply();
+            }
+            if (interleave) {
+                if (serial) { if (A > 0) project_bearing_velocities_serial(); }
+                else bearing_projection_iteration();
+            }
+        }
         persist();
     }
 
@@ -758,9 +1334,14 @@ template <class T> struct World : WorldBase {
         tick32 = (uint32_t)tick;
         uint32_t slot = (uint32_t)(tick % 3);
         std::fill(deltas.begin(), deltas.end(), 0u);
+        std::fill(mdeltas.begin(), mdeltas.end(), 0u);
         integrate();
+        if (mechanism_active()) mechanism_passes();
         bool run_collisions = collisions && C > 0;
         if (run_collisions) collision_passes();
+        if (mechanism_active() && run_collisions) post_contact_mechanism();
+        if (mechanism_active()) validate_articulated_state();
+        if (J > 0) validate_bearings(mechanism_active());
         snapshot(slot);
         return 0;
     }
@@ -834,6 +1415,53 @@ static World<T>* build_world(const MkCreation* cr, const MkConfig* cfg, uint32_t
     w->keys.resize(C); w->skeys.resize(C); w->svals.resize(C);
     for (int s = 0; s < 3; ++s) { w->snap_pos[s] = w->pos; w->snap_rot[s] = w->rot; }
     w->coords.assign(w->Q, V4<T>{0, 0, 0, 0});
+    uint32_t J = w->J;
+    w->bear.resize(J);
+    for (uint32_t j = 0; j < J; ++j) {
+        const GpuBearing& g = cr->bearings[j];
+        w->bear[j].aa = load4<T>(g.local_anchor_a); w->bear[j].ab = load4<T>(g.local_anchor_b);
+        w->bear[j].xa = load4<T>(g.local_axis_a); w->bear[j].xb = load4<T>(g.local_axis_b);
+        for (int k = 0; k < 4; ++k) w->bear[j].meta[k] = g.metadata[k];
+    }
+    w->mech.resize(B);
+    w->preorder.resize(B);
+    for (uint32_t i = 0; i < B; ++i) {
+        if (cr->mechanism_bodies) {
+            const GpuMechanismBody& g = cr->mechanism_bodies[i];
+            for (int k = 0; k < 4; ++k) { w->mech[i].meta[k] = g.metadata[k]; w->mech[i].trav[k] = g.traversal[k]; }
+            w->mech[i].bpos = load4<T>(g.bind_relative_position);
+            w->mech[i].brot = load4<T>(g.bind_relative_rotation);
+        } else {
+            w->mech[i].meta[0] = i; w->mech[i].meta[1] = INVALID; w->mech[i].meta[2] = 0; w->mech[i].meta[3] = 1;
+            for (int k = 0; k < 4; ++k) w->mech[i].trav[k] = 0;
+            w->mech[i].bpos = {0, 0, 0, 0}; w->mech[i].brot = {0, 0, 0, 1};
+        }
+        w->preorder[i] = cr->preorder ? cr->preorder[i] : i;
+    }
+    w->drives.resize(w->Q);
+    for (uint32_t c = 0; c < w->Q; ++c) {
+        Drive d{};
+        if (cr->drives) {
+            const GpuMechanismDrive& g = cr->drives[c];
+            d.mode = g.mode; d.max_acc = g.max_acceleration; d.max_speed = g.max_speed;
+            d.target_speed = g.target_speed; d.target_angle = g.target_angle;
+            d.min_angle = g.min_angle; d.max_angle = g.max_angle;
+        } else {
+            d.mode = MK_DRIVE_MODE_PASSIVE; d.min_angle = -INFINITY; d.max_angle = INFINITY;
+        }
+        w->drives[c] = d;
+    }
+    uint32_t covered = 1, rounds = 0;
+    while (covered < w->max_depth) { covered *= 2; ++rounds; }
+    if (w->max_depth > 0 && rounds == 0) rounds = 1;
+    w->jump_rounds = rounds;
+    w->final_is_a = rounds % 2 == 0;
+    w->links_a.assign(B, Link<T>{});
+    w->links_b.assign(B, Link<T>{});
+    w->mdeltas.assign(6 * (size_t)B, 0u);
+    w->grad.assign(w->Q, T(0));
+    w->dgl.assign(w->Q, T(0));
+    w->pcg.assign(w->Q, typename World<T>::Pcg{});
     return w;
 }
 
@@ -993,9 +1621,10 @@ void or_set_coordinates(OrWorld* o, const GpuMechanismCoordinate* in) {
 
 void or_get_links(const OrWorld* o, GpuLinkState* out) {
     BOTH({
-        for (size_t i = 0; i < w->links.size(); ++i) {
-            put4(out[i].position, w->links[i].pos); put4(out[i].rotation, w->links[i].rot);
-            for (int k = 0; k < 4; ++k) out[i].metadata[k] = w->links[i].meta[k];
+        const auto& L = w->links_final_const();
+        for (size_t i = 0; i < L.size(); ++i) {
+            put4(out[i].position, L[i].pos); put4(out[i].rotation, L[i].rot);
+            for (int k = 0; k < 4; ++k) out[i].metadata[k] = L[i].meta[k];
         }
     });
 }

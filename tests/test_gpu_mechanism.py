@@ -1,0 +1,94 @@
+"""GPU parity of the articulated passes against the CPU oracle (through the C ABI).
+
+Forward kinematics, bearing projection, coordinate advance and capture,
+level-synchronous velocity reconstruction, validation and the loop-closure
+Newton/PCG steps follow the oracle's arithmetic order; closure systems with
+at most 512 coordinates also keep its summation order, so every case here is
+compared bit for bit (0 ULP).
+"""
+import numpy as np
+import pytest
+
+import oracle
+from mechanic_b200 import abi, scenes
+from mechanic_b200.physics import CoordinateStateCount, DriveStateCount, GpuPhysics, GpuPhysicsConfig
+
+pytestmark = pytest.mark.gpu
+
+
+def _same(a, b, what):
+    a, b = np.ascontiguousarray(a), np.ascontiguousarray(b)
+    assert a.shape == b.shape, what
+    if a.tobytes() != b.tobytes():
+        fa, fb = a.view(np.float32).reshape(len(a), -1), b.view(np.float32).reshape(len(b), -1)
+        bad = np.nonzero((fa.view(np.uint32) != fb.view(np.uint32)).any(axis=1))[0]
+        raise AssertionError(f"{what}: {len(bad)} rows differ, first {bad[:4]}: {fa[bad[:2]]} vs {fb[bad[:2]]}")
+
+
+def _pair(scene, cfg):
+    gpu = GpuPhysics(scene, cfg, capacities={"pair_capacity": 1 << 20})
+    orc = oracle.OracleWorld(scene, cfg.to_c(), precision=32, pair_capacity=1 << 20)
+    return gpu, orc
+
+
+def _compare(gpu, orc, tick, what):
+    gpu.dispatch_tick(tick)
+    rb = gpu.read_last_tick()
+    orc.step(tick)
+    d = orc.diagnostics()
+    assert rb.error_flags == int(d["error_flags"]), f"{what} tick {tick} flags"
+    assert round(rb.anchor_residual_meters * 1e6) == int(d["max_anchor_micrometers"])
+    assert round(rb.axis_residual_degrees * 1e6) == int(d["max_axis_microdegrees"])
+    st = gpu.save_state(manifold_capacity=0)
+    tr, vel = orc.state()
+    _same(st["transforms"], tr, f"{what} tick {tick} transforms")
+    _same(st["velocities"], vel, f"{what} tick {tick} velocities")
+    _same(st["coordinates"], orc.coordinates(), f"{what} tick {tick} coordinates")
+    return rb
+
+
+@pytest.mark.parametrize("invalid", [False, True])
+def test_four_bar_bitexact_and_gate(cuda_lib, invalid):
+    scene = scenes.four_bar(invalid)
+    cfg = GpuPhysicsConfig(collisions_enabled=False)
+    gpu, orc = _pair(scene, cfg)
+    coords = np.zeros(3, abi.MECHANISM_COORDINATE)
+    coords["angle"][0] = 0.001
+    gpu.initialize_mechanism_coordinates(coords)
+    orc.set_coordinates(coords)
+    flags = 0
+    for tick in range(1, 61):
+        flags |= _compare(gpu, orc, tick, "four_bar").error_flags
+    _same(gpu.links(), orc.links(), "final links")
+    if invalid:
+        assert flags & abi.CONSTRAINT_NON_CONVERGENCE_FLAG
+    else:
+        assert flags == 0
+
+
+def test_chains_with_closures_and_contacts_bitexact(cuda_lib):
+    scene = scenes.bearing_chains(chains=40, links=5, seed=1, closure_fraction=0.3, height=0.5)
+    gpu, orc = _pair(scene, GpuPhysicsConfig())
+    for tick in range(1, 31):
+        _compare(gpu, orc, tick, "chains")
+    assert np.array_equal(gpu.pairs(), orc.pairs())
+
+
+def test_chains_without_self_collisions_bitexact(cuda_lib):
+    scene = scenes.bearing_chains(chains=16, links=5, seed=3, closure_fraction=0.0, height=0.3)
+    gpu, orc = _pair(scene, GpuPhysicsConfig(mechanism_self_collisions=False))
+    for tick in range(1, 21):
+        _compare(gpu, orc, tick, "chains no self collision")
+
+
+def test_drive_and_coordinate_counts_are_checked(cuda_lib):
+    scene = scenes.bearing_chains(chains=4, links=5, seed=0)
+    gpu = GpuPhysics(scene)
+    with pytest.raises(DriveStateCount) as e:
+        gpu.write_mechanism_drives(abi.passive_drive_rows(3))
+    assert (e.value.provided, e.value.required) == (3, 16)
+    with pytest.raises(CoordinateStateCount):
+        gpu.initialize_mechanism_coordinates(np.zeros(15, abi.MECHANISM_COORDINATE))
+    gpu.write_mechanism_drives(abi.passive_drive_rows(16))
+    gpu.dispatch_tick(1)
+    assert gpu.read_last_tick().error_flags & abi.INVALID_NUMERIC_FLAG == 0
