@@ -255,8 +255,21 @@ typedef struct MkConfig {
     float linear_damping;                /* 0 => 0.999 */
     float angular_damping;               /* 0 => 0.98 */
     int32_t device;                      /* CUDA device ordinal */
-    uint32_t reserved;
+    uint32_t warm_start;                 /* MK_WARM_CACHED (default) or MK_WARM_LEARNED */
+    float contact_tolerance;             /* 0 (default): solver_iterations fixed passes (device.rs:1343-1416);
+                                            > 0: passes until ||r|| <= tolerance * ||r_cold|| (no reference
+                                            counterpart) */
+    uint32_t contact_max_iterations;     /* cap on passes when contact_tolerance > 0; 0 => 512 */
+    float closure_tolerance;             /* MK_CLOSURE_PCG_RESIDUAL: relative PCG residual; 0 => 1e-5 */
+    uint32_t closure_max_iterations;     /* MK_CLOSURE_PCG_RESIDUAL: PCG iterations per Newton step; 0 => 256 */
+    uint32_t preconditioner;             /* MK_PRECOND_BLOCK_JACOBI (default) or MK_PRECOND_LEARNED */
 } MkConfig;
+
+#define MK_WARM_CACHED          0u  /* collision.wgsl:774-839: cached impulse x 0.5 (x 1 for cylinder-ground) */
+#define MK_WARM_LEARNED         1u  /* warm-start network next to the cached start; the lower residual wins */
+
+#define MK_PRECOND_BLOCK_JACOBI 0u  /* inverse of 2 x 2 blocks of consecutive closure coordinates */
+#define MK_PRECOND_LEARNED      1u  /* block inverse corrected by the preconditioner network */
 
 #define MK_MORTON_63            0u  /* 21 bits/axis over [-512, 512) m, index tie-break through a stable sort */
 #define MK_MORTON_REFERENCE_30  1u  /* lbvh.wgsl:93-98: 10 bits/axis, 1 m cells */
@@ -302,6 +315,9 @@ typedef struct MkTickReadback {          /* GpuTickReadback (device.rs:73-92) */
     float axis_residual_degrees;
     uint32_t closure_iterations;         /* no reference counterpart: PCG iterations used by the closure solve */
     double closure_relative_residual;    /* no reference counterpart: final ||r||/||r0|| of the closure PCG */
+    uint32_t contact_iterations;         /* no reference counterpart: contact passes run (warm pass included) */
+    uint32_t warm_start_used;            /* MK_WARM_CACHED, MK_WARM_LEARNED, or 2: learned start rejected */
+    double contact_relative_residual;    /* no reference counterpart: last ||r|| / ||r_cold|| (residual mode) */
 } MkTickReadback;
 
 /* Device pointers of the live state (all borrowed, valid until mk_destroy). */

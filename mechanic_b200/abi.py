@@ -32,6 +32,11 @@ MORTON_63 = 0
 MORTON_REFERENCE_30 = 1
 CLOSURE_REFERENCE = 0
 CLOSURE_PCG_RESIDUAL = 1
+WARM_CACHED = 0
+WARM_LEARNED = 1
+WARM_LEARNED_REJECTED = 2
+PRECOND_BLOCK_JACOBI = 0
+PRECOND_LEARNED = 1
 
 # ---------------------------------------------------------------- numpy rows
 f4 = (np.float32, 4)
@@ -120,7 +125,10 @@ class MkConfig(C.Structure):
         ("closure_mode", C.c_uint32), ("use_graph", C.c_uint32),
         ("delta_seconds", C.c_float), ("gravity_y", C.c_float),
         ("linear_damping", C.c_float), ("angular_damping", C.c_float),
-        ("device", C.c_int32), ("reserved", C.c_uint32),
+        ("device", C.c_int32), ("warm_start", C.c_uint32),
+        ("contact_tolerance", C.c_float), ("contact_max_iterations", C.c_uint32),
+        ("closure_tolerance", C.c_float), ("closure_max_iterations", C.c_uint32),
+        ("preconditioner", C.c_uint32),
     ]
 
 
@@ -152,7 +160,8 @@ class MkTickReadback(C.Structure):
                 ("pair_count", C.c_uint32), ("contact_count", C.c_uint32),
                 ("active_contact_count", C.c_uint32), ("anchor_residual_meters", C.c_float),
                 ("axis_residual_degrees", C.c_float), ("closure_iterations", C.c_uint32),
-                ("closure_relative_residual", C.c_double)]
+                ("closure_relative_residual", C.c_double), ("contact_iterations", C.c_uint32),
+                ("warm_start_used", C.c_uint32), ("contact_relative_residual", C.c_double)]
 
 
 class MkDeviceState(C.Structure):

@@ -75,6 +75,8 @@ struct MkHandle {
     // host
     mk::DevTick* h_tick = nullptr;      // pinned ring
     GpuDiagnostics* h_diag = nullptr;   // pinned, written at the end of every tick
+    mk::SolveStats* h_stats = nullptr;  // pinned, contact solve outcome (residual mode)
+    bool residual = false;              // contact solve runs to a residual
     cudaEvent_t tick_done[kTickRing] = {};
     uint64_t tick_sub[kTickRing] = {};
     cudaEvent_t stage[kStageEvents] = {};
@@ -161,6 +163,16 @@ uint64_t carve(MkHandle* h, char* base) {
     b.sort_scratch_bytes = mk::sort_scratch_bytes(C, 63);
     b.sort_scratch = c.take<char>(b.sort_scratch_bytes);
     h->staging = c.take<float4>(2ull * B);
+    if (h->residual) {
+        b.deltas64 = c.take<int64_t>(12ull * B);
+        b.res2 = c.take<double>(2 * P);
+        b.res_chunk_cap = (uint32_t)(P / 1024 + 1);
+        b.res_chunks = c.take<double>(2ull * b.res_chunk_cap);
+        b.lam_alt = c.take<float>(P);
+        b.warm_pred = c.take<float>(P);
+        b.vel_res = c.take<float4>(8ull * B);
+        b.solve_stats = c.take<mk::SolveStats>(1);
+    }
     // mechanism buffers
     if (h->mechanism_active || h->J > 0) {
         mk::carve_mechanism(h->mech, h->mech_params, h->B, h->J, h->Q,
@@ -185,6 +197,7 @@ cudaError_t enqueue_tick(MkHandle* h, int parity, bool capturing) {
     cudaMemsetAsync(b.diag, 0, sizeof(GpuDiagnostics), s);
     cudaMemsetAsync(b.counts, 0, mk::kCountResetBytes, s);
     cudaMemsetAsync(b.tickets, 0, 16 * sizeof(uint32_t), s);
+    if (h->residual) cudaMemsetAsync(b.solve_stats, 0, sizeof(mk::SolveStats), s);
     if (h->collisions) {
         cudaMemsetAsync(b.visits, 0, sizeof(uint32_t) * std::max(h->C, 1u), s);
         cudaMemsetAsync(b.deltas, 0, sizeof(int32_t) * 6ull * std::max(h->B, 1u), s);
@@ -227,6 +240,7 @@ cudaError_t enqueue_tick(MkHandle* h, int parity, bool capturing) {
     if (!fuse && (e = mk::launch_snapshot(b, h->params, s)) != cudaSuccess) return e;
     if (h->collisions && (e = mk::launch_finish_tick(b, h->params, parity, s)) != cudaSuccess) return e;
     cudaMemcpyAsync(h->h_diag, b.diag, sizeof(GpuDiagnostics), cudaMemcpyDeviceToHost, s);
+    if (h->residual) cudaMemcpyAsync(h->h_stats, b.solve_stats, sizeof(mk::SolveStats), cudaMemcpyDeviceToHost, s);
     if ((e = mark(7)) != cudaSuccess) return e;
     return cudaGetLastError();
 }
@@ -294,6 +308,7 @@ void destroy_handle(MkHandle* h) {
     if (h->arena) cudaFree(h->arena);
     if (h->h_tick) cudaFreeHost(h->h_tick);
     if (h->h_diag) cudaFreeHost(h->h_diag);
+    if (h->h_stats) cudaFreeHost(h->h_stats);
     if (h->stream) cudaStreamDestroy(h->stream);
     delete h;
 }
@@ -406,6 +421,11 @@ int mk_create(const MkCreation* cr, const MkConfig* config, const MkCapacities* 
         while (shift < 31 && (1ull << shift) < (uint64_t)h->C) ++shift;
         h->params.pair_shift = shift;
     }
+    h->params.contact_tol = c.contact_tolerance > 0.0f ? c.contact_tolerance : 0.0f;
+    h->params.contact_max_iterations = c.contact_max_iterations ? c.contact_max_iterations : 512u;
+    // the interleaved bearing form (dynamic-root mechanisms) keeps the fixed passes
+    h->residual = h->params.contact_tol > 0.0f && !(cr->max_depth > 0 && cr->has_dynamic_root);
+    if (!h->residual) h->params.contact_tol = 0.0f;
     h->launch.sm_count = h->sm_count;
     h->launch.morton_mode = c.morton_mode;
     h->launch.iterations = std::max(1u, c.solver_iterations ? c.solver_iterations : 8u);
@@ -423,6 +443,7 @@ int mk_create(const MkCreation* cr, const MkConfig* config, const MkCapacities* 
     }
     ok = ok && check(cudaMallocHost(&h->h_tick, sizeof(mk::DevTick) * kTickRing), err, "pinned tick ring");
     ok = ok && check(cudaMallocHost(&h->h_diag, sizeof(GpuDiagnostics)), err, "pinned diagnostics");
+    ok = ok && check(cudaMallocHost(&h->h_stats, sizeof(mk::SolveStats)), err, "pinned solve stats");
     for (uint32_t i = 0; ok && i < kTickRing; ++i)
         ok = check(cudaEventCreateWithFlags(&h->tick_done[i], cudaEventDisableTiming), err, "event");
     for (uint32_t i = 0; ok && i < kStageEvents; ++i) ok = check(cudaEventCreate(&h->stage[i]), err, "event");
@@ -431,6 +452,7 @@ int mk_create(const MkCreation* cr, const MkConfig* config, const MkCapacities* 
         return MK_ERR_DEVICE_FAILURE;
     }
     std::memset(h->h_diag, 0, sizeof(GpuDiagnostics));
+    std::memset(h->h_stats, 0, sizeof(mk::SolveStats));
     // Upload rows (device.rs:429-523): transforms de-interleaved into SoA.
     mk::StepBuffers& b = h->buf;
     cudaStream_t s = h->stream;
@@ -571,6 +593,14 @@ int mk_read_last_tick(MkHandle* h, MkTickReadback* out) {
         out->gpu_tick_ms = total;
     }
     mk::read_mechanism_readback(h->mech, d, out);
+    if (h->residual) {
+        const mk::SolveStats st = *h->h_stats;
+        out->contact_iterations = st.iterations;
+        out->warm_start_used = h->launch.learned_warm ? (st.chosen ? MK_WARM_LEARNED : 2u) : MK_WARM_CACHED;
+        out->contact_relative_residual = st.s0 > 0.0 ? std::sqrt(st.sk / st.s0) : 0.0;
+    } else if (h->collisions && d.active_contact_count > 0) {
+        out->contact_iterations = h->launch.iterations;
+    }
     return MK_OK;
 }
 

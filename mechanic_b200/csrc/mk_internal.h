@@ -47,6 +47,17 @@ struct StepParams {
     float dt, gravity, lin_damp, ang_damp;
     uint32_t body_count, collider_count, pair_capacity, suppression_count;
     uint32_t pair_shift;       // bits of a collider index inside a pair key
+    float contact_tol;         // > 0: iterate the contact solve to ||r|| <= tol * ||r_cold||
+    uint32_t contact_max_iterations;
+};
+
+// Outcome of a contact solve run to a residual (written by the solver).
+struct SolveStats {
+    uint32_t iterations;       // solve + apply passes executed, the warm pass included
+    uint32_t chosen;           // 0: cached (reference) warm start, 1: learned warm start
+    uint32_t converged;
+    uint32_t pad;
+    double s0, sk;             // squared norms of the cold and of the last residual
 };
 
 // Launches implemented in mk_sort.cu.
@@ -99,6 +110,15 @@ struct StepBuffers {
     DevCounts* counts;
     void* sort_scratch;
     uint64_t sort_scratch_bytes;
+    // contact solve to a residual (null unless enabled at creation)
+    int64_t* deltas64;           // 2 candidates x 6 per body, fixed point x 2^32
+    double* res2;                // 2 candidates x pair_capacity squared residuals
+    double* res_chunks;          // 2 candidates x res_chunk_cap chunk sums
+    uint32_t res_chunk_cap;
+    float* lam_alt;              // learned candidate's normal impulse per active contact
+    float* warm_pred;            // learned warm-start impulse per active contact (network output)
+    float4* vel_res;             // 4 x {lin, ang} x body_count ping-pong velocities
+    SolveStats* solve_stats;
 };
 
 struct StepLaunch {
@@ -107,6 +127,7 @@ struct StepLaunch {
     uint32_t iterations;
     bool fuse_world_mass;     // no mechanism: integrate also writes world masses + snapshot
     bool collisions;
+    bool learned_warm;        // run the learned warm start next to the cached one
 };
 
 // mk_step.cu

@@ -959,6 +959,292 @@ __global__ void __launch_bounds__(kSolveThreads) k_solve_all(StepBuffers b, Step
     }
 }
 
+// ------------------------------------------------- contact solve to a residual
+// The reference runs a fixed number of relaxed-Jacobi passes.  This form
+// runs the same passes until the normal-row residual has fallen by
+// `contact_tol` relative to the cold residual (the residual of zero impulses
+// at the integrated velocities), or `contact_max_iterations` passes.  The
+// residual of a contact at the state entering a pass is the unrelaxed
+// projected step  r = max(prev + (-vn + bias)/D, 0) - prev  (the relaxed pass
+// moves the impulse by 0.125 r when no clamp is active).  Norms are FP64
+// sums in one fixed order (1024-element stride-halving trees over chunks of
+// the active list, then over the chunk sums), so every block reaches the same
+// stopping decision and repeated runs are bitwise identical.  Velocity
+// deltas use 64-bit fixed point (x 2^32): 2^20 quantises velocity to ~1e-6
+// m/s, about the size of the residual a 1e-5 relative tolerance asks for.
+//
+// With a learned warm start two candidates run side by side for the first
+// two passes (cached start in the contact rows, learned start in lam_alt);
+// the one with the smaller residual after its first pass continues, so the
+// cached start is the fallback whenever the learned one raises the initial
+// residual.
+constexpr uint32_t kResChunk = 1024;
+constexpr float kFixed64Scale = 4294967296.0f;        // 2^32
+constexpr float kFixed64Inverse = 2.3283064365386963e-10f;   // 2^-32
+
+__device__ __forceinline__ int64_t fixed_i64(float x) { return __float2ll_rn(x); }   // half-even, saturating
+
+__device__ __forceinline__ bool run_tail_sum64(uint32_t key, int64_t* v) {
+    const uint32_t lane = lane_id();
+    const uint32_t prev = __shfl_up_sync(0xffffffffu, key, 1);
+    const uint32_t next = __shfl_down_sync(0xffffffffu, key, 1);
+    const bool head = lane == 0 || prev != key;
+    const bool tail = lane == 31 || next != key;
+    const uint32_t heads = __ballot_sync(0xffffffffu, head);
+    const uint32_t below = heads & ((2u << lane) - 1u);
+    const uint32_t head_lane = 31u - __clz(below);
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+#pragma unroll
+        for (int c = 0; c < 6; ++c) {
+            const long long u = __shfl_up_sync(0xffffffffu, (long long)v[c], o);
+            if (lane >= head_lane + (uint32_t)o) v[c] = (int64_t)((uint64_t)v[c] + (uint64_t)u);
+        }
+    }
+    return tail;
+}
+
+// Sum of x[0..n) (n <= 1024, zero padded) by the stride-halving tree; all
+// 1024 threads of the block take part.
+__device__ __forceinline__ double tree1024(double mine, double* s) {
+    const uint32_t t = threadIdx.x;
+    __syncthreads();
+    s[t] = mine;
+#pragma unroll 1
+    for (uint32_t stride = kResChunk / 2; stride >= 1; stride >>= 1) {
+        __syncthreads();
+        if (t < stride) s[t] += s[t + stride];
+    }
+    __syncthreads();
+    const double r = s[0];
+    __syncthreads();
+    return r;
+}
+
+// canonical_sum of the n chunk sums (n <= 1024 * 1024), computed by one block.
+__device__ double canonical_sum(const double* chunks, uint32_t n, double* s_tree, double* s_top) {
+    const uint32_t t = threadIdx.x;
+    if (n <= kResChunk) return tree1024(t < n ? __ldcg(chunks + t) : 0.0, s_tree);
+    const uint32_t groups = (n + kResChunk - 1) / kResChunk;
+    for (uint32_t g = 0; g < groups; ++g) {
+        const uint64_t i = (uint64_t)g * kResChunk + t;
+        const double r = tree1024(i < n ? __ldcg(chunks + i) : 0.0, s_tree);
+        if (t == 0) s_top[g] = r;
+    }
+    __syncthreads();
+    return tree1024(t < groups ? s_top[t] : 0.0, s_tree);
+}
+
+struct ResCandidate {
+    const float4* sl;   // velocities entering the pass
+    const float4* sa;
+    float4* dl;         // velocities after it
+    float4* da;
+};
+
+__device__ __forceinline__ f3 contact_velocity_cg(const float4* vl, const float4* va, uint32_t body, f3 arm) {
+    return xyz(__ldcg(vl + body)) + cross(xyz(__ldcg(va + body)), arm);
+}
+
+// One pass for candidate `c` (0: impulses in the contact rows, 1: in lam_alt).
+__device__ __forceinline__ void solve_span_res(const StepBuffers& b, const StepParams& p, GpuContact* cur, uint32_t A,
+                                               bool warm, uint32_t c, const ResCandidate& v, bool write_res) {
+    const uint32_t stride = gridDim.x * blockDim.x;
+    int64_t* deltas = b.deltas64 + 6ull * p.body_count * c;
+    double* res2 = b.res2 + (uint64_t)p.pair_capacity * c;
+    for (uint32_t base = blockIdx.x * blockDim.x; base < A; base += stride) {
+        const uint32_t t = base + threadIdx.x;
+        bool live = false;
+        uint32_t a = kInvalid, bb = kInvalid;
+        float r = 0.0f;
+        int64_t da[6] = {0, 0, 0, 0, 0, 0}, db[6] = {0, 0, 0, 0, 0, 0};
+        if (t < A) {
+            const uint32_t k = __ldcg(b.active + t);
+            float4* row = reinterpret_cast<float4*>(cur + k);
+            const float4 r0 = __ldcg(row), np = __ldcg(row + 1), aa = __ldcg(row + 2), ab = __ldcg(row + 3);
+            a = __float_as_uint(r0.x);
+            bb = __float_as_uint(r0.y);
+            const f3 arm_a = xyz(aa), arm_b = xyz(ab);
+            const float4* wa = b.world_mass + 3ull * a;
+            const float4* wb = bb != kInvalid ? b.world_mass + 3ull * bb : nullptr;
+            f3 vb = mkf3(0, 0, 0);
+            if (bb != kInvalid) vb = contact_velocity_cg(v.sl, v.sa, bb, arm_b);
+            const f3 nrm = xyz(np);
+            const float den = impulse_denominator(wa, wb, arm_a, arm_b, nrm);
+            float lam = c == 0 ? aa.w : (warm ? __ldcg(b.warm_pred + t) : __ldcg(b.lam_alt + t));
+            if (!(den <= 0.0f)) {
+                const f3 rel = vb - contact_velocity_cg(v.sl, v.sa, a, arm_a);
+                const float vn = dot(rel, nrm);
+                if (np.w <= 1.0e-5f && vn >= -1.0e-5f && lam <= 1.0e-6f) {
+                    lam = 0.0f;
+                } else {
+                    const bool cyl = ab.w < 0.0f;
+                    const float recovery = cyl ? 1.0f : 0.2f;
+                    const float bias = mnf(mxf(np.w - 0.001f, 0.0f) * recovery / p.dt, 1.0f);
+                    float acc, delta;
+                    if (warm) {
+                        const float start = c == 0 ? aa.w * (cyl ? 1.0f : 0.5f) : lam;
+                        acc = mxf(start + 0.125f * (-vn + bias) / den, 0.0f);
+                        delta = acc;
+                        r = mxf((-vn + bias) / den, 0.0f);
+                    } else {
+                        const float prev = mxf(lam, 0.0f);
+                        acc = mxf(prev + 0.125f * (-vn + bias) / den, 0.0f);
+                        delta = acc - prev;
+                        r = mxf(prev + (-vn + bias) / den, 0.0f) - prev;
+                    }
+                    lam = acc;
+                    f3 imp = nrm * delta;
+                    const f3 tv = rel - nrm * vn;
+                    const float ts = length(tv);
+                    if (ts > 1.0e-6f) {
+                        const f3 tg = tv / ts;
+                        const float tden = impulse_denominator(wa, wb, arm_a, arm_b, tg);
+                        const float fr = mnf(ts / tden, (warm ? acc : fabsf(delta)) * 0.05f);
+                        imp = imp - tg * fr;
+                    }
+                    const f3 la = -imp * wa[0].w;
+                    const f3 ga = inverse_inertia(wa, cross(arm_a, -imp));
+                    da[0] = fixed_i64(la.x * kFixed64Scale); da[1] = fixed_i64(la.y * kFixed64Scale);
+                    da[2] = fixed_i64(la.z * kFixed64Scale); da[3] = fixed_i64(ga.x * kFixed64Scale);
+                    da[4] = fixed_i64(ga.y * kFixed64Scale); da[5] = fixed_i64(ga.z * kFixed64Scale);
+                    live = true;
+                    if (wb) {
+                        const f3 lb = imp * wb[0].w;
+                        const f3 gb = inverse_inertia(wb, cross(arm_b, imp));
+                        db[0] = fixed_i64(lb.x * kFixed64Scale); db[1] = fixed_i64(lb.y * kFixed64Scale);
+                        db[2] = fixed_i64(lb.z * kFixed64Scale); db[3] = fixed_i64(gb.x * kFixed64Scale);
+                        db[4] = fixed_i64(gb.y * kFixed64Scale); db[5] = fixed_i64(gb.z * kFixed64Scale);
+                    }
+                }
+            }
+            if (c == 0) row[2] = f4(arm_a, lam);
+            else b.lam_alt[t] = lam;
+            if (write_res) res2[t] = (double)r * (double)r;
+        }
+        const uint32_t key_a = live ? a : kInvalid;
+        const bool tail = run_tail_sum64(key_a, da);
+        if (tail && key_a != kInvalid) {
+            unsigned long long* d = reinterpret_cast<unsigned long long*>(deltas + 6ull * key_a);
+#pragma unroll
+            for (int q = 0; q < 6; ++q)
+                if (da[q]) atomicAdd(d + q, (unsigned long long)da[q]);
+        }
+        if (live && bb != kInvalid) {
+            unsigned long long* d = reinterpret_cast<unsigned long long*>(deltas + 6ull * bb);
+#pragma unroll
+            for (int q = 0; q < 6; ++q)
+                if (db[q]) atomicAdd(d + q, (unsigned long long)db[q]);
+        }
+    }
+}
+
+__device__ __forceinline__ void apply_span_res(const StepBuffers& b, const StepParams& p, uint32_t c,
+                                               const ResCandidate& v) {
+    const uint32_t stride = gridDim.x * blockDim.x;
+    longlong2* dl = reinterpret_cast<longlong2*>(b.deltas64 + 6ull * p.body_count * c);
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < p.body_count; i += stride) {
+        longlong2* d = dl + 3ull * i;
+        const longlong2 x0 = __ldcg(d), x1 = __ldcg(d + 1), x2 = __ldcg(d + 2);
+        if ((x0.x | x0.y | x1.x | x1.y | x2.x | x2.y) != 0) {
+            d[0] = make_longlong2(0, 0);
+            d[1] = make_longlong2(0, 0);
+            d[2] = make_longlong2(0, 0);
+        }
+        const f3 ld = mkf3(__ll2float_rn(x0.x), __ll2float_rn(x0.y), __ll2float_rn(x1.x)) * kFixed64Inverse;
+        const f3 ad = mkf3(__ll2float_rn(x1.y), __ll2float_rn(x2.x), __ll2float_rn(x2.y)) * kFixed64Inverse;
+        v.dl[i] = f4(xyz(__ldcg(v.sl + i)) + ld, 0.0f);
+        v.da[i] = f4(xyz(__ldcg(v.sa + i)) + ad, 0.0f);
+    }
+}
+
+__device__ __forceinline__ void chunk_sums(const StepBuffers& b, const StepParams& p, uint32_t A, uint32_t ncand,
+                                           uint32_t c_first, double* s_tree) {
+    const uint32_t chunks = (A + kResChunk - 1) / kResChunk;
+    for (uint32_t job = blockIdx.x; job < chunks * ncand; job += gridDim.x) {
+        const uint32_t c = c_first + job / chunks, ch = job % chunks;
+        const uint64_t i = (uint64_t)ch * kResChunk + threadIdx.x;
+        const double* res2 = b.res2 + (uint64_t)p.pair_capacity * c;
+        const double sum = tree1024(i < A ? __ldcg(res2 + i) : 0.0, s_tree);
+        if (threadIdx.x == 0) b.res_chunks[(uint64_t)b.res_chunk_cap * c + ch] = sum;
+    }
+}
+
+__global__ void __launch_bounds__(kSolveThreads) k_solve_residual(StepBuffers b, StepParams p, GpuContact* cur,
+                                                           uint32_t learned, uint32_t* barrier) {
+    __shared__ double s_tree[kResChunk];
+    __shared__ double s_top[kResChunk];
+    const uint32_t A = b.counts->active;
+    if (A == 0u) {
+        if (blockIdx.x == 0 && threadIdx.x == 0) *b.solve_stats = SolveStats{0u, 0u, 1u, 0u, 0.0, 0.0};
+        return;
+    }
+    const size_t B = p.body_count;
+    const double tol2 = (double)p.contact_tol * (double)p.contact_tol;
+    // candidate c ping-pongs between velocity pairs 2c and 2c + 1
+    const float4* src_l[2] = {b.lin, b.lin};
+    const float4* src_a[2] = {b.ang, b.ang};
+    uint32_t next_pair[2] = {0u, 2u};
+    bool dual = learned != 0u;
+    uint32_t chosen = 0;
+    double s0 = 0.0, sk = 0.0;
+    uint32_t it = 0, converged = 0;
+    const uint32_t max_it = p.contact_max_iterations;
+    while (it < max_it) {
+        const uint32_t c_first = dual ? 0u : chosen, c_last = dual ? 1u : chosen;
+        ResCandidate v[2];
+        for (uint32_t c = c_first; c <= c_last; ++c) {
+            const uint32_t q = next_pair[c];
+            v[c] = {src_l[c], src_a[c], b.vel_res + (2ull * q) * B, b.vel_res + (2ull * q + 1) * B};
+            // the cold residual (pass 0) is the same for both candidates
+            solve_span_res(b, p, cur, A, it == 0, c, v[c], !(it == 0 && c == 1));
+        }
+        grid_barrier(barrier, &b.diag->error_flags);
+        for (uint32_t c = c_first; c <= c_last; ++c) apply_span_res(b, p, c, v[c]);
+        const uint32_t nres = (it == 0) ? 1u : (c_last - c_first + 1);
+        chunk_sums(b, p, A, nres, c_first, s_tree);
+        grid_barrier(barrier, &b.diag->error_flags);
+        const uint32_t chunks = (A + kResChunk - 1) / kResChunk;
+        double S[2] = {0.0, 0.0};
+        for (uint32_t c = c_first; c < c_first + nres; ++c)
+            S[c] = canonical_sum(b.res_chunks + (uint64_t)b.res_chunk_cap * c, chunks, s_tree, s_top);
+        for (uint32_t c = c_first; c <= c_last; ++c) {
+            src_l[c] = v[c].dl;
+            src_a[c] = v[c].da;
+            next_pair[c] ^= 1u;
+        }
+        ++it;
+        if (it == 1) {
+            s0 = S[c_first];
+            sk = s0;
+            continue;
+        }
+        if (dual) {
+            chosen = S[1] <= S[0] ? 1u : 0u;
+            dual = false;
+        }
+        sk = S[chosen];
+        if (sk <= tol2 * s0) {
+            converged = 1;
+            break;
+        }
+    }
+    // final velocities (and the learned candidate's impulses) into place
+    const uint32_t gs = gridDim.x * blockDim.x;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < B; i += gs) {
+        b.lin[i] = __ldcg(src_l[chosen] + i);
+        b.ang[i] = __ldcg(src_a[chosen] + i);
+    }
+    if (chosen == 1u) {
+        for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < A; t += gs) {
+            float4* row = reinterpret_cast<float4*>(cur + __ldcg(b.active + t));
+            const float4 aa = __ldcg(row + 2);
+            row[2] = make_float4(aa.x, aa.y, aa.z, __ldcg(b.lam_alt + t));
+        }
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) *b.solve_stats = SolveStats{it, chosen, converged, 0u, s0, sk};
+}
+
 // Per-iteration kernels for ticks that interleave bearing projection with
 // the contact iterations (device.rs:1363-1416): velocities are updated in
 // place, so each phase is its own launch.
@@ -1178,7 +1464,16 @@ cudaError_t launch_contact_solver(const StepBuffers& b, const StepParams& p, con
     uint32_t* barrier = b.grid_barrier;
     StepBuffers bb = b;
     StepParams pp = p;
+    uint32_t learned = l.learned_warm ? 1u : 0u;
+    const bool residual = p.contact_tol > 0.0f;
+    if (residual) {
+        if (!b.deltas64 || !b.vel_res) return cudaErrorInvalidValue;
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_solve_residual, kSolveThreads, 0);
+        if (e != cudaSuccess) return e;
+        if (per_sm < 1) return cudaErrorInvalidConfiguration;
+    }
     void* args[] = {&bb, &pp, &cur, (void*)&iters, &barrier};
+    void* args_res[] = {&bb, &pp, &cur, (void*)&learned, &barrier};
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(blocks);
     cfg.blockDim = dim3(kSolveThreads);
@@ -1188,7 +1483,8 @@ cudaError_t launch_contact_solver(const StepBuffers& b, const StepParams& p, con
     attr[0].val.cooperative = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    e = cudaLaunchKernelExC(&cfg, (const void*)k_solve_all, args);
+    e = residual ? cudaLaunchKernelExC(&cfg, (const void*)k_solve_residual, args_res)
+                 : cudaLaunchKernelExC(&cfg, (const void*)k_solve_all, args);
     if (e != cudaSuccess) return e;
     return cudaGetLastError();
 }

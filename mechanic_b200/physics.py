@@ -134,6 +134,12 @@ class GpuPhysicsConfig:
     closure_mode: int = abi.CLOSURE_REFERENCE
     use_graph: bool = True
     device: int = 0
+    warm_start: int = abi.WARM_CACHED
+    contact_tolerance: float = 0.0          # > 0: contact passes until ||r|| <= tol * ||r_cold||
+    contact_max_iterations: int = 0         # 0 => 512
+    closure_tolerance: float = 0.0          # 0 => 1e-5 (CLOSURE_PCG_RESIDUAL)
+    closure_max_iterations: int = 0         # 0 => 256
+    preconditioner: int = abi.PRECOND_BLOCK_JACOBI
 
     def to_c(self) -> abi.MkConfig:
         c = abi.MkConfig()
@@ -145,6 +151,12 @@ class GpuPhysicsConfig:
         c.closure_mode = int(self.closure_mode)
         c.use_graph = int(self.use_graph)
         c.device = int(self.device)
+        c.warm_start = int(self.warm_start)
+        c.contact_tolerance = float(self.contact_tolerance)
+        c.contact_max_iterations = int(self.contact_max_iterations)
+        c.closure_tolerance = float(self.closure_tolerance)
+        c.closure_max_iterations = int(self.closure_max_iterations)
+        c.preconditioner = int(self.preconditioner)
         return c
 
 
@@ -178,6 +190,9 @@ class GpuTickReadback:
     axis_residual_degrees: float
     closure_iterations: int = 0
     closure_relative_residual: float = 0.0
+    contact_iterations: int = 0
+    warm_start_used: int = 0
+    contact_relative_residual: float = 0.0
 
 
 class GpuPhysics:
@@ -241,7 +256,8 @@ class GpuPhysics:
         return GpuTickReadback(out.gpu_tick_ms, timings, out.error_flags, out.pair_count, out.contact_count,
                                out.active_contact_count, out.anchor_residual_meters,
                                out.axis_residual_degrees, out.closure_iterations,
-                               out.closure_relative_residual)
+                               out.closure_relative_residual, out.contact_iterations,
+                               out.warm_start_used, out.contact_relative_residual)
 
     def read_snapshot_transforms(self, slot: int, out: np.ndarray | None = None) -> np.ndarray:
         rows = out if out is not None else np.zeros(self._body_count, abi.TRANSFORM)

@@ -59,6 +59,8 @@ def lib():
                      "or_get_coordinates", "or_set_coordinates", "or_get_links", "or_get_karras"):
             getattr(L, name).argtypes = [vp, vp]
         L.or_get_sorted.argtypes = [vp, vp, vp]
+        L.or_get_solve_stats.argtypes = [vp, vp, vp]
+        L.or_set_warm_predictions.argtypes = [vp, vp, u32]
         L.or_get_snapshot.argtypes = [vp, u32, vp]
         L.or_get_manifold.restype = u32
         L.or_get_manifold.argtypes = [vp, vp, u32]
@@ -148,6 +150,20 @@ class OracleWorld:
         d = np.zeros(1, abi.DIAGNOSTICS)
         lib().or_get_diagnostics(self.h, _p(d))
         return d[0]
+
+    def solve_stats(self) -> dict:
+        """Outcome of the last residual-mode contact solve."""
+        u = np.zeros(3, np.uint32)
+        d = np.zeros(2, np.float64)
+        lib().or_get_solve_stats(self.h, _p(u), _p(d))
+        return {"iterations": int(u[0]), "chosen": int(u[1]), "converged": int(u[2]),
+                "s0": float(d[0]), "sk": float(d[1]),
+                "relative_residual": float(np.sqrt(d[1] / d[0])) if d[0] > 0 else 0.0}
+
+    def set_warm_predictions(self, pred) -> None:
+        """Learned warm-start impulses, by active position, for the next step's solve."""
+        pred = np.ascontiguousarray(pred, np.float32)
+        lib().or_set_warm_predictions(self.h, _p(pred), len(pred))
 
     def pairs(self):
         out = np.zeros(self.pair_count, abi.PAIR)

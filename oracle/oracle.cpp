@@ -93,6 +93,15 @@ template <class T> static inline int32_t fixed_i32(T x) {
     if (r <= T(-2147483648.0)) return INT32_MIN;
     return (int32_t)r;
 }
+// i64(round(x)) for the 2^32 fixed point of the residual-mode solve: half to
+// even, saturating, NaN to 0 (cvt.rni.s64.f32).
+template <class T> static inline int64_t fixed_i64(T x) {
+    T r = std::nearbyint(x);
+    if (r != r) return 0;
+    if (r >= T(9223372036854775807.0)) return INT64_MAX;
+    if (r <= T(-9223372036854775808.0)) return INT64_MIN;
+    return (int64_t)r;
+}
 template <class T> static inline uint32_t round_u32(T x) {
     T r = std::nearbyint(x);
     if (!(r > T(0))) return 0;
@@ -720,6 +729,142 @@ template <class T> struct World : WorldBase {
             if (A > 0) solve_apply();
         }
     }
+    // ------------------------------------------- contact solve to a residual
+    // The fixed passes of solve() repeated until ||r_k|| <= tol * ||r_cold||
+    // (or max passes), with r the unrelaxed projected step of the normal row
+    // at the state entering a pass, FP64 norms summed in one fixed order
+    // (stride-halving trees of 1024 over chunks, then over chunk sums), and
+    // 64-bit fixed-point deltas (x 2^32).  With learned predictions two
+    // candidates (cached start, predicted start) run the first two passes;
+    // the smaller residual after the first pass continues.
+    float contact_tol = 0.0f;
+    uint32_t contact_max_it = 512;
+    std::vector<float> warm_predictions;   // by active position, consumed by the next solve
+    bool learned_pending = false;
+    struct SolveStats { uint32_t iterations = 0, chosen = 0, converged = 0; double s0 = 0, sk = 0; } stats;
+
+    static double tree1024(const double* v, size_t n) {
+        double t[1024];
+        for (size_t i = 0; i < 1024; ++i) t[i] = i < n ? v[i] : 0.0;
+        for (size_t stride = 512; stride >= 1; stride >>= 1)
+            for (size_t i = 0; i < stride; ++i) t[i] += t[i + stride];
+        return t[0];
+    }
+    static double canonical_norm2(const std::vector<double>& r2) {
+        std::vector<double> v;
+        for (size_t c = 0; c < r2.size(); c += 1024) v.push_back(tree1024(&r2[c], std::min<size_t>(1024, r2.size() - c)));
+        while (v.size() > 1) {
+            std::vector<double> u;
+            for (size_t c = 0; c < v.size(); c += 1024) u.push_back(tree1024(&v[c], std::min<size_t>(1024, v.size() - c)));
+            v.swap(u);
+        }
+        return v.empty() ? 0.0 : v[0];
+    }
+    void add_delta64(std::vector<uint64_t>& d64, uint32_t b, V3<T> l, V3<T> a) {
+        const T s = T(4294967296.0f);
+        uint64_t* d = &d64[6 * (size_t)b];
+        int64_t v[6] = {fixed_i64(l.x * s), fixed_i64(l.y * s), fixed_i64(l.z * s),
+                        fixed_i64(a.x * s), fixed_i64(a.y * s), fixed_i64(a.z * s)};
+        for (int k = 0; k < 6; ++k) {
+            std::atomic_ref<uint64_t> r(d[k]);
+            r.fetch_add((uint64_t)v[k], std::memory_order_relaxed);
+        }
+    }
+    // One contact of one candidate; returns the residual (0 when skipped).
+    T solve_contact_res(uint32_t t, bool warm, uint32_t cand, const std::vector<V4<T>>& vl,
+                        const std::vector<V4<T>>& va, std::vector<T>& lam_alt, std::vector<uint64_t>& d64) {
+        Contact<T>& c = contacts[active[t]];
+        uint32_t a = c.meta[0], b = c.meta[1];
+        V3<T> arm_a = xyz(c.aa), arm_b = xyz(c.ab);
+        auto vel = [&](uint32_t body, V3<T> arm) { return xyz(vl[body]) + cross(xyz(va[body]), arm); };
+        V3<T> vb = v3<T>(0, 0, 0);
+        if (b != INVALID) vb = vel(b, arm_b);
+        V3<T> n = xyz(c.np);
+        T den = impulse_denominator(a, b, arm_a, arm_b, n);
+        T& lam = cand == 0 ? c.aa.w : lam_alt[t];
+        if (warm && cand == 1) lam = T(warm_predictions[t]);
+        if (den <= T(0)) return T(0);
+        V3<T> rel = vb - vel(a, arm_a);
+        T vn = dot(rel, n);
+        if (c.np.w <= T(1.0e-5f) && vn >= T(-1.0e-5f) && lam <= T(1.0e-6f)) { lam = T(0); return T(0); }
+        bool cyl = c.ab.w < T(0);
+        T bias = penetration_bias(c.np.w, cyl);
+        T acc, delta, r;
+        if (warm) {
+            T start = cand == 0 ? c.aa.w * (cyl ? T(1) : T(0.5f)) : lam;
+            acc = mx(start + T(0.125f) * (-vn + bias) / den, T(0));
+            delta = acc;
+            r = mx((-vn + bias) / den, T(0));
+        } else {
+            T prev = mx(lam, T(0));
+            acc = mx(prev + T(0.125f) * (-vn + bias) / den, T(0));
+            delta = acc - prev;
+            r = mx(prev + (-vn + bias) / den, T(0)) - prev;
+        }
+        lam = acc;
+        V3<T> imp = n * delta;
+        V3<T> tv = rel - n * vn;
+        T ts = length(tv);
+        if (ts > T(1.0e-6f)) {
+            V3<T> tg = tv / ts;
+            T tden = impulse_denominator(a, b, arm_a, arm_b, tg);
+            T fr = mn(ts / tden, (warm ? acc : std::fabs(delta)) * T(0.05f));
+            imp = imp - tg * fr;
+        }
+        add_delta64(d64, a, -imp * wm[a].x.w, inverse_inertia(a, cross(arm_a, -imp)));
+        if (b != INVALID) add_delta64(d64, b, imp * wm[b].x.w, inverse_inertia(b, cross(arm_b, imp)));
+        return r;
+    }
+    void solve_residual() {
+        const uint32_t A = (uint32_t)active.size();
+        stats = SolveStats{};
+        const bool learned = learned_pending;
+        learned_pending = false;
+        if (A == 0) { stats.converged = 1; return; }
+        if (learned && warm_predictions.size() < A) warm_predictions.resize(A, 0.0f);
+        std::vector<V4<T>> vl[2] = {lin, lin}, va[2] = {ang, ang};
+        std::vector<T> lam_alt(A, T(0));
+        std::vector<uint64_t> d64[2] = {std::vector<uint64_t>(6ull * B, 0), std::vector<uint64_t>(6ull * B, 0)};
+        std::vector<double> r2[2] = {std::vector<double>(A, 0.0), std::vector<double>(A, 0.0)};
+        const double tol2 = (double)contact_tol * (double)contact_tol;
+        bool dual = learned;
+        uint32_t chosen = 0, it = 0;
+        double s0 = 0.0, sk = 0.0;
+        while (it < contact_max_it) {
+            const uint32_t c_first = dual ? 0u : chosen, c_last = dual ? 1u : chosen;
+            for (uint32_t c = c_first; c <= c_last; ++c) {
+                const bool warm = it == 0;
+#pragma omp parallel for schedule(static)
+                for (int64_t t = 0; t < (int64_t)A; ++t) {
+                    T r = solve_contact_res((uint32_t)t, warm, c, vl[c], va[c], lam_alt, d64[c]);
+                    if (!(warm && c == 1)) r2[c][t] = double(r) * double(r);
+                }
+                const T s = T(2.3283064365386963e-10f);
+#pragma omp parallel for schedule(static)
+                for (int64_t bb = 0; bb < (int64_t)B; ++bb) {
+                    uint64_t* d = &d64[c][6 * bb];
+                    V3<T> ld = v3<T>(T((int64_t)d[0]), T((int64_t)d[1]), T((int64_t)d[2])) * s;
+                    V3<T> ad = v3<T>(T((int64_t)d[3]), T((int64_t)d[4]), T((int64_t)d[5])) * s;
+                    for (int k = 0; k < 6; ++k) d[k] = 0;
+                    vl[c][bb] = v4(xyz(vl[c][bb]) + ld, T(0));
+                    va[c][bb] = v4(xyz(va[c][bb]) + ad, T(0));
+                }
+            }
+            double S[2] = {0.0, 0.0};
+            if (it == 0) S[c_first] = canonical_norm2(r2[c_first]);
+            else for (uint32_t c = c_first; c <= c_last; ++c) S[c] = canonical_norm2(r2[c]);
+            ++it;
+            if (it == 1) { s0 = S[c_first]; sk = s0; continue; }
+            if (dual) { chosen = S[1] <= S[0] ? 1u : 0u; dual = false; }
+            sk = S[chosen];
+            if (sk <= tol2 * s0) { stats.converged = 1; break; }
+        }
+        lin = vl[chosen]; ang = va[chosen];
+        if (chosen == 1)
+            for (uint32_t t = 0; t < A; ++t) contacts[active[t]].aa.w = lam_alt[t];
+        stats.iterations = it; stats.chosen = chosen; stats.s0 = s0; stats.sk = sk;
+    }
+
     // persist_contacts (collision.wgsl:1071-1088) + the prepare-time writes:
     // every acquired contact's manifold entry holds this tick's values.
     void persist() {
@@ -1304,6 +1449,11 @@ template <class T> struct World : WorldBase {
         const bool interleave = mechanism_active() && has_dynamic_root;
         const bool serial = serial_mechanism();
         const uint32_t A = (uint32_t)active.size();
+        if (contact_tol > 0.0f && !interleave) {
+            solve_residual();
+            persist();
+            return;
+        }
         // warm start + apply
 #pragma omp parallel for schedule(static)
         for (int64_t k = 0; k < (int64_t)A; ++k) solve_contact(active[k], true);
@@ -1375,6 +1525,8 @@ static World<T>* build_world(const MkCreation* cr, const MkConfig* cfg, uint32_t
     w->collisions = c.collisions_enabled;
     w->self_collisions = c.mechanism_self_collisions;
     w->pair_capacity = pair_capacity ? pair_capacity : MK_DEFAULT_MAX_CONTACT_PAIRS;
+    w->contact_tol = c.contact_tolerance > 0.0f ? c.contact_tolerance : 0.0f;
+    w->contact_max_it = c.contact_max_iterations ? c.contact_max_iterations : 512u;
     uint32_t B = w->B, C = w->C;
     w->pos.resize(B); w->rot.resize(B); w->lin.resize(B); w->ang.resize(B);
     w->inv_mass.resize(B); w->mass.resize(B); w->root.resize(B); w->components.resize(B);
@@ -1561,6 +1713,15 @@ void or_set_state(OrWorld* o, const GpuTransform* tr, const GpuVelocity* vel) {
 }
 
 void or_get_diagnostics(const OrWorld* o, GpuDiagnostics* out) { BOTH(*out = w->diag); }
+// Residual-mode solve outcome of the last step: iterations, chosen, converged, s0, sk.
+void or_get_solve_stats(const OrWorld* o, uint32_t* u3, double* d2) {
+    BOTH((u3[0] = w->stats.iterations, u3[1] = w->stats.chosen, u3[2] = w->stats.converged,
+          d2[0] = w->stats.s0, d2[1] = w->stats.sk));
+}
+// Learned warm-start impulses (by active position) for the next step's solve.
+void or_set_warm_predictions(OrWorld* o, const float* pred, uint32_t n) {
+    BOTH((w->warm_predictions.assign(pred, pred + n), w->learned_pending = true));
+}
 
 void or_get_pairs(const OrWorld* o, GpuPair* out) {
     BOTH({ for (size_t p = 0; p < w->pairs.size() / 2; ++p) { out[p].collider_a = w->pairs[2 * p]; out[p].collider_b = w->pairs[2 * p + 1]; } });
