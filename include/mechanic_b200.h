@@ -488,6 +488,33 @@ MK_API int mk_op_sort_keys_static(const uint64_t* keys_in, const uint32_t* value
 MK_API int mk_op_obb_sat(const float* boxes_a, const float* boxes_b, uint32_t count,
                   float* normal_penetration, uint32_t* features, void* stream);
 
+/* ---------------------------------------------------------------------
+ * The learned parts' network (no reference counterpart): 16 inputs (input
+ * slot 15 is replaced by the constant 1 that carries the first layer's
+ * bias), two hidden layers of 64 with ReLU, 16 outputs.  Parameters are one
+ * f32 device array of mk_mlp_param_count() floats, row-major [out][in]:
+ * W1 64x16 | W2 64x64 | W3 16x64 | b2 64 | b3 16.  The kernels compute with
+ * bf16 weights and activations on the tcgen05 tensor cores, f32 accumulation.
+ * All pointers are device pointers; x and targets rows are 16 floats,
+ * 16-byte aligned.  Waits inside the kernels are bounded: a timeout sets
+ * MK_DEVICE_WAIT_TIMEOUT_FLAG in *error_flags (device memory). */
+MK_API uint32_t mk_mlp_param_count(void);
+MK_API uint64_t mk_op_mlp_scratch_bytes(uint32_t max_samples);
+/* y[n][y_cols] = net(x[n][16]), 1 <= y_cols <= 16. */
+MK_API int mk_op_mlp_forward(const float* params, const float* x, uint32_t n, float* y, uint32_t y_cols,
+                             void* scratch, uint64_t scratch_bytes, uint32_t* error_flags, void* stream);
+/* Gradient of L = (1/n) sum_s sum_o out_weights[o] (y_so - targets_so)^2 with respect to the
+ * parameters, into grad[mk_mlp_param_count() + 1] (L in the last slot). */
+MK_API int mk_op_mlp_gradient(const float* params, const float* x, const float* targets,
+                              const float* out_weights, uint32_t n, float* grad, void* scratch,
+                              uint64_t scratch_bytes, uint32_t* error_flags, void* stream);
+/* `steps` Adam steps (beta 0.9 / 0.999, eps 1e-8) over consecutive batches of `batch` samples,
+ * cycling through the n samples; losses (device, optional) receives each step's batch loss. */
+MK_API int mk_op_mlp_train(float* params, float* adam_m, float* adam_v, const float* x, const float* targets,
+                           const float* out_weights, uint32_t n, uint32_t batch, uint32_t steps, float lr,
+                           uint32_t first_step, float* losses, void* scratch, uint64_t scratch_bytes,
+                           uint32_t* error_flags, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -25,6 +25,8 @@ EXPORTS = [
     "mk_state_buffers", "mk_save_state", "mk_load_state", "mk_read_buffer", "mk_version",
     "mk_last_error", "mk_op_sort_scratch_bytes", "mk_op_sort_keys", "mk_op_obb_sat",
     "mk_tick_kernel_count", "mk_set_tuning", "mk_op_sort_keys_static",
+    "mk_mlp_param_count", "mk_op_mlp_scratch_bytes", "mk_op_mlp_forward", "mk_op_mlp_gradient",
+    "mk_op_mlp_train",
 ]
 
 _lib = None
@@ -66,6 +68,11 @@ def library(path: str | None = None):
         "mk_tick_kernel_count": (u32, [vp]),
         "mk_set_tuning": (i32, [u32, u32]),
         "mk_op_sort_keys_static": (i32, [vp, vp, vp, vp, u32, u32, vp]),
+        "mk_mlp_param_count": (u32, []),
+        "mk_op_mlp_scratch_bytes": (u64, [u32]),
+        "mk_op_mlp_forward": (i32, [vp, vp, u32, vp, u32, vp, u64, vp, vp]),
+        "mk_op_mlp_gradient": (i32, [vp, vp, vp, vp, u32, vp, vp, u64, vp, vp]),
+        "mk_op_mlp_train": (i32, [vp, vp, vp, vp, vp, vp, u32, u32, u32, C.c_float, u32, vp, vp, u64, vp, vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
