@@ -359,6 +359,8 @@ enum {
     MK_BUF_CONTACT_FEATURES = 9,   /* uint32[contact_count]: SAT axis index 0..14 | near_face_axes << 8 */
     MK_BUF_WORLD_MASSES = 10,      /* float4 x 3 per body */
     MK_BUF_LINKS = 11,             /* GpuLinkState[body_count] final mechanism links */
+    MK_BUF_WARM_PREDICTIONS = 12,  /* float[active_count] learned warm-start impulses (MK_WARM_LEARNED) */
+    MK_BUF_WARM_FEATURES = 13,     /* float[active_count][16] warm-start network inputs (contact_tolerance > 0) */
 };
 
 /* ---------------------------------------------------------------------------
@@ -487,6 +489,23 @@ MK_API int mk_op_sort_keys_static(const uint64_t* keys_in, const uint32_t* value
  * and a feature word (axis index 0..14 | near_face_axes << 8 | early-exit bit 16). */
 MK_API int mk_op_obb_sat(const float* boxes_a, const float* boxes_b, uint32_t count,
                   float* normal_penetration, uint32_t* features, void* stream);
+
+/* Learned contact warm start (no reference counterpart).  With
+ * contact_tolerance > 0 every tick records 16 inputs per active contact at
+ * the start of the contact solve (relative normal velocity, tangential
+ * speed, depth rate, normal, inverse-mass share, cached impulse, bias,
+ * cylinder-ground and ground flags, cold step, log and value of the impulse
+ * denominator D); the network maps them to the converged impulse x D.
+ * mk_set_warm_start_network loads mk_mlp_param_count() parameters (host
+ * memory); with warm_start = MK_WARM_LEARNED the learned start then runs
+ * beside the cached one and the lower residual after one pass continues.
+ * mk_read_warm_start_samples copies the last tick's inputs (count x 16
+ * floats) and targets (the converged impulse x D, count floats) into host
+ * memory; *count receives the number of active contacts, of which at most
+ * capacity rows are written. */
+MK_API int mk_set_warm_start_network(MkHandle* handle, const float* params, uint32_t count, MkError* err);
+MK_API int mk_read_warm_start_samples(MkHandle* handle, float* features, float* targets, uint32_t capacity,
+                                      uint32_t* count, MkError* err);
 
 /* ---------------------------------------------------------------------
  * The learned parts' network (no reference counterpart): 16 inputs (input

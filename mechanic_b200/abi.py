@@ -203,6 +203,8 @@ BUF_COLLIDER_KEYS = 8
 BUF_CONTACT_FEATURES = 9
 BUF_WORLD_MASSES = 10
 BUF_LINKS = 11
+BUF_WARM_PREDICTIONS = 12
+BUF_WARM_FEATURES = 13
 
 
 def ptr(a: np.ndarray | None) -> int | None:

@@ -15,6 +15,7 @@
 #include "mk_device.cuh"
 #include "mk_internal.h"
 #include "mk_mechanism.h"
+#include "mk_mlp.h"
 
 namespace {
 
@@ -77,6 +78,9 @@ struct MkHandle {
     GpuDiagnostics* h_diag = nullptr;   // pinned, written at the end of every tick
     mk::SolveStats* h_stats = nullptr;  // pinned, contact solve outcome (residual mode)
     bool residual = false;              // contact solve runs to a residual
+    float* warm_params = nullptr;       // warm-start network parameters (device, mlp::kParams)
+    void* mlp_scratch = nullptr;        // bf16 weights + partials of the network kernels
+    uint64_t mlp_scratch_bytes = 0;
     cudaEvent_t tick_done[kTickRing] = {};
     uint64_t tick_sub[kTickRing] = {};
     cudaEvent_t stage[kStageEvents] = {};
@@ -170,6 +174,10 @@ uint64_t carve(MkHandle* h, char* base) {
         b.res_chunks = c.take<double>(2ull * b.res_chunk_cap);
         b.lam_alt = c.take<float>(P);
         b.warm_pred = c.take<float>(P);
+        b.warm_features = c.take<float4>(4 * P);
+        h->warm_params = c.take<float>(mk::mlp::kParams + 16);
+        h->mlp_scratch_bytes = mk::mlp::scratch_bytes(0);
+        h->mlp_scratch = c.take<char>(h->mlp_scratch_bytes);
         b.vel_res = c.take<float4>(8ull * B);
         b.solve_stats = c.take<mk::SolveStats>(1);
     }
@@ -224,7 +232,20 @@ cudaError_t enqueue_tick(MkHandle* h, int parity, bool capturing) {
                 cudaSuccess)
                 return e;
         } else {
-            if ((e = mk::launch_contact_solver(b, h->params, l, parity, s)) != cudaSuccess) return e;
+            std::function<cudaError_t()> warm;
+            if (h->residual) {
+                warm = [&]() -> cudaError_t {
+                    cudaError_t ew = mk::launch_warm_features(b, h->params, l, parity, s);
+                    if (ew != cudaSuccess || !l.learned_warm) return ew;
+                    // network output (one column) into lam_alt, which the solve overwrites later
+                    ew = mk::mlp::forward(h->warm_params, reinterpret_cast<const float*>(b.warm_features), 0,
+                                          &b.counts->active, h->pair_capacity, b.lam_alt, 1, h->mlp_scratch,
+                                          &b.diag->error_flags, s);
+                    if (ew != cudaSuccess) return ew;
+                    return mk::launch_warm_impulses(b, l, b.lam_alt, s);
+                };
+            }
+            if ((e = mk::launch_contact_solver(b, h->params, l, parity, s, warm)) != cudaSuccess) return e;
         }
         if (h->mechanism_active) {
             if ((e = mk::enqueue_post_contact(h->mech, b, h->mech_params, s)) != cudaSuccess) return e;
@@ -426,6 +447,7 @@ int mk_create(const MkCreation* cr, const MkConfig* config, const MkCapacities* 
     // the interleaved bearing form (dynamic-root mechanisms) keeps the fixed passes
     h->residual = h->params.contact_tol > 0.0f && !(cr->max_depth > 0 && cr->has_dynamic_root);
     if (!h->residual) h->params.contact_tol = 0.0f;
+    h->launch.learned_warm = h->residual && c.warm_start == MK_WARM_LEARNED;
     h->launch.sm_count = h->sm_count;
     h->launch.morton_mode = c.morton_mode;
     h->launch.iterations = std::max(1u, c.solver_iterations ? c.solver_iterations : 8u);
@@ -434,6 +456,7 @@ int mk_create(const MkCreation* cr, const MkConfig* config, const MkCapacities* 
     const mk::MechTopology topo = mk::derive_topology(cr, h->mech_params);
 
     bool ok = check(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking), err, "stream");
+    if (ok && h->residual) ok = check(mk::mlp::init(), err, "network kernel attributes");
     const uint64_t bytes = ok ? carve(h, nullptr) : 0;
     ok = ok && check(cudaMalloc(&h->arena, bytes), err, "device arena");
     if (ok) {
@@ -495,6 +518,7 @@ int mk_create(const MkCreation* cr, const MkConfig* config, const MkCapacities* 
         ok = ok && check(cudaMemcpyAsync(b.snap_rot + (size_t)slot * h->B, b.rot, 16ull * h->B,
                                          cudaMemcpyDeviceToDevice, s), err, "snapshot init");
     }
+    if (ok && h->residual) ok = check(mk::mlp::pack(h->warm_params, h->mlp_scratch, s), err, "pack network");
     ok = ok && check(cudaStreamSynchronize(s), err, "create sync");
     if (ok && h->config.use_graph) ok = build_graphs(h, err);
     if (!ok) {
@@ -602,6 +626,59 @@ int mk_read_last_tick(MkHandle* h, MkTickReadback* out) {
         out->contact_iterations = h->launch.iterations;
     }
     return MK_OK;
+}
+
+int mk_set_warm_start_network(MkHandle* h, const float* params, uint32_t count, MkError* err) {
+    if (err) std::memset(err, 0, sizeof(*err));
+    if (!h || !params) {
+        set_error(err, MK_ERR_INVALID_ARGUMENT, "handle and params must be non-null");
+        return MK_ERR_INVALID_ARGUMENT;
+    }
+    if (!h->residual) {
+        set_error(err, MK_ERR_INVALID_ARGUMENT, "the warm-start network needs contact_tolerance > 0");
+        return MK_ERR_INVALID_ARGUMENT;
+    }
+    if (count != mk::mlp::kParams) {
+        set_error(err, MK_ERR_INVALID_ARGUMENT, "network has %u parameters, %u given", mk::mlp::kParams, count);
+        if (err) err->required = mk::mlp::kParams, err->provided = count;
+        return MK_ERR_INVALID_ARGUMENT;
+    }
+    DeviceGuard guard(h->device);
+    cudaStream_t s = h->stream;
+    cudaError_t e = cudaMemcpyAsync(h->warm_params, params, sizeof(float) * count, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = mk::mlp::pack(h->warm_params, h->mlp_scratch, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    return check(e, err, "set_warm_start_network") ? MK_OK : MK_ERR_DEVICE_FAILURE;
+}
+
+int mk_read_warm_start_samples(MkHandle* h, float* features, float* targets, uint32_t capacity, uint32_t* count,
+                               MkError* err) {
+    if (err) std::memset(err, 0, sizeof(*err));
+    if (!h || !count) {
+        set_error(err, MK_ERR_INVALID_ARGUMENT, "handle and count must be non-null");
+        return MK_ERR_INVALID_ARGUMENT;
+    }
+    *count = 0;
+    if (!h->residual || !h->collisions) {
+        set_error(err, MK_ERR_INVALID_ARGUMENT, "warm-start samples need collisions and contact_tolerance > 0");
+        return MK_ERR_INVALID_ARGUMENT;
+    }
+    DeviceGuard guard(h->device);
+    cudaStream_t s = h->stream;
+    cudaError_t e = cudaStreamSynchronize(s);
+    if (!check(e, err, "read_warm_start_samples")) return MK_ERR_DEVICE_FAILURE;
+    const uint32_t A = h->any_tick ? h->h_diag->active_contact_count : 0u;
+    const uint32_t n = std::min(A, capacity);
+    *count = A;
+    if (n == 0 || !features || !targets) return MK_OK;
+    mk::StepBuffers& b = h->buf;
+    const int last = h->parity ^ 1;
+    e = mk::launch_warm_targets(b, last, n, b.warm_pred, s);   // warm_pred is free between ticks
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(features, b.warm_features, 64ull * n, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(targets, b.warm_pred, 4ull * n, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    return check(e, err, "read_warm_start_samples") ? MK_OK : MK_ERR_DEVICE_FAILURE;
 }
 
 int mk_read_snapshot(MkHandle* h, uint8_t slot, GpuTransform* out, uint32_t capacity, MkError* err) {
@@ -849,6 +926,8 @@ int mk_read_buffer(MkHandle* h, uint32_t id, void* host, uint64_t cap_bytes, uin
         case MK_BUF_CONTACT_FEATURES: src = b.features[last]; n = counts.contacts; row = 4; break;
         case MK_BUF_WORLD_MASSES: src = b.world_mass; n = h->B; row = 48; break;
         case MK_BUF_LINKS: src = h->mech.links_final; n = h->mech.links_final ? h->B : 0; row = 48; break;
+        case MK_BUF_WARM_PREDICTIONS: src = b.warm_pred; n = b.warm_pred ? counts.active : 0; row = 4; break;
+        case MK_BUF_WARM_FEATURES: src = b.warm_features; n = b.warm_features ? counts.active : 0; row = 64; break;
         default:
             set_error(err, MK_ERR_INVALID_ARGUMENT, "unknown buffer id %u", id);
             return MK_ERR_INVALID_ARGUMENT;

@@ -117,6 +117,7 @@ struct StepBuffers {
     uint32_t res_chunk_cap;
     float* lam_alt;              // learned candidate's normal impulse per active contact
     float* warm_pred;            // learned warm-start impulse per active contact (network output)
+    float4* warm_features;       // 4 x float4 network inputs per active contact
     float4* vel_res;             // 4 x {lin, ang} x body_count ping-pong velocities
     SolveStats* solve_stats;
 };
@@ -138,8 +139,12 @@ cudaError_t launch_broadphase(const StepBuffers& b, const StepParams& p, const S
                               cudaStream_t s);
 cudaError_t launch_narrowphase(const StepBuffers& b, const StepParams& p, const StepLaunch& l, int parity,
                                cudaStream_t s);
+cudaError_t launch_warm_features(const StepBuffers& b, const StepParams& p, const StepLaunch& l, int parity,
+                                 cudaStream_t s);
+cudaError_t launch_warm_impulses(const StepBuffers& b, const StepLaunch& l, const float* y, cudaStream_t s);
+cudaError_t launch_warm_targets(const StepBuffers& b, int parity, uint32_t A, float* targets, cudaStream_t s);
 cudaError_t launch_contact_solver(const StepBuffers& b, const StepParams& p, const StepLaunch& l, int parity,
-                                  cudaStream_t s);
+                                  cudaStream_t s, const std::function<cudaError_t()>& before_solve = nullptr);
 cudaError_t launch_finish_tick(const StepBuffers& b, const StepParams& p, int parity, cudaStream_t s);
 // Contact iterations as separate launches with a hook after each velocity
 // apply (bearing projection of mechanisms with a dynamic root).

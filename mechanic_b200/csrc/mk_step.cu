@@ -1245,6 +1245,87 @@ __global__ void __launch_bounds__(kSolveThreads) k_solve_residual(StepBuffers b,
     if (blockIdx.x == 0 && threadIdx.x == 0) *b.solve_stats = SolveStats{it, chosen, converged, 0u, s0, sk};
 }
 
+// ------------------------------------------------------ learned warm start
+// Per-contact inputs of the warm-start network, taken at the state the
+// contact solve starts from (integrated velocities, this tick's contact
+// rows), in velocity units so that mass drops out:
+//   0 vn   1 tangential speed   2 depth / dt   3-5 normal
+//   6 inverse-mass share of body A   7 cached impulse x D   8 bias
+//   9 cylinder-ground   10 ground   11 max(-vn + bias, 0)   12 log D
+//   13 cached impulse present   14 D   15 (constant 1, set by the network)
+// with D the impulse denominator along the normal (inverse effective mass).
+// The network predicts the converged impulse x D; impulse = max(y, 0) / D.
+__global__ void __launch_bounds__(kBlock) k_warm_features(StepBuffers b, StepParams p, const GpuContact* cur,
+                                                          float4* features) {
+    const uint32_t A = b.counts->active;
+    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < A; t += gridDim.x * blockDim.x) {
+        const uint32_t k = b.active[t];
+        const float4* row = reinterpret_cast<const float4*>(cur + k);
+        const float4 r0 = row[0], np = row[1], aa = row[2], ab = row[3];
+        const uint32_t a = __float_as_uint(r0.x), bb = __float_as_uint(r0.y);
+        const f3 arm_a = xyz(aa), arm_b = xyz(ab);
+        const float4* wa = b.world_mass + 3ull * a;
+        const float4* wb = bb != kInvalid ? b.world_mass + 3ull * bb : nullptr;
+        const f3 nrm = xyz(np);
+        const float den = impulse_denominator(wa, wb, arm_a, arm_b, nrm);
+        float4 f[4] = {make_float4(0, 0, 0, 0), make_float4(0, 0, 0, 0), make_float4(0, 0, 0, 0),
+                       make_float4(0, 0, 0, 0)};
+        if (den > 0.0f) {
+            f3 vb = mkf3(0, 0, 0);
+            if (bb != kInvalid) vb = xyz(b.lin[bb]) + cross(xyz(b.ang[bb]), arm_b);
+            const f3 rel = vb - (xyz(b.lin[a]) + cross(xyz(b.ang[a]), arm_a));
+            const float vn = dot(rel, nrm);
+            const float ts = length(rel - nrm * vn);
+            const bool cyl = ab.w < 0.0f;
+            const float bias = mnf(mxf(np.w - 0.001f, 0.0f) * (cyl ? 1.0f : 0.2f) / p.dt, 1.0f);
+            const float inv_a = wa[0].w, inv_b = wb ? wb[0].w : 0.0f;
+            f[0] = make_float4(vn, ts, np.w / p.dt, nrm.x);
+            f[1] = make_float4(nrm.y, nrm.z, inv_a / (inv_a + inv_b), aa.w * den);
+            f[2] = make_float4(bias, cyl ? 1.0f : 0.0f, bb == kInvalid ? 1.0f : 0.0f, mxf(-vn + bias, 0.0f));
+            f[3] = make_float4(logf(den), aa.w > 0.0f ? 1.0f : 0.0f, den, 1.0f);
+        }
+        float4* out = features + 4ull * t;
+        out[0] = f[0]; out[1] = f[1]; out[2] = f[2]; out[3] = f[3];
+    }
+}
+
+// network output (one column) -> warm-start impulse
+__global__ void __launch_bounds__(kBlock) k_warm_impulses(StepBuffers b, const float4* features, const float* y,
+                                                          float* warm) {
+    const uint32_t A = b.counts->active;
+    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < A; t += gridDim.x * blockDim.x) {
+        const float den = features[4ull * t + 3].z;
+        const float v = y[t];
+        warm[t] = (den > 0.0f && v > 0.0f) ? v / den : 0.0f;   // NaN outputs give 0
+    }
+}
+
+// training targets of the last tick: converged impulse x D per active contact
+__global__ void __launch_bounds__(kBlock) k_warm_targets(StepBuffers b, const GpuContact* cur, const float4* features,
+                                                         uint32_t A, float* targets) {
+    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < A; t += gridDim.x * blockDim.x) {
+        const float lam = reinterpret_cast<const float4*>(cur + b.active[t])[2].w;
+        targets[t] = lam * features[4ull * t + 3].z;
+    }
+}
+
+cudaError_t launch_warm_features(const StepBuffers& b, const StepParams& p, const StepLaunch& l, int parity,
+                                 cudaStream_t s) {
+    k_warm_features<<<(uint32_t)l.sm_count * 8, kBlock, 0, s>>>(b, p, b.contacts[parity], b.warm_features);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_warm_impulses(const StepBuffers& b, const StepLaunch& l, const float* y, cudaStream_t s) {
+    k_warm_impulses<<<(uint32_t)l.sm_count * 8, kBlock, 0, s>>>(b, b.warm_features, y, b.warm_pred);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_warm_targets(const StepBuffers& b, int parity, uint32_t A, float* targets, cudaStream_t s) {
+    if (A == 0) return cudaSuccess;
+    k_warm_targets<<<(A + kBlock - 1) / kBlock, kBlock, 0, s>>>(b, b.contacts[parity], b.warm_features, A, targets);
+    return cudaGetLastError();
+}
+
 // Per-iteration kernels for ticks that interleave bearing projection with
 // the contact iterations (device.rs:1363-1416): velocities are updated in
 // place, so each phase is its own launch.
@@ -1447,12 +1528,16 @@ cudaError_t launch_narrowphase(const StepBuffers& b, const StepParams& p, const 
 }
 
 cudaError_t launch_contact_solver(const StepBuffers& b, const StepParams& p, const StepLaunch& l, int parity,
-                                  cudaStream_t s) {
+                                  cudaStream_t s, const std::function<cudaError_t()>& before_solve) {
     const uint32_t grid = (uint32_t)l.sm_count * 8;
     AppendSite prep{b.lookback + 3 * b.lookback_words, b.tickets + 3};
     const int prev = parity ^ 1;
     k_prepare<<<grid, kBlock, 0, s>>>(b, p, prep, b.contacts[parity], b.contact_keys[parity], b.features[parity],
                                        b.contacts[prev], b.contact_keys[prev], b.features[prev]);
+    if (before_solve) {
+        cudaError_t eb = before_solve();
+        if (eb != cudaSuccess) return eb;
+    }
     // one co-resident grid for every iteration (cooperative launch)
     int per_sm = 0;
     cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_solve_all, kSolveThreads, 0);

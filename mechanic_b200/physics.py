@@ -26,7 +26,7 @@ EXPORTS = [
     "mk_last_error", "mk_op_sort_scratch_bytes", "mk_op_sort_keys", "mk_op_obb_sat",
     "mk_tick_kernel_count", "mk_set_tuning", "mk_op_sort_keys_static",
     "mk_mlp_param_count", "mk_op_mlp_scratch_bytes", "mk_op_mlp_forward", "mk_op_mlp_gradient",
-    "mk_op_mlp_train",
+    "mk_op_mlp_train", "mk_set_warm_start_network", "mk_read_warm_start_samples",
 ]
 
 _lib = None
@@ -73,6 +73,8 @@ def library(path: str | None = None):
         "mk_op_mlp_forward": (i32, [vp, vp, u32, vp, u32, vp, u64, vp, vp]),
         "mk_op_mlp_gradient": (i32, [vp, vp, vp, vp, u32, vp, vp, u64, vp, vp]),
         "mk_op_mlp_train": (i32, [vp, vp, vp, vp, vp, vp, u32, u32, u32, C.c_float, u32, vp, vp, u64, vp, vp]),
+        "mk_set_warm_start_network": (i32, [vp, vp, u32, vp]),
+        "mk_read_warm_start_samples": (i32, [vp, vp, vp, u32, vp, vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -360,6 +362,24 @@ class GpuPhysics:
                                         C.byref(err)), err)
         return raw[: n * row_bytes].view(dtype)
 
+    def set_warm_start_network(self, params: np.ndarray) -> None:
+        """Loads the warm-start network (MK_WARM_LEARNED uses it from the next tick on)."""
+        p = np.ascontiguousarray(params, np.float32)
+        err = abi.MkError()
+        _raise(library().mk_set_warm_start_network(self._h, p.ctypes.data, len(p), C.byref(err)), err)
+
+    def warm_start_samples(self):
+        """(inputs (n, 16), targets (n,)) of the last tick's active contacts."""
+        count = C.c_uint32()
+        err = abi.MkError()
+        _raise(library().mk_read_warm_start_samples(self._h, None, None, 0, C.byref(count), C.byref(err)), err)
+        n = int(count.value)
+        feats = np.zeros((max(n, 1), 16), np.float32)
+        targ = np.zeros(max(n, 1), np.float32)
+        _raise(library().mk_read_warm_start_samples(self._h, feats.ctypes.data, targ.ctypes.data, n, C.byref(count),
+                                                     C.byref(err)), err)
+        return feats[:n], targ[:n]
+
     # convenience views of internal buffers (last completed tick)
     def pairs(self):
         return self.read_buffer(abi.BUF_PAIRS, abi.PAIR, 8)
@@ -391,6 +411,9 @@ class GpuPhysics:
 
     def links(self):
         return self.read_buffer(abi.BUF_LINKS, abi.LINK_STATE, 48)
+
+    def warm_predictions(self):
+        return self.read_buffer(abi.BUF_WARM_PREDICTIONS, np.float32, 4)
 
 
 TUNE_SORT_ITEMS = 1

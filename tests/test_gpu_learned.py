@@ -1,0 +1,97 @@
+"""Learned warm start through the C ABI (no reference counterpart).
+
+Parity: the contact solve with a learned start must equal the oracle's bit
+for bit when the oracle is given the same network outputs (the network runs
+on the tensor cores, whose f32 summation order the oracle does not model, so
+its outputs are the one input taken from the GPU).  Benefit: from identical
+states, a network trained on the plain solve's converged impulses needs
+fewer passes in total than the cached start to reach the same residual.
+"""
+import numpy as np
+import pytest
+
+import oracle
+from mechanic_b200 import abi, learned, scenes
+from mechanic_b200.net_init import init_params
+from mechanic_b200.physics import GpuPhysics
+
+from test_gpu_parity import assert_bitwise
+
+pytestmark = pytest.mark.gpu
+
+
+def test_learned_start_bitexact_given_network_outputs(cuda_lib):
+    scene = scenes.falling_cubes(1000, seed=0)
+    cfg = learned.residual_config(learned=True)
+    gpu = GpuPhysics(scene, cfg, capacities={"pair_capacity": 1 << 20})
+    gpu.set_warm_start_network(init_params(5, out_scale=1.0))
+    orc = oracle.OracleWorld(scene, cfg.to_c(), pair_capacity=1 << 20)
+    used = set()
+    for tick in range(1, 41):
+        gpu.dispatch_tick(tick)
+        rb = gpu.read_last_tick()
+        pred = gpu.warm_predictions()
+        assert len(pred) == rb.active_contact_count
+        assert np.all(np.isfinite(pred)) and np.all(pred >= 0)
+        orc.set_warm_predictions(pred)
+        orc.step(tick)
+        st = orc.solve_stats()
+        assert rb.contact_iterations == st["iterations"], f"tick {tick}"
+        if rb.active_contact_count:
+            assert rb.warm_start_used == (abi.WARM_LEARNED if st["chosen"] else abi.WARM_LEARNED_REJECTED)
+            used.add(rb.warm_start_used)
+        s = gpu.save_state(manifold_capacity=0)
+        tr, vel = orc.state()
+        assert_bitwise(s["transforms"], tr, f"tick {tick} transforms")
+        assert_bitwise(s["velocities"], vel, f"tick {tick} velocities")
+        assert_bitwise(gpu.contacts(), orc.contacts(), f"tick {tick} contacts")
+    assert used, "no tick had active contacts"
+
+
+def test_samples_match_the_recorded_inputs(cuda_lib):
+    scene = scenes.falling_cubes(500, seed=2)
+    with GpuPhysics(scene, learned.residual_config()) as gpu:
+        for tick in range(1, 31):
+            gpu.dispatch_tick(tick)
+        rb = gpu.read_last_tick()
+        x, y = gpu.warm_start_samples()
+        assert x.shape == (rb.active_contact_count, 16) and y.shape == (rb.active_contact_count,)
+        c = gpu.contacts()
+        act = gpu.active()
+        lam = c["arm_a_impulse"][act, 3]
+        np.testing.assert_array_equal(y, (lam * x[:, 14]).astype(np.float32))
+        assert np.all(x[:, 15] == 1.0)
+
+
+def _replay_passes(scene, params, ticks):
+    """Passes per tick of the cached and of the learned start, each tick taken from the
+    same state of one cached-start trajectory."""
+    cfg_plain = learned.residual_config()
+    cfg_learned = learned.residual_config(learned=True)
+    caps = {"pair_capacity": 1 << 20}
+    plain, learned_h = [], []
+    with GpuPhysics(scene, cfg_plain, capacities=caps) as ref, \
+            GpuPhysics(scene, cfg_plain, capacities=caps) as a, \
+            GpuPhysics(scene, cfg_learned, capacities=caps) as b:
+        b.set_warm_start_network(params)
+        for tick in range(1, ticks + 1):
+            st = ref.save_state()
+            for h, out in ((a, plain), (b, learned_h)):
+                h.load_state(st["transforms"], st["velocities"], manifold=st["manifold"],
+                             manifold_tick=st["manifold_tick"])
+                h.dispatch_tick(tick)
+                out.append(h.read_last_tick().contact_iterations)
+            ref.dispatch_tick(tick)
+    return np.asarray(plain), np.asarray(learned_h)
+
+
+def test_trained_warm_start_saves_passes(cuda_lib):
+    xs, ys = [], []
+    for seed in range(3):
+        x, y, _ = learned.collect_samples(scenes.falling_cubes(1000, seed=seed), 60)
+        xs.append(x)
+        ys.append(y)
+    params, losses = learned.train(np.concatenate(xs), np.concatenate(ys), steps=2000, batch=8192, lr=2e-3)
+    assert losses[-50:].mean() < 0.5 * losses[:50].mean()
+    plain, learn = _replay_passes(scenes.falling_cubes(1000, seed=7), params, 60)
+    assert learn.sum() < plain.sum(), (plain.sum(), learn.sum())
