@@ -268,8 +268,9 @@ typedef struct MkConfig {
 #define MK_WARM_CACHED          0u  /* collision.wgsl:774-839: cached impulse x 0.5 (x 1 for cylinder-ground) */
 #define MK_WARM_LEARNED         1u  /* warm-start network next to the cached start; the lower residual wins */
 
-#define MK_PRECOND_BLOCK_JACOBI 0u  /* inverse of 2 x 2 blocks of consecutive closure coordinates */
-#define MK_PRECOND_LEARNED      1u  /* block inverse corrected by the preconditioner network */
+#define MK_PRECOND_BLOCK_JACOBI 0u  /* per-closure-loop blocks: Cholesky of J^T J on each loop's coordinates */
+#define MK_PRECOND_LEARNED      1u  /* 2 x 2 blocks of consecutive closure coordinates, inverse from the network */
+#define MK_PRECOND_PAIR_BLOCKS  2u  /* 2 x 2 blocks, exact 2 x 2 inverse (the learned form's own baseline) */
 
 #define MK_MORTON_63            0u  /* 21 bits/axis over [-512, 512) m, index tie-break through a stable sort */
 #define MK_MORTON_REFERENCE_30  1u  /* lbvh.wgsl:93-98: 10 bits/axis, 1 m cells */
@@ -361,6 +362,10 @@ enum {
     MK_BUF_LINKS = 11,             /* GpuLinkState[body_count] final mechanism links */
     MK_BUF_WARM_PREDICTIONS = 12,  /* float[active_count] learned warm-start impulses (MK_WARM_LEARNED) */
     MK_BUF_WARM_FEATURES = 13,     /* float[active_count][16] warm-start network inputs (contact_tolerance > 0) */
+    MK_BUF_CLOSURE_SLOTS = 14,     /* MK_CLOSURE_PCG_RESIDUAL, last evaluated Newton step, per closure-branch joint:
+                                      {position column xyz, coordinate (u32 bits)}, {axis column xyz, closure (u32)} */
+    MK_BUF_CLOSURE_BLOCKS = 15,    /* float[blocks][16] preconditioner network inputs of the same step */
+    MK_BUF_CLOSURE_BLOCK_OUTPUTS = 16, /* float[12][blocks][3] (t11, t12, t22) the network gave at each Newton step */
 };
 
 /* ---------------------------------------------------------------------------
@@ -506,6 +511,18 @@ MK_API int mk_op_obb_sat(const float* boxes_a, const float* boxes_b, uint32_t co
 MK_API int mk_set_warm_start_network(MkHandle* handle, const float* params, uint32_t count, MkError* err);
 MK_API int mk_read_warm_start_samples(MkHandle* handle, float* features, float* targets, uint32_t capacity,
                                       uint32_t* count, MkError* err);
+
+/* Learned closure preconditioner (no reference counterpart).  With
+ * closure_mode = MK_CLOSURE_PCG_RESIDUAL and preconditioner = MK_PRECOND_LEARNED
+ * the network maps 16 inputs per 2 x 2 block of consecutive closure
+ * coordinates (normalised coupling, log diagonal ratio, off-block row sums
+ * of J^T J against ones and alternating signs, pair flag) to (y0, y1, y2),
+ * the block of S M^-1 S (S = diag(sqrt(diag(J^T J)))) being t11 = e^y0,
+ * t22 = e^y1, t12 = 0.999 tanh(y2) sqrt(t11 t22), positive definite by
+ * construction; a block whose output is not finite keeps the plain 2 x 2
+ * inverse.  MK_BUF_CLOSURE_BLOCK_OUTPUTS holds the (t11, t12, t22) used.
+ * Loads mk_mlp_param_count() parameters from host memory. */
+MK_API int mk_set_preconditioner_network(MkHandle* handle, const float* params, uint32_t count, MkError* err);
 
 /* ---------------------------------------------------------------------
  * The learned parts' network (no reference counterpart): 16 inputs (input

@@ -37,6 +37,7 @@ WARM_LEARNED = 1
 WARM_LEARNED_REJECTED = 2
 PRECOND_BLOCK_JACOBI = 0
 PRECOND_LEARNED = 1
+PRECOND_PAIR_BLOCKS = 2
 
 # ---------------------------------------------------------------- numpy rows
 f4 = (np.float32, 4)
@@ -205,6 +206,9 @@ BUF_WORLD_MASSES = 10
 BUF_LINKS = 11
 BUF_WARM_PREDICTIONS = 12
 BUF_WARM_FEATURES = 13
+BUF_CLOSURE_SLOTS = 14
+BUF_CLOSURE_BLOCKS = 15
+BUF_CLOSURE_BLOCK_OUTPUTS = 16
 
 
 def ptr(a: np.ndarray | None) -> int | None:

@@ -77,6 +77,7 @@ struct MkHandle {
     mk::DevTick* h_tick = nullptr;      // pinned ring
     GpuDiagnostics* h_diag = nullptr;   // pinned, written at the end of every tick
     mk::SolveStats* h_stats = nullptr;  // pinned, contact solve outcome (residual mode)
+    mk::ClosureState* h_cstate = nullptr;   // pinned, closure solve outcome (MK_CLOSURE_PCG_RESIDUAL)
     bool residual = false;              // contact solve runs to a residual
     float* warm_params = nullptr;       // warm-start network parameters (device, mlp::kParams)
     void* mlp_scratch = nullptr;        // bf16 weights + partials of the network kernels
@@ -262,6 +263,8 @@ cudaError_t enqueue_tick(MkHandle* h, int parity, bool capturing) {
     if (h->collisions && (e = mk::launch_finish_tick(b, h->params, parity, s)) != cudaSuccess) return e;
     cudaMemcpyAsync(h->h_diag, b.diag, sizeof(GpuDiagnostics), cudaMemcpyDeviceToHost, s);
     if (h->residual) cudaMemcpyAsync(h->h_stats, b.solve_stats, sizeof(mk::SolveStats), cudaMemcpyDeviceToHost, s);
+    if (h->mechanism_active && mk::pcg_residual_mode(h->mech_params))
+        cudaMemcpyAsync(h->h_cstate, h->mech.cstate, sizeof(mk::ClosureState), cudaMemcpyDeviceToHost, s);
     if ((e = mark(7)) != cudaSuccess) return e;
     return cudaGetLastError();
 }
@@ -330,6 +333,7 @@ void destroy_handle(MkHandle* h) {
     if (h->h_tick) cudaFreeHost(h->h_tick);
     if (h->h_diag) cudaFreeHost(h->h_diag);
     if (h->h_stats) cudaFreeHost(h->h_stats);
+    if (h->h_cstate) cudaFreeHost(h->h_cstate);
     if (h->stream) cudaStreamDestroy(h->stream);
     delete h;
 }
@@ -452,11 +456,13 @@ int mk_create(const MkCreation* cr, const MkConfig* config, const MkCapacities* 
     h->launch.morton_mode = c.morton_mode;
     h->launch.iterations = std::max(1u, c.solver_iterations ? c.solver_iterations : 8u);
     h->launch.collisions = h->collisions;
-    h->mech_params = mk::make_mech_params(cr, h->params, h->launch.iterations, c.closure_mode);
+    h->mech_params = mk::make_mech_params(cr, h->params, h->launch.iterations, c.closure_mode, c.closure_tolerance,
+                                          c.closure_max_iterations, c.preconditioner);
     const mk::MechTopology topo = mk::derive_topology(cr, h->mech_params);
 
     bool ok = check(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking), err, "stream");
-    if (ok && h->residual) ok = check(mk::mlp::init(), err, "network kernel attributes");
+    if (ok && (h->residual || h->mech_params.learned_precond))
+        ok = check(mk::mlp::init(), err, "network kernel attributes");
     const uint64_t bytes = ok ? carve(h, nullptr) : 0;
     ok = ok && check(cudaMalloc(&h->arena, bytes), err, "device arena");
     if (ok) {
@@ -467,6 +473,7 @@ int mk_create(const MkCreation* cr, const MkConfig* config, const MkCapacities* 
     ok = ok && check(cudaMallocHost(&h->h_tick, sizeof(mk::DevTick) * kTickRing), err, "pinned tick ring");
     ok = ok && check(cudaMallocHost(&h->h_diag, sizeof(GpuDiagnostics)), err, "pinned diagnostics");
     ok = ok && check(cudaMallocHost(&h->h_stats, sizeof(mk::SolveStats)), err, "pinned solve stats");
+    ok = ok && check(cudaMallocHost(&h->h_cstate, sizeof(mk::ClosureState)), err, "pinned closure state");
     for (uint32_t i = 0; ok && i < kTickRing; ++i)
         ok = check(cudaEventCreateWithFlags(&h->tick_done[i], cudaEventDisableTiming), err, "event");
     for (uint32_t i = 0; ok && i < kStageEvents; ++i) ok = check(cudaEventCreate(&h->stage[i]), err, "event");
@@ -476,6 +483,7 @@ int mk_create(const MkCreation* cr, const MkConfig* config, const MkCapacities* 
     }
     std::memset(h->h_diag, 0, sizeof(GpuDiagnostics));
     std::memset(h->h_stats, 0, sizeof(mk::SolveStats));
+    std::memset(h->h_cstate, 0, sizeof(mk::ClosureState));
     // Upload rows (device.rs:429-523): transforms de-interleaved into SoA.
     mk::StepBuffers& b = h->buf;
     cudaStream_t s = h->stream;
@@ -616,7 +624,7 @@ int mk_read_last_tick(MkHandle* h, MkTickReadback* out) {
         for (float m : ms) total += m;
         out->gpu_tick_ms = total;
     }
-    mk::read_mechanism_readback(h->mech, d, out);
+    mk::read_mechanism_readback(h->mech, h->mech_params, d, h->h_cstate, out);
     if (h->residual) {
         const mk::SolveStats st = *h->h_stats;
         out->contact_iterations = st.iterations;
@@ -649,6 +657,31 @@ int mk_set_warm_start_network(MkHandle* h, const float* params, uint32_t count, 
     if (e == cudaSuccess) e = mk::mlp::pack(h->warm_params, h->mlp_scratch, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     return check(e, err, "set_warm_start_network") ? MK_OK : MK_ERR_DEVICE_FAILURE;
+}
+
+int mk_set_preconditioner_network(MkHandle* h, const float* params, uint32_t count, MkError* err) {
+    if (err) std::memset(err, 0, sizeof(*err));
+    if (!h || !params) {
+        set_error(err, MK_ERR_INVALID_ARGUMENT, "handle and params must be non-null");
+        return MK_ERR_INVALID_ARGUMENT;
+    }
+    if (!h->mech.precond_params) {
+        set_error(err, MK_ERR_INVALID_ARGUMENT,
+                  "the preconditioner network needs closure_mode = MK_CLOSURE_PCG_RESIDUAL, "
+                  "preconditioner = MK_PRECOND_LEARNED and at least one closure");
+        return MK_ERR_INVALID_ARGUMENT;
+    }
+    if (count != mk::mlp::kParams) {
+        set_error(err, MK_ERR_INVALID_ARGUMENT, "network has %u parameters, %u given", mk::mlp::kParams, count);
+        if (err) err->required = mk::mlp::kParams, err->provided = count;
+        return MK_ERR_INVALID_ARGUMENT;
+    }
+    DeviceGuard guard(h->device);
+    cudaStream_t s = h->stream;
+    cudaError_t e = cudaMemcpyAsync(h->mech.precond_params, params, sizeof(float) * count, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = mk::mlp::pack(h->mech.precond_params, h->mech.mlp_scratch, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    return check(e, err, "set_preconditioner_network") ? MK_OK : MK_ERR_DEVICE_FAILURE;
 }
 
 int mk_read_warm_start_samples(MkHandle* h, float* features, float* targets, uint32_t capacity, uint32_t* count,
@@ -928,6 +961,13 @@ int mk_read_buffer(MkHandle* h, uint32_t id, void* host, uint64_t cap_bytes, uin
         case MK_BUF_LINKS: src = h->mech.links_final; n = h->mech.links_final ? h->B : 0; row = 48; break;
         case MK_BUF_WARM_PREDICTIONS: src = b.warm_pred; n = b.warm_pred ? counts.active : 0; row = 4; break;
         case MK_BUF_WARM_FEATURES: src = b.warm_features; n = b.warm_features ? counts.active : 0; row = 64; break;
+        case MK_BUF_CLOSURE_SLOTS: src = h->mech.slot_v; n = h->mech.slot_v ? h->mech_params.slots : 0; row = 32; break;
+        case MK_BUF_CLOSURE_BLOCKS: src = h->mech.blk_feat; n = h->mech.blk_feat ? h->mech_params.blocks : 0; row = 64; break;
+        case MK_BUF_CLOSURE_BLOCK_OUTPUTS:
+            src = h->mech.blk_hist;
+            n = h->mech.blk_hist ? 12ull * h->mech_params.blocks : 0;
+            row = 12;
+            break;
         default:
             set_error(err, MK_ERR_INVALID_ARGUMENT, "unknown buffer id %u", id);
             return MK_ERR_INVALID_ARGUMENT;

@@ -26,6 +26,7 @@
 
 #include "mk_device.cuh"
 #include "mk_mechanism.h"
+#include "mk_mlp.h"
 
 namespace mk {
 
@@ -33,9 +34,11 @@ constexpr uint32_t kMBlock = 256;
 constexpr uint32_t kClosureThreads = 1024;
 constexpr uint32_t kClosureSteps = 12;     // device.rs:974
 constexpr uint32_t kClosureRounds = 8;     // closure.wgsl:356
+constexpr uint32_t kMaxLoop = 8;           // coordinates of one per-loop preconditioner block
 
 // ----------------------------------------------------------------- host side
-MechParams make_mech_params(const MkCreation* cr, const StepParams& p, uint32_t iterations, uint32_t closure_mode) {
+MechParams make_mech_params(const MkCreation* cr, const StepParams& p, uint32_t iterations, uint32_t closure_mode,
+                            float closure_tol, uint32_t closure_max_it, uint32_t learned_precond) {
     MechParams m;
     m.body_count = cr->body_count;
     m.bearing_count = cr->bearing_count;
@@ -53,8 +56,14 @@ MechParams make_mech_params(const MkCreation* cr, const StepParams& p, uint32_t 
     m.serial_contacts = (cr->max_depth > 0 && cr->has_dynamic_root && cr->bearing_count <= 64) ? 1u : 0u;
     m.dt = p.dt;
     m.ang_damp = p.ang_damp;
+    m.closure_tol = closure_tol > 0.0f ? closure_tol : 1.0e-5f;
+    m.closure_max_it = closure_max_it ? closure_max_it : 256u;
+    m.learned_precond = (closure_mode == MK_CLOSURE_PCG_RESIDUAL && learned_precond == MK_PRECOND_LEARNED) ? 1u : 0u;
+    m.precond = learned_precond;
     return m;
 }
+
+bool pcg_residual_mode(const MechParams& p) { return p.closure_mode == MK_CLOSURE_PCG_RESIDUAL && p.closures > 0; }
 
 MechTopology derive_topology(const MkCreation* cr, MechParams& p) {
     MechTopology t;
@@ -105,10 +114,38 @@ MechTopology derive_topology(const MkCreation* cr, MechParams& p) {
             if (closure_root[body]) t.cb_bodies.push_back(i);
         }
     }
+    t.slot_closure.resize(t.slot_body.size());
+    for (size_t k = 0; k + 1 < t.cl_slot_off.size(); ++k)
+        for (uint32_t sl = t.cl_slot_off[k]; sl < t.cl_slot_off[k + 1]; ++sl) t.slot_closure[sl] = (uint32_t)k;
     p.closures = (uint32_t)t.cl_bearings.size();
     p.slots = (uint32_t)t.slot_body.size();
     p.closure_coords = (uint32_t)t.cq_coords.size();
     p.closure_bodies = (uint32_t)t.cb_bodies.size();
+    p.blocks = (p.closure_coords + 1) / 2;
+    // per-loop blocks: each closure coordinate joins the block of the first closure that
+    // contains it; loops longer than kMaxLoop are cut into consecutive pieces
+    {
+        std::map<uint32_t, uint32_t> position;
+        for (uint32_t q = 0; q < t.cq_coords.size(); ++q) position[t.cq_coords[q]] = q;
+        std::vector<uint8_t> taken(t.cq_coords.size(), 0);
+        t.loop_off.push_back(0);
+        for (size_t k = 0; k + 1 < t.cl_slot_off.size(); ++k) {
+            std::vector<uint32_t> qs;
+            for (uint32_t sl = t.cl_slot_off[k]; sl < t.cl_slot_off[k + 1]; ++sl) {
+                const uint32_t coord = cr->bearings[mb[t.slot_body[sl]].metadata[1]].metadata[2];
+                auto it = position.find(coord);
+                if (it == position.end() || taken[it->second]) continue;
+                taken[it->second] = 1;
+                qs.push_back(it->second);
+            }
+            std::sort(qs.begin(), qs.end());
+            for (size_t i = 0; i < qs.size(); i += kMaxLoop) {
+                for (size_t j = i; j < std::min(qs.size(), i + kMaxLoop); ++j) t.loop_q.push_back(qs[j]);
+                t.loop_off.push_back((uint32_t)t.loop_q.size());
+            }
+        }
+        p.loops = (uint32_t)t.loop_off.size() - 1;
+    }
     return t;
 }
 
@@ -142,6 +179,23 @@ void carve_mechanism(MechBuffers& m, const MechParams& p, uint32_t B, uint32_t J
     m.diag = f32(Q);
     m.pcg = f32(5ull * Q);
     m.links_final = p.final_is_a ? m.links_a : m.links_b;
+    if (pcg_residual_mode(p)) {
+        m.slot_closure = u32(p.slots);
+        m.slot_v = reinterpret_cast<float4*>(take(32ull * (p.slots ? p.slots : 1)));
+        m.blk_m = reinterpret_cast<float4*>(take(16ull * (p.blocks ? p.blocks : 1)));
+        m.blk_feat = reinterpret_cast<float4*>(take(64ull * (p.blocks ? p.blocks : 1)));
+        m.blk_out = f32(3ull * p.blocks);
+        m.blk_hist = f32(3ull * kClosureSteps * p.blocks);
+        m.probe = f32(2ull * Q);
+        m.cstate = reinterpret_cast<ClosureState*>(take(sizeof(ClosureState)));
+        if (p.learned_precond) {
+            m.precond_params = f32(mlp::kParams + 16);
+            m.mlp_scratch = take(mlp::scratch_bytes(0));
+        }
+        m.loop_off = u32(p.loops + 1);
+        m.loop_q = u32(p.closure_coords);
+        m.loop_l = f32(36ull * p.loops);
+    }
 }
 
 template <class T>
@@ -177,6 +231,10 @@ bool upload_mechanism(MechBuffers& m, const MechParams& p, const MechTopology& t
     if (e == cudaSuccess) e = put(m.cl_bearings, t.cl_bearings, s);
     if (e == cudaSuccess) e = put(m.cl_slot_off, t.cl_slot_off, s);
     if (e == cudaSuccess) e = put(m.cl_split, t.cl_split, s);
+    if (e == cudaSuccess && m.slot_closure) e = put(m.slot_closure, t.slot_closure, s);
+    if (e == cudaSuccess && m.loop_off) e = put(m.loop_off, t.loop_off, s);
+    if (e == cudaSuccess && m.loop_q) e = put(m.loop_q, t.loop_q, s);
+    if (e == cudaSuccess && m.precond_params) e = mlp::pack(m.precond_params, m.mlp_scratch, s);
     if (e == cudaSuccess) e = put(m.slot_body, t.slot_body, s);
     if (e == cudaSuccess) e = put(m.cq_coords, t.cq_coords, s);
     if (e == cudaSuccess) e = put(m.cq_off, t.cq_off, s);
@@ -814,6 +872,427 @@ __global__ void __launch_bounds__(kClosureThreads) k_closure_loop(StepBuffers b,
     }
 }
 
+// ------------------------------------------------- closure PCG to a residual
+// MK_CLOSURE_PCG_RESIDUAL: each Newton step of the closure loop solves
+// (J^T J) dtheta = -g by preconditioned conjugate gradients until
+// ||r|| <= closure_tol * ||r0|| (or closure_max_it iterations), with
+// FP64 dot products and residual check (f32 vectors), instead of the
+// reference's 8 diagonal-PCG rounds.  The preconditioner is block Jacobi
+// over 2 x 2 blocks of consecutive closure coordinates (a whole loop's block
+// would be the exact inverse of its independent component, leaving nothing
+// to precondition); with the learned preconditioner the network's corrected
+// block inverse replaces a block when it is positive definite.
+//
+// Each Newton step is two launches (evaluate, solve) with the network in
+// between; a converged step sets `done` and the later launches return.
+
+// Fixed-order FP64 block sum (1024 threads): per-thread partials, warp
+// shuffle-down trees, then warp 0 over the 32 warp sums.
+__device__ __forceinline__ double block_sum_d(double v, double* scratch) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    const uint32_t w = threadIdx.x >> 5, lane = threadIdx.x & 31u;
+    __syncthreads();
+    if (lane == 0) scratch[w] = v;
+    __syncthreads();
+    if (w == 0) {
+        double r = lane < (blockDim.x >> 5) ? scratch[lane] : 0.0;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) r += __shfl_down_sync(0xffffffffu, r, o);
+        if (lane == 0) scratch[32] = r;
+    }
+    __syncthreads();
+    const double r = scratch[32];
+    __syncthreads();
+    return r;
+}
+
+// out[c] = (J^T J x)[c] for the closure coordinates, from the stored columns.
+__device__ void closure_apply(const MechBuffers& m, const MechParams& p, const float* x, float* out) {
+    const uint32_t tid = threadIdx.x, nt = blockDim.x;
+    for (uint32_t k = tid; k < p.closures; k += nt) {
+        const uint32_t s0 = m.cl_slot_off[k], s1 = m.cl_slot_off[k + 1], split = m.cl_split[k];
+        f3 prod_p[2] = {mkf3(0, 0, 0), mkf3(0, 0, 0)}, prod_a[2] = {mkf3(0, 0, 0), mkf3(0, 0, 0)};
+        for (uint32_t sl = s0; sl < s1; ++sl) {
+            const int side = sl < split ? 0 : 1;
+            const f3 pd = xyz(m.slot_v[2 * sl]), ad = xyz(m.slot_v[2 * sl + 1]);
+            const float dv = x[__float_as_uint(m.slot_v[2 * sl].w)];
+            prod_p[side] = prod_p[side] + pd * dv;
+            prod_a[side] = prod_a[side] + ad * dv;
+        }
+        const f3 pp = prod_p[0] + prod_p[1], pa = prod_a[0] + prod_a[1];
+        for (uint32_t sl = s0; sl < s1; ++sl)
+            m.slot_g[sl] = dot(xyz(m.slot_v[2 * sl]), pp) + 1.0f * dot(xyz(m.slot_v[2 * sl + 1]), pa);
+    }
+    __syncthreads();
+    for (uint32_t q = tid; q < p.closure_coords; q += nt) {
+        float o = 0.0f;
+        for (uint32_t i = m.cq_off[q]; i < m.cq_off[q + 1]; ++i) o += m.slot_g[m.cq_slots[i]];
+        out[m.cq_coords[q]] = o;
+    }
+    __syncthreads();
+}
+
+// (J^T J)[i][j] for two closure coordinates (positions qi, qj in the list).
+__device__ __forceinline__ float closure_coupling(const MechBuffers& m, uint32_t qi, uint32_t qj) {
+    float r = 0.0f;
+    for (uint32_t a = m.cq_off[qi]; a < m.cq_off[qi + 1]; ++a) {
+        const uint32_t sa = m.cq_slots[a];
+        for (uint32_t bq = m.cq_off[qj]; bq < m.cq_off[qj + 1]; ++bq) {
+            const uint32_t sb = m.cq_slots[bq];
+            if (m.slot_closure[sa] != m.slot_closure[sb]) continue;
+            r += dot(xyz(m.slot_v[2 * sa]), xyz(m.slot_v[2 * sb])) +
+                 1.0f * dot(xyz(m.slot_v[2 * sa + 1]), xyz(m.slot_v[2 * sb + 1]));
+        }
+    }
+    return r;
+}
+
+__global__ void __launch_bounds__(kClosureThreads) k_closure_eval(StepBuffers b, MechBuffers m, MechParams p,
+                                                                  uint32_t step) {
+    __shared__ uint32_t s_state[2];
+    ClosureState* cs = m.cstate;
+    const uint32_t tid = threadIdx.x, nt = blockDim.x;
+    const uint32_t NC = p.closures, NQ = p.closure_coords, Q = p.coordinate_count;
+    if (step == 0) {
+        __syncthreads();
+        if (tid == 0) *cs = ClosureState{0u, 0u, 0u, 0u, 0u, 0u, 0.0};
+        __syncthreads();
+    } else if (ld_acquire_u32(&cs->done)) {
+        return;
+    }
+    if (tid == 0) { s_state[0] = 0; s_state[1] = 0; }
+    __syncthreads();
+    // slot columns and their gradient / diagonal contributions (closure.wgsl:268-319)
+    for (uint32_t k = tid; k < NC; k += nt) {
+        const GpuBearing br = m.bearings[m.cl_bearings[k]];
+        f3 aa, ab, xa, xb;
+        closure_frames(m, br, aa, ab, xa, xb);
+        const f3 rp = aa - ab, ra = xa - xb;
+        const uint32_t s0 = m.cl_slot_off[k], s1 = m.cl_slot_off[k + 1], split = m.cl_split[k];
+        bool active = true;
+        if (!finite3(rp) || !finite3(ra)) {
+            atomicOr(&b.diag->error_flags, MK_INVALID_NUMERIC_FLAG);
+            atomicMax(&s_state[0], 0xffffffffu);
+            atomicMax(&s_state[1], 0xffffffffu);
+            active = false;
+        } else {
+            const uint32_t um = round_u32(length(rp) * 1000000.0f);
+            const float deg = atan2_cr(length(cross(xa, xb)), clampf(dot(xa, xb), -1.0f, 1.0f)) * 57.295779513f;
+            const uint32_t ud = round_u32(deg * 1000000.0f);
+            atomicMax(&s_state[0], um);
+            atomicMax(&s_state[1], ud);
+            active = !(um <= 10u && ud <= 1000u);
+        }
+        for (uint32_t sl = s0; sl < s1; ++sl) {
+            const bool side_a = sl < split;
+            const f3 ea = side_a ? aa : ab, ex = side_a ? xa : xb;
+            const float sign = side_a ? 1.0f : -1.0f;
+            f3 axis, anchor;
+            uint32_t coord;
+            joint_frame(m, m.slot_body[sl], axis, anchor, coord);
+            f3 pd = mkf3(0, 0, 0), ad = mkf3(0, 0, 0);
+            float g = 0.0f, d = 0.0f;
+            uint32_t valid = 0;
+            if (coord >= Q) {
+                atomicOr(&b.diag->error_flags, MK_INVALID_NUMERIC_FLAG);
+                coord = 0;
+            } else {
+                pd = cross(axis, ea - anchor) * sign;
+                ad = cross(axis, ex) * sign;
+                if (active) {
+                    g = dot(rp, pd) + 1.0f * dot(ra, ad);
+                    d = dot(pd, pd) + 1.0f * dot(ad, ad);
+                    if (g == g && d == d) valid = 1;
+                    else atomicOr(&b.diag->error_flags, MK_INVALID_NUMERIC_FLAG);
+                }
+            }
+            m.slot_v[2 * sl] = f4(pd, __uint_as_float(coord));
+            m.slot_v[2 * sl + 1] = f4(ad, __uint_as_float(m.slot_closure[sl]));
+            m.slot_g[sl] = valid ? g : __int_as_float(0x7fffffff);
+            m.slot_d[sl] = valid ? d : 0.0f;
+        }
+    }
+    __syncthreads();
+    for (uint32_t q = tid; q < NQ; q += nt) {
+        float g = 0.0f, d = 0.0f;
+        for (uint32_t i = m.cq_off[q]; i < m.cq_off[q + 1]; ++i) {
+            const uint32_t sl = m.cq_slots[i];
+            const float sg = m.slot_g[sl];
+            if (sg == sg) { g += sg; d += m.slot_d[sl]; }
+        }
+        const uint32_t c = m.cq_coords[q];
+        m.grad[c] = g;
+        m.diag[c] = d;
+        // probe vectors: ones and alternating signs over the coordinate list
+        m.pcg[c] = 1.0f;
+        m.pcg[Q + c] = (q & 1u) ? -1.0f : 1.0f;
+    }
+    __syncthreads();
+    const bool unconverged = s_state[0] > 10u || s_state[1] > 1000u;
+    // A * ones and A * alternating signs (block inputs of the network)
+    closure_apply(m, p, m.pcg, m.probe);
+    closure_apply(m, p, m.pcg + Q, m.probe + Q);
+    // block entries (a, b, d) and the plain 2 x 2 inverse
+    float* blk_b = m.pcg + 2ull * Q;   // coupling of each block (free until the solve)
+    for (uint32_t blk = tid; blk < p.blocks; blk += nt) {
+        const uint32_t qi = 2 * blk, qj = qi + 1;
+        const bool pair = qj < NQ;
+        const float a = m.diag[m.cq_coords[qi]], d = pair ? m.diag[m.cq_coords[qj]] : 0.0f;
+        const float bij = pair ? closure_coupling(m, qi, qj) : 0.0f;
+        float4 inv = make_float4(a > 1.0e-12f ? 1.0f / a : 0.0f, 0.0f, d > 1.0e-12f ? 1.0f / d : 0.0f, 0.0f);
+        if (pair && a > 1.0e-12f && d > 1.0e-12f) {
+            const float det = a * d - bij * bij;
+            if (det > 1.0e-6f * (a * d)) inv = make_float4(d / det, -bij / det, a / det, 0.0f);
+        }
+        m.blk_m[blk] = inv;
+        blk_b[blk] = bij;
+    }
+    __syncthreads();
+    // network inputs: the diagonal-normalised entries of J^T J around the block,
+    // with the partner block (blk ^ 1) and the couplings to it recovered from
+    // the two probes (exact when the loop's coordinates are these two blocks)
+    for (uint32_t blk = tid; blk < p.blocks; blk += nt) {
+        float4 f[4] = {make_float4(0, 0, 0, 0), make_float4(0, 0, 0, 0), make_float4(0, 0, 0, 0),
+                       make_float4(0, 0, 0, 1.0f)};
+        const uint32_t qi = 2 * blk, qj = qi + 1;
+        const uint32_t ci = m.cq_coords[qi];
+        const bool pair = qj < NQ;
+        const uint32_t cj = pair ? m.cq_coords[qj] : ci;
+        const float a = m.diag[ci], d = pair ? m.diag[cj] : 0.0f, bij = blk_b[blk];
+        const uint32_t pb = blk ^ 1u;
+        const bool partner = pb < p.blocks && 2 * pb + 1 < NQ;
+        if (pair && partner && a > 1.0e-12f && d > 1.0e-12f) {
+            const float pa = m.diag[m.cq_coords[2 * pb]], pd = m.diag[m.cq_coords[2 * pb + 1]];
+            if (pa > 1.0e-12f && pd > 1.0e-12f) {
+                const float s1i = m.probe[ci] - a - bij, ssi = m.probe[Q + ci] - a + bij;
+                const float s1j = m.probe[cj] - bij - d, ssj = m.probe[Q + cj] - bij + d;
+                const float sa = sqrtf(a), sd = sqrtf(d), spa = sqrtf(pa), spd = sqrtf(pd);
+                f[0] = make_float4(bij / (sa * sd), blk_b[pb] / (spa * spd), 0.5f * (s1i + ssi) / (sa * spa),
+                                   0.5f * (s1i - ssi) / (sa * spd));
+                f[1] = make_float4(0.5f * (s1j + ssj) / (sd * spa), 0.5f * (s1j - ssj) / (sd * spd), logf(a / d),
+                                   1.0f);
+            }
+        }
+        float4* fo = m.blk_feat + 4ull * blk;
+        fo[0] = f[0]; fo[1] = f[1]; fo[2] = f[2]; fo[3] = f[3];
+    }
+    // per-loop blocks: Cholesky of J^T J on the loop's coordinates plus a ridge of
+    // 1e-6 x the mean diagonal; a failed pivot leaves the block diagonal (Jacobi)
+    if (p.precond == MK_PRECOND_BLOCK_JACOBI) {
+        for (uint32_t lp = tid; lp < p.loops; lp += nt) {
+            const uint32_t o = m.loop_off[lp], n = m.loop_off[lp + 1] - o;
+            float a[kMaxLoop * (kMaxLoop + 1) / 2];
+            float mean = 0.0f;
+            for (uint32_t i = 0; i < n; ++i) mean += m.diag[m.cq_coords[m.loop_q[o + i]]];
+            mean = n ? mean / (float)n : 0.0f;
+            for (uint32_t i = 0; i < n; ++i)
+                for (uint32_t j = 0; j <= i; ++j)
+                    a[i * (i + 1) / 2 + j] = i == j ? m.diag[m.cq_coords[m.loop_q[o + i]]] + 1.0e-6f * mean
+                                                    : closure_coupling(m, m.loop_q[o + i], m.loop_q[o + j]);
+            bool ok = mean > 1.0e-12f;
+            for (uint32_t j = 0; j < n && ok; ++j) {
+                float dj = a[j * (j + 1) / 2 + j];
+                for (uint32_t k = 0; k < j; ++k) dj -= a[j * (j + 1) / 2 + k] * a[j * (j + 1) / 2 + k];
+                if (!(dj > 0.0f)) { ok = false; break; }
+                const float ljj = sqrtf(dj);
+                a[j * (j + 1) / 2 + j] = ljj;
+                for (uint32_t i = j + 1; i < n; ++i) {
+                    float v = a[i * (i + 1) / 2 + j];
+                    for (uint32_t k = 0; k < j; ++k) v -= a[i * (i + 1) / 2 + k] * a[j * (j + 1) / 2 + k];
+                    a[i * (i + 1) / 2 + j] = v / ljj;
+                }
+            }
+            float* l = m.loop_l + 36ull * lp;
+            for (uint32_t i = 0; i < n; ++i)
+                for (uint32_t j = 0; j <= i; ++j) {
+                    float v = a[i * (i + 1) / 2 + j];
+                    if (!ok) {   // Jacobi: L = diag(sqrt(a_ii))
+                        const float dii = m.diag[m.cq_coords[m.loop_q[o + i]]];
+                        v = (i == j) ? (dii > 1.0e-12f ? sqrtf(dii) : 0.0f) : 0.0f;
+                    }
+                    l[i * (i + 1) / 2 + j] = v;
+                }
+        }
+    }
+    __syncthreads();
+    if (tid == 0) {
+        if (unconverged) {
+            cs->live_blocks = p.blocks;
+            ++cs->newton_steps;
+        } else {
+            cs->live_blocks = 0;
+            st_release_u32(&cs->done, 1u);
+        }
+    }
+}
+
+__device__ __forceinline__ void precond_apply(const MechBuffers& m, const MechParams& p, const float* r, float* z) {
+    if (p.precond == MK_PRECOND_BLOCK_JACOBI) {
+        for (uint32_t lp = threadIdx.x; lp < p.loops; lp += blockDim.x) {
+            const uint32_t o = m.loop_off[lp], n = m.loop_off[lp + 1] - o;
+            const float* l = m.loop_l + 36ull * lp;
+            float y[kMaxLoop];
+            for (uint32_t i = 0; i < n; ++i) {   // L y = r
+                float v = r[m.cq_coords[m.loop_q[o + i]]];
+                for (uint32_t k = 0; k < i; ++k) v -= l[i * (i + 1) / 2 + k] * y[k];
+                const float lii = l[i * (i + 1) / 2 + i];
+                y[i] = lii > 0.0f ? v / lii : 0.0f;
+            }
+            for (uint32_t ii = n; ii-- > 0;) {   // L^T z = y
+                float v = y[ii];
+                for (uint32_t k = ii + 1; k < n; ++k) v -= l[k * (k + 1) / 2 + ii] * y[k];
+                const float lii = l[ii * (ii + 1) / 2 + ii];
+                y[ii] = lii > 0.0f ? v / lii : 0.0f;
+            }
+            for (uint32_t i = 0; i < n; ++i) z[m.cq_coords[m.loop_q[o + i]]] = y[i];
+        }
+        __syncthreads();
+        return;
+    }
+    for (uint32_t blk = threadIdx.x; blk < p.blocks; blk += blockDim.x) {
+        const float4 mi = m.blk_m[blk];
+        const uint32_t qi = 2 * blk, qj = qi + 1;
+        const uint32_t ci = m.cq_coords[qi];
+        if (qj < p.closure_coords) {
+            const uint32_t cj = m.cq_coords[qj];
+            const float ri = r[ci], rj = r[cj];
+            z[ci] = mi.x * ri + mi.y * rj;
+            z[cj] = mi.y * ri + mi.z * rj;
+        } else {
+            z[ci] = mi.x * r[ci];
+        }
+    }
+    __syncthreads();
+}
+
+__global__ void __launch_bounds__(kClosureThreads) k_closure_pcg(StepBuffers b, MechBuffers m, MechParams p,
+                                                                 uint32_t step) {
+    __shared__ double s_red[33];
+    ClosureState* cs = m.cstate;
+    if (ld_acquire_u32(&cs->done)) return;
+    const uint32_t tid = threadIdx.x, nt = blockDim.x;
+    const uint32_t NQ = p.closure_coords, NB = p.closure_bodies, Q = p.coordinate_count;
+    float* sol = m.pcg;
+    float* res = m.pcg + Q;
+    float* pre = m.pcg + 2ull * Q;
+    float* dir = m.pcg + 3ull * Q;
+    float* op = m.pcg + 4ull * Q;
+    // learned blocks: T' = S M^-1 S with S = diag(sqrt(a), sqrt(d)), from the network's
+    // (y0, y1, y2) as t11 = e^y0, t22 = e^y1, t12 = 0.999 tanh(y2) sqrt(t11 t22): positive
+    // definite by construction (the check below only catches overflow and NaN)
+    if (p.learned_precond) {
+        uint32_t used = 0, rejected = 0;
+        for (uint32_t blk = tid; blk < p.blocks; blk += nt) {
+            const float y0 = fminf(fmaxf(m.blk_out[3 * blk], -30.0f), 30.0f);
+            const float y1 = fminf(fmaxf(m.blk_out[3 * blk + 1], -30.0f), 30.0f);
+            const float t11 = expf(y0), t22 = expf(y1);
+            const float t12 = 0.999f * tanhf(m.blk_out[3 * blk + 2]) * sqrtf(t11 * t22);
+            float* h = m.blk_hist + 3ull * ((uint64_t)step * p.blocks + blk);
+            h[0] = t11; h[1] = t12; h[2] = t22;
+            const uint32_t qi = 2 * blk, qj = qi + 1;
+            const uint32_t ci = m.cq_coords[qi];
+            const bool pair = qj < NQ;
+            const float a = m.diag[ci], d = pair ? m.diag[m.cq_coords[qj]] : 0.0f;
+            if (pair) {
+                if (a > 1.0e-12f && d > 1.0e-12f && t11 > 0.0f && t22 > 0.0f &&
+                    t11 * t22 - t12 * t12 > 1.0e-6f * (t11 * t22)) {
+                    const float sa = sqrtf(a), sd = sqrtf(d);
+                    m.blk_m[blk] = make_float4(t11 / a, t12 / (sa * sd), t22 / d, 0.0f);
+                    ++used;
+                } else {
+                    ++rejected;
+                }
+            } else if (a > 1.0e-12f && t11 > 0.0f) {
+                m.blk_m[blk] = make_float4(t11 / a, 0.0f, 0.0f, 0.0f);
+                ++used;
+            } else {
+                ++rejected;
+            }
+        }
+        if (used) atomicAdd(&cs->learned_blocks, used);
+        if (rejected) atomicAdd(&cs->rejected_blocks, rejected);
+        __syncthreads();
+    }
+    // r = -g, x = 0, z = M^-1 r, p = z
+    for (uint32_t q = tid; q < NQ; q += nt) {
+        const uint32_t c = m.cq_coords[q];
+        sol[c] = 0.0f;
+        res[c] = -m.grad[c];
+    }
+    __syncthreads();
+    precond_apply(m, p, res, pre);
+    double prz = 0.0, prr = 0.0;
+    for (uint32_t q = tid; q < NQ; q += nt) {
+        const uint32_t c = m.cq_coords[q];
+        dir[c] = pre[c];
+        prz += (double)res[c] * (double)pre[c];
+        prr += (double)res[c] * (double)res[c];
+    }
+    double rz = block_sum_d(prz, s_red);
+    const double rr0 = block_sum_d(prr, s_red);
+    double rr = rr0;
+    const double tol2 = (double)p.closure_tol * (double)p.closure_tol;
+    uint32_t it = 0;
+    while (it < p.closure_max_it && rr > tol2 * rr0) {
+        closure_apply(m, p, dir, op);
+        double ppq = 0.0;
+        for (uint32_t q = tid; q < NQ; q += nt) {
+            const uint32_t c = m.cq_coords[q];
+            ppq += (double)dir[c] * (double)op[c];
+        }
+        const double pq = block_sum_d(ppq, s_red);
+        const float alpha = fabs(pq) > 1.0e-30 ? (float)(rz / pq) : 0.0f;
+        double pr = 0.0;
+        for (uint32_t q = tid; q < NQ; q += nt) {
+            const uint32_t c = m.cq_coords[q];
+            sol[c] += alpha * dir[c];
+            res[c] -= alpha * op[c];
+            pr += (double)res[c] * (double)res[c];
+        }
+        rr = block_sum_d(pr, s_red);
+        ++it;
+        if (rr <= tol2 * rr0) break;
+        precond_apply(m, p, res, pre);
+        double pz = 0.0;
+        for (uint32_t q = tid; q < NQ; q += nt) {
+            const uint32_t c = m.cq_coords[q];
+            pz += (double)res[c] * (double)pre[c];
+        }
+        const double nrz = block_sum_d(pz, s_red);
+        const float beta = fabs(rz) > 1.0e-300 ? (float)(nrz / rz) : 0.0f;
+        for (uint32_t q = tid; q < NQ; q += nt) {
+            const uint32_t c = m.cq_coords[q];
+            dir[c] = pre[c] + beta * dir[c];
+        }
+        rz = nrz;
+        __syncthreads();
+    }
+    if (tid == 0) {
+        cs->pcg_iterations += it;
+        const double rel = rr0 > 0.0 ? sqrt(rr / rr0) : 0.0;
+        if (rel > cs->max_relative_residual) cs->max_relative_residual = rel;
+    }
+    // step the closure coordinates (closure.wgsl:416-427)
+    for (uint32_t q = tid; q < NQ; q += nt) {
+        const uint32_t c = m.cq_coords[q];
+        const float stp = clampf(0.35f * sol[c], -0.2f, 0.2f);
+        if (stp == stp) m.coords[c].angle += stp;
+        else atomicOr(&b.diag->error_flags, MK_INVALID_NUMERIC_FLAG);
+    }
+    __syncthreads();
+    // forward kinematics of the closure components (mechanism.wgsl:72-149)
+    for (uint32_t i = tid; i < NB; i += nt) prepare_link(m, m.cb_bodies[i]);
+    __syncthreads();
+    bool a_src = true;
+    for (uint32_t r = 0; r < p.jump_rounds; ++r) {
+        for (uint32_t i = tid; i < NB; i += nt)
+            jump_link(a_src ? m.links_a : m.links_b, a_src ? m.links_b : m.links_a, m.cb_bodies[i]);
+        __syncthreads();
+        a_src = !a_src;
+    }
+}
+
 // --------------------------------------------------------------- launches
 static inline uint32_t nblocks(uint32_t n) { return (n + kMBlock - 1) / kMBlock; }
 
@@ -855,7 +1334,19 @@ cudaError_t enqueue_mechanism(MechBuffers& m, const StepBuffers& b, const MechPa
         if ((e = bearing_projection_iteration(m, b, p, s)) != cudaSuccess) return e;
     k_advance_coordinates<<<nblocks(p.body_count), kMBlock, 0, s>>>(b, m, p);
     if ((e = forward_kinematics(m, p, s)) != cudaSuccess) return e;
-    if (p.closures > 0) k_closure_loop<<<1, kClosureThreads, 0, s>>>(b, m, p);
+    if (pcg_residual_mode(p)) {
+        for (uint32_t step = 0; step < kClosureSteps; ++step) {
+            k_closure_eval<<<1, kClosureThreads, 0, s>>>(b, m, p, step);
+            if (p.learned_precond) {
+                e = mlp::forward(m.precond_params, reinterpret_cast<const float*>(m.blk_feat), 0,
+                                 &m.cstate->live_blocks, p.blocks, m.blk_out, 3, m.mlp_scratch, &b.diag->error_flags, s);
+                if (e != cudaSuccess) return e;
+            }
+            k_closure_pcg<<<1, kClosureThreads, 0, s>>>(b, m, p, step);
+        }
+    } else if (p.closures > 0) {
+        k_closure_loop<<<1, kClosureThreads, 0, s>>>(b, m, p);
+    }
     k_publish<<<nblocks(p.body_count), kMBlock, 0, s>>>(b, m, p);
     return reconstruct(m, b, s);
 }
@@ -896,10 +1387,20 @@ void enqueue_validate_bearings(MechBuffers& m, const StepBuffers& b, const MechP
                                                                       b.diag);
 }
 
-void read_mechanism_readback(const MechBuffers& m, const GpuDiagnostics& d, MkTickReadback* out) {
+void read_mechanism_readback(const MechBuffers& m, const MechParams& p, const GpuDiagnostics& d,
+                             const ClosureState* cs, MkTickReadback* out) {
     (void)m;
-    out->closure_iterations = d.reserved_c;
-    out->closure_relative_residual = 0.0;
+    if (pcg_residual_mode(p) && cs) {
+        out->closure_iterations = cs->pcg_iterations;
+        out->closure_relative_residual = cs->max_relative_residual;
+    } else {
+        out->closure_iterations = d.reserved_c;
+        out->closure_relative_residual = 0.0;
+    }
+}
+
+uint64_t mechanism_mlp_scratch_bytes(const MechParams& p) {
+    return p.learned_precond ? mlp::scratch_bytes(0) : 0;
 }
 
 }  // namespace mk

@@ -25,6 +25,24 @@ struct MechParams {
     uint32_t slots = 0;              // joints on closure branches, over all closures
     uint32_t closure_coords = 0;     // distinct coordinates on closure branches
     uint32_t closure_bodies = 0;     // bodies of components that contain a closure
+    // MK_CLOSURE_PCG_RESIDUAL
+    float closure_tol = 1.0e-5f;     // relative PCG residual per Newton step
+    uint32_t closure_max_it = 256;   // PCG iterations per Newton step
+    uint32_t learned_precond = 0;    // blocks corrected by the preconditioner network
+    uint32_t precond = 0;            // MK_PRECOND_*
+    uint32_t blocks = 0;             // 2 x 2 preconditioner blocks: ceil(closure_coords / 2)
+    uint32_t loops = 0;              // per-loop preconditioner blocks (<= kMaxLoop coordinates each)
+};
+
+// Outcome of the closure solve of one tick (MK_CLOSURE_PCG_RESIDUAL).
+struct ClosureState {
+    uint32_t done;                   // converged at an earlier Newton step
+    uint32_t live_blocks;            // blocks the network runs on this step (0 once converged)
+    uint32_t newton_steps;
+    uint32_t pcg_iterations;
+    uint32_t learned_blocks;         // blocks that used the network's correction (summed over steps)
+    uint32_t rejected_blocks;        // blocks whose correction was not positive definite
+    double max_relative_residual;    // worst final ||r|| / ||r0|| over the Newton steps
 };
 
 struct MechBuffers {
@@ -57,13 +75,30 @@ struct MechBuffers {
     float* pcg = nullptr;                       // 5 x Q: sol, res, pre, dir, op (closure.wgsl:51-60)
     uint32_t readback_iterations = 0;
     double readback_residual = 0.0;
+    // MK_CLOSURE_PCG_RESIDUAL
+    uint32_t* slot_closure = nullptr;           // closure of each slot
+    float4* slot_v = nullptr;                   // 2 per slot: the joint's Jacobian column (position, axis rows)
+    float4* blk_m = nullptr;                    // per block: preconditioner inverse (m11, m12, m22, -)
+    float4* blk_feat = nullptr;                 // 4 per block: network inputs
+    float* blk_out = nullptr;                   // 3 per block: network outputs of the current step
+    float* blk_hist = nullptr;                  // 12 steps x blocks x 3: outputs used at each Newton step
+    float* probe = nullptr;                     // 2 x Q: A * ones, A * alternating signs
+    ClosureState* cstate = nullptr;
+    float* precond_params = nullptr;            // preconditioner network parameters (mlp::kParams)
+    uint32_t* loop_off = nullptr;               // loops + 1: offsets into loop_q
+    uint32_t* loop_q = nullptr;                 // closure-coordinate positions of each loop block
+    float* loop_l = nullptr;                    // 36 per loop: Cholesky factor (lower, row-major packed)
+    void* mlp_scratch = nullptr;
 };
 
-MechParams make_mech_params(const MkCreation* cr, const StepParams& p, uint32_t iterations, uint32_t closure_mode);
+MechParams make_mech_params(const MkCreation* cr, const StepParams& p, uint32_t iterations, uint32_t closure_mode,
+                            float closure_tol, uint32_t closure_max_it, uint32_t precond);
 // Host-side closure topology and depth levels; fills the counts in `p`.
 struct MechTopology {
     std::vector<uint32_t> level_bodies, level_offsets;
     std::vector<uint32_t> cl_bearings, cl_slot_off, cl_split, slot_body, cq_coords, cq_off, cq_slots, cb_bodies;
+    std::vector<uint32_t> slot_closure;
+    std::vector<uint32_t> loop_off, loop_q;
 };
 MechTopology derive_topology(const MkCreation* cr, MechParams& p);
 void carve_mechanism(MechBuffers& m, const MechParams& p, uint32_t B, uint32_t J, uint32_t Q,
@@ -72,12 +107,16 @@ bool upload_mechanism(MechBuffers& m, const MechParams& p, const MechTopology& t
                       cudaStream_t s, MkError* err);
 void enqueue_mechanism_prelude(MechBuffers& m, const StepBuffers& b, const MechParams& p, cudaStream_t s);
 cudaError_t enqueue_mechanism(MechBuffers& m, const StepBuffers& b, const MechParams& p, cudaStream_t s);
+bool pcg_residual_mode(const MechParams& p);
 cudaError_t enqueue_contact_solver_with_bearings(MechBuffers& m, const StepBuffers& b, const StepParams& sp,
                                                  const MechParams& p, const StepLaunch& l, int parity, cudaStream_t s);
 cudaError_t enqueue_post_contact(MechBuffers& m, const StepBuffers& b, const MechParams& p, cudaStream_t s);
 void enqueue_validate_state(MechBuffers& m, const StepBuffers& b, const MechParams& p, cudaStream_t s);
 void enqueue_validate_bearings(MechBuffers& m, const StepBuffers& b, const MechParams& p, bool mechanism_active,
                                cudaStream_t s);
-void read_mechanism_readback(const MechBuffers& m, const GpuDiagnostics& d, MkTickReadback* out);
+void read_mechanism_readback(const MechBuffers& m, const MechParams& p, const GpuDiagnostics& d,
+                             const ClosureState* cs, MkTickReadback* out);
+// bytes of network scratch the learned preconditioner needs (0 without it)
+uint64_t mechanism_mlp_scratch_bytes(const MechParams& p);
 
 }  // namespace mk

@@ -27,6 +27,7 @@ EXPORTS = [
     "mk_tick_kernel_count", "mk_set_tuning", "mk_op_sort_keys_static",
     "mk_mlp_param_count", "mk_op_mlp_scratch_bytes", "mk_op_mlp_forward", "mk_op_mlp_gradient",
     "mk_op_mlp_train", "mk_set_warm_start_network", "mk_read_warm_start_samples",
+    "mk_set_preconditioner_network",
 ]
 
 _lib = None
@@ -75,6 +76,7 @@ def library(path: str | None = None):
         "mk_op_mlp_train": (i32, [vp, vp, vp, vp, vp, vp, u32, u32, u32, C.c_float, u32, vp, vp, u64, vp, vp]),
         "mk_set_warm_start_network": (i32, [vp, vp, u32, vp]),
         "mk_read_warm_start_samples": (i32, [vp, vp, vp, u32, vp, vp]),
+        "mk_set_preconditioner_network": (i32, [vp, vp, u32, vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -367,6 +369,23 @@ class GpuPhysics:
         p = np.ascontiguousarray(params, np.float32)
         err = abi.MkError()
         _raise(library().mk_set_warm_start_network(self._h, p.ctypes.data, len(p), C.byref(err)), err)
+
+    def set_preconditioner_network(self, params: np.ndarray) -> None:
+        """Loads the closure preconditioner network (MK_PRECOND_LEARNED)."""
+        p = np.ascontiguousarray(params, np.float32)
+        err = abi.MkError()
+        _raise(library().mk_set_preconditioner_network(self._h, p.ctypes.data, len(p), C.byref(err)), err)
+
+    def closure_slots(self):
+        """Jacobian columns of the last evaluated Newton step: (pd (n, 3), ad (n, 3), coord, closure)."""
+        raw = self.read_buffer(abi.BUF_CLOSURE_SLOTS, np.float32, 32).reshape(-1, 8)
+        return raw[:, 0:3], raw[:, 4:7], raw[:, 3].view(np.uint32), raw[:, 7].view(np.uint32)
+
+    def closure_blocks(self):
+        return self.read_buffer(abi.BUF_CLOSURE_BLOCKS, np.float32, 64).reshape(-1, 16)
+
+    def closure_block_outputs(self):
+        return self.read_buffer(abi.BUF_CLOSURE_BLOCK_OUTPUTS, np.float32, 12).reshape(12, -1, 3)
 
     def warm_start_samples(self):
         """(inputs (n, 16), targets (n,)) of the last tick's active contacts."""

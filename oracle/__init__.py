@@ -60,6 +60,10 @@ def lib():
             getattr(L, name).argtypes = [vp, vp]
         L.or_get_sorted.argtypes = [vp, vp, vp]
         L.or_get_solve_stats.argtypes = [vp, vp, vp]
+        L.or_get_closure_stats.argtypes = [vp, vp, vp]
+        L.or_set_precond_outputs.argtypes = [vp, vp, u32]
+        L.or_get_closure_blocks.restype = u32
+        L.or_get_closure_blocks.argtypes = [vp, vp]
         L.or_set_warm_predictions.argtypes = [vp, vp, u32]
         L.or_get_snapshot.argtypes = [vp, u32, vp]
         L.or_get_manifold.restype = u32
@@ -159,6 +163,26 @@ class OracleWorld:
         return {"iterations": int(u[0]), "chosen": int(u[1]), "converged": int(u[2]),
                 "s0": float(d[0]), "sk": float(d[1]),
                 "relative_residual": float(np.sqrt(d[1] / d[0])) if d[0] > 0 else 0.0}
+
+    def closure_stats(self) -> dict:
+        """Closure solve outcome of the last step (MK_CLOSURE_PCG_RESIDUAL)."""
+        u = np.zeros(4, np.uint32)
+        d = np.zeros(1, np.float64)
+        lib().or_get_closure_stats(self.h, _p(u), _p(d))
+        return {"newton_steps": int(u[0]), "pcg_iterations": int(u[1]), "learned_blocks": int(u[2]),
+                "rejected_blocks": int(u[3]), "max_relative_residual": float(d[0])}
+
+    def set_precond_outputs(self, out) -> None:
+        """Preconditioner network outputs (12 x blocks x 3) for the next step."""
+        out = np.ascontiguousarray(out, np.float32).ravel()
+        lib().or_set_precond_outputs(self.h, _p(out), len(out))
+
+    def closure_blocks(self):
+        n = int(lib().or_get_closure_blocks(self.h, None))
+        out = np.zeros((n, 16), np.float32)
+        if n:
+            lib().or_get_closure_blocks(self.h, _p(out))
+        return out
 
     def set_warm_predictions(self, pred) -> None:
         """Learned warm-start impulses, by active position, for the next step's solve."""

@@ -16,6 +16,8 @@
 #include <cstdint>
 #include <cstring>
 #include <unordered_map>
+#include <limits>
+#include <map>
 #include <vector>
 
 #ifdef _OPENMP
@@ -65,6 +67,7 @@ template <class T> static inline T tsin(T x) { return T(std::sin(double(x))); }
 template <class T> static inline T tcos(T x) { return T(std::cos(double(x))); }
 template <class T> static inline T tacos(T x) { return T(std::acos(double(x))); }
 template <class T> static inline T tatan2(T y, T x) { return T(std::atan2(double(y), double(x))); }
+template <class T> static inline T tlog(T x) { return T(std::log(double(x))); }
 
 // physics.wgsl:46-56, collision.wgsl:97-107 (identical in every kernel file).
 template <class T> static inline V4<T> quat_multiply(V4<T> a, V4<T> b) {
@@ -1344,11 +1347,412 @@ template <class T> struct World : WorldBase {
         }
     }
 
+    // ------------------------------------------ closure PCG to a residual
+    // MK_CLOSURE_PCG_RESIDUAL: per Newton step, PCG on (J^T J) dtheta = -g
+    // until ||r|| <= tol ||r0|| with FP64 dot products summed in the order
+    // of the GPU's 1024-thread block (strided partials, warp shuffle-down
+    // trees, warp 0 over the warp sums); block Jacobi over 2 x 2 blocks of
+    // consecutive closure coordinates, optionally replaced per block by the
+    // network's output (given from outside, per Newton step).
+    uint32_t closure_mode = 0, closure_max_it = 256, learned_precond = 0, precond = 0;
+    std::vector<uint32_t> loop_off, loop_q;
+    std::vector<T> loop_l;   // 36 per loop
+    float closure_tol = 1.0e-5f;
+    struct ClosureTopo {
+        std::vector<uint32_t> cl_bearings, cl_slot_off, cl_split, slot_body, slot_closure, cq_coords, cq_off, cq_slots;
+        bool built = false;
+    } ct;
+    std::vector<V3<T>> slot_pd, slot_ad;
+    std::vector<uint32_t> slot_coord;
+    std::vector<T> slot_g, slot_d, probe1, probe2;
+    struct Blk { T m11, m12, m22; };
+    std::vector<Blk> blk_m;
+    std::vector<float> blk_feat;        // 16 per block
+    std::vector<float> precond_outputs; // 12 x blocks x 3 (learned)
+    struct ClosureStats { uint32_t newton_steps = 0, pcg_iterations = 0, learned = 0, rejected = 0; double max_rel = 0; } cstats;
+
+    void build_closure_topology() {
+        if (ct.built) return;
+        ct.built = true;
+        std::map<uint32_t, std::vector<uint32_t>> coord_slots;
+        ct.cl_slot_off.push_back(0);
+        for (uint32_t j = 0; j < J; ++j) {
+            const Bearing<T>& br = bear[j];
+            if (br.meta[3] == 0) continue;
+            const uint32_t k = (uint32_t)ct.cl_bearings.size();
+            ct.cl_bearings.push_back(j);
+            for (int side = 0; side < 2; ++side) {
+                if (side == 1) ct.cl_split.push_back((uint32_t)ct.slot_body.size());
+                uint32_t body = br.meta[side];
+                for (uint32_t guard = 0; guard <= B && body < B; ++guard) {
+                    if (mech[body].meta[3] != 0) break;
+                    const uint32_t coord = bear[mech[body].meta[1]].meta[2];
+                    coord_slots[coord].push_back((uint32_t)ct.slot_body.size());
+                    ct.slot_body.push_back(body);
+                    ct.slot_closure.push_back(k);
+                    body = mech[body].meta[0];
+                }
+            }
+            ct.cl_slot_off.push_back((uint32_t)ct.slot_body.size());
+        }
+        ct.cq_off.push_back(0);
+        for (auto& kv : coord_slots) {
+            ct.cq_coords.push_back(kv.first);
+            for (uint32_t sl : kv.second) ct.cq_slots.push_back(sl);
+            ct.cq_off.push_back((uint32_t)ct.cq_slots.size());
+        }
+        // per-loop blocks (first closure containing a coordinate; pieces of at most 8)
+        std::map<uint32_t, uint32_t> position;
+        for (uint32_t q = 0; q < ct.cq_coords.size(); ++q) position[ct.cq_coords[q]] = q;
+        std::vector<uint8_t> taken(ct.cq_coords.size(), 0);
+        loop_off.assign(1, 0);
+        loop_q.clear();
+        for (size_t k = 0; k + 1 < ct.cl_slot_off.size(); ++k) {
+            std::vector<uint32_t> qs;
+            for (uint32_t sl = ct.cl_slot_off[k]; sl < ct.cl_slot_off[k + 1]; ++sl) {
+                const uint32_t coord = bear[mech[ct.slot_body[sl]].meta[1]].meta[2];
+                auto it = position.find(coord);
+                if (it == position.end() || taken[it->second]) continue;
+                taken[it->second] = 1;
+                qs.push_back(it->second);
+            }
+            std::sort(qs.begin(), qs.end());
+            for (size_t i = 0; i < qs.size(); i += 8) {
+                for (size_t j = i; j < std::min<size_t>(qs.size(), i + 8); ++j) loop_q.push_back(qs[j]);
+                loop_off.push_back((uint32_t)loop_q.size());
+            }
+        }
+    }
+    static double block_sum_1024(const std::vector<double>& part) {   // part: 1024 per-thread partials
+        double warp[32];
+        for (int w = 0; w < 32; ++w) {
+            double v[32];
+            for (int l = 0; l < 32; ++l) v[l] = part[32 * w + l];
+            for (int o = 16; o > 0; o >>= 1) {
+                double nv[32];
+                for (int l = 0; l < 32; ++l) nv[l] = v[l] + (l + o < 32 ? v[l + o] : v[l]);
+                std::memcpy(v, nv, sizeof(v));
+            }
+            warp[w] = v[0];
+        }
+        double v[32];
+        std::memcpy(v, warp, sizeof(v));
+        for (int o = 16; o > 0; o >>= 1) {
+            double nv[32];
+            for (int l = 0; l < 32; ++l) nv[l] = v[l] + (l + o < 32 ? v[l + o] : v[l]);
+            std::memcpy(v, nv, sizeof(v));
+        }
+        return v[0];
+    }
+    template <class F> double closure_dot_d(F term) const {   // term(q) -> double
+        std::vector<double> part(1024, 0.0);
+        const uint32_t NQ = (uint32_t)ct.cq_coords.size();
+        for (uint32_t t = 0; t < 1024; ++t)
+            for (uint32_t q = t; q < NQ; q += 1024) part[t] += term(q);
+        return block_sum_1024(part);
+    }
+    void closure_apply(const std::vector<T>& x, std::vector<T>& out) {
+        const uint32_t NC = (uint32_t)ct.cl_bearings.size();
+        for (uint32_t k = 0; k < NC; ++k) {
+            const uint32_t s0 = ct.cl_slot_off[k], s1 = ct.cl_slot_off[k + 1], split = ct.cl_split[k];
+            V3<T> pp[2] = {v3<T>(0, 0, 0), v3<T>(0, 0, 0)}, pa[2] = {v3<T>(0, 0, 0), v3<T>(0, 0, 0)};
+            for (uint32_t sl = s0; sl < s1; ++sl) {
+                const int side = sl < split ? 0 : 1;
+                const T dv = x[slot_coord[sl]];
+                pp[side] = pp[side] + slot_pd[sl] * dv;
+                pa[side] = pa[side] + slot_ad[sl] * dv;
+            }
+            const V3<T> P = pp[0] + pp[1], A = pa[0] + pa[1];
+            for (uint32_t sl = s0; sl < s1; ++sl) slot_g[sl] = dot(slot_pd[sl], P) + T(1) * dot(slot_ad[sl], A);
+        }
+        for (size_t q = 0; q < ct.cq_coords.size(); ++q) {
+            T o = T(0);
+            for (uint32_t i = ct.cq_off[q]; i < ct.cq_off[q + 1]; ++i) o += slot_g[ct.cq_slots[i]];
+            out[ct.cq_coords[q]] = o;
+        }
+    }
+    T closure_coupling(uint32_t qi, uint32_t qj) const {
+        T r = T(0);
+        for (uint32_t a = ct.cq_off[qi]; a < ct.cq_off[qi + 1]; ++a) {
+            const uint32_t sa = ct.cq_slots[a];
+            for (uint32_t b = ct.cq_off[qj]; b < ct.cq_off[qj + 1]; ++b) {
+                const uint32_t sb = ct.cq_slots[b];
+                if (ct.slot_closure[sa] != ct.slot_closure[sb]) continue;
+                r += dot(slot_pd[sa], slot_pd[sb]) + T(1) * dot(slot_ad[sa], slot_ad[sb]);
+            }
+        }
+        return r;
+    }
+    // returns false once converged
+    bool closure_eval_step() {
+        const uint32_t NC = (uint32_t)ct.cl_bearings.size(), NS = (uint32_t)ct.slot_body.size();
+        const uint32_t NQ = (uint32_t)ct.cq_coords.size(), NBK = (NQ + 1) / 2;
+        slot_pd.assign(NS, v3<T>(0, 0, 0)); slot_ad.assign(NS, v3<T>(0, 0, 0)); slot_coord.assign(NS, 0);
+        slot_g.assign(NS, T(0)); slot_d.assign(NS, T(0));
+        closure_state[0] = closure_state[1] = 0;
+        auto finite3 = [](V3<T> v) {
+            const T lim = T(3.402823e+38f);
+            return v.x == v.x && v.y == v.y && v.z == v.z && std::fabs(v.x) < lim && std::fabs(v.y) < lim &&
+                   std::fabs(v.z) < lim;
+        };
+        for (uint32_t k = 0; k < NC; ++k) {
+            const Bearing<T>& br = bear[ct.cl_bearings[k]];
+            V3<T> aa, ab, xa, xb;
+            closure_frames(br, aa, ab, xa, xb);
+            V3<T> rp = aa - ab, ra = xa - xb;
+            bool active = true;
+            if (!finite3(rp) || !finite3(ra)) {
+                diag.error_flags |= MK_INVALID_NUMERIC_FLAG;
+                closure_state[0] = closure_state[1] = 0xffffffffu;
+                active = false;
+            } else {
+                uint32_t um = round_u32(length(rp) * T(1000000.0f));
+                T deg = tatan2(length(cross(xa, xb)), clampv(dot(xa, xb), T(-1), T(1))) * T(57.295779513f);
+                uint32_t ud = round_u32(deg * T(1000000.0f));
+                closure_state[0] = std::max(closure_state[0], um);
+                closure_state[1] = std::max(closure_state[1], ud);
+                active = !(um <= 10u && ud <= 1000u);
+            }
+            const uint32_t s0 = ct.cl_slot_off[k], s1 = ct.cl_slot_off[k + 1], split = ct.cl_split[k];
+            for (uint32_t sl = s0; sl < s1; ++sl) {
+                const bool side_a = sl < split;
+                const V3<T> ea = side_a ? aa : ab, ex = side_a ? xa : xb;
+                const T sign = side_a ? T(1) : T(-1);
+                V3<T> axis, anchor; uint32_t coord, parent;
+                joint_frame(ct.slot_body[sl], axis, anchor, coord, parent);
+                bool valid = false;
+                T g = T(0), d = T(0);
+                if (coord >= Q) { diag.error_flags |= MK_INVALID_NUMERIC_FLAG; coord = 0; }
+                else {
+                    slot_pd[sl] = cross(axis, ea - anchor) * sign;
+                    slot_ad[sl] = cross(axis, ex) * sign;
+                    if (active) {
+                        g = dot(rp, slot_pd[sl]) + T(1) * dot(ra, slot_ad[sl]);
+                        d = dot(slot_pd[sl], slot_pd[sl]) + T(1) * dot(slot_ad[sl], slot_ad[sl]);
+                        if (g == g && d == d) valid = true;
+                        else diag.error_flags |= MK_INVALID_NUMERIC_FLAG;
+                    }
+                }
+                slot_coord[sl] = coord;
+                slot_g[sl] = valid ? g : std::numeric_limits<T>::quiet_NaN();
+                slot_d[sl] = valid ? d : T(0);
+            }
+        }
+        for (uint32_t q = 0; q < NQ; ++q) {
+            T g = T(0), d = T(0);
+            for (uint32_t i = ct.cq_off[q]; i < ct.cq_off[q + 1]; ++i) {
+                const uint32_t sl = ct.cq_slots[i];
+                if (slot_g[sl] == slot_g[sl]) { g += slot_g[sl]; d += slot_d[sl]; }
+            }
+            grad[ct.cq_coords[q]] = g;
+            dgl[ct.cq_coords[q]] = d;
+        }
+        const bool unconverged = closure_state[0] > 10u || closure_state[1] > 1000u;
+        std::vector<T> ones(Q, T(0)), alt(Q, T(0));
+        for (uint32_t q = 0; q < NQ; ++q) { ones[ct.cq_coords[q]] = T(1); alt[ct.cq_coords[q]] = (q & 1u) ? T(-1) : T(1); }
+        probe1.assign(Q, T(0)); probe2.assign(Q, T(0));
+        closure_apply(ones, probe1);
+        closure_apply(alt, probe2);
+        blk_m.assign(NBK, Blk{T(0), T(0), T(0)});
+        blk_feat.assign(16ull * NBK, 0.0f);
+        std::vector<T> blk_b(NBK, T(0));
+        for (uint32_t blk = 0; blk < NBK; ++blk) {
+            const uint32_t qi = 2 * blk, qj = qi + 1;
+            const bool pair = qj < NQ;
+            const T a = dgl[ct.cq_coords[qi]], d = pair ? dgl[ct.cq_coords[qj]] : T(0);
+            const T bij = pair ? closure_coupling(qi, qj) : T(0);
+            Blk inv{a > T(1.0e-12f) ? T(1) / a : T(0), T(0), d > T(1.0e-12f) ? T(1) / d : T(0)};
+            if (pair && a > T(1.0e-12f) && d > T(1.0e-12f)) {
+                const T det = a * d - bij * bij;
+                if (det > T(1.0e-6f) * (a * d)) inv = Blk{d / det, -bij / det, a / det};
+            }
+            blk_m[blk] = inv;
+            blk_b[blk] = bij;
+        }
+        for (uint32_t blk = 0; blk < NBK; ++blk) {
+            float* f = &blk_feat[16ull * blk];
+            f[15] = 1.0f;
+            const uint32_t qi = 2 * blk, qj = qi + 1;
+            const uint32_t ci = ct.cq_coords[qi];
+            const bool pair = qj < NQ;
+            const uint32_t cj = pair ? ct.cq_coords[qj] : ci;
+            const T a = dgl[ci], d = pair ? dgl[cj] : T(0), bij = blk_b[blk];
+            const uint32_t pb = blk ^ 1u;
+            const bool partner = pb < NBK && 2 * pb + 1 < NQ;
+            if (pair && partner && a > T(1.0e-12f) && d > T(1.0e-12f)) {
+                const T pa = dgl[ct.cq_coords[2 * pb]], pd = dgl[ct.cq_coords[2 * pb + 1]];
+                if (pa > T(1.0e-12f) && pd > T(1.0e-12f)) {
+                    const T s1i = probe1[ci] - a - bij, ssi = probe2[ci] - a + bij;
+                    const T s1j = probe1[cj] - bij - d, ssj = probe2[cj] - bij + d;
+                    const T sa = std::sqrt(a), sd = std::sqrt(d), spa = std::sqrt(pa), spd = std::sqrt(pd);
+                    f[0] = (float)(bij / (sa * sd)); f[1] = (float)(blk_b[pb] / (spa * spd));
+                    f[2] = (float)(T(0.5f) * (s1i + ssi) / (sa * spa)); f[3] = (float)(T(0.5f) * (s1i - ssi) / (sa * spd));
+                    f[4] = (float)(T(0.5f) * (s1j + ssj) / (sd * spa)); f[5] = (float)(T(0.5f) * (s1j - ssj) / (sd * spd));
+                    f[6] = (float)tlog(a / d); f[7] = 1.0f;
+                }
+            }
+        }
+        if (precond == MK_PRECOND_BLOCK_JACOBI) {
+            const uint32_t NL = (uint32_t)loop_off.size() - 1;
+            loop_l.assign(36ull * NL, T(0));
+            for (uint32_t lp = 0; lp < NL; ++lp) {
+                const uint32_t o = loop_off[lp], n = loop_off[lp + 1] - o;
+                T a[36];
+                T mean = T(0);
+                for (uint32_t i = 0; i < n; ++i) mean += dgl[ct.cq_coords[loop_q[o + i]]];
+                mean = n ? mean / T(n) : T(0);
+                for (uint32_t i = 0; i < n; ++i)
+                    for (uint32_t j = 0; j <= i; ++j)
+                        a[i * (i + 1) / 2 + j] = i == j ? dgl[ct.cq_coords[loop_q[o + i]]] + T(1.0e-6f) * mean
+                                                        : closure_coupling(loop_q[o + i], loop_q[o + j]);
+                bool ok = mean > T(1.0e-12f);
+                for (uint32_t j = 0; j < n && ok; ++j) {
+                    T dj = a[j * (j + 1) / 2 + j];
+                    for (uint32_t k = 0; k < j; ++k) dj -= a[j * (j + 1) / 2 + k] * a[j * (j + 1) / 2 + k];
+                    if (!(dj > T(0))) { ok = false; break; }
+                    const T ljj = std::sqrt(dj);
+                    a[j * (j + 1) / 2 + j] = ljj;
+                    for (uint32_t i = j + 1; i < n; ++i) {
+                        T v = a[i * (i + 1) / 2 + j];
+                        for (uint32_t k = 0; k < j; ++k) v -= a[i * (i + 1) / 2 + k] * a[j * (j + 1) / 2 + k];
+                        a[i * (i + 1) / 2 + j] = v / ljj;
+                    }
+                }
+                T* l = &loop_l[36ull * lp];
+                for (uint32_t i = 0; i < n; ++i)
+                    for (uint32_t j = 0; j <= i; ++j) {
+                        T v = a[i * (i + 1) / 2 + j];
+                        if (!ok) {
+                            const T dii = dgl[ct.cq_coords[loop_q[o + i]]];
+                            v = (i == j) ? (dii > T(1.0e-12f) ? std::sqrt(dii) : T(0)) : T(0);
+                        }
+                        l[i * (i + 1) / 2 + j] = v;
+                    }
+            }
+        }
+        return unconverged;
+    }
+    void closure_pcg_step(uint32_t step) {
+        const uint32_t NQ = (uint32_t)ct.cq_coords.size(), NBK = (NQ + 1) / 2;
+        if (learned_precond) {
+            for (uint32_t blk = 0; blk < NBK; ++blk) {
+                const size_t o = 3ull * ((size_t)step * NBK + blk);
+                const T t11 = o + 2 < precond_outputs.size() ? T(precond_outputs[o]) : T(0);
+                const T t12 = o + 2 < precond_outputs.size() ? T(precond_outputs[o + 1]) : T(0);
+                const T t22 = o + 2 < precond_outputs.size() ? T(precond_outputs[o + 2]) : T(0);
+                const uint32_t qi = 2 * blk, qj = qi + 1;
+                const uint32_t ci = ct.cq_coords[qi];
+                const bool pair = qj < NQ;
+                const T a = dgl[ci], d = pair ? dgl[ct.cq_coords[qj]] : T(0);
+                if (pair) {
+                    if (a > T(1.0e-12f) && d > T(1.0e-12f) && t11 > T(0) && t22 > T(0) &&
+                        t11 * t22 - t12 * t12 > T(1.0e-6f) * (t11 * t22)) {
+                        const T sa = std::sqrt(a), sd = std::sqrt(d);
+                        blk_m[blk] = Blk{t11 / a, t12 / (sa * sd), t22 / d};
+                        ++cstats.learned;
+                    } else ++cstats.rejected;
+                } else if (a > T(1.0e-12f) && t11 > T(0)) {
+                    blk_m[blk] = Blk{t11 / a, T(0), T(0)};
+                    ++cstats.learned;
+                } else ++cstats.rejected;
+            }
+        }
+        std::vector<T> sol(Q, T(0)), res(Q, T(0)), pre(Q, T(0)), dir(Q, T(0)), op(Q, T(0));
+        auto precond = [&]() {
+            if (this->precond == MK_PRECOND_BLOCK_JACOBI) {
+                const uint32_t NL = (uint32_t)loop_off.size() - 1;
+                for (uint32_t lp = 0; lp < NL; ++lp) {
+                    const uint32_t o = loop_off[lp], n = loop_off[lp + 1] - o;
+                    const T* l = &loop_l[36ull * lp];
+                    T y[8];
+                    for (uint32_t i = 0; i < n; ++i) {
+                        T v = res[ct.cq_coords[loop_q[o + i]]];
+                        for (uint32_t k = 0; k < i; ++k) v -= l[i * (i + 1) / 2 + k] * y[k];
+                        const T lii = l[i * (i + 1) / 2 + i];
+                        y[i] = lii > T(0) ? v / lii : T(0);
+                    }
+                    for (uint32_t ii = n; ii-- > 0;) {
+                        T v = y[ii];
+                        for (uint32_t k = ii + 1; k < n; ++k) v -= l[k * (k + 1) / 2 + ii] * y[k];
+                        const T lii = l[ii * (ii + 1) / 2 + ii];
+                        y[ii] = lii > T(0) ? v / lii : T(0);
+                    }
+                    for (uint32_t i = 0; i < n; ++i) pre[ct.cq_coords[loop_q[o + i]]] = y[i];
+                }
+                return;
+            }
+            for (uint32_t blk = 0; blk < NBK; ++blk) {
+                const Blk& mi = blk_m[blk];
+                const uint32_t qi = 2 * blk, qj = qi + 1;
+                const uint32_t ci = ct.cq_coords[qi];
+                if (qj < NQ) {
+                    const uint32_t cj = ct.cq_coords[qj];
+                    const T ri = res[ci], rj = res[cj];
+                    pre[ci] = mi.m11 * ri + mi.m12 * rj;
+                    pre[cj] = mi.m12 * ri + mi.m22 * rj;
+                } else {
+                    pre[ci] = mi.m11 * res[ci];
+                }
+            }
+        };
+        for (uint32_t q = 0; q < NQ; ++q) { const uint32_t c = ct.cq_coords[q]; sol[c] = T(0); res[c] = -grad[c]; }
+        precond();
+        for (uint32_t q = 0; q < NQ; ++q) { const uint32_t c = ct.cq_coords[q]; dir[c] = pre[c]; }
+        auto cq = [&](uint32_t q) { return ct.cq_coords[q]; };
+        double rz = closure_dot_d([&](uint32_t q) { return (double)res[cq(q)] * (double)pre[cq(q)]; });
+        const double rr0 = closure_dot_d([&](uint32_t q) { return (double)res[cq(q)] * (double)res[cq(q)]; });
+        double rr = rr0;
+        const double tol2 = (double)closure_tol * (double)closure_tol;
+        uint32_t it = 0;
+        while (it < closure_max_it && rr > tol2 * rr0) {
+            closure_apply(dir, op);
+            const double pq = closure_dot_d([&](uint32_t q) { return (double)dir[cq(q)] * (double)op[cq(q)]; });
+            const T alpha = std::fabs(pq) > 1.0e-30 ? T(rz / pq) : T(0);
+            for (uint32_t q = 0; q < NQ; ++q) {
+                const uint32_t c = cq(q);
+                sol[c] += alpha * dir[c];
+                res[c] -= alpha * op[c];
+            }
+            rr = closure_dot_d([&](uint32_t q) { return (double)res[cq(q)] * (double)res[cq(q)]; });
+            ++it;
+            if (rr <= tol2 * rr0) break;
+            precond();
+            const double nrz = closure_dot_d([&](uint32_t q) { return (double)res[cq(q)] * (double)pre[cq(q)]; });
+            const T beta = std::fabs(rz) > 1.0e-300 ? T(nrz / rz) : T(0);
+            for (uint32_t q = 0; q < NQ; ++q) { const uint32_t c = cq(q); dir[c] = pre[c] + beta * dir[c]; }
+            rz = nrz;
+        }
+        cstats.pcg_iterations += it;
+        const double rel = rr0 > 0.0 ? std::sqrt(rr / rr0) : 0.0;
+        cstats.max_rel = std::max(cstats.max_rel, rel);
+        for (uint32_t q = 0; q < NQ; ++q) {
+            const uint32_t c = cq(q);
+            T st = clampv(T(0.35f) * sol[c], T(-0.2f), T(0.2f));
+            if (st == st) coords[c].x += st;
+            else diag.error_flags |= MK_INVALID_NUMERIC_FLAG;
+        }
+    }
+    void closure_loop_pcg() {
+        build_closure_topology();
+        cstats = ClosureStats{};
+        for (uint32_t step = 0; step < 12; ++step) {
+            std::fill(grad.begin(), grad.end(), T(0));
+            std::fill(dgl.begin(), dgl.end(), T(0));
+            if (!closure_eval_step()) break;
+            ++cstats.newton_steps;
+            closure_pcg_step(step);
+            forward_kinematics();
+        }
+    }
+
     void mechanism_passes() {   // device.rs:963-1048
         for (uint32_t it = 0; it < std::max(1u, iterations); ++it) bearing_projection_iteration();
         advance_coordinates();
         forward_kinematics();
-        if (closure_count > 0) closure_loop();
+        if (closure_count > 0) {
+            if (closure_mode == MK_CLOSURE_PCG_RESIDUAL) closure_loop_pcg();
+            else closure_loop();
+        }
         publish();
         reconstruct_body_velocities();
     }
@@ -1527,6 +1931,11 @@ static World<T>* build_world(const MkCreation* cr, const MkConfig* cfg, uint32_t
     w->pair_capacity = pair_capacity ? pair_capacity : MK_DEFAULT_MAX_CONTACT_PAIRS;
     w->contact_tol = c.contact_tolerance > 0.0f ? c.contact_tolerance : 0.0f;
     w->contact_max_it = c.contact_max_iterations ? c.contact_max_iterations : 512u;
+    w->closure_mode = c.closure_mode;
+    w->closure_tol = c.closure_tolerance > 0.0f ? c.closure_tolerance : 1.0e-5f;
+    w->closure_max_it = c.closure_max_iterations ? c.closure_max_iterations : 256u;
+    w->learned_precond = (c.closure_mode == MK_CLOSURE_PCG_RESIDUAL && c.preconditioner == MK_PRECOND_LEARNED) ? 1u : 0u;
+    w->precond = c.preconditioner;
     uint32_t B = w->B, C = w->C;
     w->pos.resize(B); w->rot.resize(B); w->lin.resize(B); w->ang.resize(B);
     w->inv_mass.resize(B); w->mass.resize(B); w->root.resize(B); w->components.resize(B);
@@ -1717,6 +2126,21 @@ void or_get_diagnostics(const OrWorld* o, GpuDiagnostics* out) { BOTH(*out = w->
 void or_get_solve_stats(const OrWorld* o, uint32_t* u3, double* d2) {
     BOTH((u3[0] = w->stats.iterations, u3[1] = w->stats.chosen, u3[2] = w->stats.converged,
           d2[0] = w->stats.s0, d2[1] = w->stats.sk));
+}
+// Closure PCG outcome of the last step: newton steps, pcg iterations, learned, rejected blocks; max rel residual.
+void or_get_closure_stats(const OrWorld* o, uint32_t* u4, double* d1) {
+    BOTH((u4[0] = w->cstats.newton_steps, u4[1] = w->cstats.pcg_iterations, u4[2] = w->cstats.learned,
+          u4[3] = w->cstats.rejected, d1[0] = w->cstats.max_rel));
+}
+// Preconditioner network outputs (12 x blocks x 3) for the next step.
+void or_set_precond_outputs(OrWorld* o, const float* out, uint32_t n) {
+    BOTH(w->precond_outputs.assign(out, out + n));
+}
+// Block inputs of the last evaluated Newton step (blocks x 16).
+uint32_t or_get_closure_blocks(const OrWorld* o, float* out) {
+    uint32_t n = 0;
+    BOTH((n = (uint32_t)w->blk_feat.size() / 16, out ? (void)std::copy(w->blk_feat.begin(), w->blk_feat.end(), out) : (void)0));
+    return n;
 }
 // Learned warm-start impulses (by active position) for the next step's solve.
 void or_set_warm_predictions(OrWorld* o, const float* pred, uint32_t n) {
