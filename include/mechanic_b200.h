@@ -385,6 +385,24 @@ MK_API int mk_create(const MkCreation* creation, const MkConfig* config,
 
 MK_API void mk_destroy(MkHandle* handle);
 
+/* Batched independent scenes (no reference counterpart): `scene_count`
+ * creations stepped together by every launch of one handle.  Rows are
+ * concatenated scene by scene with their body, bearing, coordinate and
+ * mechanism-component indices offset; colliders of different scenes never
+ * pair (each collider's sorted key carries its scene index in the top bits
+ * and the traversal stops at its scene's last leaf), while all other stages
+ * run over the concatenated rows as one scene.  Snapshots, state buffers and
+ * readbacks are the concatenated arrays; mk_scene_offsets gives the slices.
+ * Error flags and counts are totals over the batch; a contact or closure
+ * tolerance applies to the batch's joint residual.  Capacities apply to the
+ * totals. */
+MK_API int mk_create_batch(const MkCreation* scenes, uint32_t scene_count, const MkConfig* config,
+                           const MkCapacities* capacities, MkHandle** out, MkError* err);
+/* Body and collider offset of each scene plus the totals (scene_count + 1 entries each,
+ * at most `capacity` written); returns the scene count (1 for mk_create handles). */
+MK_API int mk_scene_offsets(const MkHandle* handle, uint32_t* body_offsets, uint32_t* collider_offsets,
+                            uint32_t capacity);
+
 /* GpuPhysics::dispatch_tick (device.rs:859-961): asynchronous on the
  * handle's stream; errors surface through GpuDiagnostics flags. */
 MK_API int mk_dispatch_tick(MkHandle* handle, uint64_t tick_index, MkSubmission* out);

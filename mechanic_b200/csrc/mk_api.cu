@@ -92,6 +92,9 @@ struct MkHandle {
     bool any_tick = false;
     uint32_t kernels_per_tick = 0;
     std::vector<uint32_t> mech_level_offsets;   // host side of MechBuffers::level_offsets
+    std::vector<uint32_t> scene_body_offsets;      // batched scenes: body / collider offset per scene (+ totals)
+    std::vector<uint32_t> scene_collider_offsets;
+    uint32_t scene_count = 0;
 };
 
 namespace {
@@ -165,6 +168,10 @@ uint64_t carve(MkHandle* h, char* base) {
     b.diag = c.take<GpuDiagnostics>(1);
     b.tick = c.take<mk::DevTick>(1);
     b.counts = c.take<mk::DevCounts>(1);
+    if (h->scene_count > 1) {
+        b.collider_scene = c.take<uint32_t>(C);
+        b.scene_end = c.take<uint32_t>(h->scene_count);
+    }
     b.sort_scratch_bytes = mk::sort_scratch_bytes(C, 63);
     b.sort_scratch = c.take<char>(b.sort_scratch_bytes);
     h->staging = c.take<float4>(2ull * B);
@@ -338,37 +345,153 @@ void destroy_handle(MkHandle* h) {
     delete h;
 }
 
-}  // namespace
+// Several independent scenes as one creation: rows concatenated scene by
+// scene with their indices offset (bodies, bearings, coordinates, mechanism
+// components); each collider keeps the index of its scene.
+struct Batch {
+    MkCreation creation{};
+    std::vector<GpuTransform> transforms;
+    std::vector<GpuVelocity> velocities;
+    std::vector<GpuMass> masses;
+    std::vector<GpuSpatialInertia> inertias;
+    std::vector<GpuCollider> colliders;
+    std::vector<GpuBearing> bearings;
+    std::vector<GpuPair> suppressed;
+    std::vector<GpuMechanismBody> mech;
+    std::vector<uint32_t> roots, preorder, components;
+    std::vector<GpuMechanismDrive> drives;
+    std::vector<uint32_t> collider_scene, body_offsets, collider_offsets;
+    uint32_t scene_count = 0;
+};
 
-extern "C" {
-
-void mk_config_default(MkConfig* c) {
-    if (!c) return;
-    std::memset(c, 0, sizeof(*c));
-    c->collisions_enabled = 1;
-    c->mechanism_self_collisions = 1;
-    c->solver_iterations = 8;
-    c->morton_mode = MK_MORTON_63;
-    c->closure_mode = MK_CLOSURE_REFERENCE;
-    c->use_graph = 1;
-}
-
-const char* mk_version(void) { return "mechanic_b200 0.1.0 sm_100a"; }
-
-int mk_set_tuning(uint32_t key, uint32_t value) {
-    static uint32_t sort_items = 0;
-    if (key == MK_TUNE_SORT_ITEMS) {
-        const uint32_t prev = sort_items;
-        sort_items = value;
-        mk::set_sort_items(value);
-        return (int)prev;
+bool concatenate(const MkCreation* sc, uint32_t n, Batch& out, std::string& why) {
+    uint64_t B = 0, C = 0, J = 0, S = 0, Q = 0;
+    bool any_vel = false, any_inertia = false, any_mech = false;
+    for (uint32_t i = 0; i < n; ++i) {
+        const MkCreation& c = sc[i];
+        if (c.body_count == 0 || !c.transforms || !c.masses || (c.collider_count && !c.colliders) ||
+            (c.bearing_count && !c.bearings) || (c.suppression_count && !c.suppressed_pairs) ||
+            (c.max_depth > 0 && (!c.mechanism_bodies || !c.preorder))) {
+            char msg[128];
+            std::snprintf(msg, sizeof(msg), "scene %u: creation arrays missing for the given counts", i);
+            why = msg;
+            return false;
+        }
+        B += c.body_count; C += c.collider_count; J += c.bearing_count; S += c.suppression_count;
+        Q += c.coordinate_count;
+        any_vel |= c.velocities != nullptr;
+        any_inertia |= c.spatial_inertias != nullptr;
+        any_mech |= c.max_depth > 0;
     }
-    return -1;
+    if (B > 0xffffffffull || C > 0xffffffffull || J > 0xffffffffull) {
+        why = "batch exceeds 2^32 rows";
+        return false;
+    }
+    out.scene_count = n;
+    MkCreation& r = out.creation;
+    std::memset(&r, 0, sizeof(r));
+    uint32_t bo = 0, co = 0, jo = 0, qo = 0, comp_o = 0;
+    for (uint32_t i = 0; i < n; ++i) {
+        const MkCreation& c = sc[i];
+        out.body_offsets.push_back(bo);
+        out.collider_offsets.push_back(co);
+        out.transforms.insert(out.transforms.end(), c.transforms, c.transforms + c.body_count);
+        if (any_vel) {
+            if (c.velocities) out.velocities.insert(out.velocities.end(), c.velocities, c.velocities + c.body_count);
+            else out.velocities.resize(out.velocities.size() + c.body_count, GpuVelocity{});
+        }
+        out.masses.insert(out.masses.end(), c.masses, c.masses + c.body_count);
+        if (any_inertia) {
+            if (c.spatial_inertias)
+                out.inertias.insert(out.inertias.end(), c.spatial_inertias, c.spatial_inertias + c.body_count);
+            else out.inertias.resize(out.inertias.size() + c.body_count, GpuSpatialInertia{});
+        }
+        for (uint32_t k = 0; k < c.collider_count; ++k) {
+            GpuCollider g = c.colliders[k];
+            g.metadata[0] += bo;
+            out.colliders.push_back(g);
+            out.collider_scene.push_back(i);
+        }
+        for (uint32_t k = 0; k < c.bearing_count; ++k) {
+            GpuBearing g = c.bearings[k];
+            g.metadata[0] += bo;
+            g.metadata[1] += bo;
+            if (g.metadata[2] != 0xffffffffu) g.metadata[2] += qo;
+            out.bearings.push_back(g);
+        }
+        for (uint32_t k = 0; k < c.suppression_count; ++k) {
+            GpuPair g = c.suppressed_pairs[k];
+            g.collider_a += bo;   // suppression rows hold body pairs (lbvh.wgsl:325-345)
+            g.collider_b += bo;
+            out.suppressed.push_back(g);
+        }
+        uint32_t comp_max = 0;
+        for (uint32_t k = 0; k < c.body_count; ++k) {
+            const uint32_t comp = c.body_components ? c.body_components[k] : k;
+            out.components.push_back(comp + comp_o);
+            comp_max = std::max(comp_max, comp + 1);
+            out.roots.push_back(c.root_flags ? c.root_flags[k] : 1u);
+        }
+        if (any_mech) {
+            for (uint32_t k = 0; k < c.body_count; ++k) {
+                GpuMechanismBody g{};
+                if (c.max_depth > 0) {
+                    g = c.mechanism_bodies[k];
+                    g.metadata[0] += bo;
+                    if (g.metadata[1] != 0xffffffffu) g.metadata[1] += jo;
+                    g.traversal[0] += comp_o;
+                    g.traversal[2] += bo;
+                    g.traversal[3] += bo;
+                    out.preorder.push_back(c.preorder[k] + bo);
+                } else {   // a free body: its own root (device.rs:1699-1760 for a body without bearings)
+                    g.metadata[0] = bo + k;
+                    g.metadata[1] = 0xffffffffu;
+                    g.metadata[3] = 1u;
+                    g.traversal[0] = (c.body_components ? c.body_components[k] : k) + comp_o;
+                    g.traversal[2] = bo + k;
+                    g.traversal[3] = bo + k;
+                    g.bind_relative_rotation[3] = 1.0f;
+                    out.preorder.push_back(bo + k);
+                }
+                out.mech.push_back(g);
+            }
+        }
+        for (uint32_t k = 0; k < c.coordinate_count; ++k) {
+            GpuMechanismDrive d{};
+            if (c.drives) d = c.drives[k];
+            else { d.min_angle = -INFINITY; d.max_angle = INFINITY; }   // GpuMechanismDrive::PASSIVE (abi.rs:266-275)
+            out.drives.push_back(d);
+        }
+        r.max_depth = std::max(r.max_depth, c.max_depth);
+        r.closure_count += c.closure_count;
+        r.has_dynamic_root |= c.has_dynamic_root;
+        bo += c.body_count; co += c.collider_count; jo += c.bearing_count; qo += c.coordinate_count;
+        comp_o += comp_max;
+    }
+    out.body_offsets.push_back(bo);
+    out.collider_offsets.push_back(co);
+    r.body_count = bo;
+    r.collider_count = co;
+    r.bearing_count = jo;
+    r.suppression_count = (uint32_t)out.suppressed.size();
+    r.coordinate_count = qo;
+    r.transforms = out.transforms.data();
+    r.velocities = any_vel ? out.velocities.data() : nullptr;
+    r.masses = out.masses.data();
+    r.spatial_inertias = any_inertia ? out.inertias.data() : nullptr;
+    r.colliders = out.colliders.empty() ? nullptr : out.colliders.data();
+    r.bearings = out.bearings.empty() ? nullptr : out.bearings.data();
+    r.suppressed_pairs = out.suppressed.empty() ? nullptr : out.suppressed.data();
+    r.mechanism_bodies = any_mech ? out.mech.data() : nullptr;
+    r.root_flags = out.roots.data();
+    r.preorder = any_mech ? out.preorder.data() : nullptr;
+    r.body_components = out.components.data();
+    r.drives = out.drives.empty() ? nullptr : out.drives.data();
+    return true;
 }
 
-const char* mk_last_error(void) { return g_last_error.c_str(); }
-
-int mk_create(const MkCreation* cr, const MkConfig* config, const MkCapacities* caps, MkHandle** out, MkError* err) {
+int create_impl(const MkCreation* cr, const MkConfig* config, const MkCapacities* caps, MkHandle** out, MkError* err,
+                const Batch* batch) {
     if (err) std::memset(err, 0, sizeof(*err));
     if (!cr || !out) {
         set_error(err, MK_ERR_INVALID_ARGUMENT, "creation and out must be non-null");
@@ -430,6 +553,14 @@ int mk_create(const MkCreation* cr, const MkConfig* config, const MkCapacities* 
     h->max_depth = cr->max_depth;
     h->closure_count = cr->closure_count;
     h->pair_capacity = pair_capacity;
+    if (batch && batch->scene_count > 1) {
+        h->scene_count = batch->scene_count;
+        h->scene_body_offsets = batch->body_offsets;
+        h->scene_collider_offsets = batch->collider_offsets;
+        uint32_t bits = 0;
+        while ((1u << bits) < batch->scene_count) ++bits;
+        h->params.scene_bits = bits;
+    }
     h->mechanism_active = cr->max_depth > 0;
     h->collisions = h->config.collisions_enabled && h->C > 0;
     const MkConfig& c = h->config;
@@ -506,6 +637,13 @@ int mk_create(const MkCreation* cr, const MkConfig* config, const MkCapacities* 
     ok = ok && check(upload<uint32_t>(const_cast<uint32_t*>(b.root_flags), roots.data(), h->B, s), err, "upload roots");
     ok = ok && check(upload<float4>(const_cast<float4*>(b.colliders), cr->colliders, 4ull * h->C, s), err,
                      "upload colliders");
+    if (ok && batch && h->scene_count > 1 && h->C) {
+        // scene s owns sorted leaf positions [collider_offsets[s], collider_offsets[s + 1]): its
+        // colliders' keys carry s in their top bits
+        ok = check(upload<uint32_t>(b.collider_scene, batch->collider_scene.data(), h->C, s), err, "collider scenes");
+        ok = ok && check(upload<uint32_t>(b.scene_end, batch->collider_offsets.data() + 1, h->scene_count, s), err,
+                         "scene ends");
+    }
     ok = ok && check(upload<uint2>(const_cast<uint2*>(b.suppressed), cr->suppressed_pairs, h->S, s), err,
                      "upload suppression");
     if (ok && b.components) {
@@ -536,6 +674,78 @@ int mk_create(const MkCreation* cr, const MkConfig* config, const MkCapacities* 
     *out = h;
     return MK_OK;
 }
+
+}  // namespace
+
+extern "C" {
+
+void mk_config_default(MkConfig* c) {
+    if (!c) return;
+    std::memset(c, 0, sizeof(*c));
+    c->collisions_enabled = 1;
+    c->mechanism_self_collisions = 1;
+    c->solver_iterations = 8;
+    c->morton_mode = MK_MORTON_63;
+    c->closure_mode = MK_CLOSURE_REFERENCE;
+    c->use_graph = 1;
+}
+
+const char* mk_version(void) { return "mechanic_b200 0.1.0 sm_100a"; }
+
+int mk_set_tuning(uint32_t key, uint32_t value) {
+    static uint32_t sort_items = 0;
+    if (key == MK_TUNE_SORT_ITEMS) {
+        const uint32_t prev = sort_items;
+        sort_items = value;
+        mk::set_sort_items(value);
+        return (int)prev;
+    }
+    return -1;
+}
+
+const char* mk_last_error(void) { return g_last_error.c_str(); }
+
+int mk_create(const MkCreation* cr, const MkConfig* config, const MkCapacities* caps, MkHandle** out, MkError* err) {
+    return create_impl(cr, config, caps, out, err, nullptr);
+}
+
+int mk_create_batch(const MkCreation* scenes, uint32_t scene_count, const MkConfig* config, const MkCapacities* caps,
+                    MkHandle** out, MkError* err) {
+    if (err) std::memset(err, 0, sizeof(*err));
+    if (!scenes || !out || scene_count == 0) {
+        set_error(err, MK_ERR_INVALID_ARGUMENT, "scenes, out and scene_count > 0 required");
+        return MK_ERR_INVALID_ARGUMENT;
+    }
+    if (scene_count > (1u << 16)) {
+        set_error(err, MK_ERR_INVALID_ARGUMENT, "at most 65536 scenes per batch, %u given", scene_count);
+        return MK_ERR_INVALID_ARGUMENT;
+    }
+    Batch batch;
+    std::string why;
+    if (!concatenate(scenes, scene_count, batch, why)) {
+        set_error(err, MK_ERR_INVALID_ARGUMENT, "%s", why.c_str());
+        return MK_ERR_INVALID_ARGUMENT;
+    }
+    return create_impl(&batch.creation, config, caps, out, err, &batch);
+}
+
+int mk_scene_offsets(const MkHandle* h, uint32_t* body_offsets, uint32_t* collider_offsets, uint32_t capacity) {
+    if (!h) return -1;
+    const uint32_t n = (uint32_t)h->scene_body_offsets.size();
+    if (n == 0) {   // single scene
+        if (capacity >= 2) {
+            if (body_offsets) body_offsets[0] = 0, body_offsets[1] = h->B;
+            if (collider_offsets) collider_offsets[0] = 0, collider_offsets[1] = h->C;
+        }
+        return 1;
+    }
+    for (uint32_t i = 0; i < n && i < capacity; ++i) {
+        if (body_offsets) body_offsets[i] = h->scene_body_offsets[i];
+        if (collider_offsets) collider_offsets[i] = h->scene_collider_offsets[i];
+    }
+    return (int)n - 1;
+}
+
 
 void mk_destroy(MkHandle* h) { destroy_handle(h); }
 

@@ -47,6 +47,7 @@ struct StepParams {
     float dt, gravity, lin_damp, ang_damp;
     uint32_t body_count, collider_count, pair_capacity, suppression_count;
     uint32_t pair_shift;       // bits of a collider index inside a pair key
+    uint32_t scene_bits;       // batched scenes: bits of the scene index above each collider's Morton key
     float contact_tol;         // > 0: iterate the contact solve to ||r|| <= tol * ||r_cold||
     uint32_t contact_max_iterations;
 };
@@ -110,6 +111,9 @@ struct StepBuffers {
     DevCounts* counts;
     void* sort_scratch;
     uint64_t sort_scratch_bytes;
+    // batched scenes (null for a single scene)
+    uint32_t* collider_scene;    // scene of each collider
+    uint32_t* scene_end;         // per scene: end of its sorted leaf positions
     // contact solve to a residual (null unless enabled at creation)
     int64_t* deltas64;           // 2 candidates x 6 per body, fixed point x 2^32
     double* res2;                // 2 candidates x pair_capacity squared residuals

@@ -167,7 +167,13 @@ __global__ void __launch_bounds__(kBlock) k_collider_bounds(StepBuffers b, StepP
     box[0] = f4(center, he.x);
     box[1] = r;
     box[2] = make_float4(he.y, he.z, __uint_as_float(body), __uint_as_float(meta.w));
-    b.keys[i] = morton_mode == MK_MORTON_REFERENCE_30 ? (uint64_t)morton30(center) : morton63(center);
+    uint64_t key = morton_mode == MK_MORTON_REFERENCE_30 ? (uint64_t)morton30(center) : morton63(center);
+    if (p.scene_bits) {   // batched scenes: the scene index above the spatial key
+        const uint64_t scene = b.collider_scene[i];
+        key = morton_mode == MK_MORTON_REFERENCE_30 ? (scene << 30) | key
+                                                     : (scene << (63 - p.scene_bits)) | (key >> p.scene_bits);
+    }
+    b.keys[i] = key;
     b.values[i] = i;
 }
 
@@ -314,15 +320,21 @@ __global__ void __launch_bounds__(kTravThreads) k_traverse(StepBuffers b, StepPa
         const uint32_t i = b.svals[t];
         const float4 qmin = b.node_aabbs[2ull * (leaf_base + t)], qmax = b.node_aabbs[2ull * (leaf_base + t) + 1];
         const uint32_t body_i = __float_as_uint(b.boxes[3ull * i + 2].z);
+        // batched scenes: candidates end where this collider's scene ends in sorted order
+        // (a right child starts one past its left sibling's last leaf; left children start
+        // where their parent does, which was already below the limit)
+        const uint32_t limit = b.collider_scene ? __ldg(b.scene_end + b.collider_scene[i]) : n;
         uint32_t stack[kStack];
         uint32_t sp = 0;
         uint32_t node = 0;
         for (;;) {
             const float4* rec = b.node_records + 4ull * node;
+            const uint32_t left_last = __float_as_uint(__ldg(rec + 1).w);
 #pragma unroll
             for (int side = 0; side < 2; ++side) {
                 const float4 cmax = __ldg(rec + 2 * side + 1);
                 if (__float_as_uint(cmax.w) <= t) continue;     // nothing to the right of this leaf below
+                if (side == 1 && left_last + 1u >= limit) continue;   // starts past this scene
                 const float4 cmin = __ldg(rec + 2 * side);
                 if (!overlaps(qmin, qmax, cmin, cmax)) continue;
                 const uint32_t code = __float_as_uint(cmin.w);
@@ -1501,7 +1513,7 @@ cudaError_t launch_broadphase(const StepBuffers& b, const StepParams& p, const S
     const uint32_t C = p.collider_count;
     if (C == 0) return cudaSuccess;
     k_collider_bounds<<<blocks_for(C, kBlock), kBlock, 0, s>>>(b, p, l.morton_mode);
-    const uint32_t key_bits = l.morton_mode == MK_MORTON_REFERENCE_30 ? 30u : 63u;
+    const uint32_t key_bits = l.morton_mode == MK_MORTON_REFERENCE_30 ? 30u + p.scene_bits : 63u;
     cudaError_t e = launch_sort(b.keys, b.values, b.skeys, b.svals, C, nullptr, key_bits, b.sort_scratch,
                                 b.sort_scratch_bytes, &b.diag->error_flags, s, l.sm_count);
     if (e != cudaSuccess) return e;

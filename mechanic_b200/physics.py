@@ -27,7 +27,7 @@ EXPORTS = [
     "mk_tick_kernel_count", "mk_set_tuning", "mk_op_sort_keys_static",
     "mk_mlp_param_count", "mk_op_mlp_scratch_bytes", "mk_op_mlp_forward", "mk_op_mlp_gradient",
     "mk_op_mlp_train", "mk_set_warm_start_network", "mk_read_warm_start_samples",
-    "mk_set_preconditioner_network",
+    "mk_set_preconditioner_network", "mk_create_batch", "mk_scene_offsets",
 ]
 
 _lib = None
@@ -77,6 +77,8 @@ def library(path: str | None = None):
         "mk_set_warm_start_network": (i32, [vp, vp, u32, vp]),
         "mk_read_warm_start_samples": (i32, [vp, vp, vp, u32, vp, vp]),
         "mk_set_preconditioner_network": (i32, [vp, vp, u32, vp]),
+        "mk_create_batch": (i32, [vp, u32, vp, vp, vp, vp]),
+        "mk_scene_offsets": (i32, [vp, vp, vp, u32]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -227,6 +229,40 @@ class GpuPhysics:
         _raise(rc, err)
         self._h = h
         self._body_count = scene.body_count
+
+    @classmethod
+    def batch(cls, scene_list, config: GpuPhysicsConfig | None = None, capacities=None) -> "GpuPhysics":
+        """Independent scenes stepped together by one handle (mk_create_batch)."""
+        from . import scenes as _scenes
+        self = cls.__new__(cls)
+        L = library()
+        self.scene = _scenes.concatenate(scene_list)[0]   # host-side view of the concatenated rows
+        self._scene_list = list(scene_list)
+        arr = (abi.MkCreation * len(scene_list))(*[s.creation() for s in scene_list])
+        self._creation = arr
+        self._config = (config or GpuPhysicsConfig()).to_c()
+        caps = None
+        if capacities is not None:
+            caps = abi.MkCapacities()
+            for k, v in dict(capacities).items():
+                setattr(caps, k, int(v))
+        self._caps = caps
+        h = C.c_void_p()
+        err = abi.MkError()
+        rc = L.mk_create_batch(arr, len(scene_list), C.byref(self._config),
+                               C.byref(caps) if caps is not None else None, C.byref(h), C.byref(err))
+        _raise(rc, err)
+        self._h = h
+        self._body_count = self.scene.body_count
+        return self
+
+    def scene_offsets(self):
+        """(body offsets, collider offsets) per scene, each with the total appended."""
+        n = int(library().mk_scene_offsets(self._h, None, None, 0))
+        bo = np.zeros(n + 1, np.uint32)
+        co = np.zeros(n + 1, np.uint32)
+        library().mk_scene_offsets(self._h, bo.ctypes.data, co.ctypes.data, n + 1)
+        return bo, co
 
     @classmethod
     def new_with_config(cls, scene, config: GpuPhysicsConfig, capacities=None) -> "GpuPhysics":

@@ -582,3 +582,132 @@ def four_bar(invalid: bool = False) -> Scene:
                     np.arange(4, dtype=np.uint32), np.arange(4, dtype=np.uint32),
                     np.array([3, 2, 1, 0], np.uint32))
     return with_suppression(scene, [(0, 1), (1, 2), (2, 3), (3, 0)])
+
+
+# ------------------------------------------------------------ batched scenes
+def translated(scene: Scene, offset) -> Scene:
+    """The scene moved by `offset` (x, y, z)."""
+    tr = scene.transforms.copy()
+    tr["position"][:, :3] += np.asarray(offset, np.float32)
+    return dataclasses.replace(scene, transforms=tr)
+
+
+def concatenate(scene_list) -> tuple[Scene, np.ndarray]:
+    """Scenes as one creation, rows concatenated scene by scene with body, bearing,
+    coordinate and mechanism-component indices offset (the layout mk_create_batch
+    builds).  Returns (combined scene, scene index of each collider)."""
+    any_mech = any(s.max_depth > 0 for s in scene_list)
+    parts = {k: [] for k in ("transforms", "velocities", "masses", "inertias", "colliders", "bearings",
+                             "suppressed", "mech", "roots", "preorder", "components", "drives", "scene")}
+    bo = jo = qo = comp_o = 0
+    max_depth = closures = dyn = 0
+    for si, s in enumerate(scene_list):
+        n = s.body_count
+        parts["transforms"].append(s.transforms)
+        parts["velocities"].append(s.velocities if s.velocities is not None else np.zeros(n, abi.VELOCITY))
+        parts["masses"].append(s.masses)
+        parts["inertias"].append(s.spatial_inertias if s.spatial_inertias is not None
+                                 else np.zeros(n, abi.SPATIAL_INERTIA))
+        col = s.colliders.copy()
+        col["metadata"][:, 0] += bo
+        parts["colliders"].append(col)
+        parts["scene"].append(np.full(s.collider_count, si, np.uint32))
+        br = s.bearings.copy()
+        if len(br):
+            br["metadata"][:, 0] += bo
+            br["metadata"][:, 1] += bo
+            valid = br["metadata"][:, 2] != abi.INVALID_INDEX
+            br["metadata"][valid, 2] += qo
+        parts["bearings"].append(br)
+        sp = s.suppressed_pairs.copy()
+        if len(sp):
+            sp["collider_a"] += bo
+            sp["collider_b"] += bo
+        parts["suppressed"].append(sp)
+        comp = (s.body_components.astype(np.int64) if s.body_components is not None else np.arange(n))
+        parts["components"].append((comp + comp_o).astype(np.uint32))
+        parts["roots"].append(s.root_flags.astype(np.uint32) if s.root_flags is not None else np.ones(n, np.uint32))
+        if any_mech:
+            if s.max_depth > 0:
+                mb = s.mechanism_bodies.copy()
+                mb["metadata"][:, 0] += bo
+                valid = mb["metadata"][:, 1] != abi.INVALID_INDEX
+                mb["metadata"][valid, 1] += jo
+                mb["traversal"][:, 0] += comp_o
+                mb["traversal"][:, 2] += bo
+                mb["traversal"][:, 3] += bo
+                parts["preorder"].append((s.preorder.astype(np.int64) + bo).astype(np.uint32))
+            else:
+                mb = np.zeros(n, abi.MECHANISM_BODY)
+                idx = np.arange(n, dtype=np.uint32) + np.uint32(bo)
+                mb["metadata"][:, 0] = idx
+                mb["metadata"][:, 1] = abi.INVALID_INDEX
+                mb["metadata"][:, 3] = 1
+                mb["traversal"][:, 0] = (comp + comp_o).astype(np.uint32)
+                mb["traversal"][:, 2] = idx
+                mb["traversal"][:, 3] = idx
+                mb["bind_relative_rotation"][:, 3] = 1.0
+                parts["preorder"].append(idx)
+            parts["mech"].append(mb)
+        q = int(s.coordinate_count)
+        parts["drives"].append(s.drives if s.drives is not None else abi.passive_drive_rows(q))
+        max_depth = max(max_depth, int(s.max_depth))
+        closures += int(s.closure_count)
+        dyn |= int(s.has_dynamic_root)
+        bo += n
+        jo += s.bearing_count
+        qo += q
+        comp_o += int(comp.max()) + 1 if n else 0
+    cat = lambda k, dt: np.concatenate(parts[k]) if parts[k] else np.zeros(0, dt)  # noqa: E731
+    combined = Scene(
+        transforms=cat("transforms", abi.TRANSFORM), velocities=cat("velocities", abi.VELOCITY),
+        masses=cat("masses", abi.MASS), spatial_inertias=cat("inertias", abi.SPATIAL_INERTIA),
+        colliders=cat("colliders", abi.COLLIDER), bearings=cat("bearings", abi.BEARING),
+        suppressed_pairs=cat("suppressed", abi.PAIR),
+        mechanism_bodies=cat("mech", abi.MECHANISM_BODY) if any_mech else None,
+        root_flags=cat("roots", np.uint32), preorder=cat("preorder", np.uint32) if any_mech else None,
+        body_components=cat("components", np.uint32), drives=cat("drives", abi.MECHANISM_DRIVE) if qo else None,
+        coordinate_count=qo, max_depth=max_depth, closure_count=closures, has_dynamic_root=dyn,
+        name="+".join(s.name for s in scene_list[:3]) + ("..." if len(scene_list) > 3 else ""))
+    return combined, np.concatenate(parts["scene"]) if parts["scene"] else np.zeros(0, np.uint32)
+
+
+def take_bodies(scene: Scene, n: int) -> Scene:
+    """The first n bodies of a scene without bearings (colliders are contiguous per body)."""
+    assert scene.bearing_count == 0 and scene.max_depth == 0
+    keep = scene.colliders["metadata"][:, 0] < n
+    return dataclasses.replace(scene, transforms=scene.transforms[:n], velocities=scene.velocities[:n],
+                               masses=scene.masses[:n], spatial_inertias=scene.spatial_inertias[:n],
+                               colliders=scene.colliders[keep],
+                               root_flags=None if scene.root_flags is None else scene.root_flags[:n],
+                               body_components=None if scene.body_components is None else scene.body_components[:n])
+
+
+def mixed_scene(n: int, seed: int, bearing_fraction: float = 0.02) -> Scene:
+    """One scene of the batched config: n bodies, the 100,000-body config's cube/cylinder
+    mix on a 0.26 m grid, with about `bearing_fraction` of the bodies in five-link
+    bearing chains (10% of them loop-closed) beside the grid."""
+    chain_links = 5
+    chains = int(round(bearing_fraction * n / chain_links))
+    n_grid = max(1, n - chains * chain_links)
+    ny = max(1, int(round(n_grid ** (1.0 / 3.0) * 0.75)))
+    nx = max(1, int(math.ceil(math.sqrt(n_grid / ny))))
+    nz = max(1, int(math.ceil(n_grid / (nx * ny))))
+    grid = take_bodies(stack_grid(nx, ny, nz, seed=seed), n_grid)
+    if chains == 0:
+        return dataclasses.replace(grid, name=f"mixed_{n}_{seed}")
+    ch = bearing_chains(chains=chains, links=chain_links, seed=seed + 7919, closure_fraction=0.1, height=0.3,
+                        columns=max(1, min(chains, 8)))
+    ch = translated(ch, (nx * 0.13 + 2.0, 0.0, 0.0))
+    combined, _ = concatenate([grid, ch])
+    return dataclasses.replace(combined, name=f"mixed_{n}_{seed}")
+
+
+def batched_uneven(count: int = 256, seed: int = 0, lo: int = 64, hi: int = 8192,
+                   bearing_fraction: float = 0.02) -> list[Scene]:
+    """Batched config: `count` independent scenes with body counts log-uniform in
+    [lo, hi], each a mixed scene seeded by its index (seed + index)."""
+    rng = Rng(seed)
+    u = rng.uniform("batch_sizes", count)
+    sizes = np.floor(np.exp(np.log(lo) + u * (np.log(hi) - np.log(lo)))).astype(np.int64)
+    return [mixed_scene(int(sizes[i]), seed + i, bearing_fraction) for i in range(count)]

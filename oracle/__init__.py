@@ -60,6 +60,7 @@ def lib():
             getattr(L, name).argtypes = [vp, vp]
         L.or_get_sorted.argtypes = [vp, vp, vp]
         L.or_get_solve_stats.argtypes = [vp, vp, vp]
+        L.or_set_batch.argtypes = [vp, vp, u32]
         L.or_get_closure_stats.argtypes = [vp, vp, vp]
         L.or_set_precond_outputs.argtypes = [vp, vp, u32]
         L.or_get_closure_blocks.restype = u32
@@ -111,6 +112,17 @@ class OracleWorld:
                                  precision, pair_capacity)
         if not self.h:
             raise RuntimeError("oracle creation failed")
+
+    @classmethod
+    def batch(cls, scene_list, config: abi.MkConfig | None = None, precision: int = 32, pair_capacity: int = 0):
+        """Several independent scenes as one world (the concatenation mk_create_batch makes)."""
+        from mechanic_b200 import scenes as _scenes
+        combined, collider_scene = _scenes.concatenate(scene_list)
+        w = cls(combined, config, precision, pair_capacity)
+        w._collider_scene = np.ascontiguousarray(collider_scene, np.uint32)
+        if len(scene_list) > 1:
+            lib().or_set_batch(w.h, _p(w._collider_scene), len(scene_list))
+        return w
 
     def __del__(self):
         h = getattr(self, "h", None)

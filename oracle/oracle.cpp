@@ -306,7 +306,13 @@ template <class T> struct World : WorldBase {
             V3<T> e = absv(ax) * h.x + absv(ay) * h.y + absv(az) * h.z;
             aabb_min[i] = v4(c - e, T(0));
             aabb_max[i] = v4(c + e, T(0));
-            keys[i] = morton_mode == MK_MORTON_REFERENCE_30 ? (uint64_t)morton30(c) : morton63(c);
+            uint64_t key = morton_mode == MK_MORTON_REFERENCE_30 ? (uint64_t)morton30(c) : morton63(c);
+            if (scene_bits) {   // batched scenes: scene index above the spatial key
+                const uint64_t sc = col_scene[i];
+                key = morton_mode == MK_MORTON_REFERENCE_30 ? (sc << 30) | key
+                                                            : (sc << (63 - scene_bits)) | (key >> scene_bits);
+            }
+            keys[i] = key;
         }
         // Stable sort by key == ascending (key, index) order.
         std::vector<uint32_t> perm(C);
@@ -339,9 +345,12 @@ template <class T> struct World : WorldBase {
         }
         diag.pair_count = (uint32_t)std::min<uint64_t>(count, 0xffffffffull);
     }
+    std::vector<uint32_t> col_scene;   // batched scenes: scene of each collider
+    uint32_t scene_bits = 0;
     void consider_pair(uint32_t i, uint32_t j, std::vector<uint32_t>& out) const {
         uint32_t a = col[i].meta[0], b = col[j].meta[0];
         if (a == b) return;
+        if (scene_bits && col_scene[i] != col_scene[j]) return;
         if (!overlaps(aabb_min[i], aabb_max[i], aabb_min[j], aabb_max[j])) return;
         if (pair_is_suppressed(a, b)) return;
         out.push_back(i);
@@ -369,12 +378,13 @@ template <class T> struct World : WorldBase {
             return ((uint64_t)(x & 0x1fffff) << 42) | ((uint64_t)(y & 0x1fffff) << 21) | (uint64_t)(z & 0x1fffff);
         };
         for (uint32_t i = 0; i < C; ++i) {
+            const int64_t zs = scene_bits ? (int64_t)col_scene[i] * 4096 : 0;   // one grid per scene
             int64_t x0 = cidx(aabb_min[i].x, 0), x1 = cidx(aabb_max[i].x, 0);
             int64_t y0 = cidx(aabb_min[i].y, 1), y1 = cidx(aabb_max[i].y, 1);
             int64_t z0 = cidx(aabb_min[i].z, 2), z1 = cidx(aabb_max[i].z, 2);
             for (int64_t x = x0; x <= x1; ++x)
                 for (int64_t y = y0; y <= y1; ++y)
-                    for (int64_t z = z0; z <= z1; ++z) grid[key3(x, y, z)].push_back(i);
+                    for (int64_t z = z0; z <= z1; ++z) grid[key3(x, y, z + zs)].push_back(i);
         }
         std::vector<const std::vector<uint32_t>*> cells;
         std::vector<uint64_t> cell_keys;
@@ -403,7 +413,8 @@ template <class T> struct World : WorldBase {
                         double mxv[3] = {std::max(double(aabb_min[i].x), double(aabb_min[j].x)),
                                          std::max(double(aabb_min[i].y), double(aabb_min[j].y)),
                                          std::max(double(aabb_min[i].z), double(aabb_min[j].z))};
-                        if (key3(cidx(mxv[0], 0), cidx(mxv[1], 1), cidx(mxv[2], 2)) != k) continue;
+                        const int64_t zs = scene_bits ? (int64_t)col_scene[i] * 4096 : 0;
+                        if (key3(cidx(mxv[0], 0), cidx(mxv[1], 1), cidx(mxv[2], 2) + zs) != k) continue;
                         uint32_t lo_i = std::min(i, j), hi_i = std::max(i, j);
                         consider_pair(lo_i, hi_i, out);
                     }
@@ -2141,6 +2152,12 @@ uint32_t or_get_closure_blocks(const OrWorld* o, float* out) {
     uint32_t n = 0;
     BOTH((n = (uint32_t)w->blk_feat.size() / 16, out ? (void)std::copy(w->blk_feat.begin(), w->blk_feat.end(), out) : (void)0));
     return n;
+}
+// Batched scenes: the scene of each collider (scene indices ascending with the collider index).
+void or_set_batch(OrWorld* o, const uint32_t* collider_scene, uint32_t scene_count) {
+    uint32_t bits = 0;
+    while ((1u << bits) < scene_count) ++bits;
+    BOTH((w->col_scene.assign(collider_scene, collider_scene + w->C), w->scene_bits = scene_count > 1 ? bits : 0u));
 }
 // Learned warm-start impulses (by active position) for the next step's solve.
 void or_set_warm_predictions(OrWorld* o, const float* pred, uint32_t n) {
