@@ -589,6 +589,9 @@ int create_impl(const MkCreation* cr, const MkConfig* config, const MkCapacities
     h->launch.collisions = h->collisions;
     h->mech_params = mk::make_mech_params(cr, h->params, h->launch.iterations, c.closure_mode, c.closure_tolerance,
                                           c.closure_max_iterations, c.preconditioner);
+    // a batch keeps the parallel contact form (device.rs:1370-1373 picks the serial one for
+    // small mechanisms): one scene's path must not depend on the batch it is stepped in
+    if (h->scene_count > 1) h->mech_params.serial_contacts = 0;
     const mk::MechTopology topo = mk::derive_topology(cr, h->mech_params);
 
     bool ok = check(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking), err, "stream");

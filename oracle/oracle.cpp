@@ -1850,7 +1850,9 @@ template <class T> struct World : WorldBase {
     }
 
     bool mechanism_active() const { return max_depth > 0; }
-    bool serial_mechanism() const { return mechanism_active() && has_dynamic_root && J <= 64; }
+    // device.rs:1370-1373; a batch of several scenes keeps the parallel form so that
+    // one scene's path does not depend on the batch it is stepped in
+    bool serial_mechanism() const { return mechanism_active() && has_dynamic_root && J <= 64 && !scene_bits; }
 
     // device.rs:1219-1431, with bearing projection interleaved when a
     // mechanism root is dynamic (:1363-1416)
