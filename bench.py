@@ -1,4 +1,4 @@
-"""Benchmark: body-steps/s of the plain rigid-body step at 100,000 bodies.
+"""Benchmark: body-steps/s of the rigid-body step at 100,000 bodies.
 
 Workload (N=1): the 100,000-body stack (50x40x50 grid at 0.26 m, 20% hollow
 cylinders with 16 OBB segments each, 400,855 colliders, 8 PGS iterations),
@@ -17,6 +17,19 @@ snapshot ring (what a renderer consumes) and the diagnostics, wall-clocked.
 The reference arm times the CPU restatement of the same tick on all host
 cores (the reference's own wgpu pipeline needs a graphics stack, which this
 machine does not have).
+
+Two further measurements ride along in the same JSON line ("forms"):
+  residual_1e-5  the contact solve iterated to a 1e-5 relative residual, the
+                 cached (plain) start against the learned warm start, on the
+                 1,000-cube config (60 ticks).  The 100,000-body config is not
+                 used for it: its overlapping start has dozens of contacts per
+                 body, where the reference's relaxed Jacobi (omega 0.125)
+                 diverges when it is iterated beyond its fixed 8 passes.
+  batched        the 256-scene batched config (body counts log-uniform in
+                 [64, 8192], about 413,000 bodies, 2% bearings) in one handle,
+                 K ticks; under torchrun the scenes are sharded across ranks
+                 (contiguous ranges balanced by body count) and the slowest
+                 rank's device time sets the throughput.
 """
 from __future__ import annotations
 
@@ -58,6 +71,7 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-forms", action="store_true", help="skip the residual-form and batched measurements")
     return ap.parse_args()
 
 
@@ -172,6 +186,82 @@ def run_reference(args, scene):
     }
 
 
+# ------------------------------------------------------------ extra forms
+def measure_residual_forms(local: int, ticks: int = 60):
+    """Config 1 iterated to a 1e-5 residual: cached start against the learned one."""
+    import torch
+    from mechanic_b200 import learned, scenes
+    from mechanic_b200.physics import GpuPhysics
+    weights = os.path.join(ROOT, "mechanic_b200", "data", "warm_start.npy")
+    params = np.load(weights) if os.path.exists(weights) else None
+    scene = scenes.falling_cubes(1000, seed=0)
+    out = {"workload": "1,000 cubes, 60 ticks, contact passes until ||r|| <= 1e-5 ||r_cold|| (cap 512)"}
+    forms = [("plain", learned.residual_config(device=local), None)]
+    if params is not None:
+        forms.append(("learned", learned.residual_config(learned=True, device=local), params))
+    for name, cfg, prm in forms:
+        with GpuPhysics(scene, cfg) as g:
+            if prm is not None:
+                g.set_warm_start_network(prm)
+            passes, ms, used, conv = [], 0.0, {}, 0
+            torch.cuda.synchronize()
+            for t in range(1, ticks + 1):
+                g.dispatch_tick(t)
+                rb = g.read_last_tick()
+                passes.append(rb.contact_iterations)
+                ms += rb.gpu_tick_ms
+                used[rb.warm_start_used] = used.get(rb.warm_start_used, 0) + 1
+                conv += int(rb.contact_relative_residual <= 1e-5)
+        out[name] = {"value": scene.body_count * ticks / (ms / 1e3), "unit": UNIT,
+                     "passes_per_tick": float(np.mean(passes)), "ticks_converged": conv, "ticks": ticks,
+                     "start_used": {("cached", "learned", "learned rejected")[k]: v for k, v in used.items()}}
+    if "learned" in out:
+        out["pass_ratio_plain_over_learned"] = out["plain"]["passes_per_tick"] / max(out["learned"]["passes_per_tick"], 1e-9)
+    return out
+
+
+def measure_batched(args, rank: int, world: int, local: int):
+    """The 256-scene batched config (sharded by scene across ranks)."""
+    import torch
+    from mechanic_b200 import abi, scenes, sharding
+    from mechanic_b200.physics import GpuPhysics, GpuPhysicsConfig
+    lst = scenes.batched_uneven(256, seed=args.seed)
+    counts = [s.body_count for s in lst]
+    mine = [lst[i] for i in sharding.partition(counts, world)[rank]]
+    nb = sum(s.body_count for s in mine)
+    nc = sum(s.collider_count for s in mine)
+    cfg = GpuPhysicsConfig(device=local, closure_mode=abi.CLOSURE_PCG_RESIDUAL)
+    g = GpuPhysics.batch(mine, cfg, capacities={"max_bodies": nb, "max_colliders": nc, "max_bearings": 1 << 20,
+                                                 "pair_capacity": 1 << 26})
+    st = g.state_buffers()
+    stream = torch.cuda.ExternalStream(st.stream, device=torch.device("cuda", local))
+    for t in range(1, args.warmup + 1):
+        g.dispatch_tick(t)
+    g.wait()
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    flags = 0
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    with torch.cuda.stream(stream):
+        for k in range(args.steps):
+            starts[k].record(stream)
+            g.dispatch_tick(args.warmup + k + 1)
+            ends[k].record(stream)
+            flags |= g.read_last_tick().error_flags
+    torch.cuda.synchronize()
+    ms = float(sum(s.elapsed_time(e) for s, e in zip(starts, ends)))
+    ms = sharding.max_over_ranks(ms, device=torch.device("cuda", local)) if world > 1 else ms
+    launches = g.tick_kernel_count() * args.steps
+    g.close()
+    return {"workload": "256 scenes, body counts log-uniform in [64, 8192], 2% bearings, one handle per rank, "
+                        f"ticks {args.warmup + 1}..{args.warmup + args.steps}, closure PCG per-loop blocks",
+            "bodies": int(sum(counts)), "scenes": 256, "value": sum(counts) * args.steps / (ms / 1e3), "unit": UNIT,
+            "ms_per_step": ms / args.steps, "scaling": "strong (scenes sharded)" if world > 1 else "single",
+            "gpu_launches": launches, "error_flags_seen": flags}
+
+
 # ------------------------------------------------------------------ ours
 def main():
     args = parse()
@@ -271,6 +361,12 @@ def main():
     e2e_value = world * scene.body_count * args.steps / e2e_s
 
     kernels_per_tick = gpu.tick_kernel_count()
+    gpu_launches = kernels_per_tick * args.steps
+    forms = None
+    if not args.no_forms:
+        forms = {"batched": measure_batched(args, rank, world, local)}
+        if rank == 0 and world == 1:
+            forms["residual_1e-5"] = measure_residual_forms(local)
     solve_ms = stage_ms["contact_solver"]
     broad_ms = stage_ms["broadphase"]
     peaks = {}
@@ -321,8 +417,9 @@ def main():
                          "stage_ms_per_step": {k: v / args.steps for k, v in stage_ms.items()}},
             "cpu_baseline": cpu,
             "clocks": clocks.summary(),
-            "gpu_launches": kernels_per_tick * args.steps,
+            "gpu_launches": gpu_launches,
             "error_flags": flags,
+            "forms": forms,
         }
         print(json.dumps(out), flush=True)
     gpu.close()
