@@ -263,7 +263,11 @@ typedef struct MkConfig {
     float closure_tolerance;             /* MK_CLOSURE_PCG_RESIDUAL: relative PCG residual; 0 => 1e-5 */
     uint32_t closure_max_iterations;     /* MK_CLOSURE_PCG_RESIDUAL: PCG iterations per Newton step; 0 => 256 */
     uint32_t preconditioner;             /* MK_PRECOND_BLOCK_JACOBI (default) or MK_PRECOND_LEARNED */
+    uint32_t contact_manifold;           /* MK_MANIFOLD_POINT (default) or MK_MANIFOLD_CLIPPED */
 } MkConfig;
+
+#define MK_MANIFOLD_POINT       0u  /* collision.wgsl:540-620: one averaged point per colliding pair */
+#define MK_MANIFOLD_CLIPPED     1u  /* collision.rs:68-103 rule: up to four contained vertices per pair */
 
 #define MK_WARM_CACHED          0u  /* collision.wgsl:774-839: cached impulse x 0.5 (x 1 for cylinder-ground) */
 #define MK_WARM_LEARNED         1u  /* warm-start network next to the cached start; the lower residual wins */

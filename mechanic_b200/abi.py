@@ -38,6 +38,8 @@ WARM_LEARNED_REJECTED = 2
 PRECOND_BLOCK_JACOBI = 0
 PRECOND_LEARNED = 1
 PRECOND_PAIR_BLOCKS = 2
+MANIFOLD_POINT = 0
+MANIFOLD_CLIPPED = 1
 
 # ---------------------------------------------------------------- numpy rows
 f4 = (np.float32, 4)
@@ -129,7 +131,7 @@ class MkConfig(C.Structure):
         ("device", C.c_int32), ("warm_start", C.c_uint32),
         ("contact_tolerance", C.c_float), ("contact_max_iterations", C.c_uint32),
         ("closure_tolerance", C.c_float), ("closure_max_iterations", C.c_uint32),
-        ("preconditioner", C.c_uint32),
+        ("preconditioner", C.c_uint32), ("contact_manifold", C.c_uint32),
     ]
 
 

@@ -577,6 +577,7 @@ int create_impl(const MkCreation* cr, const MkConfig* config, const MkCapacities
         while (shift < 31 && (1ull << shift) < (uint64_t)h->C) ++shift;
         h->params.pair_shift = shift;
     }
+    h->params.clipped_manifold = c.contact_manifold == MK_MANIFOLD_CLIPPED ? 1u : 0u;
     h->params.contact_tol = c.contact_tolerance > 0.0f ? c.contact_tolerance : 0.0f;
     h->params.contact_max_iterations = c.contact_max_iterations ? c.contact_max_iterations : 512u;
     // the interleaved bearing form (dynamic-root mechanisms) keeps the fixed passes

@@ -48,6 +48,7 @@ struct StepParams {
     uint32_t body_count, collider_count, pair_capacity, suppression_count;
     uint32_t pair_shift;       // bits of a collider index inside a pair key
     uint32_t scene_bits;       // batched scenes: bits of the scene index above each collider's Morton key
+    uint32_t clipped_manifold; // MK_MANIFOLD_CLIPPED: up to four points per colliding pair
     float contact_tol;         // > 0: iterate the contact solve to ||r|| <= tol * ||r_cold||
     uint32_t contact_max_iterations;
 };

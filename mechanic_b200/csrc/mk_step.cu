@@ -490,6 +490,53 @@ __device__ f3 contact_point(const Box& a, const Box& b, f3 n) {
     return (pa + pb) * 0.5f;
 }
 
+// Clipped manifold (MK_MANIFOLD_CLIPPED): the contact rule of the reference's
+// CPU narrowphase (collision.rs:68-103) on the GPU boxes: A's vertices inside B,
+// then B's vertices inside A (the containment test of contact_point), later
+// points within 1e-5 m of an earlier one dropped, sorted by (x, y, z), the
+// first four kept; no contained vertex gives the support midpoint.  Returns
+// the number of points (1..4).
+__device__ uint32_t manifold_points(const Box& a, const Box& b, f3 n, f3* out) {
+    f3 cand[16];
+    uint32_t c = 0;
+#pragma unroll 1
+    for (uint32_t side = 0; side < 2; ++side) {
+        const Box& src = side == 0 ? a : b;
+        const Box& dst = side == 0 ? b : a;
+#pragma unroll 1
+        for (uint32_t v = 0; v < 8; ++v) {
+            const f3 pt = vertex(src, v);
+            if (!contains(dst, pt)) continue;
+            bool dup = false;
+            for (uint32_t q = 0; q < c; ++q) {
+                const f3 d = cand[q] - pt;
+                if (!(dot(d, d) > 1.0e-10f)) { dup = true; break; }
+            }
+            if (!dup) cand[c++] = pt;
+        }
+    }
+    if (c == 0) {
+        out[0] = (support_point(a, n) + support_point(b, -n)) * 0.5f;
+        return 1;
+    }
+    // insertion sort by (x, y, z)
+    for (uint32_t i = 1; i < c; ++i) {
+        const f3 key = cand[i];
+        uint32_t j = i;
+        while (j > 0) {
+            const f3 prv = cand[j - 1];
+            const bool greater = prv.x != key.x ? prv.x > key.x : (prv.y != key.y ? prv.y > key.y : prv.z > key.z);
+            if (!greater) break;
+            cand[j] = prv;
+            --j;
+        }
+        cand[j] = key;
+    }
+    const uint32_t m = c < 4u ? c : 4u;
+    for (uint32_t i = 0; i < m; ++i) out[i] = cand[i];
+    return m;
+}
+
 __device__ __forceinline__ void store_contact(GpuContact* dst, uint32_t ba, uint32_t bb, uint32_t ca, uint32_t cb,
                                               float4 np, float4 aa, float4 ab) {
     float4* d = reinterpret_cast<float4*>(dst);
@@ -526,10 +573,10 @@ __global__ void __launch_bounds__(kBlock) k_narrowphase(StepBuffers b, StepParam
         const uint32_t tile = take_tile(site.ticket, &s_tile);
         if (tile >= tiles) break;
         const uint32_t idx = tile * kBlock + threadIdx.x;
-        bool emit = false;
+        uint32_t emit = 0;
         uint2 pr = make_uint2(0, 0);
         Sat s;
-        f3 pt = mkf3(0, 0, 0);
+        f3 pts[4];
         uint32_t ba = 0, bb = 0;
         if (idx < n) {
             const uint64_t key = b.pair_keys[idx];
@@ -541,13 +588,17 @@ __global__ void __launch_bounds__(kBlock) k_narrowphase(StepBuffers b, StepParam
             if (!skip) {
                 s = obb_sat(A, Bx);
                 if (!(s.pen < -1.0e-5f)) {
-                    pt = contact_point(A, Bx, s.n);
-                    emit = true;
+                    if (p.clipped_manifold) {
+                        emit = manifold_points(A, Bx, s.n, pts);
+                    } else {
+                        pts[0] = contact_point(A, Bx, s.n);
+                        emit = 1;
+                    }
                 }
             }
         }
         uint32_t total;
-        const uint32_t ex = block_exclusive_scan(emit ? 1u : 0u, s_scan, &total);
+        const uint32_t ex = block_exclusive_scan(emit, s_scan, &total);
         if (warp_id() == 0) {
             uint64_t pre = tile_lookback(site.states, tile, total, &b.diag->error_flags);
             if (lane_id() == 0) s_prefix = pre;
@@ -555,13 +606,14 @@ __global__ void __launch_bounds__(kBlock) k_narrowphase(StepBuffers b, StepParam
         __syncthreads();
         const uint64_t pre = s_prefix;
         if (emit) {
-            const uint64_t o = pre + ex;
-            if (o < p.pair_capacity) {
-                const f3 xa = xyz(b.pos[ba]), xb = xyz(b.pos[bb]);
-                store_contact(out + o, ba, bb, pr.x, pr.y, f4(s.n, mxf(s.pen, 0.0f)), f4(pt - xa, 0.0f),
-                              f4(pt - xb, (float)s.near));
+            const f3 xa = xyz(b.pos[ba]), xb = xyz(b.pos[bb]);
+            for (uint32_t q = 0; q < emit; ++q) {
+                const uint64_t o = pre + ex + q;
+                if (o >= p.pair_capacity) break;
+                store_contact(out + o, ba, bb, pr.x, pr.y, f4(s.n, mxf(s.pen, 0.0f)), f4(pts[q] - xa, 0.0f),
+                              f4(pts[q] - xb, (float)s.near));
                 out_keys[o] = ((uint64_t)pr.x << 32) | pr.y;
-                out_feat[o] = s.axis | (s.near << 8) | (s.early << 16);
+                out_feat[o] = s.axis | (s.near << 8) | (s.early << 16) | (q << 25);
             }
         }
         if (tile == tiles - 1 && threadIdx.x == 0) {
@@ -720,15 +772,22 @@ __global__ void __launch_bounds__(kBlock) k_prepare(StepBuffers b, StepParams p,
                 } else {
                     float cached = 0.0f;
                     if (prev_ok) {
+                        // the previous rows of this collider pair (one, or up to four with a
+                        // clipped manifold): the first acquired row whose normal and arm match
                         const uint64_t key = cur_keys[k];
                         const bool ground = (uint32_t)key == kInvalid;
+                        const uint32_t end = ground ? prev_all : prev_narrow;
                         const int64_t m = ground ? find_previous(prev_keys, prev_narrow, prev_all, key)
                                                  : find_previous(prev_keys, 0u, prev_narrow, key);
-                        if (m >= 0 && (__ldg(prev_feat + m) & (1u << 24))) {
-                            const float4* pr = reinterpret_cast<const float4*>(prev + m);
+                        for (int64_t r = m; r >= 0 && r < (int64_t)end && __ldg(prev_keys + r) == key; ++r) {
+                            if (!(__ldg(prev_feat + r) & (1u << 24))) continue;
+                            const float4* pr = reinterpret_cast<const float4*>(prev + r);
                             const float4 pn = __ldg(pr + 1), pa = __ldg(pr + 2);
                             const bool match = dot(xyz(pn), nrm) >= 0.98f && length(xyz(pa) - arm_a) <= 0.02f;
-                            if (match) cached = pa.w;
+                            if (match) {
+                                cached = pa.w;
+                                break;
+                            }
                         }
                     }
                     row[0] = make_float4(r0.x, r0.y, __uint_as_float(k), __uint_as_float(1u));
@@ -917,7 +976,7 @@ __device__ __forceinline__ void apply_span(const StepBuffers& b, const StepParam
 
 // Grid-wide barrier for a cooperative launch.  The wait is bounded: a block
 // that gives up raises MK_DEVICE_WAIT_TIMEOUT_FLAG and carries on.
-__device__ __forceinline__ void grid_barrier(uint32_t* state, uint32_t* error_flags) {
+__device__ __forceinline__ void grid_barrier(uint32_t* state, uint32_t* error_flags, uint32_t participants) {
     __syncthreads();
     if (threadIdx.x == 0) {
         uint32_t* count = state;
@@ -925,7 +984,7 @@ __device__ __forceinline__ void grid_barrier(uint32_t* state, uint32_t* error_fl
         const uint32_t gen = ld_acquire_u32(generation);
         __threadfence();
         const uint32_t arrived = atomicAdd(count, 1u);
-        if (arrived == gridDim.x - 1) {
+        if (arrived == participants - 1) {
             atomicExch(count, 0u);
             __threadfence();
             st_release_u32(generation, gen + 1u);
@@ -949,12 +1008,23 @@ __device__ __forceinline__ void grid_barrier(uint32_t* state, uint32_t* error_fl
 // (device.rs:1343-1416 dispatch order), separated by grid barriers.
 constexpr uint32_t kSolveThreads = 1024;   // one block per SM: 148 barrier participants
 
+// Blocks that take part in a cooperative solve: enough for the active
+// contacts and the bodies at a few items per thread, never fewer than 8;
+// the others leave at once, so light ticks pay for small grid barriers.
+__device__ __forceinline__ uint32_t solve_participants(uint32_t A, uint32_t B) {
+    const uint32_t per_block = kSolveThreads * 4u;
+    const uint32_t want = max((A + per_block - 1) / per_block, (B + 4u * per_block - 1) / (4u * per_block));
+    return min(gridDim.x, max(want, 8u));
+}
+
 __global__ void __launch_bounds__(kSolveThreads) k_solve_all(StepBuffers b, StepParams p, GpuContact* cur,
                                                       uint32_t iterations, uint32_t* barrier) {
     const uint32_t A = b.counts->active;
     if (A == 0u) return;   // collision.wgsl:744-747: no solve and no apply dispatch
+    const uint32_t parts = solve_participants(A, p.body_count);
+    if (blockIdx.x >= parts) return;
     const uint32_t first = blockIdx.x * blockDim.x;
-    const uint32_t stride = gridDim.x * blockDim.x;
+    const uint32_t stride = parts * blockDim.x;
     const size_t B = p.body_count;
     for (uint32_t it = 0; it < iterations; ++it) {
         // iteration `it` reads buffer it (0 = the integrated velocities) and
@@ -965,9 +1035,9 @@ __global__ void __launch_bounds__(kSolveThreads) k_solve_all(StepBuffers b, Step
         float4* da = it + 1 == iterations ? b.ang : b.vel_iter + (2 * it + 1) * B;
         if (it == 0) solve_span<true>(b, p, cur, A, first, stride, sl, sa);
         else solve_span<false>(b, p, cur, A, first, stride, sl, sa);
-        grid_barrier(barrier, &b.diag->error_flags);
+        grid_barrier(barrier, &b.diag->error_flags, parts);
         apply_span(b, p, first + threadIdx.x, stride, sl, sa, dl, da);
-        grid_barrier(barrier, &b.diag->error_flags);
+        grid_barrier(barrier, &b.diag->error_flags, parts);
     }
 }
 
@@ -1211,11 +1281,11 @@ __global__ void __launch_bounds__(kSolveThreads) k_solve_residual(StepBuffers b,
             // the cold residual (pass 0) is the same for both candidates
             solve_span_res(b, p, cur, A, it == 0, c, v[c], !(it == 0 && c == 1));
         }
-        grid_barrier(barrier, &b.diag->error_flags);
+        grid_barrier(barrier, &b.diag->error_flags, gridDim.x);
         for (uint32_t c = c_first; c <= c_last; ++c) apply_span_res(b, p, c, v[c]);
         const uint32_t nres = (it == 0) ? 1u : (c_last - c_first + 1);
         chunk_sums(b, p, A, nres, c_first, s_tree);
-        grid_barrier(barrier, &b.diag->error_flags);
+        grid_barrier(barrier, &b.diag->error_flags, gridDim.x);
         const uint32_t chunks = (A + kResChunk - 1) / kResChunk;
         double S[2] = {0.0, 0.0};
         for (uint32_t c = c_first; c < c_first + nres; ++c)

@@ -153,6 +153,7 @@ class GpuPhysicsConfig:
     closure_tolerance: float = 0.0          # 0 => 1e-5 (CLOSURE_PCG_RESIDUAL)
     closure_max_iterations: int = 0         # 0 => 256
     preconditioner: int = abi.PRECOND_BLOCK_JACOBI
+    contact_manifold: int = abi.MANIFOLD_POINT
 
     def to_c(self) -> abi.MkConfig:
         c = abi.MkConfig()
@@ -170,6 +171,7 @@ class GpuPhysicsConfig:
         c.closure_tolerance = float(self.closure_tolerance)
         c.closure_max_iterations = int(self.closure_max_iterations)
         c.preconditioner = int(self.preconditioner)
+        c.contact_manifold = int(self.contact_manifold)
         return c
 
 

@@ -173,6 +173,10 @@ template <class T> struct World : WorldBase {
     std::vector<uint32_t> features;
     std::vector<uint32_t> active;
     std::unordered_map<uint64_t, Manifold<T>> manifold;
+    // MK_MANIFOLD_CLIPPED: up to four contacts per collider pair; the previous
+    // tick's acquired rows of each pair in row order
+    uint32_t clipped = 0;
+    std::unordered_map<uint64_t, std::vector<Manifold<T>>> manifold_rows;
     std::vector<V4<T>> snap_pos[3], snap_rot[3];
     GpuDiagnostics diag{};
     uint32_t tick32 = 0;
@@ -517,7 +521,7 @@ template <class T> struct World : WorldBase {
     // ----------------------------------------- collision.wgsl:570-603
     void narrowphase() {
         uint64_t np = pairs.size() / 2;
-        std::vector<Contact<T>> out(np);
+        std::vector<Contact<T>> out4(4 * np);
         std::vector<uint32_t> feat(np);
         std::vector<uint8_t> emit(np);
 #pragma omp parallel for schedule(dynamic, 256)
@@ -529,23 +533,67 @@ template <class T> struct World : WorldBase {
             Sat<T> s = obb_sat(a, b);
             emit[pp] = 0;
             if (s.pen < T(-1.0e-5f)) continue;
-            V3<T> p = contact_point(a, collider_rotation(ia), b, collider_rotation(ib), s.normal, false);
+            V3<T> pts[4];
+            uint32_t cnt = 1;
+            if (clipped) cnt = manifold_points(a, collider_rotation(ia), b, collider_rotation(ib), s.normal, pts);
+            else pts[0] = contact_point(a, collider_rotation(ia), b, collider_rotation(ib), s.normal, false);
             uint32_t ba = col[ia].meta[0], bb = col[ib].meta[0];
-            Contact<T>& c = out[pp];
-            c.meta[0] = ba; c.meta[1] = bb; c.meta[2] = ia; c.meta[3] = ib;
-            c.np = v4(s.normal, mx(s.pen, T(0)));
-            c.aa = v4(p - xyz(pos[ba]), T(0));
-            c.ab = v4(p - xyz(pos[bb]), T(s.near));
+            for (uint32_t q = 0; q < cnt; ++q) {
+                Contact<T>& c = out4[4 * pp + q];
+                c.meta[0] = ba; c.meta[1] = bb; c.meta[2] = ia; c.meta[3] = ib;
+                c.np = v4(s.normal, mx(s.pen, T(0)));
+                c.aa = v4(pts[q] - xyz(pos[ba]), T(0));
+                c.ab = v4(pts[q] - xyz(pos[bb]), T(s.near));
+            }
             feat[pp] = s.axis | (s.near << 8) | (s.early << 16);
-            emit[pp] = 1;
+            emit[pp] = (uint8_t)cnt;
         }
         contacts.clear(); contact_keys.clear(); features.clear();
-        for (uint64_t pp = 0; pp < np; ++pp) {
-            if (!emit[pp]) continue;
-            contacts.push_back(out[pp]);
-            contact_keys.push_back(((uint64_t)pairs[2 * pp] << 32) | pairs[2 * pp + 1]);
-            features.push_back(feat[pp]);
+        for (uint64_t pp = 0; pp < np; ++pp)
+            for (uint32_t q = 0; q < emit[pp]; ++q) {
+                contacts.push_back(out4[4 * pp + q]);
+                contact_keys.push_back(((uint64_t)pairs[2 * pp] << 32) | pairs[2 * pp + 1]);
+                features.push_back(feat[pp]);
+            }
+    }
+    // collision.rs:68-103 on the GPU boxes (vertex order and containment of contact_point)
+    uint32_t manifold_points(const Obb<T>& a, V4<T> ra, const Obb<T>& b, V4<T> rb, V3<T> n, V3<T>* out) const {
+        V3<T> cand[16];
+        uint32_t c = 0;
+        for (uint32_t side = 0; side < 2; ++side) {
+            const Obb<T>& src = side == 0 ? a : b;
+            const Obb<T>& dst = side == 0 ? b : a;
+            const V4<T> rdst = side == 0 ? rb : ra;
+            for (uint32_t v = 0; v < 8; ++v) {
+                V3<T> pt = vertex(src, v);
+                if (!contains(dst, rdst, pt)) continue;
+                bool dup = false;
+                for (uint32_t q = 0; q < c; ++q) {
+                    V3<T> d = cand[q] - pt;
+                    if (!(dot(d, d) > T(1.0e-10f))) { dup = true; break; }
+                }
+                if (!dup) cand[c++] = pt;
+            }
         }
+        if (c == 0) {
+            out[0] = (support_point(a, n) + support_point(b, -n)) * T(0.5);
+            return 1;
+        }
+        for (uint32_t i = 1; i < c; ++i) {
+            V3<T> key = cand[i];
+            uint32_t j = i;
+            while (j > 0) {
+                V3<T> prv = cand[j - 1];
+                bool greater = prv.x != key.x ? prv.x > key.x : (prv.y != key.y ? prv.y > key.y : prv.z > key.z);
+                if (!greater) break;
+                cand[j] = prv;
+                --j;
+            }
+            cand[j] = key;
+        }
+        const uint32_t m = c < 4 ? c : 4;
+        for (uint32_t i = 0; i < m; ++i) out[i] = cand[i];
+        return m;
     }
 
     // ----------------------------------------- collision.wgsl:193-238, 622-664
@@ -632,12 +680,23 @@ template <class T> struct World : WorldBase {
             // ordered collider pair; the hash slot is not part of parity.
             uint64_t key = contact_keys[kk];
             T cached_impulse = T(0);
-            auto it = manifold.find(key);
-            if (it != manifold.end()) {
-                const Manifold<T>& m = it->second;
-                bool match = m.tick == tick32 - 1u && dot(xyz(m.np), n) >= T(0.98f) &&
-                             length(xyz(m.pi) - arm_a) <= T(0.02f);
-                if (match) cached_impulse = m.pi.w;
+            if (clipped) {   // the first of the pair's previous rows whose normal and arm match
+                auto it = manifold_rows.find(key);
+                if (it != manifold_rows.end())
+                    for (const Manifold<T>& m : it->second)
+                        if (m.tick == tick32 - 1u && dot(xyz(m.np), n) >= T(0.98f) &&
+                            length(xyz(m.pi) - arm_a) <= T(0.02f)) {
+                            cached_impulse = m.pi.w;
+                            break;
+                        }
+            } else {
+                auto it = manifold.find(key);
+                if (it != manifold.end()) {
+                    const Manifold<T>& m = it->second;
+                    bool match = m.tick == tick32 - 1u && dot(xyz(m.np), n) >= T(0.98f) &&
+                                 length(xyz(m.pi) - arm_a) <= T(0.02f);
+                    if (match) cached_impulse = m.pi.w;
+                }
             }
             c.meta[2] = (uint32_t)kk;
             c.meta[3] = 1;
@@ -882,6 +941,7 @@ template <class T> struct World : WorldBase {
     // persist_contacts (collision.wgsl:1071-1088) + the prepare-time writes:
     // every acquired contact's manifold entry holds this tick's values.
     void persist() {
+        if (clipped) manifold_rows.clear();
         for (size_t k = 0; k < contacts.size(); ++k) {
             if (acquired_flags.size() <= k || !acquired_flags[k]) continue;
             const Contact<T>& c = contacts[k];
@@ -890,7 +950,8 @@ template <class T> struct World : WorldBase {
             m.count = 1;
             m.np = c.np;
             m.pi = c.aa;
-            manifold[contact_keys[k]] = m;
+            if (clipped) manifold_rows[contact_keys[k]].push_back(m);
+            else manifold[contact_keys[k]] = m;
         }
         last_tick = tick32;
     }
@@ -1943,6 +2004,7 @@ static World<T>* build_world(const MkCreation* cr, const MkConfig* cfg, uint32_t
     w->self_collisions = c.mechanism_self_collisions;
     w->pair_capacity = pair_capacity ? pair_capacity : MK_DEFAULT_MAX_CONTACT_PAIRS;
     w->contact_tol = c.contact_tolerance > 0.0f ? c.contact_tolerance : 0.0f;
+    w->clipped = c.contact_manifold == MK_MANIFOLD_CLIPPED ? 1u : 0u;
     w->contact_max_it = c.contact_max_iterations ? c.contact_max_iterations : 512u;
     w->closure_mode = c.closure_mode;
     w->closure_tol = c.closure_tolerance > 0.0f ? c.closure_tolerance : 1.0e-5f;

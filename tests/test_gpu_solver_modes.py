@@ -52,3 +52,18 @@ def test_residual_solve_on_cube_cylinder_grid(cuda_lib):
         compare_tick(gpu, orc, tick, check_tree=False)
         assert gpu.read_last_tick().contact_iterations == orc.solve_stats()["iterations"]
     assert_bitwise(gpu.contacts(), orc.contacts(), "contact rows")
+
+
+def test_clipped_manifold_bitexact(cuda_lib):
+    """MK_MANIFOLD_CLIPPED: up to four points per pair (collision.rs:68-103 rule), warm
+    started point by point from the pair's previous rows."""
+    from mechanic_b200 import abi
+    scene = scenes.falling_cubes(1000, seed=0)
+    gpu, orc = make_pair(scene, GpuPhysicsConfig(contact_manifold=abi.MANIFOLD_CLIPPED))
+    multi = 0
+    for tick in range(1, 61):
+        compare_tick(gpu, orc, tick, check_tree=False)
+        feats = gpu.features()
+        if len(feats):
+            multi = max(multi, int(((feats >> 25) & 3).max()) + 1)   # point index within its pair
+    assert 2 <= multi <= 4
