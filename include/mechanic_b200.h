@@ -468,6 +468,25 @@ MK_API uint32_t mk_tick_kernel_count(const MkHandle* handle);
 #define MK_TUNE_SORT_ITEMS 1u
 MK_API int mk_set_tuning(uint32_t key, uint32_t value);
 
+/* Launch shapes of one handle's tick (no reference counterpart).  0 in any
+ * field means the built-in default. */
+typedef struct MkTuning {
+    uint32_t sort_items;          /* keys per thread of a onesweep tile: 2, 4 or 8 (default 8) */
+    uint32_t sort_ctas_per_sm;    /* onesweep CTAs per SM (default 3 for 8 keys, else 6) */
+    uint32_t append_ctas_per_sm;  /* CTAs per SM of the ordered-append kernels (default 8) */
+    uint32_t solve_items;         /* contacts per thread a cooperative-solve block is sized for (default 4) */
+} MkTuning;
+MK_API int mk_get_handle_tuning(const MkHandle* handle, MkTuning* out);
+/* Applies a tuning; the tick's CUDA graphs are captured again. */
+MK_API int mk_set_handle_tuning(MkHandle* handle, const MkTuning* tuning, MkError* err);
+/* Autotuner: from the handle's current state, times `ticks` ticks (after one
+ * untimed tick) for each candidate shape, varying one field at a time over
+ * two sweeps, restoring the state before every candidate.  The fastest
+ * tuning is applied and the state restored again; *best_ms_per_tick
+ * receives its time.  The handle must not be in use meanwhile. */
+MK_API int mk_autotune(MkHandle* handle, uint32_t ticks, MkTuning* best, double* best_ms_per_tick,
+                       MkError* err);
+
 /* Library identity: returns "mechanic_b200 <version> sm_100a". */
 MK_API const char* mk_version(void);
 

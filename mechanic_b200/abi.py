@@ -167,6 +167,11 @@ class MkTickReadback(C.Structure):
                 ("warm_start_used", C.c_uint32), ("contact_relative_residual", C.c_double)]
 
 
+class MkTuning(C.Structure):
+    _fields_ = [("sort_items", C.c_uint32), ("sort_ctas_per_sm", C.c_uint32),
+                ("append_ctas_per_sm", C.c_uint32), ("solve_items", C.c_uint32)]
+
+
 class MkDeviceState(C.Structure):
     _fields_ = [(n, _vp) for n in (
         "positions", "rotations", "linear_velocities", "angular_velocities",

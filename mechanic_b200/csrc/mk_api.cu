@@ -1014,6 +1014,125 @@ uint32_t mk_body_count(const MkHandle* h) { return h ? h->B : 0u; }
 
 uint32_t mk_tick_kernel_count(const MkHandle* h) { return h ? h->kernels_per_tick : 0u; }
 
+int mk_get_handle_tuning(const MkHandle* h, MkTuning* out) {
+    if (!h || !out) return MK_ERR_INVALID_ARGUMENT;
+    out->sort_items = h->launch.sort_items ? h->launch.sort_items : 8u;
+    out->sort_ctas_per_sm = h->launch.sort_ctas ? h->launch.sort_ctas : (out->sort_items == 8 ? 3u : 6u);
+    out->append_ctas_per_sm = h->launch.append_ctas ? h->launch.append_ctas : 8u;
+    out->solve_items = h->launch.solve_items ? h->launch.solve_items : 4u;
+    return MK_OK;
+}
+
+int mk_set_handle_tuning(MkHandle* h, const MkTuning* t, MkError* err) {
+    if (err) std::memset(err, 0, sizeof(*err));
+    if (!h || !t) {
+        set_error(err, MK_ERR_INVALID_ARGUMENT, "handle and tuning must be non-null");
+        return MK_ERR_INVALID_ARGUMENT;
+    }
+    const bool ok_items = t->sort_items == 0 || t->sort_items == 2 || t->sort_items == 4 || t->sort_items == 8;
+    if (!ok_items || t->sort_ctas_per_sm > 32 || t->append_ctas_per_sm > 64 || t->solve_items > 64) {
+        set_error(err, MK_ERR_INVALID_ARGUMENT, "tuning outside the supported shapes");
+        return MK_ERR_INVALID_ARGUMENT;
+    }
+    DeviceGuard guard(h->device);
+    if (!check(cudaStreamSynchronize(h->stream), err, "set_handle_tuning sync")) return MK_ERR_DEVICE_FAILURE;
+    h->launch.sort_items = t->sort_items;
+    h->launch.sort_ctas = t->sort_ctas_per_sm;
+    h->launch.append_ctas = t->append_ctas_per_sm;
+    h->launch.solve_items = t->solve_items;
+    if (!h->config.use_graph) return MK_OK;
+    for (auto& gx : h->graph)
+        if (gx) {
+            cudaGraphExecDestroy(gx);
+            gx = nullptr;
+        }
+    return build_graphs(h, err) ? MK_OK : MK_ERR_DEVICE_FAILURE;
+}
+
+int mk_autotune(MkHandle* h, uint32_t ticks, MkTuning* best, double* best_ms, MkError* err) {
+    if (err) std::memset(err, 0, sizeof(*err));
+    if (!h || ticks == 0) {
+        set_error(err, MK_ERR_INVALID_ARGUMENT, "handle and ticks > 0 required");
+        return MK_ERR_INVALID_ARGUMENT;
+    }
+    DeviceGuard guard(h->device);
+    cudaStream_t s = h->stream;
+    if (!check(cudaStreamSynchronize(s), err, "autotune sync")) return MK_ERR_DEVICE_FAILURE;
+    // the state every candidate starts from
+    mk::DevCounts counts{};
+    if (!check(cudaMemcpy(&counts, h->buf.counts, sizeof(counts), cudaMemcpyDeviceToHost), err, "autotune counts"))
+        return MK_ERR_DEVICE_FAILURE;
+    const uint32_t rows = h->collisions ? std::max(counts.contacts, 1u) : 1u;
+    std::vector<GpuTransform> tr(h->B);
+    std::vector<GpuVelocity> vel(h->B);
+    std::vector<GpuMechanismCoordinate> coords(std::max(h->Q, 1u));
+    std::vector<GpuContact> man(rows);
+    MkHostState st{tr.data(), vel.data(), coords.data(), man.data(), rows, 0, 0};
+    int rc = mk_save_state(h, &st, err);
+    if (rc != MK_OK) return rc;
+    const uint64_t base_tick = st.manifold_tick;
+    MkHostState load = st;
+    if (!h->collisions || st.manifold_count == 0) load.manifold_contacts = nullptr;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    auto measure = [&](const MkTuning& t, double* ms) -> int {
+        int r = mk_set_handle_tuning(h, &t, err);
+        if (r != MK_OK) return r;
+        r = mk_load_state(h, &load, err);
+        if (r != MK_OK) return r;
+        MkSubmission sub;
+        r = mk_dispatch_tick(h, base_tick + 1, &sub);   // untimed: graph upload, caches
+        if (r != MK_OK) return r;
+        cudaEventRecord(e0, s);
+        for (uint32_t k = 0; k < ticks; ++k)
+            if ((r = mk_dispatch_tick(h, base_tick + 2 + k, &sub)) != MK_OK) return r;
+        cudaEventRecord(e1, s);
+        if (!check(cudaEventSynchronize(e1), err, "autotune timing")) return MK_ERR_DEVICE_FAILURE;
+        float f = 0.0f;
+        cudaEventElapsedTime(&f, e0, e1);
+        *ms = f;
+        return MK_OK;
+    };
+    MkTuning cur;
+    mk_get_handle_tuning(h, &cur);
+    double cur_ms = 0.0;
+    rc = measure(cur, &cur_ms);
+    // coordinate descent over the launch shapes, two sweeps
+    const uint32_t sort_items[] = {2, 4, 8};
+    const uint32_t sort_ctas[] = {2, 3, 4, 6, 8};
+    const uint32_t append_ctas[] = {4, 8, 16};
+    const uint32_t solve_items[] = {1, 2, 4, 8};
+    for (int sweep = 0; sweep < 2 && rc == MK_OK; ++sweep) {
+        for (int field = 0; field < 4 && rc == MK_OK; ++field) {
+            const uint32_t* vals = field == 0 ? sort_items : field == 1 ? sort_ctas : field == 2 ? append_ctas : solve_items;
+            const int nv = field == 0 ? 3 : field == 1 ? 5 : field == 2 ? 3 : 4;
+            for (int i = 0; i < nv && rc == MK_OK; ++i) {
+                MkTuning cand = cur;
+                uint32_t* slot = field == 0 ? &cand.sort_items : field == 1 ? &cand.sort_ctas_per_sm
+                                 : field == 2 ? &cand.append_ctas_per_sm : &cand.solve_items;
+                if (*slot == vals[i]) continue;
+                *slot = vals[i];
+                double ms = 0.0;
+                rc = measure(cand, &ms);
+                if (rc == MK_OK && ms < cur_ms) {
+                    cur = cand;
+                    cur_ms = ms;
+                }
+            }
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (rc != MK_OK) return rc;
+    rc = mk_set_handle_tuning(h, &cur, err);
+    if (rc == MK_OK) rc = mk_load_state(h, &load, err);
+    if (rc == MK_OK && !check(cudaStreamSynchronize(s), err, "autotune restore")) rc = MK_ERR_DEVICE_FAILURE;
+    if (best) *best = cur;
+    if (best_ms) *best_ms = cur_ms / ticks;
+    return rc;
+}
+
 int mk_has_gpu_timestamps(const MkHandle* h) { return h ? 1 : 0; }
 
 int mk_state_buffers(MkHandle* h, MkDeviceState* out) {

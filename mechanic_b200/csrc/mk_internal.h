@@ -69,7 +69,8 @@ uint32_t sort_items_for(uint32_t n);
 uint64_t sort_scratch_bytes(uint32_t n, uint32_t key_bits, bool values = true);
 cudaError_t launch_sort(const uint64_t* keys_in, const uint32_t* vals_in, uint64_t* keys_out, uint32_t* vals_out,
                         uint32_t n, const uint32_t* n_dev, uint32_t key_bits, void* scratch,
-                        uint64_t scratch_bytes, uint32_t* error_flags, cudaStream_t stream, int sm_count);
+                        uint64_t scratch_bytes, uint32_t* error_flags, cudaStream_t stream, int sm_count,
+                        uint32_t items = 0, uint32_t ctas_per_sm = 0);
 
 // Device buffers of one handle's step (all device pointers).
 struct StepBuffers {
@@ -134,6 +135,11 @@ struct StepLaunch {
     bool fuse_world_mass;     // no mechanism: integrate also writes world masses + snapshot
     bool collisions;
     bool learned_warm;        // run the learned warm start next to the cached one
+    // launch shapes (0 = default); picked by mk_autotune or mk_set_handle_tuning
+    uint32_t sort_items;      // keys per thread of a onesweep tile: 2, 4 or 8
+    uint32_t sort_ctas;       // onesweep CTAs per SM
+    uint32_t append_ctas;     // CTAs per SM of the ordered-append kernels (narrowphase, ground, prepare)
+    uint32_t solve_items;     // contacts per thread a cooperative-solve block is sized for
 };
 
 // mk_step.cu

@@ -212,13 +212,15 @@ static void launch_pass(const uint64_t* sk, const uint32_t* sv, uint64_t* dk, ui
 // with a device count, n is the capacity that sizes the grid and scratch.
 cudaError_t launch_sort(const uint64_t* keys_in, const uint32_t* vals_in, uint64_t* keys_out, uint32_t* vals_out,
                         uint32_t n, const uint32_t* n_dev, uint32_t key_bits, void* scratch,
-                        uint64_t scratch_bytes, uint32_t* error_flags, cudaStream_t stream, int sm_count) {
+                        uint64_t scratch_bytes, uint32_t* error_flags, cudaStream_t stream, int sm_count,
+                        uint32_t items_override, uint32_t ctas_per_sm) {
     if (n == 0) return cudaSuccess;
     uint32_t passes = sort_passes(key_bits);
     if (passes == 0 || passes > 8) return cudaErrorInvalidValue;
     const bool values = vals_in != nullptr;
     if (scratch_bytes < sort_scratch_bytes(n, key_bits, values)) return cudaErrorInvalidValue;
-    const uint32_t items = sort_items_for(n);
+    const uint32_t items = (items_override == 2 || items_override == 4 || items_override == 8) ? items_override
+                                                                                              : sort_items_for(n);
     const uint32_t tile_keys = kSortThreads * items;
     const uint64_t tiles = (n + tile_keys - 1) / tile_keys;
     const uint64_t tiles_max = (n + 2 * kSortThreads - 1) / (2 * kSortThreads);
@@ -237,7 +239,8 @@ cudaError_t launch_sort(const uint64_t* keys_in, const uint32_t* vals_in, uint64
     k_radix_histogram<<<hist_blocks, 256, 0, stream>>>(keys_in, n_dev, n, passes, hist, lookback,
                                                        tiles_max * kRadixBins, tile_keys);
     k_radix_offsets<<<passes, kRadixBins, 0, stream>>>(hist);
-    uint32_t grid = (uint32_t)std::min<uint64_t>(tiles, (uint64_t)sm_count * (items == 8 ? 3 : 6));
+    const uint32_t per_sm = ctas_per_sm ? ctas_per_sm : (items == 8 ? 3u : 6u);
+    uint32_t grid = (uint32_t)std::min<uint64_t>(tiles, (uint64_t)sm_count * per_sm);
     if (grid == 0) grid = 1;
     // passes alternate between (tmp, out) so that the last pass writes `out`.
     const uint64_t* src_k = keys_in;

@@ -1011,17 +1011,17 @@ constexpr uint32_t kSolveThreads = 1024;   // one block per SM: 148 barrier part
 // Blocks that take part in a cooperative solve: enough for the active
 // contacts and the bodies at a few items per thread, never fewer than 8;
 // the others leave at once, so light ticks pay for small grid barriers.
-__device__ __forceinline__ uint32_t solve_participants(uint32_t A, uint32_t B) {
-    const uint32_t per_block = kSolveThreads * 4u;
+__device__ __forceinline__ uint32_t solve_participants(uint32_t A, uint32_t B, uint32_t items) {
+    const uint32_t per_block = kSolveThreads * items;
     const uint32_t want = max((A + per_block - 1) / per_block, (B + 4u * per_block - 1) / (4u * per_block));
     return min(gridDim.x, max(want, 8u));
 }
 
 __global__ void __launch_bounds__(kSolveThreads) k_solve_all(StepBuffers b, StepParams p, GpuContact* cur,
-                                                      uint32_t iterations, uint32_t* barrier) {
+                                                      uint32_t iterations, uint32_t* barrier, uint32_t items) {
     const uint32_t A = b.counts->active;
     if (A == 0u) return;   // collision.wgsl:744-747: no solve and no apply dispatch
-    const uint32_t parts = solve_participants(A, p.body_count);
+    const uint32_t parts = solve_participants(A, p.body_count, items);
     if (blockIdx.x >= parts) return;
     const uint32_t first = blockIdx.x * blockDim.x;
     const uint32_t stride = parts * blockDim.x;
@@ -1585,7 +1585,7 @@ cudaError_t launch_broadphase(const StepBuffers& b, const StepParams& p, const S
     k_collider_bounds<<<blocks_for(C, kBlock), kBlock, 0, s>>>(b, p, l.morton_mode);
     const uint32_t key_bits = l.morton_mode == MK_MORTON_REFERENCE_30 ? 30u + p.scene_bits : 63u;
     cudaError_t e = launch_sort(b.keys, b.values, b.skeys, b.svals, C, nullptr, key_bits, b.sort_scratch,
-                                b.sort_scratch_bytes, &b.diag->error_flags, s, l.sm_count);
+                                b.sort_scratch_bytes, &b.diag->error_flags, s, l.sm_count, l.sort_items, l.sort_ctas);
     if (e != cudaSuccess) return e;
     k_karras<<<blocks_for(C, kBlock), kBlock, 0, s>>>(b, p);
     k_refit<<<blocks_for(C, kBlock), kBlock, 0, s>>>(b, p);
@@ -1593,14 +1593,14 @@ cudaError_t launch_broadphase(const StepBuffers& b, const StepParams& p, const S
     k_pairs_finalize<<<1, 32, 0, s>>>(b, p);
     e = launch_sort(b.pair_stage, nullptr, b.pair_keys, nullptr, p.pair_capacity, &b.counts->pairs,
                     2 * p.pair_shift, b.pair_sort_scratch, b.pair_sort_scratch_bytes, &b.diag->error_flags, s,
-                    l.sm_count);
+                    l.sm_count, l.sort_items, l.sort_ctas);
     if (e != cudaSuccess) return e;
     return cudaGetLastError();
 }
 
 cudaError_t launch_narrowphase(const StepBuffers& b, const StepParams& p, const StepLaunch& l, int parity,
                                cudaStream_t s) {
-    const uint32_t grid = (uint32_t)l.sm_count * 8;
+    const uint32_t grid = (uint32_t)l.sm_count * (l.append_ctas ? l.append_ctas : 8u);
     AppendSite narrow{b.lookback + 1 * b.lookback_words, b.tickets + 1};
     AppendSite ground{b.lookback + 2 * b.lookback_words, b.tickets + 2};
     k_narrowphase<<<grid, kBlock, 0, s>>>(b, p, narrow, b.contacts[parity], b.contact_keys[parity], b.features[parity]);
@@ -1611,7 +1611,7 @@ cudaError_t launch_narrowphase(const StepBuffers& b, const StepParams& p, const 
 
 cudaError_t launch_contact_solver(const StepBuffers& b, const StepParams& p, const StepLaunch& l, int parity,
                                   cudaStream_t s, const std::function<cudaError_t()>& before_solve) {
-    const uint32_t grid = (uint32_t)l.sm_count * 8;
+    const uint32_t grid = (uint32_t)l.sm_count * (l.append_ctas ? l.append_ctas : 8u);
     AppendSite prep{b.lookback + 3 * b.lookback_words, b.tickets + 3};
     const int prev = parity ^ 1;
     k_prepare<<<grid, kBlock, 0, s>>>(b, p, prep, b.contacts[parity], b.contact_keys[parity], b.features[parity],
@@ -1639,7 +1639,8 @@ cudaError_t launch_contact_solver(const StepBuffers& b, const StepParams& p, con
         if (e != cudaSuccess) return e;
         if (per_sm < 1) return cudaErrorInvalidConfiguration;
     }
-    void* args[] = {&bb, &pp, &cur, (void*)&iters, &barrier};
+    uint32_t solve_items = l.solve_items ? l.solve_items : 4u;
+    void* args[] = {&bb, &pp, &cur, (void*)&iters, &barrier, &solve_items};
     void* args_res[] = {&bb, &pp, &cur, (void*)&learned, &barrier};
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(blocks);
@@ -1659,7 +1660,7 @@ cudaError_t launch_contact_solver(const StepBuffers& b, const StepParams& p, con
 cudaError_t launch_contact_solver_stepwise(const StepBuffers& b, const StepParams& p, const StepLaunch& l, int parity,
                                            bool serial, const std::function<cudaError_t(bool)>& after_apply,
                                            cudaStream_t s) {
-    const uint32_t grid = (uint32_t)l.sm_count * 8;
+    const uint32_t grid = (uint32_t)l.sm_count * (l.append_ctas ? l.append_ctas : 8u);
     AppendSite prep{b.lookback + 3 * b.lookback_words, b.tickets + 3};
     const int prev = parity ^ 1;
     GpuContact* cur = b.contacts[parity];

@@ -27,7 +27,8 @@ EXPORTS = [
     "mk_tick_kernel_count", "mk_set_tuning", "mk_op_sort_keys_static",
     "mk_mlp_param_count", "mk_op_mlp_scratch_bytes", "mk_op_mlp_forward", "mk_op_mlp_gradient",
     "mk_op_mlp_train", "mk_set_warm_start_network", "mk_read_warm_start_samples",
-    "mk_set_preconditioner_network", "mk_create_batch", "mk_scene_offsets",
+    "mk_set_preconditioner_network", "mk_create_batch", "mk_scene_offsets", "mk_get_handle_tuning",
+    "mk_set_handle_tuning", "mk_autotune",
 ]
 
 _lib = None
@@ -79,6 +80,9 @@ def library(path: str | None = None):
         "mk_set_preconditioner_network": (i32, [vp, vp, u32, vp]),
         "mk_create_batch": (i32, [vp, u32, vp, vp, vp, vp]),
         "mk_scene_offsets": (i32, [vp, vp, vp, u32]),
+        "mk_get_handle_tuning": (i32, [vp, vp]),
+        "mk_set_handle_tuning": (i32, [vp, vp, vp]),
+        "mk_autotune": (i32, [vp, u32, vp, vp, vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -257,6 +261,27 @@ class GpuPhysics:
         self._h = h
         self._body_count = self.scene.body_count
         return self
+
+    def tuning(self) -> dict:
+        t = abi.MkTuning()
+        _raise(library().mk_get_handle_tuning(self._h, C.byref(t)))
+        return {f: int(getattr(t, f)) for f, _ in abi.MkTuning._fields_}
+
+    def set_tuning(self, **fields) -> None:
+        t = abi.MkTuning(**self.tuning())
+        for k, v in fields.items():
+            setattr(t, k, int(v))
+        err = abi.MkError()
+        _raise(library().mk_set_handle_tuning(self._h, C.byref(t), C.byref(err)), err)
+
+    def autotune(self, ticks: int = 5):
+        """Times candidate launch shapes from the current state and applies the fastest;
+        returns (tuning dict, ms per tick)."""
+        t = abi.MkTuning()
+        ms = C.c_double()
+        err = abi.MkError()
+        _raise(library().mk_autotune(self._h, int(ticks), C.byref(t), C.byref(ms), C.byref(err)), err)
+        return {f: int(getattr(t, f)) for f, _ in abi.MkTuning._fields_}, float(ms.value)
 
     def scene_offsets(self):
         """(body offsets, collider offsets) per scene, each with the total appended."""
