@@ -469,19 +469,21 @@ MK_API uint32_t mk_tick_kernel_count(const MkHandle* handle);
 MK_API int mk_set_tuning(uint32_t key, uint32_t value);
 
 /* Launch shapes of one handle's tick (no reference counterpart).  0 in any
- * field means the built-in default. */
+ * field means the built-in default (for solve_items: every block). */
 typedef struct MkTuning {
     uint32_t sort_items;          /* keys per thread of a onesweep tile: 2, 4 or 8 (default 8) */
     uint32_t sort_ctas_per_sm;    /* onesweep CTAs per SM (default 3 for 8 keys, else 6) */
     uint32_t append_ctas_per_sm;  /* CTAs per SM of the ordered-append kernels (default 8) */
-    uint32_t solve_items;         /* contacts per thread a cooperative-solve block is sized for (default 4) */
+    uint32_t solve_items;         /* 0 (default): every SM's block joins the cooperative solve; n > 0: only
+                                     enough blocks for n contacts (and 4n bodies) per thread */
 } MkTuning;
 MK_API int mk_get_handle_tuning(const MkHandle* handle, MkTuning* out);
 /* Applies a tuning; the tick's CUDA graphs are captured again. */
 MK_API int mk_set_handle_tuning(MkHandle* handle, const MkTuning* tuning, MkError* err);
-/* Autotuner: from the handle's current state, times `ticks` ticks (after one
- * untimed tick) for each candidate shape, varying one field at a time over
- * two sweeps, restoring the state before every candidate.  The fastest
+/* Autotuner: from the handle's current state, times the next `ticks` ticks
+ * (graphs uploaded first) for each candidate shape, varying one field at a time over
+ * two sweeps, restoring the state before every candidate; a change is kept only
+ * when it is at least 2% faster.  The fastest
  * tuning is applied and the state restored again; *best_ms_per_tick
  * receives its time.  The handle must not be in use meanwhile. */
 MK_API int mk_autotune(MkHandle* handle, uint32_t ticks, MkTuning* best, double* best_ms_per_tick,

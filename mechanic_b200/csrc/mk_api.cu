@@ -1019,7 +1019,7 @@ int mk_get_handle_tuning(const MkHandle* h, MkTuning* out) {
     out->sort_items = h->launch.sort_items ? h->launch.sort_items : 8u;
     out->sort_ctas_per_sm = h->launch.sort_ctas ? h->launch.sort_ctas : (out->sort_items == 8 ? 3u : 6u);
     out->append_ctas_per_sm = h->launch.append_ctas ? h->launch.append_ctas : 8u;
-    out->solve_items = h->launch.solve_items ? h->launch.solve_items : 4u;
+    out->solve_items = h->launch.solve_items;
     return MK_OK;
 }
 
@@ -1081,12 +1081,12 @@ int mk_autotune(MkHandle* h, uint32_t ticks, MkTuning* best, double* best_ms, Mk
         if (r != MK_OK) return r;
         r = mk_load_state(h, &load, err);
         if (r != MK_OK) return r;
+        for (auto& gx : h->graph)
+            if (gx && !check(cudaGraphUpload(gx, s), err, "graph upload")) return MK_ERR_DEVICE_FAILURE;
         MkSubmission sub;
-        r = mk_dispatch_tick(h, base_tick + 1, &sub);   // untimed: graph upload, caches
-        if (r != MK_OK) return r;
         cudaEventRecord(e0, s);
         for (uint32_t k = 0; k < ticks; ++k)
-            if ((r = mk_dispatch_tick(h, base_tick + 2 + k, &sub)) != MK_OK) return r;
+            if ((r = mk_dispatch_tick(h, base_tick + 1 + k, &sub)) != MK_OK) return r;
         cudaEventRecord(e1, s);
         if (!check(cudaEventSynchronize(e1), err, "autotune timing")) return MK_ERR_DEVICE_FAILURE;
         float f = 0.0f;
@@ -1102,7 +1102,7 @@ int mk_autotune(MkHandle* h, uint32_t ticks, MkTuning* best, double* best_ms, Mk
     const uint32_t sort_items[] = {2, 4, 8};
     const uint32_t sort_ctas[] = {2, 3, 4, 6, 8};
     const uint32_t append_ctas[] = {4, 8, 16};
-    const uint32_t solve_items[] = {1, 2, 4, 8};
+    const uint32_t solve_items[] = {0, 1, 2, 4};
     for (int sweep = 0; sweep < 2 && rc == MK_OK; ++sweep) {
         for (int field = 0; field < 4 && rc == MK_OK; ++field) {
             const uint32_t* vals = field == 0 ? sort_items : field == 1 ? sort_ctas : field == 2 ? append_ctas : solve_items;
@@ -1115,7 +1115,7 @@ int mk_autotune(MkHandle* h, uint32_t ticks, MkTuning* best, double* best_ms, Mk
                 *slot = vals[i];
                 double ms = 0.0;
                 rc = measure(cand, &ms);
-                if (rc == MK_OK && ms < cur_ms) {
+                if (rc == MK_OK && ms < 0.98 * cur_ms) {   // a change must win by 2% (timing noise)
                     cur = cand;
                     cur_ms = ms;
                 }

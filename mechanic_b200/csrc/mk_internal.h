@@ -139,7 +139,7 @@ struct StepLaunch {
     uint32_t sort_items;      // keys per thread of a onesweep tile: 2, 4 or 8
     uint32_t sort_ctas;       // onesweep CTAs per SM
     uint32_t append_ctas;     // CTAs per SM of the ordered-append kernels (narrowphase, ground, prepare)
-    uint32_t solve_items;     // contacts per thread a cooperative-solve block is sized for
+    uint32_t solve_items;     // 0: every block joins the cooperative solve; n: blocks for n contacts per thread
 };
 
 // mk_step.cu

@@ -1008,10 +1008,12 @@ __device__ __forceinline__ void grid_barrier(uint32_t* state, uint32_t* error_fl
 // (device.rs:1343-1416 dispatch order), separated by grid barriers.
 constexpr uint32_t kSolveThreads = 1024;   // one block per SM: 148 barrier participants
 
-// Blocks that take part in a cooperative solve: enough for the active
-// contacts and the bodies at a few items per thread, never fewer than 8;
-// the others leave at once, so light ticks pay for small grid barriers.
+// Blocks that take part in a cooperative solve: with `items` > 0, enough for
+// the active contacts and the bodies at that many items per thread (at least
+// 8), the others leaving at once so that light ticks pay for smaller grid
+// barriers; with 0, every block.
 __device__ __forceinline__ uint32_t solve_participants(uint32_t A, uint32_t B, uint32_t items) {
+    if (items == 0) return gridDim.x;   // default: every SM
     const uint32_t per_block = kSolveThreads * items;
     const uint32_t want = max((A + per_block - 1) / per_block, (B + 4u * per_block - 1) / (4u * per_block));
     return min(gridDim.x, max(want, 8u));
@@ -1639,7 +1641,7 @@ cudaError_t launch_contact_solver(const StepBuffers& b, const StepParams& p, con
         if (e != cudaSuccess) return e;
         if (per_sm < 1) return cudaErrorInvalidConfiguration;
     }
-    uint32_t solve_items = l.solve_items ? l.solve_items : 4u;
+    uint32_t solve_items = l.solve_items;   // 0: all blocks take part
     void* args[] = {&bb, &pp, &cur, (void*)&iters, &barrier, &solve_items};
     void* args_res[] = {&bb, &pp, &cur, (void*)&learned, &barrier};
     cudaLaunchConfig_t cfg = {};
