@@ -9,6 +9,11 @@ the reference's field names and gate logic (main.rs:155-272).  Scenarios:
   plain_small  1,000 falling 0.25 m cubes with random pose and velocity
   plain_scale  100,000-body grid at 0.26 m with 20% hollow cylinders
   plain_medium the same mix on a 30 x 30 x 30 grid (27,000 bodies; profiling size)
+  four_bar     four-bar linkage, first coordinate perturbed by 0.001 rad, collisions off
+               (main.rs:113-132); passes with error_flags == 0
+  invalid_loop the four-bar with its closure anchor moved (main.rs:211-216); passes when
+               CONSTRAINT_NON_CONVERGENCE_FLAG is raised
+  chains_20k   4,000 five-link bearing chains, 10% loop-closed (the articulated config)
 
     python -m mechanic_b200.bench_cli --scenario dense_100k [--seconds N] [--warmup N]
                                       [--ticks N] [--warmup-ticks N]
@@ -20,6 +25,8 @@ import json
 import math
 import time
 
+import numpy as np
+
 from . import abi, scenes
 from .physics import GpuPhysics, GpuPhysicsConfig
 
@@ -29,8 +36,12 @@ SCENARIOS = {
     "plain_small": lambda: scenes.falling_cubes(1000, seed=0),
     "plain_scale": lambda: scenes.stack_grid(50, 40, 50, seed=0),
     "plain_medium": lambda: scenes.stack_grid(30, 30, 30, seed=0),
+    "four_bar": lambda: scenes.four_bar(False),
+    "invalid_loop": lambda: scenes.four_bar(True),
+    "chains_20k": lambda: scenes.bearing_chains(),
 }
-SHORT = {"smoke", "plain_small"}
+SHORT = {"smoke", "plain_small", "four_bar", "invalid_loop"}
+LINKAGES = {"four_bar", "invalid_loop"}
 
 
 def percentile_95(sorted_values):
@@ -48,7 +59,12 @@ def run(scenario: str, seconds: int | None, warmup: int | None, ticks: int | Non
     warmup = warmup if warmup is not None else (0 if scenario in SHORT else 5)
     warm = warmup_ticks if warmup_ticks is not None else warmup * 60
     measured = ticks if ticks is not None else seconds * 60
-    gpu = GpuPhysics(scene, GpuPhysicsConfig(solver_iterations=8), capacities={"pair_capacity": pair_capacity})
+    cfg = GpuPhysicsConfig(solver_iterations=8, collisions_enabled=scenario not in LINKAGES)
+    gpu = GpuPhysics(scene, cfg, capacities={"pair_capacity": pair_capacity})
+    if scenario in LINKAGES:   # main.rs:114-131: perturb the first coordinate by 0.001 rad
+        coords = np.zeros(scene.coordinate_count, abi.MECHANISM_COORDINATE)
+        coords["angle"][0] = 0.001
+        gpu.initialize_mechanism_coordinates(coords)
     for tick in range(1, warm + 1):
         gpu.dispatch_tick(tick)
     gpu.wait()
@@ -78,7 +94,10 @@ def run(scenario: str, seconds: int | None, warmup: int | None, ticks: int | Non
     mean = sum(engine) / len(engine)
     tps = 1000.0 / mean
     gpu_p95 = percentile_95(gpu_ms)
-    correctness = flags == 0
+    if scenario == "invalid_loop":   # main.rs:211-216: the bad loop must be reported
+        correctness = bool(flags & abi.CONSTRAINT_NON_CONVERGENCE_FLAG)
+    else:
+        correctness = flags == 0
     budget = tps >= 60.0 and gpu_p95 <= 16.67
     out = {
         "type": "benchmark", "scenario": scenario, "adapter": "NVIDIA B200 (libmechanic_b200)",

@@ -210,16 +210,28 @@ cudaError_t enqueue_tick(MkHandle* h, int parity, bool capturing) {
     };
     cudaError_t e;
     if ((e = mark(0)) != cudaSuccess) return e;
-    cudaMemsetAsync(b.diag, 0, sizeof(GpuDiagnostics), s);
-    cudaMemsetAsync(b.counts, 0, mk::kCountResetBytes, s);
-    cudaMemsetAsync(b.tickets, 0, 16 * sizeof(uint32_t), s);
-    if (h->residual) cudaMemsetAsync(b.solve_stats, 0, sizeof(mk::SolveStats), s);
-    if (h->collisions) {
-        cudaMemsetAsync(b.visits, 0, sizeof(uint32_t) * std::max(h->C, 1u), s);
-        cudaMemsetAsync(b.deltas, 0, sizeof(int32_t) * 6ull * std::max(h->B, 1u), s);
-        cudaMemsetAsync(b.lookback, 0, sizeof(uint64_t) * 4 * b.lookback_words, s);
+    {   // everything the tick needs at zero, in one launch
+        mk::ZeroList z{};
+        z.add(b.diag, sizeof(GpuDiagnostics));
+        z.add(b.counts, mk::kCountResetBytes);
+        z.add(b.tickets, 16 * sizeof(uint32_t));
+        if (h->residual) z.add(b.solve_stats, sizeof(mk::SolveStats));
+        if (h->collisions) {
+            z.add(b.visits, sizeof(uint32_t) * std::max(h->C, 1u));
+            z.add(b.deltas, sizeof(int32_t) * 6ull * std::max(h->B, 1u));
+            z.add(b.lookback, sizeof(uint64_t) * 4 * b.lookback_words);
+            void* r = nullptr;
+            uint64_t rb = 0;
+            const uint32_t key_bits = h->launch.morton_mode == MK_MORTON_REFERENCE_30 ? 30u + h->params.scene_bits : 63u;
+            mk::sort_clear_region(b.sort_scratch, h->C, key_bits, true, &r, &rb);
+            z.add(r, rb);
+            mk::sort_clear_region(b.pair_sort_scratch, h->pair_capacity, 2 * h->params.pair_shift, false, &r, &rb);
+            z.add(r, rb);
+        }
+        if (h->mechanism_active) z.add(h->mech.deltas, 24ull * std::max(h->B, 1u));
+        cudaError_t ez = mk::launch_tick_reset(z, h->sm_count, s);
+        if (ez != cudaSuccess) return ez;
     }
-    if (h->mechanism_active) mk::enqueue_mechanism_prelude(h->mech, b, h->mech_params, s);
     const bool fuse = !h->mechanism_active;
     mk::StepLaunch l = h->launch;
     l.fuse_world_mass = fuse;

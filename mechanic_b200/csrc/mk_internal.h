@@ -70,7 +70,8 @@ uint64_t sort_scratch_bytes(uint32_t n, uint32_t key_bits, bool values = true);
 cudaError_t launch_sort(const uint64_t* keys_in, const uint32_t* vals_in, uint64_t* keys_out, uint32_t* vals_out,
                         uint32_t n, const uint32_t* n_dev, uint32_t key_bits, void* scratch,
                         uint64_t scratch_bytes, uint32_t* error_flags, cudaStream_t stream, int sm_count,
-                        uint32_t items = 0, uint32_t ctas_per_sm = 0);
+                        uint32_t items = 0, uint32_t ctas_per_sm = 0, bool precleared = false);
+void sort_clear_region(void* scratch, uint32_t n, uint32_t key_bits, bool values, void** ptr, uint64_t* bytes);
 
 // Device buffers of one handle's step (all device pointers).
 struct StepBuffers {
@@ -142,7 +143,22 @@ struct StepLaunch {
     uint32_t solve_items;     // 0: every block joins the cooperative solve; n: blocks for n contacts per thread
 };
 
+// Device regions to clear at the start of a tick (16-byte aligned, sizes in 16-byte units).
+struct ZeroList {
+    static constexpr uint32_t kMax = 12;
+    uint4* ptr[kMax];
+    uint64_t n16[kMax];
+    uint32_t count;
+    void add(void* p, uint64_t bytes) {
+        if (!p || bytes == 0 || count >= kMax) return;
+        ptr[count] = reinterpret_cast<uint4*>(p);
+        n16[count] = (bytes + 15) / 16;   // the arena pads every buffer to 256 bytes
+        ++count;
+    }
+};
+
 // mk_step.cu
+cudaError_t launch_tick_reset(const ZeroList& z, int sm_count, cudaStream_t s);
 cudaError_t launch_integrate(const StepBuffers& b, const StepParams& p, const StepLaunch& l, cudaStream_t s);
 cudaError_t launch_world_masses(const StepBuffers& b, const StepParams& p, cudaStream_t s);
 cudaError_t launch_snapshot(const StepBuffers& b, const StepParams& p, cudaStream_t s);

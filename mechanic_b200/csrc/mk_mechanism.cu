@@ -1296,11 +1296,6 @@ __global__ void __launch_bounds__(kClosureThreads) k_closure_pcg(StepBuffers b, 
 // --------------------------------------------------------------- launches
 static inline uint32_t nblocks(uint32_t n) { return (n + kMBlock - 1) / kMBlock; }
 
-void enqueue_mechanism_prelude(MechBuffers& m, const StepBuffers& b, const MechParams& p, cudaStream_t s) {
-    (void)b;
-    cudaMemsetAsync(m.deltas, 0, 24ull * (p.body_count ? p.body_count : 1), s);
-}
-
 static cudaError_t bearing_projection_iteration(MechBuffers& m, const StepBuffers& b, const MechParams& p,
                                                 cudaStream_t s) {
     if (p.bearing_count) k_project_bearings<<<nblocks(p.bearing_count), kMBlock, 0, s>>>(b, m, p);

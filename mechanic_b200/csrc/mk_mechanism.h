@@ -105,7 +105,6 @@ void carve_mechanism(MechBuffers& m, const MechParams& p, uint32_t B, uint32_t J
                      const std::function<char*(uint64_t)>& take);
 bool upload_mechanism(MechBuffers& m, const MechParams& p, const MechTopology& topo, const MkCreation* cr,
                       cudaStream_t s, MkError* err);
-void enqueue_mechanism_prelude(MechBuffers& m, const StepBuffers& b, const MechParams& p, cudaStream_t s);
 cudaError_t enqueue_mechanism(MechBuffers& m, const StepBuffers& b, const MechParams& p, cudaStream_t s);
 bool pcg_residual_mode(const MechParams& p);
 cudaError_t enqueue_contact_solver_with_bearings(MechBuffers& m, const StepBuffers& b, const StepParams& sp,

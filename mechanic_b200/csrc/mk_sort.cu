@@ -25,7 +25,7 @@ k_radix_histogram(const uint64_t* __restrict__ keys, const uint32_t* __restrict_
                   uint32_t passes, uint32_t* __restrict__ hist /* passes x 256 */,
                   uint32_t* __restrict__ lookback, uint64_t lookback_pass_words, uint32_t tile_keys) {
     __shared__ uint32_t s_hist[8][kRadixBins];
-    const uint32_t n = n_ptr ? *n_ptr : n_fixed;
+    const uint32_t n = n_ptr ? min(*n_ptr, n_fixed) : n_fixed;   // a device count never exceeds the capacity
     // clear the look-back words the onesweep passes will use for this n only
     const uint64_t used = (uint64_t)((n + tile_keys - 1) / tile_keys) * kRadixBins;
     for (uint64_t w = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; w < used * passes;
@@ -46,16 +46,6 @@ k_radix_histogram(const uint64_t* __restrict__ keys, const uint32_t* __restrict_
     }
 }
 
-// Exclusive scan of each pass's 256-bin histogram (one block per pass).
-__global__ void __launch_bounds__(kRadixBins) k_radix_offsets(uint32_t* __restrict__ hist) {
-    __shared__ uint32_t scratch[33];
-    uint32_t* h = hist + blockIdx.x * kRadixBins;
-    uint32_t total;
-    uint32_t v = h[threadIdx.x];
-    uint32_t e = block_exclusive_scan(v, scratch, &total);
-    h[threadIdx.x] = e;
-}
-
 __device__ __forceinline__ uint32_t lanemask_lt() {
     uint32_t m;
     asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
@@ -67,7 +57,7 @@ __global__ void __launch_bounds__(kSortThreads)
 k_radix_onesweep(const uint64_t* __restrict__ keys_in, const uint32_t* __restrict__ vals_in,
                  uint64_t* __restrict__ keys_out, uint32_t* __restrict__ vals_out,
                  const uint32_t* __restrict__ n_ptr, uint32_t n_fixed, uint32_t shift,
-                 const uint32_t* __restrict__ digit_offsets /* 256 */, uint32_t* __restrict__ lookback,
+                 const uint32_t* __restrict__ digit_hist /* 256 */, uint32_t* __restrict__ lookback,
                  uint32_t* __restrict__ ticket, uint32_t* __restrict__ error_flags) {
     constexpr uint32_t kTile = kSortThreads * kSortItems;
     __shared__ uint64_t s_keys[kTile];
@@ -77,10 +67,16 @@ k_radix_onesweep(const uint64_t* __restrict__ keys_in, const uint32_t* __restric
     __shared__ uint32_t s_global_base[kRadixBins];
     __shared__ uint32_t s_scan[33];
     __shared__ uint32_t s_tile;
+    __shared__ uint32_t s_digit_offsets[kRadixBins];
 
-    const uint32_t n = n_ptr ? *n_ptr : n_fixed;
+    const uint32_t n = n_ptr ? min(*n_ptr, n_fixed) : n_fixed;   // a device count never exceeds the capacity
     const uint32_t tiles = (n + kTile - 1) / kTile;
     const uint32_t lane = lane_id(), w = warp_id();
+    {   // this pass's digit offsets: exclusive scan of its histogram (kSortThreads == kRadixBins)
+        uint32_t total_all;
+        s_digit_offsets[threadIdx.x] = block_exclusive_scan(digit_hist[threadIdx.x], s_scan, &total_all);
+        __syncthreads();
+    }
 
     for (;;) {
         if (threadIdx.x == 0) s_tile = atomicAdd(ticket, 1u);
@@ -150,7 +146,7 @@ k_radix_onesweep(const uint64_t* __restrict__ keys_in, const uint32_t* __restric
             }
             st_release_u32(lb, kDigitInclusive | (prefix + count));
         }
-        s_global_base[d] = digit_offsets[d] + prefix - local_start;
+        s_global_base[d] = s_digit_offsets[d] + prefix - local_start;
         __syncthreads();
 
         // ---- reorder through shared memory, then scatter by digit runs
@@ -188,6 +184,17 @@ uint32_t sort_items_for(uint32_t n) {
     return 8u;   // measured fastest for 0.4M-14M keys on B200 (look-back chains dominate small tiles)
 }
 
+// The histogram bins and tile tickets of a sort's scratch: the region that must
+// be zero when the sort starts (launch_sort clears it unless told it is clear).
+void sort_clear_region(void* scratch, uint32_t n, uint32_t key_bits, bool values, void** ptr, uint64_t* bytes) {
+    const uint32_t passes = sort_passes(key_bits);
+    char* p = (char*)scratch;
+    p += align256((uint64_t)n * 8);
+    p += align256((uint64_t)(values ? n : 0) * 4);
+    *ptr = p;
+    *bytes = align256((uint64_t)passes * kRadixBins * 4) + (uint64_t)passes * 4;
+}
+
 uint64_t sort_scratch_bytes(uint32_t n, uint32_t key_bits, bool values) {
     uint32_t passes = sort_passes(key_bits);
     uint64_t tiles = (n + 2 * kSortThreads - 1) / (2 * kSortThreads);   // smallest tile: 512 keys
@@ -213,7 +220,7 @@ static void launch_pass(const uint64_t* sk, const uint32_t* sv, uint64_t* dk, ui
 cudaError_t launch_sort(const uint64_t* keys_in, const uint32_t* vals_in, uint64_t* keys_out, uint32_t* vals_out,
                         uint32_t n, const uint32_t* n_dev, uint32_t key_bits, void* scratch,
                         uint64_t scratch_bytes, uint32_t* error_flags, cudaStream_t stream, int sm_count,
-                        uint32_t items_override, uint32_t ctas_per_sm) {
+                        uint32_t items_override, uint32_t ctas_per_sm, bool precleared) {
     if (n == 0) return cudaSuccess;
     uint32_t passes = sort_passes(key_bits);
     if (passes == 0 || passes > 8) return cudaErrorInvalidValue;
@@ -232,13 +239,14 @@ cudaError_t launch_sort(const uint64_t* keys_in, const uint32_t* vals_in, uint64
     uint32_t* lookback = (uint32_t*)p;
     // histogram bins and tile tickets are cleared here; look-back words by the
     // histogram kernel, only as many as the device-side count needs
-    cudaError_t e = cudaMemsetAsync(hist, 0, (uint64_t)((char*)tickets - (char*)hist) + passes * 4, stream);
-    if (e != cudaSuccess) return e;
+    if (!precleared) {
+        cudaError_t e = cudaMemsetAsync(hist, 0, (uint64_t)((char*)tickets - (char*)hist) + passes * 4, stream);
+        if (e != cudaSuccess) return e;
+    }
     uint32_t hist_blocks = (uint32_t)std::min<uint64_t>((n + 4095) / 4096, (uint64_t)sm_count * 4);
     if (hist_blocks == 0) hist_blocks = 1;
     k_radix_histogram<<<hist_blocks, 256, 0, stream>>>(keys_in, n_dev, n, passes, hist, lookback,
                                                        tiles_max * kRadixBins, tile_keys);
-    k_radix_offsets<<<passes, kRadixBins, 0, stream>>>(hist);
     const uint32_t per_sm = ctas_per_sm ? ctas_per_sm : (items == 8 ? 3u : 6u);
     uint32_t grid = (uint32_t)std::min<uint64_t>(tiles, (uint64_t)sm_count * per_sm);
     if (grid == 0) grid = 1;

@@ -374,14 +374,6 @@ __global__ void __launch_bounds__(kTravThreads) k_traverse(StepBuffers b, StepPa
         if (base + k < p.pair_capacity) b.pair_stage[base + k] = s_stage[w][k];
 }
 
-// Pair count of the tick (diag[1] keeps the requested count, lbvh.wgsl:353-358).
-__global__ void k_pairs_finalize(StepBuffers b, StepParams p) {
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
-    const uint32_t found = b.counts->pairs_found;
-    b.diag->pair_count = found;
-    b.counts->pairs = min(found, p.pair_capacity);
-    if (found > p.pair_capacity) atomicOr(&b.diag->error_flags, MK_PAIR_OVERFLOW_FLAG);
-}
 
 // ------------------------------------------------------------- narrowphase
 struct Box {
@@ -567,7 +559,14 @@ __global__ void __launch_bounds__(kBlock) k_narrowphase(StepBuffers b, StepParam
     __shared__ uint32_t s_scan[33];
     __shared__ uint32_t s_tile;
     __shared__ uint64_t s_prefix;
-    const uint32_t n = b.counts->pairs;
+    // the tick's pair count (diag[1] keeps the requested count, lbvh.wgsl:353-358)
+    const uint32_t found = b.counts->pairs_found;
+    const uint32_t n = min(found, p.pair_capacity);
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        b.diag->pair_count = found;
+        b.counts->pairs = n;
+        if (found > p.pair_capacity) atomicOr(&b.diag->error_flags, MK_PAIR_OVERFLOW_FLAG);
+    }
     const uint32_t tiles = (n + kBlock - 1) / kBlock;
     for (;;) {
         const uint32_t tile = take_tile(site.ticket, &s_tile);
@@ -1587,15 +1586,15 @@ cudaError_t launch_broadphase(const StepBuffers& b, const StepParams& p, const S
     k_collider_bounds<<<blocks_for(C, kBlock), kBlock, 0, s>>>(b, p, l.morton_mode);
     const uint32_t key_bits = l.morton_mode == MK_MORTON_REFERENCE_30 ? 30u + p.scene_bits : 63u;
     cudaError_t e = launch_sort(b.keys, b.values, b.skeys, b.svals, C, nullptr, key_bits, b.sort_scratch,
-                                b.sort_scratch_bytes, &b.diag->error_flags, s, l.sm_count, l.sort_items, l.sort_ctas);
+                                b.sort_scratch_bytes, &b.diag->error_flags, s, l.sm_count, l.sort_items, l.sort_ctas,
+                                true);   // bins and tickets cleared by the tick's reset
     if (e != cudaSuccess) return e;
     k_karras<<<blocks_for(C, kBlock), kBlock, 0, s>>>(b, p);
     k_refit<<<blocks_for(C, kBlock), kBlock, 0, s>>>(b, p);
     k_traverse<<<blocks_for(C, kTravThreads), kTravThreads, 0, s>>>(b, p);
-    k_pairs_finalize<<<1, 32, 0, s>>>(b, p);
-    e = launch_sort(b.pair_stage, nullptr, b.pair_keys, nullptr, p.pair_capacity, &b.counts->pairs,
+    e = launch_sort(b.pair_stage, nullptr, b.pair_keys, nullptr, p.pair_capacity, &b.counts->pairs_found,
                     2 * p.pair_shift, b.pair_sort_scratch, b.pair_sort_scratch_bytes, &b.diag->error_flags, s,
-                    l.sm_count, l.sort_items, l.sort_ctas);
+                    l.sm_count, l.sort_items, l.sort_ctas, true);
     if (e != cudaSuccess) return e;
     return cudaGetLastError();
 }
@@ -1690,6 +1689,24 @@ cudaError_t launch_finish_tick(const StepBuffers& b, const StepParams& p, int pa
     (void)p;
     (void)parity;
     k_finish_tick<<<1, 32, 0, s>>>(b);
+    return cudaGetLastError();
+}
+
+// Every region a tick needs at zero, cleared by one kernel (16-byte stores)
+// instead of one memset node per region.
+__global__ void __launch_bounds__(kBlock) k_tick_reset(ZeroList z) {
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    const uint64_t first = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    for (uint32_t r = 0; r < z.count; ++r)
+        for (uint64_t i = first; i < z.n16[r]; i += stride) z.ptr[r][i] = make_uint4(0u, 0u, 0u, 0u);
+}
+
+cudaError_t launch_tick_reset(const ZeroList& z, int sm_count, cudaStream_t s) {
+    uint64_t most = 0;
+    for (uint32_t r = 0; r < z.count; ++r) most = most > z.n16[r] ? most : z.n16[r];
+    const uint32_t grid = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>((most + kBlock - 1) / kBlock,
+                                                                               (uint64_t)sm_count * 4));
+    k_tick_reset<<<grid, kBlock, 0, s>>>(z);
     return cudaGetLastError();
 }
 

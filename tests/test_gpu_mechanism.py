@@ -92,3 +92,13 @@ def test_drive_and_coordinate_counts_are_checked(cuda_lib):
     gpu.write_mechanism_drives(abi.passive_drive_rows(16))
     gpu.dispatch_tick(1)
     assert gpu.read_last_tick().error_flags & abi.INVALID_NUMERIC_FLAG == 0
+
+
+@pytest.mark.parametrize("scenario", ["four_bar", "invalid_loop"])
+def test_bench_runner_linkage_gates(cuda_lib, scenario):
+    """The mechanic-bench gates (main.rs:113-132, 211-216) through the runner."""
+    from mechanic_b200 import bench_cli
+    out = bench_cli.run(scenario, None, None, 120, 0, 1 << 16)
+    assert out["correctness_passed"], out["error_flags"]
+    if scenario == "four_bar":
+        assert out["anchor_residual_m"] <= 1e-5
