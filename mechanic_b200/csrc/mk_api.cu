@@ -148,6 +148,15 @@ uint64_t carve(MkHandle* h, char* base) {
     b.children = c.take<uint2>(C);
     b.parents = c.take<uint32_t>(2ull * C);
     b.visits = c.take<uint32_t>(C);
+    b.node_ranges = c.take<uint2>(C);
+    b.leaf_scan = c.take<float4>(4ull * C);
+    b.chunk_scan = c.take<float4>(6ull * ((C + 31) / 32));
+    {
+        const uint64_t ns = (C + 1023) / 1024;
+        uint64_t levels = 1;
+        while ((1ull << levels) <= ns) ++levels;
+        b.super_table = c.take<float4>(2 * ns * levels);
+    }
     b.node_aabbs = c.take<float4>(4ull * C);
     b.node_records = c.take<float4>(4ull * C);
     b.suppressed = c.take<uint2>(std::max(h->S, 1u));
@@ -217,7 +226,6 @@ cudaError_t enqueue_tick(MkHandle* h, int parity, bool capturing) {
         z.add(b.tickets, 16 * sizeof(uint32_t));
         if (h->residual) z.add(b.solve_stats, sizeof(mk::SolveStats));
         if (h->collisions) {
-            z.add(b.visits, sizeof(uint32_t) * std::max(h->C, 1u));
             z.add(b.deltas, sizeof(int32_t) * 6ull * std::max(h->B, 1u));
             z.add(b.lookback, sizeof(uint64_t) * 4 * b.lookback_words);
             void* r = nullptr;

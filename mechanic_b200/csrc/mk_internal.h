@@ -94,6 +94,10 @@ struct StepBuffers {
     uint2* children;             // C-1
     uint32_t* parents;           // 2C-1
     uint32_t* visits;            // C-1
+    uint2* node_ranges;          // C-1: first and last sorted leaf below each internal node
+    float4* leaf_scan;           // 4 per leaf: prefix and suffix unions within its 32-leaf chunk
+    float4* chunk_scan;          // 6 per chunk: total, prefix and suffix unions within its 1024-leaf super-chunk
+    float4* super_table;         // 2 x super-chunks x levels: sparse table of super-chunk totals
     float4* node_aabbs;          // 2 x float4 per node (union boxes)
     float4* node_records;        // 4 x float4 per internal node (both children's boxes)
     const uint2* suppressed;

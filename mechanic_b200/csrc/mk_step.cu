@@ -218,6 +218,7 @@ __global__ void __launch_bounds__(kBlock) k_karras(StepBuffers b, StepParams p) 
     b.children[i] = make_uint2(left, right);
     b.parents[left] = (uint32_t)i + 1u;
     b.parents[right] = (uint32_t)i + 1u;
+    b.node_ranges[i] = make_uint2((uint32_t)first, (uint32_t)last);
 }
 
 // lbvh.wgsl:280-319: leaf boxes in sorted order, then a bottom-up climb where
@@ -229,47 +230,168 @@ __global__ void __launch_bounds__(kBlock) k_karras(StepBuffers b, StepParams p) 
 // for a leaf; "last" is the largest sorted leaf position below the child.
 constexpr uint32_t kLeafCode = 0x80000000u;
 
-__global__ void __launch_bounds__(kBlock) k_refit(StepBuffers b, StepParams p) {
+// Parallel refit.  An internal node covers a contiguous range of sorted
+// leaves (Karras), so its box is the union of the leaf boxes in that range;
+// unions are min/max, exact in any order, so this equals the bottom-up climb
+// of lbvh.wgsl:280-319 without its serial chain of tree depth.  Range unions
+// come from prefix/suffix unions within 32-leaf chunks (warp scans), within
+// 1024-leaf super-chunks (over chunk totals) and a sparse table over the
+// super-chunk totals.
+constexpr uint32_t kRefitBlock = 1024;   // one super-chunk of 32 chunks per block
+
+struct Box2 {
+    float4 mn, mx;
+};
+__device__ __forceinline__ Box2 box_empty() {
+    return {make_float4(kFloatMax, kFloatMax, kFloatMax, 0.0f), make_float4(-kFloatMax, -kFloatMax, -kFloatMax, 0.0f)};
+}
+__device__ __forceinline__ Box2 box_union(Box2 a, Box2 c) {
+    return {make_float4(mnf(a.mn.x, c.mn.x), mnf(a.mn.y, c.mn.y), mnf(a.mn.z, c.mn.z), 0.0f),
+            make_float4(mxf(a.mx.x, c.mx.x), mxf(a.mx.y, c.mx.y), mxf(a.mx.z, c.mx.z), 0.0f)};
+}
+__device__ __forceinline__ Box2 shfl_box(Box2 v, int o, bool up) {
+    Box2 r;
+    float* d = reinterpret_cast<float*>(&r);
+    const float* q = reinterpret_cast<const float*>(&v);
+#pragma unroll
+    for (int k = 0; k < 8; ++k)
+        d[k] = up ? __shfl_up_sync(0xffffffffu, q[k], o) : __shfl_down_sync(0xffffffffu, q[k], o);
+    return r;
+}
+__device__ __forceinline__ Box2 ld_box(const float4* p) { return {__ldg(p), __ldg(p + 1)}; }   // written by earlier launches
+__device__ __forceinline__ Box2 ld_box_cg(const float4* p) { return {__ldcg(p), __ldcg(p + 1)}; }
+__device__ __forceinline__ void st_box(float4* p, Box2 v) { p[0] = v.mn; p[1] = v.mx; }
+
+// Leaf boxes in sorted order, their prefix/suffix unions within 32-leaf chunks,
+// the chunks' prefix/suffix unions within the block's super-chunk, and the
+// super-chunk's total (level 0 of the sparse table).
+__global__ void __launch_bounds__(kRefitBlock) k_refit_leaves(StepBuffers b, StepParams p) {
+    __shared__ Box2 s_chunk[32];
     const uint32_t n = p.collider_count;
-    const uint32_t leaf = blockIdx.x * blockDim.x + threadIdx.x;
-    if (leaf >= n) return;
+    const uint32_t t = blockIdx.x * kRefitBlock + threadIdx.x;
+    const uint32_t lane = lane_id(), w = warp_id();
     const uint32_t leaf_base = n - 1;
-    const uint32_t j = b.svals[leaf];
-    float4 mn = b.aabbs[2ull * j], mx = b.aabbs[2ull * j + 1];
-    mn.w = __uint_as_float(leaf);
-    uint32_t cur = leaf_base + leaf;
-    b.node_aabbs[2ull * cur] = mn;
-    b.node_aabbs[2ull * cur + 1] = mx;
-    if (n <= 1) return;
-    for (uint32_t guard = 0; guard < 2 * n; ++guard) {
-        const uint32_t ep = b.parents[cur];
-        if (ep == 0u) return;
-        const uint32_t parent = ep - 1u;
-        // release: this node's box is visible to whoever arrives second;
-        // acquire: the sibling's box (released by its add) is visible to us
-        const uint32_t arrival = atomic_add_acq_rel(&b.visits[parent], 1u);
-        if (arrival == 0u) return;
-        if (arrival > 1u) {
-            atomicOr(&b.diag->error_flags, MK_PAIR_OVERFLOW_FLAG);
-            return;
-        }
-        const uint2 ch = b.children[parent];
-        const float4 lmn = __ldcg(b.node_aabbs + 2ull * ch.x), lmx = __ldcg(b.node_aabbs + 2ull * ch.x + 1);
-        const float4 rmn = __ldcg(b.node_aabbs + 2ull * ch.y), rmx = __ldcg(b.node_aabbs + 2ull * ch.y + 1);
-        const uint32_t lcode = ch.x >= leaf_base ? (kLeafCode | b.svals[ch.x - leaf_base]) : ch.x;
-        const uint32_t rcode = ch.y >= leaf_base ? (kLeafCode | b.svals[ch.y - leaf_base]) : ch.y;
-        float4* rec = b.node_records + 4ull * parent;
-        rec[0] = make_float4(lmn.x, lmn.y, lmn.z, __uint_as_float(lcode));
-        rec[1] = make_float4(lmx.x, lmx.y, lmx.z, lmn.w);
-        rec[2] = make_float4(rmn.x, rmn.y, rmn.z, __uint_as_float(rcode));
-        rec[3] = make_float4(rmx.x, rmx.y, rmx.z, rmn.w);
-        float4 pm = make_float4(mnf(lmn.x, rmn.x), mnf(lmn.y, rmn.y), mnf(lmn.z, rmn.z),
-                                __uint_as_float(max(__float_as_uint(lmn.w), __float_as_uint(rmn.w))));
-        float4 px = make_float4(mxf(lmx.x, rmx.x), mxf(lmx.y, rmx.y), mxf(lmx.z, rmx.z), 0.0f);
-        b.node_aabbs[2ull * parent] = pm;
-        b.node_aabbs[2ull * parent + 1] = px;
-        cur = parent;
+    Box2 v = box_empty();
+    if (t < n) {
+        const uint32_t j = b.svals[t];
+        float4 mn = b.aabbs[2ull * j], mx = b.aabbs[2ull * j + 1];
+        mn.w = __uint_as_float(t);
+        b.node_aabbs[2ull * (leaf_base + t)] = mn;
+        b.node_aabbs[2ull * (leaf_base + t) + 1] = mx;
+        v = {make_float4(mn.x, mn.y, mn.z, 0.0f), make_float4(mx.x, mx.y, mx.z, 0.0f)};
     }
+    Box2 pre = v, suf = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const Box2 u = shfl_box(pre, o, true);
+        if ((int)lane >= o) pre = box_union(pre, u);
+        const Box2 d = shfl_box(suf, o, false);
+        if ((int)lane + o < 32) suf = box_union(suf, d);
+    }
+    if (t < n) {
+        float4* ls = b.leaf_scan + 4ull * t;
+        ls[0] = pre.mn; ls[1] = pre.mx; ls[2] = suf.mn; ls[3] = suf.mx;
+    }
+    if (lane == 31) s_chunk[w] = pre;
+    __syncthreads();
+    if (w == 0) {
+        const Box2 c = s_chunk[lane];
+        Box2 cp = c, cs = c;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const Box2 u = shfl_box(cp, o, true);
+            if ((int)lane >= o) cp = box_union(cp, u);
+            const Box2 d = shfl_box(cs, o, false);
+            if ((int)lane + o < 32) cs = box_union(cs, d);
+        }
+        const uint32_t chunk = blockIdx.x * 32 + lane;
+        if ((uint64_t)chunk * 32 < n) {
+            float4* cr = b.chunk_scan + 6ull * chunk;   // total, prefix, suffix within the super-chunk
+            cr[0] = c.mn; cr[1] = c.mx; cr[2] = cp.mn; cr[3] = cp.mx; cr[4] = cs.mn; cr[5] = cs.mx;
+        }
+        if (lane == 31) st_box(b.super_table + 2ull * blockIdx.x, cp);
+    }
+}
+
+// Sparse table over the super-chunk totals: level k holds unions of 2^k of them.
+__global__ void __launch_bounds__(1024) k_refit_super(StepBuffers b, StepParams p) {
+    const uint32_t n = p.collider_count;
+    const uint32_t ns = (n + kRefitBlock - 1) / kRefitBlock;
+    for (uint32_t k = 1; (1u << k) <= ns; ++k) {
+        const float4* src = b.super_table + 2ull * ns * (k - 1);
+        float4* dst = b.super_table + 2ull * ns * k;
+        const uint32_t half = 1u << (k - 1);
+        for (uint32_t s = threadIdx.x; s + (1u << k) <= ns; s += blockDim.x)
+            st_box(dst + 2ull * s, box_union(ld_box_cg(src + 2ull * s), ld_box_cg(src + 2ull * (s + half))));
+        __threadfence_block();
+        __syncthreads();
+    }
+}
+
+__device__ __forceinline__ Box2 leaf_box(const StepBuffers& b, uint32_t leaf_base, uint32_t t) {
+    const float4* q = b.node_aabbs + 2ull * (leaf_base + t);
+    const float4 mn = __ldg(q), mx = __ldg(q + 1);
+    return {make_float4(mn.x, mn.y, mn.z, 0.0f), make_float4(mx.x, mx.y, mx.z, 0.0f)};
+}
+
+// Union of the chunk totals [c0, c1] inside one super-chunk.
+__device__ __forceinline__ Box2 chunks_union(const StepBuffers& b, uint32_t c0, uint32_t c1) {
+    if ((c0 & 31u) == 0) return ld_box(b.chunk_scan + 6ull * c1 + 2);   // prefix of c1
+    if ((c1 & 31u) == 31u) return ld_box(b.chunk_scan + 6ull * c0 + 4);   // suffix of c0
+    Box2 u = box_empty();
+    for (uint32_t c = c0; c <= c1; ++c) u = box_union(u, ld_box(b.chunk_scan + 6ull * c));
+    return u;
+}
+
+// Union of the sorted leaves [f, l].
+__device__ Box2 range_box(const StepBuffers& b, uint32_t n, uint32_t f, uint32_t l) {
+    const uint32_t leaf_base = n - 1;
+    const uint32_t cf = f >> 5, cl = l >> 5;
+    if (cf == cl) {
+        if ((f & 31u) == 0) return ld_box(b.leaf_scan + 4ull * l);        // prefix of l
+        if ((l & 31u) == 31u || l == n - 1) return ld_box(b.leaf_scan + 4ull * f + 2);   // suffix of f
+        Box2 u = box_empty();
+        for (uint32_t t = f; t <= l; ++t) u = box_union(u, leaf_box(b, leaf_base, t));
+        return u;
+    }
+    Box2 u = box_union(ld_box(b.leaf_scan + 4ull * f + 2), ld_box(b.leaf_scan + 4ull * l));
+    if (cf + 1 > cl - 1) return u;
+    const uint32_t a = cf + 1, z = cl - 1;
+    const uint32_t sa = a >> 5, sz = z >> 5;
+    if (sa == sz) return box_union(u, chunks_union(b, a, z));
+    u = box_union(u, ld_box(b.chunk_scan + 6ull * a + 4));   // suffix of a within its super-chunk
+    u = box_union(u, ld_box(b.chunk_scan + 6ull * z + 2));   // prefix of z within its super-chunk
+    if (sa + 1 <= sz - 1) {
+        const uint32_t ns = (n + kRefitBlock - 1) / kRefitBlock;
+        const uint32_t lo = sa + 1, hi = sz - 1, len = hi - lo + 1;
+        const uint32_t k = 31u - __clz(len);
+        const float4* lvl = b.super_table + 2ull * ns * k;
+        u = box_union(u, box_union(ld_box(lvl + 2ull * lo), ld_box(lvl + 2ull * (hi + 1 - (1u << k)))));
+    }
+    return u;
+}
+
+// Per internal node: both children's boxes, its traversal record and union.
+__global__ void __launch_bounds__(kBlock) k_refit_nodes(StepBuffers b, StepParams p) {
+    const uint32_t n = p.collider_count;
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (n <= 1 || i >= n - 1) return;
+    const uint32_t leaf_base = n - 1;
+    const uint2 ch = b.children[i];
+    const uint2 rg = b.node_ranges[i];
+    const uint32_t split = ch.x >= leaf_base ? ch.x - leaf_base : ch.x;
+    const Box2 lb = range_box(b, n, rg.x, split);
+    const Box2 rb = range_box(b, n, split + 1, rg.y);
+    const uint32_t lcode = ch.x >= leaf_base ? (kLeafCode | b.svals[ch.x - leaf_base]) : ch.x;
+    const uint32_t rcode = ch.y >= leaf_base ? (kLeafCode | b.svals[ch.y - leaf_base]) : ch.y;
+    float4* rec = b.node_records + 4ull * i;
+    rec[0] = make_float4(lb.mn.x, lb.mn.y, lb.mn.z, __uint_as_float(lcode));
+    rec[1] = make_float4(lb.mx.x, lb.mx.y, lb.mx.z, __uint_as_float(split));
+    rec[2] = make_float4(rb.mn.x, rb.mn.y, rb.mn.z, __uint_as_float(rcode));
+    rec[3] = make_float4(rb.mx.x, rb.mx.y, rb.mx.z, __uint_as_float(rg.y));
+    b.node_aabbs[2ull * i] = make_float4(mnf(lb.mn.x, rb.mn.x), mnf(lb.mn.y, rb.mn.y), mnf(lb.mn.z, rb.mn.z),
+                                         __uint_as_float(rg.y));
+    b.node_aabbs[2ull * i + 1] = make_float4(mxf(lb.mx.x, rb.mx.x), mxf(lb.mx.y, rb.mx.y), mxf(lb.mx.z, rb.mx.z), 0.0f);
 }
 
 // ---------------------------------------------------------------- traverse
@@ -629,69 +751,84 @@ __global__ void __launch_bounds__(kBlock) k_narrowphase(StepBuffers b, StepParam
 }
 
 // collision.wgsl:175-238 and :622-664: analytic contact with the y = 0 plane.
+// One collider's analytic ground contact: support point (or analytic rim
+// point of a full cylinder segment) and whether it emits.
+__device__ __forceinline__ bool ground_point(const StepBuffers& b, uint32_t i, f3& sp, uint32_t& body,
+                                             uint32_t& role) {
+    const Box o = make_box(b.boxes, i);
+    const float4 r2 = __ldg(b.boxes + 3ull * i + 2);
+    body = __float_as_uint(r2.z);
+    role = __float_as_uint(r2.w);
+    const f3 down = mkf3(0, -1, 0);
+    sp = support_point(o, down);
+    if (role != 0u) {
+        const float center_radius = __ldg(b.colliders + 4ull * i).w;
+        const float outer_radius = __ldg(b.colliders + 4ull * i + 2).w;
+        const f3 caxis = o.ax[1];
+        const float ap = dot(caxis, down);
+        const f3 radial = down - caxis * ap;
+        const float rl = length(radial);
+        const uint32_t cc = rl < 0.05f ? 4u : 1u;
+        if (role > cc) return false;
+        f3 q = o.c - o.ax[0] * center_radius;
+        if (rl < 0.05f) {
+            q = q + caxis * sgnf(ap) * o.h[1];
+            const f3 ta = normalize(mkf3(1, 0, 0) - caxis * caxis.x);
+            const f3 tb = normalize(cross(caxis, ta));
+            if (role == 1u) q = q + ta * outer_radius;
+            else if (role == 2u) q = q - ta * outer_radius;
+            else if (role == 3u) q = q + tb * outer_radius;
+            else q = q - tb * outer_radius;
+        } else {
+            q = q + radial * (outer_radius / rl);
+            if (fabsf(ap) >= 0.05f) q = q + caxis * sgnf(ap) * o.h[1];
+        }
+        sp = q;
+    }
+    return !(sp.y > 1.0e-5f);
+}
+
+// Ground contacts in collider order after the narrowphase's.  Each thread
+// takes kGroundItems consecutive colliders, so a tile covers
+// kBlock x kGroundItems of them and the ordered append needs a quarter of the
+// look-back steps (few colliders touch the ground).
+constexpr uint32_t kGroundItems = 4;
 __global__ void __launch_bounds__(kBlock) k_ground(StepBuffers b, StepParams p, AppendSite site, GpuContact* out,
                                                    uint64_t* out_keys, uint32_t* out_feat) {
     __shared__ uint32_t s_scan[33];
     __shared__ uint32_t s_tile;
     __shared__ uint64_t s_prefix;
     const uint32_t n = p.collider_count;
-    const uint32_t tiles = (n + kBlock - 1) / kBlock;
+    constexpr uint32_t kTileItems = kBlock * kGroundItems;
+    const uint32_t tiles = (n + kTileItems - 1) / kTileItems;
     const uint32_t narrow = b.counts->narrow;
     const uint32_t requested_narrow = b.counts->requested_contacts;
     for (;;) {
         const uint32_t tile = take_tile(site.ticket, &s_tile);
         if (tile >= tiles) break;
-        const uint32_t i = tile * kBlock + threadIdx.x;
-        bool emit = false;
-        f3 sp = mkf3(0, 0, 0);
-        uint32_t body = 0, role = 0;
-        if (i < n) {
-            const Box o = make_box(b.boxes, i);
-            const float4 r2 = __ldg(b.boxes + 3ull * i + 2);
-            body = __float_as_uint(r2.z);
-            role = __float_as_uint(r2.w);
-            const f3 down = mkf3(0, -1, 0);
-            sp = support_point(o, down);
-            bool skip = false;
-            if (role != 0u) {
-                const float center_radius = __ldg(b.colliders + 4ull * i).w;
-                const float outer_radius = __ldg(b.colliders + 4ull * i + 2).w;
-                const f3 caxis = o.ax[1];
-                const float ap = dot(caxis, down);
-                const f3 radial = down - caxis * ap;
-                const float rl = length(radial);
-                const uint32_t cc = rl < 0.05f ? 4u : 1u;
-                if (role > cc) {
-                    skip = true;
-                } else {
-                    f3 q = o.c - o.ax[0] * center_radius;
-                    if (rl < 0.05f) {
-                        q = q + caxis * sgnf(ap) * o.h[1];
-                        const f3 ta = normalize(mkf3(1, 0, 0) - caxis * caxis.x);
-                        const f3 tb = normalize(cross(caxis, ta));
-                        if (role == 1u) q = q + ta * outer_radius;
-                        else if (role == 2u) q = q - ta * outer_radius;
-                        else if (role == 3u) q = q + tb * outer_radius;
-                        else q = q - tb * outer_radius;
-                    } else {
-                        q = q + radial * (outer_radius / rl);
-                        if (fabsf(ap) >= 0.05f) q = q + caxis * sgnf(ap) * o.h[1];
-                    }
-                    sp = q;
-                }
-            }
-            emit = !skip && !(sp.y > 1.0e-5f);
+        const uint32_t first = tile * kTileItems + threadIdx.x * kGroundItems;
+        uint32_t mask = 0;
+        for (uint32_t k = 0; k < kGroundItems; ++k) {
+            f3 sp;
+            uint32_t body, role;
+            if (first + k < n && ground_point(b, first + k, sp, body, role)) mask |= 1u << k;
         }
         uint32_t total;
-        const uint32_t ex = block_exclusive_scan(emit ? 1u : 0u, s_scan, &total);
+        const uint32_t ex = block_exclusive_scan((uint32_t)__popc(mask), s_scan, &total);
         if (warp_id() == 0) {
             uint64_t pre = tile_lookback(site.states, tile, total, &b.diag->error_flags);
             if (lane_id() == 0) s_prefix = pre;
         }
         __syncthreads();
         const uint64_t pre = s_prefix;
-        if (emit) {
-            const uint64_t o = (uint64_t)narrow + pre + ex;
+        uint32_t q = 0;
+        for (uint32_t k = 0; k < kGroundItems; ++k) {
+            if (!((mask >> k) & 1u)) continue;
+            const uint32_t i = first + k;
+            f3 sp;
+            uint32_t body, role;
+            ground_point(b, i, sp, body, role);   // recomputed: identical arithmetic, fewer live registers
+            const uint64_t o = (uint64_t)narrow + pre + ex + q++;
             if (o < p.pair_capacity) {
                 store_contact(out + o, body, kInvalid, i, kInvalid, make_float4(0.0f, -1.0f, 0.0f, mxf(-sp.y, 0.0f)),
                               f4(sp - xyz(b.pos[body]), 0.0f), make_float4(0.0f, 0.0f, 0.0f, role != 0u ? -1.0f : 0.0f));
@@ -1590,7 +1727,9 @@ cudaError_t launch_broadphase(const StepBuffers& b, const StepParams& p, const S
                                 true);   // bins and tickets cleared by the tick's reset
     if (e != cudaSuccess) return e;
     k_karras<<<blocks_for(C, kBlock), kBlock, 0, s>>>(b, p);
-    k_refit<<<blocks_for(C, kBlock), kBlock, 0, s>>>(b, p);
+    k_refit_leaves<<<blocks_for(C, kRefitBlock), kRefitBlock, 0, s>>>(b, p);
+    k_refit_super<<<1, 1024, 0, s>>>(b, p);
+    k_refit_nodes<<<blocks_for(C, kBlock), kBlock, 0, s>>>(b, p);
     k_traverse<<<blocks_for(C, kTravThreads), kTravThreads, 0, s>>>(b, p);
     e = launch_sort(b.pair_stage, nullptr, b.pair_keys, nullptr, p.pair_capacity, &b.counts->pairs_found,
                     2 * p.pair_shift, b.pair_sort_scratch, b.pair_sort_scratch_bytes, &b.diag->error_flags, s,
@@ -1605,7 +1744,7 @@ cudaError_t launch_narrowphase(const StepBuffers& b, const StepParams& p, const 
     AppendSite narrow{b.lookback + 1 * b.lookback_words, b.tickets + 1};
     AppendSite ground{b.lookback + 2 * b.lookback_words, b.tickets + 2};
     k_narrowphase<<<grid, kBlock, 0, s>>>(b, p, narrow, b.contacts[parity], b.contact_keys[parity], b.features[parity]);
-    k_ground<<<std::min<uint32_t>(grid, blocks_for(p.collider_count, kBlock) + 1), kBlock, 0, s>>>(
+    k_ground<<<std::min<uint32_t>(grid, blocks_for(p.collider_count, kBlock * kGroundItems) + 1), kBlock, 0, s>>>(
         b, p, ground, b.contacts[parity], b.contact_keys[parity], b.features[parity]);
     return cudaGetLastError();
 }
