@@ -136,6 +136,8 @@ uint64_t carve(MkHandle* h, char* base) {
     b.root_flags = c.take<uint32_t>(B);
     b.components = nullptr;
     b.deltas = c.take<int32_t>(6ull * B);
+    b.deltas_extra = c.take<int32_t>(2 * ((6ull * B + 3) & ~3ull));
+    b.body_stamp = c.take<uint32_t>(B);
     b.snap_pos = c.take<float4>(3ull * B);
     b.snap_rot = c.take<float4>(3ull * B);
     b.colliders = c.take<float4>(4ull * C);
@@ -783,6 +785,7 @@ int mk_dispatch_tick(MkHandle* h, uint64_t tick_index, MkSubmission* out) {
     std::memset(&t, 0, sizeof(t));
     t.tick_index = (uint32_t)tick_index;    // wrapping_u32 (device.rs:868)
     t.snapshot_slot = (uint32_t)(tick_index % 3);
+    t.generation = (uint32_t)sub;
     cudaError_t e = cudaMemcpyAsync(h->buf.tick, &t, sizeof(t), cudaMemcpyHostToDevice, h->stream);
     const int parity = h->parity;
     if (e == cudaSuccess) {

@@ -19,7 +19,8 @@ void set_last_error(const char* msg);
 struct DevTick {
     uint32_t tick_index;
     uint32_t snapshot_slot;
-    uint32_t pad[14];
+    uint32_t generation;       // dispatch counter of the handle (never repeats, unlike tick_index)
+    uint32_t pad[13];
 };
 
 // Counts produced on the device during a tick.  `prev_*` describe the
@@ -83,6 +84,9 @@ struct StepBuffers {
     const uint32_t* root_flags;
     const uint32_t* components;  // null unless mechanism self-collisions are disabled
     int32_t* deltas;             // 6 per body
+    int32_t* deltas_extra;       // 2 buffers of 6 per body (each padded to 16 bytes): with `deltas`, the
+                                 // rotating deltas of the fused solve
+    uint32_t* body_stamp;        // generation of the last tick whose contacts touched the body
     float4 *snap_pos, *snap_rot; // ring base, slot-major
     const float4* colliders;     // GpuCollider rows (4 x float4)
     float4* boxes;               // 3 x float4 per collider (world box)

@@ -1005,10 +1005,45 @@ __device__ __forceinline__ f3 contact_velocity_it(const float4* vl, const float4
     return xyz(__ldg(vl + body)) + cross(xyz(__ldg(va + body)), arm);
 }
 
-template <bool kWarm>
+// Fused pass (light ticks): a pass computes the velocities of its contacts'
+// bodies itself, as the apply of the previous pass would (V_k = V_{k-1} +
+// D_{k-1} / 2^20, the same float operations), stores them as V_k for the next
+// pass, and accumulates into the next of three rotating delta buffers, so a
+// pass needs one grid barrier and no apply over all bodies.
+struct FusedPass {
+    uint32_t it;                 // pass index
+    const float4 *pl, *pa;       // V_{it-1} (it > 0), or V_0 (it == 0)
+    const int32_t* dprev;        // D_{it-1}
+    float4 *cl, *ca;             // V_it (it > 0)
+    uint32_t gen;                // generation stamped on touched bodies (pass 0)
+};
+
+__device__ __forceinline__ void fused_body(const StepBuffers& b, const FusedPass& f, uint32_t x, f3& lin, f3& ang) {
+    if (f.it == 0) {
+        lin = xyz(__ldg(f.pl + x));
+        ang = xyz(__ldg(f.pa + x));
+        b.body_stamp[x] = f.gen;
+        return;
+    }
+    const float s = (float)kFixedScale;
+    const int2* d2 = reinterpret_cast<const int2*>(f.dprev + 6ull * x);
+    const int2 x0 = __ldcg(d2), x1 = __ldcg(d2 + 1), x2 = __ldcg(d2 + 2);
+    const f3 ld = mkf3((float)x0.x, (float)x0.y, (float)x1.x) / s;
+    const f3 ad = mkf3((float)x1.y, (float)x2.x, (float)x2.y) / s;
+    const float4 nl = f4(xyz(__ldg(f.pl + x)) + ld, 0.0f);
+    const float4 na = f4(xyz(__ldg(f.pa + x)) + ad, 0.0f);
+    f.cl[x] = nl;   // every contact of the body stores the same value
+    f.ca[x] = na;
+    lin = xyz(nl);
+    ang = xyz(na);
+}
+
+template <bool kWarm, bool kFused = false>
 __device__ __forceinline__ void solve_span(const StepBuffers& b, const StepParams& p, GpuContact* cur, uint32_t A,
-                                           uint32_t first, uint32_t stride, const float4* vl, const float4* va) {
+                                           uint32_t first, uint32_t stride, const float4* vl, const float4* va,
+                                           const FusedPass* fp = nullptr, int32_t* dacc = nullptr) {
     const float scale = (float)kFixedScale;
+    int32_t* deltas = kFused ? dacc : b.deltas;
     for (uint32_t base = first; base < A; base += stride) {
         const uint32_t t = base + threadIdx.x;
         bool live = false;
@@ -1023,12 +1058,17 @@ __device__ __forceinline__ void solve_span(const StepBuffers& b, const StepParam
             const f3 arm_a = xyz(aa), arm_b = xyz(ab);
             const float4* wa = b.world_mass + 3ull * a;
             const float4* wb = bb != kInvalid ? b.world_mass + 3ull * bb : nullptr;
+            f3 la = mkf3(0, 0, 0), ga = mkf3(0, 0, 0), lb = mkf3(0, 0, 0), gb = mkf3(0, 0, 0);
+            if (kFused) {
+                fused_body(b, *fp, a, la, ga);
+                if (bb != kInvalid) fused_body(b, *fp, bb, lb, gb);
+            }
             f3 vb = mkf3(0, 0, 0);
-            if (bb != kInvalid) vb = contact_velocity_it(vl, va, bb, arm_b);
+            if (bb != kInvalid) vb = kFused ? lb + cross(gb, arm_b) : contact_velocity_it(vl, va, bb, arm_b);
             const f3 nrm = xyz(np);
             const float den = impulse_denominator(wa, wb, arm_a, arm_b, nrm);
             if (!(den <= 0.0f)) {
-                const f3 rel = vb - contact_velocity_it(vl, va, a, arm_a);
+                const f3 rel = vb - (kFused ? la + cross(ga, arm_a) : contact_velocity_it(vl, va, a, arm_a));
                 const float vn = dot(rel, nrm);
                 if (np.w <= 1.0e-5f && vn >= -1.0e-5f && aa.w <= 1.0e-6f) {
                     row[2] = f4(arm_a, 0.0f);
@@ -1075,13 +1115,13 @@ __device__ __forceinline__ void solve_span(const StepBuffers& b, const StepParam
         const uint32_t key_a = live ? a : kInvalid;
         const bool tail = run_tail_sum(key_a, da, 6);
         if (tail && key_a != kInvalid) {
-            int32_t* d = b.deltas + 6ull * key_a;
+            int32_t* d = deltas + 6ull * key_a;
 #pragma unroll
             for (int c = 0; c < 6; ++c)
                 if (da[c]) atomicAdd(d + c, da[c]);
         }
         if (live && bb != kInvalid) {
-            int32_t* d = b.deltas + 6ull * bb;
+            int32_t* d = deltas + 6ull * bb;
 #pragma unroll
             for (int c = 0; c < 6; ++c)
                 if (db[c]) atomicAdd(d + c, db[c]);
@@ -1164,6 +1204,52 @@ __global__ void __launch_bounds__(kSolveThreads) k_solve_all(StepBuffers b, Step
     const uint32_t first = blockIdx.x * blockDim.x;
     const uint32_t stride = parts * blockDim.x;
     const size_t B = p.body_count;
+    if (A <= 2u * p.body_count && b.deltas_extra && b.body_stamp) {
+        // fused passes: one grid barrier per pass, one apply at the end
+        const uint64_t dstride = (6ull * B + 3) & ~3ull;   // keeps every delta buffer 16-byte aligned
+        int32_t* D[3] = {b.deltas, b.deltas_extra, b.deltas_extra + dstride};
+        const uint32_t gen = b.tick->generation;
+        const uint32_t gtid = first + threadIdx.x;
+        for (uint32_t it = 0; it < iterations; ++it) {
+            FusedPass fp;
+            fp.it = it;
+            fp.pl = it <= 1 ? b.lin : b.vel_iter + (2 * (it - 2)) * B;
+            fp.pa = it <= 1 ? b.ang : b.vel_iter + (2 * (it - 2) + 1) * B;
+            fp.dprev = it == 0 ? nullptr : D[(it - 1) % 3];
+            fp.cl = it == 0 ? nullptr : b.vel_iter + (2 * (it - 1)) * B;
+            fp.ca = it == 0 ? nullptr : b.vel_iter + (2 * (it - 1) + 1) * B;
+            fp.gen = gen;
+            if (it == 0) solve_span<true, true>(b, p, cur, A, first, stride, nullptr, nullptr, &fp, D[0]);
+            else solve_span<false, true>(b, p, cur, A, first, stride, nullptr, nullptr, &fp, D[it % 3]);
+            int4* dz = reinterpret_cast<int4*>(D[(it + 1) % 3]);   // dead since the last barrier; used next pass
+            for (uint64_t i = gtid; i < (6ull * B) / 4; i += stride) dz[i] = make_int4(0, 0, 0, 0);
+            if (gtid == 0 && (6ull * B) % 4) {
+                for (uint64_t i = (6ull * B) & ~3ull; i < 6ull * B; ++i) D[(it + 1) % 3][i] = 0;
+            }
+            grid_barrier(barrier, &b.diag->error_flags, parts);
+        }
+        // the apply of the last pass, for every body (bodies no contact touched
+        // get the reference's apply of zero deltas)
+        const float s = (float)kFixedScale;
+        const float4* vl = iterations <= 1 ? b.lin : b.vel_iter + (2 * (iterations - 2)) * B;
+        const float4* va = iterations <= 1 ? b.ang : b.vel_iter + (2 * (iterations - 2) + 1) * B;
+        const int32_t* dl = D[(iterations - 1) % 3];
+        for (uint32_t i = gtid; i < B; i += stride) {
+            const bool touched = __ldcg(b.body_stamp + i) == gen;
+            int2 x0 = make_int2(0, 0), x1 = x0, x2 = x0;
+            if (touched) {
+                const int2* d2 = reinterpret_cast<const int2*>(dl + 6ull * i);
+                x0 = __ldcg(d2); x1 = __ldcg(d2 + 1); x2 = __ldcg(d2 + 2);
+            }
+            const f3 ld = mkf3((float)x0.x, (float)x0.y, (float)x1.x) / s;
+            const f3 ad = mkf3((float)x1.y, (float)x2.x, (float)x2.y) / s;
+            const float4 sl = touched ? __ldg(vl + i) : __ldg(b.lin + i);
+            const float4 sa = touched ? __ldg(va + i) : __ldg(b.ang + i);
+            b.lin[i] = f4(xyz(sl) + ld, 0.0f);
+            b.ang[i] = f4(xyz(sa) + ad, 0.0f);
+        }
+        return;
+    }
     for (uint32_t it = 0; it < iterations; ++it) {
         // iteration `it` reads buffer it (0 = the integrated velocities) and
         // its apply writes buffer it + 1 (the last one back into lin/ang)
