@@ -276,7 +276,8 @@ typedef struct MkConfig {
 #define MK_PRECOND_LEARNED      1u  /* 2 x 2 blocks of consecutive closure coordinates, inverse from the network */
 #define MK_PRECOND_PAIR_BLOCKS  2u  /* 2 x 2 blocks, exact 2 x 2 inverse (the learned form's own baseline) */
 
-#define MK_MORTON_63            0u  /* 21 bits/axis over [-512, 512) m, index tie-break through a stable sort */
+#define MK_MORTON_63            0u  /* 21 bits/axis over the tick's bounds of the collider centres (cubic cells),
+                                       index tie-break through a stable sort */
 #define MK_MORTON_REFERENCE_30  1u  /* lbvh.wgsl:93-98: 10 bits/axis, 1 m cells */
 
 #define MK_CLOSURE_REFERENCE    0u  /* closure.wgsl:333-427: 8 fixed diagonal-PCG rounds per Newton step */

@@ -150,6 +150,7 @@ uint64_t carve(MkHandle* h, char* base) {
     b.children = c.take<uint2>(C);
     b.parents = c.take<uint32_t>(2ull * C);
     b.visits = c.take<uint32_t>(C);
+    b.scene_bounds = c.take<uint32_t>(8);
     b.node_ranges = c.take<uint2>(C);
     b.leaf_scan = c.take<float4>(4ull * C);
     b.chunk_scan = c.take<float4>(6ull * ((C + 31) / 32));
@@ -229,6 +230,7 @@ cudaError_t enqueue_tick(MkHandle* h, int parity, bool capturing) {
         if (h->residual) z.add(b.solve_stats, sizeof(mk::SolveStats));
         if (h->collisions) {
             z.add(b.deltas, sizeof(int32_t) * 6ull * std::max(h->B, 1u));
+            z.add(b.scene_bounds, 8 * sizeof(uint32_t));
             z.add(b.lookback, sizeof(uint64_t) * 4 * b.lookback_words);
             void* r = nullptr;
             uint64_t rb = 0;

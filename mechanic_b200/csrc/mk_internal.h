@@ -123,6 +123,7 @@ struct StepBuffers {
     void* sort_scratch;
     uint64_t sort_scratch_bytes;
     // batched scenes (null for a single scene)
+    uint32_t* scene_bounds;      // 8 words, zeroed each tick: ordered max and complemented min of the centres
     uint32_t* collider_scene;    // scene of each collider
     uint32_t* scene_end;         // per scene: end of its sorted leaf positions
     // contact solve to a residual (null unless enabled at creation)

@@ -137,44 +137,98 @@ __device__ __forceinline__ uint32_t morton30(f3 c) {
     uint32_t qz = (uint32_t)clampf(floorf(c.z + 512.0f), 0.0f, 1023.0f);
     return expand10(qx) | (expand10(qy) << 1) | (expand10(qz) << 2);
 }
-// 21 bits per axis over the same [-512, 512) box: 2048 cells per metre.
-__device__ __forceinline__ uint64_t morton63(f3 c) {
-    uint64_t qx = (uint64_t)clampf(floorf((c.x + 512.0f) * 2048.0f), 0.0f, 2097151.0f);
-    uint64_t qy = (uint64_t)clampf(floorf((c.y + 512.0f) * 2048.0f), 0.0f, 2097151.0f);
-    uint64_t qz = (uint64_t)clampf(floorf((c.z + 512.0f) * 2048.0f), 0.0f, 2097151.0f);
+// 21 bits per axis over the tick's bounds of the collider centres (cubic
+// cells: one scale from the largest extent), so the keys stay distinct however
+// far the scene spreads.
+__device__ __forceinline__ uint64_t morton63(f3 c, f3 lo, float scale) {
+    uint64_t qx = (uint64_t)clampf(floorf((c.x - lo.x) * scale), 0.0f, 2097151.0f);
+    uint64_t qy = (uint64_t)clampf(floorf((c.y - lo.y) * scale), 0.0f, 2097151.0f);
+    uint64_t qz = (uint64_t)clampf(floorf((c.z - lo.z) * scale), 0.0f, 2097151.0f);
     return expand21(qx) | (expand21(qy) << 1) | (expand21(qz) << 2);
+}
+// Floats as unsigned integers in the same order (-0 below +0), for exact
+// order-free min / max with integer atomics.
+__device__ __forceinline__ uint32_t float_order(float f) {
+    const uint32_t u = __float_as_uint(f);
+    return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+__device__ __forceinline__ float float_unorder(uint32_t v) {
+    return __uint_as_float((v & 0x80000000u) ? (v & 0x7fffffffu) : ~v);
+}
+// Scene bounds words (zeroed at the start of a tick): max of the ordered x, y, z, then
+// max of their complements (the min).
+__device__ __forceinline__ void key_frame(const uint32_t* bw, f3& lo, float& scale) {
+    lo = mkf3(float_unorder(~bw[3]), float_unorder(~bw[4]), float_unorder(~bw[5]));
+    const f3 hi = mkf3(float_unorder(bw[0]), float_unorder(bw[1]), float_unorder(bw[2]));
+    const float extent = mxf(mxf(hi.x - lo.x, hi.y - lo.y), hi.z - lo.z);
+    scale = extent > 0.0f ? 2097151.0f / extent : 1.0f;
 }
 
 // lbvh.wgsl:108-130 plus the world box row the narrowphase reads:
 // box r0 = {center, half.x}, r1 = world rotation, r2 = {half.y, half.z, body, role}.
 __global__ void __launch_bounds__(kBlock) k_collider_bounds(StepBuffers b, StepParams p, uint32_t morton_mode) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= p.collider_count) return;
-    const float4* c = b.colliders + 4ull * i;
-    const float4 lc = __ldg(c), lr = __ldg(c + 1), he = __ldg(c + 2);
-    const uint4 meta = __ldg(reinterpret_cast<const uint4*>(c + 3));
-    const uint32_t body = meta.x;
-    const float4 bq = b.rot[body];
-    const f3 center = xyz(b.pos[body]) + quat_rotate(bq, xyz(lc));
-    const float4 r = quat_multiply(bq, lr);
-    const f3 ax = quat_rotate(r, mkf3(1, 0, 0));
-    const f3 ay = quat_rotate(r, mkf3(0, 1, 0));
-    const f3 az = quat_rotate(r, mkf3(0, 0, 1));
-    const f3 e = absf3(ax) * he.x + absf3(ay) * he.y + absf3(az) * he.z;
-    b.aabbs[2ull * i] = f4(center - e, 0.0f);
-    b.aabbs[2ull * i + 1] = f4(center + e, 0.0f);
-    float4* box = b.boxes + 3ull * i;
-    box[0] = f4(center, he.x);
-    box[1] = r;
-    box[2] = make_float4(he.y, he.z, __uint_as_float(body), __uint_as_float(meta.w));
-    uint64_t key = morton_mode == MK_MORTON_REFERENCE_30 ? (uint64_t)morton30(center) : morton63(center);
-    if (p.scene_bits) {   // batched scenes: the scene index above the spatial key
-        const uint64_t scene = b.collider_scene[i];
-        key = morton_mode == MK_MORTON_REFERENCE_30 ? (scene << 30) | key
-                                                     : (scene << (63 - p.scene_bits)) | (key >> p.scene_bits);
+    const bool valid = i < p.collider_count;
+    f3 center = mkf3(0, 0, 0);
+    if (valid) {
+        const float4* c = b.colliders + 4ull * i;
+        const float4 lc = __ldg(c), lr = __ldg(c + 1), he = __ldg(c + 2);
+        const uint4 meta = __ldg(reinterpret_cast<const uint4*>(c + 3));
+        const uint32_t body = meta.x;
+        const float4 bq = b.rot[body];
+        center = xyz(b.pos[body]) + quat_rotate(bq, xyz(lc));
+        const float4 r = quat_multiply(bq, lr);
+        const f3 ax = quat_rotate(r, mkf3(1, 0, 0));
+        const f3 ay = quat_rotate(r, mkf3(0, 1, 0));
+        const f3 az = quat_rotate(r, mkf3(0, 0, 1));
+        const f3 e = absf3(ax) * he.x + absf3(ay) * he.y + absf3(az) * he.z;
+        b.aabbs[2ull * i] = f4(center - e, 0.0f);
+        b.aabbs[2ull * i + 1] = f4(center + e, 0.0f);
+        float4* box = b.boxes + 3ull * i;
+        box[0] = f4(center, he.x);
+        box[1] = r;
+        box[2] = make_float4(he.y, he.z, __uint_as_float(body), __uint_as_float(meta.w));
+        b.values[i] = i;
+        if (morton_mode == MK_MORTON_REFERENCE_30) {
+            uint64_t key = morton30(center);
+            if (p.scene_bits) key |= (uint64_t)b.collider_scene[i] << 30;   // batched scenes: scene above the key
+            b.keys[i] = key;
+        }
     }
+    if (morton_mode == MK_MORTON_REFERENCE_30) return;
+    // the tick's bounds of the finite collider centres: warp reductions of the
+    // ordered integers, one atomic per warp and word (exact and order-free)
+    const bool use = valid && isfinite(center.x) && isfinite(center.y) && isfinite(center.z);
+    const float cc[3] = {center.x, center.y, center.z};
+    uint32_t w[6];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        const uint32_t o = use ? float_order(cc[a]) : 0u;
+        w[a] = o;                         // max of the ordered value
+        w[3 + a] = use ? ~o : 0u;         // max of its complement = min
+    }
+#pragma unroll
+    for (int k = 0; k < 6; ++k) {
+#pragma unroll
+        for (int d = 16; d > 0; d >>= 1) w[k] = max(w[k], __shfl_xor_sync(0xffffffffu, w[k], d));
+    }
+    if (lane_id() == 0) {
+#pragma unroll
+        for (int k = 0; k < 6; ++k)
+            if (w[k]) atomicMax(b.scene_bounds + k, w[k]);
+    }
+}
+
+// 63-bit keys over the tick's centre bounds (MK_MORTON_63).
+__global__ void __launch_bounds__(kBlock) k_morton_keys(StepBuffers b, StepParams p) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= p.collider_count) return;
+    f3 lo;
+    float scale;
+    key_frame(b.scene_bounds, lo, scale);
+    uint64_t key = morton63(xyz(b.boxes[3ull * i]), lo, scale);
+    if (p.scene_bits) key = ((uint64_t)b.collider_scene[i] << (63 - p.scene_bits)) | (key >> p.scene_bits);
     b.keys[i] = key;
-    b.values[i] = i;
 }
 
 // ------------------------------------------------------------- Karras tree
@@ -1807,6 +1861,7 @@ cudaError_t launch_broadphase(const StepBuffers& b, const StepParams& p, const S
     const uint32_t C = p.collider_count;
     if (C == 0) return cudaSuccess;
     k_collider_bounds<<<blocks_for(C, kBlock), kBlock, 0, s>>>(b, p, l.morton_mode);
+    if (l.morton_mode != MK_MORTON_REFERENCE_30) k_morton_keys<<<blocks_for(C, kBlock), kBlock, 0, s>>>(b, p);
     const uint32_t key_bits = l.morton_mode == MK_MORTON_REFERENCE_30 ? 30u + p.scene_bits : 63u;
     cudaError_t e = launch_sort(b.keys, b.values, b.skeys, b.svals, C, nullptr, key_bits, b.sort_scratch,
                                 b.sort_scratch_bytes, &b.diag->error_flags, s, l.sm_count, l.sort_items, l.sort_ctas,

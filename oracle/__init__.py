@@ -80,7 +80,7 @@ def lib():
         L.or_morton30.restype = u32
         L.or_morton30.argtypes = [C.c_float] * 3
         L.or_morton63.restype = u64
-        L.or_morton63.argtypes = [C.c_float] * 3
+        L.or_morton63.argtypes = [C.c_float] * 7
         _lib = L
     return _lib
 
@@ -316,5 +316,6 @@ def morton30(x, y, z) -> int:
     return int(lib().or_morton30(x, y, z))
 
 
-def morton63(x, y, z) -> int:
-    return int(lib().or_morton63(x, y, z))
+def morton63(x, y, z, lo=(0.0, 0.0, 0.0), scale=1.0) -> int:
+    """63-bit key of a centre in the frame (lo, scale) of the tick's centre bounds."""
+    return int(lib().or_morton63(x, y, z, lo[0], lo[1], lo[2], scale))

@@ -290,18 +290,54 @@ template <class T> struct World : WorldBase {
         };
         return expand10(q(c.x)) | (expand10(q(c.y)) << 1) | (expand10(q(c.z)) << 2);
     }
-    static uint64_t morton63(V3<T> c) {
-        auto q = [](T x) -> uint64_t {
-            T f = clampv(std::floor((x + T(512)) * T(2048)), T(0), T(2097151));
+    // 21 bits per axis over the tick's bounds of the collider centres, one
+    // scale from the largest extent (cubic cells).
+    static uint64_t morton63(V3<T> c, V3<T> lo, T scale) {
+        auto q = [&](T x, T l) -> uint64_t {
+            T f = clampv(std::floor((x - l) * scale), T(0), T(2097151));
             return (uint64_t)f;
         };
-        return expand21(q(c.x)) | (expand21(q(c.y)) << 1) | (expand21(q(c.z)) << 2);
+        return expand21(q(c.x, lo.x)) | (expand21(q(c.y, lo.y)) << 1) | (expand21(q(c.z, lo.z)) << 2);
+    }
+    // floats as unsigned integers in the same order (-0 below +0)
+    static uint32_t float_order(float f) {
+        uint32_t u;
+        std::memcpy(&u, &f, 4);
+        return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+    }
+    static float float_unorder(uint32_t v) {
+        const uint32_t u = (v & 0x80000000u) ? (v & 0x7fffffffu) : ~v;
+        float f;
+        std::memcpy(&f, &u, 4);
+        return f;
+    }
+    void key_frame(const std::vector<V3<T>>& centers, V3<T>& lo, T& scale) const {
+        uint32_t w[6] = {0, 0, 0, 0, 0, 0};
+        for (const V3<T>& c : centers) {
+            const float cc[3] = {float(c.x), float(c.y), float(c.z)};
+            if (!(std::isfinite(cc[0]) && std::isfinite(cc[1]) && std::isfinite(cc[2]))) continue;
+            for (int a = 0; a < 3; ++a) {
+                const uint32_t o = float_order(cc[a]);
+                w[a] = std::max(w[a], o);
+                w[3 + a] = std::max(w[3 + a], ~o);
+            }
+        }
+        lo = v3<T>(T(float_unorder(~w[3])), T(float_unorder(~w[4])), T(float_unorder(~w[5])));
+        const V3<T> hi = v3<T>(T(float_unorder(w[0])), T(float_unorder(w[1])), T(float_unorder(w[2])));
+        const T extent = mx(mx(hi.x - lo.x, hi.y - lo.y), hi.z - lo.z);
+        scale = extent > T(0) ? T(2097151.0f) / extent : T(1);
     }
     void compute_bounds() {
+        std::vector<V3<T>> centers(C);
+#pragma omp parallel for schedule(static)
+        for (int64_t ii = 0; ii < (int64_t)C; ++ii) centers[ii] = collider_center((uint32_t)ii);
+        V3<T> lo = v3<T>(0, 0, 0);
+        T scale = T(1);
+        if (morton_mode != MK_MORTON_REFERENCE_30) key_frame(centers, lo, scale);
 #pragma omp parallel for schedule(static)
         for (int64_t ii = 0; ii < (int64_t)C; ++ii) {
             uint32_t i = (uint32_t)ii;
-            V3<T> c = collider_center(i);
+            V3<T> c = centers[i];
             V4<T> r = collider_rotation(i);
             V3<T> ax = quat_rotate(r, v3<T>(1, 0, 0));
             V3<T> ay = quat_rotate(r, v3<T>(0, 1, 0));
@@ -310,7 +346,7 @@ template <class T> struct World : WorldBase {
             V3<T> e = absv(ax) * h.x + absv(ay) * h.y + absv(az) * h.z;
             aabb_min[i] = v4(c - e, T(0));
             aabb_max[i] = v4(c + e, T(0));
-            uint64_t key = morton_mode == MK_MORTON_REFERENCE_30 ? (uint64_t)morton30(c) : morton63(c);
+            uint64_t key = morton_mode == MK_MORTON_REFERENCE_30 ? (uint64_t)morton30(c) : morton63(c, lo, scale);
             if (scene_bits) {   // batched scenes: scene index above the spatial key
                 const uint64_t sc = col_scene[i];
                 key = morton_mode == MK_MORTON_REFERENCE_30 ? (sc << 30) | key
@@ -2495,6 +2531,8 @@ int or_cpu_contact_manifold(const float* ca, const float* qa, const float* ha, c
 }
 
 uint32_t or_morton30(float x, float y, float z) { return World<float>::morton30(v3<float>(x, y, z)); }
-uint64_t or_morton63(float x, float y, float z) { return World<float>::morton63(v3<float>(x, y, z)); }
+uint64_t or_morton63(float x, float y, float z, float lx, float ly, float lz, float scale) {
+    return World<float>::morton63(v3<float>(x, y, z), v3<float>(lx, ly, lz), scale);
+}
 
 }  // extern "C"

@@ -103,11 +103,16 @@ def test_morton30_matches_lbvh_wgsl():
 
 
 def test_morton63_orders_along_each_axis():
-    assert oracle.morton63(-512.0, -512.0, -512.0) == 0
-    assert oracle.morton63(600.0, 600.0, 600.0) == (1 << 63) - 1
-    a = oracle.morton63(0.0, 0.0, 0.0)
-    b = oracle.morton63(1.0 / 2048, 0.0, 0.0)
-    assert b == a + 1 or b > a
+    # frame of a scene whose centres span [-5, 5]^3: 2^21 - 1 cells over 10 m
+    lo, scale = (-5.0, -5.0, -5.0), float(np.float32(2097151.0) / np.float32(10.0))
+    assert oracle.morton63(-5.0, -5.0, -5.0, lo, scale) == 0
+    assert oracle.morton63(5.0, 5.0, 5.0, lo, scale) == (1 << 63) - 1
+    assert oracle.morton63(9.0, 9.0, 9.0, lo, scale) == (1 << 63) - 1     # clamped
+    cell = 10.0 / 2097151.0
+    a = oracle.morton63(0.0, 0.0, 0.0, lo, scale)
+    assert oracle.morton63(2 * cell, 0.0, 0.0, lo, scale) > a
+    assert oracle.morton63(0.0, 2 * cell, 0.0, lo, scale) > a
+    assert oracle.morton63(0.0, 0.0, 2 * cell, lo, scale) > a
 
 
 # ---------------------------------------------- compile.rs mass rules
