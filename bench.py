@@ -106,15 +106,33 @@ class ClockSampler:
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.device_index}", f"--query-gpu={self.FIELDS}",
-                 "--format=csv,noheader,nounits", "-lms", "200"],
+                 "--format=csv,noheader,nounits", "-lms", "100"],
                 stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
         except (OSError, ValueError):
             self.proc = None
-        time.sleep(0.3)
+        # nvidia-smi needs a moment to start: wait for its first row, then keep only
+        # the rows that arrive from here on
+        self.skip = 0
+        deadline = time.time() + 5.0
+        while self.proc is not None and time.time() < deadline and self._rows() == 0:
+            time.sleep(0.02)
+        self.skip = self._rows()
         return self
+
+    def _rows(self):
+        try:
+            with open(self.path) as f:
+                return sum(1 for line in f if line.endswith("\n"))
+        except OSError:
+            return 0
 
     def __exit__(self, *exc):
         if self.proc is not None:
+            # a short timed region may end between two samples: wait (bounded) for the
+            # sample that covers its end
+            deadline = time.time() + 1.0
+            while time.time() < deadline and self._rows() < self.skip + 2:
+                time.sleep(0.02)
             self.proc.terminate()
             try:
                 self.proc.wait(timeout=5)
@@ -125,7 +143,8 @@ class ClockSampler:
         if self.proc is None or not self.path or not os.path.exists(self.path):
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
         rows = []
-        for line in open(self.path):
+        lines = open(self.path).readlines()
+        for line in lines[max(self.skip - 1, 0):]:
             parts = [p.strip() for p in line.split(",")]
             if len(parts) < 9:
                 continue

@@ -231,6 +231,7 @@ cudaError_t enqueue_tick(MkHandle* h, int parity, bool capturing) {
         if (h->collisions) {
             z.add(b.deltas, sizeof(int32_t) * 6ull * std::max(h->B, 1u));
             z.add(b.scene_bounds, 8 * sizeof(uint32_t));
+            z.add(b.grid_barrier, 64 * sizeof(uint32_t));
             z.add(b.lookback, sizeof(uint64_t) * 4 * b.lookback_words);
             void* r = nullptr;
             uint64_t rb = 0;

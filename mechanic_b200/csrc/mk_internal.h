@@ -116,7 +116,7 @@ struct StepBuffers {
     uint64_t* lookback;          // look-back words for ordered compaction
     uint64_t lookback_words;     // per site
     uint32_t* tickets;           // 8 tile tickets
-    uint32_t* grid_barrier;      // count + generation of the cooperative solver's barrier
+    uint32_t* grid_barrier;      // arrival word of the cooperative solvers' grid barrier (zero at rest)
     GpuDiagnostics* diag;
     DevTick* tick;
     DevCounts* counts;

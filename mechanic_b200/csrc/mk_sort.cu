@@ -14,6 +14,7 @@ namespace mk {
 
 constexpr uint32_t kSortThreads = 256;
 constexpr uint32_t kRadixBins = 256;
+constexpr uint32_t kLookbackWindow = 16;   // predecessor tiles read per look-back round trip
 
 // 30-bit digit look-back words: bits 30-31 status, 0-29 count.
 constexpr uint32_t kDigitAggregate = 1u << 30;
@@ -124,7 +125,10 @@ k_radix_onesweep(const uint64_t* __restrict__ keys_in, const uint32_t* __restric
         uint32_t local_start = block_exclusive_scan(count, s_scan, &total);
         s_local_start[d] = local_start;
 
-        // ---- decoupled look-back for digit d (one thread per digit)
+        // ---- decoupled look-back for digit d (one thread per digit), reading a
+        // window of kLookbackWindow predecessors per round trip: with every tile
+        // starting at once, a one-word walk advances the inclusive prefixes by
+        // about two tiles per L2 round trip, a window by kLookbackWindow + 1
         uint32_t* lb = lookback + (size_t)tile * kRadixBins + d;
         uint32_t prefix = 0;
         if (tile == 0) {
@@ -133,16 +137,33 @@ k_radix_onesweep(const uint64_t* __restrict__ keys_in, const uint32_t* __restric
             st_release_u32(lb, kDigitAggregate | count);
             int64_t t = (int64_t)tile - 1;
             uint32_t spins = 0;
-            while (t >= 0) {
-                uint32_t s = ld_acquire_u32(lookback + (size_t)t * kRadixBins + d);
-                uint32_t status = s >> 30;
-                if (status == 0) {
+            for (;;) {
+                uint32_t s[kLookbackWindow];
+#pragma unroll
+                for (uint32_t j = 0; j < kLookbackWindow; ++j)   // below tile 0: an inclusive 0
+                    s[j] = t >= (int64_t)j ? ld_relaxed_u32(lookback + (size_t)(t - j) * kRadixBins + d)
+                                           : kDigitInclusive;
+                uint32_t advanced = 0;
+                bool stop = false, done = false;
+#pragma unroll
+                for (uint32_t j = 0; j < kLookbackWindow; ++j) {   // nearest first, up to the first gap
+                    const uint32_t status = s[j] >> 30;
+                    if (!stop) {
+                        if (status == 0) {
+                            stop = true;
+                        } else {
+                            prefix += s[j] & kDigitCountMask;
+                            ++advanced;
+                            if (status == 2) stop = done = true;
+                        }
+                    }
+                }
+                if (done) break;
+                if (advanced == 0) {
                     if (++spins > kSpinLimit) { if (error_flags) atomicOr(error_flags, MK_DEVICE_WAIT_TIMEOUT_FLAG); break; }
                     continue;
                 }
-                prefix += s & kDigitCountMask;
-                if (status == 2) break;
-                --t;
+                t -= advanced;
             }
             st_release_u32(lb, kDigitInclusive | (prefix + count));
         }

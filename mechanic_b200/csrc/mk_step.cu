@@ -196,8 +196,10 @@ __global__ void __launch_bounds__(kBlock) k_collider_bounds(StepBuffers b, StepP
         }
     }
     if (morton_mode == MK_MORTON_REFERENCE_30) return;
-    // the tick's bounds of the finite collider centres: warp reductions of the
-    // ordered integers, one atomic per warp and word (exact and order-free)
+    // the tick's bounds of the finite collider centres: warp then block reductions of
+    // the ordered integers, one atomic per block and word, skipped when the word
+    // already holds as much (exact and order-free; per-warp atomics on six words
+    // serialised in L2 and cost 40 us at 400k colliders)
     const bool use = valid && isfinite(center.x) && isfinite(center.y) && isfinite(center.z);
     const float cc[3] = {center.x, center.y, center.z};
     uint32_t w[6];
@@ -212,10 +214,19 @@ __global__ void __launch_bounds__(kBlock) k_collider_bounds(StepBuffers b, StepP
 #pragma unroll
         for (int d = 16; d > 0; d >>= 1) w[k] = max(w[k], __shfl_xor_sync(0xffffffffu, w[k], d));
     }
+    __shared__ uint32_t s_w[kBlock / 32][6];
+    const uint32_t warp = threadIdx.x >> 5;
     if (lane_id() == 0) {
 #pragma unroll
-        for (int k = 0; k < 6; ++k)
-            if (w[k]) atomicMax(b.scene_bounds + k, w[k]);
+        for (int k = 0; k < 6; ++k) s_w[warp][k] = w[k];
+    }
+    __syncthreads();
+    if (threadIdx.x < 6) {
+        uint32_t m = 0;
+#pragma unroll
+        for (uint32_t q = 0; q < kBlock / 32; ++q) m = max(m, s_w[q][threadIdx.x]);
+        uint32_t* word = b.scene_bounds + threadIdx.x;
+        if (m > *reinterpret_cast<volatile uint32_t*>(word)) atomicMax(word, m);
     }
 }
 
@@ -1092,11 +1103,80 @@ __device__ __forceinline__ void fused_body(const StepBuffers& b, const FusedPass
     ang = xyz(na);
 }
 
+// One relaxed-Jacobi projection of a contact (collision.wgsl:774-906) at the
+// relative velocity `rel` (vB - vA at the arms).  `acc` holds the row's stored
+// impulse on entry and the value the row keeps on return; returns whether an
+// impulse is applied (then da / db hold its fixed-point body deltas).
+template <bool kWarm>
+__device__ __forceinline__ bool contact_project(const StepParams& p, const float4* wa, const float4* wb, f3 arm_a,
+                                                f3 arm_b, f3 nrm, float depth, bool cyl, float den, f3 rel,
+                                                float& acc_io, int32_t* da, int32_t* db) {
+    const float scale = (float)kFixedScale;
+    const float vn = dot(rel, nrm);
+    if (depth <= 1.0e-5f && vn >= -1.0e-5f && acc_io <= 1.0e-6f) {
+        acc_io = 0.0f;
+        return false;
+    }
+    const float recovery = cyl ? 1.0f : 0.2f;
+    const float bias = mnf(mxf(depth - 0.001f, 0.0f) * recovery / p.dt, 1.0f);
+    float acc, delta;
+    if (kWarm) {
+        const float warmed = acc_io * (cyl ? 1.0f : 0.5f);
+        acc = mxf(warmed + 0.125f * (-vn + bias) / den, 0.0f);
+        delta = acc;
+    } else {
+        const float prev = mxf(acc_io, 0.0f);
+        acc = mxf(prev + 0.125f * (-vn + bias) / den, 0.0f);
+        delta = acc - prev;
+    }
+    acc_io = acc;
+    f3 imp = nrm * delta;
+    const f3 tv = rel - nrm * vn;
+    const float ts = length(tv);
+    if (ts > 1.0e-6f) {
+        const f3 tg = tv / ts;
+        const float tden = impulse_denominator(wa, wb, arm_a, arm_b, tg);
+        const float fr = mnf(ts / tden, (kWarm ? acc : fabsf(delta)) * 0.05f);
+        imp = imp - tg * fr;
+    }
+    const f3 la = -imp * wa[0].w;
+    const f3 ga = inverse_inertia(wa, cross(arm_a, -imp));
+    da[0] = fixed_i32(la.x * scale); da[1] = fixed_i32(la.y * scale); da[2] = fixed_i32(la.z * scale);
+    da[3] = fixed_i32(ga.x * scale); da[4] = fixed_i32(ga.y * scale); da[5] = fixed_i32(ga.z * scale);
+    if (wb) {
+        const f3 lb = imp * wb[0].w;
+        const f3 gb = inverse_inertia(wb, cross(arm_b, imp));
+        db[0] = fixed_i32(lb.x * scale); db[1] = fixed_i32(lb.y * scale); db[2] = fixed_i32(lb.z * scale);
+        db[3] = fixed_i32(gb.x * scale); db[4] = fixed_i32(gb.y * scale); db[5] = fixed_i32(gb.z * scale);
+    }
+    return true;
+}
+
+// Adds a contact's body deltas: body A's through warp sums over runs of equal
+// bodies (contacts arrive grouped by collider A; integer sums are order-free),
+// body B's directly.
+__device__ __forceinline__ void add_contact_deltas(int32_t* deltas, bool live, uint32_t a, uint32_t bb, int32_t* da,
+                                                   const int32_t* db) {
+    const uint32_t key_a = live ? a : kInvalid;
+    const bool tail = run_tail_sum(key_a, da, 6);
+    if (tail && key_a != kInvalid) {
+        int32_t* d = deltas + 6ull * key_a;
+#pragma unroll
+        for (int c = 0; c < 6; ++c)
+            if (da[c]) atomicAdd(d + c, da[c]);
+    }
+    if (live && bb != kInvalid) {
+        int32_t* d = deltas + 6ull * bb;
+#pragma unroll
+        for (int c = 0; c < 6; ++c)
+            if (db[c]) atomicAdd(d + c, db[c]);
+    }
+}
+
 template <bool kWarm, bool kFused = false>
 __device__ __forceinline__ void solve_span(const StepBuffers& b, const StepParams& p, GpuContact* cur, uint32_t A,
                                            uint32_t first, uint32_t stride, const float4* vl, const float4* va,
                                            const FusedPass* fp = nullptr, int32_t* dacc = nullptr) {
-    const float scale = (float)kFixedScale;
     int32_t* deltas = kFused ? dacc : b.deltas;
     for (uint32_t base = first; base < A; base += stride) {
         const uint32_t t = base + threadIdx.x;
@@ -1123,63 +1203,12 @@ __device__ __forceinline__ void solve_span(const StepBuffers& b, const StepParam
             const float den = impulse_denominator(wa, wb, arm_a, arm_b, nrm);
             if (!(den <= 0.0f)) {
                 const f3 rel = vb - (kFused ? la + cross(ga, arm_a) : contact_velocity_it(vl, va, a, arm_a));
-                const float vn = dot(rel, nrm);
-                if (np.w <= 1.0e-5f && vn >= -1.0e-5f && aa.w <= 1.0e-6f) {
-                    row[2] = f4(arm_a, 0.0f);
-                } else {
-                    const bool cyl = ab.w < 0.0f;
-                    const float recovery = cyl ? 1.0f : 0.2f;
-                    const float bias = mnf(mxf(np.w - 0.001f, 0.0f) * recovery / p.dt, 1.0f);
-                    float acc, delta;
-                    if (kWarm) {
-                        const float warmed = aa.w * (cyl ? 1.0f : 0.5f);
-                        acc = mxf(warmed + 0.125f * (-vn + bias) / den, 0.0f);
-                        delta = acc;
-                    } else {
-                        const float prev = mxf(aa.w, 0.0f);
-                        acc = mxf(prev + 0.125f * (-vn + bias) / den, 0.0f);
-                        delta = acc - prev;
-                    }
-                    row[2] = f4(arm_a, acc);
-                    f3 imp = nrm * delta;
-                    const f3 tv = rel - nrm * vn;
-                    const float ts = length(tv);
-                    if (ts > 1.0e-6f) {
-                        const f3 tg = tv / ts;
-                        const float tden = impulse_denominator(wa, wb, arm_a, arm_b, tg);
-                        const float fr = mnf(ts / tden, (kWarm ? acc : fabsf(delta)) * 0.05f);
-                        imp = imp - tg * fr;
-                    }
-                    const f3 la = -imp * wa[0].w;
-                    const f3 ga = inverse_inertia(wa, cross(arm_a, -imp));
-                    da[0] = fixed_i32(la.x * scale); da[1] = fixed_i32(la.y * scale); da[2] = fixed_i32(la.z * scale);
-                    da[3] = fixed_i32(ga.x * scale); da[4] = fixed_i32(ga.y * scale); da[5] = fixed_i32(ga.z * scale);
-                    live = true;
-                    if (wb) {
-                        const f3 lb = imp * wb[0].w;
-                        const f3 gb = inverse_inertia(wb, cross(arm_b, imp));
-                        db[0] = fixed_i32(lb.x * scale); db[1] = fixed_i32(lb.y * scale); db[2] = fixed_i32(lb.z * scale);
-                        db[3] = fixed_i32(gb.x * scale); db[4] = fixed_i32(gb.y * scale); db[5] = fixed_i32(gb.z * scale);
-                    }
-                }
+                float acc = aa.w;
+                live = contact_project<kWarm>(p, wa, wb, arm_a, arm_b, nrm, np.w, ab.w < 0.0f, den, rel, acc, da, db);
+                row[2] = f4(arm_a, acc);
             }
         }
-        // body A: contacts arrive grouped by collider A, so sum runs of equal
-        // bodies across the warp first (integer sums are order-free).
-        const uint32_t key_a = live ? a : kInvalid;
-        const bool tail = run_tail_sum(key_a, da, 6);
-        if (tail && key_a != kInvalid) {
-            int32_t* d = deltas + 6ull * key_a;
-#pragma unroll
-            for (int c = 0; c < 6; ++c)
-                if (da[c]) atomicAdd(d + c, da[c]);
-        }
-        if (live && bb != kInvalid) {
-            int32_t* d = deltas + 6ull * bb;
-#pragma unroll
-            for (int c = 0; c < 6; ++c)
-                if (db[c]) atomicAdd(d + c, db[c]);
-        }
+        add_contact_deltas(deltas, live, a, bb, da, db);
     }
 }
 
@@ -1204,33 +1233,97 @@ __device__ __forceinline__ void apply_span(const StepBuffers& b, const StepParam
     }
 }
 
-// Grid-wide barrier for a cooperative launch.  The wait is bounded: a block
-// that gives up raises MK_DEVICE_WAIT_TIMEOUT_FLAG and carries on.
+// Grid-wide barrier for a cooperative launch on one 32-bit word that starts at
+// zero: block 0 adds 2^31 - (participants - 1), every other block adds 1, so
+// the word's top bit flips exactly when the last block arrives and its low
+// bits return to zero for the next barrier (one atomic per block, no reset
+// step).  The wait is bounded: a block that gives up raises
+// MK_DEVICE_WAIT_TIMEOUT_FLAG and carries on.
 __device__ __forceinline__ void grid_barrier(uint32_t* state, uint32_t* error_flags, uint32_t participants) {
     __syncthreads();
     if (threadIdx.x == 0) {
-        uint32_t* count = state;
-        uint32_t* generation = state + 1;
-        const uint32_t gen = ld_acquire_u32(generation);
+        const uint32_t add = blockIdx.x == 0 ? 0x80000000u - (participants - 1u) : 1u;
         __threadfence();
-        const uint32_t arrived = atomicAdd(count, 1u);
-        if (arrived == participants - 1) {
-            atomicExch(count, 0u);
-            __threadfence();
-            st_release_u32(generation, gen + 1u);
-        } else {
-            uint32_t spins = 0;
-            while (ld_acquire_u32(generation) == gen) {
-                __nanosleep(20);
-                if (++spins > kSpinLimit) {
-                    atomicOr(error_flags, MK_DEVICE_WAIT_TIMEOUT_FLAG);
-                    break;
-                }
+        const uint32_t old = atomicAdd(state, add);
+        uint32_t spins = 0;
+        while (((ld_acquire_u32(state) ^ old) & 0x80000000u) == 0u) {
+            if (++spins > kSpinLimit) {
+                atomicOr(error_flags, MK_DEVICE_WAIT_TIMEOUT_FLAG);
+                break;
             }
         }
         __threadfence();
     }
     __syncthreads();
+}
+
+// Fused passes with one contact per thread held in registers for the whole
+// solve (active contacts <= threads of the grid): the contact row, its
+// normal-row denominator and its running impulse are loaded once, so a pass
+// reads only the two bodies' velocity state.  Each pass also clears its
+// bodies' rows of the delta buffer the next pass accumulates into (the active
+// contacts touch the same bodies in every pass; rows of other bodies are never
+// read).  The row keeps the last pass's impulse, as after per-pass stores.
+__device__ __forceinline__ void solve_fused_resident(const StepBuffers& b, const StepParams& p, GpuContact* cur,
+                                                  uint32_t A, uint32_t iterations, uint32_t t, int32_t* const* D,
+                                                  uint32_t gen, uint32_t* barrier, uint32_t parts) {
+    const bool has = t < A;
+    uint32_t a = kInvalid, bb = kInvalid;
+    f3 arm_a = mkf3(0, 0, 0), arm_b = mkf3(0, 0, 0), nrm = mkf3(0, 0, 0);
+    float depth = 0.0f, acc = 0.0f, den = 0.0f;
+    bool cyl = false;
+    float4* row = nullptr;
+    if (has) {
+        const uint32_t k = __ldcg(b.active + t);
+        row = reinterpret_cast<float4*>(cur + k);
+        const float4 r0 = __ldcg(row), np = __ldcg(row + 1), aa = __ldcg(row + 2), ab = __ldcg(row + 3);
+        a = __float_as_uint(r0.x);
+        bb = __float_as_uint(r0.y);
+        arm_a = xyz(aa);
+        arm_b = xyz(ab);
+        nrm = xyz(np);
+        depth = np.w;
+        acc = aa.w;
+        cyl = ab.w < 0.0f;
+        den = impulse_denominator(b.world_mass + 3ull * a, bb != kInvalid ? b.world_mass + 3ull * bb : nullptr,
+                                  arm_a, arm_b, nrm);
+    }
+    const size_t B = p.body_count;
+    for (uint32_t it = 0; it < iterations; ++it) {
+        FusedPass fp;
+        fp.it = it;
+        fp.pl = it <= 1 ? b.lin : b.vel_iter + (2 * (it - 2)) * B;
+        fp.pa = it <= 1 ? b.ang : b.vel_iter + (2 * (it - 2) + 1) * B;
+        fp.dprev = it == 0 ? nullptr : D[(it - 1) % 3];
+        fp.cl = it == 0 ? nullptr : b.vel_iter + (2 * (it - 1)) * B;
+        fp.ca = it == 0 ? nullptr : b.vel_iter + (2 * (it - 1) + 1) * B;
+        fp.gen = gen;
+        bool live = false;
+        int32_t da[6] = {0, 0, 0, 0, 0, 0}, db[6] = {0, 0, 0, 0, 0, 0};
+        if (has) {
+            f3 la, ga, lb = mkf3(0, 0, 0), gb = mkf3(0, 0, 0);
+            fused_body(b, fp, a, la, ga);
+            if (bb != kInvalid) fused_body(b, fp, bb, lb, gb);
+            int2* za = reinterpret_cast<int2*>(D[(it + 1) % 3] + 6ull * a);   // 24-byte rows: 8-byte aligned
+            za[0] = make_int2(0, 0); za[1] = make_int2(0, 0); za[2] = make_int2(0, 0);
+            if (bb != kInvalid) {
+                int2* zb = reinterpret_cast<int2*>(D[(it + 1) % 3] + 6ull * bb);
+                zb[0] = make_int2(0, 0); zb[1] = make_int2(0, 0); zb[2] = make_int2(0, 0);
+            }
+            if (!(den <= 0.0f)) {
+                const float4* wa = b.world_mass + 3ull * a;
+                const float4* wb = bb != kInvalid ? b.world_mass + 3ull * bb : nullptr;
+                const f3 vb = bb != kInvalid ? lb + cross(gb, arm_b) : mkf3(0, 0, 0);
+                const f3 rel = vb - (la + cross(ga, arm_a));
+                live = it == 0 ? contact_project<true>(p, wa, wb, arm_a, arm_b, nrm, depth, cyl, den, rel, acc, da, db)
+                               : contact_project<false>(p, wa, wb, arm_a, arm_b, nrm, depth, cyl, den, rel, acc, da,
+                                                        db);
+            }
+        }
+        add_contact_deltas(D[it % 3], live, a, bb, da, db);
+        grid_barrier(barrier, &b.diag->error_flags, parts);
+    }
+    if (has && !(den <= 0.0f)) row[2] = f4(arm_a, acc);
 }
 
 // All solver iterations in one cooperative launch: warm start, then
@@ -1264,6 +1357,9 @@ __global__ void __launch_bounds__(kSolveThreads) k_solve_all(StepBuffers b, Step
         int32_t* D[3] = {b.deltas, b.deltas_extra, b.deltas_extra + dstride};
         const uint32_t gen = b.tick->generation;
         const uint32_t gtid = first + threadIdx.x;
+        if (A <= stride) {
+            solve_fused_resident(b, p, cur, A, iterations, gtid, D, gen, barrier, parts);
+        } else {
         for (uint32_t it = 0; it < iterations; ++it) {
             FusedPass fp;
             fp.it = it;
@@ -1281,6 +1377,7 @@ __global__ void __launch_bounds__(kSolveThreads) k_solve_all(StepBuffers b, Step
                 for (uint64_t i = (6ull * B) & ~3ull; i < 6ull * B; ++i) D[(it + 1) % 3][i] = 0;
             }
             grid_barrier(barrier, &b.diag->error_flags, parts);
+        }
         }
         // the apply of the last pass, for every body (bodies no contact touched
         // get the reference's apply of zero deltas)
