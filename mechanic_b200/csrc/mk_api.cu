@@ -235,7 +235,7 @@ cudaError_t enqueue_tick(MkHandle* h, int parity, bool capturing) {
             z.add(b.lookback, sizeof(uint64_t) * 4 * b.lookback_words);
             void* r = nullptr;
             uint64_t rb = 0;
-            const uint32_t key_bits = h->launch.morton_mode == MK_MORTON_REFERENCE_30 ? 30u + h->params.scene_bits : 63u;
+            const uint32_t key_bits = mk::sort_key_bits(h->launch.morton_mode, h->params.scene_bits);
             mk::sort_clear_region(b.sort_scratch, h->C, key_bits, true, &r, &rb);
             z.add(r, rb);
             mk::sort_clear_region(b.pair_sort_scratch, h->pair_capacity, 2 * h->params.pair_shift, false, &r, &rb);
@@ -553,6 +553,11 @@ int create_impl(const MkCreation* cr, const MkConfig* config, const MkCapacities
         set_error(err, MK_ERR_INVALID_ARGUMENT, "creation arrays missing for the given counts");
         return MK_ERR_INVALID_ARGUMENT;
     }
+    if (config && config->morton_mode != MK_MORTON_63 && config->morton_mode != MK_MORTON_48 &&
+        config->morton_mode != MK_MORTON_REFERENCE_30) {
+        set_error(err, MK_ERR_INVALID_ARGUMENT, "unknown morton_mode %u", config->morton_mode);
+        return MK_ERR_INVALID_ARGUMENT;
+    }
     if (pair_capacity == 0 || pair_capacity > (1u << 30)) {
         set_error(err, MK_ERR_PAIR_CAPACITY, "pair capacity %u outside 1..2^30", pair_capacity);
         return MK_ERR_PAIR_CAPACITY;
@@ -714,7 +719,7 @@ void mk_config_default(MkConfig* c) {
     c->collisions_enabled = 1;
     c->mechanism_self_collisions = 1;
     c->solver_iterations = 8;
-    c->morton_mode = MK_MORTON_63;
+    c->morton_mode = MK_MORTON_48;
     c->closure_mode = MK_CLOSURE_REFERENCE;
     c->use_graph = 1;
 }

@@ -44,6 +44,24 @@ struct DevCounts {
 constexpr uint32_t kCountResetBytes = 8 * sizeof(uint32_t);
 
 // Solver-side constants of a handle.
+// Bits of the spatial Morton key per mode (MK_MORTON_*), and of the sort key
+// once a batch's scene index sits above it.
+__host__ __device__ inline uint32_t spatial_key_bits(uint32_t mode) {
+    return mode == MK_MORTON_REFERENCE_30 ? 30u : (mode == MK_MORTON_48 ? 48u : 63u);
+}
+__host__ __device__ inline uint32_t sort_key_bits(uint32_t mode, uint32_t scene_bits) {
+    const uint32_t w = spatial_key_bits(mode) + scene_bits;
+    return w < 63u ? w : 63u;
+}
+// Batched scenes: the scene index above the spatial key; when both do not fit
+// in 63 bits the spatial key loses its lowest bits.
+__host__ __device__ inline uint64_t compose_key(uint32_t mode, uint32_t scene_bits, uint64_t scene, uint64_t key) {
+    if (!scene_bits) return key;
+    const uint32_t w = spatial_key_bits(mode);
+    if (w + scene_bits <= 63u) return (scene << w) | key;
+    return (scene << (63u - scene_bits)) | (key >> (w + scene_bits - 63u));
+}
+
 struct StepParams {
     float dt, gravity, lin_damp, ang_damp;
     uint32_t body_count, collider_count, pair_capacity, suppression_count;

@@ -73,14 +73,13 @@ k_radix_onesweep(const uint64_t* __restrict__ keys_in, const uint32_t* __restric
     const uint32_t n = n_ptr ? min(*n_ptr, n_fixed) : n_fixed;   // a device count never exceeds the capacity
     const uint32_t tiles = (n + kTile - 1) / kTile;
     const uint32_t lane = lane_id(), w = warp_id();
+    if (threadIdx.x == 0) s_tile = atomicAdd(ticket, 1u);   // in flight during the offsets scan
     {   // this pass's digit offsets: exclusive scan of its histogram (kSortThreads == kRadixBins)
         uint32_t total_all;
         s_digit_offsets[threadIdx.x] = block_exclusive_scan(digit_hist[threadIdx.x], s_scan, &total_all);
-        __syncthreads();
     }
 
     for (;;) {
-        if (threadIdx.x == 0) s_tile = atomicAdd(ticket, 1u);
         for (uint32_t i = threadIdx.x; i < (kSortThreads / 32) * kRadixBins; i += kSortThreads)
             (&s_warp[0][0])[i] = 0;
         __syncthreads();
@@ -88,17 +87,23 @@ k_radix_onesweep(const uint64_t* __restrict__ keys_in, const uint32_t* __restric
         if (tile >= tiles) break;
         const uint32_t tile_base = tile * kTile;
 
-        // ---- load (warp-striped) and rank within each warp, item by item
+        // ---- load every item first (one memory round trip), then rank within
+        // each warp, item by item (warp-striped)
         uint64_t k[kSortItems];
         uint32_t v[kSortItems];
         uint32_t rank[kSortItems];
         uint32_t dig[kSortItems];
 #pragma unroll
         for (uint32_t i = 0; i < kSortItems; ++i) {
-            uint32_t idx = tile_base + w * 32 * kSortItems + i * 32 + lane;
-            bool valid = idx < n;
-            k[i] = valid ? keys_in[idx] : 0ull;
-            v[i] = (valid && vals_in) ? vals_in[idx] : 0u;
+            const uint32_t idx = tile_base + w * 32 * kSortItems + i * 32 + lane;
+            const bool valid = idx < n;
+            k[i] = valid ? __ldcg(keys_in + idx) : 0ull;
+            v[i] = (valid && vals_in) ? __ldcg(vals_in + idx) : 0u;
+        }
+#pragma unroll
+        for (uint32_t i = 0; i < kSortItems; ++i) {
+            const uint32_t idx = tile_base + w * 32 * kSortItems + i * 32 + lane;
+            const bool valid = idx < n;
             uint32_t d = valid ? (uint32_t)((k[i] >> shift) & 0xffu) : kRadixBins;
             dig[i] = d;
             uint32_t peers = __match_any_sync(0xffffffffu, d);
@@ -131,10 +136,12 @@ k_radix_onesweep(const uint64_t* __restrict__ keys_in, const uint32_t* __restric
         // about two tiles per L2 round trip, a window by kLookbackWindow + 1
         uint32_t* lb = lookback + (size_t)tile * kRadixBins + d;
         uint32_t prefix = 0;
+        // (relaxed stores: a word carries its own status and count, and a
+        // release store's fence costs about an L2 round trip per tile)
         if (tile == 0) {
-            st_release_u32(lb, kDigitInclusive | count);
+            st_relaxed_u32(lb, kDigitInclusive | count);
         } else {
-            st_release_u32(lb, kDigitAggregate | count);
+            st_relaxed_u32(lb, kDigitAggregate | count);
             int64_t t = (int64_t)tile - 1;
             uint32_t spins = 0;
             for (;;) {
@@ -165,7 +172,7 @@ k_radix_onesweep(const uint64_t* __restrict__ keys_in, const uint32_t* __restric
                 }
                 t -= advanced;
             }
-            st_release_u32(lb, kDigitInclusive | (prefix + count));
+            st_relaxed_u32(lb, kDigitInclusive | (prefix + count));
         }
         s_global_base[d] = s_digit_offsets[d] + prefix - local_start;
         __syncthreads();
@@ -188,6 +195,7 @@ k_radix_onesweep(const uint64_t* __restrict__ keys_in, const uint32_t* __restric
             if (vals_out) vals_out[dst] = s_vals[j];
         }
         __syncthreads();
+        if (threadIdx.x == 0) s_tile = atomicAdd(ticket, 1u);   // every thread has read s_tile
     }
 }
 

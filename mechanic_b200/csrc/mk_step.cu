@@ -137,15 +137,16 @@ __device__ __forceinline__ uint32_t morton30(f3 c) {
     uint32_t qz = (uint32_t)clampf(floorf(c.z + 512.0f), 0.0f, 1023.0f);
     return expand10(qx) | (expand10(qy) << 1) | (expand10(qz) << 2);
 }
-// 21 bits per axis over the tick's bounds of the collider centres (cubic
-// cells: one scale from the largest extent), so the keys stay distinct however
-// far the scene spreads.
-__device__ __forceinline__ uint64_t morton63(f3 c, f3 lo, float scale) {
-    uint64_t qx = (uint64_t)clampf(floorf((c.x - lo.x) * scale), 0.0f, 2097151.0f);
-    uint64_t qy = (uint64_t)clampf(floorf((c.y - lo.y) * scale), 0.0f, 2097151.0f);
-    uint64_t qz = (uint64_t)clampf(floorf((c.z - lo.z) * scale), 0.0f, 2097151.0f);
+// `qmax + 1` cells per axis (2^21 for 63-bit keys, 2^16 for 48-bit keys) over
+// the tick's bounds of the collider centres (cubic cells: one scale from the
+// largest extent), so the keys stay spread however far the scene moves.
+__device__ __forceinline__ uint64_t morton_frame(f3 c, f3 lo, float scale, float qmax) {
+    uint64_t qx = (uint64_t)clampf(floorf((c.x - lo.x) * scale), 0.0f, qmax);
+    uint64_t qy = (uint64_t)clampf(floorf((c.y - lo.y) * scale), 0.0f, qmax);
+    uint64_t qz = (uint64_t)clampf(floorf((c.z - lo.z) * scale), 0.0f, qmax);
     return expand21(qx) | (expand21(qy) << 1) | (expand21(qz) << 2);
 }
+__device__ __forceinline__ float frame_qmax(uint32_t mode) { return mode == MK_MORTON_48 ? 65535.0f : 2097151.0f; }
 // Floats as unsigned integers in the same order (-0 below +0), for exact
 // order-free min / max with integer atomics.
 __device__ __forceinline__ uint32_t float_order(float f) {
@@ -157,11 +158,11 @@ __device__ __forceinline__ float float_unorder(uint32_t v) {
 }
 // Scene bounds words (zeroed at the start of a tick): max of the ordered x, y, z, then
 // max of their complements (the min).
-__device__ __forceinline__ void key_frame(const uint32_t* bw, f3& lo, float& scale) {
+__device__ __forceinline__ void key_frame(const uint32_t* bw, float qmax, f3& lo, float& scale) {
     lo = mkf3(float_unorder(~bw[3]), float_unorder(~bw[4]), float_unorder(~bw[5]));
     const f3 hi = mkf3(float_unorder(bw[0]), float_unorder(bw[1]), float_unorder(bw[2]));
     const float extent = mxf(mxf(hi.x - lo.x, hi.y - lo.y), hi.z - lo.z);
-    scale = extent > 0.0f ? 2097151.0f / extent : 1.0f;
+    scale = extent > 0.0f ? qmax / extent : 1.0f;
 }
 
 // lbvh.wgsl:108-130 plus the world box row the narrowphase reads:
@@ -189,11 +190,9 @@ __global__ void __launch_bounds__(kBlock) k_collider_bounds(StepBuffers b, StepP
         box[1] = r;
         box[2] = make_float4(he.y, he.z, __uint_as_float(body), __uint_as_float(meta.w));
         b.values[i] = i;
-        if (morton_mode == MK_MORTON_REFERENCE_30) {
-            uint64_t key = morton30(center);
-            if (p.scene_bits) key |= (uint64_t)b.collider_scene[i] << 30;   // batched scenes: scene above the key
-            b.keys[i] = key;
-        }
+        if (morton_mode == MK_MORTON_REFERENCE_30)
+            b.keys[i] = compose_key(morton_mode, p.scene_bits, p.scene_bits ? b.collider_scene[i] : 0u,
+                                    morton30(center));
     }
     if (morton_mode == MK_MORTON_REFERENCE_30) return;
     // the tick's bounds of the finite collider centres: warp then block reductions of
@@ -230,16 +229,16 @@ __global__ void __launch_bounds__(kBlock) k_collider_bounds(StepBuffers b, StepP
     }
 }
 
-// 63-bit keys over the tick's centre bounds (MK_MORTON_63).
-__global__ void __launch_bounds__(kBlock) k_morton_keys(StepBuffers b, StepParams p) {
+// Keys over the tick's centre bounds (MK_MORTON_48, MK_MORTON_63).
+__global__ void __launch_bounds__(kBlock) k_morton_keys(StepBuffers b, StepParams p, uint32_t morton_mode) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= p.collider_count) return;
+    const float qmax = frame_qmax(morton_mode);
     f3 lo;
     float scale;
-    key_frame(b.scene_bounds, lo, scale);
-    uint64_t key = morton63(xyz(b.boxes[3ull * i]), lo, scale);
-    if (p.scene_bits) key = ((uint64_t)b.collider_scene[i] << (63 - p.scene_bits)) | (key >> p.scene_bits);
-    b.keys[i] = key;
+    key_frame(b.scene_bounds, qmax, lo, scale);
+    const uint64_t key = morton_frame(xyz(b.boxes[3ull * i]), lo, scale, qmax);
+    b.keys[i] = compose_key(morton_mode, p.scene_bits, p.scene_bits ? b.collider_scene[i] : 0u, key);
 }
 
 // ------------------------------------------------------------- Karras tree
@@ -1958,8 +1957,9 @@ cudaError_t launch_broadphase(const StepBuffers& b, const StepParams& p, const S
     const uint32_t C = p.collider_count;
     if (C == 0) return cudaSuccess;
     k_collider_bounds<<<blocks_for(C, kBlock), kBlock, 0, s>>>(b, p, l.morton_mode);
-    if (l.morton_mode != MK_MORTON_REFERENCE_30) k_morton_keys<<<blocks_for(C, kBlock), kBlock, 0, s>>>(b, p);
-    const uint32_t key_bits = l.morton_mode == MK_MORTON_REFERENCE_30 ? 30u + p.scene_bits : 63u;
+    if (l.morton_mode != MK_MORTON_REFERENCE_30)
+        k_morton_keys<<<blocks_for(C, kBlock), kBlock, 0, s>>>(b, p, l.morton_mode);
+    const uint32_t key_bits = sort_key_bits(l.morton_mode, p.scene_bits);
     cudaError_t e = launch_sort(b.keys, b.values, b.skeys, b.svals, C, nullptr, key_bits, b.sort_scratch,
                                 b.sort_scratch_bytes, &b.diag->error_flags, s, l.sm_count, l.sort_items, l.sort_ctas,
                                 true);   // bins and tickets cleared by the tick's reset

@@ -81,6 +81,8 @@ def lib():
         L.or_morton30.argtypes = [C.c_float] * 3
         L.or_morton63.restype = u64
         L.or_morton63.argtypes = [C.c_float] * 7
+        L.or_morton48.restype = u64
+        L.or_morton48.argtypes = [C.c_float] * 7
         _lib = L
     return _lib
 
@@ -319,3 +321,8 @@ def morton30(x, y, z) -> int:
 def morton63(x, y, z, lo=(0.0, 0.0, 0.0), scale=1.0) -> int:
     """63-bit key of a centre in the frame (lo, scale) of the tick's centre bounds."""
     return int(lib().or_morton63(x, y, z, lo[0], lo[1], lo[2], scale))
+
+
+def morton48(x, y, z, lo=(0.0, 0.0, 0.0), scale=1.0) -> int:
+    """48-bit key (16 bits per axis) of a centre in the frame (lo, scale)."""
+    return int(lib().or_morton48(x, y, z, lo[0], lo[1], lo[2], scale))

@@ -290,14 +290,27 @@ template <class T> struct World : WorldBase {
         };
         return expand10(q(c.x)) | (expand10(q(c.y)) << 1) | (expand10(q(c.z)) << 2);
     }
-    // 21 bits per axis over the tick's bounds of the collider centres, one
-    // scale from the largest extent (cubic cells).
-    static uint64_t morton63(V3<T> c, V3<T> lo, T scale) {
+    // qmax + 1 cells per axis (2^21: 63-bit keys, 2^16: 48-bit keys) over the
+    // tick's bounds of the collider centres, one scale from the largest extent
+    // (cubic cells).
+    static uint64_t morton_frame(V3<T> c, V3<T> lo, T scale, T qmax) {
         auto q = [&](T x, T l) -> uint64_t {
-            T f = clampv(std::floor((x - l) * scale), T(0), T(2097151));
+            T f = clampv(std::floor((x - l) * scale), T(0), qmax);
             return (uint64_t)f;
         };
         return expand21(q(c.x, lo.x)) | (expand21(q(c.y, lo.y)) << 1) | (expand21(q(c.z, lo.z)) << 2);
+    }
+    static T frame_qmax(uint32_t mode) { return mode == MK_MORTON_48 ? T(65535.0f) : T(2097151.0f); }
+    static uint32_t spatial_key_bits(uint32_t mode) {
+        return mode == MK_MORTON_REFERENCE_30 ? 30u : (mode == MK_MORTON_48 ? 48u : 63u);
+    }
+    // batched scenes: the scene index above the spatial key, whose lowest bits
+    // give way when both do not fit in 63 bits
+    static uint64_t compose_key(uint32_t mode, uint32_t sb, uint64_t scene, uint64_t key) {
+        if (!sb) return key;
+        const uint32_t w = spatial_key_bits(mode);
+        if (w + sb <= 63u) return (scene << w) | key;
+        return (scene << (63u - sb)) | (key >> (w + sb - 63u));
     }
     // floats as unsigned integers in the same order (-0 below +0)
     static uint32_t float_order(float f) {
@@ -311,7 +324,7 @@ template <class T> struct World : WorldBase {
         std::memcpy(&f, &u, 4);
         return f;
     }
-    void key_frame(const std::vector<V3<T>>& centers, V3<T>& lo, T& scale) const {
+    void key_frame(const std::vector<V3<T>>& centers, T qmax, V3<T>& lo, T& scale) const {
         uint32_t w[6] = {0, 0, 0, 0, 0, 0};
         for (const V3<T>& c : centers) {
             const float cc[3] = {float(c.x), float(c.y), float(c.z)};
@@ -325,7 +338,7 @@ template <class T> struct World : WorldBase {
         lo = v3<T>(T(float_unorder(~w[3])), T(float_unorder(~w[4])), T(float_unorder(~w[5])));
         const V3<T> hi = v3<T>(T(float_unorder(w[0])), T(float_unorder(w[1])), T(float_unorder(w[2])));
         const T extent = mx(mx(hi.x - lo.x, hi.y - lo.y), hi.z - lo.z);
-        scale = extent > T(0) ? T(2097151.0f) / extent : T(1);
+        scale = extent > T(0) ? qmax / extent : T(1);
     }
     void compute_bounds() {
         std::vector<V3<T>> centers(C);
@@ -333,7 +346,8 @@ template <class T> struct World : WorldBase {
         for (int64_t ii = 0; ii < (int64_t)C; ++ii) centers[ii] = collider_center((uint32_t)ii);
         V3<T> lo = v3<T>(0, 0, 0);
         T scale = T(1);
-        if (morton_mode != MK_MORTON_REFERENCE_30) key_frame(centers, lo, scale);
+        const T qmax = frame_qmax(morton_mode);
+        if (morton_mode != MK_MORTON_REFERENCE_30) key_frame(centers, qmax, lo, scale);
 #pragma omp parallel for schedule(static)
         for (int64_t ii = 0; ii < (int64_t)C; ++ii) {
             uint32_t i = (uint32_t)ii;
@@ -346,13 +360,9 @@ template <class T> struct World : WorldBase {
             V3<T> e = absv(ax) * h.x + absv(ay) * h.y + absv(az) * h.z;
             aabb_min[i] = v4(c - e, T(0));
             aabb_max[i] = v4(c + e, T(0));
-            uint64_t key = morton_mode == MK_MORTON_REFERENCE_30 ? (uint64_t)morton30(c) : morton63(c, lo, scale);
-            if (scene_bits) {   // batched scenes: scene index above the spatial key
-                const uint64_t sc = col_scene[i];
-                key = morton_mode == MK_MORTON_REFERENCE_30 ? (sc << 30) | key
-                                                            : (sc << (63 - scene_bits)) | (key >> scene_bits);
-            }
-            keys[i] = key;
+            const uint64_t key = morton_mode == MK_MORTON_REFERENCE_30 ? (uint64_t)morton30(c)
+                                                                       : morton_frame(c, lo, scale, qmax);
+            keys[i] = compose_key(morton_mode, scene_bits, scene_bits ? col_scene[i] : 0u, key);
         }
         // Stable sort by key == ascending (key, index) order.
         std::vector<uint32_t> perm(C);
@@ -2532,7 +2542,10 @@ int or_cpu_contact_manifold(const float* ca, const float* qa, const float* ha, c
 
 uint32_t or_morton30(float x, float y, float z) { return World<float>::morton30(v3<float>(x, y, z)); }
 uint64_t or_morton63(float x, float y, float z, float lx, float ly, float lz, float scale) {
-    return World<float>::morton63(v3<float>(x, y, z), v3<float>(lx, ly, lz), scale);
+    return World<float>::morton_frame(v3<float>(x, y, z), v3<float>(lx, ly, lz), scale, 2097151.0f);
+}
+uint64_t or_morton48(float x, float y, float z, float lx, float ly, float lz, float scale) {
+    return World<float>::morton_frame(v3<float>(x, y, z), v3<float>(lx, ly, lz), scale, 65535.0f);
 }
 
 }  // extern "C"

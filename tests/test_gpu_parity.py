@@ -102,6 +102,14 @@ def test_reference_morton_mode_same_pairs(cuda_lib):
         compare_tick(gpu, orc, tick)
 
 
+def test_morton63_mode_bitexact(cuda_lib):
+    """21 bits per axis (two more radix passes than the default 16): same bit-exact path."""
+    scene = scenes.stack_grid(10, 6, 10, seed=5)
+    gpu, orc = make_pair(scene, GpuPhysicsConfig(morton_mode=abi.MORTON_63))
+    for tick in range(1, 4):
+        compare_tick(gpu, orc, tick)
+
+
 def test_graph_and_direct_launch_agree(cuda_lib):
     scene = scenes.stack_grid(8, 6, 8, seed=1)
     a = GpuPhysics(scene, GpuPhysicsConfig(use_graph=True))

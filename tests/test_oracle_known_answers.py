@@ -115,6 +115,19 @@ def test_morton63_orders_along_each_axis():
     assert oracle.morton63(0.0, 0.0, 2 * cell, lo, scale) > a
 
 
+def test_morton48_is_16_bits_per_axis():
+    # 2^16 - 1 cells over 10 m; the top corner fills all 48 bits
+    lo, scale = (-5.0, -5.0, -5.0), float(np.float32(65535.0) / np.float32(10.0))
+    assert oracle.morton48(-5.0, -5.0, -5.0, lo, scale) == 0
+    assert oracle.morton48(5.0, 5.0, 5.0, lo, scale) == (1 << 48) - 1
+    assert oracle.morton48(-4.0, 9.0, -5.0, lo, scale) >> 1 & 1 == 1       # y clamped high: bit 1 set
+    cell = 10.0 / 65535.0
+    x1 = oracle.morton48(-5.0 + 1.5 * cell, -5.0, -5.0, lo, scale)
+    assert x1 == 1                                                         # one cell along x: bit 0
+    assert oracle.morton48(-5.0, -5.0 + 1.5 * cell, -5.0, lo, scale) == 2
+    assert oracle.morton48(-5.0, -5.0, -5.0 + 1.5 * cell, lo, scale) == 4
+
+
 # ---------------------------------------------- compile.rs mass rules
 def test_hollow_cylinder_mass_and_inertia():
     """compile.rs:1010-1038 at the reference density of 500 kg/m^3."""
