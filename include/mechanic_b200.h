@@ -466,7 +466,7 @@ MK_API uint32_t mk_tick_kernel_count(const MkHandle* handle);
 
 /* Process-wide tuning knobs read when a tick is captured (mk_create) or an
  * operation is launched.  Keys: MK_TUNE_SORT_ITEMS (keys per thread of a
- * radix-sort tile: 2, 4 or 8; 0 = size-based default).  Returns the previous
+ * radix-sort tile: 2, 4, 6, 8, 11 or 16; 0 = size-based default).  Returns the previous
  * value, or -1 for an unknown key. */
 #define MK_TUNE_SORT_ITEMS 1u
 MK_API int mk_set_tuning(uint32_t key, uint32_t value);
@@ -474,8 +474,9 @@ MK_API int mk_set_tuning(uint32_t key, uint32_t value);
 /* Launch shapes of one handle's tick (no reference counterpart).  0 in any
  * field means the built-in default (for solve_items: every block). */
 typedef struct MkTuning {
-    uint32_t sort_items;          /* keys per thread of a onesweep tile: 2, 4 or 8 (default 8) */
-    uint32_t sort_ctas_per_sm;    /* onesweep CTAs per SM (default 3 for 8 keys, else 6) */
+    uint32_t sort_items;          /* keys per thread of the collider sort's 256-thread onesweep tile: 2, 4, 6,
+                                     8, 11 or 16 (default by size: 8 up to 64k keys, 11 up to 2M, else 16) */
+    uint32_t sort_ctas_per_sm;    /* onesweep CTAs per SM (default 2 for 11 or 16 keys, 3 for 8, else 6) */
     uint32_t append_ctas_per_sm;  /* CTAs per SM of the ordered-append kernels (default 8) */
     uint32_t solve_items;         /* 0 (default): every SM's block joins the cooperative solve; n > 0: only
                                      enough blocks for n contacts (and 4n bodies) per thread */

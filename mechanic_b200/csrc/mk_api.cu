@@ -626,6 +626,7 @@ int create_impl(const MkCreation* cr, const MkConfig* config, const MkCapacities
     const mk::MechTopology topo = mk::derive_topology(cr, h->mech_params);
 
     bool ok = check(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking), err, "stream");
+    ok = ok && check(mk::sort_prepare(), err, "sort kernel attributes");
     if (ok && (h->residual || h->mech_params.learned_precond))
         ok = check(mk::mlp::init(), err, "network kernel attributes");
     const uint64_t bytes = ok ? carve(h, nullptr) : 0;
@@ -1047,8 +1048,8 @@ uint32_t mk_tick_kernel_count(const MkHandle* h) { return h ? h->kernels_per_tic
 
 int mk_get_handle_tuning(const MkHandle* h, MkTuning* out) {
     if (!h || !out) return MK_ERR_INVALID_ARGUMENT;
-    out->sort_items = h->launch.sort_items ? h->launch.sort_items : 8u;
-    out->sort_ctas_per_sm = h->launch.sort_ctas ? h->launch.sort_ctas : (out->sort_items == 8 ? 3u : 6u);
+    out->sort_items = h->launch.sort_items ? h->launch.sort_items : mk::sort_items_for(h->C, h->sm_count);
+    out->sort_ctas_per_sm = h->launch.sort_ctas ? h->launch.sort_ctas : mk::default_sort_ctas(out->sort_items);
     out->append_ctas_per_sm = h->launch.append_ctas ? h->launch.append_ctas : 8u;
     out->solve_items = h->launch.solve_items;
     return MK_OK;
@@ -1060,7 +1061,7 @@ int mk_set_handle_tuning(MkHandle* h, const MkTuning* t, MkError* err) {
         set_error(err, MK_ERR_INVALID_ARGUMENT, "handle and tuning must be non-null");
         return MK_ERR_INVALID_ARGUMENT;
     }
-    const bool ok_items = t->sort_items == 0 || t->sort_items == 2 || t->sort_items == 4 || t->sort_items == 8;
+    const bool ok_items = t->sort_items == 0 || mk::valid_sort_items(t->sort_items);
     if (!ok_items || t->sort_ctas_per_sm > 32 || t->append_ctas_per_sm > 64 || t->solve_items > 64) {
         set_error(err, MK_ERR_INVALID_ARGUMENT, "tuning outside the supported shapes");
         return MK_ERR_INVALID_ARGUMENT;
@@ -1130,14 +1131,14 @@ int mk_autotune(MkHandle* h, uint32_t ticks, MkTuning* best, double* best_ms, Mk
     double cur_ms = 0.0;
     rc = measure(cur, &cur_ms);
     // coordinate descent over the launch shapes, two sweeps
-    const uint32_t sort_items[] = {2, 4, 8};
-    const uint32_t sort_ctas[] = {2, 3, 4, 6, 8};
+    const uint32_t sort_items[] = {4, 6, 8, 11, 16};
+    const uint32_t sort_ctas[] = {1, 2, 3, 4, 6};
     const uint32_t append_ctas[] = {4, 8, 16};
     const uint32_t solve_items[] = {0, 1, 2, 4};
     for (int sweep = 0; sweep < 2 && rc == MK_OK; ++sweep) {
         for (int field = 0; field < 4 && rc == MK_OK; ++field) {
             const uint32_t* vals = field == 0 ? sort_items : field == 1 ? sort_ctas : field == 2 ? append_ctas : solve_items;
-            const int nv = field == 0 ? 3 : field == 1 ? 5 : field == 2 ? 3 : 4;
+            const int nv = field == 0 ? 5 : field == 1 ? 5 : field == 2 ? 3 : 4;
             for (int i = 0; i < nv && rc == MK_OK; ++i) {
                 MkTuning cand = cur;
                 uint32_t* slot = field == 0 ? &cand.sort_items : field == 1 ? &cand.sort_ctas_per_sm

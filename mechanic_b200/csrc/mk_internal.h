@@ -84,7 +84,13 @@ struct SolveStats {
 // Launches implemented in mk_sort.cu.
 uint32_t sort_passes(uint32_t key_bits);
 void set_sort_items(uint32_t items);
-uint32_t sort_items_for(uint32_t n);
+uint32_t sort_items_for(uint32_t n, int sm_count);   // keys per thread of the onesweep tile by size
+bool valid_sort_items(uint32_t items);              // 2, 4, 6, 8, 11 or 16 keys per thread
+cudaError_t sort_prepare();   // per-device kernel attributes; call outside stream capture
+// Default CTAs per SM of each onesweep shape, and the fixed shape of the pair-key
+// sort (its count is only known on the device).
+inline uint32_t default_sort_ctas(uint32_t items) { return items >= 11 ? 2u : items == 8 ? 3u : 6u; }
+constexpr uint32_t kPairSortItems = 8;
 uint64_t sort_scratch_bytes(uint32_t n, uint32_t key_bits, bool values = true);
 cudaError_t launch_sort(const uint64_t* keys_in, const uint32_t* vals_in, uint64_t* keys_out, uint32_t* vals_out,
                         uint32_t n, const uint32_t* n_dev, uint32_t key_bits, void* scratch,
@@ -164,7 +170,7 @@ struct StepLaunch {
     bool collisions;
     bool learned_warm;        // run the learned warm start next to the cached one
     // launch shapes (0 = default); picked by mk_autotune or mk_set_handle_tuning
-    uint32_t sort_items;      // keys per thread of a onesweep tile: 2, 4 or 8
+    uint32_t sort_items;      // keys per thread of the collider sort's onesweep tile (0: size-based)
     uint32_t sort_ctas;       // onesweep CTAs per SM
     uint32_t append_ctas;     // CTAs per SM of the ordered-append kernels (narrowphase, ground, prepare)
     uint32_t solve_items;     // 0: every block joins the cooperative solve; n: blocks for n contacts per thread

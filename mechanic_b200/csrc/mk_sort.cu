@@ -10,6 +10,8 @@
 #include "mk_device.cuh"
 #include "mk_internal.h"
 
+#include <atomic>
+
 namespace mk {
 
 constexpr uint32_t kSortThreads = 256;
@@ -53,17 +55,33 @@ __device__ __forceinline__ uint32_t lanemask_lt() {
     return m;
 }
 
-template <uint32_t kSortItems>
-__global__ void __launch_bounds__(kSortThreads)
+// Shared-memory layout of a onesweep tile of kThreads x kItems keys: the
+// reordered keys and values and one digit counter row per warp (dynamic
+// shared memory: a 1024 x 8 tile takes 128 KB).
+template <uint32_t kThreads, uint32_t kItems>
+struct SortTile {
+    static constexpr uint32_t kTile = kThreads * kItems;
+    static constexpr uint32_t kWarps = kThreads / 32;
+    static constexpr size_t kValsOff = (size_t)kTile * 8;
+    static constexpr size_t kWarpOff = kValsOff + (size_t)kTile * 4;
+    static constexpr size_t kBytes = kWarpOff + (size_t)kWarps * kRadixBins * 4;
+};
+
+template <uint32_t kThreads, uint32_t kItems>
+__global__ void __launch_bounds__(kThreads)
 k_radix_onesweep(const uint64_t* __restrict__ keys_in, const uint32_t* __restrict__ vals_in,
                  uint64_t* __restrict__ keys_out, uint32_t* __restrict__ vals_out,
                  const uint32_t* __restrict__ n_ptr, uint32_t n_fixed, uint32_t shift,
                  const uint32_t* __restrict__ digit_hist /* 256 */, uint32_t* __restrict__ lookback,
                  uint32_t* __restrict__ ticket, uint32_t* __restrict__ error_flags) {
-    constexpr uint32_t kTile = kSortThreads * kSortItems;
-    __shared__ uint64_t s_keys[kTile];
-    __shared__ uint32_t s_vals[kTile];
-    __shared__ uint32_t s_warp[kSortThreads / 32][kRadixBins];
+    static_assert(kThreads >= kRadixBins && kThreads % 32 == 0, "one thread per digit at least");
+    using L = SortTile<kThreads, kItems>;
+    constexpr uint32_t kTile = L::kTile;
+    constexpr uint32_t kWarps = L::kWarps;
+    extern __shared__ __align__(16) unsigned char s_dyn[];
+    uint64_t* s_keys = reinterpret_cast<uint64_t*>(s_dyn);
+    uint32_t* s_vals = reinterpret_cast<uint32_t*>(s_dyn + L::kValsOff);
+    uint32_t (*s_warp)[kRadixBins] = reinterpret_cast<uint32_t (*)[kRadixBins]>(s_dyn + L::kWarpOff);
     __shared__ uint32_t s_local_start[kRadixBins];
     __shared__ uint32_t s_global_base[kRadixBins];
     __shared__ uint32_t s_scan[33];
@@ -73,126 +91,147 @@ k_radix_onesweep(const uint64_t* __restrict__ keys_in, const uint32_t* __restric
     const uint32_t n = n_ptr ? min(*n_ptr, n_fixed) : n_fixed;   // a device count never exceeds the capacity
     const uint32_t tiles = (n + kTile - 1) / kTile;
     const uint32_t lane = lane_id(), w = warp_id();
-    if (threadIdx.x == 0) s_tile = atomicAdd(ticket, 1u);   // in flight during the offsets scan
-    {   // this pass's digit offsets: exclusive scan of its histogram (kSortThreads == kRadixBins)
-        uint32_t total_all;
-        s_digit_offsets[threadIdx.x] = block_exclusive_scan(digit_hist[threadIdx.x], s_scan, &total_all);
-    }
+    const bool digit_thread = threadIdx.x < kRadixBins;
+    const uint32_t d = threadIdx.x;   // the digit of a digit thread
+    if (threadIdx.x == 0) s_tile = atomicAdd(ticket, 1u);
+    const uint32_t hist_d = digit_thread ? digit_hist[d] : 0u;   // scanned while the first tile loads
+    bool have_offsets = false;
 
     for (;;) {
-        for (uint32_t i = threadIdx.x; i < (kSortThreads / 32) * kRadixBins; i += kSortThreads)
-            (&s_warp[0][0])[i] = 0;
+        for (uint32_t i = threadIdx.x; i < kWarps * kRadixBins; i += kThreads) (&s_warp[0][0])[i] = 0;
         __syncthreads();
         const uint32_t tile = s_tile;
         if (tile >= tiles) break;
         const uint32_t tile_base = tile * kTile;
 
-        // ---- load every item first (one memory round trip), then rank within
-        // each warp, item by item (warp-striped)
-        uint64_t k[kSortItems];
-        uint32_t v[kSortItems];
-        uint32_t rank[kSortItems];
-        uint32_t dig[kSortItems];
+        // ---- load every item first (one memory round trip), warp-striped
+        uint64_t k[kItems];
+        uint32_t v[kItems];
+        uint32_t rank[kItems];
+        uint32_t dig[kItems];
 #pragma unroll
-        for (uint32_t i = 0; i < kSortItems; ++i) {
-            const uint32_t idx = tile_base + w * 32 * kSortItems + i * 32 + lane;
+        for (uint32_t i = 0; i < kItems; ++i) {
+            const uint32_t idx = tile_base + w * 32 * kItems + i * 32 + lane;
             const bool valid = idx < n;
             k[i] = valid ? __ldcg(keys_in + idx) : 0ull;
             v[i] = (valid && vals_in) ? __ldcg(vals_in + idx) : 0u;
+            dig[i] = valid ? (uint32_t)((k[i] >> shift) & 0xffu) : kRadixBins;
         }
+        if (!have_offsets) {   // this pass's digit offsets: exclusive scan of its histogram
+            uint32_t total_all;
+            const uint32_t off = block_exclusive_scan(hist_d, s_scan, &total_all);
+            if (digit_thread) s_digit_offsets[d] = off;
+            have_offsets = true;
+        }
+
+        // ---- rank within each warp, item by item: lanes with the same digit
+        // found by eight ballots (one per digit bit) under the valid-lane mask
 #pragma unroll
-        for (uint32_t i = 0; i < kSortItems; ++i) {
-            const uint32_t idx = tile_base + w * 32 * kSortItems + i * 32 + lane;
-            const bool valid = idx < n;
-            uint32_t d = valid ? (uint32_t)((k[i] >> shift) & 0xffu) : kRadixBins;
-            dig[i] = d;
-            uint32_t peers = __match_any_sync(0xffffffffu, d);
-            uint32_t leader = __ffs(peers) - 1;
+        for (uint32_t i = 0; i < kItems; ++i) {
+            const uint32_t di = dig[i];
+            const bool valid = di < kRadixBins;
+            uint32_t peers = __ballot_sync(0xffffffffu, valid);
+#pragma unroll
+            for (uint32_t bit = 0; bit < 8; ++bit) {
+                const uint32_t on = (di >> bit) & 1u;
+                const uint32_t bal = __ballot_sync(0xffffffffu, on);
+                peers &= on ? bal : ~bal;
+            }
+            const uint32_t leader = __ffs(peers) - 1;   // invalid lanes: unused
             uint32_t base = 0;
-            if (lane == leader && valid) base = s_warp[w][d];
-            base = __shfl_sync(0xffffffffu, base, leader);
+            if (valid && lane == leader) base = s_warp[w][di];
+            base = __shfl_sync(0xffffffffu, base, valid ? leader : lane);
             rank[i] = base + __popc(peers & lanemask_lt());
-            if (lane == leader && valid) s_warp[w][d] = base + __popc(peers);
+            if (valid && lane == leader) s_warp[w][di] = base + __popc(peers);
             __syncwarp();
         }
         __syncthreads();
 
         // ---- per digit: prefix over warps, tile count, tile-local start
-        const uint32_t d = threadIdx.x;   // kSortThreads == kRadixBins
         uint32_t count = 0;
-#pragma unroll
-        for (uint32_t ww = 0; ww < kSortThreads / 32; ++ww) {
-            uint32_t c = s_warp[ww][d];
-            s_warp[ww][d] = count;
-            count += c;
+        if (digit_thread) {
+#pragma unroll 8
+            for (uint32_t ww = 0; ww < kWarps; ++ww) {
+                const uint32_t c = s_warp[ww][d];
+                s_warp[ww][d] = count;
+                count += c;
+            }
         }
         uint32_t total;
-        uint32_t local_start = block_exclusive_scan(count, s_scan, &total);
-        s_local_start[d] = local_start;
+        const uint32_t local_start = block_exclusive_scan(count, s_scan, &total);
 
-        // ---- decoupled look-back for digit d (one thread per digit), reading a
-        // window of kLookbackWindow predecessors per round trip: with every tile
-        // starting at once, a one-word walk advances the inclusive prefixes by
-        // about two tiles per L2 round trip, a window by kLookbackWindow + 1
-        uint32_t* lb = lookback + (size_t)tile * kRadixBins + d;
-        uint32_t prefix = 0;
-        // (relaxed stores: a word carries its own status and count, and a
-        // release store's fence costs about an L2 round trip per tile)
-        if (tile == 0) {
-            st_relaxed_u32(lb, kDigitInclusive | count);
-        } else {
-            st_relaxed_u32(lb, kDigitAggregate | count);
-            int64_t t = (int64_t)tile - 1;
-            uint32_t spins = 0;
-            for (;;) {
-                uint32_t s[kLookbackWindow];
+        if (digit_thread) {
+            s_local_start[d] = local_start;
+            // ---- decoupled look-back for digit d (one thread per digit), reading a
+            // window of kLookbackWindow predecessors per round trip: with every tile
+            // starting at once, a one-word walk advances the inclusive prefixes by
+            // about two tiles per L2 round trip, a window by kLookbackWindow + 1
+            // (relaxed stores: a word carries its own status and count, and a
+            // release store's fence costs about an L2 round trip per tile)
+            uint32_t* lb = lookback + (size_t)tile * kRadixBins + d;
+            uint32_t prefix = 0;
+            if (tile == 0) {
+                st_relaxed_u32(lb, kDigitInclusive | count);
+            } else {
+                st_relaxed_u32(lb, kDigitAggregate | count);
+                int64_t t = (int64_t)tile - 1;
+                uint32_t spins = 0;
+                for (;;) {
+                    uint32_t sw[kLookbackWindow];
 #pragma unroll
-                for (uint32_t j = 0; j < kLookbackWindow; ++j)   // below tile 0: an inclusive 0
-                    s[j] = t >= (int64_t)j ? ld_relaxed_u32(lookback + (size_t)(t - j) * kRadixBins + d)
-                                           : kDigitInclusive;
-                uint32_t advanced = 0;
-                bool stop = false, done = false;
+                    for (uint32_t j = 0; j < kLookbackWindow; ++j)   // below tile 0: an inclusive 0
+                        sw[j] = t >= (int64_t)j ? ld_relaxed_u32(lookback + (size_t)(t - j) * kRadixBins + d)
+                                                : kDigitInclusive;
+                    uint32_t advanced = 0;
+                    bool stop = false, done = false;
 #pragma unroll
-                for (uint32_t j = 0; j < kLookbackWindow; ++j) {   // nearest first, up to the first gap
-                    const uint32_t status = s[j] >> 30;
-                    if (!stop) {
-                        if (status == 0) {
-                            stop = true;
-                        } else {
-                            prefix += s[j] & kDigitCountMask;
-                            ++advanced;
-                            if (status == 2) stop = done = true;
+                    for (uint32_t j = 0; j < kLookbackWindow; ++j) {   // nearest first, up to the first gap
+                        const uint32_t status = sw[j] >> 30;
+                        if (!stop) {
+                            if (status == 0) {
+                                stop = true;
+                            } else {
+                                prefix += sw[j] & kDigitCountMask;
+                                ++advanced;
+                                if (status == 2) stop = done = true;
+                            }
                         }
                     }
+                    if (done) break;
+                    if (advanced == 0) {
+                        if (++spins > kSpinLimit) {
+                            if (error_flags) atomicOr(error_flags, MK_DEVICE_WAIT_TIMEOUT_FLAG);
+                            break;
+                        }
+                        continue;
+                    }
+                    t -= advanced;
                 }
-                if (done) break;
-                if (advanced == 0) {
-                    if (++spins > kSpinLimit) { if (error_flags) atomicOr(error_flags, MK_DEVICE_WAIT_TIMEOUT_FLAG); break; }
-                    continue;
-                }
-                t -= advanced;
+                st_relaxed_u32(lb, kDigitInclusive | (prefix + count));
             }
-            st_relaxed_u32(lb, kDigitInclusive | (prefix + count));
+            s_global_base[d] = s_digit_offsets[d] + prefix - local_start;
         }
-        s_global_base[d] = s_digit_offsets[d] + prefix - local_start;
         __syncthreads();
 
         // ---- reorder through shared memory, then scatter by digit runs
 #pragma unroll
-        for (uint32_t i = 0; i < kSortItems; ++i) {
+        for (uint32_t i = 0; i < kItems; ++i) {
             if (dig[i] < kRadixBins) {
-                uint32_t r = s_local_start[dig[i]] + s_warp[w][dig[i]] + rank[i];
+                const uint32_t r = s_local_start[dig[i]] + s_warp[w][dig[i]] + rank[i];
                 s_keys[r] = k[i];
                 if (vals_out) s_vals[r] = v[i];
             }
         }
         __syncthreads();
-        for (uint32_t j = threadIdx.x; j < total; j += kSortThreads) {
-            uint64_t kk = s_keys[j];
-            uint32_t dd = (uint32_t)((kk >> shift) & 0xffu);
-            uint32_t dst = s_global_base[dd] + j;
-            keys_out[dst] = kk;
-            if (vals_out) vals_out[dst] = s_vals[j];
+#pragma unroll
+        for (uint32_t i = 0; i < kItems; ++i) {
+            const uint32_t j = threadIdx.x + i * kThreads;
+            if (j < total) {
+                const uint64_t kk = s_keys[j];
+                const uint32_t dst = s_global_base[(uint32_t)((kk >> shift) & 0xffu)] + j;
+                keys_out[dst] = kk;
+                if (vals_out) vals_out[dst] = s_vals[j];
+            }
         }
         __syncthreads();
         if (threadIdx.x == 0) s_tile = atomicAdd(ticket, 1u);   // every thread has read s_tile
@@ -201,16 +240,23 @@ k_radix_onesweep(const uint64_t* __restrict__ keys_in, const uint32_t* __restric
 
 uint32_t sort_passes(uint32_t key_bits) { return (key_bits + 7) / 8; }
 
-// Keys per thread of the onesweep tile: smaller tiles spread small sorts over
-// more SMs, larger tiles amortise the look-back on large ones.  The choice is
-// a tuning parameter (set_sort_items overrides the size-based default).
+// Keys per thread of a 256-thread onesweep tile.  The pass is latency bound:
+// its critical path is one tile's ranking (issue bound, so two tiles on one SM
+// take twice as long) plus the look-back chain (one L2 round trip per
+// kLookbackWindow tiles), so fewer, larger tiles win over spreading a sort
+// across every SM.  Measured per pass on B200: 100k keys 10.8 us at 8 keys per
+// thread (15.5 at 4); 400k 12.9 us at 11 or 16 (17.1 at 8); 1.6M 29.5 us at
+// 11; 6.4M 82 us at 16.  set_sort_items overrides the default (a tuning
+// parameter).
 static uint32_t g_sort_items_override = 0;
+bool valid_sort_items(uint32_t items) {
+    return items == 2 || items == 4 || items == 6 || items == 8 || items == 11 || items == 16;
+}
 void set_sort_items(uint32_t items) { g_sort_items_override = items; }
-uint32_t sort_items_for(uint32_t n) {
-    if (g_sort_items_override == 2 || g_sort_items_override == 4 || g_sort_items_override == 8)
-        return g_sort_items_override;
-    (void)n;
-    return 8u;   // measured fastest for 0.4M-14M keys on B200 (look-back chains dominate small tiles)
+uint32_t sort_items_for(uint32_t n, int sm_count) {
+    if (valid_sort_items(g_sort_items_override)) return g_sort_items_override;
+    (void)sm_count;
+    return n <= (1u << 16) ? 8u : n <= (1u << 21) ? 11u : 16u;
 }
 
 // The histogram bins and tile tickets of a sort's scratch: the region that must
@@ -226,7 +272,7 @@ void sort_clear_region(void* scratch, uint32_t n, uint32_t key_bits, bool values
 
 uint64_t sort_scratch_bytes(uint32_t n, uint32_t key_bits, bool values) {
     uint32_t passes = sort_passes(key_bits);
-    uint64_t tiles = (n + 2 * kSortThreads - 1) / (2 * kSortThreads);   // smallest tile: 512 keys
+    uint64_t tiles = (n + 511) / 512;   // smallest tile: 512 keys
     uint64_t b = 0;
     b += align256((uint64_t)n * 8);                       // ping-pong keys
     b += align256((uint64_t)(values ? n : 0) * 4);        // ping-pong values
@@ -240,8 +286,32 @@ template <uint32_t kItems>
 static void launch_pass(const uint64_t* sk, const uint32_t* sv, uint64_t* dk, uint32_t* dv, const uint32_t* n_dev,
                         uint32_t n, uint32_t shift, const uint32_t* offsets, uint32_t* lookback, uint32_t* ticket,
                         uint32_t* error_flags, uint32_t grid, cudaStream_t stream) {
-    k_radix_onesweep<kItems><<<grid, kSortThreads, 0, stream>>>(sk, sv, dk, dv, n_dev, n, shift, offsets, lookback,
-                                                                ticket, error_flags);
+    k_radix_onesweep<kSortThreads, kItems><<<grid, kSortThreads, SortTile<kSortThreads, kItems>::kBytes, stream>>>(
+        sk, sv, dk, dv, n_dev, n, shift, offsets, lookback, ticket, error_flags);
+}
+
+// Dynamic shared memory of every tile shape, set once per device (outside
+// stream capture: the first sort on a device, or handle creation).
+cudaError_t sort_prepare() {
+    static std::atomic<uint64_t> done{0};
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    const uint64_t bit = 1ull << (dev & 63);
+    if (done.load() & bit) return cudaSuccess;
+#define MK_SORT_ATTR(I)                                                                                       \
+    if (e == cudaSuccess)                                                                                    \
+        e = cudaFuncSetAttribute(k_radix_onesweep<kSortThreads, I>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
+                                 (int)SortTile<kSortThreads, I>::kBytes);
+    MK_SORT_ATTR(2)
+    MK_SORT_ATTR(4)
+    MK_SORT_ATTR(6)
+    MK_SORT_ATTR(8)
+    MK_SORT_ATTR(11)
+    MK_SORT_ATTR(16)
+#undef MK_SORT_ATTR
+    if (e == cudaSuccess) done.fetch_or(bit);
+    return e;
 }
 
 // Stream-ordered sort.  `n_dev` (device count) may be null, then n is used;
@@ -251,15 +321,16 @@ cudaError_t launch_sort(const uint64_t* keys_in, const uint32_t* vals_in, uint64
                         uint64_t scratch_bytes, uint32_t* error_flags, cudaStream_t stream, int sm_count,
                         uint32_t items_override, uint32_t ctas_per_sm, bool precleared) {
     if (n == 0) return cudaSuccess;
+    cudaError_t ep = sort_prepare();
+    if (ep != cudaSuccess) return ep;
     uint32_t passes = sort_passes(key_bits);
     if (passes == 0 || passes > 8) return cudaErrorInvalidValue;
     const bool values = vals_in != nullptr;
     if (scratch_bytes < sort_scratch_bytes(n, key_bits, values)) return cudaErrorInvalidValue;
-    const uint32_t items = (items_override == 2 || items_override == 4 || items_override == 8) ? items_override
-                                                                                              : sort_items_for(n);
+    const uint32_t items = valid_sort_items(items_override) ? items_override : sort_items_for(n, sm_count);
     const uint32_t tile_keys = kSortThreads * items;
     const uint64_t tiles = (n + tile_keys - 1) / tile_keys;
-    const uint64_t tiles_max = (n + 2 * kSortThreads - 1) / (2 * kSortThreads);
+    const uint64_t tiles_max = (n + 511) / 512;
     char* p = (char*)scratch;
     uint64_t* tmp_keys = (uint64_t*)p; p += align256((uint64_t)n * 8);
     uint32_t* tmp_vals = values ? (uint32_t*)p : nullptr; p += align256((uint64_t)(values ? n : 0) * 4);
@@ -276,7 +347,7 @@ cudaError_t launch_sort(const uint64_t* keys_in, const uint32_t* vals_in, uint64
     if (hist_blocks == 0) hist_blocks = 1;
     k_radix_histogram<<<hist_blocks, 256, 0, stream>>>(keys_in, n_dev, n, passes, hist, lookback,
                                                        tiles_max * kRadixBins, tile_keys);
-    const uint32_t per_sm = ctas_per_sm ? ctas_per_sm : (items == 8 ? 3u : 6u);
+    const uint32_t per_sm = ctas_per_sm ? ctas_per_sm : default_sort_ctas(items);
     uint32_t grid = (uint32_t)std::min<uint64_t>(tiles, (uint64_t)sm_count * per_sm);
     if (grid == 0) grid = 1;
     // passes alternate between (tmp, out) so that the last pass writes `out`.
@@ -287,15 +358,18 @@ cudaError_t launch_sort(const uint64_t* keys_in, const uint32_t* vals_in, uint64
         uint64_t* dk = to_out ? keys_out : tmp_keys;
         uint32_t* dv = values ? (to_out ? vals_out : tmp_vals) : nullptr;
         uint32_t* lb = lookback + (size_t)pass * tiles_max * kRadixBins;
-        if (items == 2)
-            launch_pass<2>(src_k, src_v, dk, dv, n_dev, n, 8 * pass, hist + pass * kRadixBins, lb, tickets + pass,
-                           error_flags, grid, stream);
-        else if (items == 4)
-            launch_pass<4>(src_k, src_v, dk, dv, n_dev, n, 8 * pass, hist + pass * kRadixBins, lb, tickets + pass,
-                           error_flags, grid, stream);
-        else
-            launch_pass<8>(src_k, src_v, dk, dv, n_dev, n, 8 * pass, hist + pass * kRadixBins, lb, tickets + pass,
-                           error_flags, grid, stream);
+        const uint32_t* offs = hist + pass * kRadixBins;
+#define MK_SORT_PASS(I)                                                                                          \
+    launch_pass<I>(src_k, src_v, dk, dv, n_dev, n, 8 * pass, offs, lb, tickets + pass, error_flags, grid, stream)
+        switch (items) {
+            case 2: MK_SORT_PASS(2); break;
+            case 4: MK_SORT_PASS(4); break;
+            case 6: MK_SORT_PASS(6); break;
+            case 8: MK_SORT_PASS(8); break;
+            case 11: MK_SORT_PASS(11); break;
+            default: MK_SORT_PASS(16); break;
+        }
+#undef MK_SORT_PASS
         src_k = dk;
         src_v = dv;
     }

@@ -1971,7 +1971,7 @@ cudaError_t launch_broadphase(const StepBuffers& b, const StepParams& p, const S
     k_traverse<<<blocks_for(C, kTravThreads), kTravThreads, 0, s>>>(b, p);
     e = launch_sort(b.pair_stage, nullptr, b.pair_keys, nullptr, p.pair_capacity, &b.counts->pairs_found,
                     2 * p.pair_shift, b.pair_sort_scratch, b.pair_sort_scratch_bytes, &b.diag->error_flags, s,
-                    l.sm_count, l.sort_items, l.sort_ctas, true);
+                    l.sm_count, kPairSortItems, 0, true);
     if (e != cudaSuccess) return e;
     return cudaGetLastError();
 }

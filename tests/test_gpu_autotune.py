@@ -25,7 +25,7 @@ def test_autotune_keeps_results_and_state(cuda_lib):
         b.dispatch_tick(tick)
     before = a.save_state()
     tuning, ms = a.autotune(ticks=2)
-    assert ms > 0 and tuning["sort_items"] in (2, 4, 8)
+    assert ms > 0 and tuning["sort_items"] in (2, 4, 6, 8, 11, 16)
     after = a.save_state()
     assert_bitwise(after["transforms"], before["transforms"], "restored transforms")
     assert_bitwise(after["velocities"], before["velocities"], "restored velocities")
