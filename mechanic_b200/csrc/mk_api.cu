@@ -154,6 +154,7 @@ uint64_t carve(MkHandle* h, char* base) {
     b.node_ranges = c.take<uint2>(C);
     b.leaf_scan = c.take<float4>(4ull * C);
     b.chunk_scan = c.take<float4>(6ull * ((C + 31) / 32));
+    b.chunk_table = c.take<float4>(8ull * ((C + 31) / 32));
     {
         const uint64_t ns = (C + 1023) / 1024;
         uint64_t levels = 1;
@@ -161,7 +162,7 @@ uint64_t carve(MkHandle* h, char* base) {
         b.super_table = c.take<float4>(2 * ns * levels);
     }
     b.node_aabbs = c.take<float4>(4ull * C);
-    b.node_records = c.take<float4>(4ull * C);
+    b.node_records = c.take<float4>(8ull * C);   // 128-byte 4-wide record per internal node
     b.suppressed = c.take<uint2>(std::max(h->S, 1u));
     b.pair_stage = c.take<uint64_t>(P);
     b.pair_keys = c.take<uint64_t>(P);

@@ -126,8 +126,9 @@ struct StepBuffers {
     float4* leaf_scan;           // 4 per leaf: prefix and suffix unions within its 32-leaf chunk
     float4* chunk_scan;          // 6 per chunk: total, prefix and suffix unions within its 1024-leaf super-chunk
     float4* super_table;         // 2 x super-chunks x levels: sparse table of super-chunk totals
+    float4* chunk_table;         // 2 x chunks x 4: sparse table levels 1-4 of chunk totals within a super-chunk
     float4* node_aabbs;          // 2 x float4 per node (union boxes)
-    float4* node_records;        // 4 x float4 per internal node (both children's boxes)
+    float4* node_records;        // 8 x float4 per internal node (4-wide record of its grandchildren)
     const uint2* suppressed;
     uint64_t* pair_stage;        // pair keys as found (pair_capacity)
     uint64_t* pair_keys;         // pair keys sorted: canonical pair list

@@ -26,9 +26,11 @@ constexpr uint32_t kDigitCountMask = (1u << 30) - 1;
 __global__ void __launch_bounds__(kSortThreads)
 k_radix_histogram(const uint64_t* __restrict__ keys, const uint32_t* __restrict__ n_ptr, uint32_t n_fixed,
                   uint32_t passes, uint32_t* __restrict__ hist /* passes x 256 */,
-                  uint32_t* __restrict__ lookback, uint64_t lookback_pass_words, uint32_t tile_keys) {
+                  uint32_t* __restrict__ lookback, uint64_t lookback_pass_words, uint32_t tile_keys,
+                  uint32_t small_n) {
     __shared__ uint32_t s_hist[8][kRadixBins];
     const uint32_t n = n_ptr ? min(*n_ptr, n_fixed) : n_fixed;   // a device count never exceeds the capacity
+    if (n <= small_n) return;   // sorted by k_radix_small
     // clear the look-back words the onesweep passes will use for this n only
     const uint64_t used = (uint64_t)((n + tile_keys - 1) / tile_keys) * kRadixBins;
     for (uint64_t w = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; w < used * passes;
@@ -55,9 +57,122 @@ __device__ __forceinline__ uint32_t lanemask_lt() {
     return m;
 }
 
+// Ranks this warp's items by digit, item by item: lanes with the same digit
+// are found by eight ballots (one per digit bit) under the valid-lane mask,
+// and s_warp_row counts each digit over the warp's earlier items.  Digit
+// kRadixBins marks an invalid item.
+template <uint32_t kItems>
+__device__ __forceinline__ void warp_rank(const uint32_t (&dig)[kItems], uint32_t (&rank)[kItems],
+                                          uint32_t* s_warp_row, uint32_t lane) {
+#pragma unroll
+    for (uint32_t i = 0; i < kItems; ++i) {
+        const uint32_t di = dig[i];
+        const bool valid = di < kRadixBins;
+        uint32_t peers = __ballot_sync(0xffffffffu, valid);
+#pragma unroll
+        for (uint32_t bit = 0; bit < 8; ++bit) {
+            const uint32_t on = (di >> bit) & 1u;
+            const uint32_t bal = __ballot_sync(0xffffffffu, on);
+            peers &= on ? bal : ~bal;
+        }
+        const uint32_t leader = __ffs(peers) - 1;   // invalid lanes: unused
+        uint32_t base = 0;
+        if (valid && lane == leader) base = s_warp_row[di];
+        base = __shfl_sync(0xffffffffu, base, valid ? leader : lane);
+        rank[i] = base + __popc(peers & lanemask_lt());
+        if (valid && lane == leader) s_warp_row[di] = base + __popc(peers);
+        __syncwarp();
+    }
+}
+
+// Sorts up to kSmallSortKeys keys in one 1024-thread CTA, every pass in shared
+// memory (no look-back, no histogram kernel: the tile's digit counts are the
+// whole sort's).  Light ticks sort a few thousand pair keys: one launch instead
+// of a histogram and one onesweep launch per digit.  With a device count above
+// kSmallSortKeys it returns at once and the onesweep passes sort.
+constexpr uint32_t kSmallThreads = 1024, kSmallItems = 8;
+constexpr uint32_t kSmallSortKeys = kSmallThreads * kSmallItems;
+constexpr size_t kSmallSmem = (size_t)kSmallSortKeys * 12 + (kSmallThreads / 32) * kRadixBins * 4;
+
+__global__ void __launch_bounds__(kSmallThreads)
+k_radix_small(const uint64_t* __restrict__ keys_in, const uint32_t* __restrict__ vals_in,
+              uint64_t* __restrict__ keys_out, uint32_t* __restrict__ vals_out, const uint32_t* __restrict__ n_ptr,
+              uint32_t n_fixed, uint32_t passes) {
+    const uint32_t n = n_ptr ? min(*n_ptr, n_fixed) : n_fixed;
+    if (n == 0 || n > kSmallSortKeys) return;
+    extern __shared__ __align__(16) unsigned char s_dyn[];
+    uint64_t* s_keys = reinterpret_cast<uint64_t*>(s_dyn);
+    uint32_t* s_vals = reinterpret_cast<uint32_t*>(s_dyn + (size_t)kSmallSortKeys * 8);
+    uint32_t (*s_warp)[kRadixBins] = reinterpret_cast<uint32_t (*)[kRadixBins]>(s_dyn + (size_t)kSmallSortKeys * 12);
+    __shared__ uint32_t s_local_start[kRadixBins];
+    __shared__ uint32_t s_scan[33];
+    const uint32_t lane = lane_id(), w = warp_id();
+    const uint32_t d = threadIdx.x;   // the digit of threads below kRadixBins
+    uint64_t k[kSmallItems];
+    uint32_t v[kSmallItems], dig[kSmallItems], rank[kSmallItems];
+#pragma unroll
+    for (uint32_t i = 0; i < kSmallItems; ++i) {   // warp-striped: items in index order
+        const uint32_t idx = w * 32 * kSmallItems + i * 32 + lane;
+        k[i] = idx < n ? keys_in[idx] : 0ull;
+        v[i] = (idx < n && vals_in) ? vals_in[idx] : 0u;
+    }
+    for (uint32_t pass = 0; pass < passes; ++pass) {
+        const uint32_t shift = 8 * pass;
+        for (uint32_t q = threadIdx.x; q < (kSmallThreads / 32) * kRadixBins; q += kSmallThreads)
+            (&s_warp[0][0])[q] = 0;
+        __syncthreads();
+#pragma unroll
+        for (uint32_t i = 0; i < kSmallItems; ++i) {
+            const uint32_t idx = w * 32 * kSmallItems + i * 32 + lane;
+            dig[i] = idx < n ? (uint32_t)((k[i] >> shift) & 0xffu) : kRadixBins;
+        }
+        warp_rank<kSmallItems>(dig, rank, s_warp[w], lane);
+        __syncthreads();
+        uint32_t count = 0;
+        if (d < kRadixBins) {
+#pragma unroll 8
+            for (uint32_t ww = 0; ww < kSmallThreads / 32; ++ww) {
+                const uint32_t c = s_warp[ww][d];
+                s_warp[ww][d] = count;
+                count += c;
+            }
+        }
+        uint32_t total;
+        const uint32_t start = block_exclusive_scan(count, s_scan, &total);
+        if (d < kRadixBins) s_local_start[d] = start;
+        __syncthreads();
+#pragma unroll
+        for (uint32_t i = 0; i < kSmallItems; ++i) {
+            if (dig[i] < kRadixBins) {
+                const uint32_t r = s_local_start[dig[i]] + s_warp[w][dig[i]] + rank[i];
+                s_keys[r] = k[i];
+                s_vals[r] = v[i];
+            }
+        }
+        __syncthreads();
+#pragma unroll
+        for (uint32_t i = 0; i < kSmallItems; ++i) {
+            const uint32_t idx = w * 32 * kSmallItems + i * 32 + lane;
+            if (idx < n) {
+                k[i] = s_keys[idx];
+                v[i] = s_vals[idx];
+            }
+        }
+        __syncthreads();
+    }
+#pragma unroll
+    for (uint32_t i = 0; i < kSmallItems; ++i) {
+        const uint32_t idx = w * 32 * kSmallItems + i * 32 + lane;
+        if (idx < n) {
+            keys_out[idx] = k[i];
+            if (vals_out) vals_out[idx] = v[i];
+        }
+    }
+}
+
 // Shared-memory layout of a onesweep tile of kThreads x kItems keys: the
 // reordered keys and values and one digit counter row per warp (dynamic
-// shared memory: a 1024 x 8 tile takes 128 KB).
+// shared memory: a 256 x 16 tile takes 56 KB).
 template <uint32_t kThreads, uint32_t kItems>
 struct SortTile {
     static constexpr uint32_t kTile = kThreads * kItems;
@@ -73,7 +188,7 @@ k_radix_onesweep(const uint64_t* __restrict__ keys_in, const uint32_t* __restric
                  uint64_t* __restrict__ keys_out, uint32_t* __restrict__ vals_out,
                  const uint32_t* __restrict__ n_ptr, uint32_t n_fixed, uint32_t shift,
                  const uint32_t* __restrict__ digit_hist /* 256 */, uint32_t* __restrict__ lookback,
-                 uint32_t* __restrict__ ticket, uint32_t* __restrict__ error_flags) {
+                 uint32_t* __restrict__ ticket, uint32_t* __restrict__ error_flags, uint32_t small_n) {
     static_assert(kThreads >= kRadixBins && kThreads % 32 == 0, "one thread per digit at least");
     using L = SortTile<kThreads, kItems>;
     constexpr uint32_t kTile = L::kTile;
@@ -90,6 +205,9 @@ k_radix_onesweep(const uint64_t* __restrict__ keys_in, const uint32_t* __restric
 
     const uint32_t n = n_ptr ? min(*n_ptr, n_fixed) : n_fixed;   // a device count never exceeds the capacity
     const uint32_t tiles = (n + kTile - 1) / kTile;
+    // a small device count was sorted by k_radix_small; CTAs past the tile count
+    // leave before taking a ticket (the grid is sized for the capacity)
+    if (n <= small_n || blockIdx.x >= tiles) return;
     const uint32_t lane = lane_id(), w = warp_id();
     const bool digit_thread = threadIdx.x < kRadixBins;
     const uint32_t d = threadIdx.x;   // the digit of a digit thread
@@ -124,27 +242,8 @@ k_radix_onesweep(const uint64_t* __restrict__ keys_in, const uint32_t* __restric
             have_offsets = true;
         }
 
-        // ---- rank within each warp, item by item: lanes with the same digit
-        // found by eight ballots (one per digit bit) under the valid-lane mask
-#pragma unroll
-        for (uint32_t i = 0; i < kItems; ++i) {
-            const uint32_t di = dig[i];
-            const bool valid = di < kRadixBins;
-            uint32_t peers = __ballot_sync(0xffffffffu, valid);
-#pragma unroll
-            for (uint32_t bit = 0; bit < 8; ++bit) {
-                const uint32_t on = (di >> bit) & 1u;
-                const uint32_t bal = __ballot_sync(0xffffffffu, on);
-                peers &= on ? bal : ~bal;
-            }
-            const uint32_t leader = __ffs(peers) - 1;   // invalid lanes: unused
-            uint32_t base = 0;
-            if (valid && lane == leader) base = s_warp[w][di];
-            base = __shfl_sync(0xffffffffu, base, valid ? leader : lane);
-            rank[i] = base + __popc(peers & lanemask_lt());
-            if (valid && lane == leader) s_warp[w][di] = base + __popc(peers);
-            __syncwarp();
-        }
+        // ---- rank within each warp
+        warp_rank<kItems>(dig, rank, s_warp[w], lane);
         __syncthreads();
 
         // ---- per digit: prefix over warps, tile count, tile-local start
@@ -285,9 +384,9 @@ uint64_t sort_scratch_bytes(uint32_t n, uint32_t key_bits, bool values) {
 template <uint32_t kItems>
 static void launch_pass(const uint64_t* sk, const uint32_t* sv, uint64_t* dk, uint32_t* dv, const uint32_t* n_dev,
                         uint32_t n, uint32_t shift, const uint32_t* offsets, uint32_t* lookback, uint32_t* ticket,
-                        uint32_t* error_flags, uint32_t grid, cudaStream_t stream) {
+                        uint32_t* error_flags, uint32_t grid, uint32_t small_n, cudaStream_t stream) {
     k_radix_onesweep<kSortThreads, kItems><<<grid, kSortThreads, SortTile<kSortThreads, kItems>::kBytes, stream>>>(
-        sk, sv, dk, dv, n_dev, n, shift, offsets, lookback, ticket, error_flags);
+        sk, sv, dk, dv, n_dev, n, shift, offsets, lookback, ticket, error_flags, small_n);
 }
 
 // Dynamic shared memory of every tile shape, set once per device (outside
@@ -310,6 +409,8 @@ cudaError_t sort_prepare() {
     MK_SORT_ATTR(11)
     MK_SORT_ATTR(16)
 #undef MK_SORT_ATTR
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_radix_small, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmallSmem);
     if (e == cudaSuccess) done.fetch_or(bit);
     return e;
 }
@@ -327,6 +428,11 @@ cudaError_t launch_sort(const uint64_t* keys_in, const uint32_t* vals_in, uint64
     if (passes == 0 || passes > 8) return cudaErrorInvalidValue;
     const bool values = vals_in != nullptr;
     if (scratch_bytes < sort_scratch_bytes(n, key_bits, values)) return cudaErrorInvalidValue;
+    // at most kSmallSortKeys keys: one CTA sorts them in shared memory; with a
+    // device count it runs first and the histogram and passes skip small counts
+    k_radix_small<<<1, kSmallThreads, kSmallSmem, stream>>>(keys_in, vals_in, keys_out, vals_out, n_dev, n, passes);
+    if (!n_dev && n <= kSmallSortKeys) return cudaGetLastError();
+    const uint32_t small_n = n_dev ? kSmallSortKeys : 0u;
     const uint32_t items = valid_sort_items(items_override) ? items_override : sort_items_for(n, sm_count);
     const uint32_t tile_keys = kSortThreads * items;
     const uint64_t tiles = (n + tile_keys - 1) / tile_keys;
@@ -346,7 +452,7 @@ cudaError_t launch_sort(const uint64_t* keys_in, const uint32_t* vals_in, uint64
     uint32_t hist_blocks = (uint32_t)std::min<uint64_t>((n + 4095) / 4096, (uint64_t)sm_count * 4);
     if (hist_blocks == 0) hist_blocks = 1;
     k_radix_histogram<<<hist_blocks, 256, 0, stream>>>(keys_in, n_dev, n, passes, hist, lookback,
-                                                       tiles_max * kRadixBins, tile_keys);
+                                                       tiles_max * kRadixBins, tile_keys, small_n);
     const uint32_t per_sm = ctas_per_sm ? ctas_per_sm : default_sort_ctas(items);
     uint32_t grid = (uint32_t)std::min<uint64_t>(tiles, (uint64_t)sm_count * per_sm);
     if (grid == 0) grid = 1;
@@ -360,7 +466,8 @@ cudaError_t launch_sort(const uint64_t* keys_in, const uint32_t* vals_in, uint64
         uint32_t* lb = lookback + (size_t)pass * tiles_max * kRadixBins;
         const uint32_t* offs = hist + pass * kRadixBins;
 #define MK_SORT_PASS(I)                                                                                          \
-    launch_pass<I>(src_k, src_v, dk, dv, n_dev, n, 8 * pass, offs, lb, tickets + pass, error_flags, grid, stream)
+    launch_pass<I>(src_k, src_v, dk, dv, n_dev, n, 8 * pass, offs, lb, tickets + pass, error_flags, grid, small_n, \
+                   stream)
         switch (items) {
             case 2: MK_SORT_PASS(2); break;
             case 4: MK_SORT_PASS(4); break;

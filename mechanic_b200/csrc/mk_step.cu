@@ -322,13 +322,48 @@ __device__ __forceinline__ Box2 shfl_box(Box2 v, int o, bool up) {
         d[k] = up ? __shfl_up_sync(0xffffffffu, q[k], o) : __shfl_down_sync(0xffffffffu, q[k], o);
     return r;
 }
+__device__ __forceinline__ Box2 shfl_box_idx(Box2 v, uint32_t src) {
+    Box2 r;
+    float* d = reinterpret_cast<float*>(&r);
+    const float* q = reinterpret_cast<const float*>(&v);
+#pragma unroll
+    for (int k = 0; k < 8; ++k) d[k] = __shfl_sync(0xffffffffu, q[k], src);
+    return r;
+}
+// Sparse table over a warp's 32 boxes: T[k] at lane l is the union of lanes
+// [l, l + 2^k) (cut at lane 31), so the union of lanes [a, z] is that of
+// T[k] at a and at z + 1 - 2^k with k = min(floor(log2(z - a + 1)), 4).
+__device__ __forceinline__ void warp_sparse_table(Box2 (&T)[5], Box2 v, uint32_t lane) {
+    T[0] = v;
+#pragma unroll
+    for (int k = 1; k < 5; ++k) {
+        const Box2 d = shfl_box(T[k - 1], 1 << (k - 1), false);
+        T[k] = (int)lane + (1 << (k - 1)) < 32 ? box_union(T[k - 1], d) : T[k - 1];
+    }
+}
+// Union of lanes [a, z] from the table (every lane takes part; `want` marks the
+// lanes whose result is used).
+__device__ __forceinline__ Box2 warp_range_union(const Box2 (&T)[5], bool want, uint32_t a, uint32_t z, uint32_t lane) {
+    const uint32_t k = want ? min(31u - __clz(z - a + 1u), 4u) : 0u;   // 32 lanes: two 16-lane windows
+    const uint32_t s0 = want ? a : lane, s1 = want ? z + 1u - (1u << k) : lane;
+    Box2 r = box_empty();
+#pragma unroll
+    for (uint32_t kk = 0; kk < 5; ++kk) {
+        const Box2 x0 = shfl_box_idx(T[kk], s0), x1 = shfl_box_idx(T[kk], s1);
+        if (kk == k) r = box_union(x0, x1);
+    }
+    return r;
+}
 __device__ __forceinline__ Box2 ld_box(const float4* p) { return {__ldg(p), __ldg(p + 1)}; }   // written by earlier launches
 __device__ __forceinline__ Box2 ld_box_cg(const float4* p) { return {__ldcg(p), __ldcg(p + 1)}; }
 __device__ __forceinline__ void st_box(float4* p, Box2 v) { p[0] = v.mn; p[1] = v.mx; }
 
 // Leaf boxes in sorted order, their prefix/suffix unions within 32-leaf chunks,
-// the chunks' prefix/suffix unions within the block's super-chunk, and the
-// super-chunk's total (level 0 of the sparse table).
+// the boxes of the internal nodes whose leaf range lies inside one chunk (from
+// a warp sparse table; Karras node i's range has i at one end, so the warp of
+// leaf i owns node i), the chunks' prefix/suffix unions and sparse table within
+// the block's super-chunk, and the super-chunk's total (level 0 of the sparse
+// table over super-chunks).
 __global__ void __launch_bounds__(kRefitBlock) k_refit_leaves(StepBuffers b, StepParams p) {
     __shared__ Box2 s_chunk[32];
     const uint32_t n = p.collider_count;
@@ -356,6 +391,21 @@ __global__ void __launch_bounds__(kRefitBlock) k_refit_leaves(StepBuffers b, Ste
         float4* ls = b.leaf_scan + 4ull * t;
         ls[0] = pre.mn; ls[1] = pre.mx; ls[2] = suf.mn; ls[3] = suf.mx;
     }
+    {
+        Box2 T[5];
+        warp_sparse_table(T, v, lane);
+        uint2 rg = make_uint2(1u, 0u);
+        bool inner = false;
+        if (n > 1 && t < n - 1) {
+            rg = b.node_ranges[t];
+            inner = (rg.x >> 5) == (rg.y >> 5);
+        }
+        const Box2 r = warp_range_union(T, inner, rg.x & 31u, rg.y & 31u, lane);
+        if (inner) {
+            b.node_aabbs[2ull * t] = make_float4(r.mn.x, r.mn.y, r.mn.z, __uint_as_float(rg.y));
+            b.node_aabbs[2ull * t + 1] = make_float4(r.mx.x, r.mx.y, r.mx.z, 0.0f);
+        }
+    }
     if (lane == 31) s_chunk[w] = pre;
     __syncthreads();
     if (w == 0) {
@@ -374,6 +424,13 @@ __global__ void __launch_bounds__(kRefitBlock) k_refit_leaves(StepBuffers b, Ste
             cr[0] = c.mn; cr[1] = c.mx; cr[2] = cp.mn; cr[3] = cp.mx; cr[4] = cs.mn; cr[5] = cs.mx;
         }
         if (lane == 31) st_box(b.super_table + 2ull * blockIdx.x, cp);
+        Box2 T[5];
+        warp_sparse_table(T, c, lane);
+        const uint32_t chunks = (n + 31) / 32;
+        if (chunk < chunks) {
+#pragma unroll
+            for (int k = 1; k < 5; ++k) st_box(b.chunk_table + 2ull * (chunks * (k - 1) + chunk), T[k]);
+        }
     }
 }
 
@@ -398,13 +455,15 @@ __device__ __forceinline__ Box2 leaf_box(const StepBuffers& b, uint32_t leaf_bas
     return {make_float4(mn.x, mn.y, mn.z, 0.0f), make_float4(mx.x, mx.y, mx.z, 0.0f)};
 }
 
-// Union of the chunk totals [c0, c1] inside one super-chunk.
-__device__ __forceinline__ Box2 chunks_union(const StepBuffers& b, uint32_t c0, uint32_t c1) {
+// Union of the chunk totals [c0, c1] inside one super-chunk: a prefix, a
+// suffix, or two entries of the chunk sparse table.
+__device__ __forceinline__ Box2 chunks_union(const StepBuffers& b, uint32_t n, uint32_t c0, uint32_t c1) {
     if ((c0 & 31u) == 0) return ld_box(b.chunk_scan + 6ull * c1 + 2);   // prefix of c1
     if ((c1 & 31u) == 31u) return ld_box(b.chunk_scan + 6ull * c0 + 4);   // suffix of c0
-    Box2 u = box_empty();
-    for (uint32_t c = c0; c <= c1; ++c) u = box_union(u, ld_box(b.chunk_scan + 6ull * c));
-    return u;
+    const uint32_t k = 31u - __clz(c1 - c0 + 1u);
+    if (k == 0) return ld_box(b.chunk_scan + 6ull * c0);   // one chunk's total
+    const float4* lvl = b.chunk_table + 2ull * ((n + 31) / 32) * (k - 1);
+    return box_union(ld_box(lvl + 2ull * c0), ld_box(lvl + 2ull * (c1 + 1u - (1u << k))));
 }
 
 // Union of the sorted leaves [f, l].
@@ -422,7 +481,7 @@ __device__ Box2 range_box(const StepBuffers& b, uint32_t n, uint32_t f, uint32_t
     if (cf + 1 > cl - 1) return u;
     const uint32_t a = cf + 1, z = cl - 1;
     const uint32_t sa = a >> 5, sz = z >> 5;
-    if (sa == sz) return box_union(u, chunks_union(b, a, z));
+    if (sa == sz) return box_union(u, chunks_union(b, n, a, z));
     u = box_union(u, ld_box(b.chunk_scan + 6ull * a + 4));   // suffix of a within its super-chunk
     u = box_union(u, ld_box(b.chunk_scan + 6ull * z + 2));   // prefix of z within its super-chunk
     if (sa + 1 <= sz - 1) {
@@ -435,7 +494,19 @@ __device__ Box2 range_box(const StepBuffers& b, uint32_t n, uint32_t f, uint32_t
     return u;
 }
 
-// Per internal node: both children's boxes, its traversal record and union.
+// Per internal node: its union box and a 4-wide traversal record (128 bytes,
+// one cache line) holding its grandchildren in leaf order -- a leaf child is
+// one entry, an internal child gives its two children -- so a traversal step
+// descends two levels with one load.  Entry: {min.xyz, code} {max.xyz, last
+// leaf}, code = child node index or kLeafCode | collider index; unused
+// trailing entries have last leaf 0.  An entry's first leaf is one past the
+// last leaf of the entry before it (the first entry starts where the node
+// does).
+struct TravEntry {
+    Box2 box;
+    uint32_t code, last;
+};
+
 __global__ void __launch_bounds__(kBlock) k_refit_nodes(StepBuffers b, StepParams p) {
     const uint32_t n = p.collider_count;
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -444,18 +515,50 @@ __global__ void __launch_bounds__(kBlock) k_refit_nodes(StepBuffers b, StepParam
     const uint2 ch = b.children[i];
     const uint2 rg = b.node_ranges[i];
     const uint32_t split = ch.x >= leaf_base ? ch.x - leaf_base : ch.x;
-    const Box2 lb = range_box(b, n, rg.x, split);
-    const Box2 rb = range_box(b, n, split + 1, rg.y);
-    const uint32_t lcode = ch.x >= leaf_base ? (kLeafCode | b.svals[ch.x - leaf_base]) : ch.x;
-    const uint32_t rcode = ch.y >= leaf_base ? (kLeafCode | b.svals[ch.y - leaf_base]) : ch.y;
-    float4* rec = b.node_records + 4ull * i;
-    rec[0] = make_float4(lb.mn.x, lb.mn.y, lb.mn.z, __uint_as_float(lcode));
-    rec[1] = make_float4(lb.mx.x, lb.mx.y, lb.mx.z, __uint_as_float(split));
-    rec[2] = make_float4(rb.mn.x, rb.mn.y, rb.mn.z, __uint_as_float(rcode));
-    rec[3] = make_float4(rb.mx.x, rb.mx.y, rb.mx.z, __uint_as_float(rg.y));
-    b.node_aabbs[2ull * i] = make_float4(mnf(lb.mn.x, rb.mn.x), mnf(lb.mn.y, rb.mn.y), mnf(lb.mn.z, rb.mn.z),
-                                         __uint_as_float(rg.y));
-    b.node_aabbs[2ull * i + 1] = make_float4(mxf(lb.mx.x, rb.mx.x), mxf(lb.mx.y, rb.mx.y), mxf(lb.mx.z, rb.mx.z), 0.0f);
+    // children's children (Karras: an internal node's left child covers [first, split])
+    const uint2 cl = ch.x < leaf_base ? b.children[ch.x] : make_uint2(0u, 0u);
+    const uint2 cr = ch.y < leaf_base ? b.children[ch.y] : make_uint2(0u, 0u);
+    auto code_of = [&](uint32_t c) { return c >= leaf_base ? (kLeafCode | b.svals[c - leaf_base]) : c; };
+    auto split_of = [&](uint32_t left) { return left >= leaf_base ? left - leaf_base : left; };
+    // a node's box: a leaf's own, an in-chunk node's from k_refit_leaves, else a range union
+    auto box_of = [&](uint32_t c, uint32_t f, uint32_t l) -> Box2 {
+        if (c >= leaf_base) return leaf_box(b, leaf_base, f);
+        if ((f >> 5) == (l >> 5)) return ld_box(b.node_aabbs + 2ull * c);
+        return range_box(b, n, f, l);
+    };
+    TravEntry e[4];
+    uint32_t m = 0;
+    if (ch.x >= leaf_base) {
+        e[m++] = {leaf_box(b, leaf_base, rg.x), code_of(ch.x), rg.x};
+    } else {
+        const uint32_t s = split_of(cl.x);
+        e[m++] = {box_of(cl.x, rg.x, s), code_of(cl.x), s};
+        e[m++] = {box_of(cl.y, s + 1, split), code_of(cl.y), split};
+    }
+    if (ch.y >= leaf_base) {
+        e[m++] = {leaf_box(b, leaf_base, rg.y), code_of(ch.y), rg.y};
+    } else {
+        const uint32_t s = split_of(cr.x);
+        e[m++] = {box_of(cr.x, split + 1, s), code_of(cr.x), s};
+        e[m++] = {box_of(cr.y, s + 1, rg.y), code_of(cr.y), rg.y};
+    }
+    float4* rec = b.node_records + 8ull * i;
+    Box2 u = box_empty();
+#pragma unroll
+    for (uint32_t k = 0; k < 4; ++k) {
+        if (k < m) {
+            u = box_union(u, e[k].box);
+            rec[2 * k] = make_float4(e[k].box.mn.x, e[k].box.mn.y, e[k].box.mn.z, __uint_as_float(e[k].code));
+            rec[2 * k + 1] = make_float4(e[k].box.mx.x, e[k].box.mx.y, e[k].box.mx.z, __uint_as_float(e[k].last));
+        } else {
+            rec[2 * k] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+            rec[2 * k + 1] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        }
+    }
+    if ((rg.x >> 5) != (rg.y >> 5)) {   // in-chunk nodes were written by k_refit_leaves
+        b.node_aabbs[2ull * i] = make_float4(u.mn.x, u.mn.y, u.mn.z, __uint_as_float(rg.y));
+        b.node_aabbs[2ull * i + 1] = make_float4(u.mx.x, u.mx.y, u.mx.z, 0.0f);
+    }
 }
 
 // ---------------------------------------------------------------- traverse
@@ -514,14 +617,15 @@ __global__ void __launch_bounds__(kTravThreads) k_traverse(StepBuffers b, StepPa
         uint32_t sp = 0;
         uint32_t node = 0;
         for (;;) {
-            const float4* rec = b.node_records + 4ull * node;
-            const uint32_t left_last = __float_as_uint(__ldg(rec + 1).w);
+            const float4* rec = b.node_records + 8ull * node;   // 4-wide: two levels per step
+            float4 r[8];
 #pragma unroll
-            for (int side = 0; side < 2; ++side) {
-                const float4 cmax = __ldg(rec + 2 * side + 1);
+            for (int q = 0; q < 8; ++q) r[q] = __ldg(rec + q);
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                const float4 cmin = r[2 * k], cmax = r[2 * k + 1];
                 if (__float_as_uint(cmax.w) <= t) continue;     // nothing to the right of this leaf below
-                if (side == 1 && left_last + 1u >= limit) continue;   // starts past this scene
-                const float4 cmin = __ldg(rec + 2 * side);
+                if (k > 0 && __float_as_uint(r[2 * k - 1].w) + 1u >= limit) continue;   // starts past this scene
                 if (!overlaps(qmin, qmax, cmin, cmax)) continue;
                 const uint32_t code = __float_as_uint(cmin.w);
                 if (code & kLeafCode) {
@@ -1172,17 +1276,28 @@ __device__ __forceinline__ void add_contact_deltas(int32_t* deltas, bool live, u
     }
 }
 
+// This block's contiguous, warp-aligned slice [x, y) of the A active contacts:
+// every SM gets about A / blocks of them (a pass is issue bound on the SMs
+// that hold contacts, so whole 1024-contact blocks on a few SMs left the
+// others idle).  Contacts keep their order inside a warp.
+__device__ __forceinline__ uint2 contact_slice(uint32_t A, uint32_t blocks) {
+    const uint32_t per = ((A + blocks - 1u) / blocks + 31u) & ~31u;
+    const uint32_t begin = (uint32_t)min((uint64_t)A, (uint64_t)blockIdx.x * per);
+    return make_uint2(begin, min(A, begin + per));
+}
+
+// The contacts [sl.x, sl.y) of this block, blockDim.x at a time.
 template <bool kWarm, bool kFused = false>
-__device__ __forceinline__ void solve_span(const StepBuffers& b, const StepParams& p, GpuContact* cur, uint32_t A,
-                                           uint32_t first, uint32_t stride, const float4* vl, const float4* va,
-                                           const FusedPass* fp = nullptr, int32_t* dacc = nullptr) {
+__device__ __forceinline__ void solve_span(const StepBuffers& b, const StepParams& p, GpuContact* cur, uint2 sl,
+                                           const float4* vl, const float4* va, const FusedPass* fp = nullptr,
+                                           int32_t* dacc = nullptr) {
     int32_t* deltas = kFused ? dacc : b.deltas;
-    for (uint32_t base = first; base < A; base += stride) {
+    for (uint32_t base = sl.x; base < sl.y; base += blockDim.x) {
         const uint32_t t = base + threadIdx.x;
         bool live = false;
         uint32_t a = kInvalid, bb = kInvalid;
         int32_t da[6] = {0, 0, 0, 0, 0, 0}, db[6] = {0, 0, 0, 0, 0, 0};
-        if (t < A) {
+        if (t < sl.y) {
             const uint32_t k = __ldcg(b.active + t);
             float4* row = reinterpret_cast<float4*>(cur + k);
             const float4 r0 = __ldcg(row), np = __ldcg(row + 1), aa = __ldcg(row + 2), ab = __ldcg(row + 3);
@@ -1264,9 +1379,11 @@ __device__ __forceinline__ void grid_barrier(uint32_t* state, uint32_t* error_fl
 // contacts touch the same bodies in every pass; rows of other bodies are never
 // read).  The row keeps the last pass's impulse, as after per-pass stores.
 __device__ __forceinline__ void solve_fused_resident(const StepBuffers& b, const StepParams& p, GpuContact* cur,
-                                                  uint32_t A, uint32_t iterations, uint32_t t, int32_t* const* D,
+                                                  uint32_t A, uint32_t iterations, int32_t* const* D,
                                                   uint32_t gen, uint32_t* barrier, uint32_t parts) {
-    const bool has = t < A;
+    const uint2 sl = contact_slice(A, parts);   // at most blockDim.x contacts: A <= parts * blockDim.x
+    const uint32_t t = sl.x + threadIdx.x;
+    const bool has = t < sl.y;
     uint32_t a = kInvalid, bb = kInvalid;
     f3 arm_a = mkf3(0, 0, 0), arm_b = mkf3(0, 0, 0), nrm = mkf3(0, 0, 0);
     float depth = 0.0f, acc = 0.0f, den = 0.0f;
@@ -1357,7 +1474,7 @@ __global__ void __launch_bounds__(kSolveThreads) k_solve_all(StepBuffers b, Step
         const uint32_t gen = b.tick->generation;
         const uint32_t gtid = first + threadIdx.x;
         if (A <= stride) {
-            solve_fused_resident(b, p, cur, A, iterations, gtid, D, gen, barrier, parts);
+            solve_fused_resident(b, p, cur, A, iterations, D, gen, barrier, parts);
         } else {
         for (uint32_t it = 0; it < iterations; ++it) {
             FusedPass fp;
@@ -1368,8 +1485,8 @@ __global__ void __launch_bounds__(kSolveThreads) k_solve_all(StepBuffers b, Step
             fp.cl = it == 0 ? nullptr : b.vel_iter + (2 * (it - 1)) * B;
             fp.ca = it == 0 ? nullptr : b.vel_iter + (2 * (it - 1) + 1) * B;
             fp.gen = gen;
-            if (it == 0) solve_span<true, true>(b, p, cur, A, first, stride, nullptr, nullptr, &fp, D[0]);
-            else solve_span<false, true>(b, p, cur, A, first, stride, nullptr, nullptr, &fp, D[it % 3]);
+            if (it == 0) solve_span<true, true>(b, p, cur, contact_slice(A, parts), nullptr, nullptr, &fp, D[0]);
+            else solve_span<false, true>(b, p, cur, contact_slice(A, parts), nullptr, nullptr, &fp, D[it % 3]);
             int4* dz = reinterpret_cast<int4*>(D[(it + 1) % 3]);   // dead since the last barrier; used next pass
             for (uint64_t i = gtid; i < (6ull * B) / 4; i += stride) dz[i] = make_int4(0, 0, 0, 0);
             if (gtid == 0 && (6ull * B) % 4) {
@@ -1407,8 +1524,8 @@ __global__ void __launch_bounds__(kSolveThreads) k_solve_all(StepBuffers b, Step
         const float4* sa = it == 0 ? b.ang : b.vel_iter + (2 * (it - 1) + 1) * B;
         float4* dl = it + 1 == iterations ? b.lin : b.vel_iter + (2 * it) * B;
         float4* da = it + 1 == iterations ? b.ang : b.vel_iter + (2 * it + 1) * B;
-        if (it == 0) solve_span<true>(b, p, cur, A, first, stride, sl, sa);
-        else solve_span<false>(b, p, cur, A, first, stride, sl, sa);
+        if (it == 0) solve_span<true>(b, p, cur, contact_slice(A, parts), sl, sa);
+        else solve_span<false>(b, p, cur, contact_slice(A, parts), sl, sa);
         grid_barrier(barrier, &b.diag->error_flags, parts);
         apply_span(b, p, first + threadIdx.x, stride, sl, sa, dl, da);
         grid_barrier(barrier, &b.diag->error_flags, parts);
@@ -1505,16 +1622,16 @@ __device__ __forceinline__ f3 contact_velocity_cg(const float4* vl, const float4
 // One pass for candidate `c` (0: impulses in the contact rows, 1: in lam_alt).
 __device__ __forceinline__ void solve_span_res(const StepBuffers& b, const StepParams& p, GpuContact* cur, uint32_t A,
                                                bool warm, uint32_t c, const ResCandidate& v, bool write_res) {
-    const uint32_t stride = gridDim.x * blockDim.x;
     int64_t* deltas = b.deltas64 + 6ull * p.body_count * c;
     double* res2 = b.res2 + (uint64_t)p.pair_capacity * c;
-    for (uint32_t base = blockIdx.x * blockDim.x; base < A; base += stride) {
+    const uint2 sl = contact_slice(A, gridDim.x);
+    for (uint32_t base = sl.x; base < sl.y; base += blockDim.x) {
         const uint32_t t = base + threadIdx.x;
         bool live = false;
         uint32_t a = kInvalid, bb = kInvalid;
         float r = 0.0f;
         int64_t da[6] = {0, 0, 0, 0, 0, 0}, db[6] = {0, 0, 0, 0, 0, 0};
-        if (t < A) {
+        if (t < sl.y) {
             const uint32_t k = __ldcg(b.active + t);
             float4* row = reinterpret_cast<float4*>(cur + k);
             const float4 r0 = __ldcg(row), np = __ldcg(row + 1), aa = __ldcg(row + 2), ab = __ldcg(row + 3);
@@ -1788,7 +1905,7 @@ cudaError_t launch_warm_targets(const StepBuffers& b, int parity, uint32_t A, fl
 template <bool kWarm>
 __global__ void __launch_bounds__(kBlock) k_solve_iter(StepBuffers b, StepParams p, GpuContact* cur) {
     const uint32_t A = b.counts->active;
-    solve_span<kWarm>(b, p, cur, A, blockIdx.x * blockDim.x, gridDim.x * blockDim.x, b.lin, b.ang);
+    solve_span<kWarm>(b, p, cur, contact_slice(A, gridDim.x), b.lin, b.ang);
 }
 
 __global__ void __launch_bounds__(kBlock) k_apply_iter(StepBuffers b, StepParams p) {

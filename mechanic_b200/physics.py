@@ -488,6 +488,10 @@ class GpuPhysics:
     def node_children(self):
         return self.read_buffer(abi.BUF_NODE_CHILDREN, np.uint32, 8).reshape(-1, 2)
 
+    def node_aabbs(self):
+        """(2C - 1, 8) float32: min.xyz, w, max.xyz, 0 per node (internal nodes first, then sorted leaves)."""
+        return self.read_buffer(abi.BUF_NODE_AABBS, np.float32, 32).reshape(-1, 8)
+
     def world_masses(self):
         return self.read_buffer(abi.BUF_WORLD_MASSES, np.float32, 48).reshape(-1, 12)
 

@@ -110,6 +110,43 @@ def test_morton63_mode_bitexact(cuda_lib):
         compare_tick(gpu, orc, tick)
 
 
+def test_node_boxes_are_leaf_range_unions(cuda_lib):
+    """Every LBVH node box equals the min/max over the AABBs of its leaf range
+    (exact: unions are min/max), over ticks with dense and sparse contact."""
+    scene = scenes.stack_grid(14, 9, 14, seed=11)
+    gpu = GpuPhysics(scene, GpuPhysicsConfig(), capacities={"pair_capacity": 1 << 22})
+    for tick in range(1, 7):
+        gpu.dispatch_tick(tick)
+        gpu.wait()
+        if tick not in (1, 3, 6):
+            continue
+        ch = gpu.node_children().astype(np.int64)
+        nodes = gpu.node_aabbs()
+        _, vals = gpu.sorted_entries()
+        ab = gpu.aabbs()
+        C = len(vals)
+        I = C - 1
+        leaf_min, leaf_max = ab[vals, 0:3], ab[vals, 4:7]
+        assert np.array_equal(nodes[I:, 0:3], leaf_min) and np.array_equal(nodes[I:, 4:7], leaf_max)
+        first = np.zeros(I, np.int64)
+        last = np.zeros(I, np.int64)
+        order, stack = [], [0]
+        while stack:
+            x = stack.pop()
+            order.append(x)
+            stack.extend(int(c) for c in ch[x] if c < I)
+        for x in reversed(order):   # children before parents
+            lo = [c - I if c >= I else first[c] for c in ch[x]]
+            hi = [c - I if c >= I else last[c] for c in ch[x]]
+            first[x], last[x] = min(lo), max(hi)
+        for x in range(I):
+            want_min = leaf_min[first[x]:last[x] + 1].min(axis=0)
+            want_max = leaf_max[first[x]:last[x] + 1].max(axis=0)
+            assert np.array_equal(nodes[x, 0:3], want_min), f"tick {tick} node {x} min"
+            assert np.array_equal(nodes[x, 4:7], want_max), f"tick {tick} node {x} max"
+            assert nodes[x, 3:4].view(np.uint32)[0] == last[x]
+
+
 def test_graph_and_direct_launch_agree(cuda_lib):
     scene = scenes.stack_grid(8, 6, 8, seed=1)
     a = GpuPhysics(scene, GpuPhysicsConfig(use_graph=True))
@@ -222,7 +259,7 @@ def test_standalone_sort_matches_stable_sort(cuda_lib):
     import torch
     from mechanic_b200 import ops
     rng = np.random.default_rng(0)
-    for n in (1, 1000, 2048, 2049, 300_001):
+    for n in (1, 1000, 2048, 2049, 8192, 8193, 20_000, 300_001):   # one-CTA sort up to 8192 keys
         keys = rng.integers(0, 1 << 63, n, dtype=np.uint64)
         keys[: n // 3] = keys[0]                       # many ties
         vals = np.arange(n, dtype=np.uint32)
@@ -231,6 +268,37 @@ def test_standalone_sort_matches_stable_sort(cuda_lib):
         order = np.argsort(keys, kind="stable")
         assert np.array_equal(k_out.cpu().numpy().view(np.uint64), keys[order])
         assert np.array_equal(v_out.cpu().numpy().view(np.uint32), vals[order])
+
+
+@pytest.mark.parametrize("items", [2, 4, 6, 8, 11, 16])
+def test_standalone_sort_every_tile_shape(cuda_lib, items):
+    """Each onesweep tile shape (keys per thread) gives the stable order."""
+    import torch
+    from mechanic_b200 import ops, physics
+    rng = np.random.default_rng(items)
+    n = 123_457
+    keys = rng.integers(0, 1 << 48, n, dtype=np.uint64)
+    keys[::7] = keys[3]                                  # ties across tiles
+    vals = np.arange(n, dtype=np.uint32)
+    prev = physics.set_tuning(physics.TUNE_SORT_ITEMS, items)
+    try:
+        k_out, v_out = ops.sort_keys(torch.from_numpy(keys.view(np.int64)).cuda(),
+                                     torch.from_numpy(vals.view(np.int32)).cuda(), key_bits=48)
+        torch.cuda.synchronize()
+    finally:
+        physics.set_tuning(physics.TUNE_SORT_ITEMS, max(prev, 0))
+    order = np.argsort(keys, kind="stable")
+    assert np.array_equal(k_out.cpu().numpy().view(np.uint64), keys[order])
+    assert np.array_equal(v_out.cpu().numpy().view(np.uint32), vals[order])
+
+
+def test_grid_above_one_sort_tile_bitexact(cuda_lib):
+    """16,000 colliders: the collider sort takes the onesweep passes, not the one-CTA sort."""
+    scene = scenes.stack_grid(20, 10, 20, seed=13)
+    assert scene.collider_count > 8192
+    gpu, orc = make_pair(scene)
+    for tick in range(1, 4):
+        compare_tick(gpu, orc, tick)
 
 
 def test_standalone_sat_matches_oracle(cuda_lib):
