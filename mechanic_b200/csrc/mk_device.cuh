@@ -167,8 +167,16 @@ __device__ __forceinline__ uint32_t ld_acquire_u32(const uint32_t* p) {
 __device__ __forceinline__ void st_release_u32(uint32_t* p, uint32_t v) {
     asm volatile("st.release.gpu.global.u32 [%0], %1;" :: "l"(p), "r"(v) : "memory");
 }
-// Coherent GPU-scope store / load with no ordering (a word written and read for
-// its own value only: no fence, unlike a release store).
+// Coherent GPU-scope stores / loads with no ordering (a word written and read
+// for its own value only: no fence, unlike a release store).
+__device__ __forceinline__ void st_relaxed_u64(uint64_t* p, uint64_t v) {
+    asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" :: "l"(p), "l"(v) : "memory");
+}
+__device__ __forceinline__ uint64_t ld_relaxed_u64(const uint64_t* p) {
+    uint64_t v;
+    asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
 __device__ __forceinline__ void st_relaxed_u32(uint32_t* p, uint32_t v) {
     asm volatile("st.relaxed.gpu.global.u32 [%0], %1;" :: "l"(p), "r"(v) : "memory");
 }
@@ -188,22 +196,24 @@ __device__ __forceinline__ uint32_t atomic_add_acq_rel(uint32_t* p, uint32_t v) 
 }
 
 // Called by warp 0 of a block (all 32 lanes).  Returns the exclusive prefix
-// of `tile` and publishes its inclusive prefix.
+// of `tile` and publishes its inclusive prefix.  The words are stored and read
+// relaxed: each carries its own status and count, nothing else is published
+// through them, and a release store's fence costs an L2 round trip per tile.
 __device__ __forceinline__ uint64_t tile_lookback(uint64_t* states, uint32_t tile, uint64_t aggregate,
                                                   uint32_t* error_flags) {
     const uint32_t lane = lane_id();
     if (tile == 0) {
-        if (lane == 0) st_release_u64(states, kStatusInclusive | aggregate);
+        if (lane == 0) st_relaxed_u64(states, kStatusInclusive | aggregate);
         return 0;
     }
-    if (lane == 0) st_release_u64(states + tile, kStatusAggregate | aggregate);
+    if (lane == 0) st_relaxed_u64(states + tile, kStatusAggregate | aggregate);
     uint64_t exclusive = 0;
     int64_t base = (int64_t)tile - 1;
     uint32_t spins = 0;
     bool timed_out = false;
     while (base >= 0) {
         int64_t idx = base - (int64_t)lane;
-        uint64_t v = idx >= 0 ? ld_acquire_u64(states + idx) : kStatusInclusive;
+        uint64_t v = idx >= 0 ? ld_relaxed_u64(states + idx) : kStatusInclusive;
         uint32_t ready = __ballot_sync(0xffffffffu, (v >> 62) != 0);
         if (ready != 0xffffffffu) {
             if (++spins > kSpinLimit) { timed_out = true; v = (v >> 62) ? v : kStatusInclusive; }
@@ -220,7 +230,7 @@ __device__ __forceinline__ uint64_t tile_lookback(uint64_t* states, uint32_t til
         spins = 0;
     }
     if (timed_out && lane == 0) atomicOr(error_flags, MK_DEVICE_WAIT_TIMEOUT_FLAG);
-    if (lane == 0) st_release_u64(states + tile, kStatusInclusive | (exclusive + aggregate));
+    if (lane == 0) st_relaxed_u64(states + tile, kStatusInclusive | (exclusive + aggregate));
     return exclusive;
 }
 

@@ -430,7 +430,8 @@ cudaError_t launch_sort(const uint64_t* keys_in, const uint32_t* vals_in, uint64
     if (scratch_bytes < sort_scratch_bytes(n, key_bits, values)) return cudaErrorInvalidValue;
     // at most kSmallSortKeys keys: one CTA sorts them in shared memory; with a
     // device count it runs first and the histogram and passes skip small counts
-    k_radix_small<<<1, kSmallThreads, kSmallSmem, stream>>>(keys_in, vals_in, keys_out, vals_out, n_dev, n, passes);
+    if (n_dev || n <= kSmallSortKeys)
+        k_radix_small<<<1, kSmallThreads, kSmallSmem, stream>>>(keys_in, vals_in, keys_out, vals_out, n_dev, n, passes);
     if (!n_dev && n <= kSmallSortKeys) return cudaGetLastError();
     const uint32_t small_n = n_dev ? kSmallSortKeys : 0u;
     const uint32_t items = valid_sort_items(items_override) ? items_override : sort_items_for(n, sm_count);
