@@ -85,12 +85,14 @@ __device__ __forceinline__ void warp_rank(const uint32_t (&dig)[kItems], uint32_
     }
 }
 
-// Sorts up to kSmallSortKeys keys in one 1024-thread CTA, every pass in shared
-// memory (no look-back, no histogram kernel: the tile's digit counts are the
-// whole sort's).  Light ticks sort a few thousand pair keys: one launch instead
-// of a histogram and one onesweep launch per digit.  With a device count above
-// kSmallSortKeys it returns at once and the onesweep passes sort.
-constexpr uint32_t kSmallThreads = 1024, kSmallItems = 8;
+// Sorts up to kSmallSortKeys keys in one CTA, every pass in shared memory (no
+// look-back, no histogram kernel: the tile's digit counts are the whole
+// sort's); only the warps that hold keys rank.  Light ticks sort at most a few
+// thousand pair keys: one launch instead of a histogram and one onesweep launch
+// per digit.  With a device count above kSmallSortKeys it returns at once and
+// the onesweep passes sort (one SM ranking 8,192 keys per pass was slower than
+// four tiles on four SMs).
+constexpr uint32_t kSmallThreads = 512, kSmallItems = 8;
 constexpr uint32_t kSmallSortKeys = kSmallThreads * kSmallItems;
 constexpr size_t kSmallSmem = (size_t)kSmallSortKeys * 12 + (kSmallThreads / 32) * kRadixBins * 4;
 
@@ -108,6 +110,7 @@ k_radix_small(const uint64_t* __restrict__ keys_in, const uint32_t* __restrict__
     __shared__ uint32_t s_scan[33];
     const uint32_t lane = lane_id(), w = warp_id();
     const uint32_t d = threadIdx.x;   // the digit of threads below kRadixBins
+    const uint32_t warps = (n + 32 * kSmallItems - 1) / (32 * kSmallItems);   // warps holding keys
     uint64_t k[kSmallItems];
     uint32_t v[kSmallItems], dig[kSmallItems], rank[kSmallItems];
 #pragma unroll
@@ -118,20 +121,18 @@ k_radix_small(const uint64_t* __restrict__ keys_in, const uint32_t* __restrict__
     }
     for (uint32_t pass = 0; pass < passes; ++pass) {
         const uint32_t shift = 8 * pass;
-        for (uint32_t q = threadIdx.x; q < (kSmallThreads / 32) * kRadixBins; q += kSmallThreads)
-            (&s_warp[0][0])[q] = 0;
+        for (uint32_t q = threadIdx.x; q < warps * kRadixBins; q += kSmallThreads) (&s_warp[0][0])[q] = 0;
         __syncthreads();
 #pragma unroll
         for (uint32_t i = 0; i < kSmallItems; ++i) {
             const uint32_t idx = w * 32 * kSmallItems + i * 32 + lane;
             dig[i] = idx < n ? (uint32_t)((k[i] >> shift) & 0xffu) : kRadixBins;
         }
-        warp_rank<kSmallItems>(dig, rank, s_warp[w], lane);
+        if (w < warps) warp_rank<kSmallItems>(dig, rank, s_warp[w], lane);
         __syncthreads();
         uint32_t count = 0;
         if (d < kRadixBins) {
-#pragma unroll 8
-            for (uint32_t ww = 0; ww < kSmallThreads / 32; ++ww) {
+            for (uint32_t ww = 0; ww < warps; ++ww) {
                 const uint32_t c = s_warp[ww][d];
                 s_warp[ww][d] = count;
                 count += c;

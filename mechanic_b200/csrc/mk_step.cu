@@ -285,13 +285,8 @@ __global__ void __launch_bounds__(kBlock) k_karras(StepBuffers b, StepParams p) 
     b.node_ranges[i] = make_uint2((uint32_t)first, (uint32_t)last);
 }
 
-// lbvh.wgsl:280-319: leaf boxes in sorted order, then a bottom-up climb where
-// the second arrival at a node writes the union.  Besides the union (kept for
-// the climb, min.w = last sorted leaf position below the node) each internal
-// node gets a 64-byte traversal record with both children's boxes:
-// {lmin, left code}, {lmax, left last}, {rmin, right code}, {rmax, right last}.
-// A child code is the internal node index, or 0x80000000 | collider index
-// for a leaf; "last" is the largest sorted leaf position below the child.
+// Traversal record codes: an internal node index, or kLeafCode | collider index
+// for a leaf.
 constexpr uint32_t kLeafCode = 0x80000000u;
 
 // Parallel refit.  An internal node covers a contiguous range of sorted

@@ -259,7 +259,7 @@ def test_standalone_sort_matches_stable_sort(cuda_lib):
     import torch
     from mechanic_b200 import ops
     rng = np.random.default_rng(0)
-    for n in (1, 1000, 2048, 2049, 8192, 8193, 20_000, 300_001):   # one-CTA sort up to 8192 keys
+    for n in (1, 1000, 2048, 2049, 4096, 4097, 20_000, 300_001):   # one-CTA sort up to 4096 keys
         keys = rng.integers(0, 1 << 63, n, dtype=np.uint64)
         keys[: n // 3] = keys[0]                       # many ties
         vals = np.arange(n, dtype=np.uint32)
@@ -295,7 +295,7 @@ def test_standalone_sort_every_tile_shape(cuda_lib, items):
 def test_grid_above_one_sort_tile_bitexact(cuda_lib):
     """16,000 colliders: the collider sort takes the onesweep passes, not the one-CTA sort."""
     scene = scenes.stack_grid(20, 10, 20, seed=13)
-    assert scene.collider_count > 8192
+    assert scene.collider_count > 4096
     gpu, orc = make_pair(scene)
     for tick in range(1, 4):
         compare_tick(gpu, orc, tick)
