@@ -421,8 +421,12 @@ MK_API int mk_wait(MkHandle* handle, uint64_t submission_index);
 MK_API int mk_read_last_tick(MkHandle* handle, MkTickReadback* out);
 
 /* GpuPhysics::read_snapshot_transforms (device.rs:1534-1570); `out` holds
- * `capacity` rows of caller-owned host memory.  MK_ERR_INVALID_SNAPSHOT_SLOT
- * for slot >= 3. */
+ * `capacity` rows of caller-owned host memory (pinned memory copies fastest).
+ * MK_ERR_INVALID_SNAPSHOT_SLOT for slot >= 3.  Reads the slot as the last
+ * dispatched tick that wrote it left it, and waits for that tick and the copy
+ * only: ticks dispatched after it keep running (the copy runs on the handle's
+ * copy stream), so a caller that dispatches tick k + 1 before reading tick k's
+ * slot overlaps the two. */
 MK_API int mk_read_snapshot(MkHandle* handle, uint8_t slot, GpuTransform* out,
                      uint32_t capacity, MkError* err);
 

@@ -73,6 +73,15 @@ struct MkHandle {
     void* arena = nullptr;
     size_t arena_bytes = 0;
     float4* staging = nullptr;          // 2 x float4 per body (interleaved transforms)
+    float4* snap_staging = nullptr;     // the same for snapshot reads on copy_stream
+    // Snapshot reads run on their own stream: a read of slot s waits for the
+    // tick that last wrote s (slot_written), and the next tick that writes s
+    // waits for the read (slot_read), so reading tick k's slot overlaps the
+    // ticks dispatched after it.
+    cudaStream_t copy_stream = nullptr;
+    cudaEvent_t slot_written[3] = {};
+    cudaEvent_t slot_read[3] = {};
+    bool slot_read_pending[3] = {};
     // host
     mk::DevTick* h_tick = nullptr;      // pinned ring
     GpuDiagnostics* h_diag = nullptr;   // pinned, written at the end of every tick
@@ -188,6 +197,7 @@ uint64_t carve(MkHandle* h, char* base) {
     b.sort_scratch_bytes = mk::sort_scratch_bytes(C, 63);
     b.sort_scratch = c.take<char>(b.sort_scratch_bytes);
     h->staging = c.take<float4>(2ull * B);
+    h->snap_staging = c.take<float4>(2ull * B);
     if (h->residual) {
         b.deltas64 = c.take<int64_t>(12ull * B);
         b.res2 = c.take<double>(2 * P);
@@ -356,8 +366,14 @@ void destroy_handle(MkHandle* h) {
     if (!h) return;
     DeviceGuard g(h->device);
     if (h->stream) cudaStreamSynchronize(h->stream);
+    if (h->copy_stream) cudaStreamSynchronize(h->copy_stream);
     for (auto& gx : h->graph)
         if (gx) cudaGraphExecDestroy(gx);
+    for (uint32_t i = 0; i < 3; ++i) {
+        if (h->slot_written[i]) cudaEventDestroy(h->slot_written[i]);
+        if (h->slot_read[i]) cudaEventDestroy(h->slot_read[i]);
+    }
+    if (h->copy_stream) cudaStreamDestroy(h->copy_stream);
     for (auto& e : h->tick_done)
         if (e) cudaEventDestroy(e);
     for (auto& e : h->stage)
@@ -644,6 +660,11 @@ int create_impl(const MkCreation* cr, const MkConfig* config, const MkCapacities
     for (uint32_t i = 0; ok && i < kTickRing; ++i)
         ok = check(cudaEventCreateWithFlags(&h->tick_done[i], cudaEventDisableTiming), err, "event");
     for (uint32_t i = 0; ok && i < kStageEvents; ++i) ok = check(cudaEventCreate(&h->stage[i]), err, "event");
+    ok = ok && check(cudaStreamCreateWithFlags(&h->copy_stream, cudaStreamNonBlocking), err, "copy stream");
+    for (uint32_t i = 0; ok && i < 3; ++i) {
+        ok = check(cudaEventCreateWithFlags(&h->slot_written[i], cudaEventDisableTiming), err, "event");
+        ok = ok && check(cudaEventCreateWithFlags(&h->slot_read[i], cudaEventDisableTiming), err, "event");
+    }
     if (!ok) {
         destroy_handle(h);
         return MK_ERR_DEVICE_FAILURE;
@@ -796,13 +817,20 @@ int mk_dispatch_tick(MkHandle* h, uint64_t tick_index, MkSubmission* out) {
     t.tick_index = (uint32_t)tick_index;    // wrapping_u32 (device.rs:868)
     t.snapshot_slot = (uint32_t)(tick_index % 3);
     t.generation = (uint32_t)sub;
-    cudaError_t e = cudaMemcpyAsync(h->buf.tick, &t, sizeof(t), cudaMemcpyHostToDevice, h->stream);
+    const uint32_t snap = t.snapshot_slot;
+    cudaError_t e = cudaSuccess;
+    if (h->slot_read_pending[snap]) {   // a read of this snapshot slot may still be copying it
+        e = cudaStreamWaitEvent(h->stream, h->slot_read[snap], 0);
+        h->slot_read_pending[snap] = false;
+    }
+    if (e == cudaSuccess) e = cudaMemcpyAsync(h->buf.tick, &t, sizeof(t), cudaMemcpyHostToDevice, h->stream);
     const int parity = h->parity;
     if (e == cudaSuccess) {
         if (h->graph[parity]) e = cudaGraphLaunch(h->graph[parity], h->stream);
         else e = enqueue_tick(h, parity, false);
     }
     if (e == cudaSuccess) e = cudaEventRecord(h->tick_done[slot], h->stream);
+    if (e == cudaSuccess) e = cudaEventRecord(h->slot_written[snap], h->stream);
     if (e != cudaSuccess) {
         set_error(nullptr, MK_ERR_DEVICE_FAILURE, "dispatch_tick: %s", cudaGetErrorString(e));
         return MK_ERR_DEVICE_FAILURE;
@@ -973,11 +1001,21 @@ int mk_read_snapshot(MkHandle* h, uint8_t slot, GpuTransform* out, uint32_t capa
         return MK_ERR_INVALID_ARGUMENT;
     }
     DeviceGuard guard(h->device);
-    cudaStream_t s = h->stream;
-    k_interleave<<<(h->B + 255) / 256, 256, 0, s>>>(h->buf.snap_pos + (size_t)slot * h->B,
-                                                     h->buf.snap_rot + (size_t)slot * h->B, h->staging, h->B);
-    cudaError_t e = cudaMemcpyAsync(out, h->staging, sizeof(GpuTransform) * h->B, cudaMemcpyDeviceToHost, s);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    // on the copy stream, after the tick that last wrote this slot only: ticks
+    // dispatched later keep running while the slot is copied
+    cudaStream_t s = h->copy_stream;
+    cudaError_t e = cudaStreamWaitEvent(s, h->slot_written[slot], 0);
+    if (e == cudaSuccess) {
+        k_interleave<<<(h->B + 255) / 256, 256, 0, s>>>(h->buf.snap_pos + (size_t)slot * h->B,
+                                                         h->buf.snap_rot + (size_t)slot * h->B, h->snap_staging,
+                                                         h->B);
+        e = cudaMemcpyAsync(out, h->snap_staging, sizeof(GpuTransform) * h->B, cudaMemcpyDeviceToHost, s);
+    }
+    if (e == cudaSuccess) e = cudaEventRecord(h->slot_read[slot], s);
+    if (e == cudaSuccess) {
+        h->slot_read_pending[slot] = true;
+        e = cudaEventSynchronize(h->slot_read[slot]);
+    }
     if (!check(e, err, "read_snapshot")) return MK_ERR_DEVICE_FAILURE;
     return MK_OK;
 }

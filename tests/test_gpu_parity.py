@@ -147,6 +147,35 @@ def test_node_boxes_are_leaf_range_unions(cuda_lib):
             assert nodes[x, 3:4].view(np.uint32)[0] == last[x]
 
 
+def test_snapshot_reads_overlap_later_ticks(cuda_lib):
+    """A snapshot read waits for the tick that last wrote its slot, not for ticks dispatched
+    after it, and a tick that rewrites a slot waits for a read of it: reading tick k's slot
+    after dispatching tick k + 1 gives the rows a fully synchronised read gives."""
+    scene = scenes.stack_grid(10, 6, 10, seed=17)
+    ref = GpuPhysics(scene, GpuPhysicsConfig())
+    want = []
+    for tick in range(1, 8):
+        sub = ref.dispatch_tick(tick)
+        ref.wait()
+        want.append(ref.read_snapshot_transforms(sub.snapshot_slot).copy())
+    gpu = GpuPhysics(scene, GpuPhysicsConfig())
+    got, prev = [], None
+    for tick in range(1, 8):
+        sub = gpu.dispatch_tick(tick)
+        if prev is not None:
+            got.append(gpu.read_snapshot_transforms(prev.snapshot_slot).copy())
+        prev = sub
+    got.append(gpu.read_snapshot_transforms(prev.snapshot_slot).copy())
+    for k, (a, b) in enumerate(zip(got, want)):
+        assert_bitwise(a, b, f"snapshot of tick {k + 1}")
+    # a slot read after later ticks rewrote it holds the newest writer's rows
+    for tick in range(8, 11):
+        gpu.dispatch_tick(tick)
+        ref.dispatch_tick(tick)
+    ref.wait()
+    assert_bitwise(gpu.read_snapshot_transforms(10 % 3), ref.read_snapshot_transforms(10 % 3), "slot of tick 10")
+
+
 def test_graph_and_direct_launch_agree(cuda_lib):
     scene = scenes.stack_grid(8, 6, 8, seed=1)
     a = GpuPhysics(scene, GpuPhysicsConfig(use_graph=True))
