@@ -60,8 +60,9 @@ BYTES_SOLVE_PER_CONTACT_ITER = 284     # contact 64 + idx 4 + 2 x (v 16 + w 16 +
 BYTES_APPLY_PER_BODY_ITER = 112        # deltas 24 + velocities 32 read, velocities 32 + deltas 24 written
 BYTES_PREPARE_PER_CONTACT = 340        # contact 64 + 2 x (v/w 32 + world mass 48) + manifold 96, 16 + 48 + 4 written
 # broadphase per collider: AABB + Morton 140 (collider 64 + pose 32 read, AABB 32 + key/value 12 written),
-# onesweep sort 204 (2 x 12 x 8 digit passes + 12), Karras 24, refit 96 + 32, traversal 32
-BYTES_BROADPHASE_PER_COLLIDER = 140 + 204 + 24 + 96 + 32 + 32
+# onesweep sort 156 (2 x 12 x 6 digit passes over the 48-bit keys + 12), Karras 24, refit 96 + 32,
+# traversal 32
+BYTES_BROADPHASE_PER_COLLIDER = 140 + 156 + 24 + 96 + 32 + 32
 # per candidate pair: traversal output 8 + pair-key sort (5 digit passes x 16 + 8)
 BYTES_BROADPHASE_PER_PAIR = 8 + 88
 
@@ -363,9 +364,11 @@ def main():
                 counts.append((rb.pair_count, rb.contact_count, rb.active_contact_count))
                 broad_bytes += (BYTES_BROADPHASE_PER_COLLIDER * scene.collider_count
                                 + BYTES_BROADPHASE_PER_PAIR * rb.pair_count)
+                # the apply touches at most the active contacts' bodies (2 per contact): light
+                # ticks apply only those, so counting every body would overstate the traffic
+                applied = min(scene.body_count, 2 * rb.active_contact_count)
                 solve_bytes += (8 * (BYTES_SOLVE_PER_CONTACT_ITER * rb.active_contact_count
-                                     + (BYTES_APPLY_PER_BODY_ITER * scene.body_count
-                                        if rb.active_contact_count else 0))
+                                     + BYTES_APPLY_PER_BODY_ITER * applied)
                                 + BYTES_PREPARE_PER_CONTACT * rb.contact_count)
         torch.cuda.synchronize()
     per_tick = [s.elapsed_time(e) for s, e in zip(starts, ends)]
