@@ -831,7 +831,7 @@ __device__ __forceinline__ uint32_t take_tile(uint32_t* ticket, uint32_t* s_tile
 }
 
 // collision.wgsl:570-620 (narrowphase with the optional self-collision filter).
-__global__ void __launch_bounds__(kBlock) k_narrowphase(StepBuffers b, StepParams p, AppendSite site,
+__global__ void __launch_bounds__(kBlock, 3) k_narrowphase(StepBuffers b, StepParams p, AppendSite site,
                                                         GpuContact* out, uint64_t* out_keys, uint32_t* out_feat) {
     __shared__ uint32_t s_scan[33];
     __shared__ uint32_t s_tile;
