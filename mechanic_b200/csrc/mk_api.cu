@@ -164,6 +164,8 @@ uint64_t carve(MkHandle* h, char* base) {
     b.leaf_scan = c.take<float4>(4ull * C);
     b.chunk_scan = c.take<float4>(6ull * ((C + 31) / 32));
     b.chunk_table = c.take<float4>(8ull * ((C + 31) / 32));
+    b.ground_mask = c.take<uint32_t>((C + 31) / 32);
+    b.ground_tile_count = c.take<uint32_t>((C + 1023) / 1024);
     {
         const uint64_t ns = (C + 1023) / 1024;
         uint64_t levels = 1;
@@ -243,6 +245,7 @@ cudaError_t enqueue_tick(MkHandle* h, int parity, bool capturing) {
             z.add(b.deltas, sizeof(int32_t) * 6ull * std::max(h->B, 1u));
             z.add(b.scene_bounds, 8 * sizeof(uint32_t));
             z.add(b.grid_barrier, 64 * sizeof(uint32_t));
+            z.add(b.ground_tile_count, sizeof(uint32_t) * ((h->C + 1023) / 1024));
             z.add(b.lookback, sizeof(uint64_t) * 4 * b.lookback_words);
             void* r = nullptr;
             uint64_t rb = 0;
@@ -253,6 +256,7 @@ cudaError_t enqueue_tick(MkHandle* h, int parity, bool capturing) {
             z.add(r, rb);
         }
         if (h->mechanism_active) z.add(h->mech.deltas, 24ull * std::max(h->B, 1u));
+        if (z.dropped) return cudaErrorInvalidValue;   // more per-tick clears than the list holds
         cudaError_t ez = mk::launch_tick_reset(z, h->sm_count, s);
         if (ez != cudaSuccess) return ez;
     }

@@ -127,6 +127,8 @@ struct StepBuffers {
     float4* chunk_scan;          // 6 per chunk: total, prefix and suffix unions within its 1024-leaf super-chunk
     float4* super_table;         // 2 x super-chunks x levels: sparse table of super-chunk totals
     float4* chunk_table;         // 2 x chunks x 4: sparse table levels 1-4 of chunk totals within a super-chunk
+    uint32_t* ground_mask;       // a bit per collider: touches the ground plane this tick
+    uint32_t* ground_tile_count; // touching colliders per 1,024-collider tile (zeroed per tick)
     float4* node_aabbs;          // 2 x float4 per node (union boxes)
     float4* node_records;        // 8 x float4 per internal node (4-wide record of its grandchildren)
     const uint2* suppressed;
@@ -179,12 +181,17 @@ struct StepLaunch {
 
 // Device regions to clear at the start of a tick (16-byte aligned, sizes in 16-byte units).
 struct ZeroList {
-    static constexpr uint32_t kMax = 12;
+    static constexpr uint32_t kMax = 16;   // a tick adds at most 12 regions
     uint4* ptr[kMax];
     uint64_t n16[kMax];
     uint32_t count;
+    uint32_t dropped;                      // regions that did not fit (the tick refuses to run)
     void add(void* p, uint64_t bytes) {
-        if (!p || bytes == 0 || count >= kMax) return;
+        if (!p || bytes == 0) return;
+        if (count >= kMax) {
+            ++dropped;
+            return;
+        }
         ptr[count] = reinterpret_cast<uint4*>(p);
         n16[count] = (bytes + 15) / 16;   // the arena pads every buffer to 256 bytes
         ++count;

@@ -165,6 +165,13 @@ __device__ __forceinline__ void key_frame(const uint32_t* bw, float qmax, f3& lo
     scale = extent > 0.0f ? qmax / extent : 1.0f;
 }
 
+constexpr uint32_t kGroundTile = 1024;   // colliders per ground-contact tile (32 mask words)
+
+// collision.wgsl:622-664 support point of collider i against the ground plane
+// (defined with the ground contacts below); true when it touches.
+__device__ __forceinline__ bool ground_point(const StepBuffers& b, uint32_t i, f3& sp, uint32_t& body,
+                                             uint32_t& role);
+
 // lbvh.wgsl:108-130 plus the world box row the narrowphase reads:
 // box r0 = {center, half.x}, r1 = world rotation, r2 = {half.y, half.z, body, role}.
 __global__ void __launch_bounds__(kBlock) k_collider_bounds(StepBuffers b, StepParams p, uint32_t morton_mode) {
@@ -193,6 +200,21 @@ __global__ void __launch_bounds__(kBlock) k_collider_bounds(StepBuffers b, StepP
         if (morton_mode == MK_MORTON_REFERENCE_30)
             b.keys[i] = compose_key(morton_mode, p.scene_bits, p.scene_bits ? b.collider_scene[i] : 0u,
                                     morton30(center));
+    }
+    {   // ground test of each collider from its fresh box: a bit per collider and a
+        // count per ground tile, so the ground contacts need neither a second
+        // pass over every box nor an ordered-append look-back
+        bool touch = false;
+        if (valid) {
+            f3 sp;
+            uint32_t body, role;
+            touch = ground_point(b, i, sp, body, role);
+        }
+        const uint32_t m = __ballot_sync(0xffffffffu, touch);
+        if (lane_id() == 0 && (uint64_t)i < p.collider_count) {
+            b.ground_mask[i >> 5] = m;
+            if (m) atomicAdd(b.ground_tile_count + i / kGroundTile, (uint32_t)__popc(m));
+        }
     }
     if (morton_mode == MK_MORTON_REFERENCE_30) return;
     // the tick's bounds of the finite collider centres: warp then block reductions of
@@ -943,47 +965,35 @@ __device__ __forceinline__ bool ground_point(const StepBuffers& b, uint32_t i, f
     return !(sp.y > 1.0e-5f);
 }
 
-// Ground contacts in collider order after the narrowphase's.  Each thread
-// takes kGroundItems consecutive colliders, so a tile covers
-// kBlock x kGroundItems of them and the ordered append needs a quarter of the
-// look-back steps (few colliders touch the ground; 16 per thread measured
-// twice as slow).
-constexpr uint32_t kGroundItems = 4;
-__global__ void __launch_bounds__(kBlock) k_ground(StepBuffers b, StepParams p, AppendSite site, GpuContact* out,
-                                                   uint64_t* out_keys, uint32_t* out_feat) {
+// Ground contacts in collider order after the narrowphase's.  k_collider_bounds
+// left a bit per collider and a count per tile of kGroundTile colliders, so a
+// tile's output offset is the sum of the earlier tiles' counts (no look-back
+// chain) and only the touching colliders' boxes are read again.  Each thread
+// takes kGroundItems consecutive colliders of its tile.
+constexpr uint32_t kGroundItems = kGroundTile / kBlock;
+__global__ void __launch_bounds__(kBlock) k_ground(StepBuffers b, StepParams p, GpuContact* out, uint64_t* out_keys,
+                                                   uint32_t* out_feat) {
     __shared__ uint32_t s_scan[33];
-    __shared__ uint32_t s_tile;
-    __shared__ uint64_t s_prefix;
     const uint32_t n = p.collider_count;
-    constexpr uint32_t kTileItems = kBlock * kGroundItems;
-    const uint32_t tiles = (n + kTileItems - 1) / kTileItems;
+    const uint32_t tiles = (n + kGroundTile - 1) / kGroundTile;
     const uint32_t narrow = b.counts->narrow;
     const uint32_t requested_narrow = b.counts->requested_contacts;
-    for (;;) {
-        const uint32_t tile = take_tile(site.ticket, &s_tile);
-        if (tile >= tiles) break;
-        const uint32_t first = tile * kTileItems + threadIdx.x * kGroundItems;
-        uint32_t mask = 0;
-        for (uint32_t k = 0; k < kGroundItems; ++k) {
-            f3 sp;
-            uint32_t body, role;
-            if (first + k < n && ground_point(b, first + k, sp, body, role)) mask |= 1u << k;
-        }
+    for (uint32_t tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
+        uint32_t part = 0;
+        for (uint32_t q = threadIdx.x; q < tile; q += blockDim.x) part += __ldg(b.ground_tile_count + q);
+        uint32_t pre;
+        block_exclusive_scan(part, s_scan, &pre);   // pre = touching colliders of the tiles before this one
+        const uint32_t first = tile * kGroundTile + threadIdx.x * kGroundItems;   // 4-aligned: one mask word
+        const uint32_t mask = first < n ? (__ldg(b.ground_mask + (first >> 5)) >> (first & 31u)) & 0xfu : 0u;
         uint32_t total;
         const uint32_t ex = block_exclusive_scan((uint32_t)__popc(mask), s_scan, &total);
-        if (warp_id() == 0) {
-            uint64_t pre = tile_lookback(site.states, tile, total, &b.diag->error_flags);
-            if (lane_id() == 0) s_prefix = pre;
-        }
-        __syncthreads();
-        const uint64_t pre = s_prefix;
         uint32_t q = 0;
         for (uint32_t k = 0; k < kGroundItems; ++k) {
             if (!((mask >> k) & 1u)) continue;
             const uint32_t i = first + k;
             f3 sp;
             uint32_t body, role;
-            ground_point(b, i, sp, body, role);   // recomputed: identical arithmetic, fewer live registers
+            ground_point(b, i, sp, body, role);
             const uint64_t o = (uint64_t)narrow + pre + ex + q++;
             if (o < p.pair_capacity) {
                 store_contact(out + o, body, kInvalid, i, kInvalid, make_float4(0.0f, -1.0f, 0.0f, mxf(-sp.y, 0.0f)),
@@ -2085,10 +2095,9 @@ cudaError_t launch_narrowphase(const StepBuffers& b, const StepParams& p, const 
                                cudaStream_t s) {
     const uint32_t grid = (uint32_t)l.sm_count * (l.append_ctas ? l.append_ctas : 8u);
     AppendSite narrow{b.lookback + 1 * b.lookback_words, b.tickets + 1};
-    AppendSite ground{b.lookback + 2 * b.lookback_words, b.tickets + 2};
     k_narrowphase<<<grid, kBlock, 0, s>>>(b, p, narrow, b.contacts[parity], b.contact_keys[parity], b.features[parity]);
-    k_ground<<<std::min<uint32_t>(grid, blocks_for(p.collider_count, kBlock * kGroundItems) + 1), kBlock, 0, s>>>(
-        b, p, ground, b.contacts[parity], b.contact_keys[parity], b.features[parity]);
+    k_ground<<<std::max<uint32_t>(1u, blocks_for(p.collider_count, kGroundTile)), kBlock, 0, s>>>(
+        b, p, b.contacts[parity], b.contact_keys[parity], b.features[parity]);
     return cudaGetLastError();
 }
 
