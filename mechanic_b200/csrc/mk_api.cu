@@ -164,6 +164,7 @@ uint64_t carve(MkHandle* h, char* base) {
     b.leaf_scan = c.take<float4>(4ull * C);
     b.chunk_scan = c.take<float4>(6ull * ((C + 31) / 32));
     b.chunk_table = c.take<float4>(8ull * ((C + 31) / 32));
+    b.contact_index = c.take<uint2>(4ull * C);
     b.ground_mask = c.take<uint32_t>((C + 31) / 32);
     b.ground_tile_count = c.take<uint32_t>((C + 1023) / 1024);
     {
@@ -1338,6 +1339,7 @@ int mk_load_state(MkHandle* h, const MkHostState* st, MkError* err) {
         counts.prev_contacts = n;
         counts.prev_tick = (uint32_t)st->manifold_tick;
         counts.prev_valid = st->manifold_contacts ? 1u : 0u;
+        counts.prev_indexed = 0u;   // a loaded list has no run index: prepare searches it
         if (e == cudaSuccess) e = cudaMemcpy(h->buf.counts, &counts, sizeof(counts), cudaMemcpyHostToDevice);
     }
     return check(e, err, "load_state") ? MK_OK : MK_ERR_DEVICE_FAILURE;

@@ -39,7 +39,8 @@ struct DevCounts {
     uint32_t prev_contacts;    // previous tick: all contacts
     uint32_t prev_tick;        // previous tick index
     uint32_t prev_valid;       // 1 when the previous list may be matched
-    uint32_t pad[4];
+    uint32_t prev_indexed;     // 1 when the previous tick's prepare wrote its run index
+    uint32_t pad[3];
 };
 constexpr uint32_t kCountResetBytes = 8 * sizeof(uint32_t);
 
@@ -127,6 +128,7 @@ struct StepBuffers {
     float4* chunk_scan;          // 6 per chunk: total, prefix and suffix unions within its 1024-leaf super-chunk
     float4* super_table;         // 2 x super-chunks x levels: sparse table of super-chunk totals
     float4* chunk_table;         // 2 x chunks x 4: sparse table levels 1-4 of chunk totals within a super-chunk
+    uint2* contact_index;        // [parity][narrow, ground][collider]: {tick, first row} of the collider's run
     uint32_t* ground_mask;       // a bit per collider: touches the ground plane this tick
     uint32_t* ground_tile_count; // touching colliders per 1,024-collider tile (zeroed per tick)
     float4* node_aabbs;          // 2 x float4 per node (union boxes)

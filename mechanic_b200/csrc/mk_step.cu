@@ -1049,12 +1049,24 @@ __global__ void __launch_bounds__(kBlock) k_prepare(StepBuffers b, StepParams p,
     const uint32_t tick = b.tick->tick_index;
     const bool prev_ok = b.counts->prev_valid != 0u && b.counts->prev_tick == tick - 1u;
     const uint32_t prev_narrow = b.counts->prev_narrow, prev_all = b.counts->prev_contacts;
+    // run index: [parity][0 narrow, 1 ground][collider] = {tick, first row of the collider's rows}
+    const uint64_t C = p.collider_count;
+    uint2* index_cur = b.contact_index + 2ull * C * (tick & 1u);
+    const uint2* index_prev = b.contact_index + 2ull * C * ((tick - 1u) & 1u);
+    const bool indexed = prev_ok && b.counts->prev_indexed != 0u;
+    const uint32_t narrow_now = b.counts->narrow;
     for (;;) {
         const uint32_t tile = take_tile(site.ticket, &s_tile);
         if (tile >= tiles) break;
         const uint32_t k = tile * kBlock + threadIdx.x;
         bool act = false;
         if (k < n) {
+            {   // index this tick's list for the next tick's lookups
+                const uint64_t key = cur_keys[k];
+                const uint32_t ca = (uint32_t)(key >> 32);
+                if (k >= narrow_now) index_cur[C + ca] = make_uint2(tick, k);            // one ground row per collider
+                else if (k == 0 || (uint32_t)(cur_keys[k - 1] >> 32) != ca) index_cur[ca] = make_uint2(tick, k);
+            }
             float4* row = reinterpret_cast<float4*>(cur + k);
             const float4 r0 = row[0], np = row[1], aa = row[2], ab = row[3];
             const uint32_t a = __float_as_uint(r0.x), bb = __float_as_uint(r0.y);
@@ -1079,8 +1091,20 @@ __global__ void __launch_bounds__(kBlock) k_prepare(StepBuffers b, StepParams p,
                         const uint64_t key = cur_keys[k];
                         const bool ground = (uint32_t)key == kInvalid;
                         const uint32_t end = ground ? prev_all : prev_narrow;
-                        const int64_t m = ground ? find_previous(prev_keys, prev_narrow, prev_all, key)
-                                                 : find_previous(prev_keys, 0u, prev_narrow, key);
+                        int64_t m = -1;
+                        if (indexed) {   // the collider's run, then a short scan to the key
+                            const uint32_t ca = (uint32_t)(key >> 32);
+                            const uint2 e = __ldg(index_prev + (ground ? C : 0ull) + ca);
+                            if (e.x == tick - 1u) {
+                                uint32_t r = e.y;
+                                while (r < end && __ldg(prev_keys + r) < key && (uint32_t)(__ldg(prev_keys + r) >> 32) == ca)
+                                    ++r;
+                                if (r < end && __ldg(prev_keys + r) == key) m = r;
+                            }
+                        } else {
+                            m = ground ? find_previous(prev_keys, prev_narrow, prev_all, key)
+                                       : find_previous(prev_keys, 0u, prev_narrow, key);
+                        }
                         for (int64_t r = m; r >= 0 && r < (int64_t)end && __ldg(prev_keys + r) == key; ++r) {
                             if (!(__ldg(prev_feat + r) & (1u << 24))) continue;
                             const float4* pr = reinterpret_cast<const float4*>(prev + r);
@@ -2005,6 +2029,7 @@ __global__ void k_finish_tick(StepBuffers b) {
     c->prev_contacts = c->contacts;
     c->prev_tick = b.tick->tick_index;
     c->prev_valid = 1u;
+    c->prev_indexed = 1u;   // this tick's prepare indexed its list
 }
 
 // physics.wgsl:73-90
