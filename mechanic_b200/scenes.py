@@ -373,6 +373,16 @@ def config_plain_scale(seed: int = 0) -> Scene:
     return stack_grid(50, 40, 50, seed)
 
 
+def config_full(seed: int = 0, grid: int = 100, chains: int = 50_000) -> Scene:
+    """The full form at scale: the 100,000-body mix on a grid x grid x grid lattice
+    (1,000,000 bodies at grid 100) and `chains` five-body bearing chains (10%
+    loop-closed), laid out 100 m beside the lattice so the two do not overlap."""
+    lattice = stack_grid(grid, grid, grid, seed)
+    field = translated(bearing_chains(chains, 5, seed=seed + 1, closure_fraction=0.1), (100.0, 0.0, 0.0))
+    scene, _ = concatenate([lattice, field])
+    return scene
+
+
 def with_suppression(scene: Scene, body_pairs: np.ndarray) -> Scene:
     """Adds sorted, de-duplicated suppressed body pairs (compile.rs:373, ordered_pair)."""
     p = np.sort(np.asarray(body_pairs, np.uint32).reshape(-1, 2), axis=1)

@@ -79,3 +79,15 @@ def test_batched_config_sizes():
     assert 300_000 < sizes.sum() < 700_000
     frac = sum(s.bearing_count for s in lst) / sizes.sum()
     assert 0.005 < frac < 0.03
+
+
+def test_full_scale_scene_layout():
+    """The full form's generator at a small size: the lattice and the chain field are one
+    creation, the chain field beside the lattice (no overlap), 10% of the chains closed."""
+    lattice = scenes.stack_grid(6, 6, 6, seed=0)
+    full = scenes.config_full(0, grid=6, chains=40)
+    assert full.body_count == lattice.body_count + 40 * 5
+    assert full.collider_count == lattice.collider_count + 40 * 5
+    x = full.transforms["position"][:, 0]
+    assert x[: lattice.body_count].max() < 10.0 and x[lattice.body_count:].min() > 50.0
+    assert full.bearing_count > 0 and full.max_depth > 0
