@@ -257,6 +257,13 @@ cudaError_t enqueue_tick(MkHandle* h, int parity, bool capturing) {
             z.add(r, rb);
         }
         if (h->mechanism_active) z.add(h->mech.deltas, 24ull * std::max(h->B, 1u));
+        if (h->mechanism_active) {   // the closure loop's barrier word and per-step maxima
+            void* mp[2];
+            uint64_t mb[2];
+            uint32_t mc = 0;
+            mk::mechanism_tick_clears(h->mech, h->mech_params, mp, mb, &mc);
+            for (uint32_t k = 0; k < mc; ++k) z.add(mp[k], mb[k]);
+        }
         if (z.dropped) return cudaErrorInvalidValue;   // more per-tick clears than the list holds
         cudaError_t ez = mk::launch_tick_reset(z, h->sm_count, s);
         if (ez != cudaSuccess) return ez;
@@ -760,6 +767,11 @@ int mk_set_tuning(uint32_t key, uint32_t value) {
         const uint32_t prev = sort_items;
         sort_items = value;
         mk::set_sort_items(value);
+        return (int)prev;
+    }
+    if (key == MK_TUNE_CLOSURE_GRID) {
+        const uint32_t prev = mk::closure_grid_mode();
+        mk::set_closure_grid(value);
         return (int)prev;
     }
     return -1;

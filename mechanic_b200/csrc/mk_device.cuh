@@ -234,4 +234,28 @@ __device__ __forceinline__ uint64_t tile_lookback(uint64_t* states, uint32_t til
     return exclusive;
 }
 
+// Grid-wide barrier for a cooperative launch on one 32-bit word that starts at
+// zero: block 0 adds 2^31 - (participants - 1), every other block adds 1, so
+// the word's top bit flips exactly when the last block arrives and its low
+// bits return to zero for the next barrier (one atomic per block, no reset
+// step).  The wait is bounded: a block that gives up raises
+// MK_DEVICE_WAIT_TIMEOUT_FLAG and carries on.
+__device__ __forceinline__ void grid_barrier(uint32_t* state, uint32_t* error_flags, uint32_t participants) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const uint32_t add = blockIdx.x == 0 ? 0x80000000u - (participants - 1u) : 1u;
+        __threadfence();
+        const uint32_t old = atomicAdd(state, add);
+        uint32_t spins = 0;
+        while (((ld_acquire_u32(state) ^ old) & 0x80000000u) == 0u) {
+            if (++spins > kSpinLimit) {
+                atomicOr(error_flags, MK_DEVICE_WAIT_TIMEOUT_FLAG);
+                break;
+            }
+        }
+        __threadfence();
+    }
+    __syncthreads();
+}
+
 }  // namespace mk

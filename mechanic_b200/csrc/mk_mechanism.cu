@@ -178,6 +178,9 @@ void carve_mechanism(MechBuffers& m, const MechParams& p, uint32_t B, uint32_t J
     m.grad = f32(Q);
     m.diag = f32(Q);
     m.pcg = f32(5ull * Q);
+    m.grid_barrier = u32(64);   // its own 256-byte line
+    m.loop_state = u32(2ull * kClosureSteps);
+    m.chunk_part = f32(2ull * ((p.closure_coords + kClosureThreads - 1) / kClosureThreads));
     m.links_final = p.final_is_a ? m.links_a : m.links_b;
     if (pcg_residual_mode(p)) {
         m.slot_closure = u32(p.slots);
@@ -622,27 +625,53 @@ __device__ __forceinline__ float block_sum(float v, float* scratch) {
     return scratch[32];
 }
 
-// Dot product over the closure coordinates.  Up to kSerialDot coordinates it
-// is summed by one thread in ascending coordinate order (the serial order of
-// closure.wgsl:339-414, so small systems reproduce it bit for bit); larger
-// systems use the fixed-order block tree of the per-thread partials.
+// Dot products over the closure coordinates.  Up to kSerialDot coordinates
+// one thread sums them in ascending coordinate order (the serial order of
+// closure.wgsl:339-414, so small systems reproduce it bit for bit).  Larger
+// systems sum per chunk of 1,024 coordinates: thread t of the chunk's block
+// holds coordinate 1024 c + t, the block tree sums the chunk, and the chunk
+// sums are added in chunk order -- the same result whether one block or the
+// whole grid walks the chunks.
 constexpr uint32_t kSerialDot = 512;
-enum DotKind { kDotRZ, kDotDirOp };
-__device__ __forceinline__ float closure_dot(DotKind kind, float partial, const MechBuffers& m, uint32_t nq,
-                                             const float* a, const float* bvec, float* scratch) {
-    if (nq > kSerialDot) return block_sum(partial, scratch);
-    (void)kind;
-    __syncthreads();
+constexpr uint32_t kDotChunk = kClosureThreads;
+
+// Sync of the closure loop: the block, or the whole cooperative grid.
+template <bool kGrid>
+__device__ __forceinline__ void loop_sync(uint32_t* barrier, uint32_t* error_flags) {
+    if (kGrid) grid_barrier(barrier, error_flags, gridDim.x);
+    else __syncthreads();
+}
+
+// The chunked dot: `part` is this thread's term for the coordinate of chunk
+// `c` it holds (0 when none); the block tree sum of the chunk goes to
+// chunk_part[c].  Call for every chunk the block walks, all threads together.
+__device__ __forceinline__ void chunk_dot(float part, float* chunk_part, uint32_t c, float* scratch) {
+    const float s = block_sum(part, scratch);
+    if (threadIdx.x == 0) chunk_part[c] = s;
+}
+
+// The total after a loop_sync: serial over the coordinates (small systems) or
+// the chunk sums in chunk order, computed by thread 0 of every block and
+// shared through scratch[32].
+__device__ __forceinline__ float dot_total(uint32_t nq, const MechBuffers& m, const float* a, const float* bvec,
+                                           const float* chunk_part, float* scratch) {
     if (threadIdx.x == 0) {
         float acc = 0.0f;
-        for (uint32_t q = 0; q < nq; ++q) {
-            const uint32_t c = m.cq_coords[q];
-            acc += a[c] * bvec[c];
+        if (nq <= kSerialDot) {
+            for (uint32_t q = 0; q < nq; ++q) {
+                const uint32_t c = m.cq_coords[q];
+                acc += a[c] * bvec[c];
+            }
+        } else {
+            const uint32_t chunks = (nq + kDotChunk - 1) / kDotChunk;
+            for (uint32_t c = 0; c < chunks; ++c) acc += chunk_part[c];
         }
         scratch[32] = acc;
     }
     __syncthreads();
-    return scratch[32];
+    const float r = scratch[32];
+    __syncthreads();
+    return r;
 }
 
 // Joint frame of `body` in its root's frame (closure.wgsl:168-181).
@@ -674,32 +703,39 @@ __device__ __forceinline__ bool finite3(f3 v) {
            fabsf(v.z) < kFloatMax;
 }
 
-// The closure loop of device.rs:973-1020 in one block: 12 Newton steps of
+// The closure loop of device.rs:973-1020: 12 Newton steps of
 // closure.wgsl:268-427 (evaluate, finalize, 8-round diagonal PCG, step the
 // coordinates), each followed by forward kinematics of the closure
 // components.  Accumulations go through per-joint slots summed per
-// coordinate in the serial order; dot products are fixed-order block sums.
+// coordinate in the serial order; dot products as above.  kGrid = false runs
+// it in one block (few closures: block syncs are nearly free); kGrid = true
+// spreads closures, coordinate chunks and bodies over a cooperative grid with
+// grid barriers in place of the block syncs (thousands of closures).  Both
+// compute the same values.
+template <bool kGrid>
 __global__ void __launch_bounds__(kClosureThreads) k_closure_loop(StepBuffers b, MechBuffers m, MechParams p) {
     __shared__ float s_red[33];
-    __shared__ uint32_t s_state[2];
-    __shared__ uint32_t s_unconverged, s_converged_prev;
-    __shared__ uint32_t s_steps, s_rounds;
-    const uint32_t tid = threadIdx.x, nt = blockDim.x;
+    const uint32_t gtid = blockIdx.x * blockDim.x + threadIdx.x, gnt = gridDim.x * blockDim.x;
     const uint32_t NC = p.closures, NQ = p.closure_coords, NB = p.closure_bodies, Q = p.coordinate_count;
+    const uint32_t chunks = (NQ + kDotChunk - 1) / kDotChunk;
     float* sol = m.pcg;
     float* res = m.pcg + Q;
     float* pre = m.pcg + 2ull * Q;
     float* dir = m.pcg + 3ull * Q;
     float* op = m.pcg + 4ull * Q;
-    if (tid == 0) { s_converged_prev = 0; s_steps = 0; s_rounds = 0; }
-    __syncthreads();
+    uint32_t* flags = &b.diag->error_flags;
+    // per-step residual maxima (zeroed at the start of the tick) and chunk sums
+    uint32_t* state = m.loop_state;
+    float* part_a = m.chunk_part;
+    float* part_b = m.chunk_part + chunks;
+    bool converged_prev = false;
+    uint32_t steps = 0, rounds = 0;
     for (uint32_t step = 0; step < kClosureSteps; ++step) {
-        if (tid == 0) { s_state[0] = 0; s_state[1] = 0; }
-        __syncthreads();
-        const bool evaluate = step == 0 || !s_converged_prev;
+        uint32_t* st = state + 2 * step;
+        const bool evaluate = step == 0 || !converged_prev;
         // evaluate_closures (closure.wgsl:268-319): slot contributions
         if (evaluate) {
-            for (uint32_t k = tid; k < NC; k += nt) {
+            for (uint32_t k = gtid; k < NC; k += gnt) {
                 const GpuBearing br = m.bearings[m.cl_bearings[k]];
                 f3 aa, ab, xa, xb;
                 closure_frames(m, br, aa, ab, xa, xb);
@@ -707,9 +743,9 @@ __global__ void __launch_bounds__(kClosureThreads) k_closure_loop(StepBuffers b,
                 const uint32_t s0 = m.cl_slot_off[k], s1 = m.cl_slot_off[k + 1], split = m.cl_split[k];
                 bool active = true;
                 if (!finite3(rp) || !finite3(ra)) {
-                    atomicOr(&b.diag->error_flags, MK_INVALID_NUMERIC_FLAG);
-                    atomicMax(&s_state[0], 0xffffffffu);
-                    atomicMax(&s_state[1], 0xffffffffu);
+                    atomicOr(flags, MK_INVALID_NUMERIC_FLAG);
+                    atomicMax(&st[0], 0xffffffffu);
+                    atomicMax(&st[1], 0xffffffffu);
                     active = false;
                 } else {
                     const uint32_t um = round_u32(length(rp) * 1000000.0f);
@@ -718,8 +754,8 @@ __global__ void __launch_bounds__(kClosureThreads) k_closure_loop(StepBuffers b,
                     const float deg =
                         atan2_cr(length(cross(xa, xb)), clampf(dot(xa, xb), -1.0f, 1.0f)) * 57.295779513f;
                     const uint32_t ud = round_u32(deg * 1000000.0f);
-                    atomicMax(&s_state[0], um);
-                    atomicMax(&s_state[1], ud);
+                    atomicMax(&st[0], um);
+                    atomicMax(&st[1], ud);
                     active = !(um <= 10u && ud <= 1000u);
                 }
                 for (uint32_t sl = s0; sl < s1; ++sl) {
@@ -733,14 +769,14 @@ __global__ void __launch_bounds__(kClosureThreads) k_closure_loop(StepBuffers b,
                         uint32_t coord;
                         joint_frame(m, m.slot_body[sl], axis, anchor, coord);
                         if (coord >= Q) {
-                            atomicOr(&b.diag->error_flags, MK_INVALID_NUMERIC_FLAG);
+                            atomicOr(flags, MK_INVALID_NUMERIC_FLAG);
                         } else {
                             const f3 pd = cross(axis, ea - anchor) * sign;
                             const f3 ad = cross(axis, ex) * sign;
                             g = dot(rp, pd) + 1.0f * dot(ra, ad);
                             d = dot(pd, pd) + 1.0f * dot(ad, ad);
                             if (g == g && d == d) valid = 1;
-                            else atomicOr(&b.diag->error_flags, MK_INVALID_NUMERIC_FLAG);
+                            else atomicOr(flags, MK_INVALID_NUMERIC_FLAG);
                         }
                     }
                     // NaN marks "no contribution" so the gather skips it
@@ -749,42 +785,41 @@ __global__ void __launch_bounds__(kClosureThreads) k_closure_loop(StepBuffers b,
                 }
             }
         }
-        __syncthreads();
-        // gather per coordinate in the serial accumulation order
-        for (uint32_t q = tid; q < NQ; q += nt) {
-            float g = 0.0f, d = 0.0f;
-            if (evaluate) {
-                for (uint32_t i = m.cq_off[q]; i < m.cq_off[q + 1]; ++i) {
-                    const uint32_t sl = m.cq_slots[i];
-                    const float sg = m.slot_g[sl];
-                    if (sg == sg) { g += sg; d += m.slot_d[sl]; }
+        loop_sync<kGrid>(m.grid_barrier, flags);
+        const bool unconverged = ld_relaxed_u32(&st[0]) > 10u || ld_relaxed_u32(&st[1]) > 1000u;
+        if (unconverged) ++steps;
+        // gather per coordinate in the serial accumulation order, then the PCG's
+        // initial vectors (solve_closure_pcg, closure.wgsl:333-427), chunk by chunk
+        for (uint32_t c = blockIdx.x; c < chunks; c += gridDim.x) {
+            const uint32_t q = c * kDotChunk + threadIdx.x;
+            float part = 0.0f;
+            if (q < NQ) {
+                float g = 0.0f, d = 0.0f;
+                if (evaluate) {
+                    for (uint32_t i = m.cq_off[q]; i < m.cq_off[q + 1]; ++i) {
+                        const uint32_t sl = m.cq_slots[i];
+                        const float sg = m.slot_g[sl];
+                        if (sg == sg) { g += sg; d += m.slot_d[sl]; }
+                    }
+                }
+                const uint32_t cc = m.cq_coords[q];
+                m.grad[cc] = g;
+                m.diag[cc] = d;
+                if (unconverged) {
+                    float r = 0.0f, z = 0.0f;
+                    if (d > 1.0e-12f) { r = -g; z = r / d; }
+                    sol[cc] = 0.0f; res[cc] = r; pre[cc] = z; dir[cc] = z; op[cc] = 0.0f;
+                    part = r * z;
                 }
             }
-            const uint32_t c = m.cq_coords[q];
-            m.grad[c] = g;
-            m.diag[c] = d;
+            if (unconverged && NQ > kSerialDot) chunk_dot(part, part_a, c, s_red);
         }
-        if (tid == 0) {
-            s_unconverged = (s_state[0] > 10u || s_state[1] > 1000u) ? 1u : 0u;
-            if (s_unconverged) ++s_steps;
-        }
-        __syncthreads();
-        const bool unconverged = s_unconverged != 0u;
         if (unconverged) {
-            // solve_closure_pcg (closure.wgsl:333-427)
-            float part = 0.0f;
-            for (uint32_t q = tid; q < NQ; q += nt) {
-                const uint32_t c = m.cq_coords[q];
-                const float g = m.grad[c], d = m.diag[c];
-                float r = 0.0f, z = 0.0f;
-                if (d > 1.0e-12f) { r = -g; z = r / d; }
-                sol[c] = 0.0f; res[c] = r; pre[c] = z; dir[c] = z; op[c] = 0.0f;
-                part += r * z;
-            }
-            float rz = closure_dot(kDotRZ, part, m, NQ, res, pre, s_red);
+            loop_sync<kGrid>(m.grid_barrier, flags);
+            float rz = dot_total(NQ, m, res, pre, part_a, s_red);
             for (uint32_t round = 0; round < kClosureRounds; ++round) {
                 // J^T J dir per closure: branch products then transposes (closure.wgsl:194-266)
-                for (uint32_t k = tid; k < NC; k += nt) {
+                for (uint32_t k = gtid; k < NC; k += gnt) {
                     const GpuBearing br = m.bearings[m.cl_bearings[k]];
                     f3 aa, ab, xa, xb;
                     closure_frames(m, br, aa, ab, xa, xb);
@@ -814,61 +849,73 @@ __global__ void __launch_bounds__(kClosureThreads) k_closure_loop(StepBuffers b,
                         m.slot_g[sl] = dot(pd, pp) + 1.0f * dot(ad, pa);
                     }
                 }
-                __syncthreads();
-                float dpart = 0.0f;
-                for (uint32_t q = tid; q < NQ; q += nt) {
-                    float o = 0.0f;
-                    for (uint32_t i = m.cq_off[q]; i < m.cq_off[q + 1]; ++i) o += m.slot_g[m.cq_slots[i]];
-                    const uint32_t c = m.cq_coords[q];
-                    op[c] = o;
-                    dpart += dir[c] * o;
+                loop_sync<kGrid>(m.grid_barrier, flags);
+                for (uint32_t c = blockIdx.x; c < chunks; c += gridDim.x) {
+                    const uint32_t q = c * kDotChunk + threadIdx.x;
+                    float dpart = 0.0f;
+                    if (q < NQ) {
+                        float o = 0.0f;
+                        for (uint32_t i = m.cq_off[q]; i < m.cq_off[q + 1]; ++i) o += m.slot_g[m.cq_slots[i]];
+                        const uint32_t cc = m.cq_coords[q];
+                        op[cc] = o;
+                        dpart = dir[cc] * o;
+                    }
+                    if (NQ > kSerialDot) chunk_dot(dpart, part_b, c, s_red);
                 }
-                const float dop = closure_dot(kDotDirOp, dpart, m, NQ, dir, op, s_red);
+                loop_sync<kGrid>(m.grid_barrier, flags);
+                const float dop = dot_total(NQ, m, dir, op, part_b, s_red);
                 const float alpha = fabsf(dop) > 1.0e-20f ? rz / dop : 0.0f;
-                float npart = 0.0f;
-                for (uint32_t q = tid; q < NQ; q += nt) {
-                    const uint32_t c = m.cq_coords[q];
-                    sol[c] += alpha * dir[c];
-                    res[c] -= alpha * op[c];
-                    const float d = m.diag[c];
-                    pre[c] = 0.0f;
-                    if (d > 1.0e-12f) pre[c] = res[c] / d;
-                    npart += res[c] * pre[c];
+                for (uint32_t c = blockIdx.x; c < chunks; c += gridDim.x) {
+                    const uint32_t q = c * kDotChunk + threadIdx.x;
+                    float npart = 0.0f;
+                    if (q < NQ) {
+                        const uint32_t cc = m.cq_coords[q];
+                        sol[cc] += alpha * dir[cc];
+                        res[cc] -= alpha * op[cc];
+                        const float d = m.diag[cc];
+                        pre[cc] = 0.0f;
+                        if (d > 1.0e-12f) pre[cc] = res[cc] / d;
+                        npart = res[cc] * pre[cc];
+                    }
+                    if (NQ > kSerialDot) chunk_dot(npart, part_a, c, s_red);
                 }
-                const float nrz = closure_dot(kDotRZ, npart, m, NQ, res, pre, s_red);
+                loop_sync<kGrid>(m.grid_barrier, flags);
+                const float nrz = dot_total(NQ, m, res, pre, part_a, s_red);
                 const float beta = fabsf(rz) > 1.0e-20f ? nrz / rz : 0.0f;
-                for (uint32_t q = tid; q < NQ; q += nt) {
-                    const uint32_t c = m.cq_coords[q];
-                    dir[c] = pre[c] + beta * dir[c];
+                for (uint32_t c = blockIdx.x; c < chunks; c += gridDim.x) {
+                    const uint32_t q = c * kDotChunk + threadIdx.x;
+                    if (q < NQ) {
+                        const uint32_t cc = m.cq_coords[q];
+                        dir[cc] = pre[cc] + beta * dir[cc];
+                    }
                 }
                 rz = nrz;
-                if (tid == 0) ++s_rounds;
-                __syncthreads();
+                ++rounds;
+                loop_sync<kGrid>(m.grid_barrier, flags);
             }
             // step every coordinate (coordinates off the closure branches add 0)
-            for (uint32_t c = tid; c < Q; c += nt) {
+            for (uint32_t c = gtid; c < Q; c += gnt) {
                 const float stp = clampf(0.35f * sol[c], -0.2f, 0.2f);
                 if (stp == stp) m.coords[c].angle += stp;
-                else atomicOr(&b.diag->error_flags, MK_INVALID_NUMERIC_FLAG);
+                else atomicOr(flags, MK_INVALID_NUMERIC_FLAG);
             }
-            __syncthreads();
+            loop_sync<kGrid>(m.grid_barrier, flags);
             // forward kinematics of the closure components (mechanism.wgsl:72-149)
-            for (uint32_t i = tid; i < NB; i += nt) prepare_link(m, m.cb_bodies[i]);
-            __syncthreads();
+            for (uint32_t i = gtid; i < NB; i += gnt) prepare_link(m, m.cb_bodies[i]);
+            loop_sync<kGrid>(m.grid_barrier, flags);
             bool a_src = true;
             for (uint32_t r = 0; r < p.jump_rounds; ++r) {
-                for (uint32_t i = tid; i < NB; i += nt)
+                for (uint32_t i = gtid; i < NB; i += gnt)
                     jump_link(a_src ? m.links_a : m.links_b, a_src ? m.links_b : m.links_a, m.cb_bodies[i]);
-                __syncthreads();
+                loop_sync<kGrid>(m.grid_barrier, flags);
                 a_src = !a_src;
             }
         }
-        if (tid == 0) s_converged_prev = unconverged ? 0u : 1u;
-        __syncthreads();
+        converged_prev = !unconverged;
     }
-    if (tid == 0) {
-        atomicAdd(&b.diag->reserved_b, s_steps);
-        atomicAdd(&b.diag->reserved_c, s_rounds);
+    if (gtid == 0) {
+        atomicAdd(&b.diag->reserved_b, steps);
+        atomicAdd(&b.diag->reserved_c, rounds);
     }
 }
 
@@ -1322,6 +1369,23 @@ static cudaError_t reconstruct(MechBuffers& m, const StepBuffers& b, cudaStream_
     return cudaGetLastError();
 }
 
+// Reference-mode closure loop: one block below kGridClosures closures, the
+// whole grid from there (both compute the same values); a tuning override.
+constexpr uint32_t kGridClosures = 256;
+static uint32_t g_closure_grid = 0;
+void set_closure_grid(uint32_t mode) { g_closure_grid = mode <= 2u ? mode : 0u; }
+uint32_t closure_grid_mode() { return g_closure_grid; }
+
+void mechanism_tick_clears(const MechBuffers& m, const MechParams& p, void** ptr, uint64_t* bytes, uint32_t* count) {
+    *count = 0;
+    if (p.closures == 0) return;
+    ptr[0] = m.grid_barrier;
+    bytes[0] = 64 * sizeof(uint32_t);
+    ptr[1] = m.loop_state;
+    bytes[1] = 2ull * kClosureSteps * sizeof(uint32_t);
+    *count = 2;
+}
+
 // device.rs:963-1048
 cudaError_t enqueue_mechanism(MechBuffers& m, const StepBuffers& b, const MechParams& p, cudaStream_t s) {
     cudaError_t e;
@@ -1340,7 +1404,34 @@ cudaError_t enqueue_mechanism(MechBuffers& m, const StepBuffers& b, const MechPa
             k_closure_pcg<<<1, kClosureThreads, 0, s>>>(b, m, p, step);
         }
     } else if (p.closures > 0) {
-        k_closure_loop<<<1, kClosureThreads, 0, s>>>(b, m, p);
+        const uint32_t mode = g_closure_grid;
+        const bool grid = mode == 2u || (mode == 0u && p.closures >= kGridClosures);
+        if (grid) {
+            // one co-resident 1,024-thread block per SM (cooperative launch: grid barriers)
+            int dev = 0, sms = 0, per_sm = 0;
+            if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
+            if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
+            if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_closure_loop<true>, kClosureThreads, 0)) !=
+                cudaSuccess)
+                return e;
+            if (per_sm < 1) return cudaErrorInvalidConfiguration;
+            StepBuffers bb = b;
+            MechBuffers mm = m;
+            MechParams pp = p;
+            void* args[] = {&bb, &mm, &pp};
+            cudaLaunchConfig_t cfg = {};
+            cfg.gridDim = dim3((uint32_t)sms);
+            cfg.blockDim = dim3(kClosureThreads);
+            cfg.stream = s;
+            cudaLaunchAttribute attr[1];
+            attr[0].id = cudaLaunchAttributeCooperative;
+            attr[0].val.cooperative = 1;
+            cfg.attrs = attr;
+            cfg.numAttrs = 1;
+            if ((e = cudaLaunchKernelExC(&cfg, (const void*)k_closure_loop<true>, args)) != cudaSuccess) return e;
+        } else {
+            k_closure_loop<false><<<1, kClosureThreads, 0, s>>>(b, m, p);
+        }
     }
     k_publish<<<nblocks(p.body_count), kMBlock, 0, s>>>(b, m, p);
     return reconstruct(m, b, s);

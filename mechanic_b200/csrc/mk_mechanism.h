@@ -73,6 +73,9 @@ struct MechBuffers {
     float* grad = nullptr;                      // Q (closure.wgsl:46-49 accumulators)
     float* diag = nullptr;                      // Q
     float* pcg = nullptr;                       // 5 x Q: sol, res, pre, dir, op (closure.wgsl:51-60)
+    uint32_t* grid_barrier = nullptr;           // arrival word of the grid-wide closure loop (zero at rest)
+    uint32_t* loop_state = nullptr;             // 12 steps x 2: largest residuals (um, udeg), zeroed per tick
+    float* chunk_part = nullptr;                // 2 x chunks of 1,024 closure coordinates: dot-product sums
     uint32_t readback_iterations = 0;
     double readback_residual = 0.0;
     // MK_CLOSURE_PCG_RESIDUAL
@@ -101,6 +104,11 @@ struct MechTopology {
     std::vector<uint32_t> loop_off, loop_q;
 };
 MechTopology derive_topology(const MkCreation* cr, MechParams& p);
+// Reference-mode closure loop: 0 = by size, 1 = one block, 2 = the whole grid.
+void set_closure_grid(uint32_t mode);
+uint32_t closure_grid_mode();
+// Regions of the mechanism buffers to clear at the start of every tick.
+void mechanism_tick_clears(const MechBuffers& m, const MechParams& p, void** ptr, uint64_t* bytes, uint32_t* count);
 void carve_mechanism(MechBuffers& m, const MechParams& p, uint32_t B, uint32_t J, uint32_t Q,
                      const std::function<char*(uint64_t)>& take);
 bool upload_mechanism(MechBuffers& m, const MechParams& p, const MechTopology& topo, const MkCreation* cr,

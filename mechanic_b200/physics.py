@@ -503,6 +503,7 @@ class GpuPhysics:
 
 
 TUNE_SORT_ITEMS = 1
+TUNE_CLOSURE_GRID = 2   # reference-mode closure loop: 0 by size, 1 one block, 2 the whole grid
 
 
 def set_tuning(key: int, value: int) -> int:

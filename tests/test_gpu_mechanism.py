@@ -74,6 +74,44 @@ def test_chains_with_closures_and_contacts_bitexact(cuda_lib):
     assert np.array_equal(gpu.pairs(), orc.pairs())
 
 
+def _with_closure_grid(mode, make):
+    from mechanic_b200 import physics
+    prev = physics.set_tuning(physics.TUNE_CLOSURE_GRID, mode)
+    try:
+        return make()
+    finally:
+        physics.set_tuning(physics.TUNE_CLOSURE_GRID, max(prev, 0))
+
+
+def test_grid_closure_loop_bitexact(cuda_lib):
+    """The closure loop spread over the whole cooperative grid (grid barriers between its
+    phases) gives the oracle's values bit for bit on a system small enough for the serial
+    dot order."""
+    scene = scenes.bearing_chains(chains=40, links=5, seed=1, closure_fraction=0.3, height=0.5)
+    gpu, orc = _with_closure_grid(2, lambda: _pair(scene, GpuPhysicsConfig()))
+    for tick in range(1, 16):
+        _compare(gpu, orc, tick, "grid closure loop")
+
+
+def test_grid_and_block_closure_loops_agree(cuda_lib):
+    """Above 1,024 closure coordinates the dot products sum per 1,024-coordinate chunk in
+    chunk order, so one block and the whole grid compute the same values."""
+    scene = scenes.bearing_chains(chains=3000, links=5, seed=4, closure_fraction=0.1, height=0.5)
+    runs = []
+    for mode in (1, 2):
+        gpu = _with_closure_grid(mode, lambda: GpuPhysics(scene, GpuPhysicsConfig(), capacities={"pair_capacity": 1 << 21}))
+        for tick in range(1, 9):
+            gpu.dispatch_tick(tick)
+        rb = gpu.read_last_tick()
+        runs.append((gpu.save_state(manifold_capacity=0), rb))
+        gpu.close()
+    (a, ra), (b, rb) = runs
+    assert ra.closure_iterations == rb.closure_iterations
+    _same(a["transforms"], b["transforms"], "grid vs block transforms")
+    _same(a["velocities"], b["velocities"], "grid vs block velocities")
+    _same(a["coordinates"], b["coordinates"], "grid vs block coordinates")
+
+
 def test_chains_without_self_collisions_bitexact(cuda_lib):
     scene = scenes.bearing_chains(chains=16, links=5, seed=3, closure_fraction=0.0, height=0.3)
     gpu, orc = _pair(scene, GpuPhysicsConfig(mechanism_self_collisions=False))
