@@ -471,9 +471,10 @@ MK_API uint32_t mk_tick_kernel_count(const MkHandle* handle);
 /* Process-wide tuning knobs read when a tick is captured (mk_create) or an
  * operation is launched.  Keys: MK_TUNE_SORT_ITEMS (keys per thread of a
  * radix-sort tile: 2, 4, 6, 8, 11 or 16; 0 = size-based default);
- * MK_TUNE_CLOSURE_GRID (the reference-mode closure loop: 0 = by size, one
- * block below 256 closures and the whole grid from there, 1 = always one
- * block, 2 = always the grid; both give the same results).  Returns the
+ * MK_TUNE_CLOSURE_GRID (the closure solves, the reference's loop and the PCG
+ * to a residual: 0 = by size, one block below 256 closures and the whole grid
+ * from there, 1 = always one block, 2 = always the grid; both give the same
+ * results).  Returns the
  * previous value, or -1 for an unknown key. */
 #define MK_TUNE_SORT_ITEMS 1u
 #define MK_TUNE_CLOSURE_GRID 2u

@@ -181,6 +181,7 @@ void carve_mechanism(MechBuffers& m, const MechParams& p, uint32_t B, uint32_t J
     m.grid_barrier = u32(64);   // its own 256-byte line
     m.loop_state = u32(2ull * kClosureSteps);
     m.chunk_part = f32(2ull * ((p.closure_coords + kClosureThreads - 1) / kClosureThreads));
+    m.chunk_part_d = reinterpret_cast<double*>(take(16ull * ((p.closure_coords + kClosureThreads - 1) / kClosureThreads + 1)));
     m.links_final = p.final_is_a ? m.links_a : m.links_b;
     if (pcg_residual_mode(p)) {
         m.slot_closure = u32(p.slots);
@@ -954,9 +955,28 @@ __device__ __forceinline__ double block_sum_d(double v, double* scratch) {
     return r;
 }
 
-// out[c] = (J^T J x)[c] for the closure coordinates, from the stored columns.
-__device__ void closure_apply(const MechBuffers& m, const MechParams& p, const float* x, float* out) {
-    const uint32_t tid = threadIdx.x, nt = blockDim.x;
+// The FP64 dot product after a loop_sync: the chunk sums in chunk order (thread
+// 0 of every block), shared through scratch[32].  Chunks of 1,024 coordinates
+// with one coordinate per thread: up to 1,024 coordinates this is the block
+// tree of the per-thread terms, and one block or the whole grid give the same.
+__device__ __forceinline__ double chunk_total_d(const double* part, uint32_t chunks, double* scratch) {
+    if (threadIdx.x == 0) {
+        double acc = 0.0;
+        for (uint32_t c = 0; c < chunks; ++c) acc += part[c];
+        scratch[32] = acc;
+    }
+    __syncthreads();
+    const double r = scratch[32];
+    __syncthreads();
+    return r;
+}
+
+// out[c] = (J^T J x)[c] for the closure coordinates, from the stored columns
+// (the block, or with kGrid the whole cooperative grid).
+template <bool kGrid>
+__device__ void closure_apply(const MechBuffers& m, const MechParams& p, const float* x, float* out,
+                              uint32_t* flags) {
+    const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x, nt = gridDim.x * blockDim.x;
     for (uint32_t k = tid; k < p.closures; k += nt) {
         const uint32_t s0 = m.cl_slot_off[k], s1 = m.cl_slot_off[k + 1], split = m.cl_split[k];
         f3 prod_p[2] = {mkf3(0, 0, 0), mkf3(0, 0, 0)}, prod_a[2] = {mkf3(0, 0, 0), mkf3(0, 0, 0)};
@@ -971,13 +991,13 @@ __device__ void closure_apply(const MechBuffers& m, const MechParams& p, const f
         for (uint32_t sl = s0; sl < s1; ++sl)
             m.slot_g[sl] = dot(xyz(m.slot_v[2 * sl]), pp) + 1.0f * dot(xyz(m.slot_v[2 * sl + 1]), pa);
     }
-    __syncthreads();
+    loop_sync<kGrid>(m.grid_barrier, flags);
     for (uint32_t q = tid; q < p.closure_coords; q += nt) {
         float o = 0.0f;
         for (uint32_t i = m.cq_off[q]; i < m.cq_off[q + 1]; ++i) o += m.slot_g[m.cq_slots[i]];
         out[m.cq_coords[q]] = o;
     }
-    __syncthreads();
+    loop_sync<kGrid>(m.grid_barrier, flags);
 }
 
 // (J^T J)[i][j] for two closure coordinates (positions qi, qj in the list).
@@ -995,21 +1015,19 @@ __device__ __forceinline__ float closure_coupling(const MechBuffers& m, uint32_t
     return r;
 }
 
+template <bool kGrid>
 __global__ void __launch_bounds__(kClosureThreads) k_closure_eval(StepBuffers b, MechBuffers m, MechParams p,
                                                                   uint32_t step) {
-    __shared__ uint32_t s_state[2];
     ClosureState* cs = m.cstate;
-    const uint32_t tid = threadIdx.x, nt = blockDim.x;
+    const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x, nt = gridDim.x * blockDim.x;
     const uint32_t NC = p.closures, NQ = p.closure_coords, Q = p.coordinate_count;
+    uint32_t* flags = &b.diag->error_flags;
     if (step == 0) {
-        __syncthreads();
         if (tid == 0) *cs = ClosureState{0u, 0u, 0u, 0u, 0u, 0u, 0.0};
-        __syncthreads();
     } else if (ld_acquire_u32(&cs->done)) {
         return;
     }
-    if (tid == 0) { s_state[0] = 0; s_state[1] = 0; }
-    __syncthreads();
+    uint32_t* s_state = m.loop_state + 2 * step;   // largest residuals of this step (zeroed per tick)
     // slot columns and their gradient / diagonal contributions (closure.wgsl:268-319)
     for (uint32_t k = tid; k < NC; k += nt) {
         const GpuBearing br = m.bearings[m.cl_bearings[k]];
@@ -1019,7 +1037,7 @@ __global__ void __launch_bounds__(kClosureThreads) k_closure_eval(StepBuffers b,
         const uint32_t s0 = m.cl_slot_off[k], s1 = m.cl_slot_off[k + 1], split = m.cl_split[k];
         bool active = true;
         if (!finite3(rp) || !finite3(ra)) {
-            atomicOr(&b.diag->error_flags, MK_INVALID_NUMERIC_FLAG);
+            atomicOr(flags, MK_INVALID_NUMERIC_FLAG);
             atomicMax(&s_state[0], 0xffffffffu);
             atomicMax(&s_state[1], 0xffffffffu);
             active = false;
@@ -1042,7 +1060,7 @@ __global__ void __launch_bounds__(kClosureThreads) k_closure_eval(StepBuffers b,
             float g = 0.0f, d = 0.0f;
             uint32_t valid = 0;
             if (coord >= Q) {
-                atomicOr(&b.diag->error_flags, MK_INVALID_NUMERIC_FLAG);
+                atomicOr(flags, MK_INVALID_NUMERIC_FLAG);
                 coord = 0;
             } else {
                 pd = cross(axis, ea - anchor) * sign;
@@ -1051,7 +1069,7 @@ __global__ void __launch_bounds__(kClosureThreads) k_closure_eval(StepBuffers b,
                     g = dot(rp, pd) + 1.0f * dot(ra, ad);
                     d = dot(pd, pd) + 1.0f * dot(ad, ad);
                     if (g == g && d == d) valid = 1;
-                    else atomicOr(&b.diag->error_flags, MK_INVALID_NUMERIC_FLAG);
+                    else atomicOr(flags, MK_INVALID_NUMERIC_FLAG);
                 }
             }
             m.slot_v[2 * sl] = f4(pd, __uint_as_float(coord));
@@ -1060,7 +1078,7 @@ __global__ void __launch_bounds__(kClosureThreads) k_closure_eval(StepBuffers b,
             m.slot_d[sl] = valid ? d : 0.0f;
         }
     }
-    __syncthreads();
+    loop_sync<kGrid>(m.grid_barrier, flags);
     for (uint32_t q = tid; q < NQ; q += nt) {
         float g = 0.0f, d = 0.0f;
         for (uint32_t i = m.cq_off[q]; i < m.cq_off[q + 1]; ++i) {
@@ -1075,11 +1093,11 @@ __global__ void __launch_bounds__(kClosureThreads) k_closure_eval(StepBuffers b,
         m.pcg[c] = 1.0f;
         m.pcg[Q + c] = (q & 1u) ? -1.0f : 1.0f;
     }
-    __syncthreads();
-    const bool unconverged = s_state[0] > 10u || s_state[1] > 1000u;
+    loop_sync<kGrid>(m.grid_barrier, flags);
+    const bool unconverged = ld_relaxed_u32(&s_state[0]) > 10u || ld_relaxed_u32(&s_state[1]) > 1000u;
     // A * ones and A * alternating signs (block inputs of the network)
-    closure_apply(m, p, m.pcg, m.probe);
-    closure_apply(m, p, m.pcg + Q, m.probe + Q);
+    closure_apply<kGrid>(m, p, m.pcg, m.probe, flags);
+    closure_apply<kGrid>(m, p, m.pcg + Q, m.probe + Q, flags);
     // block entries (a, b, d) and the plain 2 x 2 inverse
     float* blk_b = m.pcg + 2ull * Q;   // coupling of each block (free until the solve)
     for (uint32_t blk = tid; blk < p.blocks; blk += nt) {
@@ -1095,7 +1113,7 @@ __global__ void __launch_bounds__(kClosureThreads) k_closure_eval(StepBuffers b,
         m.blk_m[blk] = inv;
         blk_b[blk] = bij;
     }
-    __syncthreads();
+    loop_sync<kGrid>(m.grid_barrier, flags);
     // network inputs: the diagonal-normalised entries of J^T J around the block,
     // with the partner block (blk ^ 1) and the couplings to it recovered from
     // the two probes (exact when the loop's coordinates are these two blocks)
@@ -1162,7 +1180,7 @@ __global__ void __launch_bounds__(kClosureThreads) k_closure_eval(StepBuffers b,
                 }
         }
     }
-    __syncthreads();
+    loop_sync<kGrid>(m.grid_barrier, flags);
     if (tid == 0) {
         if (unconverged) {
             cs->live_blocks = p.blocks;
@@ -1174,9 +1192,12 @@ __global__ void __launch_bounds__(kClosureThreads) k_closure_eval(StepBuffers b,
     }
 }
 
-__device__ __forceinline__ void precond_apply(const MechBuffers& m, const MechParams& p, const float* r, float* z) {
+template <bool kGrid>
+__device__ __forceinline__ void precond_apply(const MechBuffers& m, const MechParams& p, const float* r, float* z,
+                                              uint32_t* flags) {
+    const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x, nt = gridDim.x * blockDim.x;
     if (p.precond == MK_PRECOND_BLOCK_JACOBI) {
-        for (uint32_t lp = threadIdx.x; lp < p.loops; lp += blockDim.x) {
+        for (uint32_t lp = tid; lp < p.loops; lp += nt) {
             const uint32_t o = m.loop_off[lp], n = m.loop_off[lp + 1] - o;
             const float* l = m.loop_l + 36ull * lp;
             float y[kMaxLoop];
@@ -1194,10 +1215,10 @@ __device__ __forceinline__ void precond_apply(const MechBuffers& m, const MechPa
             }
             for (uint32_t i = 0; i < n; ++i) z[m.cq_coords[m.loop_q[o + i]]] = y[i];
         }
-        __syncthreads();
+        loop_sync<kGrid>(m.grid_barrier, flags);
         return;
     }
-    for (uint32_t blk = threadIdx.x; blk < p.blocks; blk += blockDim.x) {
+    for (uint32_t blk = tid; blk < p.blocks; blk += nt) {
         const float4 mi = m.blk_m[blk];
         const uint32_t qi = 2 * blk, qj = qi + 1;
         const uint32_t ci = m.cq_coords[qi];
@@ -1210,16 +1231,21 @@ __device__ __forceinline__ void precond_apply(const MechBuffers& m, const MechPa
             z[ci] = mi.x * r[ci];
         }
     }
-    __syncthreads();
+    loop_sync<kGrid>(m.grid_barrier, flags);
 }
 
+template <bool kGrid>
 __global__ void __launch_bounds__(kClosureThreads) k_closure_pcg(StepBuffers b, MechBuffers m, MechParams p,
                                                                  uint32_t step) {
     __shared__ double s_red[33];
     ClosureState* cs = m.cstate;
     if (ld_acquire_u32(&cs->done)) return;
-    const uint32_t tid = threadIdx.x, nt = blockDim.x;
+    const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x, nt = gridDim.x * blockDim.x;
     const uint32_t NQ = p.closure_coords, NB = p.closure_bodies, Q = p.coordinate_count;
+    const uint32_t chunks = (NQ + kDotChunk - 1) / kDotChunk;
+    uint32_t* flags = &b.diag->error_flags;
+    double* part_a = m.chunk_part_d;            // chunk sums of the FP64 dot products
+    double* part_b = m.chunk_part_d + chunks;
     float* sol = m.pcg;
     float* res = m.pcg + Q;
     float* pre = m.pcg + 2ull * Q;
@@ -1259,7 +1285,7 @@ __global__ void __launch_bounds__(kClosureThreads) k_closure_pcg(StepBuffers b, 
         }
         if (used) atomicAdd(&cs->learned_blocks, used);
         if (rejected) atomicAdd(&cs->rejected_blocks, rejected);
-        __syncthreads();
+        loop_sync<kGrid>(m.grid_barrier, flags);
     }
     // r = -g, x = 0, z = M^-1 r, p = z
     for (uint32_t q = tid; q < NQ; q += nt) {
@@ -1267,53 +1293,79 @@ __global__ void __launch_bounds__(kClosureThreads) k_closure_pcg(StepBuffers b, 
         sol[c] = 0.0f;
         res[c] = -m.grad[c];
     }
-    __syncthreads();
-    precond_apply(m, p, res, pre);
-    double prz = 0.0, prr = 0.0;
-    for (uint32_t q = tid; q < NQ; q += nt) {
-        const uint32_t c = m.cq_coords[q];
-        dir[c] = pre[c];
-        prz += (double)res[c] * (double)pre[c];
-        prr += (double)res[c] * (double)res[c];
+    loop_sync<kGrid>(m.grid_barrier, flags);
+    precond_apply<kGrid>(m, p, res, pre, flags);
+    // coordinate loops that feed a dot product walk chunks of 1,024 coordinates
+    // (thread t of the chunk's block holds coordinate 1024 c + t)
+    for (uint32_t c = blockIdx.x; c < chunks; c += gridDim.x) {
+        const uint32_t q = c * kDotChunk + threadIdx.x;
+        double prz = 0.0, prr = 0.0;
+        if (q < NQ) {
+            const uint32_t cc = m.cq_coords[q];
+            dir[cc] = pre[cc];
+            prz = (double)res[cc] * (double)pre[cc];
+            prr = (double)res[cc] * (double)res[cc];
+        }
+        const double sz = block_sum_d(prz, s_red), sr = block_sum_d(prr, s_red);
+        if (threadIdx.x == 0) { part_a[c] = sz; part_b[c] = sr; }
     }
-    double rz = block_sum_d(prz, s_red);
-    const double rr0 = block_sum_d(prr, s_red);
+    loop_sync<kGrid>(m.grid_barrier, flags);
+    double rz = chunk_total_d(part_a, chunks, s_red);
+    const double rr0 = chunk_total_d(part_b, chunks, s_red);
     double rr = rr0;
     const double tol2 = (double)p.closure_tol * (double)p.closure_tol;
     uint32_t it = 0;
     while (it < p.closure_max_it && rr > tol2 * rr0) {
-        closure_apply(m, p, dir, op);
-        double ppq = 0.0;
-        for (uint32_t q = tid; q < NQ; q += nt) {
-            const uint32_t c = m.cq_coords[q];
-            ppq += (double)dir[c] * (double)op[c];
+        closure_apply<kGrid>(m, p, dir, op, flags);
+        for (uint32_t c = blockIdx.x; c < chunks; c += gridDim.x) {
+            const uint32_t q = c * kDotChunk + threadIdx.x;
+            double ppq = 0.0;
+            if (q < NQ) {
+                const uint32_t cc = m.cq_coords[q];
+                ppq = (double)dir[cc] * (double)op[cc];
+            }
+            const double sq = block_sum_d(ppq, s_red);
+            if (threadIdx.x == 0) part_a[c] = sq;
         }
-        const double pq = block_sum_d(ppq, s_red);
+        loop_sync<kGrid>(m.grid_barrier, flags);
+        const double pq = chunk_total_d(part_a, chunks, s_red);
         const float alpha = fabs(pq) > 1.0e-30 ? (float)(rz / pq) : 0.0f;
-        double pr = 0.0;
-        for (uint32_t q = tid; q < NQ; q += nt) {
-            const uint32_t c = m.cq_coords[q];
-            sol[c] += alpha * dir[c];
-            res[c] -= alpha * op[c];
-            pr += (double)res[c] * (double)res[c];
+        for (uint32_t c = blockIdx.x; c < chunks; c += gridDim.x) {
+            const uint32_t q = c * kDotChunk + threadIdx.x;
+            double pr = 0.0;
+            if (q < NQ) {
+                const uint32_t cc = m.cq_coords[q];
+                sol[cc] += alpha * dir[cc];
+                res[cc] -= alpha * op[cc];
+                pr = (double)res[cc] * (double)res[cc];
+            }
+            const double sr = block_sum_d(pr, s_red);
+            if (threadIdx.x == 0) part_b[c] = sr;
         }
-        rr = block_sum_d(pr, s_red);
+        loop_sync<kGrid>(m.grid_barrier, flags);
+        rr = chunk_total_d(part_b, chunks, s_red);
         ++it;
         if (rr <= tol2 * rr0) break;
-        precond_apply(m, p, res, pre);
-        double pz = 0.0;
-        for (uint32_t q = tid; q < NQ; q += nt) {
-            const uint32_t c = m.cq_coords[q];
-            pz += (double)res[c] * (double)pre[c];
+        precond_apply<kGrid>(m, p, res, pre, flags);
+        for (uint32_t c = blockIdx.x; c < chunks; c += gridDim.x) {
+            const uint32_t q = c * kDotChunk + threadIdx.x;
+            double pz = 0.0;
+            if (q < NQ) {
+                const uint32_t cc = m.cq_coords[q];
+                pz = (double)res[cc] * (double)pre[cc];
+            }
+            const double sz = block_sum_d(pz, s_red);
+            if (threadIdx.x == 0) part_a[c] = sz;
         }
-        const double nrz = block_sum_d(pz, s_red);
+        loop_sync<kGrid>(m.grid_barrier, flags);
+        const double nrz = chunk_total_d(part_a, chunks, s_red);
         const float beta = fabs(rz) > 1.0e-300 ? (float)(nrz / rz) : 0.0f;
         for (uint32_t q = tid; q < NQ; q += nt) {
-            const uint32_t c = m.cq_coords[q];
-            dir[c] = pre[c] + beta * dir[c];
+            const uint32_t cc = m.cq_coords[q];
+            dir[cc] = pre[cc] + beta * dir[cc];
         }
         rz = nrz;
-        __syncthreads();
+        loop_sync<kGrid>(m.grid_barrier, flags);
     }
     if (tid == 0) {
         cs->pcg_iterations += it;
@@ -1325,17 +1377,17 @@ __global__ void __launch_bounds__(kClosureThreads) k_closure_pcg(StepBuffers b, 
         const uint32_t c = m.cq_coords[q];
         const float stp = clampf(0.35f * sol[c], -0.2f, 0.2f);
         if (stp == stp) m.coords[c].angle += stp;
-        else atomicOr(&b.diag->error_flags, MK_INVALID_NUMERIC_FLAG);
+        else atomicOr(flags, MK_INVALID_NUMERIC_FLAG);
     }
-    __syncthreads();
+    loop_sync<kGrid>(m.grid_barrier, flags);
     // forward kinematics of the closure components (mechanism.wgsl:72-149)
     for (uint32_t i = tid; i < NB; i += nt) prepare_link(m, m.cb_bodies[i]);
-    __syncthreads();
+    loop_sync<kGrid>(m.grid_barrier, flags);
     bool a_src = true;
     for (uint32_t r = 0; r < p.jump_rounds; ++r) {
         for (uint32_t i = tid; i < NB; i += nt)
             jump_link(a_src ? m.links_a : m.links_b, a_src ? m.links_b : m.links_a, m.cb_bodies[i]);
-        __syncthreads();
+        loop_sync<kGrid>(m.grid_barrier, flags);
         a_src = !a_src;
     }
 }
@@ -1369,12 +1421,43 @@ static cudaError_t reconstruct(MechBuffers& m, const StepBuffers& b, cudaStream_
     return cudaGetLastError();
 }
 
-// Reference-mode closure loop: one block below kGridClosures closures, the
-// whole grid from there (both compute the same values); a tuning override.
+// Closure solves (the reference's loop and the PCG to a residual): one block
+// below kGridClosures closures, the whole grid from there (both compute the
+// same values); a tuning override.
 constexpr uint32_t kGridClosures = 256;
 static uint32_t g_closure_grid = 0;
 void set_closure_grid(uint32_t mode) { g_closure_grid = mode <= 2u ? mode : 0u; }
 uint32_t closure_grid_mode() { return g_closure_grid; }
+
+// One co-resident 1,024-thread block per SM for the grid-wide closure kernels
+// (cooperative launch: they sync with grid barriers).  `step` is passed when
+// the kernel takes one (kNoStep: it does not).
+constexpr uint32_t kNoStep = 0xffffffffu;
+static cudaError_t launch_grid(const void* kernel, const StepBuffers& b, const MechBuffers& m, const MechParams& p,
+                               uint32_t step, cudaStream_t s) {
+    int dev = 0, sms = 0, per_sm = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kClosureThreads, 0);
+    if (e != cudaSuccess) return e;
+    if (per_sm < 1) return cudaErrorInvalidConfiguration;
+    StepBuffers bb = b;
+    MechBuffers mm = m;
+    MechParams pp = p;
+    uint32_t st = step;
+    void* args3[] = {&bb, &mm, &pp};
+    void* args4[] = {&bb, &mm, &pp, &st};
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((uint32_t)sms);
+    cfg.blockDim = dim3(kClosureThreads);
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelExC(&cfg, kernel, step == kNoStep ? args3 : args4);
+}
 
 void mechanism_tick_clears(const MechBuffers& m, const MechParams& p, void** ptr, uint64_t* bytes, uint32_t* count) {
     *count = 0;
@@ -1393,42 +1476,29 @@ cudaError_t enqueue_mechanism(MechBuffers& m, const StepBuffers& b, const MechPa
         if ((e = bearing_projection_iteration(m, b, p, s)) != cudaSuccess) return e;
     k_advance_coordinates<<<nblocks(p.body_count), kMBlock, 0, s>>>(b, m, p);
     if ((e = forward_kinematics(m, p, s)) != cudaSuccess) return e;
+    const uint32_t mode = g_closure_grid;
+    const bool grid = p.closures > 0 && (mode == 2u || (mode == 0u && p.closures >= kGridClosures));
     if (pcg_residual_mode(p)) {
         for (uint32_t step = 0; step < kClosureSteps; ++step) {
-            k_closure_eval<<<1, kClosureThreads, 0, s>>>(b, m, p, step);
+            if (grid) {
+                if ((e = launch_grid((const void*)k_closure_eval<true>, b, m, p, step, s)) != cudaSuccess) return e;
+            } else {
+                k_closure_eval<false><<<1, kClosureThreads, 0, s>>>(b, m, p, step);
+            }
             if (p.learned_precond) {
                 e = mlp::forward(m.precond_params, reinterpret_cast<const float*>(m.blk_feat), 0,
                                  &m.cstate->live_blocks, p.blocks, m.blk_out, 3, m.mlp_scratch, &b.diag->error_flags, s);
                 if (e != cudaSuccess) return e;
             }
-            k_closure_pcg<<<1, kClosureThreads, 0, s>>>(b, m, p, step);
+            if (grid) {
+                if ((e = launch_grid((const void*)k_closure_pcg<true>, b, m, p, step, s)) != cudaSuccess) return e;
+            } else {
+                k_closure_pcg<false><<<1, kClosureThreads, 0, s>>>(b, m, p, step);
+            }
         }
     } else if (p.closures > 0) {
-        const uint32_t mode = g_closure_grid;
-        const bool grid = mode == 2u || (mode == 0u && p.closures >= kGridClosures);
         if (grid) {
-            // one co-resident 1,024-thread block per SM (cooperative launch: grid barriers)
-            int dev = 0, sms = 0, per_sm = 0;
-            if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
-            if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
-            if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_closure_loop<true>, kClosureThreads, 0)) !=
-                cudaSuccess)
-                return e;
-            if (per_sm < 1) return cudaErrorInvalidConfiguration;
-            StepBuffers bb = b;
-            MechBuffers mm = m;
-            MechParams pp = p;
-            void* args[] = {&bb, &mm, &pp};
-            cudaLaunchConfig_t cfg = {};
-            cfg.gridDim = dim3((uint32_t)sms);
-            cfg.blockDim = dim3(kClosureThreads);
-            cfg.stream = s;
-            cudaLaunchAttribute attr[1];
-            attr[0].id = cudaLaunchAttributeCooperative;
-            attr[0].val.cooperative = 1;
-            cfg.attrs = attr;
-            cfg.numAttrs = 1;
-            if ((e = cudaLaunchKernelExC(&cfg, (const void*)k_closure_loop<true>, args)) != cudaSuccess) return e;
+            if ((e = launch_grid((const void*)k_closure_loop<true>, b, m, p, kNoStep, s)) != cudaSuccess) return e;
         } else {
             k_closure_loop<false><<<1, kClosureThreads, 0, s>>>(b, m, p);
         }

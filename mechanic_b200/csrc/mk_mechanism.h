@@ -76,6 +76,7 @@ struct MechBuffers {
     uint32_t* grid_barrier = nullptr;           // arrival word of the grid-wide closure loop (zero at rest)
     uint32_t* loop_state = nullptr;             // 12 steps x 2: largest residuals (um, udeg), zeroed per tick
     float* chunk_part = nullptr;                // 2 x chunks of 1,024 closure coordinates: dot-product sums
+    double* chunk_part_d = nullptr;             // the same in FP64 (closure PCG to a residual)
     uint32_t readback_iterations = 0;
     double readback_residual = 0.0;
     // MK_CLOSURE_PCG_RESIDUAL

@@ -1562,12 +1562,17 @@ template <class T> struct World : WorldBase {
         }
         return v[0];
     }
+    // The GPU's order: chunks of 1,024 coordinates (one per thread), the block
+    // tree per chunk, the chunk sums added in chunk order.
     template <class F> double closure_dot_d(F term) const {   // term(q) -> double
-        std::vector<double> part(1024, 0.0);
         const uint32_t NQ = (uint32_t)ct.cq_coords.size();
-        for (uint32_t t = 0; t < 1024; ++t)
-            for (uint32_t q = t; q < NQ; q += 1024) part[t] += term(q);
-        return block_sum_1024(part);
+        double acc = 0.0;
+        for (uint32_t c0 = 0; c0 < NQ; c0 += 1024) {
+            std::vector<double> part(1024, 0.0);
+            for (uint32_t t = 0; t < 1024 && c0 + t < NQ; ++t) part[t] = term(c0 + t);
+            acc += block_sum_1024(part);
+        }
+        return acc;
     }
     void closure_apply(const std::vector<T>& x, std::vector<T>& out) {
         const uint32_t NC = (uint32_t)ct.cl_bearings.size();

@@ -79,3 +79,34 @@ def test_learned_preconditioner_bitexact_given_outputs(cuda_lib):
                     params=init_params(9, out_scale=1.0))
     cs = orc.closure_stats()
     assert cs["learned_blocks"] + cs["rejected_blocks"] > 0
+
+
+def _closure_grid(mode):
+    from mechanic_b200 import physics
+    return physics.set_tuning(physics.TUNE_CLOSURE_GRID, mode)
+
+
+@pytest.mark.parametrize("precond", [abi.PRECOND_BLOCK_JACOBI, abi.PRECOND_PAIR_BLOCKS])
+def test_grid_closure_pcg_bitexact(cuda_lib, precond):
+    """The evaluate and PCG kernels spread over the whole cooperative grid (grid barriers
+    between phases) agree with the oracle bit for bit."""
+    cfg = learned.closure_config(max_iterations=64)
+    cfg.preconditioner = precond
+    prev = _closure_grid(2)
+    try:
+        _run(scenes.bearing_chains(chains=40, links=5, seed=1, closure_fraction=0.5, height=0.5), cfg, 6)
+    finally:
+        _closure_grid(max(prev, 0))
+
+
+def test_grid_and_block_closure_pcg_agree_and_match_oracle(cuda_lib):
+    """Above 1,024 closure coordinates the FP64 dot products sum per 1,024-coordinate
+    chunk in chunk order: one block and the whole grid give the oracle's values."""
+    scene = scenes.bearing_chains(chains=1500, links=5, seed=6, closure_fraction=0.2, height=0.5)
+    cfg = learned.closure_config()
+    for mode in (1, 2):
+        prev = _closure_grid(mode)
+        try:
+            _run(scene, cfg, 3)
+        finally:
+            _closure_grid(max(prev, 0))
