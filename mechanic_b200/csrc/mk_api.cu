@@ -21,7 +21,7 @@ namespace {
 
 thread_local std::string g_last_error;
 
-constexpr uint32_t kTickRing = 64;       // pinned tick-config slots in flight
+constexpr uint32_t kTickRing = 64;       // tick-config slots in flight
 constexpr uint32_t kStageEvents = 8;
 
 struct DeviceGuard {
@@ -83,10 +83,13 @@ struct MkHandle {
     cudaEvent_t slot_read[3] = {};
     bool slot_read_pending[3] = {};
     // host
-    mk::DevTick* h_tick = nullptr;      // pinned ring
+    mk::DevTick* h_tick = nullptr;      // tick rows as dispatched (a ring: at most kTickRing ticks in flight)
     GpuDiagnostics* h_diag = nullptr;   // pinned, written at the end of every tick
     mk::SolveStats* h_stats = nullptr;  // pinned, contact solve outcome (residual mode)
     mk::ClosureState* h_cstate = nullptr;   // pinned, closure solve outcome (MK_CLOSURE_PCG_RESIDUAL)
+    GpuDiagnostics* d_diag = nullptr;   // the three pinned rows above as device addresses
+    mk::SolveStats* d_stats = nullptr;
+    mk::ClosureState* d_cstate = nullptr;
     bool residual = false;              // contact solve runs to a residual
     float* warm_params = nullptr;       // warm-start network parameters (device, mlp::kParams)
     void* mlp_scratch = nullptr;        // bf16 weights + partials of the network kernels
@@ -224,6 +227,31 @@ uint64_t carve(MkHandle* h, char* base) {
     return c.off;
 }
 
+// The tick's config row, passed by value.  A host-to-device copy there is a
+// copy-engine operation between two ticks: it queues behind a snapshot read
+// in flight on the copy engines and holds the next tick back by the read's
+// length.
+__global__ void k_set_tick(mk::DevTick* dst, mk::DevTick v) {
+    if (threadIdx.x == 0) *dst = v;
+}
+
+// End-of-tick host rows (diagnostics, solve outcomes), stored by the device
+// into pinned host memory mapped into its address space: no copy-engine
+// operation inside the tick either.
+struct HostRows {
+    const uint32_t* src[3];
+    uint32_t* dst[3];
+    uint32_t words[3];
+    uint32_t count;
+};
+__global__ void k_publish_host_rows(HostRows r) {
+    for (uint32_t c = 0; c < r.count; ++c)
+        for (uint32_t i = threadIdx.x; i < r.words[c]; i += blockDim.x) r.dst[c][i] = __ldcg(r.src[c] + i);
+    __threadfence_system();
+}
+static_assert(sizeof(GpuDiagnostics) % 4 == 0 && sizeof(mk::SolveStats) % 4 == 0 &&
+              sizeof(mk::ClosureState) % 4 == 0, "host rows are copied as 32-bit words");
+
 // The full tick on `stream` (captured into a graph or launched directly).
 cudaError_t enqueue_tick(MkHandle* h, int parity, bool capturing) {
     cudaStream_t s = h->stream;
@@ -316,10 +344,20 @@ cudaError_t enqueue_tick(MkHandle* h, int parity, bool capturing) {
     if ((e = mark(6)) != cudaSuccess) return e;
     if (!fuse && (e = mk::launch_snapshot(b, h->params, s)) != cudaSuccess) return e;
     if (h->collisions && (e = mk::launch_finish_tick(b, h->params, parity, s)) != cudaSuccess) return e;
-    cudaMemcpyAsync(h->h_diag, b.diag, sizeof(GpuDiagnostics), cudaMemcpyDeviceToHost, s);
-    if (h->residual) cudaMemcpyAsync(h->h_stats, b.solve_stats, sizeof(mk::SolveStats), cudaMemcpyDeviceToHost, s);
-    if (h->mechanism_active && mk::pcg_residual_mode(h->mech_params))
-        cudaMemcpyAsync(h->h_cstate, h->mech.cstate, sizeof(mk::ClosureState), cudaMemcpyDeviceToHost, s);
+    {
+        HostRows r{};
+        auto add = [&](const void* src, void* dst, size_t bytes) {
+            r.src[r.count] = static_cast<const uint32_t*>(src);
+            r.dst[r.count] = static_cast<uint32_t*>(dst);
+            r.words[r.count] = (uint32_t)(bytes / 4);
+            ++r.count;
+        };
+        add(b.diag, h->d_diag, sizeof(GpuDiagnostics));
+        if (h->residual) add(b.solve_stats, h->d_stats, sizeof(mk::SolveStats));
+        if (h->mechanism_active && mk::pcg_residual_mode(h->mech_params))
+            add(h->mech.cstate, h->d_cstate, sizeof(mk::ClosureState));
+        k_publish_host_rows<<<1, 32, 0, s>>>(r);
+    }
     if ((e = mark(7)) != cudaSuccess) return e;
     return cudaGetLastError();
 }
@@ -669,6 +707,9 @@ int create_impl(const MkCreation* cr, const MkConfig* config, const MkCapacities
     ok = ok && check(cudaMallocHost(&h->h_diag, sizeof(GpuDiagnostics)), err, "pinned diagnostics");
     ok = ok && check(cudaMallocHost(&h->h_stats, sizeof(mk::SolveStats)), err, "pinned solve stats");
     ok = ok && check(cudaMallocHost(&h->h_cstate, sizeof(mk::ClosureState)), err, "pinned closure state");
+    ok = ok && check(cudaHostGetDevicePointer((void**)&h->d_diag, h->h_diag, 0), err, "mapped diagnostics");
+    ok = ok && check(cudaHostGetDevicePointer((void**)&h->d_stats, h->h_stats, 0), err, "mapped solve stats");
+    ok = ok && check(cudaHostGetDevicePointer((void**)&h->d_cstate, h->h_cstate, 0), err, "mapped closure state");
     for (uint32_t i = 0; ok && i < kTickRing; ++i)
         ok = check(cudaEventCreateWithFlags(&h->tick_done[i], cudaEventDisableTiming), err, "event");
     for (uint32_t i = 0; ok && i < kStageEvents; ++i) ok = check(cudaEventCreate(&h->stage[i]), err, "event");
@@ -840,7 +881,10 @@ int mk_dispatch_tick(MkHandle* h, uint64_t tick_index, MkSubmission* out) {
         e = cudaStreamWaitEvent(h->stream, h->slot_read[snap], 0);
         h->slot_read_pending[snap] = false;
     }
-    if (e == cudaSuccess) e = cudaMemcpyAsync(h->buf.tick, &t, sizeof(t), cudaMemcpyHostToDevice, h->stream);
+    if (e == cudaSuccess) {
+        k_set_tick<<<1, 32, 0, h->stream>>>(h->buf.tick, t);
+        e = cudaGetLastError();
+    }
     const int parity = h->parity;
     if (e == cudaSuccess) {
         if (h->graph[parity]) e = cudaGraphLaunch(h->graph[parity], h->stream);

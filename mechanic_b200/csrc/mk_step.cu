@@ -367,6 +367,77 @@ __device__ __forceinline__ Box2 ld_box(const float4* p) { return {__ldg(p), __ld
 __device__ __forceinline__ Box2 ld_box_cg(const float4* p) { return {__ldcg(p), __ldcg(p + 1)}; }
 __device__ __forceinline__ void st_box(float4* p, Box2 v) { p[0] = v.mn; p[1] = v.mx; }
 
+// Per internal node: its union box and a 4-wide traversal record (128 bytes,
+// one cache line) holding its grandchildren in leaf order -- a leaf child is
+// one entry, an internal child gives its two children -- so a traversal step
+// descends two levels with one load.  Entry: {min.xyz, code} {max.xyz, last
+// leaf}, code = child node index or kLeafCode | collider index; unused
+// trailing entries are zero (last leaf 0).  An entry's first leaf is one past
+// the last leaf of the entry before it (the first entry starts where the node
+// does).
+struct TravEntry {
+    Box2 box;
+    uint32_t code, last;
+};
+__device__ __forceinline__ void store_record(float4* rec, const TravEntry (&e)[4], uint32_t m) {
+#pragma unroll
+    for (uint32_t k = 0; k < 4; ++k) {
+        if (k < m) {
+            rec[2 * k] = make_float4(e[k].box.mn.x, e[k].box.mn.y, e[k].box.mn.z, __uint_as_float(e[k].code));
+            rec[2 * k + 1] = make_float4(e[k].box.mx.x, e[k].box.mx.y, e[k].box.mx.z, __uint_as_float(e[k].last));
+        } else {
+            rec[2 * k] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+            rec[2 * k + 1] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        }
+    }
+}
+
+// Traversal records of the in-chunk nodes, written by the warp that owns the
+// chunk: every descendant of a node whose leaf range lies in one 32-leaf
+// chunk is an internal node or leaf of that chunk (Karras node c sits at one
+// end of its range), so children come from the lane c & 31 and boxes from
+// the lane of the node or leaf -- no global reads besides the node's own
+// children.  `v`/`j` are this lane's leaf box and collider index, `r` its
+// node's box (valid where `inner`).  Every lane takes part in the shuffles.
+__device__ __forceinline__ void write_chunk_records(const StepBuffers& b, bool inner, uint2 rg, Box2 r, Box2 v,
+                                                    uint32_t j, uint32_t t, uint32_t leaf_base, uint32_t lane) {
+    const uint2 ch = inner ? b.children[t] : make_uint2(0u, 0u);
+    const Box2 nb = inner ? r : box_empty();
+    auto lane_of_node = [&](uint32_t c) { return inner && c < leaf_base ? (c & 31u) : lane; };
+    const uint32_t lx = lane_of_node(ch.x), ly = lane_of_node(ch.y);
+    const uint2 cl = make_uint2(__shfl_sync(0xffffffffu, ch.x, lx), __shfl_sync(0xffffffffu, ch.y, lx));
+    const uint2 cr = make_uint2(__shfl_sync(0xffffffffu, ch.x, ly), __shfl_sync(0xffffffffu, ch.y, ly));
+    const uint32_t split = ch.x >= leaf_base ? ch.x - leaf_base : ch.x;
+    // slots: left child's (one leaf, or its two children), then the right's
+    uint32_t node[4], first[4], last[4];
+    bool use[4];
+    auto child = [&](uint32_t s, uint32_t c, uint2 cc, uint32_t f, uint32_t l) {
+        if (c >= leaf_base) {   // a leaf child: one entry
+            node[s] = c; first[s] = f; last[s] = f; use[s] = true;
+            node[s + 1] = 0u; first[s + 1] = 0u; last[s + 1] = 0u; use[s + 1] = false;
+        } else {
+            const uint32_t sp = cc.x >= leaf_base ? cc.x - leaf_base : cc.x;
+            node[s] = cc.x; first[s] = f; last[s] = sp; use[s] = true;
+            node[s + 1] = cc.y; first[s + 1] = sp + 1u; last[s + 1] = l; use[s + 1] = true;
+        }
+    };
+    child(0, ch.x, cl, rg.x, split);
+    child(2, ch.y, cr, split + 1u, rg.y);
+    TravEntry sl[4];
+#pragma unroll
+    for (uint32_t s = 0; s < 4; ++s) {
+        const bool leaf = node[s] >= leaf_base;
+        const uint32_t src = inner && use[s] ? (leaf ? first[s] & 31u : node[s] & 31u) : lane;
+        const Box2 lb = shfl_box_idx(v, src), ib = shfl_box_idx(nb, src);
+        const uint32_t jj = __shfl_sync(0xffffffffu, j, src);
+        sl[s] = {leaf ? lb : ib, leaf ? (kLeafCode | jj) : node[s], last[s]};
+    }
+    // compact in leaf order: a leaf child leaves its second slot empty
+    const bool li = use[1], ri = use[3];
+    const TravEntry e[4] = {sl[0], li ? sl[1] : sl[2], li ? sl[2] : sl[3], sl[3]};
+    if (inner) store_record(b.node_records + 8ull * t, e, (li ? 2u : 1u) + (ri ? 2u : 1u));
+}
+
 // Leaf boxes in sorted order, their prefix/suffix unions within 32-leaf chunks,
 // the boxes of the internal nodes whose leaf range lies inside one chunk (from
 // a warp sparse table; Karras node i's range has i at one end, so the warp of
@@ -380,8 +451,8 @@ __global__ void __launch_bounds__(kRefitBlock) k_refit_leaves(StepBuffers b, Ste
     const uint32_t lane = lane_id(), w = warp_id();
     const uint32_t leaf_base = n - 1;
     Box2 v = box_empty();
+    const uint32_t j = t < n ? b.svals[t] : 0u;
     if (t < n) {
-        const uint32_t j = b.svals[t];
         float4 mn = b.aabbs[2ull * j], mx = b.aabbs[2ull * j + 1];
         mn.w = __uint_as_float(t);
         b.node_aabbs[2ull * (leaf_base + t)] = mn;
@@ -414,6 +485,7 @@ __global__ void __launch_bounds__(kRefitBlock) k_refit_leaves(StepBuffers b, Ste
             b.node_aabbs[2ull * t] = make_float4(r.mn.x, r.mn.y, r.mn.z, __uint_as_float(rg.y));
             b.node_aabbs[2ull * t + 1] = make_float4(r.mx.x, r.mx.y, r.mx.z, 0.0f);
         }
+        write_chunk_records(b, inner, rg, r, v, j, t, leaf_base, lane);
     }
     if (lane == 31) s_chunk[w] = pre;
     __syncthreads();
@@ -503,26 +575,16 @@ __device__ Box2 range_box(const StepBuffers& b, uint32_t n, uint32_t f, uint32_t
     return u;
 }
 
-// Per internal node: its union box and a 4-wide traversal record (128 bytes,
-// one cache line) holding its grandchildren in leaf order -- a leaf child is
-// one entry, an internal child gives its two children -- so a traversal step
-// descends two levels with one load.  Entry: {min.xyz, code} {max.xyz, last
-// leaf}, code = child node index or kLeafCode | collider index; unused
-// trailing entries have last leaf 0.  An entry's first leaf is one past the
-// last leaf of the entry before it (the first entry starts where the node
-// does).
-struct TravEntry {
-    Box2 box;
-    uint32_t code, last;
-};
-
+// Cross-chunk internal nodes: their union box and traversal record (in-chunk
+// nodes got both from k_refit_leaves).
 __global__ void __launch_bounds__(kBlock) k_refit_nodes(StepBuffers b, StepParams p) {
     const uint32_t n = p.collider_count;
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (n <= 1 || i >= n - 1) return;
     const uint32_t leaf_base = n - 1;
-    const uint2 ch = b.children[i];
     const uint2 rg = b.node_ranges[i];
+    if ((rg.x >> 5) == (rg.y >> 5)) return;
+    const uint2 ch = b.children[i];
     const uint32_t split = ch.x >= leaf_base ? ch.x - leaf_base : ch.x;
     // children's children (Karras: an internal node's left child covers [first, split])
     const uint2 cl = ch.x < leaf_base ? b.children[ch.x] : make_uint2(0u, 0u);
@@ -551,23 +613,13 @@ __global__ void __launch_bounds__(kBlock) k_refit_nodes(StepBuffers b, StepParam
         e[m++] = {box_of(cr.x, split + 1, s), code_of(cr.x), s};
         e[m++] = {box_of(cr.y, s + 1, rg.y), code_of(cr.y), rg.y};
     }
-    float4* rec = b.node_records + 8ull * i;
+    store_record(b.node_records + 8ull * i, e, m);
     Box2 u = box_empty();
 #pragma unroll
-    for (uint32_t k = 0; k < 4; ++k) {
-        if (k < m) {
-            u = box_union(u, e[k].box);
-            rec[2 * k] = make_float4(e[k].box.mn.x, e[k].box.mn.y, e[k].box.mn.z, __uint_as_float(e[k].code));
-            rec[2 * k + 1] = make_float4(e[k].box.mx.x, e[k].box.mx.y, e[k].box.mx.z, __uint_as_float(e[k].last));
-        } else {
-            rec[2 * k] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-            rec[2 * k + 1] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-        }
-    }
-    if ((rg.x >> 5) != (rg.y >> 5)) {   // in-chunk nodes were written by k_refit_leaves
-        b.node_aabbs[2ull * i] = make_float4(u.mn.x, u.mn.y, u.mn.z, __uint_as_float(rg.y));
-        b.node_aabbs[2ull * i + 1] = make_float4(u.mx.x, u.mx.y, u.mx.z, 0.0f);
-    }
+    for (uint32_t k = 0; k < 4; ++k)
+        if (k < m) u = box_union(u, e[k].box);
+    b.node_aabbs[2ull * i] = make_float4(u.mn.x, u.mn.y, u.mn.z, __uint_as_float(rg.y));
+    b.node_aabbs[2ull * i + 1] = make_float4(u.mx.x, u.mx.y, u.mx.z, 0.0f);
 }
 
 // ---------------------------------------------------------------- traverse
@@ -593,6 +645,7 @@ __device__ __forceinline__ bool pair_is_suppressed(const uint2* __restrict__ sup
 }
 
 constexpr uint32_t kStack = 64;
+constexpr uint32_t kNoNode = 0xffffffffu;
 constexpr uint32_t kTravThreads = 128;
 constexpr uint32_t kStage = 512;   // pair keys staged per warp in shared memory
 
@@ -630,6 +683,11 @@ __global__ void __launch_bounds__(kTravThreads) k_traverse(StepBuffers b, StepPa
             float4 r[8];
 #pragma unroll
             for (int q = 0; q < 8; ++q) r[q] = __ldg(rec + q);
+            // the first overlapping internal entry is visited next without a
+            // trip through the stack (the pair keys are sorted afterwards, so
+            // the visiting order does not matter)
+            uint32_t next = kNoNode;
+            bool overflow = false;
 #pragma unroll
             for (int k = 0; k < 4; ++k) {
                 const float4 cmin = r[2 * k], cmax = r[2 * k + 1];
@@ -651,14 +709,21 @@ __global__ void __launch_bounds__(kTravThreads) k_traverse(StepBuffers b, StepPa
                         const uint32_t g = atomicAdd(found, 1u);
                         if (g < p.pair_capacity) b.pair_stage[g] = key;
                     }
+                } else if (next == kNoNode) {
+                    next = code;
                 } else {
                     if (sp >= kStack) {   // lbvh.wgsl:389-392
                         atomicOr(&b.diag->error_flags, MK_PAIR_OVERFLOW_FLAG);
-                        sp = 0;
+                        overflow = true;
                         break;
                     }
                     stack[sp++] = code;
                 }
+            }
+            if (overflow) break;
+            if (next != kNoNode) {
+                node = next;
+                continue;
             }
             if (sp == 0) break;
             node = stack[--sp];
@@ -867,6 +932,9 @@ __global__ void __launch_bounds__(kBlock, 3) k_narrowphase(StepBuffers b, StepPa
         if (found > p.pair_capacity) atomicOr(&b.diag->error_flags, MK_PAIR_OVERFLOW_FLAG);
     }
     const uint32_t tiles = (n + kBlock - 1) / kBlock;
+    // the grid is sized for the capacity: CTAs past the tile count leave
+    // before taking a ticket (block 0 stays for the empty-list counts)
+    if (blockIdx.x != 0 && blockIdx.x >= tiles) return;
     for (;;) {
         const uint32_t tile = take_tile(site.ticket, &s_tile);
         if (tile >= tiles) break;
@@ -1055,6 +1123,7 @@ __global__ void __launch_bounds__(kBlock) k_prepare(StepBuffers b, StepParams p,
     const uint2* index_prev = b.contact_index + 2ull * C * ((tick - 1u) & 1u);
     const bool indexed = prev_ok && b.counts->prev_indexed != 0u;
     const uint32_t narrow_now = b.counts->narrow;
+    if (blockIdx.x != 0 && blockIdx.x >= tiles) return;   // as in k_narrowphase
     for (;;) {
         const uint32_t tile = take_tile(site.ticket, &s_tile);
         if (tile >= tiles) break;
