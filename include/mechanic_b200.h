@@ -472,7 +472,7 @@ MK_API uint32_t mk_tick_kernel_count(const MkHandle* handle);
  * operation is launched.  Keys: MK_TUNE_SORT_ITEMS (keys per thread of a
  * radix-sort tile: 2, 4, 6, 8, 11 or 16; 0 = size-based default);
  * MK_TUNE_CLOSURE_GRID (the closure solves, the reference's loop and the PCG
- * to a residual: 0 = by size, one block below 256 closures and the whole grid
+ * to a residual: 0 = by size, one block below 512 closures and the whole grid
  * from there, 1 = always one block, 2 = always the grid; both give the same
  * results).  Returns the
  * previous value, or -1 for an unknown key. */

@@ -161,7 +161,7 @@ uint64_t carve(MkHandle* h, char* base) {
     b.svals = c.take<uint32_t>(C);
     b.children = c.take<uint2>(C);
     b.parents = c.take<uint32_t>(2ull * C);
-    b.visits = c.take<uint32_t>(C);
+    b.cross_nodes = c.take<uint32_t>(C);
     b.scene_bounds = c.take<uint32_t>(8);
     b.node_ranges = c.take<uint2>(C);
     b.leaf_scan = c.take<float4>(4ull * C);

@@ -33,7 +33,8 @@ struct DevCounts {
     uint32_t active;           // active contacts
     uint32_t pairs_found;      // candidate pairs found by the traversal
     uint32_t requested_contacts;
-    uint32_t reset_pad[2];
+    uint32_t cross_nodes;      // entries of StepBuffers::cross_nodes
+    uint32_t reset_pad;
     // carried across ticks
     uint32_t prev_narrow;      // previous tick: narrowphase contacts
     uint32_t prev_contacts;    // previous tick: all contacts
@@ -122,7 +123,7 @@ struct StepBuffers {
     uint32_t* svals;
     uint2* children;             // C-1
     uint32_t* parents;           // 2C-1
-    uint32_t* visits;            // C-1
+    uint32_t* cross_nodes;       // C-1: this tick's internal nodes whose leaf range crosses a 32-leaf chunk
     uint2* node_ranges;          // C-1: first and last sorted leaf below each internal node
     float4* leaf_scan;           // 4 per leaf: prefix and suffix unions within its 32-leaf chunk
     float4* chunk_scan;          // 6 per chunk: total, prefix and suffix unions within its 1024-leaf super-chunk

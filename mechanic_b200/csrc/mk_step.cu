@@ -486,6 +486,15 @@ __global__ void __launch_bounds__(kRefitBlock) k_refit_leaves(StepBuffers b, Ste
             b.node_aabbs[2ull * t + 1] = make_float4(r.mx.x, r.mx.y, r.mx.z, 0.0f);
         }
         write_chunk_records(b, inner, rg, r, v, j, t, leaf_base, lane);
+        // the other internal nodes, listed for k_refit_nodes (one reservation per warp)
+        const bool cross = n > 1 && t < n - 1 && !inner;
+        const uint32_t cm = __ballot_sync(0xffffffffu, cross);
+        if (cm) {
+            uint32_t base = 0;
+            if (lane == 0) base = atomicAdd(&b.counts->cross_nodes, (uint32_t)__popc(cm));
+            base = __shfl_sync(0xffffffffu, base, 0);
+            if (cross) b.cross_nodes[base + __popc(cm & ((1u << lane) - 1u))] = t;
+        }
     }
     if (lane == 31) s_chunk[w] = pre;
     __syncthreads();
@@ -575,15 +584,10 @@ __device__ Box2 range_box(const StepBuffers& b, uint32_t n, uint32_t f, uint32_t
     return u;
 }
 
-// Cross-chunk internal nodes: their union box and traversal record (in-chunk
-// nodes got both from k_refit_leaves).
-__global__ void __launch_bounds__(kBlock) k_refit_nodes(StepBuffers b, StepParams p) {
-    const uint32_t n = p.collider_count;
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (n <= 1 || i >= n - 1) return;
+// The box and traversal record of internal node i, whose leaf range crosses a chunk.
+__device__ __forceinline__ void refit_cross_node(const StepBuffers& b, uint32_t n, uint32_t i) {
     const uint32_t leaf_base = n - 1;
     const uint2 rg = b.node_ranges[i];
-    if ((rg.x >> 5) == (rg.y >> 5)) return;
     const uint2 ch = b.children[i];
     const uint32_t split = ch.x >= leaf_base ? ch.x - leaf_base : ch.x;
     // children's children (Karras: an internal node's left child covers [first, split])
@@ -597,22 +601,27 @@ __global__ void __launch_bounds__(kBlock) k_refit_nodes(StepBuffers b, StepParam
         if ((f >> 5) == (l >> 5)) return ld_box(b.node_aabbs + 2ull * c);
         return range_box(b, n, f, l);
     };
-    TravEntry e[4];
-    uint32_t m = 0;
-    if (ch.x >= leaf_base) {
-        e[m++] = {leaf_box(b, leaf_base, rg.x), code_of(ch.x), rg.x};
+    // slots: the left child's entries (one leaf, or its two children), then the right's
+    const bool li = ch.x < leaf_base, ri = ch.y < leaf_base;
+    TravEntry sl[4];
+    sl[1] = sl[3] = {box_empty(), 0u, 0u};
+    if (!li) {
+        sl[0] = {leaf_box(b, leaf_base, rg.x), code_of(ch.x), rg.x};
     } else {
         const uint32_t s = split_of(cl.x);
-        e[m++] = {box_of(cl.x, rg.x, s), code_of(cl.x), s};
-        e[m++] = {box_of(cl.y, s + 1, split), code_of(cl.y), split};
+        sl[0] = {box_of(cl.x, rg.x, s), code_of(cl.x), s};
+        sl[1] = {box_of(cl.y, s + 1, split), code_of(cl.y), split};
     }
-    if (ch.y >= leaf_base) {
-        e[m++] = {leaf_box(b, leaf_base, rg.y), code_of(ch.y), rg.y};
+    if (!ri) {
+        sl[2] = {leaf_box(b, leaf_base, rg.y), code_of(ch.y), rg.y};
     } else {
         const uint32_t s = split_of(cr.x);
-        e[m++] = {box_of(cr.x, split + 1, s), code_of(cr.x), s};
-        e[m++] = {box_of(cr.y, s + 1, rg.y), code_of(cr.y), rg.y};
+        sl[2] = {box_of(cr.x, split + 1, s), code_of(cr.x), s};
+        sl[3] = {box_of(cr.y, s + 1, rg.y), code_of(cr.y), rg.y};
     }
+    // compacted in leaf order with static indices (no local-memory array)
+    const TravEntry e[4] = {sl[0], li ? sl[1] : sl[2], li ? sl[2] : sl[3], sl[3]};
+    const uint32_t m = (li ? 2u : 1u) + (ri ? 2u : 1u);
     store_record(b.node_records + 8ull * i, e, m);
     Box2 u = box_empty();
 #pragma unroll
@@ -622,6 +631,17 @@ __global__ void __launch_bounds__(kBlock) k_refit_nodes(StepBuffers b, StepParam
     b.node_aabbs[2ull * i + 1] = make_float4(u.mx.x, u.mx.y, u.mx.z, 0.0f);
 }
 
+// Cross-chunk internal nodes: their union box and traversal record (in-chunk
+// nodes got both from k_refit_leaves, which listed the others; a list keeps
+// the warps dense where a grid over every node would leave each with a few
+// active lanes).
+__global__ void __launch_bounds__(kBlock) k_refit_nodes(StepBuffers b, StepParams p) {
+    const uint32_t n = p.collider_count;
+    if (n <= 1) return;
+    const uint32_t count = b.counts->cross_nodes;
+    for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < count; q += gridDim.x * blockDim.x)
+        refit_cross_node(b, n, b.cross_nodes[q]);
+}
 // ---------------------------------------------------------------- traverse
 __device__ __forceinline__ bool overlaps(float4 amin, float4 amax, float4 bmin, float4 bmax) {
     return amin.x <= bmax.x && amin.y <= bmax.y && amin.z <= bmax.z && bmin.x <= amax.x && bmin.y <= amax.y &&
@@ -2152,7 +2172,8 @@ cudaError_t launch_broadphase(const StepBuffers& b, const StepParams& p, const S
     k_karras<<<blocks_for(C, kBlock), kBlock, 0, s>>>(b, p);
     k_refit_leaves<<<blocks_for(C, kRefitBlock), kRefitBlock, 0, s>>>(b, p);
     k_refit_super<<<1, 1024, 0, s>>>(b, p);
-    k_refit_nodes<<<blocks_for(C, kBlock), kBlock, 0, s>>>(b, p);
+    // persistent over the listed nodes (their count is known on the device only)
+    k_refit_nodes<<<std::min<uint32_t>(blocks_for(C, kBlock), (uint32_t)l.sm_count * 2u), kBlock, 0, s>>>(b, p);
     k_traverse<<<blocks_for(C, kTravThreads), kTravThreads, 0, s>>>(b, p);
     e = launch_sort(b.pair_stage, nullptr, b.pair_keys, nullptr, p.pair_capacity, &b.counts->pairs_found,
                     2 * p.pair_shift, b.pair_sort_scratch, b.pair_sort_scratch_bytes, &b.diag->error_flags, s,
