@@ -677,6 +677,7 @@ constexpr uint32_t kStage = 512;   // pair keys staged per warp in shared memory
 // (min index << shift) | max index into a per-warp shared-memory stage that
 // is flushed with one global reservation; the keys are radix-sorted next,
 // which yields the canonical (collider_a, collider_b) order.
+template <bool kBatched>
 __global__ void __launch_bounds__(kTravThreads) k_traverse(StepBuffers b, StepParams p) {
     __shared__ uint64_t s_stage[kTravThreads / 32][kStage];
     __shared__ uint32_t s_count[kTravThreads / 32];
@@ -694,7 +695,7 @@ __global__ void __launch_bounds__(kTravThreads) k_traverse(StepBuffers b, StepPa
         // batched scenes: candidates end where this collider's scene ends in sorted order
         // (a right child starts one past its left sibling's last leaf; left children start
         // where their parent does, which was already below the limit)
-        const uint32_t limit = b.collider_scene ? __ldg(b.scene_end + b.collider_scene[i]) : n;
+        const uint32_t limit = kBatched ? __ldg(b.scene_end + b.collider_scene[i]) : n;
         uint32_t stack[kStack];
         uint32_t sp = 0;
         uint32_t node = 0;
@@ -712,7 +713,7 @@ __global__ void __launch_bounds__(kTravThreads) k_traverse(StepBuffers b, StepPa
             for (int k = 0; k < 4; ++k) {
                 const float4 cmin = r[2 * k], cmax = r[2 * k + 1];
                 if (__float_as_uint(cmax.w) <= t) continue;     // nothing to the right of this leaf below
-                if (k > 0 && __float_as_uint(r[2 * k - 1].w) + 1u >= limit) continue;   // starts past this scene
+                if (kBatched && k > 0 && __float_as_uint(r[2 * k - 1].w) + 1u >= limit) continue;   // past the scene
                 if (!overlaps(qmin, qmax, cmin, cmax)) continue;
                 const uint32_t code = __float_as_uint(cmin.w);
                 if (code & kLeafCode) {
@@ -2174,7 +2175,8 @@ cudaError_t launch_broadphase(const StepBuffers& b, const StepParams& p, const S
     k_refit_super<<<1, 1024, 0, s>>>(b, p);
     // persistent over the listed nodes (their count is known on the device only)
     k_refit_nodes<<<std::min<uint32_t>(blocks_for(C, kBlock), (uint32_t)l.sm_count * 2u), kBlock, 0, s>>>(b, p);
-    k_traverse<<<blocks_for(C, kTravThreads), kTravThreads, 0, s>>>(b, p);
+    if (b.collider_scene) k_traverse<true><<<blocks_for(C, kTravThreads), kTravThreads, 0, s>>>(b, p);
+    else k_traverse<false><<<blocks_for(C, kTravThreads), kTravThreads, 0, s>>>(b, p);
     e = launch_sort(b.pair_stage, nullptr, b.pair_keys, nullptr, p.pair_capacity, &b.counts->pairs_found,
                     2 * p.pair_shift, b.pair_sort_scratch, b.pair_sort_scratch_bytes, &b.diag->error_flags, s,
                     l.sm_count, kPairSortItems, 0, true);
