@@ -373,6 +373,9 @@ enum {
                                       {position column xyz, coordinate (u32 bits)}, {axis column xyz, closure (u32)} */
     MK_BUF_CLOSURE_BLOCKS = 15,    /* float[blocks][16] preconditioner network inputs of the same step */
     MK_BUF_CLOSURE_BLOCK_OUTPUTS = 16, /* float[12][blocks][3] (t11, t12, t22) the network gave at each Newton step */
+    MK_BUF_NODE_RECORDS = 17,      /* float4[8] per internal node (collider_count-1): its traversal record, up to
+                                      four grandchildren in leaf order as {min.xyz, code} {max.xyz, last leaf};
+                                      code = node index or 0x80000000 | collider index; unused entries zero */
 };
 
 /* ---------------------------------------------------------------------------

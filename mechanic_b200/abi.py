@@ -217,6 +217,7 @@ BUF_WARM_FEATURES = 13
 BUF_CLOSURE_SLOTS = 14
 BUF_CLOSURE_BLOCKS = 15
 BUF_CLOSURE_BLOCK_OUTPUTS = 16
+BUF_NODE_RECORDS = 17
 
 
 def ptr(a: np.ndarray | None) -> int | None:

@@ -1418,6 +1418,7 @@ int mk_read_buffer(MkHandle* h, uint32_t id, void* host, uint64_t cap_bytes, uin
         case MK_BUF_COLLIDER_AABBS: src = b.aabbs; n = h->C; row = 32; break;
         case MK_BUF_NODE_CHILDREN: src = b.children; n = h->C ? h->C - 1 : 0; row = 8; break;
         case MK_BUF_NODE_AABBS: src = b.node_aabbs; n = h->C ? 2ull * h->C - 1 : 0; row = 32; break;
+        case MK_BUF_NODE_RECORDS: src = b.node_records; n = h->C > 1 ? h->C - 1ull : 0; row = 128; break;
         case MK_BUF_PAIRS: src = b.pair_keys; n = counts.pairs; row = 8; break;
         case MK_BUF_CONTACTS: src = b.contacts[last]; n = counts.contacts; row = 64; break;
         case MK_BUF_ACTIVE: src = b.active; n = counts.active; row = 4; break;

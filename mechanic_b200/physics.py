@@ -492,6 +492,11 @@ class GpuPhysics:
         """(2C - 1, 8) float32: min.xyz, w, max.xyz, 0 per node (internal nodes first, then sorted leaves)."""
         return self.read_buffer(abi.BUF_NODE_AABBS, np.float32, 32).reshape(-1, 8)
 
+    def node_records(self):
+        """(C - 1, 32) float32: the 4-wide traversal record of each internal node, entries
+        {min.xyz, code bits} {max.xyz, last-leaf bits} of its grandchildren in leaf order."""
+        return self.read_buffer(abi.BUF_NODE_RECORDS, np.float32, 128).reshape(-1, 32)
+
     def world_masses(self):
         return self.read_buffer(abi.BUF_WORLD_MASSES, np.float32, 48).reshape(-1, 12)
 

@@ -147,6 +147,55 @@ def test_node_boxes_are_leaf_range_unions(cuda_lib):
             assert nodes[x, 3:4].view(np.uint32)[0] == last[x]
 
 
+def _expected_records(ch, nodes, vals):
+    """Traversal records rebuilt from the topology and node boxes: per internal node its
+    grandchildren in leaf order (a leaf child is one entry), {min.xyz, code} {max.xyz, last}."""
+    I = len(ch)
+    u = nodes.view(np.uint32)
+    rec = np.zeros((I, 32), np.float32)
+    ru = rec.view(np.uint32)
+
+    def entry(c):
+        row = nodes[c]
+        if c >= I:
+            return row[0:3], row[4:7], 0x80000000 | int(vals[c - I]), c - I
+        return row[0:3], row[4:7], c, int(u[c, 3])
+
+    for x in range(I):
+        ents = []
+        for c in ch[x]:
+            ents += [entry(int(c))] if c >= I else [entry(int(g)) for g in ch[c]]
+        for k, (mn, mx, code, last) in enumerate(ents):
+            rec[x, 8 * k:8 * k + 3] = mn
+            ru[x, 8 * k + 3] = code
+            rec[x, 8 * k + 4:8 * k + 7] = mx
+            ru[x, 8 * k + 7] = last
+    return rec
+
+
+@pytest.mark.parametrize("scene_fn", [lambda: scenes.falling_cubes(20, seed=3),
+                                      lambda: scenes.falling_cubes(40, seed=3),
+                                      lambda: scenes.stack_grid(14, 9, 14, seed=11)],
+                         ids=["20-colliders", "40-colliders", "stack-grid"])
+def test_traversal_records_match_tree(cuda_lib, scene_fn):
+    """Each internal node's 4-wide traversal record holds exactly its grandchildren in leaf
+    order with their node or leaf boxes, codes and last leaves: records of nodes inside one
+    32-leaf chunk come from the leaf refit's warp lanes, the others from the cross-chunk list."""
+    scene = scene_fn()
+    gpu = GpuPhysics(scene, GpuPhysicsConfig(), capacities={"pair_capacity": 1 << 22})
+    for tick in range(1, 4):
+        gpu.dispatch_tick(tick)
+        gpu.wait()
+        ch = gpu.node_children().astype(np.int64)
+        nodes = gpu.node_aabbs()
+        _, vals = gpu.sorted_entries()
+        want = _expected_records(ch, nodes, vals)
+        got = gpu.node_records()
+        assert got.shape == want.shape
+        bad = np.nonzero((got.view(np.uint32) != want.view(np.uint32)).any(axis=1))[0]
+        assert len(bad) == 0, f"tick {tick}: {len(bad)} records differ, first nodes {bad[:5]}"
+
+
 def test_snapshot_reads_overlap_later_ticks(cuda_lib):
     """A snapshot read waits for the tick that last wrote its slot, not for ticks dispatched
     after it, and a tick that rewrites a slot waits for a read of it: reading tick k's slot
