@@ -183,9 +183,9 @@ void carve_mechanism(MechBuffers& m, const MechParams& p, uint32_t B, uint32_t J
     m.chunk_part = f32(2ull * ((p.closure_coords + kClosureThreads - 1) / kClosureThreads));
     m.chunk_part_d = reinterpret_cast<double*>(take(16ull * ((p.closure_coords + kClosureThreads - 1) / kClosureThreads + 1)));
     m.links_final = p.final_is_a ? m.links_a : m.links_b;
+    m.slot_v = reinterpret_cast<float4*>(take(32ull * (p.slots ? p.slots : 1)));   // Jacobian columns
     if (pcg_residual_mode(p)) {
         m.slot_closure = u32(p.slots);
-        m.slot_v = reinterpret_cast<float4*>(take(32ull * (p.slots ? p.slots : 1)));
         m.blk_m = reinterpret_cast<float4*>(take(16ull * (p.blocks ? p.blocks : 1)));
         m.blk_feat = reinterpret_cast<float4*>(take(64ull * (p.blocks ? p.blocks : 1)));
         m.blk_out = f32(3ull * p.blocks);
@@ -675,6 +675,27 @@ __device__ __forceinline__ float dot_total(uint32_t nq, const MechBuffers& m, co
     return r;
 }
 
+// slot_g[sl] = the slot's share of J^T J x: per closure the branch products
+// (sums over its slots in slot order, branch a then b) and their transposes,
+// from the stored Jacobian columns; closures strided over the block or grid.
+__device__ __forceinline__ void closure_products(const MechBuffers& m, const MechParams& p, const float* x) {
+    const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x, nt = gridDim.x * blockDim.x;
+    for (uint32_t k = tid; k < p.closures; k += nt) {
+        const uint32_t s0 = m.cl_slot_off[k], s1 = m.cl_slot_off[k + 1], split = m.cl_split[k];
+        f3 prod_p[2] = {mkf3(0, 0, 0), mkf3(0, 0, 0)}, prod_a[2] = {mkf3(0, 0, 0), mkf3(0, 0, 0)};
+        for (uint32_t sl = s0; sl < s1; ++sl) {
+            const int side = sl < split ? 0 : 1;
+            const f3 pd = xyz(m.slot_v[2 * sl]), ad = xyz(m.slot_v[2 * sl + 1]);
+            const float dv = x[__float_as_uint(m.slot_v[2 * sl].w)];
+            prod_p[side] = prod_p[side] + pd * dv;
+            prod_a[side] = prod_a[side] + ad * dv;
+        }
+        const f3 pp = prod_p[0] + prod_p[1], pa = prod_a[0] + prod_a[1];
+        for (uint32_t sl = s0; sl < s1; ++sl)
+            m.slot_g[sl] = dot(xyz(m.slot_v[2 * sl]), pp) + 1.0f * dot(xyz(m.slot_v[2 * sl + 1]), pa);
+    }
+}
+
 // Joint frame of `body` in its root's frame (closure.wgsl:168-181).
 __device__ __forceinline__ void joint_frame(const MechBuffers& m, uint32_t body, f3& axis, f3& anchor, uint32_t& coord) {
     const GpuMechanismBody mb = m.bodies[body];
@@ -762,18 +783,23 @@ __global__ void __launch_bounds__(kClosureThreads) k_closure_loop(StepBuffers b,
                 for (uint32_t sl = s0; sl < s1; ++sl) {
                     float g = 0.0f, d = 0.0f;
                     uint32_t valid = 0;
+                    // the slot's Jacobian column: the links do not move during the
+                    // step's PCG rounds, so closure.wgsl:194-266's recomputation in
+                    // every round gives these same floats (sign * v == v * sign)
+                    const bool side_a = sl < split;
+                    const f3 ea = side_a ? aa : ab, ex = side_a ? xa : xb;
+                    const float sign = side_a ? 1.0f : -1.0f;
+                    f3 axis, anchor;
+                    uint32_t coord;
+                    joint_frame(m, m.slot_body[sl], axis, anchor, coord);
+                    const f3 pd = cross(axis, ea - anchor) * sign;
+                    const f3 ad = cross(axis, ex) * sign;
+                    m.slot_v[2 * sl] = f4(pd, __uint_as_float(coord < Q ? coord : 0u));
+                    m.slot_v[2 * sl + 1] = f4(ad, 0.0f);
                     if (active) {
-                        const bool side_a = sl < split;
-                        const f3 ea = side_a ? aa : ab, ex = side_a ? xa : xb;
-                        const float sign = side_a ? 1.0f : -1.0f;
-                        f3 axis, anchor;
-                        uint32_t coord;
-                        joint_frame(m, m.slot_body[sl], axis, anchor, coord);
                         if (coord >= Q) {
                             atomicOr(flags, MK_INVALID_NUMERIC_FLAG);
                         } else {
-                            const f3 pd = cross(axis, ea - anchor) * sign;
-                            const f3 ad = cross(axis, ex) * sign;
                             g = dot(rp, pd) + 1.0f * dot(ra, ad);
                             d = dot(pd, pd) + 1.0f * dot(ad, ad);
                             if (g == g && d == d) valid = 1;
@@ -819,37 +845,9 @@ __global__ void __launch_bounds__(kClosureThreads) k_closure_loop(StepBuffers b,
             loop_sync<kGrid>(m.grid_barrier, flags);
             float rz = dot_total(NQ, m, res, pre, part_a, s_red);
             for (uint32_t round = 0; round < kClosureRounds; ++round) {
-                // J^T J dir per closure: branch products then transposes (closure.wgsl:194-266)
-                for (uint32_t k = gtid; k < NC; k += gnt) {
-                    const GpuBearing br = m.bearings[m.cl_bearings[k]];
-                    f3 aa, ab, xa, xb;
-                    closure_frames(m, br, aa, ab, xa, xb);
-                    const uint32_t s0 = m.cl_slot_off[k], s1 = m.cl_slot_off[k + 1], split = m.cl_split[k];
-                    f3 prod_p[2] = {mkf3(0, 0, 0), mkf3(0, 0, 0)}, prod_a[2] = {mkf3(0, 0, 0), mkf3(0, 0, 0)};
-                    for (uint32_t sl = s0; sl < s1; ++sl) {
-                        const int side = sl < split ? 0 : 1;
-                        const f3 ea = side == 0 ? aa : ab, ex = side == 0 ? xa : xb;
-                        const float sign = side == 0 ? 1.0f : -1.0f;
-                        f3 axis, anchor;
-                        uint32_t coord;
-                        joint_frame(m, m.slot_body[sl], axis, anchor, coord);
-                        const float dv = dir[coord];
-                        prod_p[side] = prod_p[side] + sign * cross(axis, ea - anchor) * dv;
-                        prod_a[side] = prod_a[side] + sign * cross(axis, ex) * dv;
-                    }
-                    const f3 pp = prod_p[0] + prod_p[1], pa = prod_a[0] + prod_a[1];
-                    for (uint32_t sl = s0; sl < s1; ++sl) {
-                        const bool side_a = sl < split;
-                        const f3 ea = side_a ? aa : ab, ex = side_a ? xa : xb;
-                        const float sign = side_a ? 1.0f : -1.0f;
-                        f3 axis, anchor;
-                        uint32_t coord;
-                        joint_frame(m, m.slot_body[sl], axis, anchor, coord);
-                        const f3 pd = sign * cross(axis, ea - anchor);
-                        const f3 ad = sign * cross(axis, ex);
-                        m.slot_g[sl] = dot(pd, pp) + 1.0f * dot(ad, pa);
-                    }
-                }
+                // J^T J dir per closure: branch products then transposes
+                // (closure.wgsl:194-266), from the step's stored columns
+                closure_products(m, p, dir);
                 loop_sync<kGrid>(m.grid_barrier, flags);
                 for (uint32_t c = blockIdx.x; c < chunks; c += gridDim.x) {
                     const uint32_t q = c * kDotChunk + threadIdx.x;
@@ -977,20 +975,7 @@ template <bool kGrid>
 __device__ void closure_apply(const MechBuffers& m, const MechParams& p, const float* x, float* out,
                               uint32_t* flags) {
     const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x, nt = gridDim.x * blockDim.x;
-    for (uint32_t k = tid; k < p.closures; k += nt) {
-        const uint32_t s0 = m.cl_slot_off[k], s1 = m.cl_slot_off[k + 1], split = m.cl_split[k];
-        f3 prod_p[2] = {mkf3(0, 0, 0), mkf3(0, 0, 0)}, prod_a[2] = {mkf3(0, 0, 0), mkf3(0, 0, 0)};
-        for (uint32_t sl = s0; sl < s1; ++sl) {
-            const int side = sl < split ? 0 : 1;
-            const f3 pd = xyz(m.slot_v[2 * sl]), ad = xyz(m.slot_v[2 * sl + 1]);
-            const float dv = x[__float_as_uint(m.slot_v[2 * sl].w)];
-            prod_p[side] = prod_p[side] + pd * dv;
-            prod_a[side] = prod_a[side] + ad * dv;
-        }
-        const f3 pp = prod_p[0] + prod_p[1], pa = prod_a[0] + prod_a[1];
-        for (uint32_t sl = s0; sl < s1; ++sl)
-            m.slot_g[sl] = dot(xyz(m.slot_v[2 * sl]), pp) + 1.0f * dot(xyz(m.slot_v[2 * sl + 1]), pa);
-    }
+    closure_products(m, p, x);
     loop_sync<kGrid>(m.grid_barrier, flags);
     for (uint32_t q = tid; q < p.closure_coords; q += nt) {
         float o = 0.0f;
