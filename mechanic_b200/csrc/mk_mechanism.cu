@@ -682,15 +682,24 @@ __device__ __forceinline__ void closure_products(const MechBuffers& m, const Mec
     const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x, nt = gridDim.x * blockDim.x;
     for (uint32_t k = tid; k < p.closures; k += nt) {
         const uint32_t s0 = m.cl_slot_off[k], s1 = m.cl_slot_off[k + 1], split = m.cl_split[k];
-        f3 prod_p[2] = {mkf3(0, 0, 0), mkf3(0, 0, 0)}, prod_a[2] = {mkf3(0, 0, 0), mkf3(0, 0, 0)};
+        // branch a's and branch b's sums in registers (no indexed array), unrolled so
+        // the columns' loads issue together; each sum keeps slot order
+        f3 pp_a = mkf3(0, 0, 0), pa_a = mkf3(0, 0, 0), pp_b = mkf3(0, 0, 0), pa_b = mkf3(0, 0, 0);
+#pragma unroll 4
         for (uint32_t sl = s0; sl < s1; ++sl) {
-            const int side = sl < split ? 0 : 1;
             const f3 pd = xyz(m.slot_v[2 * sl]), ad = xyz(m.slot_v[2 * sl + 1]);
             const float dv = x[__float_as_uint(m.slot_v[2 * sl].w)];
-            prod_p[side] = prod_p[side] + pd * dv;
-            prod_a[side] = prod_a[side] + ad * dv;
+            const f3 tp = pd * dv, ta = ad * dv;
+            if (sl < split) {
+                pp_a = pp_a + tp;
+                pa_a = pa_a + ta;
+            } else {
+                pp_b = pp_b + tp;
+                pa_b = pa_b + ta;
+            }
         }
-        const f3 pp = prod_p[0] + prod_p[1], pa = prod_a[0] + prod_a[1];
+        const f3 pp = pp_a + pp_b, pa = pa_a + pa_b;
+#pragma unroll 4
         for (uint32_t sl = s0; sl < s1; ++sl)
             m.slot_g[sl] = dot(xyz(m.slot_v[2 * sl]), pp) + 1.0f * dot(xyz(m.slot_v[2 * sl + 1]), pa);
     }
