@@ -91,6 +91,15 @@ __device__ __forceinline__ uint32_t round_u32(float x) {
     return (uint32_t)r;
 }
 
+// An apply of zero deltas, f4(xyz(v) + 0.0f, 0.0f), reproduces v bit for bit
+// unless a component is -0.0 (it becomes +0.0) or NaN (it may come back with
+// another payload), or w is not +0.0: then the row must still be written.
+__device__ __forceinline__ bool zero_apply_is_identity(float4 v) {
+    const uint32_t nz = 0x80000000u;
+    return __float_as_uint(v.x) != nz && __float_as_uint(v.y) != nz && __float_as_uint(v.z) != nz &&
+           v.x == v.x && v.y == v.y && v.z == v.z && __float_as_uint(v.w) == 0u;
+}
+
 // ------------------------------------------------------------- loads/stores
 __device__ __forceinline__ float4 ldg4(const float4* p) { return __ldg(p); }
 __device__ __forceinline__ float4 ld4(const float4* p) { return *p; }

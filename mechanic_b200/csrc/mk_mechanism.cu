@@ -271,6 +271,28 @@ __device__ __forceinline__ f3 wii(const StepBuffers& b, uint32_t body, f3 v) {
 }
 __device__ __forceinline__ float inv_mass(const StepBuffers& b, uint32_t body) { return b.mass[4ull * body].x; }
 
+// One body's fixed-point deltas summed in registers: a row's contribution is
+// converted as add_mdelta does and the integer sums wrap as the atomics do,
+// so one atomic per component gives the same totals as one per row.
+struct MDelta {
+    uint32_t v[6];
+};
+__device__ __forceinline__ void mdelta_add(MDelta& acc, f3 l, f3 a) {
+    const float s = 1048576.0f;
+    acc.v[0] += (uint32_t)fixed_i32(l.x * s);
+    acc.v[1] += (uint32_t)fixed_i32(l.y * s);
+    acc.v[2] += (uint32_t)fixed_i32(l.z * s);
+    acc.v[3] += (uint32_t)fixed_i32(a.x * s);
+    acc.v[4] += (uint32_t)fixed_i32(a.y * s);
+    acc.v[5] += (uint32_t)fixed_i32(a.z * s);
+}
+__device__ __forceinline__ void mdelta_flush(int32_t* deltas, uint32_t body, const MDelta& acc) {
+    int32_t* d = deltas + 6ull * body;
+#pragma unroll
+    for (int c = 0; c < 6; ++c)
+        if (acc.v[c]) atomicAdd(d + c, (int32_t)acc.v[c]);
+}
+
 __device__ __forceinline__ void add_mdelta(int32_t* deltas, uint32_t body, f3 l, f3 a) {   // :104-112
     const float s = 1048576.0f;
     int32_t* d = deltas + 6ull * body;
@@ -304,6 +326,7 @@ __global__ void __launch_bounds__(kMBlock) k_project_bearings(StepBuffers b, Mec
     const f3 rel = vb - va;
     const float ima = inv_mass(b, a), imb = inv_mass(b, c);
     const f3 dirs[3] = {mkf3(1, 0, 0), mkf3(0, 1, 0), mkf3(0, 0, 1)};
+    MDelta da{}, dc{};   // every row reads the velocities of before the pass (Jacobi)
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
         const f3 d = dirs[k];
@@ -311,8 +334,8 @@ __global__ void __launch_bounds__(kMBlock) k_project_bearings(StepBuffers b, Mec
         const float den = ima + imb + dot(ang_a, wii(b, a, ang_a)) + dot(ang_b, wii(b, c, ang_b));
         if (den <= 1.0e-12f) continue;
         const f3 imp = d * (0.5f * dot(rel, d) / den);
-        add_mdelta(m.deltas, a, imp * ima, wii(b, a, cross(arm_a, imp)));
-        add_mdelta(m.deltas, c, -imp * imb, wii(b, c, cross(arm_b, -imp)));
+        mdelta_add(da, imp * ima, wii(b, a, cross(arm_a, imp)));
+        mdelta_add(dc, -imp * imb, wii(b, c, cross(arm_b, -imp)));
     }
     f3 ta, tb;
     hinge_tangents(b, a, c, br, ta, tb);
@@ -325,9 +348,11 @@ __global__ void __launch_bounds__(kMBlock) k_project_bearings(StepBuffers b, Mec
         const float den = dot(axis, ia + ib);
         if (den <= 1.0e-12f) continue;
         const float imp = 0.5f * dot(rang, axis) / den;
-        add_mdelta(m.deltas, a, mkf3(0, 0, 0), ia * imp);
-        add_mdelta(m.deltas, c, mkf3(0, 0, 0), -ib * imp);
+        mdelta_add(da, mkf3(0, 0, 0), ia * imp);
+        mdelta_add(dc, mkf3(0, 0, 0), -ib * imp);
     }
+    mdelta_flush(m.deltas, a, da);
+    mdelta_flush(m.deltas, c, dc);
 }
 
 // articulated.wgsl:318-337
@@ -336,9 +361,15 @@ __global__ void __launch_bounds__(kMBlock) k_apply_mdeltas(StepBuffers b, MechBu
     if (i >= p.body_count) return;
     int2* d2 = reinterpret_cast<int2*>(m.deltas + 6ull * i);
     const int2 x0 = d2[0], x1 = d2[1], x2 = d2[2];
-    d2[0] = make_int2(0, 0);
-    d2[1] = make_int2(0, 0);
-    d2[2] = make_int2(0, 0);
+    if ((x0.x | x0.y | x1.x | x1.y | x2.x | x2.y) == 0) {
+        // most bodies have no bearing: their apply changes no bit unless a
+        // velocity holds -0.0 or NaN, so only those are written
+        if (zero_apply_is_identity(b.lin[i]) && zero_apply_is_identity(b.ang[i])) return;
+    } else {
+        d2[0] = make_int2(0, 0);
+        d2[1] = make_int2(0, 0);
+        d2[2] = make_int2(0, 0);
+    }
     const float s = 1048576.0f;
     const f3 ld = mkf3((float)x0.x, (float)x0.y, (float)x1.x) / s;
     const f3 ad = mkf3((float)x1.y, (float)x2.x, (float)x2.y) / s;
@@ -1391,7 +1422,8 @@ static inline uint32_t nblocks(uint32_t n) { return (n + kMBlock - 1) / kMBlock;
 
 static cudaError_t bearing_projection_iteration(MechBuffers& m, const StepBuffers& b, const MechParams& p,
                                                 cudaStream_t s) {
-    if (p.bearing_count) k_project_bearings<<<nblocks(p.bearing_count), kMBlock, 0, s>>>(b, m, p);
+    // 64-thread blocks spread the bearings' atomics over more SMs
+    if (p.bearing_count) k_project_bearings<<<(p.bearing_count + 63) / 64, 64, 0, s>>>(b, m, p);
     k_apply_mdeltas<<<nblocks(p.body_count), kMBlock, 0, s>>>(b, m, p);
     return cudaGetLastError();
 }

@@ -2004,9 +2004,13 @@ __global__ void __launch_bounds__(kBlock) k_apply_iter(StepBuffers b, StepParams
     for (uint32_t i = first; i < p.body_count; i += stride) {
         int2* d2 = reinterpret_cast<int2*>(b.deltas + 6ull * i);
         const int2 x0 = d2[0], x1 = d2[1], x2 = d2[2];
-        d2[0] = make_int2(0, 0);
-        d2[1] = make_int2(0, 0);
-        d2[2] = make_int2(0, 0);
+        if ((x0.x | x0.y | x1.x | x1.y | x2.x | x2.y) == 0) {   // untouched body: write only if bits change
+            if (zero_apply_is_identity(b.lin[i]) && zero_apply_is_identity(b.ang[i])) continue;
+        } else {
+            d2[0] = make_int2(0, 0);
+            d2[1] = make_int2(0, 0);
+            d2[2] = make_int2(0, 0);
+        }
         const f3 ld = mkf3((float)x0.x, (float)x0.y, (float)x1.x) / s;
         const f3 ad = mkf3((float)x1.y, (float)x2.x, (float)x2.y) / s;
         b.lin[i] = f4(xyz(b.lin[i]) + ld, 0.0f);
