@@ -199,6 +199,7 @@ uint64_t carve(MkHandle* h, char* base) {
     if (h->scene_count > 1) {
         b.collider_scene = c.take<uint32_t>(C);
         b.scene_end = c.take<uint32_t>(h->scene_count);
+        b.scene_root = c.take<uint32_t>(h->scene_count);
     }
     b.sort_scratch_bytes = mk::sort_scratch_bytes(C, 63);
     b.sort_scratch = c.take<char>(b.sort_scratch_bytes);

@@ -156,6 +156,7 @@ struct StepBuffers {
     uint32_t* scene_bounds;      // 8 words, zeroed each tick: ordered max and complemented min of the centres
     uint32_t* collider_scene;    // scene of each collider
     uint32_t* scene_end;         // per scene: end of its sorted leaf positions
+    uint32_t* scene_root;        // per scene: the internal node over exactly its leaves (scenes of >= 2 colliders)
     // contact solve to a residual (null unless enabled at creation)
     int64_t* deltas64;           // 2 candidates x 6 per body, fixed point x 2^32
     double* res2;                // 2 candidates x pair_capacity squared residuals

@@ -299,6 +299,11 @@ __global__ void __launch_bounds__(kBlock) k_karras(StepBuffers b, StepParams p) 
     const int split = i + split_off * dir + min(dir, 0);
     const int first = min(i, other), last = max(i, other);
     const uint32_t leaf_base = (uint32_t)(n - 1);
+    if (b.collider_scene) {   // batched scenes: the node over exactly one scene's leaves is that scene's root
+        const uint32_t sc = b.collider_scene[v[first]];
+        const uint32_t begin = sc ? b.scene_end[sc - 1] : 0u;
+        if ((uint32_t)first == begin && (uint32_t)last + 1u == b.scene_end[sc]) b.scene_root[sc] = (uint32_t)i;
+    }
     const uint32_t left = split == first ? leaf_base + (uint32_t)split : (uint32_t)split;
     const uint32_t right = split + 1 == last ? leaf_base + (uint32_t)(split + 1) : (uint32_t)(split + 1);
     b.children[i] = make_uint2(left, right);
@@ -692,14 +697,21 @@ __global__ void __launch_bounds__(kTravThreads) k_traverse(StepBuffers b, StepPa
         const uint32_t i = b.svals[t];
         const float4 qmin = b.node_aabbs[2ull * (leaf_base + t)], qmax = b.node_aabbs[2ull * (leaf_base + t) + 1];
         const uint32_t body_i = __float_as_uint(b.boxes[3ull * i + 2].z);
-        // batched scenes: candidates end where this collider's scene ends in sorted order
-        // (a right child starts one past its left sibling's last leaf; left children start
-        // where their parent does, which was already below the limit)
-        const uint32_t limit = kBatched ? __ldg(b.scene_end + b.collider_scene[i]) : n;
+        // batched scenes: the walk starts at the scene's own subtree (Karras keeps
+        // each scene's leaves under one node: the scene index sits above the
+        // Morton bits), so every entry it meets lies inside the scene; a scene of
+        // one collider has no pairs
+        uint32_t node = 0;
+        bool none = false;
+        if (kBatched) {
+            const uint32_t sc = b.collider_scene[i];
+            const uint32_t begin = sc ? __ldg(b.scene_end + sc - 1) : 0u, end = __ldg(b.scene_end + sc);
+            none = end - begin < 2u;
+            if (!none) node = __ldg(b.scene_root + sc);
+        }
         uint32_t stack[kStack];
         uint32_t sp = 0;
-        uint32_t node = 0;
-        for (;;) {
+        while (!none) {
             const float4* rec = b.node_records + 8ull * node;   // 4-wide: two levels per step
             float4 r[8];
 #pragma unroll
@@ -713,7 +725,6 @@ __global__ void __launch_bounds__(kTravThreads) k_traverse(StepBuffers b, StepPa
             for (int k = 0; k < 4; ++k) {
                 const float4 cmin = r[2 * k], cmax = r[2 * k + 1];
                 if (__float_as_uint(cmax.w) <= t) continue;     // nothing to the right of this leaf below
-                if (kBatched && k > 0 && __float_as_uint(r[2 * k - 1].w) + 1u >= limit) continue;   // past the scene
                 if (!overlaps(qmin, qmax, cmin, cmax)) continue;
                 const uint32_t code = __float_as_uint(cmin.w);
                 if (code & kLeafCode) {
