@@ -530,9 +530,47 @@ __global__ void __launch_bounds__(kRefitBlock) k_refit_leaves(StepBuffers b, Ste
 }
 
 // Sparse table over the super-chunk totals: level k holds unions of 2^k of them.
+// Up to kSuperSmem super-chunks (2M colliders) the levels are built in shared
+// memory and written out as they complete; beyond, level by level through L2.
+constexpr uint32_t kSuperSmem = 2048;
 __global__ void __launch_bounds__(1024) k_refit_super(StepBuffers b, StepParams p) {
     const uint32_t n = p.collider_count;
     const uint32_t ns = (n + kRefitBlock - 1) / kRefitBlock;
+    if (ns <= kSuperSmem) {
+        constexpr uint32_t kPer = kSuperSmem / 1024;
+        __shared__ float s_t[6][kSuperSmem];   // min.xyz, max.xyz of the current level
+        for (uint32_t q = threadIdx.x; q < ns; q += blockDim.x) {
+            const Box2 v = ld_box_cg(b.super_table + 2ull * q);
+            s_t[0][q] = v.mn.x; s_t[1][q] = v.mn.y; s_t[2][q] = v.mn.z;
+            s_t[3][q] = v.mx.x; s_t[4][q] = v.mx.y; s_t[5][q] = v.mx.z;
+        }
+        __syncthreads();
+        auto at = [&](uint32_t q) -> Box2 {
+            return {make_float4(s_t[0][q], s_t[1][q], s_t[2][q], 0.0f), make_float4(s_t[3][q], s_t[4][q], s_t[5][q], 0.0f)};
+        };
+        for (uint32_t k = 1; (1u << k) <= ns; ++k) {
+            const uint32_t half = 1u << (k - 1);
+            float4* dst = b.super_table + 2ull * ns * k;
+            Box2 u[kPer];
+#pragma unroll
+            for (uint32_t e = 0; e < kPer; ++e) {
+                const uint32_t q = threadIdx.x + e * 1024u;
+                if (q + (1u << k) <= ns) u[e] = box_union(at(q), at(q + half));
+            }
+            __syncthreads();   // every read of the level below is done
+#pragma unroll
+            for (uint32_t e = 0; e < kPer; ++e) {
+                const uint32_t q = threadIdx.x + e * 1024u;
+                if (q + (1u << k) <= ns) {
+                    s_t[0][q] = u[e].mn.x; s_t[1][q] = u[e].mn.y; s_t[2][q] = u[e].mn.z;
+                    s_t[3][q] = u[e].mx.x; s_t[4][q] = u[e].mx.y; s_t[5][q] = u[e].mx.z;
+                    st_box(dst + 2ull * q, u[e]);
+                }
+            }
+            __syncthreads();
+        }
+        return;
+    }
     for (uint32_t k = 1; (1u << k) <= ns; ++k) {
         const float4* src = b.super_table + 2ull * ns * (k - 1);
         float4* dst = b.super_table + 2ull * ns * k;

@@ -110,15 +110,19 @@ def test_morton63_mode_bitexact(cuda_lib):
         compare_tick(gpu, orc, tick)
 
 
-def test_node_boxes_are_leaf_range_unions(cuda_lib):
+@pytest.mark.parametrize("grid,ticks", [((14, 9, 14), (1, 3, 6)), ((30, 30, 30), (2,))],
+                         ids=["7k-colliders", "100k-colliders"])
+def test_node_boxes_are_leaf_range_unions(cuda_lib, grid, ticks):
     """Every LBVH node box equals the min/max over the AABBs of its leaf range
-    (exact: unions are min/max), over ticks with dense and sparse contact."""
-    scene = scenes.stack_grid(14, 9, 14, seed=11)
-    gpu = GpuPhysics(scene, GpuPhysicsConfig(), capacities={"pair_capacity": 1 << 22})
-    for tick in range(1, 7):
+    (exact: unions are min/max), over ticks with dense and sparse contact; the
+    larger scene spans about a hundred 1,024-leaf super-chunks, so its long
+    ranges go through every level of the super-chunk sparse table."""
+    scene = scenes.stack_grid(*grid, seed=11)
+    gpu = GpuPhysics(scene, GpuPhysicsConfig(), capacities={"pair_capacity": 1 << 24})
+    for tick in range(1, max(ticks) + 1):
         gpu.dispatch_tick(tick)
         gpu.wait()
-        if tick not in (1, 3, 6):
+        if tick not in ticks:
             continue
         ch = gpu.node_children().astype(np.int64)
         nodes = gpu.node_aabbs()
