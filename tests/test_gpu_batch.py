@@ -48,6 +48,27 @@ def test_batch_bitexact_against_oracle(cuda_lib):
         assert_bitwise(st["velocities"], vel, f"tick {tick} velocities")
 
 
+def test_batch_tiny_scenes_against_oracle(cuda_lib):
+    """Scenes of one, two and three colliders beside a larger one: a one-collider scene has no
+    subtree of its own (its walk is skipped), the others are walked from their own subtree roots."""
+    lst = [scenes.falling_cubes(1, seed=7), scenes.falling_cubes(2, seed=8, box=0.2), scenes.mixed_scene(90, seed=4),
+           scenes.falling_cubes(3, seed=9, box=0.3), scenes.falling_cubes(1, seed=10)]
+    cfg = GpuPhysicsConfig()
+    gpu = GpuPhysics.batch(lst, cfg, capacities={"pair_capacity": 1 << 16})
+    orc = oracle.OracleWorld.batch(lst, cfg.to_c(), pair_capacity=1 << 16)
+    seen = 0
+    for tick in range(1, 5):
+        gpu.dispatch_tick(tick)
+        rb = gpu.read_last_tick()
+        orc.step(tick)
+        d = orc.diagnostics()
+        assert rb.error_flags == int(d["error_flags"]) and rb.pair_count == int(d["pair_count"]), tick
+        assert np.array_equal(gpu.pairs(), orc.pairs()), tick
+        assert_bitwise(gpu.contacts(), orc.contacts(), f"tick {tick} contacts")
+        seen += rb.pair_count
+    assert seen > 0
+
+
 def test_batch_slices_equal_single_scenes(cuda_lib):
     # plain scenes only: a batch holding a mechanism takes the reference's mechanism
     # contact path (device.rs:1370-1417) for all of its contacts
