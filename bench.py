@@ -60,9 +60,9 @@ BYTES_SOLVE_PER_CONTACT_ITER = 284     # contact 64 + idx 4 + 2 x (v 16 + w 16 +
 BYTES_APPLY_PER_BODY_ITER = 112        # deltas 24 + velocities 32 read, velocities 32 + deltas 24 written
 BYTES_PREPARE_PER_CONTACT = 340        # contact 64 + 2 x (v/w 32 + world mass 48) + manifold 96, 16 + 48 + 4 written
 # broadphase per collider: AABB + Morton 140 (collider 64 + pose 32 read, AABB 32 + key/value 12 written),
-# onesweep sort 156 (2 x 12 x 6 digit passes over the 48-bit keys + 12), Karras 24, refit 96 + 32,
+# onesweep sort 132 (2 x 12 x 5 digit passes over the 39-bit keys + 12), Karras 24, refit 96 + 32,
 # traversal 32
-BYTES_BROADPHASE_PER_COLLIDER = 140 + 156 + 24 + 96 + 32 + 32
+BYTES_BROADPHASE_PER_COLLIDER = 140 + 132 + 24 + 96 + 32 + 32
 # per candidate pair: traversal output 8 + pair-key sort (5 digit passes x 16 + 8)
 BYTES_BROADPHASE_PER_PAIR = 8 + 88
 
@@ -172,8 +172,9 @@ class ClockSampler:
 def cpu_trajectory(scene, ticks: int, budget_s: float, threads: int):
     """Steps the CPU oracle along ticks 1..ticks, stopping early once budget_s has passed."""
     import oracle
+    from mechanic_b200.physics import GpuPhysicsConfig
     oracle.set_threads(threads)
-    w = oracle.OracleWorld(scene, pair_capacity=PAIR_CAPACITY)
+    w = oracle.OracleWorld(scene, GpuPhysicsConfig().to_c(), pair_capacity=PAIR_CAPACITY)   # the GPU arm's config
     t0 = time.perf_counter()
     done = 0
     for tick in range(1, ticks + 1):
@@ -190,7 +191,8 @@ def run_reference(args, scene):
     import oracle
     oracle.build()
     oracle.set_threads(threads)
-    warm = oracle.OracleWorld(scene, pair_capacity=PAIR_CAPACITY)
+    from mechanic_b200.physics import GpuPhysicsConfig
+    warm = oracle.OracleWorld(scene, GpuPhysicsConfig().to_c(), pair_capacity=PAIR_CAPACITY)
     for tick in range(1, args.warmup + 1):
         warm.step(tick)
     del warm

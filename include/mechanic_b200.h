@@ -247,7 +247,7 @@ typedef struct MkConfig {
     uint32_t collisions_enabled;         /* default 1 */
     uint32_t mechanism_self_collisions;  /* default 1 */
     uint32_t solver_iterations;          /* default 8 */
-    uint32_t morton_mode;                /* MK_MORTON_48 (default), MK_MORTON_63 or MK_MORTON_REFERENCE_30 */
+    uint32_t morton_mode;                /* MK_MORTON_39 (default), MK_MORTON_48, MK_MORTON_63 or MK_MORTON_REFERENCE_30 */
     uint32_t closure_mode;               /* MK_CLOSURE_* */
     uint32_t use_graph;                  /* 1: capture the tick into a CUDA graph (default) */
     float delta_seconds;                 /* 0 => 1/60 (lib.rs:31) */
@@ -279,8 +279,10 @@ typedef struct MkConfig {
 #define MK_MORTON_63            0u  /* 21 bits/axis over the tick's bounds of the collider centres (cubic cells),
                                        index tie-break through a stable sort */
 #define MK_MORTON_REFERENCE_30  1u  /* lbvh.wgsl:93-98: 10 bits/axis, 1 m cells */
-#define MK_MORTON_48            2u  /* default: 16 bits/axis over the same bounds; two radix passes fewer than
+#define MK_MORTON_48            2u  /* 16 bits/axis over the same bounds; two radix passes fewer than
                                        MK_MORTON_63 (cells of extent / 65535) */
+#define MK_MORTON_39            3u  /* default: 13 bits/axis over the same bounds; one radix pass fewer than
+                                       MK_MORTON_48 (cells of extent / 8191) */
 
 #define MK_CLOSURE_REFERENCE    0u  /* closure.wgsl:333-427: 8 fixed diagonal-PCG rounds per Newton step */
 #define MK_CLOSURE_PCG_RESIDUAL 1u  /* parallel block-Jacobi PCG to a relative residual, FP64 reductions */

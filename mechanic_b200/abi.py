@@ -31,6 +31,7 @@ MAX_CONTACT_PAIRS = 2_097_152               # lib.rs:45
 MORTON_63 = 0
 MORTON_REFERENCE_30 = 1
 MORTON_48 = 2
+MORTON_39 = 3
 CLOSURE_REFERENCE = 0
 CLOSURE_PCG_RESIDUAL = 1
 WARM_CACHED = 0

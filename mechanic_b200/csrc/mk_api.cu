@@ -622,7 +622,7 @@ int create_impl(const MkCreation* cr, const MkConfig* config, const MkCapacities
         return MK_ERR_INVALID_ARGUMENT;
     }
     if (config && config->morton_mode != MK_MORTON_63 && config->morton_mode != MK_MORTON_48 &&
-        config->morton_mode != MK_MORTON_REFERENCE_30) {
+        config->morton_mode != MK_MORTON_39 && config->morton_mode != MK_MORTON_REFERENCE_30) {
         set_error(err, MK_ERR_INVALID_ARGUMENT, "unknown morton_mode %u", config->morton_mode);
         return MK_ERR_INVALID_ARGUMENT;
     }
@@ -796,7 +796,7 @@ void mk_config_default(MkConfig* c) {
     c->collisions_enabled = 1;
     c->mechanism_self_collisions = 1;
     c->solver_iterations = 8;
-    c->morton_mode = MK_MORTON_48;
+    c->morton_mode = MK_MORTON_39;
     c->closure_mode = MK_CLOSURE_REFERENCE;
     c->use_graph = 1;
 }

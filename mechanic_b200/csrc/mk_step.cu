@@ -146,7 +146,9 @@ __device__ __forceinline__ uint64_t morton_frame(f3 c, f3 lo, float scale, float
     uint64_t qz = (uint64_t)clampf(floorf((c.z - lo.z) * scale), 0.0f, qmax);
     return expand21(qx) | (expand21(qy) << 1) | (expand21(qz) << 2);
 }
-__device__ __forceinline__ float frame_qmax(uint32_t mode) { return mode == MK_MORTON_48 ? 65535.0f : 2097151.0f; }
+__device__ __forceinline__ float frame_qmax(uint32_t mode) {
+    return mode == MK_MORTON_39 ? 8191.0f : mode == MK_MORTON_48 ? 65535.0f : 2097151.0f;
+}
 // Floats as unsigned integers in the same order (-0 below +0), for exact
 // order-free min / max with integer atomics.
 __device__ __forceinline__ uint32_t float_order(float f) {
@@ -251,7 +253,7 @@ __global__ void __launch_bounds__(kBlock) k_collider_bounds(StepBuffers b, StepP
     }
 }
 
-// Keys over the tick's centre bounds (MK_MORTON_48, MK_MORTON_63).
+// Keys over the tick's centre bounds (MK_MORTON_39, MK_MORTON_48, MK_MORTON_63).
 __global__ void __launch_bounds__(kBlock) k_morton_keys(StepBuffers b, StepParams p, uint32_t morton_mode) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= p.collider_count) return;

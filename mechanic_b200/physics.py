@@ -147,7 +147,7 @@ class GpuPhysicsConfig:
     collisions_enabled: bool = True
     mechanism_self_collisions: bool = True
     solver_iterations: int = 8
-    morton_mode: int = abi.MORTON_48
+    morton_mode: int = abi.MORTON_39
     closure_mode: int = abi.CLOSURE_REFERENCE
     use_graph: bool = True
     device: int = 0

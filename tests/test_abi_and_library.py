@@ -86,7 +86,7 @@ def test_library_loads_without_gpu_and_reports_version():
     c = abi.MkConfig()
     lib.mk_config_default(ctypes.byref(c))
     assert (c.collisions_enabled, c.mechanism_self_collisions, c.solver_iterations) == (1, 1, 8)
-    assert c.use_graph == 1 and c.morton_mode == abi.MORTON_48
+    assert c.use_graph == 1 and c.morton_mode == abi.MORTON_39
 
 
 def test_create_rejects_over_capacity_before_touching_a_device():

@@ -102,10 +102,12 @@ def test_reference_morton_mode_same_pairs(cuda_lib):
         compare_tick(gpu, orc, tick)
 
 
-def test_morton63_mode_bitexact(cuda_lib):
-    """21 bits per axis (two more radix passes than the default 16): same bit-exact path."""
+@pytest.mark.parametrize("mode", [abi.MORTON_63, abi.MORTON_48], ids=["63-bit", "48-bit"])
+def test_other_morton_modes_bitexact(cuda_lib, mode):
+    """21 and 16 bits per axis (three and one radix passes more than the default 13): the same
+    bit-exact path (keys, permutation, topology, pairs, contacts, state)."""
     scene = scenes.stack_grid(10, 6, 10, seed=5)
-    gpu, orc = make_pair(scene, GpuPhysicsConfig(morton_mode=abi.MORTON_63))
+    gpu, orc = make_pair(scene, GpuPhysicsConfig(morton_mode=mode))
     for tick in range(1, 4):
         compare_tick(gpu, orc, tick)
 

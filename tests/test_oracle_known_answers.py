@@ -115,6 +115,20 @@ def test_morton63_orders_along_each_axis():
     assert oracle.morton63(0.0, 0.0, 2 * cell, lo, scale) > a
 
 
+def test_morton39_is_13_bits_per_axis():
+    # 2^13 - 1 cells over 10 m; the top corner fills all 39 bits
+    lo, scale = (-5.0, -5.0, -5.0), float(np.float32(8191.0) / np.float32(10.0))
+    assert oracle.morton39(-5.0, -5.0, -5.0, lo, scale) == 0
+    assert oracle.morton39(5.0, 5.0, 5.0, lo, scale) == (1 << 39) - 1
+    assert oracle.morton39(-4.0, 9.0, -5.0, lo, scale) >> 1 & 1 == 1       # y clamped high: bit 1 set
+    cell = 10.0 / 8191.0
+    assert oracle.morton39(-5.0 + 1.5 * cell, -5.0, -5.0, lo, scale) == 1   # one cell along x: bit 0
+    assert oracle.morton39(-5.0, -5.0 + 1.5 * cell, -5.0, lo, scale) == 2
+    assert oracle.morton39(-5.0, -5.0, -5.0 + 1.5 * cell, lo, scale) == 4
+    # the same point's 39-bit key is its 48-bit key's cell at a coarser grid: both keep axis order
+    assert oracle.morton39(1.0, 2.0, 3.0, lo, scale) < oracle.morton39(1.0, 2.0, 3.5, lo, scale)
+
+
 def test_morton48_is_16_bits_per_axis():
     # 2^16 - 1 cells over 10 m; the top corner fills all 48 bits
     lo, scale = (-5.0, -5.0, -5.0), float(np.float32(65535.0) / np.float32(10.0))
