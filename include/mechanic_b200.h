@@ -247,7 +247,8 @@ typedef struct MkConfig {
     uint32_t collisions_enabled;         /* default 1 */
     uint32_t mechanism_self_collisions;  /* default 1 */
     uint32_t solver_iterations;          /* default 8 */
-    uint32_t morton_mode;                /* MK_MORTON_39 (default), MK_MORTON_48, MK_MORTON_63 or MK_MORTON_REFERENCE_30 */
+    uint32_t morton_mode;                /* MK_MORTON_39 (default), MK_MORTON_30_ADAPTIVE, MK_MORTON_48, MK_MORTON_63 or
+                                            MK_MORTON_REFERENCE_30 */
     uint32_t closure_mode;               /* MK_CLOSURE_* */
     uint32_t use_graph;                  /* 1: capture the tick into a CUDA graph (default) */
     float delta_seconds;                 /* 0 => 1/60 (lib.rs:31) */
@@ -283,6 +284,9 @@ typedef struct MkConfig {
                                        MK_MORTON_63 (cells of extent / 65535) */
 #define MK_MORTON_39            3u  /* default: 13 bits/axis over the same bounds; one radix pass fewer than
                                        MK_MORTON_48 (cells of extent / 8191) */
+#define MK_MORTON_30_ADAPTIVE   4u  /* 10 bits/axis over the same bounds; one radix pass fewer than MK_MORTON_39
+                                       (cells of extent / 1023, coarse for large scenes with dense clusters):
+                                       mk_autotune chooses between the two by timing */
 
 #define MK_CLOSURE_REFERENCE    0u  /* closure.wgsl:333-427: 8 fixed diagonal-PCG rounds per Newton step */
 #define MK_CLOSURE_PCG_RESIDUAL 1u  /* parallel block-Jacobi PCG to a relative residual, FP64 reductions */
@@ -494,13 +498,17 @@ typedef struct MkTuning {
     uint32_t append_ctas_per_sm;  /* CTAs per SM of the ordered-append kernels (default 8) */
     uint32_t solve_items;         /* 0 (default): every SM's block joins the cooperative solve; n > 0: only
                                      enough blocks for n contacts (and 4n bodies) per thread */
+    uint32_t morton_mode;         /* the broadphase's key mode (MK_MORTON_*; the creation config's until
+                                     tuned): start from mk_get_handle_tuning, since 0 is MK_MORTON_63 */
 } MkTuning;
 MK_API int mk_get_handle_tuning(const MkHandle* handle, MkTuning* out);
 /* Applies a tuning; the tick's CUDA graphs are captured again. */
 MK_API int mk_set_handle_tuning(MkHandle* handle, const MkTuning* tuning, MkError* err);
 /* Autotuner: from the handle's current state, times the next `ticks` ticks
  * (graphs uploaded first) for each candidate shape, varying one field at a time over
- * two sweeps, restoring the state before every candidate; a change is kept only
+ * two sweeps (the launch shapes and, for a handle in MK_MORTON_39 or
+ * MK_MORTON_30_ADAPTIVE, the key mode between those two), restoring the state
+ * before every candidate; a change is kept only
  * when it is at least 2% faster.  The fastest
  * tuning is applied and the state restored again; *best_ms_per_tick
  * receives its time.  The handle must not be in use meanwhile. */

@@ -32,6 +32,7 @@ MORTON_63 = 0
 MORTON_REFERENCE_30 = 1
 MORTON_48 = 2
 MORTON_39 = 3
+MORTON_30_ADAPTIVE = 4
 CLOSURE_REFERENCE = 0
 CLOSURE_PCG_RESIDUAL = 1
 WARM_CACHED = 0
@@ -171,7 +172,7 @@ class MkTickReadback(C.Structure):
 
 class MkTuning(C.Structure):
     _fields_ = [("sort_items", C.c_uint32), ("sort_ctas_per_sm", C.c_uint32),
-                ("append_ctas_per_sm", C.c_uint32), ("solve_items", C.c_uint32)]
+                ("append_ctas_per_sm", C.c_uint32), ("solve_items", C.c_uint32), ("morton_mode", C.c_uint32)]
 
 
 class MkDeviceState(C.Structure):

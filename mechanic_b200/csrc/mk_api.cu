@@ -22,6 +22,11 @@ namespace {
 thread_local std::string g_last_error;
 
 constexpr uint32_t kTickRing = 64;       // tick-config slots in flight
+
+static bool valid_morton_mode(uint32_t m) {
+    return m == MK_MORTON_63 || m == MK_MORTON_REFERENCE_30 || m == MK_MORTON_48 || m == MK_MORTON_39 ||
+           m == MK_MORTON_30_ADAPTIVE;
+}
 constexpr uint32_t kStageEvents = 8;
 
 struct DeviceGuard {
@@ -621,8 +626,7 @@ int create_impl(const MkCreation* cr, const MkConfig* config, const MkCapacities
         set_error(err, MK_ERR_INVALID_ARGUMENT, "creation arrays missing for the given counts");
         return MK_ERR_INVALID_ARGUMENT;
     }
-    if (config && config->morton_mode != MK_MORTON_63 && config->morton_mode != MK_MORTON_48 &&
-        config->morton_mode != MK_MORTON_39 && config->morton_mode != MK_MORTON_REFERENCE_30) {
+    if (config && !valid_morton_mode(config->morton_mode)) {
         set_error(err, MK_ERR_INVALID_ARGUMENT, "unknown morton_mode %u", config->morton_mode);
         return MK_ERR_INVALID_ARGUMENT;
     }
@@ -1153,6 +1157,7 @@ int mk_get_handle_tuning(const MkHandle* h, MkTuning* out) {
     out->sort_ctas_per_sm = h->launch.sort_ctas ? h->launch.sort_ctas : mk::default_sort_ctas(out->sort_items);
     out->append_ctas_per_sm = h->launch.append_ctas ? h->launch.append_ctas : 8u;
     out->solve_items = h->launch.solve_items;
+    out->morton_mode = h->launch.morton_mode;
     return MK_OK;
 }
 
@@ -1163,7 +1168,8 @@ int mk_set_handle_tuning(MkHandle* h, const MkTuning* t, MkError* err) {
         return MK_ERR_INVALID_ARGUMENT;
     }
     const bool ok_items = t->sort_items == 0 || mk::valid_sort_items(t->sort_items);
-    if (!ok_items || t->sort_ctas_per_sm > 32 || t->append_ctas_per_sm > 64 || t->solve_items > 64) {
+    if (!ok_items || t->sort_ctas_per_sm > 32 || t->append_ctas_per_sm > 64 || t->solve_items > 64 ||
+        !valid_morton_mode(t->morton_mode)) {
         set_error(err, MK_ERR_INVALID_ARGUMENT, "tuning outside the supported shapes");
         return MK_ERR_INVALID_ARGUMENT;
     }
@@ -1173,6 +1179,7 @@ int mk_set_handle_tuning(MkHandle* h, const MkTuning* t, MkError* err) {
     h->launch.sort_ctas = t->sort_ctas_per_sm;
     h->launch.append_ctas = t->append_ctas_per_sm;
     h->launch.solve_items = t->solve_items;
+    h->launch.morton_mode = t->morton_mode;   // the sort's scratch holds 63-bit keys: any mode fits
     if (!h->config.use_graph) return MK_OK;
     for (auto& gx : h->graph)
         if (gx) {
@@ -1236,14 +1243,21 @@ int mk_autotune(MkHandle* h, uint32_t ticks, MkTuning* best, double* best_ms, Mk
     const uint32_t sort_ctas[] = {1, 2, 3, 4, 6};
     const uint32_t append_ctas[] = {4, 8, 16};
     const uint32_t solve_items[] = {0, 1, 2, 4};
+    // the key mode: between the two scene-adaptive widths of a handle that uses
+    // one of them (every mode yields the same pairs); other modes are kept
+    const uint32_t key_modes[] = {MK_MORTON_39, MK_MORTON_30_ADAPTIVE};
+    const bool tune_keys = cur.morton_mode == MK_MORTON_39 || cur.morton_mode == MK_MORTON_30_ADAPTIVE;
     for (int sweep = 0; sweep < 2 && rc == MK_OK; ++sweep) {
-        for (int field = 0; field < 4 && rc == MK_OK; ++field) {
-            const uint32_t* vals = field == 0 ? sort_items : field == 1 ? sort_ctas : field == 2 ? append_ctas : solve_items;
-            const int nv = field == 0 ? 5 : field == 1 ? 5 : field == 2 ? 3 : 4;
+        for (int field = 0; field < 5 && rc == MK_OK; ++field) {
+            if (field == 4 && !tune_keys) continue;
+            const uint32_t* vals = field == 0 ? sort_items : field == 1 ? sort_ctas : field == 2 ? append_ctas
+                                   : field == 3 ? solve_items : key_modes;
+            const int nv = field == 0 ? 5 : field == 1 ? 5 : field == 2 ? 3 : field == 3 ? 4 : 2;
             for (int i = 0; i < nv && rc == MK_OK; ++i) {
                 MkTuning cand = cur;
                 uint32_t* slot = field == 0 ? &cand.sort_items : field == 1 ? &cand.sort_ctas_per_sm
-                                 : field == 2 ? &cand.append_ctas_per_sm : &cand.solve_items;
+                                 : field == 2 ? &cand.append_ctas_per_sm : field == 3 ? &cand.solve_items
+                                 : &cand.morton_mode;
                 if (*slot == vals[i]) continue;
                 *slot = vals[i];
                 double ms = 0.0;

@@ -49,7 +49,10 @@ constexpr uint32_t kCountResetBytes = 8 * sizeof(uint32_t);
 // Bits of the spatial Morton key per mode (MK_MORTON_*), and of the sort key
 // once a batch's scene index sits above it.
 __host__ __device__ inline uint32_t spatial_key_bits(uint32_t mode) {
-    return mode == MK_MORTON_REFERENCE_30 ? 30u : mode == MK_MORTON_39 ? 39u : mode == MK_MORTON_48 ? 48u : 63u;
+    return mode == MK_MORTON_REFERENCE_30 || mode == MK_MORTON_30_ADAPTIVE ? 30u
+           : mode == MK_MORTON_39                                        ? 39u
+           : mode == MK_MORTON_48                                        ? 48u
+                                                                         : 63u;
 }
 __host__ __device__ inline uint32_t sort_key_bits(uint32_t mode, uint32_t scene_bits) {
     const uint32_t w = spatial_key_bits(mode) + scene_bits;

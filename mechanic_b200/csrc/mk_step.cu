@@ -147,7 +147,10 @@ __device__ __forceinline__ uint64_t morton_frame(f3 c, f3 lo, float scale, float
     return expand21(qx) | (expand21(qy) << 1) | (expand21(qz) << 2);
 }
 __device__ __forceinline__ float frame_qmax(uint32_t mode) {
-    return mode == MK_MORTON_39 ? 8191.0f : mode == MK_MORTON_48 ? 65535.0f : 2097151.0f;
+    return mode == MK_MORTON_30_ADAPTIVE ? 1023.0f
+           : mode == MK_MORTON_39      ? 8191.0f
+           : mode == MK_MORTON_48      ? 65535.0f
+                                       : 2097151.0f;
 }
 // Floats as unsigned integers in the same order (-0 below +0), for exact
 // order-free min / max with integer atomics.
@@ -253,7 +256,7 @@ __global__ void __launch_bounds__(kBlock) k_collider_bounds(StepBuffers b, StepP
     }
 }
 
-// Keys over the tick's centre bounds (MK_MORTON_39, MK_MORTON_48, MK_MORTON_63).
+// Keys over the tick's centre bounds (every mode but MK_MORTON_REFERENCE_30).
 __global__ void __launch_bounds__(kBlock) k_morton_keys(StepBuffers b, StepParams p, uint32_t morton_mode) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= p.collider_count) return;

@@ -85,6 +85,8 @@ def lib():
         L.or_morton48.argtypes = [C.c_float] * 7
         L.or_morton39.restype = u64
         L.or_morton39.argtypes = [C.c_float] * 7
+        L.or_morton30a.restype = u64
+        L.or_morton30a.argtypes = [C.c_float] * 7
         _lib = L
     return _lib
 
@@ -323,6 +325,11 @@ def morton30(x, y, z) -> int:
 def morton63(x, y, z, lo=(0.0, 0.0, 0.0), scale=1.0) -> int:
     """63-bit key of a centre in the frame (lo, scale) of the tick's centre bounds."""
     return int(lib().or_morton63(x, y, z, lo[0], lo[1], lo[2], scale))
+
+
+def morton30a(x, y, z, lo=(0.0, 0.0, 0.0), scale=1.0) -> int:
+    """10 bits per axis over the tick's centre bounds (lo, scale = 1023 / largest extent)."""
+    return int(lib().or_morton30a(x, y, z, lo[0], lo[1], lo[2], scale))
 
 
 def morton39(x, y, z, lo=(0.0, 0.0, 0.0), scale=1.0) -> int:

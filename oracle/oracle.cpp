@@ -301,10 +301,16 @@ template <class T> struct World : WorldBase {
         return expand21(q(c.x, lo.x)) | (expand21(q(c.y, lo.y)) << 1) | (expand21(q(c.z, lo.z)) << 2);
     }
     static T frame_qmax(uint32_t mode) {
-        return mode == MK_MORTON_39 ? T(8191.0f) : mode == MK_MORTON_48 ? T(65535.0f) : T(2097151.0f);
+        return mode == MK_MORTON_30_ADAPTIVE ? T(1023.0f)
+               : mode == MK_MORTON_39      ? T(8191.0f)
+               : mode == MK_MORTON_48      ? T(65535.0f)
+                                           : T(2097151.0f);
     }
     static uint32_t spatial_key_bits(uint32_t mode) {
-        return mode == MK_MORTON_REFERENCE_30 ? 30u : mode == MK_MORTON_39 ? 39u : mode == MK_MORTON_48 ? 48u : 63u;
+        return mode == MK_MORTON_REFERENCE_30 || mode == MK_MORTON_30_ADAPTIVE ? 30u
+               : mode == MK_MORTON_39                                        ? 39u
+               : mode == MK_MORTON_48                                        ? 48u
+                                                                             : 63u;
     }
     // batched scenes: the scene index above the spatial key, whose lowest bits
     // give way when both do not fit in 63 bits
@@ -2556,6 +2562,9 @@ uint64_t or_morton48(float x, float y, float z, float lx, float ly, float lz, fl
 }
 uint64_t or_morton39(float x, float y, float z, float lx, float ly, float lz, float scale) {
     return World<float>::morton_frame(v3<float>(x, y, z), v3<float>(lx, ly, lz), scale, 8191.0f);
+}
+uint64_t or_morton30a(float x, float y, float z, float lx, float ly, float lz, float scale) {
+    return World<float>::morton_frame(v3<float>(x, y, z), v3<float>(lx, ly, lz), scale, 1023.0f);
 }
 
 }  // extern "C"

@@ -104,6 +104,7 @@ uint32_t or_morton30(float x, float y, float z);   /* lbvh.wgsl:84-98 */
 uint64_t or_morton63(float x, float y, float z, float lx, float ly, float lz, float scale);   /* 21 bits/axis over the centre bounds (lo, scale) */
 uint64_t or_morton48(float x, float y, float z, float lx, float ly, float lz, float scale);   /* 16 bits/axis over the centre bounds (lo, scale) */
 uint64_t or_morton39(float x, float y, float z, float lx, float ly, float lz, float scale);   /* 13 bits/axis over the centre bounds (lo, scale) */
+uint64_t or_morton30a(float x, float y, float z, float lx, float ly, float lz, float scale);  /* 10 bits/axis over the centre bounds (lo, scale) */
 
 #ifdef __cplusplus
 }

@@ -7,7 +7,7 @@ the handle's state must be restored after the search.
 """
 import pytest
 
-from mechanic_b200 import scenes
+from mechanic_b200 import abi, scenes
 from mechanic_b200.physics import GpuPhysics, GpuPhysicsConfig
 
 from test_gpu_parity import assert_bitwise
@@ -26,6 +26,7 @@ def test_autotune_keeps_results_and_state(cuda_lib):
     before = a.save_state()
     tuning, ms = a.autotune(ticks=2)
     assert ms > 0 and tuning["sort_items"] in (2, 4, 6, 8, 11, 16)
+    assert tuning["morton_mode"] in (abi.MORTON_39, abi.MORTON_30_ADAPTIVE)   # either key width: same pairs
     after = a.save_state()
     assert_bitwise(after["transforms"], before["transforms"], "restored transforms")
     assert_bitwise(after["velocities"], before["velocities"], "restored velocities")

@@ -102,10 +102,11 @@ def test_reference_morton_mode_same_pairs(cuda_lib):
         compare_tick(gpu, orc, tick)
 
 
-@pytest.mark.parametrize("mode", [abi.MORTON_63, abi.MORTON_48], ids=["63-bit", "48-bit"])
+@pytest.mark.parametrize("mode", [abi.MORTON_63, abi.MORTON_48, abi.MORTON_30_ADAPTIVE],
+                         ids=["63-bit", "48-bit", "30-bit-adaptive"])
 def test_other_morton_modes_bitexact(cuda_lib, mode):
-    """21 and 16 bits per axis (three and one radix passes more than the default 13): the same
-    bit-exact path (keys, permutation, topology, pairs, contacts, state)."""
+    """21, 16 and 10 bits per axis (the default has 13): the same bit-exact path (keys,
+    permutation, topology, pairs, contacts, state)."""
     scene = scenes.stack_grid(10, 6, 10, seed=5)
     gpu, orc = make_pair(scene, GpuPhysicsConfig(morton_mode=mode))
     for tick in range(1, 4):

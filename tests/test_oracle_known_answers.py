@@ -129,6 +129,15 @@ def test_morton39_is_13_bits_per_axis():
     assert oracle.morton39(1.0, 2.0, 3.0, lo, scale) < oracle.morton39(1.0, 2.0, 3.5, lo, scale)
 
 
+def test_morton30a_is_10_bits_per_axis():
+    lo, scale = (-5.0, -5.0, -5.0), float(np.float32(1023.0) / np.float32(10.0))
+    assert oracle.morton30a(-5.0, -5.0, -5.0, lo, scale) == 0
+    assert oracle.morton30a(5.0, 5.0, 5.0, lo, scale) == (1 << 30) - 1
+    cell = 10.0 / 1023.0
+    assert oracle.morton30a(-5.0 + 1.5 * cell, -5.0, -5.0, lo, scale) == 1
+    assert oracle.morton30a(-5.0, -5.0, -5.0 + 1.5 * cell, lo, scale) == 4
+
+
 def test_morton48_is_16_bits_per_axis():
     # 2^16 - 1 cells over 10 m; the top corner fills all 48 bits
     lo, scale = (-5.0, -5.0, -5.0), float(np.float32(65535.0) / np.float32(10.0))
