@@ -60,9 +60,14 @@ BYTES_SOLVE_PER_CONTACT_ITER = 284     # contact 64 + idx 4 + 2 x (v 16 + w 16 +
 BYTES_APPLY_PER_BODY_ITER = 112        # deltas 24 + velocities 32 read, velocities 32 + deltas 24 written
 BYTES_PREPARE_PER_CONTACT = 340        # contact 64 + 2 x (v/w 32 + world mass 48) + manifold 96, 16 + 48 + 4 written
 # broadphase per collider: AABB + Morton 140 (collider 64 + pose 32 read, AABB 32 + key/value 12 written),
-# onesweep sort 132 (2 x 12 x 5 digit passes over the 39-bit keys + 12), Karras 24, refit 96 + 32,
-# traversal 32
-BYTES_BROADPHASE_PER_COLLIDER = 140 + 132 + 24 + 96 + 32 + 32
+# onesweep sort 2 x 12 per 8-bit digit pass over the key mode's bits + 12 histogram read, Karras 24,
+# refit 96 + 32, traversal 32
+KEY_BITS = {0: 63, 1: 30, 2: 48, 3: 39, 4: 30}   # MK_MORTON_63, _REFERENCE_30, _48, _39, _30_ADAPTIVE
+
+
+def bytes_broadphase_per_collider(morton_mode: int) -> int:
+    passes = (KEY_BITS[morton_mode] + 7) // 8
+    return 140 + (2 * 12 * passes + 12) + 24 + 96 + 32 + 32
 # per candidate pair: traversal output 8 + pair-key sort (5 digit passes x 16 + 8)
 BYTES_BROADPHASE_PER_PAIR = 8 + 88
 
@@ -364,7 +369,7 @@ def main():
                 stage_ms["narrowphase"] += kt.narrowphase_ms
                 stage_ms["contact_solver"] += kt.contact_solver_ms
                 counts.append((rb.pair_count, rb.contact_count, rb.active_contact_count))
-                broad_bytes += (BYTES_BROADPHASE_PER_COLLIDER * scene.collider_count
+                broad_bytes += (bytes_broadphase_per_collider(tuning["morton_mode"]) * scene.collider_count
                                 + BYTES_BROADPHASE_PER_PAIR * rb.pair_count)
                 # the apply touches at most the active contacts' bodies (2 per contact): light
                 # ticks apply only those, so counting every body would overstate the traffic
