@@ -1168,8 +1168,24 @@ __global__ void __launch_bounds__(kClosureThreads) k_closure_eval(StepBuffers b,
         fo[0] = f[0]; fo[1] = f[1]; fo[2] = f[2]; fo[3] = f[3];
     }
     // per-loop blocks: Cholesky of J^T J on the loop's coordinates plus a ridge of
-    // 1e-6 x the mean diagonal; a failed pivot leaves the block diagonal (Jacobi)
+    // 1e-6 x the mean diagonal; a failed pivot leaves the block diagonal (Jacobi).
+    // Across the grid the off-diagonal couplings (chains of dependent loads) are
+    // computed first, one entry per thread, into the block's packed storage, and
+    // one thread per loop then factors it; in one block the loop's thread
+    // computes them itself (the extra sync and round trip cost more there).
     if (p.precond == MK_PRECOND_BLOCK_JACOBI) {
+        if (kGrid) {
+            constexpr uint32_t kOff = kMaxLoop * (kMaxLoop - 1) / 2;   // strict lower entries of a block
+            for (uint32_t e = tid; e < p.loops * kOff; e += nt) {
+                const uint32_t lp = e / kOff;
+                uint32_t r = e % kOff, i = 1;
+                while (r >= i) { r -= i; ++i; }   // (i, r): row i > column r
+                const uint32_t o = m.loop_off[lp], n = m.loop_off[lp + 1] - o;
+                if (i < n)
+                    m.loop_l[36ull * lp + i * (i + 1) / 2 + r] = closure_coupling(m, m.loop_q[o + i], m.loop_q[o + r]);
+            }
+            loop_sync<kGrid>(m.grid_barrier, flags);
+        }
         for (uint32_t lp = tid; lp < p.loops; lp += nt) {
             const uint32_t o = m.loop_off[lp], n = m.loop_off[lp + 1] - o;
             float a[kMaxLoop * (kMaxLoop + 1) / 2];
@@ -1178,8 +1194,9 @@ __global__ void __launch_bounds__(kClosureThreads) k_closure_eval(StepBuffers b,
             mean = n ? mean / (float)n : 0.0f;
             for (uint32_t i = 0; i < n; ++i)
                 for (uint32_t j = 0; j <= i; ++j)
-                    a[i * (i + 1) / 2 + j] = i == j ? m.diag[m.cq_coords[m.loop_q[o + i]]] + 1.0e-6f * mean
-                                                    : closure_coupling(m, m.loop_q[o + i], m.loop_q[o + j]);
+                    a[i * (i + 1) / 2 + j] = i == j  ? m.diag[m.cq_coords[m.loop_q[o + i]]] + 1.0e-6f * mean
+                                             : kGrid ? m.loop_l[36ull * lp + i * (i + 1) / 2 + j]
+                                                     : closure_coupling(m, m.loop_q[o + i], m.loop_q[o + j]);
             bool ok = mean > 1.0e-12f;
             for (uint32_t j = 0; j < n && ok; ++j) {
                 float dj = a[j * (j + 1) / 2 + j];
