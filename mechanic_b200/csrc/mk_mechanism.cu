@@ -315,44 +315,61 @@ __device__ __forceinline__ void hinge_tangents(const StepBuffers& b, uint32_t a,
 }
 
 // articulated.wgsl:114-155, 287-316
+// One bearing per group of kRowLanes lanes, one row per lane (three linear,
+// two angular); the rows' fixed-point deltas are summed over the group by
+// shuffles (integer sums: the same totals in any order) and one lane flushes
+// them.  Every row reads the velocities of before the pass (Jacobi).
+constexpr uint32_t kRowLanes = 8;
 __global__ void __launch_bounds__(kMBlock) k_project_bearings(StepBuffers b, MechBuffers m, MechParams p) {
-    const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
-    if (j >= p.bearing_count) return;
-    const GpuBearing br = m.bearings[j];
-    const uint32_t a = br.metadata[0], c = br.metadata[1];
-    const f3 arm_a = quat_rotate(b.rot[a], r3(br.local_anchor_a)), arm_b = quat_rotate(b.rot[c], r3(br.local_anchor_b));
-    const f3 va = xyz(b.lin[a]) + cross(xyz(b.ang[a]), arm_a);
-    const f3 vb = xyz(b.lin[c]) + cross(xyz(b.ang[c]), arm_b);
-    const f3 rel = vb - va;
-    const float ima = inv_mass(b, a), imb = inv_mass(b, c);
-    const f3 dirs[3] = {mkf3(1, 0, 0), mkf3(0, 1, 0), mkf3(0, 0, 1)};
-    MDelta da{}, dc{};   // every row reads the velocities of before the pass (Jacobi)
-#pragma unroll
-    for (int k = 0; k < 3; ++k) {
-        const f3 d = dirs[k];
-        const f3 ang_a = cross(arm_a, d), ang_b = cross(arm_b, d);
-        const float den = ima + imb + dot(ang_a, wii(b, a, ang_a)) + dot(ang_b, wii(b, c, ang_b));
-        if (den <= 1.0e-12f) continue;
-        const f3 imp = d * (0.5f * dot(rel, d) / den);
-        mdelta_add(da, imp * ima, wii(b, a, cross(arm_a, imp)));
-        mdelta_add(dc, -imp * imb, wii(b, c, cross(arm_b, -imp)));
+    const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t j = g / kRowLanes, row = g % kRowLanes;
+    const bool live = j < p.bearing_count;   // whole groups share this (the grid covers whole groups)
+    MDelta da{}, dc{};
+    uint32_t a = 0, c = 0;
+    if (live) {
+        const GpuBearing br = m.bearings[j];
+        a = br.metadata[0];
+        c = br.metadata[1];
+        if (row < 3) {
+            const f3 arm_a = quat_rotate(b.rot[a], r3(br.local_anchor_a)), arm_b = quat_rotate(b.rot[c], r3(br.local_anchor_b));
+            const f3 va = xyz(b.lin[a]) + cross(xyz(b.ang[a]), arm_a);
+            const f3 vb = xyz(b.lin[c]) + cross(xyz(b.ang[c]), arm_b);
+            const f3 rel = vb - va;
+            const float ima = inv_mass(b, a), imb = inv_mass(b, c);
+            const f3 d = row == 0 ? mkf3(1, 0, 0) : row == 1 ? mkf3(0, 1, 0) : mkf3(0, 0, 1);
+            const f3 ang_a = cross(arm_a, d), ang_b = cross(arm_b, d);
+            const float den = ima + imb + dot(ang_a, wii(b, a, ang_a)) + dot(ang_b, wii(b, c, ang_b));
+            if (!(den <= 1.0e-12f)) {
+                const f3 imp = d * (0.5f * dot(rel, d) / den);
+                mdelta_add(da, imp * ima, wii(b, a, cross(arm_a, imp)));
+                mdelta_add(dc, -imp * imb, wii(b, c, cross(arm_b, -imp)));
+            }
+        } else if (row < 5) {
+            f3 ta, tb;
+            hinge_tangents(b, a, c, br, ta, tb);
+            const f3 rang = xyz(b.ang[c]) - xyz(b.ang[a]);
+            const f3 axis = row == 3 ? ta : tb;
+            const f3 ia = wii(b, a, axis), ib = wii(b, c, axis);
+            const float den = dot(axis, ia + ib);
+            if (!(den <= 1.0e-12f)) {
+                const float imp = 0.5f * dot(rang, axis) / den;
+                mdelta_add(da, mkf3(0, 0, 0), ia * imp);
+                mdelta_add(dc, mkf3(0, 0, 0), -ib * imp);
+            }
+        }
     }
-    f3 ta, tb;
-    hinge_tangents(b, a, c, br, ta, tb);
-    const f3 rang = xyz(b.ang[c]) - xyz(b.ang[a]);
-    const f3 tangents[2] = {ta, tb};
 #pragma unroll
-    for (int k = 0; k < 2; ++k) {
-        const f3 axis = tangents[k];
-        const f3 ia = wii(b, a, axis), ib = wii(b, c, axis);
-        const float den = dot(axis, ia + ib);
-        if (den <= 1.0e-12f) continue;
-        const float imp = 0.5f * dot(rang, axis) / den;
-        mdelta_add(da, mkf3(0, 0, 0), ia * imp);
-        mdelta_add(dc, mkf3(0, 0, 0), -ib * imp);
+    for (uint32_t o = kRowLanes / 2; o > 0; o >>= 1) {
+#pragma unroll
+        for (int q = 0; q < 6; ++q) {
+            da.v[q] += __shfl_down_sync(0xffffffffu, da.v[q], o, kRowLanes);
+            dc.v[q] += __shfl_down_sync(0xffffffffu, dc.v[q], o, kRowLanes);
+        }
     }
-    mdelta_flush(m.deltas, a, da);
-    mdelta_flush(m.deltas, c, dc);
+    if (live && row == 0) {
+        mdelta_flush(m.deltas, a, da);
+        mdelta_flush(m.deltas, c, dc);
+    }
 }
 
 // articulated.wgsl:318-337
@@ -1439,8 +1456,8 @@ static inline uint32_t nblocks(uint32_t n) { return (n + kMBlock - 1) / kMBlock;
 
 static cudaError_t bearing_projection_iteration(MechBuffers& m, const StepBuffers& b, const MechParams& p,
                                                 cudaStream_t s) {
-    // 64-thread blocks spread the bearings' atomics over more SMs
-    if (p.bearing_count) k_project_bearings<<<(p.bearing_count + 63) / 64, 64, 0, s>>>(b, m, p);
+    // a group of kRowLanes lanes per bearing, in 64-thread blocks (8 bearings each)
+    if (p.bearing_count) k_project_bearings<<<(p.bearing_count + 7) / 8, 64, 0, s>>>(b, m, p);
     k_apply_mdeltas<<<nblocks(p.body_count), kMBlock, 0, s>>>(b, m, p);
     return cudaGetLastError();
 }
