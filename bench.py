@@ -174,6 +174,21 @@ class ClockSampler:
 
 
 # ------------------------------------------------------------- cpu legs
+def bench_config(scene, args, world: int = 1) -> dict:
+    """The workload description both arms print (the same keys and values)."""
+    # HBM state every tick reads and writes: per body position, rotation, velocities,
+    # inverse mass, mass row, world inverse inertia, root flag, deltas, snapshot (240 B);
+    # per collider its row, world box, AABB, keys and values (ping-pong), LBVH node boxes,
+    # records, children, parents and visit counters (316 B)
+    working_set = 240 * scene.body_count + 316 * scene.collider_count
+    return {"workload": WORKLOAD, "bodies": scene.body_count, "colliders": scene.collider_count,
+            "ticks": f"1..{args.steps} from the generated state (warm-up state reloaded)",
+            "seed": args.seed, "pair_capacity": PAIR_CAPACITY,
+            "parallelism": "replicas" if world > 1 else "single",
+            "l2": ("flushed between ticks (256 MB written)" if args.flush_l2 else
+                   f"not flushed: per-tick state {working_set / 1e6:.0f} MB > 126 MB L2")}
+
+
 def cpu_trajectory(scene, ticks: int, budget_s: float, threads: int):
     """Steps the CPU oracle along ticks 1..ticks, stopping early once budget_s has passed."""
     import oracle
@@ -209,8 +224,7 @@ def run_reference(args, scene):
         "metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": 0,
         "steps": done, "warmup": args.warmup, "ms_per_step": 1e3 * elapsed / done, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded generator)",
-        "config": {"workload": WORKLOAD, "bodies": scene.body_count, "colliders": scene.collider_count,
-                   "ticks": args.steps, "seed": args.seed},
+        "config": bench_config(scene, args),
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": used, "kind": "port", "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "note": "the reference's wgpu pipeline needs a graphics stack that is unavailable on this box; "
@@ -322,11 +336,6 @@ def main():
     st = gpu.state_buffers()
     stream = torch.cuda.ExternalStream(st.stream, device=torch.device("cuda", local))
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{local}") if args.flush_l2 else None
-    # HBM state every tick reads and writes: per body position, rotation, velocities,
-    # inverse mass, mass row, world inverse inertia, root flag, deltas, snapshot (240 B);
-    # per collider its row, world box, AABB, keys and values (ping-pong), LBVH node boxes,
-    # records, children, parents and visit counters (316 B)
-    working_set = 240 * scene.body_count + 316 * scene.collider_count
 
     def reset():
         gpu.load_state(initial["transforms"], initial["velocities"], manifold=np.zeros(0, abi.CONTACT),
@@ -451,13 +460,9 @@ def main():
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded generator)",
-            "config": {"workload": WORKLOAD, "bodies": scene.body_count, "colliders": scene.collider_count,
-                       "ticks": f"1..{args.steps} from the generated state (warm-up state reloaded)",
-                       "parallelism": "replicas" if world > 1 else "single", "l2": ("flushed between ticks (256 MB written)" if args.flush_l2 else
-                              f"not flushed: per-tick state {working_set / 1e6:.0f} MB > 126 MB L2"),
-                       "pair_capacity": PAIR_CAPACITY, "tick1_pairs_contacts_active": list(tick1),
-                       "seed": args.seed, "launch_shapes": tuning,
-                       "autotune": "mk_autotune over the 8 ticks after the warm-up, state restored" if tuned_ms else "off"},
+            "config": bench_config(scene, args, world),
+            "run": {"tick1_pairs_contacts_active": list(tick1), "launch_shapes": tuning,
+                    "autotune": "mk_autotune over the 8 ticks after the warm-up, state restored" if tuned_ms else "off"},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 64,
                     "d2h_bytes_per_step": scene.body_count * abi.TRANSFORM.itemsize + 32 / args.steps,
                     "pipelining": "tick k's snapshot slot is read while tick k + 1 runs; diagnostics read after "

@@ -535,22 +535,28 @@ MK_API uint64_t mk_op_sort_scratch_bytes(uint32_t n);
  * sort_local_merge passes, lbvh.wgsl:132-217).  Equal keys keep input order,
  * which is the reference's (code, index) tie-break when values are indices.
  * `scratch` must hold mk_op_sort_scratch_bytes(n) bytes, 256-byte aligned.
- * Results land in keys_out / values_out; inputs are left unchanged. */
+ * Results land in keys_out / values_out; inputs are left unchanged.  Inputs
+ * and outputs must not overlap (MK_ERR_INVALID_ARGUMENT otherwise). */
 MK_API int mk_op_sort_keys(const uint64_t* keys_in, const uint32_t* values_in,
                     uint64_t* keys_out, uint32_t* values_out, uint32_t n,
                     uint32_t key_bits, void* scratch, uint64_t scratch_bytes,
                     void* stream);
 
 /* The same sort for callers that cannot allocate device memory when they
- * need it (code inside host callbacks or allocator hooks, embedders with a
- * fixed memory budget).  No counterpart in the reference.  Its scratch is a
- * static device array owned by the library (about 14 MB on every GPU that
- * loads it, kept until exit), so only inputs and outputs are passed and
- * nothing is allocated.  At most MK_STATIC_SORT_MAX_KEYS keys; larger n
- * returns MK_ERR_INVALID_ARGUMENT with the reason in mk_last_error().  The
- * first call on each device (with it current) looks up the array's device
- * address: make it before any stream capture.  All calls share the array, so
- * calls that overlap on the GPU race and must be ordered by the caller. */
+ * need it (allocator and memory-pool hooks that must not recurse into the
+ * allocator, embedders with a fixed memory budget).  No counterpart in the
+ * reference.  Its scratch is a static device array owned by the library
+ * (about 14 MB on every GPU that loads it, kept until exit), so only inputs
+ * and outputs are passed and nothing is allocated.  It launches kernels on
+ * `stream`, so it must not be called from inside a CUDA host function
+ * (cudaLaunchHostFunc, stream callbacks), where no CUDA call is allowed.  At
+ * most MK_STATIC_SORT_MAX_KEYS keys; larger n, or inputs that overlap the
+ * outputs, return MK_ERR_INVALID_ARGUMENT with the reason in mk_last_error().
+ * The first call on each device (with it current) looks up the array's
+ * device address and keeps it: make that call before any stream capture, and
+ * make no call after cudaDeviceReset in the same process (the kept address
+ * belongs to the context the reset destroyed).  All calls share the array,
+ * so calls that overlap on the GPU race and must be ordered by the caller. */
 #define MK_STATIC_SORT_MAX_KEYS 524288u
 MK_API int mk_op_sort_keys_static(const uint64_t* keys_in, const uint32_t* values_in,
                                   uint64_t* keys_out, uint32_t* values_out, uint32_t n,

@@ -138,6 +138,20 @@ class MkConfig(C.Structure):
     ]
 
 
+def config_default() -> MkConfig:
+    """The values mk_config_default writes (GpuPhysicsConfig::default,
+    device.rs:33-41, plus this build's key width), filled without loading the
+    CUDA library so that CPU-only code can build a configuration row."""
+    c = MkConfig()
+    c.collisions_enabled = 1
+    c.mechanism_self_collisions = 1
+    c.solver_iterations = 8
+    c.morton_mode = MORTON_39
+    c.closure_mode = CLOSURE_REFERENCE
+    c.use_graph = 1
+    return c
+
+
 class MkCapacities(C.Structure):
     _fields_ = [("max_bodies", C.c_uint32), ("max_colliders", C.c_uint32),
                 ("max_bearings", C.c_uint32), ("pair_capacity", C.c_uint32)]

@@ -1484,6 +1484,10 @@ int mk_op_sort_keys(const uint64_t* keys_in, const uint32_t* values_in, uint64_t
         set_error(nullptr, MK_ERR_INVALID_ARGUMENT, "sort: scratch too small or not 256-byte aligned");
         return MK_ERR_INVALID_ARGUMENT;
     }
+    if (mk::sort_buffers_overlap(keys_in, values_in, keys_out, values_out, n)) {
+        set_error(nullptr, MK_ERR_INVALID_ARGUMENT, "sort: input and output buffers overlap");
+        return MK_ERR_INVALID_ARGUMENT;
+    }
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);

@@ -12,6 +12,22 @@ namespace mk {
 
 inline uint64_t align256(uint64_t b) { return (b + 255) & ~255ull; }
 
+// True when the byte ranges [a, a + a_bytes) and [b, b + b_bytes) share a byte.
+inline bool ranges_overlap(const void* a, uint64_t a_bytes, const void* b, uint64_t b_bytes) {
+    const uintptr_t x = (uintptr_t)a, y = (uintptr_t)b;
+    return x < y + b_bytes && y < x + a_bytes;
+}
+
+// A sort whose input and output overlap gives wrong results: with an odd
+// pass count the first pass reads keys_in while it writes keys_out.
+inline bool sort_buffers_overlap(const void* keys_in, const void* values_in, const void* keys_out,
+                                 const void* values_out, uint32_t n) {
+    const uint64_t kb = 8ull * n, vb = 4ull * n;
+    return ranges_overlap(keys_in, kb, keys_out, kb) || ranges_overlap(keys_in, kb, values_out, vb) ||
+           ranges_overlap(values_in, vb, keys_out, kb) || ranges_overlap(values_in, vb, values_out, vb) ||
+           ranges_overlap(keys_out, kb, values_out, vb);
+}
+
 // Records the text mk_last_error() returns on this thread.
 void set_last_error(const char* msg);
 

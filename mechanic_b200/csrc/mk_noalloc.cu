@@ -1,19 +1,23 @@
 // mk_noalloc.cu — the LBVH key sort for callers that cannot allocate.
 //
 // Some callers cannot call cudaMalloc at the point where they need the sort:
-// code running inside a host callback or a stream-ordered completion handler
-// (where CUDA API calls that may synchronize are forbidden), allocators and
-// memory-pool hooks that must not recurse into the allocator, and embedders
-// whose memory budget is fixed up front and must not grow.  For them this
-// file keeps the sort's scratch in one statically sized device array that the
-// library owns, so a call needs only the caller's input and output buffers.
+// allocators and memory-pool hooks that must not recurse into the allocator,
+// and embedders whose memory budget is fixed up front and must not grow.  For
+// them this file keeps the sort's scratch in one statically sized device array
+// that the library owns, so a call needs only the caller's input and output
+// buffers.  The call still launches kernels on the caller's stream, so it is
+// not for code running inside a CUDA host function (cudaLaunchHostFunc or a
+// stream callback), where CUDA forbids every CUDA API call.
 //
 // The array is a file-scope __device__ variable: every GPU that loads the
 // library holds it until the process exits.  In host code its name is only a
 // host-side stand-in, never a device address, so the first call on each
 // device (with that device current) looks up the real address with
 // cudaGetSymbolAddress and caches it; make that first call before any stream
-// capture, because the lookup may load the module.  Every call shares the one
+// capture, because the lookup may load the module.  The cached address belongs
+// to the device's primary context: after cudaDeviceReset (or anything else that
+// destroys and recreates that context) it is stale, and this entry point must
+// not be called again in that process.  Every call shares the one
 // array and it keeps the previous call's contents: the sort clears what must
 // start at zero (bins, tile tickets, look-back words) itself, and two calls
 // whose work overlaps on the GPU (different streams, or several host threads)
@@ -64,6 +68,8 @@ int mk_op_sort_keys_static(const uint64_t* keys_in, const uint32_t* values_in, u
                       kStaticSortMaxKeys);
         return fail(MK_ERR_INVALID_ARGUMENT, msg);
     }
+    if (mk::sort_buffers_overlap(keys_in, values_in, keys_out, values_out, n))
+        return fail(MK_ERR_INVALID_ARGUMENT, "sort_keys_static: input and output buffers overlap");
     if (mk::sort_scratch_bytes(n, key_bits, true) > kStaticSortScratchBytes)
         return fail(MK_ERR_INVALID_ARGUMENT, "sort_keys_static: scratch layout exceeds the static array");
     int dev = 0;

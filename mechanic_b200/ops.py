@@ -26,9 +26,7 @@ def sort_keys(keys: torch.Tensor, values: torch.Tensor, key_bits: int = 63):
     if n == 0:
         return k_out, v_out
     L = library()
-    need = int(L.mk_op_sort_scratch_bytes(n)) if key_bits == 63 else None
-    if need is None:
-        need = int(L.mk_op_sort_scratch_bytes(n))
+    need = int(L.mk_op_sort_scratch_bytes(n))   # sized for the widest (64-bit) keys, so any key_bits fits
     scratch = torch.empty(need + 256, dtype=torch.uint8, device=keys.device)
     base = scratch.data_ptr()
     aligned = (base + 255) & ~255

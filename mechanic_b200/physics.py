@@ -160,8 +160,7 @@ class GpuPhysicsConfig:
     contact_manifold: int = abi.MANIFOLD_POINT
 
     def to_c(self) -> abi.MkConfig:
-        c = abi.MkConfig()
-        library().mk_config_default(C.byref(c))
+        c = abi.config_default()   # equals mk_config_default's row (checked by a CPU test)
         c.collisions_enabled = int(self.collisions_enabled)
         c.mechanism_self_collisions = int(self.mechanism_self_collisions)
         c.solver_iterations = int(self.solver_iterations)

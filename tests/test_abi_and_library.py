@@ -9,6 +9,7 @@ import ctypes
 import os
 import re
 import subprocess
+import sys
 
 import numpy as np
 import pytest
@@ -87,6 +88,20 @@ def test_library_loads_without_gpu_and_reports_version():
     lib.mk_config_default(ctypes.byref(c))
     assert (c.collisions_enabled, c.mechanism_self_collisions, c.solver_iterations) == (1, 1, 8)
     assert c.use_graph == 1 and c.morton_mode == abi.MORTON_39
+    # the host-side default row (used without loading the library) is the same bytes
+    assert bytes(abi.config_default()) == bytes(c)
+
+
+def test_config_row_needs_no_library():
+    """GpuPhysicsConfig.to_c() (used by the CPU oracle's callers) does not load libmechanic_b200."""
+    code = ("import sys; sys.path.insert(0, %r)\n"
+            "from mechanic_b200.physics import GpuPhysicsConfig\n"
+            "from mechanic_b200 import physics\n"
+            "c = GpuPhysicsConfig(solver_iterations=4).to_c()\n"
+            "assert c.solver_iterations == 4 and physics._lib is None\n"
+            "maps = open('/proc/self/maps').read()\n"
+            "assert 'libmechanic_b200' not in maps, 'library mapped'\n") % ROOT
+    subprocess.run([sys.executable, "-c", code], check=True)
 
 
 def test_create_rejects_over_capacity_before_touching_a_device():
