@@ -382,6 +382,8 @@ enum {
     MK_BUF_NODE_RECORDS = 17,      /* float4[8] per internal node (collider_count-1): its traversal record, up to
                                       four grandchildren in leaf order as {min.xyz, code} {max.xyz, last leaf};
                                       code = node index or 0x80000000 | collider index; unused entries zero */
+    MK_BUF_CONTACT_KEYS = 18,      /* uint64[contact_count]: collider a << 32 | collider b (0xffffffff for the
+                                      ground) of each contact row */
 };
 
 /* ---------------------------------------------------------------------------
@@ -625,6 +627,32 @@ MK_API int mk_op_mlp_train(float* params, float* adam_m, float* adam_v, const fl
                            const float* out_weights, uint32_t n, uint32_t batch, uint32_t steps, float lr,
                            uint32_t first_step, float* losses, void* scratch, uint64_t scratch_bytes,
                            uint32_t* error_flags, void* stream);
+
+/* ---------------------------------------------------------------------
+ * Self-test of the bounded device waits (no reference counterpart: the
+ * reference's waits, the storageBarrier refit of lbvh.wgsl:290-319, assume
+ * arrival).  Every spin-wait in this library's kernels gives up after an
+ * iteration limit, raises MK_DEVICE_WAIT_TIMEOUT_FLAG and returns.  This
+ * call runs the same device wait functions on a wait that nothing can
+ * satisfy, with `spin_limit` (1..65536) polls instead of the kernels' 2^20:
+ * a grid barrier expecting one block more than were launched, an ordered-
+ * append look-back tile whose predecessor never publishes, or an mbarrier
+ * no thread arrives on.  It allocates a few bytes of device memory on the
+ * current device, runs on its own stream and returns once the probe ended. */
+enum {
+    MK_WAIT_PROBE_GRID_BARRIER = 0,
+    MK_WAIT_PROBE_LOOKBACK = 1,
+    MK_WAIT_PROBE_MBARRIER = 2,
+};
+typedef struct MkWaitProbe {
+    uint32_t error_flags;       /* MK_DEVICE_WAIT_TIMEOUT_FLAG when the wait gave up */
+    uint32_t blocks_launched;
+    uint32_t blocks_finished;   /* blocks that reached the end of the probe kernel */
+    uint32_t pad;
+    uint64_t lookback_prefix;   /* look-back probe: the prefix the tile went on with (0) */
+    double elapsed_ms;          /* device time of the probe kernel */
+} MkWaitProbe;
+MK_API int mk_selftest_bounded_wait(uint32_t which, uint32_t spin_limit, MkWaitProbe* out, MkError* err);
 
 #ifdef __cplusplus
 }

@@ -138,6 +138,16 @@ class MkConfig(C.Structure):
     ]
 
 
+class MkWaitProbe(C.Structure):
+    _fields_ = [("error_flags", C.c_uint32), ("blocks_launched", C.c_uint32), ("blocks_finished", C.c_uint32),
+                ("pad", C.c_uint32), ("lookback_prefix", C.c_uint64), ("elapsed_ms", C.c_double)]
+
+
+WAIT_PROBE_GRID_BARRIER = 0
+WAIT_PROBE_LOOKBACK = 1
+WAIT_PROBE_MBARRIER = 2
+
+
 def config_default() -> MkConfig:
     """The values mk_config_default writes (GpuPhysicsConfig::default,
     device.rs:33-41, plus this build's key width), filled without loading the
@@ -234,6 +244,7 @@ BUF_CLOSURE_SLOTS = 14
 BUF_CLOSURE_BLOCKS = 15
 BUF_CLOSURE_BLOCK_OUTPUTS = 16
 BUF_NODE_RECORDS = 17
+BUF_CONTACT_KEYS = 18
 
 
 def ptr(a: np.ndarray | None) -> int | None:

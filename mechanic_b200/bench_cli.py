@@ -14,6 +14,8 @@ the reference's field names and gate logic (main.rs:155-272).  Scenarios:
   invalid_loop the four-bar with its closure anchor moved (main.rs:211-216); passes when
                CONSTRAINT_NON_CONVERGENCE_FLAG is raised
   chains_20k   4,000 five-link bearing chains, 10% loop-closed (the articulated config)
+  loops_100k   100 x 100 x 10 lattice of 1 m cubes joined by 198,009 bearings, 98,010 of them
+               loop closures (main.rs:370, build_loops_100k)
 
     python -m mechanic_b200.bench_cli --scenario dense_100k [--seconds N] [--warmup N]
                                       [--ticks N] [--warmup-ticks N]
@@ -39,6 +41,7 @@ SCENARIOS = {
     "four_bar": lambda: scenes.four_bar(False),
     "invalid_loop": lambda: scenes.four_bar(True),
     "chains_20k": lambda: scenes.bearing_chains(),
+    "loops_100k": lambda: scenes.loops_grid(100, 100, 10),
 }
 SHORT = {"smoke", "plain_small", "four_bar", "invalid_loop"}
 LINKAGES = {"four_bar", "invalid_loop"}

@@ -15,7 +15,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB_PATH = os.path.join(HERE, "libmechanic_b200.so")
 BUILD_DIR = os.path.join(HERE, "_build")
-SOURCES = ["mk_api.cu", "mk_step.cu", "mk_sort.cu", "mk_mechanism.cu", "mk_noalloc.cu", "mk_mlp.cu"]
+SOURCES = ["mk_api.cu", "mk_step.cu", "mk_sort.cu", "mk_mechanism.cu", "mk_noalloc.cu", "mk_mlp.cu",
+           "mk_waits.cu"]
 HEADERS = ["mk_device.cuh", "mk_internal.h", "mk_mechanism.h", "mk_mlp.h", "mk_tc.cuh"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "--fmad=false", "-prec-div=true", "-prec-sqrt=true",

@@ -1439,6 +1439,7 @@ int mk_read_buffer(MkHandle* h, uint32_t id, void* host, uint64_t cap_bytes, uin
         case MK_BUF_ACTIVE: src = b.active; n = counts.active; row = 4; break;
         case MK_BUF_COLLIDER_KEYS: src = b.keys; n = h->C; row = 8; break;
         case MK_BUF_CONTACT_FEATURES: src = b.features[last]; n = counts.contacts; row = 4; break;
+        case MK_BUF_CONTACT_KEYS: src = b.contact_keys[last]; n = counts.contacts; row = 8; break;
         case MK_BUF_WORLD_MASSES: src = b.world_mass; n = h->B; row = 48; break;
         case MK_BUF_LINKS: src = h->mech.links_final; n = h->mech.links_final ? h->B : 0; row = 48; break;
         case MK_BUF_WARM_PREDICTIONS: src = b.warm_pred; n = b.warm_pred ? counts.active : 0; row = 4; break;

@@ -152,7 +152,8 @@ __device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t v, uint32_t* s
 // --------------------------------------------------- ordered tile look-back
 // Decoupled look-back over tiles handed out in ticket order.  Each 64-bit
 // word packs status (bits 62-63: 1 = aggregate, 2 = inclusive prefix) and a
-// 62-bit count.  Waits are bounded: after kSpinLimit polls the tile gives up,
+// 62-bit count.  Waits are bounded: after kSpinLimit polls (a smaller limit
+// only in the bounded-wait self-test) the tile gives up,
 // raises MK_DEVICE_WAIT_TIMEOUT_FLAG and treats the missing predecessor as 0
 // (results are then wrong but the GPU never hangs).
 constexpr uint64_t kStatusAggregate = 1ull << 62;
@@ -209,7 +210,7 @@ __device__ __forceinline__ uint32_t atomic_add_acq_rel(uint32_t* p, uint32_t v) 
 // relaxed: each carries its own status and count, nothing else is published
 // through them, and a release store's fence costs an L2 round trip per tile.
 __device__ __forceinline__ uint64_t tile_lookback(uint64_t* states, uint32_t tile, uint64_t aggregate,
-                                                  uint32_t* error_flags) {
+                                                  uint32_t* error_flags, uint32_t spin_limit = kSpinLimit) {
     const uint32_t lane = lane_id();
     if (tile == 0) {
         if (lane == 0) st_relaxed_u64(states, kStatusInclusive | aggregate);
@@ -225,7 +226,7 @@ __device__ __forceinline__ uint64_t tile_lookback(uint64_t* states, uint32_t til
         uint64_t v = idx >= 0 ? ld_relaxed_u64(states + idx) : kStatusInclusive;
         uint32_t ready = __ballot_sync(0xffffffffu, (v >> 62) != 0);
         if (ready != 0xffffffffu) {
-            if (++spins > kSpinLimit) { timed_out = true; v = (v >> 62) ? v : kStatusInclusive; }
+            if (++spins > spin_limit) { timed_out = true; v = (v >> 62) ? v : kStatusInclusive; }
             else continue;
         }
         uint32_t inclusive = __ballot_sync(0xffffffffu, (v >> 62) == 2);
@@ -249,7 +250,8 @@ __device__ __forceinline__ uint64_t tile_lookback(uint64_t* states, uint32_t til
 // bits return to zero for the next barrier (one atomic per block, no reset
 // step).  The wait is bounded: a block that gives up raises
 // MK_DEVICE_WAIT_TIMEOUT_FLAG and carries on.
-__device__ __forceinline__ void grid_barrier(uint32_t* state, uint32_t* error_flags, uint32_t participants) {
+__device__ __forceinline__ void grid_barrier(uint32_t* state, uint32_t* error_flags, uint32_t participants,
+                                             uint32_t spin_limit = kSpinLimit) {
     __syncthreads();
     if (threadIdx.x == 0) {
         const uint32_t add = blockIdx.x == 0 ? 0x80000000u - (participants - 1u) : 1u;
@@ -257,7 +259,7 @@ __device__ __forceinline__ void grid_barrier(uint32_t* state, uint32_t* error_fl
         const uint32_t old = atomicAdd(state, add);
         uint32_t spins = 0;
         while (((ld_acquire_u32(state) ^ old) & 0x80000000u) == 0u) {
-            if (++spins > kSpinLimit) {
+            if (++spins > spin_limit) {
                 atomicOr(error_flags, MK_DEVICE_WAIT_TIMEOUT_FLAG);
                 break;
             }

@@ -28,7 +28,7 @@ EXPORTS = [
     "mk_mlp_param_count", "mk_op_mlp_scratch_bytes", "mk_op_mlp_forward", "mk_op_mlp_gradient",
     "mk_op_mlp_train", "mk_set_warm_start_network", "mk_read_warm_start_samples",
     "mk_set_preconditioner_network", "mk_create_batch", "mk_scene_offsets", "mk_get_handle_tuning",
-    "mk_set_handle_tuning", "mk_autotune",
+    "mk_set_handle_tuning", "mk_autotune", "mk_selftest_bounded_wait",
 ]
 
 _lib = None
@@ -83,6 +83,7 @@ def library(path: str | None = None):
         "mk_get_handle_tuning": (i32, [vp, vp]),
         "mk_set_handle_tuning": (i32, [vp, vp, vp]),
         "mk_autotune": (i32, [vp, u32, vp, vp, vp]),
+        "mk_selftest_bounded_wait": (i32, [u32, u32, vp, vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -468,6 +469,10 @@ class GpuPhysics:
     def contacts(self):
         return self.read_buffer(abi.BUF_CONTACTS, abi.CONTACT, 64)
 
+    def contact_keys(self):
+        """collider a << 32 | collider b of each contact row (0xffffffff: the ground)."""
+        return self.read_buffer(abi.BUF_CONTACT_KEYS, np.uint64, 8)
+
     def features(self):
         return self.read_buffer(abi.BUF_CONTACT_FEATURES, np.uint32, 4)
 
@@ -513,6 +518,14 @@ TUNE_CLOSURE_GRID = 2   # reference-mode closure loop: 0 by size, 1 one block, 2
 def set_tuning(key: int, value: int) -> int:
     """Process-wide tuning knob (mk_set_tuning); applies to handles created afterwards."""
     return int(library().mk_set_tuning(int(key), int(value)))
+
+
+def selftest_bounded_wait(which: int, spin_limit: int = 1000) -> abi.MkWaitProbe:
+    """Runs one bounded-wait probe (abi.WAIT_PROBE_*) on the current device."""
+    out = abi.MkWaitProbe()
+    err = abi.MkError()
+    _raise(library().mk_selftest_bounded_wait(int(which), int(spin_limit), C.byref(out), C.byref(err)), err)
+    return out
 
 
 def version() -> str:

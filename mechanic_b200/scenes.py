@@ -594,6 +594,191 @@ def four_bar(invalid: bool = False) -> Scene:
     return with_suppression(scene, [(0, 1), (1, 2), (2, 3), (3, 0)])
 
 
+# ---------------------------------------------------- mechanism compilation
+class _DisjointSet:
+    """Union by rank with path compression; on equal ranks the first argument's root
+    stays the root (compile.rs:936-976), so representatives match the reference's."""
+
+    def __init__(self, n: int):
+        self.parent = list(range(n))
+        self.rank = [0] * n
+
+    def find(self, item: int) -> int:
+        root = item
+        while self.parent[root] != root:
+            root = self.parent[root]
+        while self.parent[item] != item:
+            self.parent[item], item = root, self.parent[item]
+        return root
+
+    def union(self, a: int, b: int) -> None:
+        ra, rb = self.find(a), self.find(b)
+        if ra == rb:
+            return
+        if self.rank[ra] < self.rank[rb]:
+            ra, rb = rb, ra
+        self.parent[rb] = ra
+        if self.rank[ra] == self.rank[rb]:
+            self.rank[ra] += 1
+
+
+def compile_mechanism(scene: Scene, body_a, body_b, anchors, axes, driven=None, drives=None) -> Scene:
+    """Bearing topology of a creation, as mechanic-core's compile does it, for bearings
+    given in graph order as (body a, body b, shared world anchor, world axis); bodies are
+    single compounds with identity root rotation (compile.rs:333), so a bearing's local
+    anchors are the anchor minus each body's centre and both local axes are the axis.
+
+    Restates compile.rs:394-475 (spanning forest: driven bearings first, then the rest, in
+    graph order, never joining two fixed trees; tree bearings get coordinates in graph
+    order, the others are loop closures), :477-486 (mechanism components: bearing-connected
+    bodies keyed by their union-find representative), :504-609 (BFS from each component's
+    static bodies, else its first body, over tree bearings sorted by (neighbour, bearing,
+    direction); postorder by depth descending, then body) and device.rs:1699-1760 (the
+    GpuMechanismBody rows).  `drives` (one GpuMechanismDrive per coordinate) defaults to
+    passive rows.  Returns the scene with bearings, drives, mechanism rows and the
+    bearing-connected body pairs suppressed (compile.rs:373)."""
+    n = scene.body_count
+    a = np.asarray(body_a, np.int64)
+    b = np.asarray(body_b, np.int64)
+    J = len(a)
+    anchors = np.asarray(anchors, np.float64).reshape(J, 3)
+    axes = np.asarray(axes, np.float32).reshape(J, 3)
+    driven = np.zeros(J, bool) if driven is None else np.asarray(driven, bool)
+    static = scene.masses["inverse_mass"][:, 0] == 0.0
+    # spanning forest (compile.rs:401-425)
+    forest = _DisjointSet(n)
+    fixed = static.tolist()
+    tree = np.zeros(J, bool)
+    al, bl = a.tolist(), b.tolist()
+    for driven_pass in (True, False):
+        for j in np.nonzero(driven == driven_pass)[0].tolist():
+            ra, rb = forest.find(al[j]), forest.find(bl[j])
+            if ra == rb or (fixed[ra] and fixed[rb]):
+                continue
+            has_fixed = fixed[ra] or fixed[rb]
+            forest.union(ra, rb)
+            fixed[forest.find(ra)] = has_fixed
+            tree[j] = True
+    if np.any(driven & ~tree):
+        raise ValueError("a driven bearing closes a loop (TopologyError::DrivenClosureBearing)")
+    coord = np.full(J, abi.INVALID_INDEX, np.uint32)
+    coord[tree] = np.arange(int(tree.sum()), dtype=np.uint32)
+    pos = scene.transforms["position"][:, :3].astype(np.float64)
+    rows = np.zeros(J, abi.BEARING)
+    rows["local_anchor_a"][:, :3] = (anchors - pos[a]).astype(np.float32)
+    rows["local_anchor_b"][:, :3] = (anchors - pos[b]).astype(np.float32)
+    rows["local_axis_a"][:, :3] = axes
+    rows["local_axis_b"][:, :3] = axes
+    rows["metadata"][:, 0] = a
+    rows["metadata"][:, 1] = b
+    rows["metadata"][:, 2] = coord
+    rows["metadata"][:, 3] = (~tree).astype(np.uint32)
+    # mechanism components (compile.rs:348, :477-484): representative order, bodies ascending
+    comps = _DisjointSet(n)
+    for j in range(J):
+        comps.union(al[j], bl[j])
+    rep = np.array([comps.find(i) for i in range(n)], np.int64)
+    reps, first = np.unique(rep, return_index=True)          # ascending representative
+    component_of = np.searchsorted(reps, rep).astype(np.uint32)
+    members = [np.nonzero(rep == r)[0] for r in reps] if len(reps) < 64 else None
+    # adjacency over tree bearings, sorted by (neighbour, bearing row, direction)
+    ta, tb, tj = a[tree], b[tree], np.nonzero(tree)[0]
+    nb = np.concatenate([tb, ta])
+    src = np.concatenate([ta, tb])
+    jj = np.concatenate([tj, tj])
+    dirn = np.concatenate([np.zeros(len(tj), np.int64), np.ones(len(tj), np.int64)])
+    order = np.lexsort((dirn, jj, nb, src))
+    src, nb, jj, dirn = src[order], nb[order], jj[order], dirn[order]
+    starts = np.searchsorted(src, np.arange(n + 1))
+    parent = np.full(n, -1, np.int64)
+    tree_bearing = np.full(n, -1, np.int64)
+    direction = np.zeros(n, np.uint32)
+    depth = np.zeros(n, np.int64)
+    pre = np.zeros(n, np.int64)
+    visited = np.zeros(n, bool)
+    count = 0
+    from collections import deque
+    nb_l, jj_l, dir_l, st_l = nb.tolist(), jj.tolist(), dirn.tolist(), starts.tolist()
+    for ci, r in enumerate(reps.tolist()):
+        body_list = members[ci] if members is not None else np.nonzero(rep == r)[0]
+        roots = [int(x) for x in body_list if static[x]] or [int(body_list[0])]
+        for root in roots:
+            if visited[root]:
+                continue
+            visited[root] = True
+            queue = deque([root])
+            while queue:
+                p = queue.popleft()
+                pre[p] = count
+                count += 1
+                for e in range(st_l[p], st_l[p + 1]):
+                    c = nb_l[e]
+                    if visited[c]:
+                        continue
+                    visited[c] = True
+                    parent[c] = p
+                    tree_bearing[c] = jj_l[e]
+                    direction[c] = dir_l[e]
+                    depth[c] = depth[p] + 1
+                    queue.append(c)
+    post_order = np.lexsort((np.arange(n), -depth))
+    post = np.zeros(n, np.int64)
+    post[post_order] = np.arange(n)
+    scene = dataclasses.replace(scene, bearings=rows)
+    q = int(tree.sum())
+    scene.drives = abi.passive_drive_rows(q) if drives is None else drives
+    scene.coordinate_count = q
+    scene.max_depth = int(depth.max()) if n else 0
+    scene.closure_count = int((~tree).sum())
+    root = parent < 0
+    scene.has_dynamic_root = int(np.any(root & ~static))
+    _mechanism_rows(scene, parent, tree_bearing, component_of, depth.astype(np.uint32), pre.astype(np.uint32),
+                    post.astype(np.uint32))
+    scene.mechanism_bodies["metadata"][:, 2] = np.where(root, 0, direction).astype(np.uint32)
+    return with_suppression(scene, np.stack([a, b], 1))
+
+
+def loops_grid(width: int = 100, height: int = 100, depth: int = 10) -> Scene:
+    """mechanic-bench's loops_100k (crates/mechanic-bench/src/main.rs:456-524): a width x
+    height x depth lattice of one-metre cubes at 1 m pitch, centres at (x, y, z) metres,
+    reference density 500 kg/m^3; in every z layer each cube is joined to its +x
+    neighbour by a bearing about X at the shared face centre and to its +y neighbour by
+    one about Y, and the (0, 0) cubes of consecutive layers by bearings about Z.  At
+    100 x 100 x 10: 100,000 bodies, 198,009 bearings, 99,999 tree coordinates and 98,010
+    loop closures."""
+    part = lambda x, y, z: (z * height + y) * width + x   # noqa: E731
+    n = width * height * depth
+    idx = np.arange(n)
+    x, y, z = idx % width, (idx // width) % height, idx // (width * height)
+    translation = np.stack([x, y, z], 1).astype(np.float32)
+    rotation = np.zeros((n, 4))
+    rotation[:, 3] = 1.0
+    zeros = np.zeros(n)
+    scene = _assemble(translation, rotation, np.zeros(n, bool), zeros, zeros, zeros, (1.0, 1.0, 1.0),
+                      f"loops_{n}", density=REFERENCE_DENSITY)
+    A, Bb, anchor, axis = [], [], [], []
+    gx, gy = np.meshgrid(np.arange(width - 1), np.arange(height), indexing="xy")
+    hx, hy = np.meshgrid(np.arange(width), np.arange(height - 1), indexing="xy")
+    for zz in range(depth):
+        xa = part(gx, gy, zz).ravel()
+        A.append(xa)
+        Bb.append(xa + 1)
+        anchor.append(np.stack([gx.ravel() + 0.5, gy.ravel(), np.full(gx.size, zz)], 1))
+        axis.append(np.tile([1.0, 0.0, 0.0], (gx.size, 1)))
+        ya = part(hx, hy, zz).ravel()
+        A.append(ya)
+        Bb.append(ya + width)
+        anchor.append(np.stack([hx.ravel(), hy.ravel() + 0.5, np.full(hx.size, zz)], 1))
+        axis.append(np.tile([0.0, 1.0, 0.0], (hx.size, 1)))
+    zs = np.arange(depth - 1)
+    A.append(part(0, 0, zs))
+    Bb.append(part(0, 0, zs + 1))
+    anchor.append(np.stack([np.zeros(depth - 1), np.zeros(depth - 1), zs + 0.5], 1))
+    axis.append(np.tile([0.0, 0.0, 1.0], (depth - 1, 1)))
+    return compile_mechanism(scene, np.concatenate(A), np.concatenate(Bb), np.concatenate(anchor),
+                             np.concatenate(axis))
+
+
 # ------------------------------------------------------------ batched scenes
 def translated(scene: Scene, offset) -> Scene:
     """The scene moved by `offset` (x, y, z)."""

@@ -33,3 +33,19 @@ def cuda_lib():
     if rc != 0 or count.value == 0:
         pytest.fail("gpu test selected but no CUDA device is visible")
     return lib
+
+
+# One-line reports (FP64 error tables) that GPU tests add with report(); printed
+# after the run, so they show in quiet mode too.
+_REPORTS: list[str] = []
+
+
+def report(line: str) -> None:
+    _REPORTS.append(line)
+
+
+def pytest_terminal_summary(terminalreporter, exitstatus, config):
+    if _REPORTS:
+        terminalreporter.section("error against the FP64 oracle (one step from an identical state)")
+        for line in _REPORTS:
+            terminalreporter.write_line(line)
