@@ -83,6 +83,8 @@ def parse():
     ap.add_argument("--no-forms", action="store_true", help="skip the residual-form and batched measurements")
     ap.add_argument("--no-autotune", action="store_true", help="keep the default launch shapes")
     ap.add_argument("--flush-l2", action="store_true", help="zero a 256 MB buffer between timed ticks")
+    ap.add_argument("--cpu-table", action="store_true",
+                    help="time the CPU restatement on every configuration (all cores and one core) and exit")
     return ap.parse_args()
 
 
@@ -205,6 +207,49 @@ def cpu_trajectory(scene, ticks: int, budget_s: float, threads: int):
     return done, time.perf_counter() - t0, oracle.threads()
 
 
+def cpu_table(budget_s: float = 20.0) -> dict:
+    """The CPU restatement timed on the host's cores and on one core for every
+    configuration (a bounded sample of each: the ticks that fit `budget_s`, at
+    least one), for the CPU baseline table.  Prints nothing; returns the rows."""
+    import oracle
+    from mechanic_b200 import learned, scenes
+    from mechanic_b200.physics import GpuPhysicsConfig
+    oracle.build()
+    cores = os.cpu_count() or 1
+    # (name, scenes, config, ticks, thread counts).  The overlapping first tick of configs 2
+    # and 4 (14M and 44M candidate pairs) takes minutes on one core, so those are timed on
+    # all cores only; config 5's first tick (145M pairs) needs more host memory than a
+    # sample is worth and is not timed.
+    configs = [
+        ("1: 1,000 cubes", lambda: [scenes.falling_cubes(1000, seed=0)], GpuPhysicsConfig(), 60, (cores, 1)),
+        ("2: 100,000 mixed bodies", lambda: [scenes.stack_grid(50, 40, 50, seed=0)], GpuPhysicsConfig(), 120,
+         (cores,)),
+        ("3: 4,000 chains, closure PCG to 1e-5", lambda: [scenes.bearing_chains(4000)],
+         learned.closure_config(), 60, (cores, 1)),
+        ("4: 256 batched scenes", lambda: scenes.batched_uneven(256, seed=0), GpuPhysicsConfig(), 60, (cores,)),
+    ]
+    rows = []
+    for name, make, cfg, ticks, thread_counts in configs:
+        lst = make()
+        for threads in thread_counts:
+            oracle.set_threads(threads)
+            w = (oracle.OracleWorld.batch(lst, cfg.to_c(), pair_capacity=1 << 28) if len(lst) > 1 else
+                 oracle.OracleWorld(lst[0], cfg.to_c(), pair_capacity=1 << 28))
+            bodies = sum(x.body_count for x in lst)
+            t0 = time.perf_counter()
+            done = 0
+            for tick in range(1, ticks + 1):
+                w.step(tick)
+                done += 1
+                if time.perf_counter() - t0 > budget_s:
+                    break
+            el = time.perf_counter() - t0
+            rows.append({"config": name, "threads": oracle.threads(), "ticks": f"1..{done} of {ticks}",
+                         "seconds": round(el, 2), "body_steps_per_s": bodies * done / el})
+            del w
+    return {"cpu_table": rows, "host_cores": cores}
+
+
 def run_reference(args, scene):
     """The CPU restatement on all host cores (reference arm)."""
     threads = os.cpu_count() or 1
@@ -266,6 +311,43 @@ def measure_residual_forms(local: int, ticks: int = 60):
     return out
 
 
+def measure_closure_forms(local: int, ticks: int = 20, chains: int = 4000):
+    """The articulated config (4,000 five-body chains, 10% loop-closed): closure PCG to a
+    1e-5 relative residual under each preconditioner -- the reference's diagonal (Jacobi)
+    one, exact 2 x 2 blocks, the network-corrected 2 x 2 blocks (trained here on the GPU on
+    the first ticks' systems) and per-loop block Jacobi.  PCG iterations per tick (12 Newton
+    steps, at most 256 iterations each), the largest relative residual reached, and the
+    device time per tick."""
+    from mechanic_b200 import abi, learned, scenes
+    from mechanic_b200.physics import GpuPhysics
+    scene = scenes.bearing_chains(chains)
+    xs, ts, _ = learned.collect_closure_samples(scene, 8, learned.closure_config(
+        preconditioner=abi.PRECOND_PAIR_BLOCKS, device=local))
+    params, _ = learned.train_preconditioner(xs, ts, steps=2000)
+    out = {"workload": f"{chains} five-body chains, 10% loop-closed, closure PCG until ||r|| <= 1e-5 ||r0|| "
+                       f"(cap 256 per Newton step), ticks 1..{ticks}",
+           "training": f"network trained on {len(xs)} 2 x 2 blocks of ticks 1-8 (pair-block runs)"}
+    for name, pc in (("diagonal (reference Jacobi)", abi.PRECOND_DIAGONAL), ("pair blocks", abi.PRECOND_PAIR_BLOCKS),
+                     ("learned pair blocks", abi.PRECOND_LEARNED), ("block Jacobi (per loop)", abi.PRECOND_BLOCK_JACOBI)):
+        with GpuPhysics(scene, learned.closure_config(preconditioner=pc, device=local)) as g:
+            if pc == abi.PRECOND_LEARNED:
+                g.set_preconditioner_network(params)
+            its, res, ms = [], [], 0.0
+            for t in range(1, ticks + 1):
+                g.dispatch_tick(t)
+                rb = g.read_last_tick()
+                its.append(rb.closure_iterations)
+                res.append(rb.closure_relative_residual)
+                ms += rb.gpu_tick_ms
+        out[name] = {"pcg_iterations_per_tick": float(np.mean(its)), "max_relative_residual": float(np.max(res)),
+                     "ticks_at_tolerance": int(sum(r <= 1e-5 for r in res)), "ms_per_tick": ms / ticks}
+    d, b = out["diagonal (reference Jacobi)"], out["block Jacobi (per loop)"]
+    out["iteration_ratio_diagonal_over_block"] = d["pcg_iterations_per_tick"] / max(b["pcg_iterations_per_tick"], 1e-9)
+    out["iteration_ratio_pair_over_learned"] = (out["pair blocks"]["pcg_iterations_per_tick"] /
+                                                max(out["learned pair blocks"]["pcg_iterations_per_tick"], 1e-9))
+    return out
+
+
 def measure_batched(args, rank: int, world: int, local: int):
     """The 256-scene batched config (sharded by scene across ranks)."""
     import torch
@@ -314,6 +396,10 @@ def main():
     args = parse()
     rank, world, local = dist_env()
     from mechanic_b200 import scenes
+    if args.cpu_table:
+        if rank == 0:
+            print(json.dumps(cpu_table()), flush=True)
+        return
     scene = scenes.stack_grid(50, 40, 50, seed=args.seed)
 
     if args.impl == "reference":
@@ -427,6 +513,7 @@ def main():
         forms = {"batched": measure_batched(args, rank, world, local)}
         if rank == 0 and world == 1:
             forms["residual_1e-5"] = measure_residual_forms(local)
+            forms["closure_1e-5"] = measure_closure_forms(local)
     solve_ms = stage_ms["contact_solver"]
     broad_ms = stage_ms["broadphase"]
     peaks = {}

@@ -263,7 +263,7 @@ typedef struct MkConfig {
     uint32_t contact_max_iterations;     /* cap on passes when contact_tolerance > 0; 0 => 512 */
     float closure_tolerance;             /* MK_CLOSURE_PCG_RESIDUAL: relative PCG residual; 0 => 1e-5 */
     uint32_t closure_max_iterations;     /* MK_CLOSURE_PCG_RESIDUAL: PCG iterations per Newton step; 0 => 256 */
-    uint32_t preconditioner;             /* MK_PRECOND_BLOCK_JACOBI (default) or MK_PRECOND_LEARNED */
+    uint32_t preconditioner;             /* MK_PRECOND_BLOCK_JACOBI (default), _LEARNED, _PAIR_BLOCKS, _DIAGONAL */
     uint32_t contact_manifold;           /* MK_MANIFOLD_POINT (default) or MK_MANIFOLD_CLIPPED */
 } MkConfig;
 
@@ -276,6 +276,7 @@ typedef struct MkConfig {
 #define MK_PRECOND_BLOCK_JACOBI 0u  /* per-closure-loop blocks: Cholesky of J^T J on each loop's coordinates */
 #define MK_PRECOND_LEARNED      1u  /* 2 x 2 blocks of consecutive closure coordinates, inverse from the network */
 #define MK_PRECOND_PAIR_BLOCKS  2u  /* 2 x 2 blocks, exact 2 x 2 inverse (the learned form's own baseline) */
+#define MK_PRECOND_DIAGONAL     3u  /* the reference's Jacobi preconditioner r / diag(J^T J) (closure.wgsl:343-400) */
 
 #define MK_MORTON_63            0u  /* 21 bits/axis over the tick's bounds of the collider centres (cubic cells),
                                        index tie-break through a stable sort */
@@ -358,6 +359,21 @@ typedef struct MkHostState {
     uint32_t manifold_count;             /* out (save) / in (load) */
     uint64_t manifold_tick;              /* tick that wrote the manifold rows (out / in) */
 } MkHostState;
+
+/* PublishedGpuState (runtime.rs:60-75): the newest complete pair of snapshot
+ * slots.  Each mk_dispatch_tick publishes its tick (publish_tick,
+ * runtime.rs:222-237): previous <- current, current <- (tick % 3, tick).
+ * The slots' contents are complete once the submission has finished. */
+typedef struct MkPublishedState {
+    uint64_t generation;                 /* changes with every handle (scene) created in the process */
+    uint8_t previous_slot;
+    uint8_t current_slot;
+    uint8_t pad[6];
+    uint64_t previous_tick;
+    uint64_t current_tick;
+    uint32_t body_count;
+    uint32_t ticks_published;            /* 0, 1 or 2: how many of the pair hold a tick */
+} MkPublishedState;
 
 /* Internal buffers readable for parity checks (mk_read_buffer). */
 enum {
@@ -446,6 +462,18 @@ MK_API int mk_read_snapshot(MkHandle* handle, uint8_t slot, GpuTransform* out,
 MK_API int mk_snapshot_buffers(MkHandle* handle, uint8_t slot, void** positions,
                         void** rotations, MkError* err);
 
+/* Render hand-off between the published pair (scheduler.rs:69-73 gives the
+ * fraction alpha of the way from the previous to the current tick): writes
+ * body_count float4 positions lerp(p_prev, p_cur, alpha) and float4 unit
+ * rotations slerp(q_prev, q_cur, alpha) along the shorter arc into caller
+ * device memory (16-byte aligned), on `stream`, after the ticks that wrote
+ * both slots; the next tick that rewrites either slot waits for it.  alpha
+ * outside [0, 1] returns MK_ERR_INVALID_ARGUMENT.  No graphics interop: the
+ * outputs are plain device buffers. */
+MK_API int mk_published_state(MkHandle* handle, MkPublishedState* out);
+MK_API int mk_interpolate_snapshot(MkHandle* handle, float alpha, void* positions_out, void* rotations_out,
+                                   void* stream, MkError* err);
+
 /* GpuPhysics::apply_impulse (device.rs:821-857 / physics.wgsl:73-90). */
 MK_API int mk_apply_impulse(MkHandle* handle, uint32_t body_index,
                      const float world_point[3], const float impulse[3], MkError* err);
@@ -489,6 +517,11 @@ MK_API uint32_t mk_tick_kernel_count(const MkHandle* handle);
  * previous value, or -1 for an unknown key. */
 #define MK_TUNE_SORT_ITEMS 1u
 #define MK_TUNE_CLOSURE_GRID 2u
+/* Contact solve of heavy ticks (more active contacts than twice the bodies):
+ * 0 (default) each contact writes its fixed-point deltas to its own slot and
+ * each body sums its contacts' slots through an incidence list; 1 keeps the
+ * per-contact atomic adds into the bodies' delta rows.  Same bits either way. */
+#define MK_TUNE_HEAVY_SOLVE 3u
 MK_API int mk_set_tuning(uint32_t key, uint32_t value);
 
 /* Launch shapes of one handle's tick (no reference counterpart).  0 in any

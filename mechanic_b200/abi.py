@@ -41,6 +41,7 @@ WARM_LEARNED_REJECTED = 2
 PRECOND_BLOCK_JACOBI = 0
 PRECOND_LEARNED = 1
 PRECOND_PAIR_BLOCKS = 2
+PRECOND_DIAGONAL = 3       # the reference's Jacobi preconditioner, iterated to the residual
 MANIFOLD_POINT = 0
 MANIFOLD_CLIPPED = 1
 
@@ -136,6 +137,12 @@ class MkConfig(C.Structure):
         ("closure_tolerance", C.c_float), ("closure_max_iterations", C.c_uint32),
         ("preconditioner", C.c_uint32), ("contact_manifold", C.c_uint32),
     ]
+
+
+class MkPublishedState(C.Structure):
+    _fields_ = [("generation", C.c_uint64), ("previous_slot", C.c_uint8), ("current_slot", C.c_uint8),
+                ("pad", C.c_uint8 * 6), ("previous_tick", C.c_uint64), ("current_tick", C.c_uint64),
+                ("body_count", C.c_uint32), ("ticks_published", C.c_uint32)]
 
 
 class MkWaitProbe(C.Structure):

@@ -7,6 +7,7 @@
 // contact list is the manifold cache of the next).
 #include <cmath>
 #include <cstdarg>
+#include <atomic>
 #include <cstdio>
 #include <cstring>
 #include <string>
@@ -87,6 +88,14 @@ struct MkHandle {
     cudaEvent_t slot_written[3] = {};
     cudaEvent_t slot_read[3] = {};
     bool slot_read_pending[3] = {};
+    // the same for interpolations, which run on the caller's stream
+    cudaEvent_t slot_interp[3] = {};
+    bool slot_interp_pending[3] = {};
+    // published snapshot pair (runtime.rs:60-75, publish_tick :222-237): the
+    // two most recently dispatched ticks' slots
+    uint64_t pub_generation = 0;
+    uint64_t pub_prev_tick = 0, pub_cur_tick = 0;
+    uint8_t pub_prev_slot = 0, pub_cur_slot = 0;
     // host
     mk::DevTick* h_tick = nullptr;      // tick rows as dispatched (a ring: at most kTickRing ticks in flight)
     GpuDiagnostics* h_diag = nullptr;   // pinned, written at the end of every tick
@@ -194,6 +203,11 @@ uint64_t carve(MkHandle* h, char* base) {
         b.features[k] = c.take<uint32_t>(P);
     }
     b.active = c.take<uint32_t>(P);
+    b.contact_deltas = c.take<int32_t>(12 * P);
+    b.inc_count = c.take<uint32_t>(B);
+    b.inc_off = c.take<uint32_t>(B + 1ull);
+    b.inc_list = c.take<uint32_t>(2 * P);
+    b.inc_blocks = c.take<uint32_t>(1024);
     b.lookback_words = std::max<uint64_t>(P / 256 + 2, C / 256 + 2);
     b.lookback = c.take<uint64_t>(4 * b.lookback_words);
     b.tickets = c.take<uint32_t>(16);
@@ -404,6 +418,46 @@ cudaError_t upload(T* dst, const void* src, uint64_t count, cudaStream_t s) {
     return cudaMemcpyAsync(dst, src, count * sizeof(T), cudaMemcpyHostToDevice, s);
 }
 
+// Generation of a loaded scene (runtime.rs:139, changes whenever a scene is
+// loaded): one process-wide counter for handle creation and state loads.
+uint64_t next_generation() {
+    static std::atomic<uint64_t> counter{0};
+    return counter.fetch_add(1) + 1;
+}
+
+// Render hand-off between the published pair of snapshot slots: positions
+// lerp(p0, p1, alpha); rotations the shortest-arc slerp of q0 and q1 (q1
+// negated when q0 . q1 < 0), a normalised lerp when they are within 0.0316
+// rad (dot > 0.9995), where slerp's sin(theta) loses its digits.
+__global__ void k_interpolate_snapshot(const float4* __restrict__ p0, const float4* __restrict__ q0,
+                                       const float4* __restrict__ p1, const float4* __restrict__ q1, float alpha,
+                                       float4* __restrict__ pos_out, float4* __restrict__ rot_out, uint32_t n) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float4 a = __ldg(p0 + i), b = __ldg(p1 + i);
+    pos_out[i] = make_float4(a.x + (b.x - a.x) * alpha, a.y + (b.y - a.y) * alpha, a.z + (b.z - a.z) * alpha, 0.0f);
+    const float4 r = __ldg(q0 + i);
+    float4 t = __ldg(q1 + i);
+    float d = r.x * t.x + r.y * t.y + r.z * t.z + r.w * t.w;
+    if (d < 0.0f) {
+        t = make_float4(-t.x, -t.y, -t.z, -t.w);
+        d = -d;
+    }
+    float s0, s1;
+    if (d > 0.9995f) {
+        s0 = 1.0f - alpha;
+        s1 = alpha;
+    } else {
+        const float theta = acosf(fminf(d, 1.0f));
+        const float inv = 1.0f / sinf(theta);
+        s0 = sinf((1.0f - alpha) * theta) * inv;
+        s1 = sinf(alpha * theta) * inv;
+    }
+    float4 q = make_float4(r.x * s0 + t.x * s1, r.y * s0 + t.y * s1, r.z * s0 + t.z * s1, r.w * s0 + t.w * s1);
+    const float inv_len = 1.0f / sqrtf(q.x * q.x + q.y * q.y + q.z * q.z + q.w * q.w);
+    rot_out[i] = make_float4(q.x * inv_len, q.y * inv_len, q.z * inv_len, q.w * inv_len);
+}
+
 // Interleaves float4 pos/rot rows into GpuTransform rows on the device.
 __global__ void k_interleave(const float4* a, const float4* b, float4* out, uint32_t n) {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -428,6 +482,7 @@ void destroy_handle(MkHandle* h) {
     for (uint32_t i = 0; i < 3; ++i) {
         if (h->slot_written[i]) cudaEventDestroy(h->slot_written[i]);
         if (h->slot_read[i]) cudaEventDestroy(h->slot_read[i]);
+        if (h->slot_interp[i]) cudaEventDestroy(h->slot_interp[i]);
     }
     if (h->copy_stream) cudaStreamDestroy(h->copy_stream);
     for (auto& e : h->tick_done)
@@ -722,7 +777,9 @@ int create_impl(const MkCreation* cr, const MkConfig* config, const MkCapacities
     for (uint32_t i = 0; ok && i < 3; ++i) {
         ok = check(cudaEventCreateWithFlags(&h->slot_written[i], cudaEventDisableTiming), err, "event");
         ok = ok && check(cudaEventCreateWithFlags(&h->slot_read[i], cudaEventDisableTiming), err, "event");
+        ok = ok && check(cudaEventCreateWithFlags(&h->slot_interp[i], cudaEventDisableTiming), err, "event");
     }
+    h->pub_generation = next_generation();
     if (!ok) {
         destroy_handle(h);
         return MK_ERR_DEVICE_FAILURE;
@@ -820,6 +877,11 @@ int mk_set_tuning(uint32_t key, uint32_t value) {
         mk::set_closure_grid(value);
         return (int)prev;
     }
+    if (key == MK_TUNE_HEAVY_SOLVE) {
+        const uint32_t prev = mk::heavy_solve_form();
+        mk::set_heavy_solve_form(value);
+        return (int)prev;
+    }
     return -1;
 }
 
@@ -886,6 +948,10 @@ int mk_dispatch_tick(MkHandle* h, uint64_t tick_index, MkSubmission* out) {
         e = cudaStreamWaitEvent(h->stream, h->slot_read[snap], 0);
         h->slot_read_pending[snap] = false;
     }
+    if (e == cudaSuccess && h->slot_interp_pending[snap]) {   // or an interpolation reading it
+        e = cudaStreamWaitEvent(h->stream, h->slot_interp[snap], 0);
+        h->slot_interp_pending[snap] = false;
+    }
     if (e == cudaSuccess) {
         k_set_tick<<<1, 32, 0, h->stream>>>(h->buf.tick, t);
         e = cudaGetLastError();
@@ -903,6 +969,10 @@ int mk_dispatch_tick(MkHandle* h, uint64_t tick_index, MkSubmission* out) {
     }
     h->tick_sub[slot] = sub;
     h->last_submission = sub;
+    h->pub_prev_slot = h->pub_cur_slot;
+    h->pub_prev_tick = h->pub_cur_tick;
+    h->pub_cur_slot = (uint8_t)snap;
+    h->pub_cur_tick = tick_index;
     h->parity ^= (h->collisions ? 1 : 0);
     h->any_tick = true;
     if (out) {
@@ -1083,6 +1153,52 @@ int mk_read_snapshot(MkHandle* h, uint8_t slot, GpuTransform* out, uint32_t capa
         e = cudaEventSynchronize(h->slot_read[slot]);
     }
     if (!check(e, err, "read_snapshot")) return MK_ERR_DEVICE_FAILURE;
+    return MK_OK;
+}
+
+int mk_published_state(MkHandle* h, MkPublishedState* out) {
+    if (!h || !out) return MK_ERR_INVALID_ARGUMENT;
+    std::memset(out, 0, sizeof(*out));
+    out->generation = h->pub_generation;
+    out->previous_slot = h->pub_prev_slot;
+    out->current_slot = h->pub_cur_slot;
+    out->previous_tick = h->pub_prev_tick;
+    out->current_tick = h->pub_cur_tick;
+    out->body_count = h->B;
+    out->ticks_published = h->any_tick ? (h->last_submission >= 2 ? 2u : 1u) : 0u;
+    return MK_OK;
+}
+
+int mk_interpolate_snapshot(MkHandle* h, float alpha, void* positions_out, void* rotations_out, void* stream,
+                            MkError* err) {
+    if (!h) return MK_ERR_INVALID_ARGUMENT;
+    if (!positions_out || !rotations_out || !(alpha >= 0.0f && alpha <= 1.0f)) {
+        set_error(err, MK_ERR_INVALID_ARGUMENT, "interpolate_snapshot: null output or alpha outside [0, 1]");
+        return MK_ERR_INVALID_ARGUMENT;
+    }
+    if ((((uintptr_t)positions_out) | ((uintptr_t)rotations_out)) & 15u) {
+        set_error(err, MK_ERR_INVALID_ARGUMENT, "interpolate_snapshot: outputs must be 16-byte aligned");
+        return MK_ERR_INVALID_ARGUMENT;
+    }
+    if (h->B == 0) return MK_OK;
+    DeviceGuard guard(h->device);
+    cudaStream_t s = (cudaStream_t)stream;
+    const uint8_t a = h->pub_prev_slot, b = h->pub_cur_slot;
+    // after the ticks that wrote both slots; the next tick that rewrites either waits for this
+    cudaError_t e = cudaStreamWaitEvent(s, h->slot_written[a], 0);
+    if (e == cudaSuccess && b != a) e = cudaStreamWaitEvent(s, h->slot_written[b], 0);
+    if (e == cudaSuccess) {
+        const size_t B = h->B;
+        k_interpolate_snapshot<<<(h->B + 255) / 256, 256, 0, s>>>(
+            h->buf.snap_pos + a * B, h->buf.snap_rot + a * B, h->buf.snap_pos + b * B, h->buf.snap_rot + b * B, alpha,
+            (float4*)positions_out, (float4*)rotations_out, h->B);
+        e = cudaGetLastError();
+    }
+    for (uint8_t slot : {a, b}) {
+        if (e == cudaSuccess) e = cudaEventRecord(h->slot_interp[slot], s);
+        if (e == cudaSuccess) h->slot_interp_pending[slot] = true;
+    }
+    if (!check(e, err, "interpolate_snapshot")) return MK_ERR_DEVICE_FAILURE;
     return MK_OK;
 }
 

@@ -162,6 +162,12 @@ struct StepBuffers {
     uint64_t* contact_keys[2];
     uint32_t* features[2];
     uint32_t* active;            // pair_capacity
+    // gather form of the contact solve (heavy ticks: more active contacts than 2 x bodies)
+    int32_t* contact_deltas;     // 12 per active contact: fixed-point deltas of body a, then of body b
+    uint32_t* inc_count;         // per body: contacts touching it (then a countdown while listing them)
+    uint32_t* inc_off;           // body_count + 1: each body's first entry in inc_list
+    uint32_t* inc_list;          // 2 x pair_capacity: 2 t + side of every active contact t, grouped by body
+    uint32_t* inc_blocks;        // per block of the cooperative solve: its bodies' entry total
     uint64_t* lookback;          // look-back words for ordered compaction
     uint64_t lookback_words;     // per site
     uint32_t* tickets;           // 8 tile tickets
@@ -237,6 +243,8 @@ cudaError_t launch_warm_targets(const StepBuffers& b, int parity, uint32_t A, fl
 cudaError_t launch_contact_solver(const StepBuffers& b, const StepParams& p, const StepLaunch& l, int parity,
                                   cudaStream_t s, const std::function<cudaError_t()>& before_solve = nullptr);
 cudaError_t launch_finish_tick(const StepBuffers& b, const StepParams& p, int parity, cudaStream_t s);
+void set_heavy_solve_form(uint32_t form);   // MK_TUNE_HEAVY_SOLVE: 0 gather, 1 scatter
+uint32_t heavy_solve_form();
 // Contact iterations as separate launches with a hook after each velocity
 // apply (bearing projection of mechanisms with a dynamic root).
 cudaError_t launch_contact_solver_stepwise(const StepBuffers& b, const StepParams& p, const StepLaunch& l, int parity,

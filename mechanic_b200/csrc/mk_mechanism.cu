@@ -1255,6 +1255,15 @@ template <bool kGrid>
 __device__ __forceinline__ void precond_apply(const MechBuffers& m, const MechParams& p, const float* r, float* z,
                                               uint32_t* flags) {
     const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x, nt = gridDim.x * blockDim.x;
+    if (p.precond == MK_PRECOND_DIAGONAL) {   // closure.wgsl:343-346, :396-400
+        for (uint32_t q = tid; q < p.closure_coords; q += nt) {
+            const uint32_t c = m.cq_coords[q];
+            const float d = m.diag[c];
+            z[c] = d > 1.0e-12f ? r[c] / d : 0.0f;
+        }
+        loop_sync<kGrid>(m.grid_barrier, flags);
+        return;
+    }
     if (p.precond == MK_PRECOND_BLOCK_JACOBI) {
         for (uint32_t lp = tid; lp < p.loops; lp += nt) {
             const uint32_t o = m.loop_off[lp], n = m.loop_off[lp + 1] - o;

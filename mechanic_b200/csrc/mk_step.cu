@@ -735,26 +735,33 @@ __global__ void __launch_bounds__(kTravThreads) k_traverse(StepBuffers b, StepPa
     __syncwarp();
     uint32_t* found = &b.counts->pairs_found;
     const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t < n && n > 1) {
+    uint32_t i = 0, body_i = 0, node = 0, sp = 0;
+    uint32_t stack[kStack];
+    float4 qmin = make_float4(0, 0, 0, 0), qmax = qmin;
+    bool active = t < n && n > 1;
+    if (active) {
         const uint32_t leaf_base = n - 1;
-        const uint32_t i = b.svals[t];
-        const float4 qmin = b.node_aabbs[2ull * (leaf_base + t)], qmax = b.node_aabbs[2ull * (leaf_base + t) + 1];
-        const uint32_t body_i = __float_as_uint(b.boxes[3ull * i + 2].z);
+        i = b.svals[t];
+        qmin = b.node_aabbs[2ull * (leaf_base + t)];
+        qmax = b.node_aabbs[2ull * (leaf_base + t) + 1];
+        body_i = __float_as_uint(b.boxes[3ull * i + 2].z);
         // batched scenes: the walk starts at the scene's own subtree (Karras keeps
         // each scene's leaves under one node: the scene index sits above the
         // Morton bits), so every entry it meets lies inside the scene; a scene of
         // one collider has no pairs
-        uint32_t node = 0;
-        bool none = false;
         if (kBatched) {
             const uint32_t sc = b.collider_scene[i];
             const uint32_t begin = sc ? __ldg(b.scene_end + sc - 1) : 0u, end = __ldg(b.scene_end + sc);
-            none = end - begin < 2u;
-            if (!none) node = __ldg(b.scene_root + sc);
+            active = end - begin >= 2u;
+            if (active) node = __ldg(b.scene_root + sc);
         }
-        uint32_t stack[kStack];
-        uint32_t sp = 0;
-        while (!none) {
+    }
+    // The warp steps in lockstep (one record per lane per step, at most four
+    // pairs per lane), so the warp's shared-memory stage can be flushed with
+    // one global reservation whenever fewer than 128 free entries remain: no
+    // pair ever takes a global atomic of its own, however many a warp finds.
+    while (__any_sync(0xffffffffu, active)) {
+        if (active) {
             const float4* rec = b.node_records + 8ull * node;   // 4-wide: two levels per step
             float4 r[8];
 #pragma unroll
@@ -777,13 +784,8 @@ __global__ void __launch_bounds__(kTravThreads) k_traverse(StepBuffers b, StepPa
                     if (p.suppression_count && pair_is_suppressed(b.suppressed, p.suppression_count, body_i, body_j))
                         continue;
                     const uint64_t key = ((uint64_t)min(i, j) << p.pair_shift) | max(i, j);
-                    const uint32_t k = atomicAdd(&s_count[w], 1u);
-                    if (k < kStage) {
-                        s_stage[w][k] = key;
-                    } else {
-                        const uint32_t g = atomicAdd(found, 1u);
-                        if (g < p.pair_capacity) b.pair_stage[g] = key;
-                    }
+                    const uint32_t slot = atomicAdd(&s_count[w], 1u);   // < kStage: flushed below
+                    s_stage[w][slot] = key;
                 } else if (next == kNoNode) {
                     next = code;
                 } else {
@@ -795,17 +797,31 @@ __global__ void __launch_bounds__(kTravThreads) k_traverse(StepBuffers b, StepPa
                     stack[sp++] = code;
                 }
             }
-            if (overflow) break;
-            if (next != kNoNode) {
+            if (overflow) {
+                active = false;
+            } else if (next != kNoNode) {
                 node = next;
-                continue;
+            } else if (sp == 0) {
+                active = false;
+            } else {
+                node = stack[--sp];
             }
-            if (sp == 0) break;
-            node = stack[--sp];
+        }
+        __syncwarp();
+        const uint32_t staged = s_count[w];
+        if (staged > kStage - 4u * 32u) {
+            uint32_t base = 0;
+            if (lane == 0) base = atomicAdd(found, staged);
+            base = __shfl_sync(0xffffffffu, base, 0);
+            for (uint32_t k = lane; k < staged; k += 32)
+                if (base + k < p.pair_capacity) b.pair_stage[base + k] = s_stage[w][k];
+            __syncwarp();
+            if (lane == 0) s_count[w] = 0;
+            __syncwarp();
         }
     }
     __syncwarp();
-    const uint32_t staged = min(s_count[w], kStage);
+    const uint32_t staged = s_count[w];
     uint32_t base = 0;
     if (lane == 0 && staged) base = atomicAdd(found, staged);
     base = __shfl_sync(0xffffffffu, base, 0);
@@ -1584,6 +1600,148 @@ __device__ __forceinline__ void solve_fused_resident(const StepBuffers& b, const
     if (has && !(den <= 0.0f)) row[2] = f4(arm_a, acc);
 }
 
+// ------------------------------------------- gather form of the contact solve
+// On heavy ticks (more active contacts than twice the bodies, e.g. an
+// overlapping start with dozens of contacts per body) the atomics of the
+// scatter form serialise on the bodies' 24-byte delta rows.  This form writes
+// each contact's twelve fixed-point deltas to its own slot instead, and each
+// body then sums the slots of its contacts through an incidence list built
+// once per tick (counts, a grid scan, a fill).  The integer sums wrap as the
+// atomics do and are order-free, so the velocities are bit-identical to the
+// scatter form (and to the reference's atomic Jacobi, collision.wgsl:752-1069).
+
+// Exclusive scan of inc_count[0, B) into inc_off over the grid: each
+// participating block scans a contiguous segment after adding up the totals
+// of the segments before it (published in inc_blocks).
+__device__ __forceinline__ void gather_scan(const StepBuffers& b, uint32_t B, uint32_t parts, uint32_t* barrier,
+                                            uint32_t* flags, uint32_t* s_scan) {
+    const uint32_t seg = (B + parts - 1) / parts;
+    const uint32_t lo = min(B, blockIdx.x * seg), hi = min(B, lo + seg);
+    uint32_t sum = 0;
+    for (uint32_t i = lo + threadIdx.x; i < hi; i += blockDim.x) sum += b.inc_count[i];
+    uint32_t total;
+    block_exclusive_scan(sum, s_scan, &total);
+    if (threadIdx.x == 0) b.inc_blocks[blockIdx.x] = total;
+    grid_barrier(barrier, flags, parts);
+    uint32_t base = 0;
+    for (uint32_t j = threadIdx.x; j < blockIdx.x; j += blockDim.x) base += __ldcg(b.inc_blocks + j);
+    block_exclusive_scan(base, s_scan, &base);
+    for (uint32_t c0 = lo; c0 < hi; c0 += blockDim.x) {
+        const uint32_t i = c0 + threadIdx.x;
+        const uint32_t v = i < hi ? __ldcg(b.inc_count + i) : 0u;
+        uint32_t chunk;
+        const uint32_t ex = block_exclusive_scan(v, s_scan, &chunk);
+        if (i < hi) b.inc_off[i] = base + ex;
+        base += chunk;
+    }
+    if (blockIdx.x == parts - 1 && threadIdx.x == 0) b.inc_off[B] = base;
+}
+
+// Bodies of active contact t (its row is read through the active list).
+__device__ __forceinline__ uint2 active_bodies(const StepBuffers& b, const GpuContact* cur, uint32_t t) {
+    const uint32_t k = __ldcg(b.active + t);
+    const float4 r0 = __ldcg(reinterpret_cast<const float4*>(cur + k));
+    return make_uint2(__float_as_uint(r0.x), __float_as_uint(r0.y));
+}
+
+__device__ void solve_gather(const StepBuffers& b, const StepParams& p, GpuContact* cur, uint32_t A,
+                             uint32_t iterations, uint32_t* barrier, uint32_t parts) {
+    __shared__ uint32_t s_scan[33];
+    uint32_t* flags = &b.diag->error_flags;
+    const uint32_t B = p.body_count;
+    const uint32_t gtid = blockIdx.x * blockDim.x + threadIdx.x, stride = parts * blockDim.x;
+    // ---- incidence lists: counts, offsets, fill (2 t + side, grouped by body)
+    for (uint32_t i = gtid; i < B; i += stride) b.inc_count[i] = 0u;
+    grid_barrier(barrier, flags, parts);
+    for (uint32_t t = gtid; t < A; t += stride) {
+        const uint2 ab = active_bodies(b, cur, t);
+        atomicAdd(b.inc_count + ab.x, 1u);
+        if (ab.y != kInvalid) atomicAdd(b.inc_count + ab.y, 1u);
+    }
+    grid_barrier(barrier, flags, parts);
+    gather_scan(b, B, parts, barrier, flags, s_scan);
+    grid_barrier(barrier, flags, parts);
+    for (uint32_t t = gtid; t < A; t += stride) {
+        const uint2 ab = active_bodies(b, cur, t);
+        b.inc_list[__ldcg(b.inc_off + ab.x) + atomicSub(b.inc_count + ab.x, 1u) - 1u] = 2u * t;
+        if (ab.y != kInvalid)
+            b.inc_list[__ldcg(b.inc_off + ab.y) + atomicSub(b.inc_count + ab.y, 1u) - 1u] = 2u * t + 1u;
+    }
+    grid_barrier(barrier, flags, parts);
+    const size_t Bs = B;
+    const float s = (float)kFixedScale;
+    const uint32_t lane = lane_id();
+    const uint32_t gwarp = gtid >> 5, nwarps = stride >> 5;
+    const uint2 sl = contact_slice(A, parts);
+    for (uint32_t it = 0; it < iterations; ++it) {
+        // iteration `it` reads buffer it (0 = the integrated velocities) and
+        // writes buffer it + 1 (the last one back into lin/ang)
+        const float4* vl = it == 0 ? b.lin : b.vel_iter + (2 * (it - 1)) * Bs;
+        const float4* va = it == 0 ? b.ang : b.vel_iter + (2 * (it - 1) + 1) * Bs;
+        float4* dl = it + 1 == iterations ? b.lin : b.vel_iter + (2 * it) * Bs;
+        float4* da_out = it + 1 == iterations ? b.ang : b.vel_iter + (2 * it + 1) * Bs;
+        // ---- each contact's projection into its own delta slot
+        for (uint32_t t = sl.x + threadIdx.x; t < sl.y; t += blockDim.x) {
+            const uint32_t k = __ldcg(b.active + t);
+            float4* row = reinterpret_cast<float4*>(cur + k);
+            const float4 r0 = __ldcg(row), np = __ldcg(row + 1), aa = __ldcg(row + 2), ab = __ldcg(row + 3);
+            const uint32_t a = __float_as_uint(r0.x), bb = __float_as_uint(r0.y);
+            const f3 arm_a = xyz(aa), arm_b = xyz(ab);
+            const float4* wa = b.world_mass + 3ull * a;
+            const float4* wb = bb != kInvalid ? b.world_mass + 3ull * bb : nullptr;
+            int32_t da[6] = {0, 0, 0, 0, 0, 0}, db[6] = {0, 0, 0, 0, 0, 0};
+            const f3 vb = bb != kInvalid ? contact_velocity_it(vl, va, bb, arm_b) : mkf3(0, 0, 0);
+            const f3 nrm = xyz(np);
+            const float den = impulse_denominator(wa, wb, arm_a, arm_b, nrm);
+            if (!(den <= 0.0f)) {
+                const f3 rel = vb - contact_velocity_it(vl, va, a, arm_a);
+                float acc = aa.w;
+                const bool live = it == 0
+                    ? contact_project<true>(p, wa, wb, arm_a, arm_b, nrm, np.w, ab.w < 0.0f, den, rel, acc, da, db)
+                    : contact_project<false>(p, wa, wb, arm_a, arm_b, nrm, np.w, ab.w < 0.0f, den, rel, acc, da, db);
+                if (!live) {
+#pragma unroll
+                    for (int c = 0; c < 6; ++c) da[c] = db[c] = 0;
+                }
+                row[2] = f4(arm_a, acc);
+            }
+            int4* d = reinterpret_cast<int4*>(b.contact_deltas + 12ull * t);
+            d[0] = make_int4(da[0], da[1], da[2], da[3]);
+            d[1] = make_int4(da[4], da[5], db[0], db[1]);
+            d[2] = make_int4(db[2], db[3], db[4], db[5]);
+        }
+        grid_barrier(barrier, flags, parts);
+        // ---- each body (one warp) sums its contacts' slots: v += delta / 2^20
+        for (uint32_t x = gwarp; x < B; x += nwarps) {
+            const uint32_t e0 = __ldcg(b.inc_off + x), e1 = __ldcg(b.inc_off + x + 1);
+            int32_t sum[6] = {0, 0, 0, 0, 0, 0};
+            for (uint32_t e = e0 + lane; e < e1; e += 32) {
+                const uint32_t ent = __ldcg(b.inc_list + e);
+                const int2* q = reinterpret_cast<const int2*>(b.contact_deltas + 12ull * (ent >> 1) + 6u * (ent & 1u));
+                const int2 x0 = __ldcg(q), x1 = __ldcg(q + 1), x2 = __ldcg(q + 2);
+                sum[0] = (int32_t)((uint32_t)sum[0] + (uint32_t)x0.x);
+                sum[1] = (int32_t)((uint32_t)sum[1] + (uint32_t)x0.y);
+                sum[2] = (int32_t)((uint32_t)sum[2] + (uint32_t)x1.x);
+                sum[3] = (int32_t)((uint32_t)sum[3] + (uint32_t)x1.y);
+                sum[4] = (int32_t)((uint32_t)sum[4] + (uint32_t)x2.x);
+                sum[5] = (int32_t)((uint32_t)sum[5] + (uint32_t)x2.y);
+            }
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1)
+#pragma unroll
+                for (int c = 0; c < 6; ++c)
+                    sum[c] = (int32_t)((uint32_t)sum[c] + (uint32_t)__shfl_down_sync(0xffffffffu, sum[c], o));
+            if (lane == 0) {
+                const f3 ld = mkf3((float)sum[0], (float)sum[1], (float)sum[2]) / s;
+                const f3 ad = mkf3((float)sum[3], (float)sum[4], (float)sum[5]) / s;
+                dl[x] = f4(xyz(__ldg(vl + x)) + ld, 0.0f);
+                da_out[x] = f4(xyz(__ldg(va + x)) + ad, 0.0f);
+            }
+        }
+        grid_barrier(barrier, flags, parts);
+    }
+}
+
 // All solver iterations in one cooperative launch: warm start, then
 // (iterations - 1) projections, each followed by the velocity apply
 // (device.rs:1343-1416 dispatch order), separated by grid barriers.
@@ -1657,6 +1815,10 @@ __global__ void __launch_bounds__(kSolveThreads) k_solve_all(StepBuffers b, Step
             b.lin[i] = f4(xyz(sl) + ld, 0.0f);
             b.ang[i] = f4(xyz(sa) + ad, 0.0f);
         }
+        return;
+    }
+    if (b.contact_deltas) {   // heavy tick: no per-contact atomics
+        solve_gather(b, p, cur, A, iterations, barrier, parts);
         return;
     }
     for (uint32_t it = 0; it < iterations; ++it) {
@@ -2252,6 +2414,12 @@ cudaError_t launch_narrowphase(const StepBuffers& b, const StepParams& p, const 
     return cudaGetLastError();
 }
 
+// Heavy ticks: the gather form (0, default) or the scatter form with per-contact
+// atomics (1); both give the same bits.  Read when a tick is captured.
+static uint32_t g_heavy_solve_scatter = 0;
+void set_heavy_solve_form(uint32_t form) { g_heavy_solve_scatter = form == 1u ? 1u : 0u; }
+uint32_t heavy_solve_form() { return g_heavy_solve_scatter; }
+
 cudaError_t launch_contact_solver(const StepBuffers& b, const StepParams& p, const StepLaunch& l, int parity,
                                   cudaStream_t s, const std::function<cudaError_t()>& before_solve) {
     const uint32_t grid = (uint32_t)l.sm_count * (l.append_ctas ? l.append_ctas : 8u);
@@ -2273,6 +2441,7 @@ cudaError_t launch_contact_solver(const StepBuffers& b, const StepParams& p, con
     GpuContact* cur = b.contacts[parity];
     uint32_t* barrier = b.grid_barrier;
     StepBuffers bb = b;
+    if (g_heavy_solve_scatter) bb.contact_deltas = nullptr;   // heavy ticks keep the per-contact atomics
     StepParams pp = p;
     uint32_t learned = l.learned_warm ? 1u : 0u;
     const bool residual = p.contact_tol > 0.0f;

@@ -28,7 +28,8 @@ EXPORTS = [
     "mk_mlp_param_count", "mk_op_mlp_scratch_bytes", "mk_op_mlp_forward", "mk_op_mlp_gradient",
     "mk_op_mlp_train", "mk_set_warm_start_network", "mk_read_warm_start_samples",
     "mk_set_preconditioner_network", "mk_create_batch", "mk_scene_offsets", "mk_get_handle_tuning",
-    "mk_set_handle_tuning", "mk_autotune", "mk_selftest_bounded_wait",
+    "mk_set_handle_tuning", "mk_autotune", "mk_selftest_bounded_wait", "mk_published_state",
+    "mk_interpolate_snapshot",
 ]
 
 _lib = None
@@ -84,6 +85,8 @@ def library(path: str | None = None):
         "mk_set_handle_tuning": (i32, [vp, vp, vp]),
         "mk_autotune": (i32, [vp, u32, vp, vp, vp]),
         "mk_selftest_bounded_wait": (i32, [u32, u32, vp, vp]),
+        "mk_published_state": (i32, [vp, vp]),
+        "mk_interpolate_snapshot": (i32, [vp, C.c_float, vp, vp, vp, vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -349,6 +352,19 @@ class GpuPhysics:
         _raise(library().mk_snapshot_buffers(self._h, slot, C.byref(p), C.byref(r), C.byref(err)), err)
         return int(p.value), int(r.value)
 
+    def published_state(self) -> abi.MkPublishedState:
+        """PublishedGpuState (runtime.rs:60-75): the newest complete pair of snapshot slots."""
+        out = abi.MkPublishedState()
+        _raise(library().mk_published_state(self._h, C.byref(out)))
+        return out
+
+    def interpolate_snapshot(self, alpha: float, positions_out: int, rotations_out: int, stream: int = 0) -> None:
+        """Render hand-off: positions and rotations a fraction `alpha` of the way from the
+        published previous slot to the current one, into device buffers (float4 per body)."""
+        err = abi.MkError()
+        _raise(library().mk_interpolate_snapshot(self._h, float(alpha), positions_out, rotations_out,
+                                                  stream or None, C.byref(err)), err)
+
     def apply_impulse(self, body_index: int, world_point, impulse) -> None:
         p = (C.c_float * 3)(*[float(x) for x in world_point])
         j = (C.c_float * 3)(*[float(x) for x in impulse])
@@ -513,6 +529,7 @@ class GpuPhysics:
 
 TUNE_SORT_ITEMS = 1
 TUNE_CLOSURE_GRID = 2   # reference-mode closure loop: 0 by size, 1 one block, 2 the whole grid
+TUNE_HEAVY_SOLVE = 3    # heavy-tick contact solve: 0 gather (per-contact delta slots), 1 scatter (atomics)
 
 
 def set_tuning(key: int, value: int) -> int:

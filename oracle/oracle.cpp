@@ -1790,6 +1790,13 @@ template <class T> struct World : WorldBase {
         }
         std::vector<T> sol(Q, T(0)), res(Q, T(0)), pre(Q, T(0)), dir(Q, T(0)), op(Q, T(0));
         auto precond = [&]() {
+            if (this->precond == MK_PRECOND_DIAGONAL) {   // closure.wgsl:343-346, :396-400
+                for (uint32_t q = 0; q < NQ; ++q) {
+                    const uint32_t c = ct.cq_coords[q];
+                    pre[c] = dgl[c] > T(1.0e-12f) ? res[c] / dgl[c] : T(0);
+                }
+                return;
+            }
             if (this->precond == MK_PRECOND_BLOCK_JACOBI) {
                 const uint32_t NL = (uint32_t)loop_off.size() - 1;
                 for (uint32_t lp = 0; lp < NL; ++lp) {

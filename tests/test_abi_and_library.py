@@ -46,7 +46,7 @@ def test_passive_drive_never_clamps():
 def test_header_struct_sizes_with_gcc(tmp_path):
     names = list(abi.ROW_SIZES) + ["MkCreation", "MkConfig", "MkCapacities", "MkError", "MkSubmission",
                                    "MkKernelTimings", "MkTickReadback", "MkDeviceState", "MkHostState",
-                                   "MkTuning", "MkWaitProbe"]
+                                   "MkTuning", "MkWaitProbe", "MkPublishedState"]
     src = tmp_path / "sizes.c"
     body = "\n".join(f'    printf("{n} %zu\\n", sizeof({n}));' for n in names)
     src.write_text(f'#include <stdio.h>\n#include "{HEADER}"\nint main(void) {{\n{body}\n    return 0;\n}}\n')
@@ -57,7 +57,7 @@ def test_header_struct_sizes_with_gcc(tmp_path):
     for name, (dtype, size) in abi.ROW_SIZES.items():
         assert int(sizes[name]) == size, name
     for name in ("MkCreation", "MkConfig", "MkCapacities", "MkError", "MkSubmission", "MkKernelTimings",
-                 "MkTickReadback", "MkDeviceState", "MkHostState", "MkTuning", "MkWaitProbe"):
+                 "MkTickReadback", "MkDeviceState", "MkHostState", "MkTuning", "MkWaitProbe", "MkPublishedState"):
         assert int(sizes[name]) == ctypes.sizeof(getattr(abi, name)), name
 
 

@@ -94,4 +94,10 @@ def test_trained_warm_start_saves_passes(cuda_lib):
     params, losses = learned.train(np.concatenate(xs), np.concatenate(ys), steps=2000, batch=8192, lr=2e-3)
     assert losses[-50:].mean() < 0.5 * losses[:50].mean()
     plain, learn = _replay_passes(scenes.falling_cubes(1000, seed=7), params, 60)
-    assert learn.sum() < plain.sum(), (plain.sum(), learn.sum())
+    ratio = plain.sum() / learn.sum()
+    from conftest import report
+    report(f"learned warm start, 1,000 cubes seed 7, 60 ticks: {plain.mean():.1f} -> {learn.mean():.1f} passes "
+           f"per tick to 1e-5 (plain / learned = {ratio:.3f})")
+    # measured 1.07 on seed 0: a per-contact start cannot do much better, since relaxed
+    # Jacobi (omega 0.125) removes about 12.5% of the remaining error per pass
+    assert ratio >= 1.02, (plain.sum(), learn.sum())
