@@ -83,6 +83,8 @@ def parse():
     ap.add_argument("--no-forms", action="store_true", help="skip the residual-form and batched measurements")
     ap.add_argument("--no-autotune", action="store_true", help="keep the default launch shapes")
     ap.add_argument("--flush-l2", action="store_true", help="zero a 256 MB buffer between timed ticks")
+    ap.add_argument("--full-form", action="store_true",
+                    help="measure the 1,250,000-body full form (reference passes, plain and learned to 1e-5) and exit")
     ap.add_argument("--cpu-table", action="store_true",
                     help="time the CPU restatement on every configuration (all cores and one core) and exit")
     return ap.parse_args()
@@ -348,6 +350,55 @@ def measure_closure_forms(local: int, ticks: int = 20, chains: int = 4000):
     return out
 
 
+def measure_full_forms(local: int, ticks: int = 6) -> dict:
+    """The full form at scale (1,250,000 bodies: the 100,000-body mix on a 100^3 lattice and
+    50,000 five-body chains, 10% loop-closed), ticks 1..`ticks` from the generated state in
+    three forms: the reference's fixed passes (8 contact passes, 12 x 8 closure rounds); the
+    plain form iterated to 1e-5 (cached warm start, per-loop block-Jacobi closure PCG); the
+    learned form (network warm start, network-corrected closure blocks) to the same residual."""
+    import torch
+    from mechanic_b200 import abi, learned, scenes
+    from mechanic_b200.physics import GpuPhysics, GpuPhysicsConfig
+    scene = scenes.config_full()
+    warm = np.load(os.path.join(ROOT, "mechanic_b200", "data", "warm_start.npy"))
+    xs, ts, _ = learned.collect_closure_samples(scenes.bearing_chains(4000), 8, learned.closure_config(
+        preconditioner=abi.PRECOND_PAIR_BLOCKS, device=local))
+    precond, _ = learned.train_preconditioner(xs, ts, steps=2000)
+    caps = {"pair_capacity": 1 << 28}
+    forms = {
+        "reference passes": GpuPhysicsConfig(device=local),
+        "plain to 1e-5": GpuPhysicsConfig(device=local, contact_tolerance=1e-5, contact_max_iterations=512,
+                                          closure_mode=abi.CLOSURE_PCG_RESIDUAL, closure_tolerance=1e-5),
+        "learned to 1e-5": GpuPhysicsConfig(device=local, contact_tolerance=1e-5, contact_max_iterations=512,
+                                            warm_start=abi.WARM_LEARNED, closure_mode=abi.CLOSURE_PCG_RESIDUAL,
+                                            closure_tolerance=1e-5, preconditioner=abi.PRECOND_LEARNED),
+    }
+    out = {"workload": f"1,250,000 bodies (100^3 lattice of the 100,000-body mix + 50,000 five-body chains, 10% "
+                       f"loop-closed), ticks 1..{ticks}", "bodies": scene.body_count,
+           "colliders": scene.collider_count}
+    for name, cfg in forms.items():
+        with GpuPhysics(scene, cfg, capacities=caps) as g:
+            if cfg.warm_start == abi.WARM_LEARNED:
+                g.set_warm_start_network(warm)
+            if cfg.preconditioner == abi.PRECOND_LEARNED:
+                g.set_preconditioner_network(precond)
+            rows = []
+            for t in range(1, ticks + 1):
+                g.dispatch_tick(t)
+                rb = g.read_last_tick()
+                rows.append({"tick": t, "ms": round(rb.gpu_tick_ms, 3), "contacts": rb.contact_count,
+                             "active": rb.active_contact_count, "contact_passes": rb.contact_iterations,
+                             "contact_rel_residual": rb.contact_relative_residual,
+                             "closure_pcg_iterations": rb.closure_iterations,
+                             "closure_rel_residual": rb.closure_relative_residual, "flags": rb.error_flags,
+                             "warm_start_used": rb.warm_start_used})
+            ms = sum(r["ms"] for r in rows)
+            out[name] = {"ticks": rows, "ms_per_tick": ms / ticks,
+                         "body_steps_per_s": scene.body_count * ticks / (ms / 1e3)}
+        torch.cuda.synchronize()
+    return out
+
+
 def measure_batched(args, rank: int, world: int, local: int):
     """The 256-scene batched config (sharded by scene across ranks)."""
     import torch
@@ -399,6 +450,12 @@ def main():
     if args.cpu_table:
         if rank == 0:
             print(json.dumps(cpu_table()), flush=True)
+        return
+    if args.full_form:
+        if rank == 0:
+            import torch
+            torch.cuda.set_device(local)
+            print(json.dumps(measure_full_forms(local)), flush=True)
         return
     scene = scenes.stack_grid(50, 40, 50, seed=args.seed)
 
