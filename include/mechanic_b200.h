@@ -518,9 +518,12 @@ MK_API uint32_t mk_tick_kernel_count(const MkHandle* handle);
 #define MK_TUNE_SORT_ITEMS 1u
 #define MK_TUNE_CLOSURE_GRID 2u
 /* Contact solve of heavy ticks (more active contacts than twice the bodies):
- * 0 (default) each contact writes its fixed-point deltas to its own slot and
- * each body sums its contacts' slots through an incidence list; 1 keeps the
- * per-contact atomic adds into the bodies' delta rows.  Same bits either way. */
+ * 0 = the default (the fastest measured form); 1 = scatter: per-contact
+ * atomic adds into the bodies' delta rows; 2 = gather: each contact writes
+ * its fixed-point deltas to its own slot and each body sums its contacts'
+ * slots through an incidence list; 3 = split: body a (contacts arrive grouped
+ * by it) by warp-summed atomics, body b through slots and incidence lists.
+ * Same bits in every form. */
 #define MK_TUNE_HEAVY_SOLVE 3u
 MK_API int mk_set_tuning(uint32_t key, uint32_t value);
 

@@ -208,6 +208,7 @@ uint64_t carve(MkHandle* h, char* base) {
     b.inc_off = c.take<uint32_t>(B + 1ull);
     b.inc_list = c.take<uint32_t>(2 * P);
     b.inc_blocks = c.take<uint32_t>(1024);
+    b.lam_heavy = c.take<float>(P);
     b.lookback_words = std::max<uint64_t>(P / 256 + 2, C / 256 + 2);
     b.lookback = c.take<uint64_t>(4 * b.lookback_words);
     b.tickets = c.take<uint32_t>(16);

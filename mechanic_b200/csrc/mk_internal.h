@@ -168,6 +168,8 @@ struct StepBuffers {
     uint32_t* inc_off;           // body_count + 1: each body's first entry in inc_list
     uint32_t* inc_list;          // 2 x pair_capacity: 2 t + side of every active contact t, grouped by body
     uint32_t* inc_blocks;        // per block of the cooperative solve: its bodies' entry total
+    float* lam_heavy;            // split form: running normal impulse per active contact
+    uint32_t heavy_form;         // heavy ticks: MK_HEAVY_SCATTER, MK_HEAVY_GATHER or MK_HEAVY_SPLIT
     uint64_t* lookback;          // look-back words for ordered compaction
     uint64_t lookback_words;     // per site
     uint32_t* tickets;           // 8 tile tickets
@@ -243,7 +245,9 @@ cudaError_t launch_warm_targets(const StepBuffers& b, int parity, uint32_t A, fl
 cudaError_t launch_contact_solver(const StepBuffers& b, const StepParams& p, const StepLaunch& l, int parity,
                                   cudaStream_t s, const std::function<cudaError_t()>& before_solve = nullptr);
 cudaError_t launch_finish_tick(const StepBuffers& b, const StepParams& p, int parity, cudaStream_t s);
-void set_heavy_solve_form(uint32_t form);   // MK_TUNE_HEAVY_SOLVE: 0 gather, 1 scatter
+// Contact solve forms of heavy ticks (MK_TUNE_HEAVY_SOLVE).
+constexpr uint32_t MK_HEAVY_SCATTER = 1, MK_HEAVY_GATHER = 2, MK_HEAVY_SPLIT = 3;
+void set_heavy_solve_form(uint32_t form);   // 0 = the default form
 uint32_t heavy_solve_form();
 // Contact iterations as separate launches with a hook after each velocity
 // apply (bearing projection of mechanisms with a dynamic root).

@@ -1742,6 +1742,132 @@ __device__ void solve_gather(const StepBuffers& b, const StepParams& p, GpuConta
     }
 }
 
+// Split form: contacts arrive grouped by body a (sorted by collider a), so
+// body a's deltas take warp-aggregated atomics over runs (one per run and
+// component, as in the scatter form), while body b's -- one atomic per
+// contact and component in the scatter form, spread over many bodies and
+// serialised per body -- go to the contact's own 24-byte slot and each body
+// sums its slots through an incidence list in the apply.  The running normal
+// impulses live in a dense array during the solve (the rows are read-only
+// until the last pass writes them back).  Same integer sums, same bits.
+__device__ void solve_split(const StepBuffers& b, const StepParams& p, GpuContact* cur, uint32_t A,
+                            uint32_t iterations, uint32_t* barrier, uint32_t parts) {
+    __shared__ uint32_t s_scan[33];
+    uint32_t* flags = &b.diag->error_flags;
+    const uint32_t B = p.body_count;
+    const uint32_t gtid = blockIdx.x * blockDim.x + threadIdx.x, stride = parts * blockDim.x;
+    // ---- incidence lists of body b: counts, offsets, fill (active positions t)
+    for (uint32_t i = gtid; i < B; i += stride) b.inc_count[i] = 0u;
+    grid_barrier(barrier, flags, parts);
+    for (uint32_t t = gtid; t < A; t += stride) {
+        const uint2 ab = active_bodies(b, cur, t);
+        if (ab.y != kInvalid) atomicAdd(b.inc_count + ab.y, 1u);
+    }
+    grid_barrier(barrier, flags, parts);
+    gather_scan(b, B, parts, barrier, flags, s_scan);
+    grid_barrier(barrier, flags, parts);
+    for (uint32_t t = gtid; t < A; t += stride) {
+        const uint2 ab = active_bodies(b, cur, t);
+        if (ab.y != kInvalid)
+            b.inc_list[__ldcg(b.inc_off + ab.y) + atomicSub(b.inc_count + ab.y, 1u) - 1u] = t;
+    }
+    grid_barrier(barrier, flags, parts);
+    const size_t Bs = B;
+    const float s = (float)kFixedScale;
+    const uint32_t lane = lane_id();
+    const uint32_t gwarp = gtid >> 5, nwarps = stride >> 5;
+    const uint2 sl = contact_slice(A, parts);
+    int2* slots = reinterpret_cast<int2*>(b.contact_deltas);   // 3 x int2 per active contact
+    for (uint32_t it = 0; it < iterations; ++it) {
+        const float4* vl = it == 0 ? b.lin : b.vel_iter + (2 * (it - 1)) * Bs;
+        const float4* va = it == 0 ? b.ang : b.vel_iter + (2 * (it - 1) + 1) * Bs;
+        float4* dl = it + 1 == iterations ? b.lin : b.vel_iter + (2 * it) * Bs;
+        float4* da_out = it + 1 == iterations ? b.ang : b.vel_iter + (2 * it + 1) * Bs;
+        // ---- projections: body a by run sums and atomics, body b into the slot
+        for (uint32_t base = sl.x; base < sl.y; base += blockDim.x) {
+            const uint32_t t = base + threadIdx.x;
+            bool live = false;
+            uint32_t a = kInvalid;
+            int32_t da[6] = {0, 0, 0, 0, 0, 0}, db[6] = {0, 0, 0, 0, 0, 0};
+            if (t < sl.y) {
+                const uint32_t k = __ldcg(b.active + t);
+                const float4* row = reinterpret_cast<const float4*>(cur + k);
+                const float4 r0 = __ldg(row), np = __ldg(row + 1), aa = __ldg(row + 2), ab = __ldg(row + 3);
+                a = __float_as_uint(r0.x);
+                const uint32_t bb = __float_as_uint(r0.y);
+                const f3 arm_a = xyz(aa), arm_b = xyz(ab);
+                const float4* wa = b.world_mass + 3ull * a;
+                const float4* wb = bb != kInvalid ? b.world_mass + 3ull * bb : nullptr;
+                const f3 vb = bb != kInvalid ? contact_velocity_it(vl, va, bb, arm_b) : mkf3(0, 0, 0);
+                const f3 nrm = xyz(np);
+                const float den = impulse_denominator(wa, wb, arm_a, arm_b, nrm);
+                float acc = it == 0 ? aa.w : __ldcg(b.lam_heavy + t);
+                if (!(den <= 0.0f)) {
+                    const f3 rel = vb - contact_velocity_it(vl, va, a, arm_a);
+                    live = it == 0
+                        ? contact_project<true>(p, wa, wb, arm_a, arm_b, nrm, np.w, ab.w < 0.0f, den, rel, acc, da, db)
+                        : contact_project<false>(p, wa, wb, arm_a, arm_b, nrm, np.w, ab.w < 0.0f, den, rel, acc, da, db);
+                    if (!live) {
+#pragma unroll
+                        for (int c = 0; c < 6; ++c) da[c] = db[c] = 0;
+                    }
+                }
+                b.lam_heavy[t] = acc;
+                if (bb != kInvalid) {
+                    int2* q = slots + 3ull * t;
+                    q[0] = make_int2(db[0], db[1]);
+                    q[1] = make_int2(db[2], db[3]);
+                    q[2] = make_int2(db[4], db[5]);
+                }
+                if (it + 1 == iterations && !(den <= 0.0f))
+                    reinterpret_cast<float*>(cur + k)[11] = acc;   // the row's impulse (arm_a_impulse.w)
+            }
+            add_contact_deltas(b.deltas, live, a, kInvalid, da, db);
+        }
+        grid_barrier(barrier, flags, parts);
+        // ---- apply: body a's atomic sums plus the slots of the contacts where it is b
+        for (uint32_t x = gwarp; x < B; x += nwarps) {
+            const uint32_t e0 = __ldcg(b.inc_off + x), e1 = __ldcg(b.inc_off + x + 1);
+            int32_t sum[6] = {0, 0, 0, 0, 0, 0};
+            for (uint32_t e = e0 + lane; e < e1; e += 32) {
+                const int2* q = slots + 3ull * __ldcg(b.inc_list + e);
+                const int2 x0 = __ldcg(q), x1 = __ldcg(q + 1), x2 = __ldcg(q + 2);
+                sum[0] = (int32_t)((uint32_t)sum[0] + (uint32_t)x0.x);
+                sum[1] = (int32_t)((uint32_t)sum[1] + (uint32_t)x0.y);
+                sum[2] = (int32_t)((uint32_t)sum[2] + (uint32_t)x1.x);
+                sum[3] = (int32_t)((uint32_t)sum[3] + (uint32_t)x1.y);
+                sum[4] = (int32_t)((uint32_t)sum[4] + (uint32_t)x2.x);
+                sum[5] = (int32_t)((uint32_t)sum[5] + (uint32_t)x2.y);
+            }
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1)
+#pragma unroll
+                for (int c = 0; c < 6; ++c)
+                    sum[c] = (int32_t)((uint32_t)sum[c] + (uint32_t)__shfl_down_sync(0xffffffffu, sum[c], o));
+            if (lane == 0) {
+                int2* d2 = reinterpret_cast<int2*>(b.deltas + 6ull * x);   // 24-byte rows are 8-byte aligned
+                const int2 x0 = __ldcg(d2), x1 = __ldcg(d2 + 1), x2 = __ldcg(d2 + 2);
+                if ((x0.x | x0.y | x1.x | x1.y | x2.x | x2.y) != 0) {
+                    d2[0] = make_int2(0, 0);
+                    d2[1] = make_int2(0, 0);
+                    d2[2] = make_int2(0, 0);
+                }
+                const int32_t t0 = (int32_t)((uint32_t)sum[0] + (uint32_t)x0.x);
+                const int32_t t1 = (int32_t)((uint32_t)sum[1] + (uint32_t)x0.y);
+                const int32_t t2 = (int32_t)((uint32_t)sum[2] + (uint32_t)x1.x);
+                const int32_t t3 = (int32_t)((uint32_t)sum[3] + (uint32_t)x1.y);
+                const int32_t t4 = (int32_t)((uint32_t)sum[4] + (uint32_t)x2.x);
+                const int32_t t5 = (int32_t)((uint32_t)sum[5] + (uint32_t)x2.y);
+                const f3 ld = mkf3((float)t0, (float)t1, (float)t2) / s;
+                const f3 ad = mkf3((float)t3, (float)t4, (float)t5) / s;
+                dl[x] = f4(xyz(__ldg(vl + x)) + ld, 0.0f);
+                da_out[x] = f4(xyz(__ldg(va + x)) + ad, 0.0f);
+            }
+        }
+        grid_barrier(barrier, flags, parts);
+    }
+}
+
 // All solver iterations in one cooperative launch: warm start, then
 // (iterations - 1) projections, each followed by the velocity apply
 // (device.rs:1343-1416 dispatch order), separated by grid barriers.
@@ -1817,8 +1943,12 @@ __global__ void __launch_bounds__(kSolveThreads) k_solve_all(StepBuffers b, Step
         }
         return;
     }
-    if (b.contact_deltas) {   // heavy tick: no per-contact atomics
+    if (b.heavy_form == MK_HEAVY_GATHER) {   // no per-contact atomics
         solve_gather(b, p, cur, A, iterations, barrier, parts);
+        return;
+    }
+    if (b.heavy_form == MK_HEAVY_SPLIT) {   // body a's deltas by atomics, body b's gathered
+        solve_split(b, p, cur, A, iterations, barrier, parts);
         return;
     }
     for (uint32_t it = 0; it < iterations; ++it) {
@@ -2414,11 +2544,12 @@ cudaError_t launch_narrowphase(const StepBuffers& b, const StepParams& p, const 
     return cudaGetLastError();
 }
 
-// Heavy ticks: the gather form (0, default) or the scatter form with per-contact
-// atomics (1); both give the same bits.  Read when a tick is captured.
-static uint32_t g_heavy_solve_scatter = 0;
-void set_heavy_solve_form(uint32_t form) { g_heavy_solve_scatter = form == 1u ? 1u : 0u; }
-uint32_t heavy_solve_form() { return g_heavy_solve_scatter; }
+// Form of the heavy-tick solve (MK_TUNE_HEAVY_SOLVE; 0 = the default, the
+// fastest measured); every form gives the same bits.  Read when a tick is captured.
+static uint32_t g_heavy_solve_form = 0;
+void set_heavy_solve_form(uint32_t form) { g_heavy_solve_form = form <= MK_HEAVY_SPLIT ? form : 0u; }
+uint32_t heavy_solve_form() { return g_heavy_solve_form; }
+constexpr uint32_t kDefaultHeavyForm = MK_HEAVY_SCATTER;
 
 cudaError_t launch_contact_solver(const StepBuffers& b, const StepParams& p, const StepLaunch& l, int parity,
                                   cudaStream_t s, const std::function<cudaError_t()>& before_solve) {
@@ -2441,7 +2572,7 @@ cudaError_t launch_contact_solver(const StepBuffers& b, const StepParams& p, con
     GpuContact* cur = b.contacts[parity];
     uint32_t* barrier = b.grid_barrier;
     StepBuffers bb = b;
-    if (g_heavy_solve_scatter) bb.contact_deltas = nullptr;   // heavy ticks keep the per-contact atomics
+    bb.heavy_form = g_heavy_solve_form ? g_heavy_solve_form : kDefaultHeavyForm;
     StepParams pp = p;
     uint32_t learned = l.learned_warm ? 1u : 0u;
     const bool residual = p.contact_tol > 0.0f;

@@ -529,7 +529,7 @@ class GpuPhysics:
 
 TUNE_SORT_ITEMS = 1
 TUNE_CLOSURE_GRID = 2   # reference-mode closure loop: 0 by size, 1 one block, 2 the whole grid
-TUNE_HEAVY_SOLVE = 3    # heavy-tick contact solve: 0 gather (per-contact delta slots), 1 scatter (atomics)
+TUNE_HEAVY_SOLVE = 3    # heavy-tick contact solve: 0 default, 1 scatter (atomics), 2 gather (slots), 3 split
 
 
 def set_tuning(key: int, value: int) -> int:

@@ -1415,6 +1415,7 @@ template <class T> struct World : WorldBase {
     }
     uint32_t closure_pcg_rounds = 8;
     void solve_closure_pcg() {   // closure.wgsl:333-427 (one Newton step, 8 diagonal-PCG rounds)
+        const bool chunked = ct.cq_coords.size() > kSerialDot;
         T rz = T(0);
         for (uint32_t c = 0; c < Q; ++c) {
             T g = grad[c], d = dgl[c], r = T(0), z = T(0);
@@ -1422,6 +1423,7 @@ template <class T> struct World : WorldBase {
             pcg[c] = {T(0), r, z, z, T(0)};
             rz += r * z;
         }
+        if (chunked) rz = closure_dot_chunked([&](uint32_t c) { return pcg[c].res * pcg[c].pre; });
         for (uint32_t it = 0; it < closure_pcg_rounds; ++it) {
             for (uint32_t c = 0; c < Q; ++c) pcg[c].op = T(0);
             for (uint32_t j = 0; j < J; ++j) {
@@ -1437,6 +1439,7 @@ template <class T> struct World : WorldBase {
             }
             T dop = T(0);
             for (uint32_t c = 0; c < Q; ++c) dop += pcg[c].dir * pcg[c].op;
+            if (chunked) dop = closure_dot_chunked([&](uint32_t c) { return pcg[c].dir * pcg[c].op; });
             T alpha = std::fabs(dop) > T(1.0e-20f) ? rz / dop : T(0);
             T nrz = T(0);
             for (uint32_t c = 0; c < Q; ++c) {
@@ -1447,6 +1450,7 @@ template <class T> struct World : WorldBase {
                 if (d > T(1.0e-12f)) pcg[c].pre = pcg[c].res / d;
                 nrz += pcg[c].res * pcg[c].pre;
             }
+            if (chunked) nrz = closure_dot_chunked([&](uint32_t c) { return pcg[c].res * pcg[c].pre; });
             T beta = std::fabs(rz) > T(1.0e-20f) ? nrz / rz : T(0);
             for (uint32_t c = 0; c < Q; ++c) pcg[c].dir = pcg[c].pre + beta * pcg[c].dir;
             rz = nrz;
@@ -1458,6 +1462,7 @@ template <class T> struct World : WorldBase {
         }
     }
     void closure_loop() {   // device.rs:973-1020
+        build_closure_topology();
         bool converged_prev = false;
         for (uint32_t step = 0; step < 12; ++step) {
             std::fill(grad.begin(), grad.end(), T(0));
@@ -1549,26 +1554,42 @@ template <class T> struct World : WorldBase {
             }
         }
     }
-    static double block_sum_1024(const std::vector<double>& part) {   // part: 1024 per-thread partials
-        double warp[32];
+    template <class S>
+    static S block_sum_1024(const std::vector<S>& part) {   // part: 1024 per-thread partials
+        S warp[32];
         for (int w = 0; w < 32; ++w) {
-            double v[32];
+            S v[32];
             for (int l = 0; l < 32; ++l) v[l] = part[32 * w + l];
             for (int o = 16; o > 0; o >>= 1) {
-                double nv[32];
+                S nv[32];
                 for (int l = 0; l < 32; ++l) nv[l] = v[l] + (l + o < 32 ? v[l + o] : v[l]);
                 std::memcpy(v, nv, sizeof(v));
             }
             warp[w] = v[0];
         }
-        double v[32];
+        S v[32];
         std::memcpy(v, warp, sizeof(v));
         for (int o = 16; o > 0; o >>= 1) {
-            double nv[32];
+            S nv[32];
             for (int l = 0; l < 32; ++l) nv[l] = v[l] + (l + o < 32 ? v[l + o] : v[l]);
             std::memcpy(v, nv, sizeof(v));
         }
         return v[0];
+    }
+    // The reference loop's dot products above 512 closure coordinates, in the GPU's
+    // order: per chunk of 1,024 closure coordinates the block tree of the per-thread
+    // terms (in T), the chunk sums added in chunk order.  Up to 512 the reference's
+    // serial sum over the coordinates is kept.
+    static constexpr uint32_t kSerialDot = 512;
+    template <class F> T closure_dot_chunked(F term) const {   // term(c) -> T for coordinate c
+        const uint32_t NQ = (uint32_t)ct.cq_coords.size();
+        T acc = T(0);
+        for (uint32_t c0 = 0; c0 < NQ; c0 += 1024) {
+            std::vector<T> part(1024, T(0));
+            for (uint32_t t = 0; t < 1024 && c0 + t < NQ; ++t) part[t] = term(ct.cq_coords[c0 + t]);
+            acc += block_sum_1024(part);
+        }
+        return acc;
     }
     // The GPU's order: chunks of 1,024 coordinates (one per thread), the block
     // tree per chunk, the chunk sums added in chunk order.
