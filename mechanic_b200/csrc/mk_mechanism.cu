@@ -35,6 +35,7 @@ constexpr uint32_t kClosureThreads = 1024;
 constexpr uint32_t kClosureSteps = 12;     // device.rs:974
 constexpr uint32_t kClosureRounds = 8;     // closure.wgsl:356
 constexpr uint32_t kMaxLoop = 8;           // coordinates of one per-loop preconditioner block
+constexpr uint32_t kLongList = 256;        // slot runs longer than this are summed by a warp
 
 // ----------------------------------------------------------------- host side
 MechParams make_mech_params(const MkCreation* cr, const StepParams& p, uint32_t iterations, uint32_t closure_mode,
@@ -114,6 +115,14 @@ MechTopology derive_topology(const MkCreation* cr, MechParams& p) {
             if (closure_root[body]) t.cb_bodies.push_back(i);
         }
     }
+    // slot values are stored at their position in cq_slots, so each coordinate reads its
+    // run contiguously; runs longer than kLongList (coordinates near the root of a large
+    // loop lattice carry a slot of nearly every closure) are summed by a warp
+    t.slot_pos.assign(t.slot_body.size(), 0u);
+    for (uint32_t i = 0; i < (uint32_t)t.cq_slots.size(); ++i) t.slot_pos[t.cq_slots[i]] = i;
+    for (uint32_t q = 0; q + 1 < (uint32_t)t.cq_off.size(); ++q)
+        if (t.cq_off[q + 1] - t.cq_off[q] > kLongList) t.long_q.push_back(q);
+    p.long_coords = (uint32_t)t.long_q.size();
     t.slot_closure.resize(t.slot_body.size());
     for (size_t k = 0; k + 1 < t.cl_slot_off.size(); ++k)
         for (uint32_t sl = t.cl_slot_off[k]; sl < t.cl_slot_off[k + 1]; ++sl) t.slot_closure[sl] = (uint32_t)k;
@@ -175,6 +184,8 @@ void carve_mechanism(MechBuffers& m, const MechParams& p, uint32_t B, uint32_t J
     m.cb_bodies = u32(p.closure_bodies);
     m.slot_g = f32(p.slots);
     m.slot_d = f32(p.slots);
+    m.slot_pos = u32(p.slots);
+    m.long_q = u32(p.long_coords);
     m.grad = f32(Q);
     m.diag = f32(Q);
     m.pcg = f32(5ull * Q);
@@ -243,6 +254,8 @@ bool upload_mechanism(MechBuffers& m, const MechParams& p, const MechTopology& t
     if (e == cudaSuccess) e = put(m.cq_coords, t.cq_coords, s);
     if (e == cudaSuccess) e = put(m.cq_off, t.cq_off, s);
     if (e == cudaSuccess) e = put(m.cq_slots, t.cq_slots, s);
+    if (e == cudaSuccess) e = put(m.slot_pos, t.slot_pos, s);
+    if (e == cudaSuccess && !t.long_q.empty()) e = put(m.long_q, t.long_q, s);
     if (e == cudaSuccess) e = put(m.cb_bodies, t.cb_bodies, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     (void)p;
@@ -726,6 +739,45 @@ __device__ __forceinline__ float dot_total(uint32_t nq, const MechBuffers& m, co
 // slot_g[sl] = the slot's share of J^T J x: per closure the branch products
 // (sums over its slots in slot order, branch a then b) and their transposes,
 // from the stored Jacobian columns; closures strided over the block or grid.
+// Serial sums of the slot values of the closure coordinates whose runs are longer
+// than kLongList, one warp per coordinate: the lanes load 32 consecutive values
+// of the run and the warp adds them one by one in run order, so the sum is the
+// same as the one-thread loop over the run (closure index, branch a before b).
+// kEval: evaluation sums (a NaN gradient marks a slot without contribution,
+// diagonal summed beside it) into out_g / out_d; else plain sums into out_g.
+template <bool kEval>
+__device__ __forceinline__ void gather_long_runs(const MechBuffers& m, const MechParams& p, float* out_g,
+                                                 float* out_d) {
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t gwarp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nwarps = (gridDim.x * blockDim.x) >> 5;
+    for (uint32_t w = gwarp; w < p.long_coords; w += nwarps) {
+        const uint32_t q = m.long_q[w];
+        const uint32_t i0 = m.cq_off[q], i1 = m.cq_off[q + 1];
+        float g = 0.0f, d = 0.0f;
+        for (uint32_t base = i0; base < i1; base += 32u) {
+            const uint32_t i = base + lane;
+            const float vg = i < i1 ? __ldcg(m.slot_g + i) : 0.0f;
+            const float vd = (kEval && i < i1) ? __ldcg(m.slot_d + i) : 0.0f;
+            const uint32_t cnt = min(32u, i1 - base);
+            for (uint32_t j = 0; j < cnt; ++j) {
+                const float sg = __shfl_sync(0xffffffffu, vg, j);
+                if (kEval) {
+                    const float sd = __shfl_sync(0xffffffffu, vd, j);
+                    if (sg == sg) { g += sg; d += sd; }
+                } else {
+                    g += sg;
+                }
+            }
+        }
+        if (lane == 0) {
+            const uint32_t c = m.cq_coords[q];
+            out_g[c] = g;
+            if (kEval) out_d[c] = d;
+        }
+    }
+}
+__device__ __forceinline__ bool long_run(const MechBuffers& m, uint32_t q) { return m.cq_off[q + 1] - m.cq_off[q] > kLongList; }
+
 __device__ __forceinline__ void closure_products(const MechBuffers& m, const MechParams& p, const float* x) {
     const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x, nt = gridDim.x * blockDim.x;
     for (uint32_t k = tid; k < p.closures; k += nt) {
@@ -749,7 +801,7 @@ __device__ __forceinline__ void closure_products(const MechBuffers& m, const Mec
         const f3 pp = pp_a + pp_b, pa = pa_a + pa_b;
 #pragma unroll 4
         for (uint32_t sl = s0; sl < s1; ++sl)
-            m.slot_g[sl] = dot(xyz(m.slot_v[2 * sl]), pp) + 1.0f * dot(xyz(m.slot_v[2 * sl + 1]), pa);
+            m.slot_g[m.slot_pos[sl]] = dot(xyz(m.slot_v[2 * sl]), pp) + 1.0f * dot(xyz(m.slot_v[2 * sl + 1]), pa);
     }
 }
 
@@ -864,14 +916,18 @@ __global__ void __launch_bounds__(kClosureThreads) k_closure_loop(StepBuffers b,
                         }
                     }
                     // NaN marks "no contribution" so the gather skips it
-                    m.slot_g[sl] = valid ? g : __int_as_float(0x7fffffff);
-                    m.slot_d[sl] = valid ? d : 0.0f;
+                    m.slot_g[m.slot_pos[sl]] = valid ? g : __int_as_float(0x7fffffff);
+                    m.slot_d[m.slot_pos[sl]] = valid ? d : 0.0f;
                 }
             }
         }
         loop_sync<kGrid>(m.grid_barrier, flags);
         const bool unconverged = ld_relaxed_u32(&st[0]) > 10u || ld_relaxed_u32(&st[1]) > 1000u;
         if (unconverged) ++steps;
+        if (evaluate && p.long_coords) {   // long runs first, one warp each
+            gather_long_runs<true>(m, p, m.grad, m.diag);
+            loop_sync<kGrid>(m.grid_barrier, flags);
+        }
         // gather per coordinate in the serial accumulation order, then the PCG's
         // initial vectors (solve_closure_pcg, closure.wgsl:333-427), chunk by chunk
         for (uint32_t c = blockIdx.x; c < chunks; c += gridDim.x) {
@@ -879,11 +935,13 @@ __global__ void __launch_bounds__(kClosureThreads) k_closure_loop(StepBuffers b,
             float part = 0.0f;
             if (q < NQ) {
                 float g = 0.0f, d = 0.0f;
-                if (evaluate) {
+                if (evaluate && long_run(m, q)) {
+                    g = m.grad[m.cq_coords[q]];
+                    d = m.diag[m.cq_coords[q]];
+                } else if (evaluate) {
                     for (uint32_t i = m.cq_off[q]; i < m.cq_off[q + 1]; ++i) {
-                        const uint32_t sl = m.cq_slots[i];
-                        const float sg = m.slot_g[sl];
-                        if (sg == sg) { g += sg; d += m.slot_d[sl]; }
+                        const float sg = m.slot_g[i];
+                        if (sg == sg) { g += sg; d += m.slot_d[i]; }
                     }
                 }
                 const uint32_t cc = m.cq_coords[q];
@@ -906,12 +964,18 @@ __global__ void __launch_bounds__(kClosureThreads) k_closure_loop(StepBuffers b,
                 // (closure.wgsl:194-266), from the step's stored columns
                 closure_products(m, p, dir);
                 loop_sync<kGrid>(m.grid_barrier, flags);
+                if (p.long_coords) {
+                    gather_long_runs<false>(m, p, op, nullptr);
+                    loop_sync<kGrid>(m.grid_barrier, flags);
+                }
                 for (uint32_t c = blockIdx.x; c < chunks; c += gridDim.x) {
                     const uint32_t q = c * kDotChunk + threadIdx.x;
                     float dpart = 0.0f;
                     if (q < NQ) {
                         float o = 0.0f;
-                        for (uint32_t i = m.cq_off[q]; i < m.cq_off[q + 1]; ++i) o += m.slot_g[m.cq_slots[i]];
+                        if (long_run(m, q)) o = op[m.cq_coords[q]];
+                        else
+                            for (uint32_t i = m.cq_off[q]; i < m.cq_off[q + 1]; ++i) o += m.slot_g[i];
                         const uint32_t cc = m.cq_coords[q];
                         op[cc] = o;
                         dpart = dir[cc] * o;
@@ -1034,9 +1098,11 @@ __device__ void closure_apply(const MechBuffers& m, const MechParams& p, const f
     const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x, nt = gridDim.x * blockDim.x;
     closure_products(m, p, x);
     loop_sync<kGrid>(m.grid_barrier, flags);
+    gather_long_runs<false>(m, p, out, nullptr);
     for (uint32_t q = tid; q < p.closure_coords; q += nt) {
+        if (long_run(m, q)) continue;
         float o = 0.0f;
-        for (uint32_t i = m.cq_off[q]; i < m.cq_off[q + 1]; ++i) o += m.slot_g[m.cq_slots[i]];
+        for (uint32_t i = m.cq_off[q]; i < m.cq_off[q + 1]; ++i) o += m.slot_g[i];
         out[m.cq_coords[q]] = o;
     }
     loop_sync<kGrid>(m.grid_barrier, flags);
@@ -1116,21 +1182,26 @@ __global__ void __launch_bounds__(kClosureThreads) k_closure_eval(StepBuffers b,
             }
             m.slot_v[2 * sl] = f4(pd, __uint_as_float(coord));
             m.slot_v[2 * sl + 1] = f4(ad, __uint_as_float(m.slot_closure[sl]));
-            m.slot_g[sl] = valid ? g : __int_as_float(0x7fffffff);
-            m.slot_d[sl] = valid ? d : 0.0f;
+            m.slot_g[m.slot_pos[sl]] = valid ? g : __int_as_float(0x7fffffff);
+            m.slot_d[m.slot_pos[sl]] = valid ? d : 0.0f;
         }
     }
     loop_sync<kGrid>(m.grid_barrier, flags);
+    if (p.long_coords) {
+        gather_long_runs<true>(m, p, m.grad, m.diag);
+        loop_sync<kGrid>(m.grid_barrier, flags);
+    }
     for (uint32_t q = tid; q < NQ; q += nt) {
-        float g = 0.0f, d = 0.0f;
-        for (uint32_t i = m.cq_off[q]; i < m.cq_off[q + 1]; ++i) {
-            const uint32_t sl = m.cq_slots[i];
-            const float sg = m.slot_g[sl];
-            if (sg == sg) { g += sg; d += m.slot_d[sl]; }
-        }
         const uint32_t c = m.cq_coords[q];
-        m.grad[c] = g;
-        m.diag[c] = d;
+        if (!long_run(m, q)) {
+            float g = 0.0f, d = 0.0f;
+            for (uint32_t i = m.cq_off[q]; i < m.cq_off[q + 1]; ++i) {
+                const float sg = m.slot_g[i];
+                if (sg == sg) { g += sg; d += m.slot_d[i]; }
+            }
+            m.grad[c] = g;
+            m.diag[c] = d;
+        }
         // probe vectors: ones and alternating signs over the coordinate list
         m.pcg[c] = 1.0f;
         m.pcg[Q + c] = (q & 1u) ? -1.0f : 1.0f;

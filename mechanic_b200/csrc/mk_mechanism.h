@@ -23,6 +23,7 @@ struct MechParams {
     // closure topology (host-derived, static)
     uint32_t closures = 0;           // closure bearings
     uint32_t slots = 0;              // joints on closure branches, over all closures
+    uint32_t long_coords = 0;        // closure coordinates with more than kLongList slots
     uint32_t closure_coords = 0;     // distinct coordinates on closure branches
     uint32_t closure_bodies = 0;     // bodies of components that contain a closure
     // MK_CLOSURE_PCG_RESIDUAL
@@ -68,8 +69,10 @@ struct MechBuffers {
     uint32_t* cq_off = nullptr;                 // closure_coords + 1: CSR into cq_slots
     uint32_t* cq_slots = nullptr;               // slots of each coordinate, in serial accumulation order
     uint32_t* cb_bodies = nullptr;              // bodies of closure components
-    float* slot_g = nullptr;                    // per-slot gradient / operator contributions
-    float* slot_d = nullptr;
+    float* slot_g = nullptr;                    // per-slot gradient / operator contributions, stored at the
+    float* slot_d = nullptr;                    // slot's position in cq_slots (each coordinate's run contiguous)
+    uint32_t* slot_pos = nullptr;               // position of each slot in cq_slots
+    uint32_t* long_q = nullptr;                 // closure coordinates (positions) with long slot lists
     float* grad = nullptr;                      // Q (closure.wgsl:46-49 accumulators)
     float* diag = nullptr;                      // Q
     float* pcg = nullptr;                       // 5 x Q: sol, res, pre, dir, op (closure.wgsl:51-60)
@@ -101,7 +104,7 @@ MechParams make_mech_params(const MkCreation* cr, const StepParams& p, uint32_t 
 struct MechTopology {
     std::vector<uint32_t> level_bodies, level_offsets;
     std::vector<uint32_t> cl_bearings, cl_slot_off, cl_split, slot_body, cq_coords, cq_off, cq_slots, cb_bodies;
-    std::vector<uint32_t> slot_closure;
+    std::vector<uint32_t> slot_closure, slot_pos, long_q;
     std::vector<uint32_t> loop_off, loop_q;
 };
 MechTopology derive_topology(const MkCreation* cr, MechParams& p);

@@ -140,3 +140,24 @@ def test_bench_runner_linkage_gates(cuda_lib, scenario):
     assert out["correctness_passed"], out["error_flags"]
     if scenario == "four_bar":
         assert out["anchor_residual_m"] <= 1e-5
+
+
+@pytest.mark.parametrize("mode", ["reference", "pcg"])
+def test_loop_lattice_long_slot_runs_bitexact(cuda_lib, mode):
+    """mechanic-bench's loop lattice (main.rs:456-524) at 20 x 20 x 3: 1,083 closures on one
+    spanning tree, so the coordinates near its root lie on hundreds of closure branches (38 of
+    them on more than 256, up to 1,444).  Those runs are summed by a warp in the same serial
+    order as the one-thread runs: coordinates, state and contacts equal the oracle's bit for bit."""
+    from mechanic_b200 import learned
+    scene = scenes.loops_grid(20, 20, 3)
+    cfg = GpuPhysicsConfig() if mode == "reference" else learned.closure_config(
+        preconditioner=abi.PRECOND_DIAGONAL, max_iterations=16)
+    gpu, orc = _pair(scene, cfg)
+    # disturb the lattice so the closures are not converged from the start
+    coords = np.zeros(scene.coordinate_count, abi.MECHANISM_COORDINATE)
+    coords["angle"][::7] = 0.01
+    gpu.initialize_mechanism_coordinates(coords)
+    orc.set_coordinates(coords)
+    for tick in range(1, 4):
+        _compare(gpu, orc, tick, f"loop lattice {mode}")
+    _same(gpu.contacts(), orc.contacts(), "loop lattice contacts")
