@@ -351,32 +351,42 @@ def measure_closure_forms(local: int, ticks: int = 20, chains: int = 4000):
 
 
 def measure_full_forms(local: int, ticks: int = 6) -> dict:
-    """The full form at scale (1,250,000 bodies: the 100,000-body mix on a 100^3 lattice and
-    50,000 five-body chains, 10% loop-closed), ticks 1..`ticks` from the generated state in
-    three forms: the reference's fixed passes (8 contact passes, 12 x 8 closure rounds); the
-    plain form iterated to 1e-5 (cached warm start, per-loop block-Jacobi closure PCG); the
-    learned form (network warm start, network-corrected closure blocks) to the same residual."""
+    """The full form at scale, ticks 1..`ticks` from the generated state.
+
+    Closures: the 1,250,000-body scene (the 100,000-body mix on a 100^3 lattice and 50,000
+    five-body chains, 10% loop-closed) with the reference's 12 x 8 closure rounds, and with
+    closure PCG to 1e-5 under per-loop block Jacobi and under the network-corrected blocks.  Its
+    chains have dynamic roots, so its contact solve keeps the reference's interleaved fixed
+    passes (device.rs:1108-1155), which the residual mode does not iterate.
+    Contacts: the 1,000,000-body lattice alone, 8 fixed passes against passes until 1e-5 with the
+    cached and with the learned warm start (cap 512)."""
     import torch
     from mechanic_b200 import abi, learned, scenes
     from mechanic_b200.physics import GpuPhysics, GpuPhysicsConfig
-    scene = scenes.config_full()
     warm = np.load(os.path.join(ROOT, "mechanic_b200", "data", "warm_start.npy"))
     xs, ts, _ = learned.collect_closure_samples(scenes.bearing_chains(4000), 8, learned.closure_config(
         preconditioner=abi.PRECOND_PAIR_BLOCKS, device=local))
     precond, _ = learned.train_preconditioner(xs, ts, steps=2000)
     caps = {"pair_capacity": 1 << 28}
-    forms = {
-        "reference passes": GpuPhysicsConfig(device=local),
-        "plain to 1e-5": GpuPhysicsConfig(device=local, contact_tolerance=1e-5, contact_max_iterations=512,
-                                          closure_mode=abi.CLOSURE_PCG_RESIDUAL, closure_tolerance=1e-5),
-        "learned to 1e-5": GpuPhysicsConfig(device=local, contact_tolerance=1e-5, contact_max_iterations=512,
-                                            warm_start=abi.WARM_LEARNED, closure_mode=abi.CLOSURE_PCG_RESIDUAL,
-                                            closure_tolerance=1e-5, preconditioner=abi.PRECOND_LEARNED),
-    }
-    out = {"workload": f"1,250,000 bodies (100^3 lattice of the 100,000-body mix + 50,000 five-body chains, 10% "
-                       f"loop-closed), ticks 1..{ticks}", "bodies": scene.body_count,
-           "colliders": scene.collider_count}
-    for name, cfg in forms.items():
+    full = scenes.config_full()
+    lattice = scenes.stack_grid(100, 100, 100, seed=0)
+    forms = [
+        ("full: reference passes", full, GpuPhysicsConfig(device=local)),
+        ("full: closure PCG to 1e-5, block Jacobi", full,
+         GpuPhysicsConfig(device=local, closure_mode=abi.CLOSURE_PCG_RESIDUAL, closure_tolerance=1e-5)),
+        ("full: closure PCG to 1e-5, learned blocks", full,
+         GpuPhysicsConfig(device=local, closure_mode=abi.CLOSURE_PCG_RESIDUAL, closure_tolerance=1e-5,
+                          preconditioner=abi.PRECOND_LEARNED)),
+        ("lattice: 8 contact passes", lattice, GpuPhysicsConfig(device=local)),
+        ("lattice: contacts to 1e-5, cached start", lattice,
+         GpuPhysicsConfig(device=local, contact_tolerance=1e-5, contact_max_iterations=512)),
+        ("lattice: contacts to 1e-5, learned start", lattice,
+         GpuPhysicsConfig(device=local, contact_tolerance=1e-5, contact_max_iterations=512,
+                          warm_start=abi.WARM_LEARNED)),
+    ]
+    out = {"workload": f"full: 1,250,000 bodies ({full.collider_count} colliders); lattice: 1,000,000 bodies "
+                       f"({lattice.collider_count} colliders); ticks 1..{ticks} from the generated state"}
+    for name, scene, cfg in forms:
         with GpuPhysics(scene, cfg, capacities=caps) as g:
             if cfg.warm_start == abi.WARM_LEARNED:
                 g.set_warm_start_network(warm)
