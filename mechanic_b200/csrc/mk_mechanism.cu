@@ -748,24 +748,53 @@ __device__ __forceinline__ float dot_total(uint32_t nq, const MechBuffers& m, co
 template <bool kEval>
 __device__ __forceinline__ void gather_long_runs(const MechBuffers& m, const MechParams& p, float* out_g,
                                                  float* out_d) {
+    constexpr uint32_t kAhead = 4;   // batches of 32 values in flight per warp
     const uint32_t lane = threadIdx.x & 31u;
     const uint32_t gwarp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nwarps = (gridDim.x * blockDim.x) >> 5;
     for (uint32_t w = gwarp; w < p.long_coords; w += nwarps) {
         const uint32_t q = m.long_q[w];
         const uint32_t i0 = m.cq_off[q], i1 = m.cq_off[q + 1];
+        float pg[kAhead], pd[kAhead];
+#pragma unroll
+        for (uint32_t k = 0; k < kAhead; ++k) {
+            const uint32_t i = i0 + 32u * k + lane;
+            pg[k] = i < i1 ? __ldcg(m.slot_g + i) : 0.0f;
+            pd[k] = (kEval && i < i1) ? __ldcg(m.slot_d + i) : 0.0f;
+        }
         float g = 0.0f, d = 0.0f;
         for (uint32_t base = i0; base < i1; base += 32u) {
-            const uint32_t i = base + lane;
-            const float vg = i < i1 ? __ldcg(m.slot_g + i) : 0.0f;
-            const float vd = (kEval && i < i1) ? __ldcg(m.slot_d + i) : 0.0f;
+            const float vg = pg[0], vd = pd[0];
+#pragma unroll
+            for (uint32_t k = 0; k + 1 < kAhead; ++k) {
+                pg[k] = pg[k + 1];
+                pd[k] = pd[k + 1];
+            }
+            {
+                const uint32_t i = base + 32u * kAhead + lane;
+                pg[kAhead - 1] = i < i1 ? __ldcg(m.slot_g + i) : 0.0f;
+                pd[kAhead - 1] = (kEval && i < i1) ? __ldcg(m.slot_d + i) : 0.0f;
+            }
             const uint32_t cnt = min(32u, i1 - base);
-            for (uint32_t j = 0; j < cnt; ++j) {
-                const float sg = __shfl_sync(0xffffffffu, vg, j);
-                if (kEval) {
-                    const float sd = __shfl_sync(0xffffffffu, vd, j);
-                    if (sg == sg) { g += sg; d += sd; }
-                } else {
-                    g += sg;
+            if (cnt == 32u) {
+#pragma unroll
+                for (uint32_t j = 0; j < 32u; ++j) {
+                    const float sg = __shfl_sync(0xffffffffu, vg, j);
+                    if (kEval) {
+                        const float sd = __shfl_sync(0xffffffffu, vd, j);
+                        if (sg == sg) { g += sg; d += sd; }
+                    } else {
+                        g += sg;
+                    }
+                }
+            } else {
+                for (uint32_t j = 0; j < cnt; ++j) {
+                    const float sg = __shfl_sync(0xffffffffu, vg, j);
+                    if (kEval) {
+                        const float sd = __shfl_sync(0xffffffffu, vd, j);
+                        if (sg == sg) { g += sg; d += sd; }
+                    } else {
+                        g += sg;
+                    }
                 }
             }
         }
