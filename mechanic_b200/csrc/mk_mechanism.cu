@@ -35,7 +35,7 @@ constexpr uint32_t kClosureThreads = 1024;
 constexpr uint32_t kClosureSteps = 12;     // device.rs:974
 constexpr uint32_t kClosureRounds = 8;     // closure.wgsl:356
 constexpr uint32_t kMaxLoop = 8;           // coordinates of one per-loop preconditioner block
-constexpr uint32_t kLongList = 256;        // slot runs longer than this are summed by a warp
+constexpr uint32_t kLongList = 256;        // slot runs longer than this are summed in chunks of this many
 
 // ----------------------------------------------------------------- host side
 MechParams make_mech_params(const MkCreation* cr, const StepParams& p, uint32_t iterations, uint32_t closure_mode,
@@ -117,12 +117,20 @@ MechTopology derive_topology(const MkCreation* cr, MechParams& p) {
     }
     // slot values are stored at their position in cq_slots, so each coordinate reads its
     // run contiguously; runs longer than kLongList (coordinates near the root of a large
-    // loop lattice carry a slot of nearly every closure) are summed by a warp
+    // loop lattice carry a slot of nearly every closure) are summed in chunks
     t.slot_pos.assign(t.slot_body.size(), 0u);
     for (uint32_t i = 0; i < (uint32_t)t.cq_slots.size(); ++i) t.slot_pos[t.cq_slots[i]] = i;
-    for (uint32_t q = 0; q + 1 < (uint32_t)t.cq_off.size(); ++q)
-        if (t.cq_off[q + 1] - t.cq_off[q] > kLongList) t.long_q.push_back(q);
+    t.long_chunk_off.push_back(0);
+    for (uint32_t q = 0; q + 1 < (uint32_t)t.cq_off.size(); ++q) {
+        const uint32_t n = t.cq_off[q + 1] - t.cq_off[q];
+        if (n <= kLongList) continue;
+        const uint32_t w = (uint32_t)t.long_q.size();
+        t.long_q.push_back(q);
+        for (uint32_t c = 0; c < (n + kLongList - 1) / kLongList; ++c) t.chunk_long.push_back(w);
+        t.long_chunk_off.push_back((uint32_t)t.chunk_long.size());
+    }
     p.long_coords = (uint32_t)t.long_q.size();
+    p.long_chunks = (uint32_t)t.chunk_long.size();
     t.slot_closure.resize(t.slot_body.size());
     for (size_t k = 0; k + 1 < t.cl_slot_off.size(); ++k)
         for (uint32_t sl = t.cl_slot_off[k]; sl < t.cl_slot_off[k + 1]; ++sl) t.slot_closure[sl] = (uint32_t)k;
@@ -186,6 +194,10 @@ void carve_mechanism(MechBuffers& m, const MechParams& p, uint32_t B, uint32_t J
     m.slot_d = f32(p.slots);
     m.slot_pos = u32(p.slots);
     m.long_q = u32(p.long_coords);
+    m.long_chunk_off = u32(p.long_coords + 1);
+    m.chunk_long = u32(p.long_chunks);
+    m.chunk_g = f32(p.long_chunks);
+    m.chunk_d = f32(p.long_chunks);
     m.grad = f32(Q);
     m.diag = f32(Q);
     m.pcg = f32(5ull * Q);
@@ -256,6 +268,8 @@ bool upload_mechanism(MechBuffers& m, const MechParams& p, const MechTopology& t
     if (e == cudaSuccess) e = put(m.cq_slots, t.cq_slots, s);
     if (e == cudaSuccess) e = put(m.slot_pos, t.slot_pos, s);
     if (e == cudaSuccess && !t.long_q.empty()) e = put(m.long_q, t.long_q, s);
+    if (e == cudaSuccess && !t.long_q.empty()) e = put(m.long_chunk_off, t.long_chunk_off, s);
+    if (e == cudaSuccess && !t.chunk_long.empty()) e = put(m.chunk_long, t.chunk_long, s);
     if (e == cudaSuccess) e = put(m.cb_bodies, t.cb_bodies, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     (void)p;
@@ -704,6 +718,52 @@ __device__ __forceinline__ void loop_sync(uint32_t* barrier, uint32_t* error_fla
     else __syncthreads();
 }
 
+// Sums of the slot values of the closure coordinates whose runs are longer than
+// kLongList slots (near the root of a large loop lattice a coordinate lies on a
+// branch of nearly every closure: up to 176k slots).  Such a run is summed in two
+// levels, so that no thread adds it alone: each chunk of kLongList consecutive
+// slots serially, in parallel over the chunks, then the chunk sums serially in
+// chunk order.  Runs of up to kLongList slots keep the one serial sum.  The
+// accumulation order of the reference (CAS float atomics, closure.wgsl:128-192) is
+// a race, so any fixed order is as faithful; the oracle restates this one.
+// kEval: evaluation sums (a NaN gradient marks a slot without contribution, the
+// diagonal summed beside it) into out_g / out_d; else plain sums into out_g.
+template <bool kGrid, bool kEval>
+__device__ void gather_long_runs(const MechBuffers& m, const MechParams& p, float* out_g, float* out_d,
+                                 uint32_t* flags) {
+    const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x, nt = gridDim.x * blockDim.x;
+    for (uint32_t c = tid; c < p.long_chunks; c += nt) {
+        const uint32_t w = m.chunk_long[c];
+        const uint32_t q = m.long_q[w];
+        const uint32_t begin = m.cq_off[q] + kLongList * (c - m.long_chunk_off[w]);
+        const uint32_t end = min(begin + kLongList, m.cq_off[q + 1]);
+        float g = 0.0f, d = 0.0f;
+#pragma unroll 8
+        for (uint32_t i = begin; i < end; ++i) {
+            const float sg = __ldcg(m.slot_g + i);
+            if (kEval) {
+                if (sg == sg) { g += sg; d += __ldcg(m.slot_d + i); }
+            } else {
+                g += sg;
+            }
+        }
+        m.chunk_g[c] = g;
+        if (kEval) m.chunk_d[c] = d;
+    }
+    loop_sync<kGrid>(m.grid_barrier, flags);
+    for (uint32_t w = tid; w < p.long_coords; w += nt) {
+        float g = 0.0f, d = 0.0f;
+        for (uint32_t c = m.long_chunk_off[w]; c < m.long_chunk_off[w + 1]; ++c) {
+            g += __ldcg(m.chunk_g + c);
+            if (kEval) d += __ldcg(m.chunk_d + c);
+        }
+        const uint32_t cc = m.cq_coords[m.long_q[w]];
+        out_g[cc] = g;
+        if (kEval) out_d[cc] = d;
+    }
+    loop_sync<kGrid>(m.grid_barrier, flags);
+}
+
 // The chunked dot: `part` is this thread's term for the coordinate of chunk
 // `c` it holds (0 when none); the block tree sum of the chunk goes to
 // chunk_part[c].  Call for every chunk the block walks, all threads together.
@@ -739,72 +799,6 @@ __device__ __forceinline__ float dot_total(uint32_t nq, const MechBuffers& m, co
 // slot_g[sl] = the slot's share of J^T J x: per closure the branch products
 // (sums over its slots in slot order, branch a then b) and their transposes,
 // from the stored Jacobian columns; closures strided over the block or grid.
-// Serial sums of the slot values of the closure coordinates whose runs are longer
-// than kLongList, one warp per coordinate: the lanes load 32 consecutive values
-// of the run and the warp adds them one by one in run order, so the sum is the
-// same as the one-thread loop over the run (closure index, branch a before b).
-// kEval: evaluation sums (a NaN gradient marks a slot without contribution,
-// diagonal summed beside it) into out_g / out_d; else plain sums into out_g.
-template <bool kEval>
-__device__ __forceinline__ void gather_long_runs(const MechBuffers& m, const MechParams& p, float* out_g,
-                                                 float* out_d) {
-    constexpr uint32_t kAhead = 4;   // batches of 32 values in flight per warp
-    const uint32_t lane = threadIdx.x & 31u;
-    const uint32_t gwarp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nwarps = (gridDim.x * blockDim.x) >> 5;
-    for (uint32_t w = gwarp; w < p.long_coords; w += nwarps) {
-        const uint32_t q = m.long_q[w];
-        const uint32_t i0 = m.cq_off[q], i1 = m.cq_off[q + 1];
-        float pg[kAhead], pd[kAhead];
-#pragma unroll
-        for (uint32_t k = 0; k < kAhead; ++k) {
-            const uint32_t i = i0 + 32u * k + lane;
-            pg[k] = i < i1 ? __ldcg(m.slot_g + i) : 0.0f;
-            pd[k] = (kEval && i < i1) ? __ldcg(m.slot_d + i) : 0.0f;
-        }
-        float g = 0.0f, d = 0.0f;
-        for (uint32_t base = i0; base < i1; base += 32u) {
-            const float vg = pg[0], vd = pd[0];
-#pragma unroll
-            for (uint32_t k = 0; k + 1 < kAhead; ++k) {
-                pg[k] = pg[k + 1];
-                pd[k] = pd[k + 1];
-            }
-            {
-                const uint32_t i = base + 32u * kAhead + lane;
-                pg[kAhead - 1] = i < i1 ? __ldcg(m.slot_g + i) : 0.0f;
-                pd[kAhead - 1] = (kEval && i < i1) ? __ldcg(m.slot_d + i) : 0.0f;
-            }
-            const uint32_t cnt = min(32u, i1 - base);
-            if (cnt == 32u) {
-#pragma unroll
-                for (uint32_t j = 0; j < 32u; ++j) {
-                    const float sg = __shfl_sync(0xffffffffu, vg, j);
-                    if (kEval) {
-                        const float sd = __shfl_sync(0xffffffffu, vd, j);
-                        if (sg == sg) { g += sg; d += sd; }
-                    } else {
-                        g += sg;
-                    }
-                }
-            } else {
-                for (uint32_t j = 0; j < cnt; ++j) {
-                    const float sg = __shfl_sync(0xffffffffu, vg, j);
-                    if (kEval) {
-                        const float sd = __shfl_sync(0xffffffffu, vd, j);
-                        if (sg == sg) { g += sg; d += sd; }
-                    } else {
-                        g += sg;
-                    }
-                }
-            }
-        }
-        if (lane == 0) {
-            const uint32_t c = m.cq_coords[q];
-            out_g[c] = g;
-            if (kEval) out_d[c] = d;
-        }
-    }
-}
 __device__ __forceinline__ bool long_run(const MechBuffers& m, uint32_t q) { return m.cq_off[q + 1] - m.cq_off[q] > kLongList; }
 
 __device__ __forceinline__ void closure_products(const MechBuffers& m, const MechParams& p, const float* x) {
@@ -953,10 +947,7 @@ __global__ void __launch_bounds__(kClosureThreads) k_closure_loop(StepBuffers b,
         loop_sync<kGrid>(m.grid_barrier, flags);
         const bool unconverged = ld_relaxed_u32(&st[0]) > 10u || ld_relaxed_u32(&st[1]) > 1000u;
         if (unconverged) ++steps;
-        if (evaluate && p.long_coords) {   // long runs first, one warp each
-            gather_long_runs<true>(m, p, m.grad, m.diag);
-            loop_sync<kGrid>(m.grid_barrier, flags);
-        }
+        if (evaluate && p.long_coords) gather_long_runs<kGrid, true>(m, p, m.grad, m.diag, flags);   // long runs first
         // gather per coordinate in the serial accumulation order, then the PCG's
         // initial vectors (solve_closure_pcg, closure.wgsl:333-427), chunk by chunk
         for (uint32_t c = blockIdx.x; c < chunks; c += gridDim.x) {
@@ -993,10 +984,7 @@ __global__ void __launch_bounds__(kClosureThreads) k_closure_loop(StepBuffers b,
                 // (closure.wgsl:194-266), from the step's stored columns
                 closure_products(m, p, dir);
                 loop_sync<kGrid>(m.grid_barrier, flags);
-                if (p.long_coords) {
-                    gather_long_runs<false>(m, p, op, nullptr);
-                    loop_sync<kGrid>(m.grid_barrier, flags);
-                }
+                if (p.long_coords) gather_long_runs<kGrid, false>(m, p, op, nullptr, flags);
                 for (uint32_t c = blockIdx.x; c < chunks; c += gridDim.x) {
                     const uint32_t q = c * kDotChunk + threadIdx.x;
                     float dpart = 0.0f;
@@ -1127,7 +1115,7 @@ __device__ void closure_apply(const MechBuffers& m, const MechParams& p, const f
     const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x, nt = gridDim.x * blockDim.x;
     closure_products(m, p, x);
     loop_sync<kGrid>(m.grid_barrier, flags);
-    gather_long_runs<false>(m, p, out, nullptr);
+    if (p.long_coords) gather_long_runs<kGrid, false>(m, p, out, nullptr, flags);
     for (uint32_t q = tid; q < p.closure_coords; q += nt) {
         if (long_run(m, q)) continue;
         float o = 0.0f;
@@ -1216,10 +1204,7 @@ __global__ void __launch_bounds__(kClosureThreads) k_closure_eval(StepBuffers b,
         }
     }
     loop_sync<kGrid>(m.grid_barrier, flags);
-    if (p.long_coords) {
-        gather_long_runs<true>(m, p, m.grad, m.diag);
-        loop_sync<kGrid>(m.grid_barrier, flags);
-    }
+    if (p.long_coords) gather_long_runs<kGrid, true>(m, p, m.grad, m.diag, flags);
     for (uint32_t q = tid; q < NQ; q += nt) {
         const uint32_t c = m.cq_coords[q];
         if (!long_run(m, q)) {

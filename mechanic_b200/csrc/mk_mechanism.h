@@ -24,6 +24,7 @@ struct MechParams {
     uint32_t closures = 0;           // closure bearings
     uint32_t slots = 0;              // joints on closure branches, over all closures
     uint32_t long_coords = 0;        // closure coordinates with more than kLongList slots
+    uint32_t long_chunks = 0;        // chunks of at most kLongList slots over those coordinates' runs
     uint32_t closure_coords = 0;     // distinct coordinates on closure branches
     uint32_t closure_bodies = 0;     // bodies of components that contain a closure
     // MK_CLOSURE_PCG_RESIDUAL
@@ -73,6 +74,10 @@ struct MechBuffers {
     float* slot_d = nullptr;                    // slot's position in cq_slots (each coordinate's run contiguous)
     uint32_t* slot_pos = nullptr;               // position of each slot in cq_slots
     uint32_t* long_q = nullptr;                 // closure coordinates (positions) with long slot lists
+    uint32_t* long_chunk_off = nullptr;         // long_coords + 1: each long coordinate's first chunk
+    uint32_t* chunk_long = nullptr;             // per chunk: its long coordinate (index into long_q)
+    float* chunk_g = nullptr;                   // per chunk: its partial sums
+    float* chunk_d = nullptr;
     float* grad = nullptr;                      // Q (closure.wgsl:46-49 accumulators)
     float* diag = nullptr;                      // Q
     float* pcg = nullptr;                       // 5 x Q: sol, res, pre, dir, op (closure.wgsl:51-60)
@@ -104,7 +109,7 @@ MechParams make_mech_params(const MkCreation* cr, const StepParams& p, uint32_t 
 struct MechTopology {
     std::vector<uint32_t> level_bodies, level_offsets;
     std::vector<uint32_t> cl_bearings, cl_slot_off, cl_split, slot_body, cq_coords, cq_off, cq_slots, cb_bodies;
-    std::vector<uint32_t> slot_closure, slot_pos, long_q;
+    std::vector<uint32_t> slot_closure, slot_pos, long_q, long_chunk_off, chunk_long;
     std::vector<uint32_t> loop_off, loop_q;
 };
 MechTopology derive_topology(const MkCreation* cr, MechParams& p);

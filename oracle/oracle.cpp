@@ -1338,7 +1338,12 @@ template <class T> struct World : WorldBase {
         ax_a = normalize(quat_rotate(pa.rot, xyz(br.xa)));
         ax_b = normalize(quat_rotate(pb.rot, xyz(br.xb)));
     }
-    void accumulate_branch(uint32_t start, V3<T> ea, V3<T> ex, V3<T> rp, V3<T> ra, T sign) {   // closure.wgsl:128-192
+    // Reference-loop slot values, kept only when a coordinate's run is long enough for
+    // the GPU's two-level sum (gather_run): rec_g/rec_d per slot (NaN: no contribution).
+    bool rec_long = false;
+    std::vector<T> rec_g, rec_d;
+    void accumulate_branch(uint32_t start, V3<T> ea, V3<T> ex, V3<T> rp, V3<T> ra, T sign,
+                           uint32_t* slot = nullptr) {   // closure.wgsl:128-192
         uint32_t body = start;
         for (uint32_t guard = 0; guard <= B; ++guard) {
             if (mech[body].meta[3] != 0) break;
@@ -1350,16 +1355,38 @@ template <class T> struct World : WorldBase {
                 V3<T> ad = cross(axis, ex) * sign;
                 T g = dot(rp, pd) + T(1) * dot(ra, ad);
                 T d = dot(pd, pd) + T(1) * dot(ad, ad);
-                if (g == g && d == d) { grad[c] += g; dgl[c] += d; }
+                if (g == g && d == d) {
+                    grad[c] += g; dgl[c] += d;
+                    if (slot) { rec_g[*slot] = g; rec_d[*slot] = d; }
+                }
                 else diag.error_flags |= MK_INVALID_NUMERIC_FLAG;
             }
+            if (slot) ++*slot;
             body = parent;
         }
     }
+    // After the serial accumulation: the long runs summed in the GPU's two levels instead.
+    void regather_long(std::vector<T>& out_g, std::vector<T>* out_d) const {
+        for (size_t q = 0; q + 1 < ct.cq_off.size(); ++q) {
+            if (ct.cq_off[q + 1] - ct.cq_off[q] <= kLongList) continue;
+            T g, d;
+            if (out_d) gather_run<true>((uint32_t)q, rec_g, rec_d, g, d);
+            else gather_run<false>((uint32_t)q, rec_g, rec_g, g, d);
+            out_g[ct.cq_coords[q]] = g;
+            if (out_d) (*out_d)[ct.cq_coords[q]] = d;
+        }
+    }
     void evaluate_closures() {   // closure.wgsl:268-319 (sequential in bearing order)
+        if (rec_long) {
+            rec_g.assign(ct.slot_body.size(), std::numeric_limits<T>::quiet_NaN());
+            rec_d.assign(ct.slot_body.size(), T(0));
+        }
+        uint32_t k = 0;
         for (uint32_t j = 0; j < J; ++j) {
             const Bearing<T>& br = bear[j];
             if (br.meta[3] == 0) continue;
+            uint32_t slot = rec_long ? ct.cl_slot_off[k] : 0u;
+            ++k;
             V3<T> aa, ab, xa, xb;
             closure_frames(br, aa, ab, xa, xb);
             V3<T> rp = aa - ab, ra = xa - xb;
@@ -1383,9 +1410,10 @@ template <class T> struct World : WorldBase {
             closure_state[0] = std::max(closure_state[0], um);
             closure_state[1] = std::max(closure_state[1], ud);
             if (um <= 10u && ud <= 1000u) continue;
-            accumulate_branch(br.meta[0], aa, xa, rp, ra, T(1));
-            accumulate_branch(br.meta[1], ab, xb, rp, ra, T(-1));
+            accumulate_branch(br.meta[0], aa, xa, rp, ra, T(1), rec_long ? &slot : nullptr);
+            accumulate_branch(br.meta[1], ab, xb, rp, ra, T(-1), rec_long ? &slot : nullptr);
         }
+        if (rec_long) regather_long(grad, &dgl);
     }
     Vec2 branch_product(uint32_t start, V3<T> ea, V3<T> ex, T sign) const {   // closure.wgsl:194-230
         Vec2 prod{v3<T>(0, 0, 0), v3<T>(0, 0, 0)};
@@ -1401,7 +1429,8 @@ template <class T> struct World : WorldBase {
         }
         return prod;
     }
-    void branch_transpose(uint32_t start, V3<T> ea, V3<T> ex, const Vec2& prod, T sign) {   // closure.wgsl:232-266
+    void branch_transpose(uint32_t start, V3<T> ea, V3<T> ex, const Vec2& prod, T sign,
+                          uint32_t* slot = nullptr) {   // closure.wgsl:232-266
         uint32_t body = start;
         for (uint32_t guard = 0; guard <= B; ++guard) {
             if (mech[body].meta[3] != 0) break;
@@ -1409,7 +1438,9 @@ template <class T> struct World : WorldBase {
             joint_frame(body, axis, anchor, c, parent);
             V3<T> pd = sign * cross(axis, ea - anchor);
             V3<T> ad = sign * cross(axis, ex);
-            pcg[c].op += dot(pd, prod.p) + T(1) * dot(ad, prod.a);
+            const T v = dot(pd, prod.p) + T(1) * dot(ad, prod.a);
+            pcg[c].op += v;
+            if (slot) rec_g[(*slot)++] = v;
             body = parent;
         }
     }
@@ -1426,6 +1457,7 @@ template <class T> struct World : WorldBase {
         if (chunked) rz = closure_dot_chunked([&](uint32_t c) { return pcg[c].res * pcg[c].pre; });
         for (uint32_t it = 0; it < closure_pcg_rounds; ++it) {
             for (uint32_t c = 0; c < Q; ++c) pcg[c].op = T(0);
+            uint32_t slot = 0;
             for (uint32_t j = 0; j < J; ++j) {
                 const Bearing<T>& br = bear[j];
                 if (br.meta[3] == 0) continue;
@@ -1434,8 +1466,14 @@ template <class T> struct World : WorldBase {
                 Vec2 pa = branch_product(br.meta[0], aa, xa, T(1));
                 Vec2 pb = branch_product(br.meta[1], ab, xb, T(-1));
                 Vec2 prod{pa.p + pb.p, pa.a + pb.a};
-                branch_transpose(br.meta[0], aa, xa, prod, T(1));
-                branch_transpose(br.meta[1], ab, xb, prod, T(-1));
+                branch_transpose(br.meta[0], aa, xa, prod, T(1), rec_long ? &slot : nullptr);
+                branch_transpose(br.meta[1], ab, xb, prod, T(-1), rec_long ? &slot : nullptr);
+            }
+            if (rec_long) {
+                std::vector<T> op_long(Q, T(0));
+                regather_long(op_long, nullptr);
+                for (size_t q = 0; q + 1 < ct.cq_off.size(); ++q)
+                    if (ct.cq_off[q + 1] - ct.cq_off[q] > kLongList) pcg[ct.cq_coords[q]].op = op_long[ct.cq_coords[q]];
             }
             T dop = T(0);
             for (uint32_t c = 0; c < Q; ++c) dop += pcg[c].dir * pcg[c].op;
@@ -1463,6 +1501,7 @@ template <class T> struct World : WorldBase {
     }
     void closure_loop() {   // device.rs:973-1020
         build_closure_topology();
+        rec_long = has_long_runs();
         bool converged_prev = false;
         for (uint32_t step = 0; step < 12; ++step) {
             std::fill(grad.begin(), grad.end(), T(0));
@@ -1603,6 +1642,42 @@ template <class T> struct World : WorldBase {
         }
         return acc;
     }
+    // The GPU's summation order of a closure coordinate's slot values: its run
+    // serially when it has at most kLongList slots, else each chunk of kLongList
+    // consecutive slots serially, then the chunk sums serially in chunk order.
+    // kEval: a NaN gradient marks a slot without contribution (diagonal beside it).
+    static constexpr uint32_t kLongList = 256;
+    template <bool kEval>
+    void gather_run(uint32_t q, const std::vector<T>& vg, const std::vector<T>& vd, T& g, T& d) const {
+        const uint32_t i0 = ct.cq_off[q], i1 = ct.cq_off[q + 1];
+        auto part = [&](uint32_t a, uint32_t b, T& pg, T& pd) {
+            pg = T(0);
+            pd = T(0);
+            for (uint32_t i = a; i < b; ++i) {
+                const uint32_t sl = ct.cq_slots[i];
+                const T sg = vg[sl];
+                if (kEval) {
+                    if (sg == sg) { pg += sg; pd += vd[sl]; }
+                } else {
+                    pg += sg;
+                }
+            }
+        };
+        if (i1 - i0 <= kLongList) { part(i0, i1, g, d); return; }
+        g = T(0);
+        d = T(0);
+        for (uint32_t a = i0; a < i1; a += kLongList) {
+            T pg, pd;
+            part(a, std::min(a + kLongList, i1), pg, pd);
+            g += pg;
+            if (kEval) d += pd;
+        }
+    }
+    bool has_long_runs() const {
+        for (size_t q = 0; q + 1 < ct.cq_off.size(); ++q)
+            if (ct.cq_off[q + 1] - ct.cq_off[q] > kLongList) return true;
+        return false;
+    }
     void closure_apply(const std::vector<T>& x, std::vector<T>& out) {
         const uint32_t NC = (uint32_t)ct.cl_bearings.size();
         for (uint32_t k = 0; k < NC; ++k) {
@@ -1618,8 +1693,8 @@ template <class T> struct World : WorldBase {
             for (uint32_t sl = s0; sl < s1; ++sl) slot_g[sl] = dot(slot_pd[sl], P) + T(1) * dot(slot_ad[sl], A);
         }
         for (size_t q = 0; q < ct.cq_coords.size(); ++q) {
-            T o = T(0);
-            for (uint32_t i = ct.cq_off[q]; i < ct.cq_off[q + 1]; ++i) o += slot_g[ct.cq_slots[i]];
+            T o, unused;
+            gather_run<false>((uint32_t)q, slot_g, slot_g, o, unused);
             out[ct.cq_coords[q]] = o;
         }
     }
@@ -1691,11 +1766,8 @@ template <class T> struct World : WorldBase {
             }
         }
         for (uint32_t q = 0; q < NQ; ++q) {
-            T g = T(0), d = T(0);
-            for (uint32_t i = ct.cq_off[q]; i < ct.cq_off[q + 1]; ++i) {
-                const uint32_t sl = ct.cq_slots[i];
-                if (slot_g[sl] == slot_g[sl]) { g += slot_g[sl]; d += slot_d[sl]; }
-            }
+            T g, d;
+            gather_run<true>(q, slot_g, slot_d, g, d);
             grad[ct.cq_coords[q]] = g;
             dgl[ct.cq_coords[q]] = d;
         }
