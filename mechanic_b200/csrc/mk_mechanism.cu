@@ -182,7 +182,6 @@ void carve_mechanism(MechBuffers& m, const MechParams& p, uint32_t B, uint32_t J
     m.links_b = reinterpret_cast<GpuLinkState*>(take(sizeof(GpuLinkState) * (uint64_t)B));
     m.deltas = reinterpret_cast<int32_t*>(take(24ull * B));
     m.level_bodies = u32(B);
-    m.level_offsets_dev = u32(p.max_depth + 2);
     m.cl_bearings = u32(p.closures);
     m.cl_slot_off = u32(p.closures + 1);
     m.cl_split = u32(p.closures);
@@ -256,7 +255,6 @@ bool upload_mechanism(MechBuffers& m, const MechParams& p, const MechTopology& t
         if (e == cudaSuccess) e = put(m.drives, d, s);
     }
     if (e == cudaSuccess) e = put(m.level_bodies, t.level_bodies, s);
-    if (e == cudaSuccess && !t.level_offsets.empty()) e = put(m.level_offsets_dev, t.level_offsets, s);
     if (e == cudaSuccess) e = put(m.cl_bearings, t.cl_bearings, s);
     if (e == cudaSuccess) e = put(m.cl_slot_off, t.cl_slot_off, s);
     if (e == cudaSuccess) e = put(m.cl_split, t.cl_split, s);
@@ -609,7 +607,11 @@ __global__ void __launch_bounds__(kMBlock) k_publish(StepBuffers b, MechBuffers 
 }
 
 // articulated.wgsl:431-456 for the bodies of one depth level.
-__device__ __forceinline__ void reconstruct_body(const StepBuffers& b, const MechBuffers& m, uint32_t body) {
+__global__ void __launch_bounds__(kMBlock) k_reconstruct_level(StepBuffers b, MechBuffers m, uint32_t begin,
+                                                               uint32_t end) {
+    const uint32_t t = begin + blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= end) return;
+    const uint32_t body = m.level_bodies[t];
     const GpuMechanismBody mb = m.bodies[body];
     const uint32_t parent = mb.metadata[0];
     const GpuBearing& br = m.bearings[mb.metadata[1]];
@@ -628,27 +630,6 @@ __device__ __forceinline__ void reconstruct_body(const StepBuffers& b, const Mec
     const f3 av = xyz(b.lin[parent]) + cross(wp, pa);
     b.lin[body] = f4(av - cross(angular, ca), 0.0f);
     b.ang[body] = f4(angular, 0.0f);
-}
-
-__global__ void __launch_bounds__(kMBlock) k_reconstruct_level(StepBuffers b, MechBuffers m, uint32_t begin,
-                                                               uint32_t end) {
-    const uint32_t t = begin + blockIdx.x * blockDim.x + threadIdx.x;
-    if (t < end) reconstruct_body(b, m, m.level_bodies[t]);
-}
-
-// A run of small consecutive levels [l0, l1) in one block: a level's bodies read
-// their parents' velocities, written by the block's previous level before the
-// __syncthreads between them.  Deep trees with a few hundred bodies per level
-// (the loop lattice: 207 levels) take one launch instead of one per level.
-constexpr uint32_t kLevelBlock = 1024;
-constexpr uint32_t kSmallLevel = 2 * kLevelBlock;   // bodies of a level taken by the one-block form
-__global__ void __launch_bounds__(kLevelBlock) k_reconstruct_levels(StepBuffers b, MechBuffers m, uint32_t l0,
-                                                                    uint32_t l1) {
-    for (uint32_t l = l0; l < l1; ++l) {
-        const uint32_t begin = m.level_offsets_dev[l], end = m.level_offsets_dev[l + 1];
-        for (uint32_t t = begin + threadIdx.x; t < end; t += blockDim.x) reconstruct_body(b, m, m.level_bodies[t]);
-        __syncthreads();
-    }
 }
 
 // articulated.wgsl:458-484
@@ -1587,19 +1568,9 @@ static cudaError_t forward_kinematics(MechBuffers& m, const MechParams& p, cudaS
 }
 
 static cudaError_t reconstruct(MechBuffers& m, const StepBuffers& b, cudaStream_t s) {
-    uint32_t l = 1;
-    while (l < m.level_count) {
-        // a run of at least two small levels: one block walks them
-        uint32_t r = l;
-        while (r < m.level_count && m.level_offsets[r + 1] - m.level_offsets[r] <= kSmallLevel) ++r;
-        if (r - l >= 2) {
-            k_reconstruct_levels<<<1, kLevelBlock, 0, s>>>(b, m, l, r);
-            l = r;
-            continue;
-        }
+    for (uint32_t l = 1; l < m.level_count; ++l) {
         const uint32_t begin = m.level_offsets[l], end = m.level_offsets[l + 1];
         if (end > begin) k_reconstruct_level<<<nblocks(end - begin), kMBlock, 0, s>>>(b, m, begin, end);
-        ++l;
     }
     return cudaGetLastError();
 }

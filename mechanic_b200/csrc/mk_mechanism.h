@@ -60,7 +60,6 @@ struct MechBuffers {
     // reconstruct_body_velocities by depth level (level l: bodies [off[l], off[l+1]))
     uint32_t* level_bodies = nullptr;
     const uint32_t* level_offsets = nullptr;    // host memory owned by the handle, level_count + 1 entries
-    uint32_t* level_offsets_dev = nullptr;      // the same offsets in device memory
     uint32_t level_count = 0;
     // closure loop
     uint32_t* cl_bearings = nullptr;            // closure bearing rows
