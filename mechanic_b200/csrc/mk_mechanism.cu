@@ -35,6 +35,7 @@ constexpr uint32_t kClosureThreads = 1024;
 constexpr uint32_t kClosureSteps = 12;     // device.rs:974
 constexpr uint32_t kClosureRounds = 8;     // closure.wgsl:356
 constexpr uint32_t kMaxLoop = 8;           // coordinates of one per-loop preconditioner block
+constexpr uint32_t kBearingCache = 9;     // float4 per bearing in the projection cache
 constexpr uint32_t kLongList = 256;        // slot runs longer than this are summed in chunks of this many
 
 // ----------------------------------------------------------------- host side
@@ -130,6 +131,7 @@ MechTopology derive_topology(const MkCreation* cr, MechParams& p) {
         t.long_chunk_off.push_back((uint32_t)t.chunk_long.size());
     }
     p.long_coords = (uint32_t)t.long_q.size();
+    p.wide_closures = (!t.cl_bearings.empty() && t.slot_body.size() >= 32ull * t.cl_bearings.size()) ? 1u : 0u;
     p.long_chunks = (uint32_t)t.chunk_long.size();
     t.slot_closure.resize(t.slot_body.size());
     for (size_t k = 0; k + 1 < t.cl_slot_off.size(); ++k)
@@ -181,6 +183,7 @@ void carve_mechanism(MechBuffers& m, const MechParams& p, uint32_t B, uint32_t J
     m.links_a = reinterpret_cast<GpuLinkState*>(take(sizeof(GpuLinkState) * (uint64_t)B));
     m.links_b = reinterpret_cast<GpuLinkState*>(take(sizeof(GpuLinkState) * (uint64_t)B));
     m.deltas = reinterpret_cast<int32_t*>(take(24ull * B));
+    m.bear_cache = reinterpret_cast<float4*>(take(16ull * kBearingCache * (J ? J : 1)));
     m.level_bodies = u32(B);
     m.cl_bearings = u32(p.closures);
     m.cl_slot_off = u32(p.closures + 1);
@@ -341,11 +344,51 @@ __device__ __forceinline__ void hinge_tangents(const StepBuffers& b, uint32_t a,
     tb = cross(hinge, ta);
 }
 
+// The parts of a bearing's five rows that depend on the poses only: they stay
+// fixed over a set of projection passes (the poses change at the forward
+// kinematics, not between passes), so they are computed once per set, with the
+// same expressions as the rows would compute them.  9 float4 per bearing:
+// {arm_a, 1/m_a} {arm_b, 1/m_b} {den0, den1, den2, -} {t_a, den3} {t_b, den4}
+// {I_a t_a} {I_b t_a} {I_a t_b} {I_b t_b}: arms of the three linear rows (world
+// axes), hinge tangents of the two angular rows, world inverse inertia products
+// and the rows' denominators.
+__global__ void __launch_bounds__(kMBlock) k_bearing_cache(StepBuffers b, MechBuffers m, MechParams p) {
+    const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= p.bearing_count) return;
+    const GpuBearing br = m.bearings[j];
+    const uint32_t a = br.metadata[0], c = br.metadata[1];
+    const f3 arm_a = quat_rotate(b.rot[a], r3(br.local_anchor_a)), arm_b = quat_rotate(b.rot[c], r3(br.local_anchor_b));
+    const float ima = inv_mass(b, a), imb = inv_mass(b, c);
+    float den[5];
+#pragma unroll
+    for (uint32_t row = 0; row < 3; ++row) {
+        const f3 d = row == 0 ? mkf3(1, 0, 0) : row == 1 ? mkf3(0, 1, 0) : mkf3(0, 0, 1);
+        const f3 ang_a = cross(arm_a, d), ang_b = cross(arm_b, d);
+        den[row] = ima + imb + dot(ang_a, wii(b, a, ang_a)) + dot(ang_b, wii(b, c, ang_b));
+    }
+    f3 ta, tb;
+    hinge_tangents(b, a, c, br, ta, tb);
+    const f3 ia3 = wii(b, a, ta), ib3 = wii(b, c, ta), ia4 = wii(b, a, tb), ib4 = wii(b, c, tb);
+    den[3] = dot(ta, ia3 + ib3);
+    den[4] = dot(tb, ia4 + ib4);
+    float4* o = m.bear_cache + (uint64_t)kBearingCache * j;
+    o[0] = f4(arm_a, ima);
+    o[1] = f4(arm_b, imb);
+    o[2] = make_float4(den[0], den[1], den[2], 0.0f);
+    o[3] = f4(ta, den[3]);
+    o[4] = f4(tb, den[4]);
+    o[5] = f4(ia3, 0.0f);
+    o[6] = f4(ib3, 0.0f);
+    o[7] = f4(ia4, 0.0f);
+    o[8] = f4(ib4, 0.0f);
+}
+
 // articulated.wgsl:114-155, 287-316
 // One bearing per group of kRowLanes lanes, one row per lane (three linear,
 // two angular); the rows' fixed-point deltas are summed over the group by
 // shuffles (integer sums: the same totals in any order) and one lane flushes
-// them.  Every row reads the velocities of before the pass (Jacobi).
+// them.  Every row reads the velocities of before the pass (Jacobi); the
+// pose-only parts come from the set's bearing cache.
 constexpr uint32_t kRowLanes = 8;
 __global__ void __launch_bounds__(kMBlock) k_project_bearings(StepBuffers b, MechBuffers m, MechParams p) {
     const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
@@ -354,30 +397,30 @@ __global__ void __launch_bounds__(kMBlock) k_project_bearings(StepBuffers b, Mec
     MDelta da{}, dc{};
     uint32_t a = 0, c = 0;
     if (live) {
-        const GpuBearing br = m.bearings[j];
-        a = br.metadata[0];
-        c = br.metadata[1];
+        const uint4 meta = *reinterpret_cast<const uint4*>(m.bearings[j].metadata);
+        a = meta.x;
+        c = meta.y;
+        const float4* cache = m.bear_cache + (uint64_t)kBearingCache * j;
         if (row < 3) {
-            const f3 arm_a = quat_rotate(b.rot[a], r3(br.local_anchor_a)), arm_b = quat_rotate(b.rot[c], r3(br.local_anchor_b));
+            const float4 ca = __ldg(cache), cb = __ldg(cache + 1), cd = __ldg(cache + 2);
+            const f3 arm_a = xyz(ca), arm_b = xyz(cb);
             const f3 va = xyz(b.lin[a]) + cross(xyz(b.ang[a]), arm_a);
             const f3 vb = xyz(b.lin[c]) + cross(xyz(b.ang[c]), arm_b);
             const f3 rel = vb - va;
-            const float ima = inv_mass(b, a), imb = inv_mass(b, c);
+            const float ima = ca.w, imb = cb.w;
             const f3 d = row == 0 ? mkf3(1, 0, 0) : row == 1 ? mkf3(0, 1, 0) : mkf3(0, 0, 1);
-            const f3 ang_a = cross(arm_a, d), ang_b = cross(arm_b, d);
-            const float den = ima + imb + dot(ang_a, wii(b, a, ang_a)) + dot(ang_b, wii(b, c, ang_b));
+            const float den = row == 0 ? cd.x : row == 1 ? cd.y : cd.z;
             if (!(den <= 1.0e-12f)) {
                 const f3 imp = d * (0.5f * dot(rel, d) / den);
                 mdelta_add(da, imp * ima, wii(b, a, cross(arm_a, imp)));
                 mdelta_add(dc, -imp * imb, wii(b, c, cross(arm_b, -imp)));
             }
         } else if (row < 5) {
-            f3 ta, tb;
-            hinge_tangents(b, a, c, br, ta, tb);
+            const float4 ax = __ldg(cache + row);   // {t_a, den3} or {t_b, den4}
+            const f3 ia = xyz(__ldg(cache + (row == 3 ? 5 : 7))), ib = xyz(__ldg(cache + (row == 3 ? 6 : 8)));
             const f3 rang = xyz(b.ang[c]) - xyz(b.ang[a]);
-            const f3 axis = row == 3 ? ta : tb;
-            const f3 ia = wii(b, a, axis), ib = wii(b, c, axis);
-            const float den = dot(axis, ia + ib);
+            const f3 axis = xyz(ax);
+            const float den = ax.w;
             if (!(den <= 1.0e-12f)) {
                 const float imp = 0.5f * dot(rang, axis) / den;
                 mdelta_add(da, mkf3(0, 0, 0), ia * imp);
@@ -866,6 +909,70 @@ __device__ __forceinline__ bool finite3(f3 v) {
 // spreads closures, coordinate chunks and bodies over a cooperative grid with
 // grid barriers in place of the block syncs (thousands of closures).  Both
 // compute the same values.
+// evaluate_closures (closure.wgsl:268-319) for closure k: its residual against the
+// tolerance (lane 0 of the walkers records the step's maxima), then the slots
+// first + i * step of its branches: the joint's Jacobian column and the slot's
+// gradient and diagonal contributions (NaN: none).  With step 32 a warp walks
+// one closure; every slot's arithmetic is the same whoever computes it.
+__device__ __forceinline__ void evaluate_closure(const MechBuffers& m, uint32_t k, uint32_t* st, uint32_t* flags,
+                                                 uint32_t Q, uint32_t first, uint32_t step) {
+    const GpuBearing br = m.bearings[m.cl_bearings[k]];
+    f3 aa, ab, xa, xb;
+    closure_frames(m, br, aa, ab, xa, xb);
+    const f3 rp = aa - ab, ra = xa - xb;
+    const uint32_t s0 = m.cl_slot_off[k], s1 = m.cl_slot_off[k + 1], split = m.cl_split[k];
+    bool active = true;
+    if (!finite3(rp) || !finite3(ra)) {
+        if (first == 0) {
+            atomicOr(flags, MK_INVALID_NUMERIC_FLAG);
+            atomicMax(&st[0], 0xffffffffu);
+            atomicMax(&st[1], 0xffffffffu);
+        }
+        active = false;
+    } else {
+        const uint32_t um = round_u32(length(rp) * 1000000.0f);
+        // axis error as atan2(|a x b|, a . b): FP32 acos (closure.wgsl:295) reads 0
+        // below ~3.5e-4 rad, blind to the 1000 micro-degree tolerance
+        const float deg = atan2_cr(length(cross(xa, xb)), clampf(dot(xa, xb), -1.0f, 1.0f)) * 57.295779513f;
+        const uint32_t ud = round_u32(deg * 1000000.0f);
+        if (first == 0) {
+            atomicMax(&st[0], um);
+            atomicMax(&st[1], ud);
+        }
+        active = !(um <= 10u && ud <= 1000u);
+    }
+    for (uint32_t sl = s0 + first; sl < s1; sl += step) {
+        float g = 0.0f, d = 0.0f;
+        uint32_t valid = 0;
+        // the slot's Jacobian column: the links do not move during the
+        // step's PCG rounds, so closure.wgsl:194-266's recomputation in
+        // every round gives these same floats (sign * v == v * sign)
+        const bool side_a = sl < split;
+        const f3 ea = side_a ? aa : ab, ex = side_a ? xa : xb;
+        const float sign = side_a ? 1.0f : -1.0f;
+        f3 axis, anchor;
+        uint32_t coord;
+        joint_frame(m, m.slot_body[sl], axis, anchor, coord);
+        const f3 pd = cross(axis, ea - anchor) * sign;
+        const f3 ad = cross(axis, ex) * sign;
+        m.slot_v[2 * sl] = f4(pd, __uint_as_float(coord < Q ? coord : 0u));
+        m.slot_v[2 * sl + 1] = f4(ad, 0.0f);
+        if (active) {
+            if (coord >= Q) {
+                atomicOr(flags, MK_INVALID_NUMERIC_FLAG);
+            } else {
+                g = dot(rp, pd) + 1.0f * dot(ra, ad);
+                d = dot(pd, pd) + 1.0f * dot(ad, ad);
+                if (g == g && d == d) valid = 1;
+                else atomicOr(flags, MK_INVALID_NUMERIC_FLAG);
+            }
+        }
+        // NaN marks "no contribution" so the gather skips it
+        m.slot_g[m.slot_pos[sl]] = valid ? g : __int_as_float(0x7fffffff);
+        m.slot_d[m.slot_pos[sl]] = valid ? d : 0.0f;
+    }
+}
+
 template <bool kGrid>
 __global__ void __launch_bounds__(kClosureThreads) k_closure_loop(StepBuffers b, MechBuffers m, MechParams p) {
     __shared__ float s_red[33];
@@ -889,59 +996,11 @@ __global__ void __launch_bounds__(kClosureThreads) k_closure_loop(StepBuffers b,
         const bool evaluate = step == 0 || !converged_prev;
         // evaluate_closures (closure.wgsl:268-319): slot contributions
         if (evaluate) {
-            for (uint32_t k = gtid; k < NC; k += gnt) {
-                const GpuBearing br = m.bearings[m.cl_bearings[k]];
-                f3 aa, ab, xa, xb;
-                closure_frames(m, br, aa, ab, xa, xb);
-                const f3 rp = aa - ab, ra = xa - xb;
-                const uint32_t s0 = m.cl_slot_off[k], s1 = m.cl_slot_off[k + 1], split = m.cl_split[k];
-                bool active = true;
-                if (!finite3(rp) || !finite3(ra)) {
-                    atomicOr(flags, MK_INVALID_NUMERIC_FLAG);
-                    atomicMax(&st[0], 0xffffffffu);
-                    atomicMax(&st[1], 0xffffffffu);
-                    active = false;
-                } else {
-                    const uint32_t um = round_u32(length(rp) * 1000000.0f);
-                    // axis error as atan2(|a x b|, a . b): FP32 acos (closure.wgsl:295) reads 0
-                    // below ~3.5e-4 rad, blind to the 1000 micro-degree tolerance
-                    const float deg =
-                        atan2_cr(length(cross(xa, xb)), clampf(dot(xa, xb), -1.0f, 1.0f)) * 57.295779513f;
-                    const uint32_t ud = round_u32(deg * 1000000.0f);
-                    atomicMax(&st[0], um);
-                    atomicMax(&st[1], ud);
-                    active = !(um <= 10u && ud <= 1000u);
-                }
-                for (uint32_t sl = s0; sl < s1; ++sl) {
-                    float g = 0.0f, d = 0.0f;
-                    uint32_t valid = 0;
-                    // the slot's Jacobian column: the links do not move during the
-                    // step's PCG rounds, so closure.wgsl:194-266's recomputation in
-                    // every round gives these same floats (sign * v == v * sign)
-                    const bool side_a = sl < split;
-                    const f3 ea = side_a ? aa : ab, ex = side_a ? xa : xb;
-                    const float sign = side_a ? 1.0f : -1.0f;
-                    f3 axis, anchor;
-                    uint32_t coord;
-                    joint_frame(m, m.slot_body[sl], axis, anchor, coord);
-                    const f3 pd = cross(axis, ea - anchor) * sign;
-                    const f3 ad = cross(axis, ex) * sign;
-                    m.slot_v[2 * sl] = f4(pd, __uint_as_float(coord < Q ? coord : 0u));
-                    m.slot_v[2 * sl + 1] = f4(ad, 0.0f);
-                    if (active) {
-                        if (coord >= Q) {
-                            atomicOr(flags, MK_INVALID_NUMERIC_FLAG);
-                        } else {
-                            g = dot(rp, pd) + 1.0f * dot(ra, ad);
-                            d = dot(pd, pd) + 1.0f * dot(ad, ad);
-                            if (g == g && d == d) valid = 1;
-                            else atomicOr(flags, MK_INVALID_NUMERIC_FLAG);
-                        }
-                    }
-                    // NaN marks "no contribution" so the gather skips it
-                    m.slot_g[m.slot_pos[sl]] = valid ? g : __int_as_float(0x7fffffff);
-                    m.slot_d[m.slot_pos[sl]] = valid ? d : 0.0f;
-                }
+            if (p.wide_closures) {   // a warp per closure, its slots spread over the lanes
+                const uint32_t lane = threadIdx.x & 31u;
+                for (uint32_t k = gtid >> 5; k < NC; k += gnt >> 5) evaluate_closure(m, k, st, flags, Q, lane, 32u);
+            } else {
+                for (uint32_t k = gtid; k < NC; k += gnt) evaluate_closure(m, k, st, flags, Q, 0u, 1u);
             }
         }
         loop_sync<kGrid>(m.grid_barrier, flags);
@@ -1548,6 +1607,12 @@ __global__ void __launch_bounds__(kClosureThreads) k_closure_pcg(StepBuffers b, 
 // --------------------------------------------------------------- launches
 static inline uint32_t nblocks(uint32_t n) { return (n + kMBlock - 1) / kMBlock; }
 
+// The pose-only parts of the bearing rows, before a set of projection passes.
+static cudaError_t bearing_cache(MechBuffers& m, const StepBuffers& b, const MechParams& p, cudaStream_t s) {
+    if (p.bearing_count) k_bearing_cache<<<nblocks(p.bearing_count), kMBlock, 0, s>>>(b, m, p);
+    return cudaGetLastError();
+}
+
 static cudaError_t bearing_projection_iteration(MechBuffers& m, const StepBuffers& b, const MechParams& p,
                                                 cudaStream_t s) {
     // a group of kRowLanes lanes per bearing, in 64-thread blocks (8 bearings each)
@@ -1629,6 +1694,7 @@ void mechanism_tick_clears(const MechBuffers& m, const MechParams& p, void** ptr
 // device.rs:963-1048
 cudaError_t enqueue_mechanism(MechBuffers& m, const StepBuffers& b, const MechParams& p, cudaStream_t s) {
     cudaError_t e;
+    if ((e = bearing_cache(m, b, p, s)) != cudaSuccess) return e;
     for (uint32_t it = 0; it < std::max(1u, p.iterations); ++it)
         if ((e = bearing_projection_iteration(m, b, p, s)) != cudaSuccess) return e;
     k_advance_coordinates<<<nblocks(p.body_count), kMBlock, 0, s>>>(b, m, p);
@@ -1661,7 +1727,10 @@ cudaError_t enqueue_mechanism(MechBuffers& m, const StepBuffers& b, const MechPa
         }
     }
     k_publish<<<nblocks(p.body_count), kMBlock, 0, s>>>(b, m, p);
-    return reconstruct(m, b, s);
+    if ((e = reconstruct(m, b, s)) != cudaSuccess) return e;
+    // the published poses hold for the rest of the tick: the projection passes
+    // during and after the contact solve share one cache
+    return bearing_cache(m, b, p, s);
 }
 
 // device.rs:1343-1416 with a dynamic mechanism root

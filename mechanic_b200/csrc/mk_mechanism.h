@@ -25,6 +25,7 @@ struct MechParams {
     uint32_t slots = 0;              // joints on closure branches, over all closures
     uint32_t long_coords = 0;        // closure coordinates with more than kLongList slots
     uint32_t long_chunks = 0;        // chunks of at most kLongList slots over those coordinates' runs
+    uint32_t wide_closures = 0;      // closures average 32 slots or more: a warp walks each
     uint32_t closure_coords = 0;     // distinct coordinates on closure branches
     uint32_t closure_bodies = 0;     // bodies of components that contain a closure
     // MK_CLOSURE_PCG_RESIDUAL
@@ -58,6 +59,7 @@ struct MechBuffers {
     GpuLinkState* links_final = nullptr;        // alias of a or b
     int32_t* deltas = nullptr;                  // 6 per body (bearing projection)
     // reconstruct_body_velocities by depth level (level l: bodies [off[l], off[l+1]))
+    float4* bear_cache = nullptr;               // 9 float4 per bearing: pose-only parts of its projection rows
     uint32_t* level_bodies = nullptr;
     const uint32_t* level_offsets = nullptr;    // host memory owned by the handle, level_count + 1 entries
     uint32_t level_count = 0;
