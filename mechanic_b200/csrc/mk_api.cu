@@ -1562,7 +1562,13 @@ int mk_read_buffer(MkHandle* h, uint32_t id, void* host, uint64_t cap_bytes, uin
         case MK_BUF_WARM_PREDICTIONS: src = b.warm_pred; n = b.warm_pred ? counts.active : 0; row = 4; break;
         case MK_BUF_WARM_FEATURES: src = b.warm_features; n = b.warm_features ? counts.active : 0; row = 64; break;
         case MK_BUF_CLOSURE_SLOTS: src = h->mech.slot_v; n = h->mech.slot_v ? h->mech_params.slots : 0; row = 32; break;
-        case MK_BUF_CLOSURE_BLOCKS: src = h->mech.blk_feat; n = h->mech.blk_feat ? h->mech_params.blocks : 0; row = 64; break;
+        case MK_BUF_CLOSURE_BLOCKS:   // computed for the 2 x 2 block preconditioners only
+            src = h->mech.blk_feat;
+            n = (h->mech.blk_feat && (h->mech_params.precond == MK_PRECOND_LEARNED ||
+                                      h->mech_params.precond == MK_PRECOND_PAIR_BLOCKS))
+                    ? h->mech_params.blocks : 0;
+            row = 64;
+            break;
         case MK_BUF_CLOSURE_BLOCK_OUTPUTS:
             src = h->mech.blk_hist;
             n = h->mech.blk_hist ? 12ull * h->mech_params.blocks : 0;

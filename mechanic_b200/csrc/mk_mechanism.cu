@@ -1281,12 +1281,14 @@ __global__ void __launch_bounds__(kClosureThreads) k_closure_eval(StepBuffers b,
     }
     loop_sync<kGrid>(m.grid_barrier, flags);
     const bool unconverged = ld_relaxed_u32(&s_state[0]) > 10u || ld_relaxed_u32(&s_state[1]) > 1000u;
+    // the 2 x 2 blocks and the network's inputs, for the preconditioners that use them
+    const bool pair_blocks = p.precond == MK_PRECOND_LEARNED || p.precond == MK_PRECOND_PAIR_BLOCKS;
     // A * ones and A * alternating signs (block inputs of the network)
-    closure_apply<kGrid>(m, p, m.pcg, m.probe, flags);
-    closure_apply<kGrid>(m, p, m.pcg + Q, m.probe + Q, flags);
+    if (pair_blocks) closure_apply<kGrid>(m, p, m.pcg, m.probe, flags);
+    if (pair_blocks) closure_apply<kGrid>(m, p, m.pcg + Q, m.probe + Q, flags);
     // block entries (a, b, d) and the plain 2 x 2 inverse
     float* blk_b = m.pcg + 2ull * Q;   // coupling of each block (free until the solve)
-    for (uint32_t blk = tid; blk < p.blocks; blk += nt) {
+    for (uint32_t blk = tid; pair_blocks && blk < p.blocks; blk += nt) {
         const uint32_t qi = 2 * blk, qj = qi + 1;
         const bool pair = qj < NQ;
         const float a = m.diag[m.cq_coords[qi]], d = pair ? m.diag[m.cq_coords[qj]] : 0.0f;
@@ -1299,11 +1301,11 @@ __global__ void __launch_bounds__(kClosureThreads) k_closure_eval(StepBuffers b,
         m.blk_m[blk] = inv;
         blk_b[blk] = bij;
     }
-    loop_sync<kGrid>(m.grid_barrier, flags);
+    if (pair_blocks) loop_sync<kGrid>(m.grid_barrier, flags);
     // network inputs: the diagonal-normalised entries of J^T J around the block,
     // with the partner block (blk ^ 1) and the couplings to it recovered from
     // the two probes (exact when the loop's coordinates are these two blocks)
-    for (uint32_t blk = tid; blk < p.blocks; blk += nt) {
+    for (uint32_t blk = tid; pair_blocks && blk < p.blocks; blk += nt) {
         float4 f[4] = {make_float4(0, 0, 0, 0), make_float4(0, 0, 0, 0), make_float4(0, 0, 0, 0),
                        make_float4(0, 0, 0, 1.0f)};
         const uint32_t qi = 2 * blk, qj = qi + 1;

@@ -141,7 +141,8 @@ def output_targets(blocks: np.ndarray) -> np.ndarray:
 
 def collect_closure_samples(scene, ticks: int, config: GpuPhysicsConfig | None = None, params=None):
     """(inputs (n, 16), targets (n, 3), PCG iterations per tick) from `ticks` ticks."""
-    cfg = config or closure_config(learned=params is not None)
+    cfg = config or closure_config(learned=params is not None,
+                                   preconditioner=None if params is not None else abi.PRECOND_PAIR_BLOCKS)
     xs, ts, its = [], [], []
     with GpuPhysics(scene, cfg) as gpu:
         if params is not None:

@@ -1772,15 +1772,17 @@ template <class T> struct World : WorldBase {
             dgl[ct.cq_coords[q]] = d;
         }
         const bool unconverged = closure_state[0] > 10u || closure_state[1] > 1000u;
+        // the 2 x 2 blocks and the network's inputs, for the preconditioners that use them
+        const bool pair_blocks = this->precond == MK_PRECOND_LEARNED || this->precond == MK_PRECOND_PAIR_BLOCKS;
         std::vector<T> ones(Q, T(0)), alt(Q, T(0));
         for (uint32_t q = 0; q < NQ; ++q) { ones[ct.cq_coords[q]] = T(1); alt[ct.cq_coords[q]] = (q & 1u) ? T(-1) : T(1); }
         probe1.assign(Q, T(0)); probe2.assign(Q, T(0));
-        closure_apply(ones, probe1);
-        closure_apply(alt, probe2);
+        if (pair_blocks) closure_apply(ones, probe1);
+        if (pair_blocks) closure_apply(alt, probe2);
         blk_m.assign(NBK, Blk{T(0), T(0), T(0)});
-        blk_feat.assign(16ull * NBK, 0.0f);
+        blk_feat.assign(pair_blocks ? 16ull * NBK : 0ull, 0.0f);
         std::vector<T> blk_b(NBK, T(0));
-        for (uint32_t blk = 0; blk < NBK; ++blk) {
+        for (uint32_t blk = 0; pair_blocks && blk < NBK; ++blk) {
             const uint32_t qi = 2 * blk, qj = qi + 1;
             const bool pair = qj < NQ;
             const T a = dgl[ct.cq_coords[qi]], d = pair ? dgl[ct.cq_coords[qj]] : T(0);
@@ -1793,7 +1795,7 @@ template <class T> struct World : WorldBase {
             blk_m[blk] = inv;
             blk_b[blk] = bij;
         }
-        for (uint32_t blk = 0; blk < NBK; ++blk) {
+        for (uint32_t blk = 0; pair_blocks && blk < NBK; ++blk) {
             float* f = &blk_feat[16ull * blk];
             f[15] = 1.0f;
             const uint32_t qi = 2 * blk, qj = qi + 1;
