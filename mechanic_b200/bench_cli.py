@@ -130,10 +130,12 @@ def main(argv=None):
     ap.add_argument("--ticks", type=int, help="measured ticks (overrides --seconds)")
     ap.add_argument("--warmup-ticks", type=int, help="warm-up ticks (overrides --warmup)")
     ap.add_argument("--pair-capacity", type=int, default=1 << 24)
+    ap.add_argument("--exit-zero", action="store_true",
+                    help="exit 0 whatever the gate says (runs under a profiler, whose replays break the budget)")
     a = ap.parse_args(argv)
     out = run(a.scenario, a.seconds, a.warmup, a.ticks, a.warmup_ticks, a.pair_capacity)
     print(json.dumps(out), flush=True)
-    return 0 if out["gate_passed"] else 1
+    return 0 if out["gate_passed"] or a.exit_zero else 1
 
 
 if __name__ == "__main__":

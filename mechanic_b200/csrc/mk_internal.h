@@ -164,9 +164,11 @@ struct StepBuffers {
     uint32_t* active;            // pair_capacity
     // gather form of the contact solve (heavy ticks: more active contacts than 2 x bodies)
     int32_t* contact_deltas;     // 12 per active contact: fixed-point deltas of body a, then of body b
+                                 // (split form: 8 per slot of body b, the slots grouped by body)
     uint32_t* inc_count;         // per body: contacts touching it (then a countdown while listing them)
-    uint32_t* inc_off;           // body_count + 1: each body's first entry in inc_list
+    uint32_t* inc_off;           // body_count + 1: each body's first entry in inc_list (split form: its first slot)
     uint32_t* inc_list;          // 2 x pair_capacity: 2 t + side of every active contact t, grouped by body
+                                 // (split form: the slot position of each active contact t)
     uint32_t* inc_blocks;        // per block of the cooperative solve: its bodies' entry total
     float* lam_heavy;            // split form: running normal impulse per active contact
     uint32_t heavy_form;         // heavy ticks: MK_HEAVY_SCATTER, MK_HEAVY_GATHER or MK_HEAVY_SPLIT

@@ -386,6 +386,24 @@ def test_grid_above_one_sort_tile_bitexact(cuda_lib):
         compare_tick(gpu, orc, tick)
 
 
+@pytest.mark.parametrize("form", [1, 2, 3])
+def test_heavy_tick_solve_forms_bitexact(cuda_lib, form):
+    """The three forms of the heavy-tick solve (more active contacts than twice the bodies):
+    per-contact atomics (1); per-contact slots summed per body through an incidence list (2);
+    body a by run sums and atomics, body b by slots grouped per body (3, the default)."""
+    from mechanic_b200 import physics
+    prev = physics.set_tuning(physics.TUNE_HEAVY_SOLVE, form)
+    try:
+        scene = scenes.stack_grid(12, 8, 12, seed=3)
+        gpu, orc = make_pair(scene)
+        compare_tick(gpu, orc, 1)
+        assert gpu.read_last_tick().active_contact_count > 2 * scene.body_count
+        compare_tick(gpu, orc, 2)
+        gpu.close()
+    finally:
+        physics.set_tuning(physics.TUNE_HEAVY_SOLVE, max(prev, 0))
+
+
 def test_standalone_sat_matches_oracle(cuda_lib):
     import torch
     from mechanic_b200 import ops
