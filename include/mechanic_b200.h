@@ -509,7 +509,8 @@ MK_API uint32_t mk_tick_kernel_count(const MkHandle* handle);
 
 /* Process-wide tuning knobs read when a tick is captured (mk_create) or an
  * operation is launched.  Keys: MK_TUNE_SORT_ITEMS (keys per thread of a
- * radix-sort tile: 2, 4, 6, 8, 11 or 16; 0 = size-based default);
+ * radix-sort tile: 2, 4, 6, 8, 11 or 16, or 32 for the 8,192-key tile of 512
+ * threads x 16 keys; 0 = size-based default);
  * MK_TUNE_CLOSURE_GRID (the closure solves, the reference's loop and the PCG
  * to a residual: 0 = by size, one block below 512 closures and the whole grid
  * from there, 1 = always one block, 2 = always the grid; both give the same
@@ -525,14 +526,20 @@ MK_API uint32_t mk_tick_kernel_count(const MkHandle* handle);
  * by it) by warp-summed atomics, body b through slots and incidence lists.
  * Same bits in every form. */
 #define MK_TUNE_HEAVY_SOLVE 3u
+/* Tile of the pair-key sort (keys per thread, as MK_TUNE_SORT_ITEMS; 0 = the
+ * default), fixed when a tick is captured: the pair count is known on the
+ * device only. */
+#define MK_TUNE_PAIR_SORT_ITEMS 4u
 MK_API int mk_set_tuning(uint32_t key, uint32_t value);
 
 /* Launch shapes of one handle's tick (no reference counterpart).  0 in any
  * field means the built-in default (for solve_items: every block). */
 typedef struct MkTuning {
     uint32_t sort_items;          /* keys per thread of the collider sort's 256-thread onesweep tile: 2, 4, 6,
-                                     8, 11 or 16 (default by size: 8 up to 64k keys, 11 up to 2M, else 16) */
-    uint32_t sort_ctas_per_sm;    /* onesweep CTAs per SM (default 2 for 11 or 16 keys, 3 for 8, else 6) */
+                                     8, 11 or 16, or 32 for 512 threads x 16 (default by size: 8 up to 64k keys,
+                                     11 up to 2M, else 16) */
+    uint32_t sort_ctas_per_sm;    /* onesweep CTAs per SM (default 1 for the 8,192-key tile, 2 for 11 or 16
+                                     keys, 3 for 8, else 6) */
     uint32_t append_ctas_per_sm;  /* CTAs per SM of the ordered-append kernels (default 8) */
     uint32_t solve_items;         /* 0 (default): every SM's block joins the cooperative solve; n > 0: only
                                      enough blocks for n contacts (and 4n bodies) per thread */

@@ -883,6 +883,11 @@ int mk_set_tuning(uint32_t key, uint32_t value) {
         mk::set_heavy_solve_form(value);
         return (int)prev;
     }
+    if (key == MK_TUNE_PAIR_SORT_ITEMS) {
+        const uint32_t prev = mk::pair_sort_items();
+        mk::set_pair_sort_items(value);
+        return (int)prev;
+    }
     return -1;
 }
 

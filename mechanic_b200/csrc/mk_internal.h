@@ -110,8 +110,11 @@ bool valid_sort_items(uint32_t items);              // 2, 4, 6, 8, 11 or 16 keys
 cudaError_t sort_prepare();   // per-device kernel attributes; call outside stream capture
 // Default CTAs per SM of each onesweep shape, and the fixed shape of the pair-key
 // sort (its count is only known on the device).
-inline uint32_t default_sort_ctas(uint32_t items) { return items >= 11 ? 2u : items == 8 ? 3u : 6u; }
-constexpr uint32_t kPairSortItems = 8;
+inline uint32_t default_sort_ctas(uint32_t items) {
+    return items == 32 ? 1u : items >= 11 ? 2u : items == 8 ? 3u : 6u;
+}
+uint32_t pair_sort_items();                  // keys per thread of the pair-key sort's tile (MK_TUNE_PAIR_SORT_ITEMS)
+void set_pair_sort_items(uint32_t items);    // 0 = the default
 uint64_t sort_scratch_bytes(uint32_t n, uint32_t key_bits, bool values = true);
 cudaError_t launch_sort(const uint64_t* keys_in, const uint32_t* vals_in, uint64_t* keys_out, uint32_t* vals_out,
                         uint32_t n, const uint32_t* n_dev, uint32_t key_bits, void* scratch,
@@ -164,11 +167,9 @@ struct StepBuffers {
     uint32_t* active;            // pair_capacity
     // gather form of the contact solve (heavy ticks: more active contacts than 2 x bodies)
     int32_t* contact_deltas;     // 12 per active contact: fixed-point deltas of body a, then of body b
-                                 // (split form: 8 per slot of body b, the slots grouped by body)
     uint32_t* inc_count;         // per body: contacts touching it (then a countdown while listing them)
-    uint32_t* inc_off;           // body_count + 1: each body's first entry in inc_list (split form: its first slot)
+    uint32_t* inc_off;           // body_count + 1: each body's first entry in inc_list
     uint32_t* inc_list;          // 2 x pair_capacity: 2 t + side of every active contact t, grouped by body
-                                 // (split form: the slot position of each active contact t)
     uint32_t* inc_blocks;        // per block of the cooperative solve: its bodies' entry total
     float* lam_heavy;            // split form: running normal impulse per active contact
     uint32_t heavy_form;         // heavy ticks: MK_HEAVY_SCATTER, MK_HEAVY_GATHER or MK_HEAVY_SPLIT

@@ -348,11 +348,24 @@ uint32_t sort_passes(uint32_t key_bits) { return (key_bits + 7) / 8; }
 // thread (15.5 at 4); 400k 12.9 us at 11 or 16 (17.1 at 8); 1.6M 29.5 us at
 // 11; 6.4M 82 us at 16.  set_sort_items overrides the default (a tuning
 // parameter).
+// 32 names the 8,192-key tile of 512 threads x 16 keys (the same keys per 256
+// threads as 32 keys each): half the tiles of the 4,096-key shape, so the
+// look-back frontier, which advances a window of tiles per L2 round trip,
+// covers twice the keys per round trip.
 static uint32_t g_sort_items_override = 0;
 bool valid_sort_items(uint32_t items) {
-    return items == 2 || items == 4 || items == 6 || items == 8 || items == 11 || items == 16;
+    return items == 2 || items == 4 || items == 6 || items == 8 || items == 11 || items == 16 || items == 32;
 }
 void set_sort_items(uint32_t items) { g_sort_items_override = items; }
+
+// The pair-key sort's tile is fixed when the tick is captured (its key count
+// is only known on the device).  The 8,192-key tile: on the 100,000-body
+// start (14.0M pairs) the five passes take 0.32 ms less than with 2,048-key
+// tiles, and ticks with 8k-40k pairs about 20 us more each (one B200).
+static uint32_t g_pair_sort_items = 0;
+constexpr uint32_t kPairSortItemsDefault = 32;
+uint32_t pair_sort_items() { return valid_sort_items(g_pair_sort_items) ? g_pair_sort_items : kPairSortItemsDefault; }
+void set_pair_sort_items(uint32_t items) { g_pair_sort_items = valid_sort_items(items) ? items : 0u; }
 uint32_t sort_items_for(uint32_t n, int sm_count) {
     if (valid_sort_items(g_sort_items_override)) return g_sort_items_override;
     (void)sm_count;
@@ -382,11 +395,11 @@ uint64_t sort_scratch_bytes(uint32_t n, uint32_t key_bits, bool values) {
     return b;
 }
 
-template <uint32_t kItems>
+template <uint32_t kThreads, uint32_t kItems>
 static void launch_pass(const uint64_t* sk, const uint32_t* sv, uint64_t* dk, uint32_t* dv, const uint32_t* n_dev,
                         uint32_t n, uint32_t shift, const uint32_t* offsets, uint32_t* lookback, uint32_t* ticket,
                         uint32_t* error_flags, uint32_t grid, uint32_t small_n, cudaStream_t stream) {
-    k_radix_onesweep<kSortThreads, kItems><<<grid, kSortThreads, SortTile<kSortThreads, kItems>::kBytes, stream>>>(
+    k_radix_onesweep<kThreads, kItems><<<grid, kThreads, SortTile<kThreads, kItems>::kBytes, stream>>>(
         sk, sv, dk, dv, n_dev, n, shift, offsets, lookback, ticket, error_flags, small_n);
 }
 
@@ -399,16 +412,17 @@ cudaError_t sort_prepare() {
     if (e != cudaSuccess) return e;
     const uint64_t bit = 1ull << (dev & 63);
     if (done.load() & bit) return cudaSuccess;
-#define MK_SORT_ATTR(I)                                                                                       \
+#define MK_SORT_ATTR(T, I)                                                                                    \
     if (e == cudaSuccess)                                                                                    \
-        e = cudaFuncSetAttribute(k_radix_onesweep<kSortThreads, I>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
-                                 (int)SortTile<kSortThreads, I>::kBytes);
-    MK_SORT_ATTR(2)
-    MK_SORT_ATTR(4)
-    MK_SORT_ATTR(6)
-    MK_SORT_ATTR(8)
-    MK_SORT_ATTR(11)
-    MK_SORT_ATTR(16)
+        e = cudaFuncSetAttribute(k_radix_onesweep<T, I>, cudaFuncAttributeMaxDynamicSharedMemorySize,            \
+                                 (int)SortTile<T, I>::kBytes);
+    MK_SORT_ATTR(kSortThreads, 2)
+    MK_SORT_ATTR(kSortThreads, 4)
+    MK_SORT_ATTR(kSortThreads, 6)
+    MK_SORT_ATTR(kSortThreads, 8)
+    MK_SORT_ATTR(kSortThreads, 11)
+    MK_SORT_ATTR(kSortThreads, 16)
+    MK_SORT_ATTR(2 * kSortThreads, 16)
 #undef MK_SORT_ATTR
     if (e == cudaSuccess)
         e = cudaFuncSetAttribute(k_radix_small, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmallSmem);
@@ -467,16 +481,17 @@ cudaError_t launch_sort(const uint64_t* keys_in, const uint32_t* vals_in, uint64
         uint32_t* dv = values ? (to_out ? vals_out : tmp_vals) : nullptr;
         uint32_t* lb = lookback + (size_t)pass * tiles_max * kRadixBins;
         const uint32_t* offs = hist + pass * kRadixBins;
-#define MK_SORT_PASS(I)                                                                                          \
-    launch_pass<I>(src_k, src_v, dk, dv, n_dev, n, 8 * pass, offs, lb, tickets + pass, error_flags, grid, small_n, \
-                   stream)
+#define MK_SORT_PASS(T, I)                                                                                       \
+    launch_pass<T, I>(src_k, src_v, dk, dv, n_dev, n, 8 * pass, offs, lb, tickets + pass, error_flags, grid, small_n, \
+                      stream)
         switch (items) {
-            case 2: MK_SORT_PASS(2); break;
-            case 4: MK_SORT_PASS(4); break;
-            case 6: MK_SORT_PASS(6); break;
-            case 8: MK_SORT_PASS(8); break;
-            case 11: MK_SORT_PASS(11); break;
-            default: MK_SORT_PASS(16); break;
+            case 2: MK_SORT_PASS(kSortThreads, 2); break;
+            case 4: MK_SORT_PASS(kSortThreads, 4); break;
+            case 6: MK_SORT_PASS(kSortThreads, 6); break;
+            case 8: MK_SORT_PASS(kSortThreads, 8); break;
+            case 11: MK_SORT_PASS(kSortThreads, 11); break;
+            case 32: MK_SORT_PASS(2 * kSortThreads, 16); break;
+            default: MK_SORT_PASS(kSortThreads, 16); break;
         }
 #undef MK_SORT_PASS
         src_k = dk;

@@ -1746,19 +1746,17 @@ __device__ void solve_gather(const StepBuffers& b, const StepParams& p, GpuConta
 // body a's deltas take warp-aggregated atomics over runs (one per run and
 // component, as in the scatter form), while body b's -- one atomic per
 // contact and component in the scatter form, spread over many bodies and
-// serialised per body -- go to a 32-byte slot.  The slots are grouped by
-// body b (each contact's slot position is listed once per solve), so the
-// projection's writes scatter and the apply reads each body's slots as one
-// contiguous run.  The running normal impulses live in a dense array during
-// the solve (the rows are read-only until the last pass writes them back).
-// Same integer sums, same bits.
+// serialised per body -- go to the contact's own 24-byte slot and each body
+// sums its slots through an incidence list in the apply.  The running normal
+// impulses live in a dense array during the solve (the rows are read-only
+// until the last pass writes them back).  Same integer sums, same bits.
 __device__ void solve_split(const StepBuffers& b, const StepParams& p, GpuContact* cur, uint32_t A,
                             uint32_t iterations, uint32_t* barrier, uint32_t parts) {
     __shared__ uint32_t s_scan[33];
     uint32_t* flags = &b.diag->error_flags;
     const uint32_t B = p.body_count;
     const uint32_t gtid = blockIdx.x * blockDim.x + threadIdx.x, stride = parts * blockDim.x;
-    // ---- body b's slots: counts, offsets, and each contact's slot position
+    // ---- incidence lists of body b: counts, offsets, fill (active positions t)
     for (uint32_t i = gtid; i < B; i += stride) b.inc_count[i] = 0u;
     grid_barrier(barrier, flags, parts);
     for (uint32_t t = gtid; t < A; t += stride) {
@@ -1768,11 +1766,10 @@ __device__ void solve_split(const StepBuffers& b, const StepParams& p, GpuContac
     grid_barrier(barrier, flags, parts);
     gather_scan(b, B, parts, barrier, flags, s_scan);
     grid_barrier(barrier, flags, parts);
-    uint32_t* slot_of = b.inc_list;   // per active contact: its slot, or kInvalid without a body b
     for (uint32_t t = gtid; t < A; t += stride) {
         const uint2 ab = active_bodies(b, cur, t);
-        slot_of[t] = ab.y != kInvalid ? __ldcg(b.inc_off + ab.y) + atomicSub(b.inc_count + ab.y, 1u) - 1u
-                                      : kInvalid;
+        if (ab.y != kInvalid)
+            b.inc_list[__ldcg(b.inc_off + ab.y) + atomicSub(b.inc_count + ab.y, 1u) - 1u] = t;
     }
     grid_barrier(barrier, flags, parts);
     const size_t Bs = B;
@@ -1780,7 +1777,7 @@ __device__ void solve_split(const StepBuffers& b, const StepParams& p, GpuContac
     const uint32_t lane = lane_id();
     const uint32_t gwarp = gtid >> 5, nwarps = stride >> 5;
     const uint2 sl = contact_slice(A, parts);
-    int4* slots = reinterpret_cast<int4*>(b.contact_deltas);   // 2 x int4 per slot (6 deltas, 2 unused)
+    int2* slots = reinterpret_cast<int2*>(b.contact_deltas);   // 3 x int2 per active contact
     for (uint32_t it = 0; it < iterations; ++it) {
         const float4* vl = it == 0 ? b.lin : b.vel_iter + (2 * (it - 1)) * Bs;
         const float4* va = it == 0 ? b.ang : b.vel_iter + (2 * (it - 1) + 1) * Bs;
@@ -1819,9 +1816,10 @@ __device__ void solve_split(const StepBuffers& b, const StepParams& p, GpuContac
                 }
                 b.lam_heavy[t] = acc;
                 if (bb != kInvalid) {
-                    int4* q = slots + 2ull * __ldcg(slot_of + t);
-                    q[0] = make_int4(db[0], db[1], db[2], db[3]);
-                    q[1] = make_int4(db[4], db[5], 0, 0);
+                    int2* q = slots + 3ull * t;
+                    q[0] = make_int2(db[0], db[1]);
+                    q[1] = make_int2(db[2], db[3]);
+                    q[2] = make_int2(db[4], db[5]);
                 }
                 if (it + 1 == iterations && !(den <= 0.0f))
                     reinterpret_cast<float*>(cur + k)[11] = acc;   // the row's impulse (arm_a_impulse.w)
@@ -1830,20 +1828,19 @@ __device__ void solve_split(const StepBuffers& b, const StepParams& p, GpuContac
             add_contact_deltas(b.deltas, live, a, kInvalid, da, db);
         }
         grid_barrier(barrier, flags, parts);
-        // ---- apply: body a's atomic sums plus the body's run of slots (where it is b)
+        // ---- apply: body a's atomic sums plus the slots of the contacts where it is b
         for (uint32_t x = gwarp; x < B; x += nwarps) {
             const uint32_t e0 = __ldcg(b.inc_off + x), e1 = __ldcg(b.inc_off + x + 1);
             int32_t sum[6] = {0, 0, 0, 0, 0, 0};
             for (uint32_t e = e0 + lane; e < e1; e += 32) {
-                const int4* q = slots + 2ull * e;
-                const int4 x0 = __ldcg(q);
-                const int2 x1 = __ldcg(reinterpret_cast<const int2*>(q + 1));
+                const int2* q = slots + 3ull * __ldcg(b.inc_list + e);
+                const int2 x0 = __ldcg(q), x1 = __ldcg(q + 1), x2 = __ldcg(q + 2);
                 sum[0] = (int32_t)((uint32_t)sum[0] + (uint32_t)x0.x);
                 sum[1] = (int32_t)((uint32_t)sum[1] + (uint32_t)x0.y);
-                sum[2] = (int32_t)((uint32_t)sum[2] + (uint32_t)x0.z);
-                sum[3] = (int32_t)((uint32_t)sum[3] + (uint32_t)x0.w);
-                sum[4] = (int32_t)((uint32_t)sum[4] + (uint32_t)x1.x);
-                sum[5] = (int32_t)((uint32_t)sum[5] + (uint32_t)x1.y);
+                sum[2] = (int32_t)((uint32_t)sum[2] + (uint32_t)x1.x);
+                sum[3] = (int32_t)((uint32_t)sum[3] + (uint32_t)x1.y);
+                sum[4] = (int32_t)((uint32_t)sum[4] + (uint32_t)x2.x);
+                sum[5] = (int32_t)((uint32_t)sum[5] + (uint32_t)x2.y);
             }
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1)
@@ -2535,7 +2532,7 @@ cudaError_t launch_broadphase(const StepBuffers& b, const StepParams& p, const S
     else k_traverse<false><<<blocks_for(C, kTravThreads), kTravThreads, 0, s>>>(b, p);
     e = launch_sort(b.pair_stage, nullptr, b.pair_keys, nullptr, p.pair_capacity, &b.counts->pairs_found,
                     2 * p.pair_shift, b.pair_sort_scratch, b.pair_sort_scratch_bytes, &b.diag->error_flags, s,
-                    l.sm_count, kPairSortItems, 0, true);
+                    l.sm_count, pair_sort_items(), 0, true);
     if (e != cudaSuccess) return e;
     return cudaGetLastError();
 }

@@ -530,6 +530,7 @@ class GpuPhysics:
 TUNE_SORT_ITEMS = 1
 TUNE_CLOSURE_GRID = 2   # reference-mode closure loop: 0 by size, 1 one block, 2 the whole grid
 TUNE_HEAVY_SOLVE = 3    # heavy-tick contact solve: 0 default, 1 scatter (atomics), 2 gather (slots), 3 split
+TUNE_PAIR_SORT_ITEMS = 4   # pair-key sort tile (keys per thread as TUNE_SORT_ITEMS; 32 = 512 x 16); 0 default
 
 
 def set_tuning(key: int, value: int) -> int:

@@ -355,7 +355,7 @@ def test_standalone_sort_matches_stable_sort(cuda_lib):
         assert np.array_equal(v_out.cpu().numpy().view(np.uint32), vals[order])
 
 
-@pytest.mark.parametrize("items", [2, 4, 6, 8, 11, 16])
+@pytest.mark.parametrize("items", [2, 4, 6, 8, 11, 16, 32])
 def test_standalone_sort_every_tile_shape(cuda_lib, items):
     """Each onesweep tile shape (keys per thread) gives the stable order."""
     import torch
@@ -386,11 +386,27 @@ def test_grid_above_one_sort_tile_bitexact(cuda_lib):
         compare_tick(gpu, orc, tick)
 
 
+@pytest.mark.parametrize("items", [8, 16, 32])
+def test_pair_sort_tiles_bitexact(cuda_lib, items):
+    """The pair-key sort's tile shapes (2,048, 4,096 and 8,192 keys) give the canonical pair list."""
+    from mechanic_b200 import physics
+    prev = physics.set_tuning(physics.TUNE_PAIR_SORT_ITEMS, items)
+    try:
+        scene = scenes.stack_grid(12, 8, 12, seed=3)
+        gpu, orc = make_pair(scene)
+        compare_tick(gpu, orc, 1)
+        assert gpu.read_last_tick().pair_count > 4 * 8192
+        compare_tick(gpu, orc, 2)
+        gpu.close()
+    finally:
+        physics.set_tuning(physics.TUNE_PAIR_SORT_ITEMS, max(prev, 0))
+
+
 @pytest.mark.parametrize("form", [1, 2, 3])
 def test_heavy_tick_solve_forms_bitexact(cuda_lib, form):
     """The three forms of the heavy-tick solve (more active contacts than twice the bodies):
     per-contact atomics (1); per-contact slots summed per body through an incidence list (2);
-    body a by run sums and atomics, body b by slots grouped per body (3, the default)."""
+    body a by run sums and atomics, body b by per-contact slots summed per body (3, the default)."""
     from mechanic_b200 import physics
     prev = physics.set_tuning(physics.TUNE_HEAVY_SOLVE, form)
     try:
