@@ -1130,24 +1130,21 @@ __global__ void __launch_bounds__(kClosureThreads) k_closure_loop(StepBuffers b,
 // between; a converged step sets `done` and the later launches return.
 
 // Fixed-order FP64 block sum (1024 threads): per-thread partials, warp
-// shuffle-down trees, then warp 0 over the 32 warp sums.
+// shuffle-down trees, then the same shuffle-down tree over the 32 warp sums,
+// which every warp evaluates for itself (identical operands and order, so
+// identical bits) instead of warp 0 publishing it through shared memory: two
+// barriers per sum instead of four.
 __device__ __forceinline__ double block_sum_d(double v, double* scratch) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
     const uint32_t w = threadIdx.x >> 5, lane = threadIdx.x & 31u;
-    __syncthreads();
+    __syncthreads();   // the previous sum's readers are done with scratch
     if (lane == 0) scratch[w] = v;
     __syncthreads();
-    if (w == 0) {
-        double r = lane < (blockDim.x >> 5) ? scratch[lane] : 0.0;
+    double r = lane < (blockDim.x >> 5) ? scratch[lane] : 0.0;
 #pragma unroll
-        for (int o = 16; o > 0; o >>= 1) r += __shfl_down_sync(0xffffffffu, r, o);
-        if (lane == 0) scratch[32] = r;
-    }
-    __syncthreads();
-    const double r = scratch[32];
-    __syncthreads();
-    return r;
+    for (int o = 16; o > 0; o >>= 1) r += __shfl_down_sync(0xffffffffu, r, o);
+    return __shfl_sync(0xffffffffu, r, 0);
 }
 
 // The FP64 dot product after a loop_sync: the chunk sums in chunk order (thread
@@ -1460,6 +1457,11 @@ __global__ void __launch_bounds__(kClosureThreads) k_closure_pcg(StepBuffers b, 
     uint32_t* flags = &b.diag->error_flags;
     double* part_a = m.chunk_part_d;            // chunk sums of the FP64 dot products
     double* part_b = m.chunk_part_d + chunks;
+    // one block over one chunk: a dot product's block sum is its total (the chunk-order
+    // total is 0.0 + the chunk sums), and the sum's barriers order the loop's writes, so
+    // neither the chunk sums in memory nor the sync that publishes them are needed
+    const bool one = !kGrid && chunks == 1;
+    double one_a = 0.0, one_b = 0.0;
     float* sol = m.pcg;
     float* res = m.pcg + Q;
     float* pre = m.pcg + 2ull * Q;
@@ -1521,11 +1523,12 @@ __global__ void __launch_bounds__(kClosureThreads) k_closure_pcg(StepBuffers b, 
             prr = (double)res[cc] * (double)res[cc];
         }
         const double sz = block_sum_d(prz, s_red), sr = block_sum_d(prr, s_red);
-        if (threadIdx.x == 0) { part_a[c] = sz; part_b[c] = sr; }
+        if (one) { one_a = sz; one_b = sr; }
+        else if (threadIdx.x == 0) { part_a[c] = sz; part_b[c] = sr; }
     }
-    loop_sync<kGrid>(m.grid_barrier, flags);
-    double rz = chunk_total_d(part_a, chunks, s_red);
-    const double rr0 = chunk_total_d(part_b, chunks, s_red);
+    if (!one) loop_sync<kGrid>(m.grid_barrier, flags);
+    double rz = one ? 0.0 + one_a : chunk_total_d(part_a, chunks, s_red);
+    const double rr0 = one ? 0.0 + one_b : chunk_total_d(part_b, chunks, s_red);
     double rr = rr0;
     const double tol2 = (double)p.closure_tol * (double)p.closure_tol;
     uint32_t it = 0;
@@ -1539,10 +1542,11 @@ __global__ void __launch_bounds__(kClosureThreads) k_closure_pcg(StepBuffers b, 
                 ppq = (double)dir[cc] * (double)op[cc];
             }
             const double sq = block_sum_d(ppq, s_red);
-            if (threadIdx.x == 0) part_a[c] = sq;
+            if (one) one_a = sq;
+            else if (threadIdx.x == 0) part_a[c] = sq;
         }
-        loop_sync<kGrid>(m.grid_barrier, flags);
-        const double pq = chunk_total_d(part_a, chunks, s_red);
+        if (!one) loop_sync<kGrid>(m.grid_barrier, flags);
+        const double pq = one ? 0.0 + one_a : chunk_total_d(part_a, chunks, s_red);
         const float alpha = fabs(pq) > 1.0e-30 ? (float)(rz / pq) : 0.0f;
         for (uint32_t c = blockIdx.x; c < chunks; c += gridDim.x) {
             const uint32_t q = c * kDotChunk + threadIdx.x;
@@ -1554,10 +1558,11 @@ __global__ void __launch_bounds__(kClosureThreads) k_closure_pcg(StepBuffers b, 
                 pr = (double)res[cc] * (double)res[cc];
             }
             const double sr = block_sum_d(pr, s_red);
-            if (threadIdx.x == 0) part_b[c] = sr;
+            if (one) one_b = sr;
+            else if (threadIdx.x == 0) part_b[c] = sr;
         }
-        loop_sync<kGrid>(m.grid_barrier, flags);
-        rr = chunk_total_d(part_b, chunks, s_red);
+        if (!one) loop_sync<kGrid>(m.grid_barrier, flags);
+        rr = one ? 0.0 + one_b : chunk_total_d(part_b, chunks, s_red);
         ++it;
         if (rr <= tol2 * rr0) break;
         precond_apply<kGrid>(m, p, res, pre, flags);
@@ -1569,10 +1574,11 @@ __global__ void __launch_bounds__(kClosureThreads) k_closure_pcg(StepBuffers b, 
                 pz = (double)res[cc] * (double)pre[cc];
             }
             const double sz = block_sum_d(pz, s_red);
-            if (threadIdx.x == 0) part_a[c] = sz;
+            if (one) one_a = sz;
+            else if (threadIdx.x == 0) part_a[c] = sz;
         }
-        loop_sync<kGrid>(m.grid_barrier, flags);
-        const double nrz = chunk_total_d(part_a, chunks, s_red);
+        if (!one) loop_sync<kGrid>(m.grid_barrier, flags);
+        const double nrz = one ? 0.0 + one_a : chunk_total_d(part_a, chunks, s_red);
         const float beta = fabs(rz) > 1.0e-300 ? (float)(nrz / rz) : 0.0f;
         for (uint32_t q = tid; q < NQ; q += nt) {
             const uint32_t cc = m.cq_coords[q];

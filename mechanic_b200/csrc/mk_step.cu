@@ -1197,14 +1197,26 @@ __device__ __forceinline__ int64_t find_previous(const uint64_t* __restrict__ ke
 
 // collision.wgsl:674-736 with the persistent manifold of the previous tick
 // read from its contact list (acquired rows carry feature bit 24).
+// A tile is `rows` rows of kBlock contacts (contact k of row j is
+// (tile * rows + j) * kBlock + threadIdx.x), with rows = 1..kPrepareItems
+// chosen from the count so that every CTA of the grid still gets a tile: on
+// heavy ticks the ordered append's look-back frontier, which advances 32
+// tiles per L2 round trip, then covers 8 x the contacts per round trip (9.5M
+// contacts are 4,624 tiles, not 36,991), while light ticks keep one row per
+// tile and every contact's lookup in flight at once.
+constexpr uint32_t kPrepareItems = 8;
+constexpr uint32_t kPrepareWarps = kBlock / 32;
 __global__ void __launch_bounds__(kBlock) k_prepare(StepBuffers b, StepParams p, AppendSite site, GpuContact* cur,
                                                     uint64_t* cur_keys, uint32_t* cur_feat, const GpuContact* prev,
                                                     const uint64_t* prev_keys, const uint32_t* prev_feat) {
-    __shared__ uint32_t s_scan[33];
+    __shared__ uint32_t s_rows[kPrepareItems * kPrepareWarps];   // active count of each (row, warp), then its offset
+    __shared__ uint32_t s_total;
     __shared__ uint32_t s_tile;
     __shared__ uint64_t s_prefix;
     const uint32_t n = b.counts->contacts;
-    const uint32_t tiles = (n + kBlock - 1) / kBlock;
+    const uint32_t rows = min(kPrepareItems, max(1u, n / (kBlock * gridDim.x)));
+    const uint32_t tile_contacts = rows * kBlock;
+    const uint32_t tiles = (n + tile_contacts - 1) / tile_contacts;
     const uint32_t tick = b.tick->tick_index;
     const bool prev_ok = b.counts->prev_valid != 0u && b.counts->prev_tick == tick - 1u;
     const uint32_t prev_narrow = b.counts->prev_narrow, prev_all = b.counts->prev_contacts;
@@ -1215,86 +1227,113 @@ __global__ void __launch_bounds__(kBlock) k_prepare(StepBuffers b, StepParams p,
     const bool indexed = prev_ok && b.counts->prev_indexed != 0u;
     const uint32_t narrow_now = b.counts->narrow;
     if (blockIdx.x != 0 && blockIdx.x >= tiles) return;   // as in k_narrowphase
+    const uint32_t lane = lane_id(), w = warp_id();
     for (;;) {
         const uint32_t tile = take_tile(site.ticket, &s_tile);
         if (tile >= tiles) break;
-        const uint32_t k = tile * kBlock + threadIdx.x;
-        bool act = false;
-        if (k < n) {
-            {   // index this tick's list for the next tick's lookups
-                const uint64_t key = cur_keys[k];
-                const uint32_t ca = (uint32_t)(key >> 32);
-                if (k >= narrow_now) index_cur[C + ca] = make_uint2(tick, k);            // one ground row per collider
-                else if (k == 0 || (uint32_t)(cur_keys[k - 1] >> 32) != ca) index_cur[ca] = make_uint2(tick, k);
-            }
-            float4* row = reinterpret_cast<float4*>(cur + k);
-            const float4 r0 = row[0], np = row[1], aa = row[2], ab = row[3];
-            const uint32_t a = __float_as_uint(r0.x), bb = __float_as_uint(r0.y);
-            const f3 arm_a = xyz(aa), arm_b = xyz(ab);
-            float inv_b = 0.0f;
-            f3 vb = mkf3(0, 0, 0);
-            if (bb != kInvalid) {
-                inv_b = b.world_mass[3ull * bb].w;
-                vb = contact_velocity(b, bb, arm_b);
-            }
-            if (!(b.world_mass[3ull * a].w + inv_b <= 0.0f)) {
-                const f3 rel = vb - contact_velocity(b, a, arm_a);
-                const f3 nrm = xyz(np);
-                const float vn = dot(rel, nrm);
-                if (np.w <= 1.0e-6f && vn >= 0.0f) {
-                    row[0] = make_float4(r0.x, r0.y, __uint_as_float(kInvalid), __uint_as_float(0u));
-                } else {
-                    float cached = 0.0f;
-                    if (prev_ok) {
-                        // the previous rows of this collider pair (one, or up to four with a
-                        // clipped manifold): the first acquired row whose normal and arm match
-                        const uint64_t key = cur_keys[k];
-                        const bool ground = (uint32_t)key == kInvalid;
-                        const uint32_t end = ground ? prev_all : prev_narrow;
-                        int64_t m = -1;
-                        if (indexed) {   // the collider's run, then a short scan to the key
-                            const uint32_t ca = (uint32_t)(key >> 32);
-                            const uint2 e = __ldg(index_prev + (ground ? C : 0ull) + ca);
-                            if (e.x == tick - 1u) {
-                                uint32_t r = e.y;
-                                while (r < end && __ldg(prev_keys + r) < key && (uint32_t)(__ldg(prev_keys + r) >> 32) == ca)
-                                    ++r;
-                                if (r < end && __ldg(prev_keys + r) == key) m = r;
+        uint32_t act_rows = 0;   // bit j: this thread's contact of row j is active
+#pragma unroll 1
+        for (uint32_t j = 0; j < rows; ++j) {
+            const uint32_t k = tile * tile_contacts + j * kBlock + threadIdx.x;
+            bool act = false;
+            if (k < n) {
+                {   // index this tick's list for the next tick's lookups
+                    const uint64_t key = cur_keys[k];
+                    const uint32_t ca = (uint32_t)(key >> 32);
+                    if (k >= narrow_now) index_cur[C + ca] = make_uint2(tick, k);            // one ground row per collider
+                    else if (k == 0 || (uint32_t)(cur_keys[k - 1] >> 32) != ca) index_cur[ca] = make_uint2(tick, k);
+                }
+                float4* row = reinterpret_cast<float4*>(cur + k);
+                const float4 r0 = row[0], np = row[1], aa = row[2], ab = row[3];
+                const uint32_t a = __float_as_uint(r0.x), bb = __float_as_uint(r0.y);
+                const f3 arm_a = xyz(aa), arm_b = xyz(ab);
+                float inv_b = 0.0f;
+                f3 vb = mkf3(0, 0, 0);
+                if (bb != kInvalid) {
+                    inv_b = b.world_mass[3ull * bb].w;
+                    vb = contact_velocity(b, bb, arm_b);
+                }
+                if (!(b.world_mass[3ull * a].w + inv_b <= 0.0f)) {
+                    const f3 rel = vb - contact_velocity(b, a, arm_a);
+                    const f3 nrm = xyz(np);
+                    const float vn = dot(rel, nrm);
+                    if (np.w <= 1.0e-6f && vn >= 0.0f) {
+                        row[0] = make_float4(r0.x, r0.y, __uint_as_float(kInvalid), __uint_as_float(0u));
+                    } else {
+                        float cached = 0.0f;
+                        if (prev_ok) {
+                            // the previous rows of this collider pair (one, or up to four with a
+                            // clipped manifold): the first acquired row whose normal and arm match
+                            const uint64_t key = cur_keys[k];
+                            const bool ground = (uint32_t)key == kInvalid;
+                            const uint32_t end = ground ? prev_all : prev_narrow;
+                            int64_t m = -1;
+                            if (indexed) {   // the collider's run, then a short scan to the key
+                                const uint32_t ca = (uint32_t)(key >> 32);
+                                const uint2 e = __ldg(index_prev + (ground ? C : 0ull) + ca);
+                                if (e.x == tick - 1u) {
+                                    uint32_t r = e.y;
+                                    while (r < end && __ldg(prev_keys + r) < key && (uint32_t)(__ldg(prev_keys + r) >> 32) == ca)
+                                        ++r;
+                                    if (r < end && __ldg(prev_keys + r) == key) m = r;
+                                }
+                            } else {
+                                m = ground ? find_previous(prev_keys, prev_narrow, prev_all, key)
+                                           : find_previous(prev_keys, 0u, prev_narrow, key);
                             }
-                        } else {
-                            m = ground ? find_previous(prev_keys, prev_narrow, prev_all, key)
-                                       : find_previous(prev_keys, 0u, prev_narrow, key);
-                        }
-                        for (int64_t r = m; r >= 0 && r < (int64_t)end && __ldg(prev_keys + r) == key; ++r) {
-                            if (!(__ldg(prev_feat + r) & (1u << 24))) continue;
-                            const float4* pr = reinterpret_cast<const float4*>(prev + r);
-                            const float4 pn = __ldg(pr + 1), pa = __ldg(pr + 2);
-                            const bool match = dot(xyz(pn), nrm) >= 0.98f && length(xyz(pa) - arm_a) <= 0.02f;
-                            if (match) {
-                                cached = pa.w;
-                                break;
+                            for (int64_t r = m; r >= 0 && r < (int64_t)end && __ldg(prev_keys + r) == key; ++r) {
+                                if (!(__ldg(prev_feat + r) & (1u << 24))) continue;
+                                const float4* pr = reinterpret_cast<const float4*>(prev + r);
+                                const float4 pn = __ldg(pr + 1), pa = __ldg(pr + 2);
+                                const bool match = dot(xyz(pn), nrm) >= 0.98f && length(xyz(pa) - arm_a) <= 0.02f;
+                                if (match) {
+                                    cached = pa.w;
+                                    break;
+                                }
                             }
                         }
+                        row[0] = make_float4(r0.x, r0.y, __uint_as_float(k), __uint_as_float(1u));
+                        row[2] = f4(arm_a, cached);
+                        cur_feat[k] |= 1u << 24;
+                        act = np.w > 1.0e-5f || vn < -1.0e-5f || cached > 1.0e-6f;
                     }
-                    row[0] = make_float4(r0.x, r0.y, __uint_as_float(k), __uint_as_float(1u));
-                    row[2] = f4(arm_a, cached);
-                    cur_feat[k] |= 1u << 24;
-                    act = np.w > 1.0e-5f || vn < -1.0e-5f || cached > 1.0e-6f;
                 }
             }
+            const uint32_t m = __ballot_sync(0xffffffffu, act);
+            if (act) act_rows |= 1u << j;
+            if (lane == 0) s_rows[j * kPrepareWarps + w] = __popc(m);
         }
-        uint32_t total;
-        const uint32_t ex = block_exclusive_scan(act ? 1u : 0u, s_scan, &total);
-        if (warp_id() == 0) {
-            uint64_t pre = tile_lookback(site.states, tile, total, &b.diag->error_flags);
-            if (lane_id() == 0) s_prefix = pre;
+        __syncthreads();
+        // offsets of the (row, warp) groups in contact order, then the tile's prefix
+        if (w == 0) {
+            uint32_t carry = 0;
+            for (uint32_t e0 = 0; e0 < rows * kPrepareWarps; e0 += 32) {
+                const uint32_t e = e0 + lane;
+                const uint32_t c = e < rows * kPrepareWarps ? s_rows[e] : 0u;
+                const uint32_t inc = warp_inclusive_scan(c);
+                if (e < rows * kPrepareWarps) s_rows[e] = carry + inc - c;
+                carry += __shfl_sync(0xffffffffu, inc, 31);
+            }
+            const uint64_t pre = tile_lookback(site.states, tile, carry, &b.diag->error_flags);
+            if (lane == 0) {
+                s_prefix = pre;
+                s_total = carry;
+            }
         }
         __syncthreads();
         const uint64_t pre = s_prefix;
-        if (act) b.active[pre + ex] = k;
+        const uint32_t below = (1u << lane) - 1u;
+#pragma unroll 1
+        for (uint32_t j = 0; j < rows; ++j) {
+            const bool act = (act_rows >> j) & 1u;
+            const uint32_t m = __ballot_sync(0xffffffffu, act);
+            if (act)
+                b.active[pre + s_rows[j * kPrepareWarps + w] + __popc(m & below)] =
+                    tile * tile_contacts + j * kBlock + threadIdx.x;
+        }
         if (tile == tiles - 1 && threadIdx.x == 0) {
-            b.counts->active = (uint32_t)(pre + total);
-            b.diag->active_contact_count = (uint32_t)(pre + total);
+            b.counts->active = (uint32_t)(pre + s_total);
+            b.diag->active_contact_count = (uint32_t)(pre + s_total);
         }
         __syncthreads();
     }
