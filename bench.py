@@ -624,6 +624,9 @@ def main():
             "roofline": {"bound": "hbm", "kernel": stages[dominant]["kernel"],
                          "achieved": stages[dominant]["achieved"], "peak": peak, "unit": "GB/s",
                          "frac": stages[dominant]["achieved"] / peak, "peak_source": peak_note, "traffic": None,
+                         "traffic_note": "the line is a stage of several kernels; per-kernel ncu DRAM bytes are in "
+                                         "profiles/ (k_solve_all heavy tick: 142 B per contact and pass, against "
+                                         f"{BYTES_SOLVE_PER_CONTACT_ITER} algorithmic: the body rows hit L2)",
                          "algorithmic_bytes_per_step": stages[dominant]["bytes_per_step"],
                          "secondary": {"kernel": stages[other]["kernel"], "achieved": stages[other]["achieved"],
                                        "frac": stages[other]["achieved"] / peak,
