@@ -1199,11 +1199,12 @@ __device__ __forceinline__ int64_t find_previous(const uint64_t* __restrict__ ke
 // read from its contact list (acquired rows carry feature bit 24).
 // A tile is `rows` rows of kBlock contacts (contact k of row j is
 // (tile * rows + j) * kBlock + threadIdx.x), with rows = 1..kPrepareItems
-// chosen from the count so that every CTA of the grid still gets a tile: on
-// heavy ticks the ordered append's look-back frontier, which advances 32
-// tiles per L2 round trip, then covers 8 x the contacts per round trip (9.5M
-// contacts are 4,624 tiles, not 36,991), while light ticks keep one row per
-// tile and every contact's lookup in flight at once.
+// chosen from the count so that every CTA of the grid still gets at least
+// four tiles: on the heaviest ticks the ordered append's look-back frontier,
+// which advances 32 tiles per L2 round trip, then covers up to 8 x the
+// contacts per round trip (9.5M contacts: 7 rows, 5,285 tiles instead of
+// 36,991), while smaller counts keep one row per tile and every contact's
+// lookup in flight at once.
 constexpr uint32_t kPrepareItems = 8;
 constexpr uint32_t kPrepareWarps = kBlock / 32;
 __global__ void __launch_bounds__(kBlock) k_prepare(StepBuffers b, StepParams p, AppendSite site, GpuContact* cur,
@@ -1214,7 +1215,7 @@ __global__ void __launch_bounds__(kBlock) k_prepare(StepBuffers b, StepParams p,
     __shared__ uint32_t s_tile;
     __shared__ uint64_t s_prefix;
     const uint32_t n = b.counts->contacts;
-    const uint32_t rows = min(kPrepareItems, max(1u, n / (kBlock * gridDim.x)));
+    const uint32_t rows = min(kPrepareItems, max(1u, n / (4u * kBlock * gridDim.x)));
     const uint32_t tile_contacts = rows * kBlock;
     const uint32_t tiles = (n + tile_contacts - 1) / tile_contacts;
     const uint32_t tick = b.tick->tick_index;

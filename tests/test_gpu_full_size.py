@@ -164,13 +164,16 @@ def test_chains_4000_full_size_bitexact(cuda_lib, mode):
     gpu.close()
 
 
-def test_chains_4000_fp64_error(cuda_lib):
+@pytest.mark.parametrize("mode", ["reference", "pcg"])
+def test_chains_4000_fp64_error(cuda_lib, mode):
+    """One step of the articulated config against the FP64 oracle, with the reference's closure
+    loop and with block-Jacobi PCG to a 1e-5 residual (the three-way comparison's GPU legs)."""
     scene = scenes.bearing_chains(4000)
-    cfg = GpuPhysicsConfig()
+    cfg = GpuPhysicsConfig() if mode == "reference" else learned.closure_config()
     gpu = GpuPhysics(scene, cfg, capacities={"pair_capacity": 1 << 22})
     for tick in (1, 2, 3):
         gpu.dispatch_tick(tick)
-    tab = _fp64_table("4,000 chains, tick 4", scene, cfg, gpu, 4, 1 << 22)
+    tab = _fp64_table(f"4,000 chains ({mode} closures), tick 4", scene, cfg, gpu, 4, 1 << 22)
     c = tab["counts"]
     assert c["matched"] >= 0.999 * max(c["fp32"], c["fp64"], 1), c
     assert tab["position_m"]["rel_inf"] <= REL_BOUND
