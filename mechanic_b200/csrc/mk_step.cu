@@ -1008,6 +1008,110 @@ __device__ __forceinline__ uint32_t take_tile(uint32_t* ticket, uint32_t* s_tile
     return t;
 }
 
+// Heavy ticks with one contact per pair (the averaged point): tiles of
+// kNarrowRows rows of kBlock pairs.  Each row's contacts are staged in shared
+// memory (normal and depth, point and feature word, bodies and colliders:
+// 48 bytes) and the tile takes one ordered-append offset for all its rows, so
+// the look-back and the tile's barriers are paid once per 512 pairs.  The
+// rows are written in pair order, as with one row per tile.
+constexpr uint32_t kNarrowRows = 2;
+constexpr uint32_t kNarrowWarps = kBlock / 32;
+// Its own kernel, launched after k_narrowphase with the same grid: each leaves
+// at once where the other one takes the tick (one register allocation each;
+// as one kernel the single-row path spilled more and light ticks slowed).
+__device__ __forceinline__ bool narrowphase_takes_rows(const StepParams& p, uint32_t n) {
+    return !p.clipped_manifold && n >= 4u * kNarrowRows * kBlock * gridDim.x;
+}
+__global__ void __launch_bounds__(kBlock, 3) k_narrowphase_rows(StepBuffers b, StepParams p, AppendSite site,
+                                                             GpuContact* out, uint64_t* out_keys, uint32_t* out_feat) {
+    const uint32_t n = min(b.counts->pairs_found, p.pair_capacity);
+    if (!narrowphase_takes_rows(p, n)) return;
+    __shared__ float4 s_np[kNarrowRows * kBlock];
+    __shared__ float4 s_pt[kNarrowRows * kBlock];
+    __shared__ uint4 s_ids[kNarrowRows * kBlock];
+    __shared__ uint32_t s_rows[kNarrowRows * kNarrowWarps];
+    __shared__ uint32_t s_total;
+    __shared__ uint32_t s_tile;
+    __shared__ uint64_t s_prefix;
+    constexpr uint32_t kTile = kNarrowRows * kBlock;
+    const uint32_t tiles = (n + kTile - 1) / kTile;
+    const uint32_t lane = lane_id(), w = warp_id();
+    for (;;) {
+        const uint32_t tile = take_tile(site.ticket, &s_tile);
+        if (tile >= tiles) break;
+        uint32_t emit_rows = 0;
+#pragma unroll 1
+        for (uint32_t j = 0; j < kNarrowRows; ++j) {
+            const uint32_t idx = tile * kTile + j * kBlock + threadIdx.x;
+            bool emit = false;
+            if (idx < n) {
+                const uint64_t key = b.pair_keys[idx];
+                const uint2 pr = make_uint2((uint32_t)(key >> p.pair_shift),
+                                            (uint32_t)(key & ((1ull << p.pair_shift) - 1)));
+                const Box A = make_box(b.boxes, pr.x), Bx = make_box(b.boxes, pr.y);
+                const uint32_t ba = __float_as_uint(__ldg(b.boxes + 3ull * pr.x + 2).z);
+                const uint32_t bb = __float_as_uint(__ldg(b.boxes + 3ull * pr.y + 2).z);
+                const bool skip = b.components && __ldg(b.components + ba) == __ldg(b.components + bb);
+                if (!skip) {
+                    const Sat st = obb_sat(A, Bx);
+                    if (!(st.pen < -1.0e-5f)) {
+                        const f3 pt = contact_point(A, Bx, st.n);
+                        const uint32_t feat = st.axis | (st.near << 8) | (st.early << 16);
+                        const uint32_t slot = j * kBlock + threadIdx.x;
+                        s_np[slot] = f4(st.n, mxf(st.pen, 0.0f));
+                        s_pt[slot] = f4(pt, __uint_as_float(feat));
+                        s_ids[slot] = make_uint4(ba, bb, pr.x, pr.y);
+                        emit = true;
+                    }
+                }
+            }
+            const uint32_t m = __ballot_sync(0xffffffffu, emit);
+            if (emit) emit_rows |= 1u << j;
+            if (lane == 0) s_rows[j * kNarrowWarps + w] = __popc(m);
+        }
+        __syncthreads();
+        // offsets of the (row, warp) groups in pair order, then the tile's prefix
+        if (w == 0) {
+            const uint32_t c = lane < kNarrowRows * kNarrowWarps ? s_rows[lane] : 0u;
+            const uint32_t inc = warp_inclusive_scan(c);
+            if (lane < kNarrowRows * kNarrowWarps) s_rows[lane] = inc - c;
+            const uint32_t total = __shfl_sync(0xffffffffu, inc, 31);
+            const uint64_t pre = tile_lookback(site.states, tile, total, &b.diag->error_flags);
+            if (lane == 0) {
+                s_prefix = pre;
+                s_total = total;
+            }
+        }
+        __syncthreads();
+        const uint64_t pre = s_prefix;
+        const uint32_t below = (1u << lane) - 1u;
+#pragma unroll 1
+        for (uint32_t j = 0; j < kNarrowRows; ++j) {
+            const bool emit = (emit_rows >> j) & 1u;
+            const uint32_t m = __ballot_sync(0xffffffffu, emit);
+            if (!emit) continue;
+            const uint64_t o = pre + s_rows[j * kNarrowWarps + w] + __popc(m & below);
+            if (o >= p.pair_capacity) continue;
+            const uint32_t slot = j * kBlock + threadIdx.x;
+            const float4 np = s_np[slot], pt4 = s_pt[slot];
+            const uint4 ids = s_ids[slot];
+            const uint32_t feat = __float_as_uint(pt4.w);
+            const f3 pt = xyz(pt4);
+            const f3 xa = xyz(b.pos[ids.x]), xb = xyz(b.pos[ids.y]);
+            store_contact(out + o, ids.x, ids.y, ids.z, ids.w, np, f4(pt - xa, 0.0f),
+                          f4(pt - xb, (float)((feat >> 8) & 0xffu)));
+            out_keys[o] = ((uint64_t)ids.z << 32) | ids.w;
+            out_feat[o] = feat;
+        }
+        if (tile == tiles - 1 && threadIdx.x == 0) {
+            const uint64_t all = pre + s_total;
+            b.counts->narrow = (uint32_t)umin64(all, p.pair_capacity);
+            b.counts->requested_contacts = (uint32_t)umin64(all, 0xffffffffull);
+        }
+        __syncthreads();
+    }
+}
+
 // collision.wgsl:570-620 (narrowphase with the optional self-collision filter).
 __global__ void __launch_bounds__(kBlock, 3) k_narrowphase(StepBuffers b, StepParams p, AppendSite site,
                                                         GpuContact* out, uint64_t* out_keys, uint32_t* out_feat) {
@@ -1026,6 +1130,8 @@ __global__ void __launch_bounds__(kBlock, 3) k_narrowphase(StepBuffers b, StepPa
     // the grid is sized for the capacity: CTAs past the tile count leave
     // before taking a ticket (block 0 stays for the empty-list counts)
     if (blockIdx.x != 0 && blockIdx.x >= tiles) return;
+    // several rows per tile (k_narrowphase_rows) only where every CTA still gets four tiles of them
+    if (narrowphase_takes_rows(p, n)) return;
     for (;;) {
         const uint32_t tile = take_tile(site.ticket, &s_tile);
         if (tile >= tiles) break;
@@ -2582,6 +2688,8 @@ cudaError_t launch_narrowphase(const StepBuffers& b, const StepParams& p, const 
     const uint32_t grid = (uint32_t)l.sm_count * (l.append_ctas ? l.append_ctas : 8u);
     AppendSite narrow{b.lookback + 1 * b.lookback_words, b.tickets + 1};
     k_narrowphase<<<grid, kBlock, 0, s>>>(b, p, narrow, b.contacts[parity], b.contact_keys[parity], b.features[parity]);
+    k_narrowphase_rows<<<grid, kBlock, 0, s>>>(b, p, narrow, b.contacts[parity], b.contact_keys[parity],
+                                               b.features[parity]);
     k_ground<<<std::max<uint32_t>(1u, blocks_for(p.collider_count, kGroundTile)), kBlock, 0, s>>>(
         b, p, b.contacts[parity], b.contact_keys[parity], b.features[parity]);
     return cudaGetLastError();
