@@ -193,8 +193,10 @@ def bench_config(scene, args, world: int = 1) -> dict:
                    f"not flushed: per-tick state {working_set / 1e6:.0f} MB > 126 MB L2")}
 
 
-def cpu_trajectory(scene, ticks: int, budget_s: float, threads: int):
-    """Steps the CPU oracle along ticks 1..ticks, stopping early once budget_s has passed."""
+def cpu_trajectory(scene, ticks: int, budget_s: float, threads: int, keep_world: bool = False):
+    """Steps the CPU oracle along ticks 1..ticks, stopping early once budget_s has passed.
+    With keep_world the oracle world comes back as a fourth item (its state after the
+    last tick stepped), so the same sample also serves as the checker of the GPU run."""
     import oracle
     from mechanic_b200.physics import GpuPhysicsConfig
     oracle.set_threads(threads)
@@ -206,7 +208,52 @@ def cpu_trajectory(scene, ticks: int, budget_s: float, threads: int):
         done += 1
         if time.perf_counter() - t0 > budget_s:
             break
-    return done, time.perf_counter() - t0, oracle.threads()
+    elapsed = time.perf_counter() - t0
+    if keep_world:
+        return done, elapsed, oracle.threads(), w
+    return done, elapsed, oracle.threads()
+
+
+def parity_against_oracle(gpu, scene, reset, done: int, world) -> dict:
+    """Checks the GPU's trajectory with the CPU baseline's own sample: the GPU steps ticks
+    1..done again from the generated state (outside every timed region) and its poses and
+    velocities are compared bit for bit with the FP32 oracle's after the same ticks; then
+    one more tick from that identical state is compared with the FP64 oracle (normwise
+    relative error of each quantity)."""
+    import numpy as np
+    from oracle import errors
+    from mechanic_b200.physics import GpuPhysicsConfig
+    reset()
+    for tick in range(1, done + 1):
+        gpu.dispatch_tick(tick)
+    gpu.wait()
+    cap = 1 << 21   # the manifold of a light tick (tens of thousands of rows)
+    st = gpu.save_state(manifold_capacity=cap)
+    tr, vel = world.state()
+    same_tr = bool(np.array_equal(np.ascontiguousarray(st["transforms"]).view(np.uint8),
+                                  np.ascontiguousarray(tr).view(np.uint8)))
+    same_vel = bool(np.array_equal(np.ascontiguousarray(st["velocities"]).view(np.uint8),
+                                   np.ascontiguousarray(vel).view(np.uint8)))
+    out = {"checker": f"FP32 oracle over ticks 1..{done} (the cpu_baseline sample)", "ticks_bitexact": done,
+           "transforms_bitexact": same_tr, "velocities_bitexact": same_vel, "fp64_one_step": None}
+    if len(st["manifold"]) >= cap:   # a heavy tick's manifold: too large for a one-step FP64 check here
+        return out
+    start = {"transforms": st["transforms"], "velocities": st["velocities"], "coordinates": st["coordinates"],
+             "manifold": st["manifold"], "manifold_tick": st["manifold_tick"]}
+    nxt = done + 1
+    gpu.dispatch_tick(nxt)
+    gpu.wait()
+    after = gpu.save_state(manifold_capacity=0)
+    res = {"transforms": after["transforms"], "velocities": after["velocities"], "contacts": gpu.contacts(),
+           "contact_keys": gpu.contact_keys()}
+    tab = errors.one_step_errors(scene, GpuPhysicsConfig().to_c(), start, nxt, res, pair_capacity=PAIR_CAPACITY)
+    keys = ("position_m", "rotation", "linear_velocity_mps", "angular_velocity_rps", "point_arm_a_m", "depth_m",
+            "normal", "impulse")
+    out["checker"] += f", then the FP64 oracle for tick {nxt} from the identical state"
+    out["fp64_one_step"] = {"tick": nxt, "contacts": tab["counts"],
+                            "rel_inf": {k: tab[k]["rel_inf"] for k in keys},
+                            "max_abs": {k: tab[k]["max_abs"] for k in keys}}
+    return out
 
 
 def cpu_table(budget_s: float = 20.0) -> dict:
@@ -604,11 +651,15 @@ def main():
 
     if rank == 0:
         cpu = None
+        parity = None
         if not args.no_cpu_baseline and world == 1:
-            done, elapsed, used = cpu_trajectory(scene, args.steps, 30.0, os.cpu_count() or 1)
+            done, elapsed, used, oworld = cpu_trajectory(scene, args.steps, 30.0, os.cpu_count() or 1,
+                                                         keep_world=True)
             cpu = {"value": scene.body_count * done / elapsed, "unit": UNIT, "cores": used, "kind": "port",
                    "sample": f"ticks 1..{done} of the same trajectory on the CPU restatement (FP32), {used} threads, "
                              f"{elapsed:.1f} s"}
+            parity = parity_against_oracle(gpu, scene, reset, done, oworld)
+            del oworld
         tick1 = counts[0] if counts else (0, 0, 0)
         out = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -633,6 +684,7 @@ def main():
                                        "algorithmic_bytes_per_step": stages[other]["bytes_per_step"]},
                          "stage_ms_per_step": {k: v / args.steps for k, v in stage_ms.items()}},
             "cpu_baseline": cpu,
+            "parity": parity,
             "clocks": clocks.summary(),
             "gpu_launches": gpu_launches,
             "error_flags": flags,
