@@ -168,6 +168,7 @@ uint64_t carve(MkHandle* h, char* base) {
     b.snap_rot = c.take<float4>(3ull * B);
     b.colliders = c.take<float4>(4ull * C);
     b.boxes = c.take<float4>(3ull * C);
+    b.collider_body = c.take<uint32_t>(C);
     b.aabbs = c.take<float4>(2ull * C);
     b.keys = c.take<uint64_t>(C);
     b.values = c.take<uint32_t>(C);
@@ -810,6 +811,13 @@ int create_impl(const MkCreation* cr, const MkConfig* config, const MkCapacities
     ok = ok && check(upload<uint32_t>(const_cast<uint32_t*>(b.root_flags), roots.data(), h->B, s), err, "upload roots");
     ok = ok && check(upload<float4>(const_cast<float4*>(b.colliders), cr->colliders, 4ull * h->C, s), err,
                      "upload colliders");
+    if (ok && h->C) {   // the traversal's same-body test reads 4 bytes per collider, not a box row
+        std::vector<uint32_t> cbody(h->C);
+        for (uint32_t i = 0; i < h->C; ++i) cbody[i] = cr->colliders[i].metadata[0];
+        ok = check(upload<uint32_t>(const_cast<uint32_t*>(b.collider_body), cbody.data(), h->C, s), err,
+                   "collider bodies");
+        ok = ok && check(cudaStreamSynchronize(s), err, "sync");
+    }
     if (ok && batch && h->scene_count > 1 && h->C) {
         // scene s owns sorted leaf positions [collider_offsets[s], collider_offsets[s + 1]): its
         // colliders' keys carry s in their top bits

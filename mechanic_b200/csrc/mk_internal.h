@@ -138,6 +138,7 @@ struct StepBuffers {
     float4 *snap_pos, *snap_rot; // ring base, slot-major
     const float4* colliders;     // GpuCollider rows (4 x float4)
     float4* boxes;               // 3 x float4 per collider (world box)
+    const uint32_t* collider_body;   // per collider: its body (the collider rows' metadata.x, set at creation)
     float4* aabbs;               // 2 x float4 per collider
     uint64_t* keys;              // per collider
     uint32_t* values;            // identity

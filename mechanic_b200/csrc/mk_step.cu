@@ -744,7 +744,7 @@ __global__ void __launch_bounds__(kTravThreads) k_traverse(StepBuffers b, StepPa
         i = b.svals[t];
         qmin = b.node_aabbs[2ull * (leaf_base + t)];
         qmax = b.node_aabbs[2ull * (leaf_base + t) + 1];
-        body_i = __float_as_uint(b.boxes[3ull * i + 2].z);
+        body_i = __ldg(b.collider_body + i);
         // batched scenes: the walk starts at the scene's own subtree (Karras keeps
         // each scene's leaves under one node: the scene index sits above the
         // Morton bits), so every entry it meets lies inside the scene; a scene of
@@ -779,7 +779,7 @@ __global__ void __launch_bounds__(kTravThreads) k_traverse(StepBuffers b, StepPa
                 const uint32_t code = __float_as_uint(cmin.w);
                 if (code & kLeafCode) {
                     const uint32_t j = code & ~kLeafCode;
-                    const uint32_t body_j = __float_as_uint(__ldg(b.boxes + 3ull * j + 2).z);
+                    const uint32_t body_j = __ldg(b.collider_body + j);
                     if (body_i == body_j) continue;
                     if (p.suppression_count && pair_is_suppressed(b.suppressed, p.suppression_count, body_i, body_j))
                         continue;
