@@ -85,6 +85,9 @@ def parse():
     ap.add_argument("--flush-l2", action="store_true", help="zero a 256 MB buffer between timed ticks")
     ap.add_argument("--full-form", action="store_true",
                     help="measure the 1,250,000-body full form (reference passes, plain and learned to 1e-5) and exit")
+    ap.add_argument("--long-loops", action="store_true",
+                    help="the closure preconditioners on 400 sixteen-body loops (longer than one per-loop block) "
+                         "and exit")
     ap.add_argument("--cpu-table", action="store_true",
                     help="time the CPU restatement on every configuration (all cores and one core) and exit")
     return ap.parse_args()
@@ -360,24 +363,33 @@ def measure_residual_forms(local: int, ticks: int = 60):
     return out
 
 
-def measure_closure_forms(local: int, ticks: int = 20, chains: int = 4000):
-    """The articulated config (4,000 five-body chains, 10% loop-closed): closure PCG to a
-    1e-5 relative residual under each preconditioner -- the reference's diagonal (Jacobi)
-    one, exact 2 x 2 blocks, the network-corrected 2 x 2 blocks (trained here on the GPU on
-    the first ticks' systems) and per-loop block Jacobi.  PCG iterations per tick (12 Newton
-    steps, at most 256 iterations each), the largest relative residual reached, and the
-    device time per tick."""
+def measure_closure_forms(local: int, ticks: int = 20, chains: int = 4000, links: int = 5,
+                          closure_fraction: float = 0.1):
+    """The articulated config (4,000 five-body chains, 10% loop-closed; or other chains):
+    closure PCG to a 1e-5 relative residual under each preconditioner -- the reference's
+    diagonal (Jacobi) one, exact 2 x 2 blocks, the network-corrected 2 x 2 blocks (trained
+    here on the GPU on the first ticks' systems) and per-loop block Jacobi (exact on loops of
+    at most 8 coordinates; longer loops are cut into blocks of 8).  PCG iterations per tick
+    (12 Newton steps, at most 256 iterations each), the largest relative residual reached, and
+    the device time per tick."""
     from mechanic_b200 import abi, learned, scenes
     from mechanic_b200.physics import GpuPhysics
-    scene = scenes.bearing_chains(chains)
+    scene = scenes.bearing_chains(chains, links=links, closure_fraction=closure_fraction)
     xs, ts, _ = learned.collect_closure_samples(scene, 8, learned.closure_config(
         preconditioner=abi.PRECOND_PAIR_BLOCKS, device=local))
-    params, _ = learned.train_preconditioner(xs, ts, steps=2000)
-    out = {"workload": f"{chains} five-body chains, 10% loop-closed, closure PCG until ||r|| <= 1e-5 ||r0|| "
-                       f"(cap 256 per Newton step), ticks 1..{ticks}",
-           "training": f"network trained on {len(xs)} 2 x 2 blocks of ticks 1-8 (pair-block runs)"}
-    for name, pc in (("diagonal (reference Jacobi)", abi.PRECOND_DIAGONAL), ("pair blocks", abi.PRECOND_PAIR_BLOCKS),
-                     ("learned pair blocks", abi.PRECOND_LEARNED), ("block Jacobi (per loop)", abi.PRECOND_BLOCK_JACOBI)):
+    out = {"workload": f"{chains} chains of {links} bodies, {closure_fraction:.0%} loop-closed, closure PCG until "
+                       f"||r|| <= 1e-5 ||r0|| (cap 256 per Newton step), ticks 1..{ticks}"}
+    forms = [("diagonal (reference Jacobi)", abi.PRECOND_DIAGONAL), ("pair blocks", abi.PRECOND_PAIR_BLOCKS)]
+    if len(xs):
+        params, _ = learned.train_preconditioner(xs, ts, steps=2000)
+        out["training"] = f"network trained on {len(xs)} 2 x 2 blocks of ticks 1-8 (pair-block runs)"
+        forms.append(("learned pair blocks", abi.PRECOND_LEARNED))
+    else:   # a loop of more than five coordinates has a singular J^T J: its blocks have no inverse to learn
+        params = None
+        out["training"] = ("no training targets: every loop's J^T J is singular (more coordinates than the rank "
+                           "5 of its closure's rows)")
+    forms.append(("block Jacobi (per loop)", abi.PRECOND_BLOCK_JACOBI))
+    for name, pc in forms:
         with GpuPhysics(scene, learned.closure_config(preconditioner=pc, device=local)) as g:
             if pc == abi.PRECOND_LEARNED:
                 g.set_preconditioner_network(params)
@@ -392,8 +404,9 @@ def measure_closure_forms(local: int, ticks: int = 20, chains: int = 4000):
                      "ticks_at_tolerance": int(sum(r <= 1e-5 for r in res)), "ms_per_tick": ms / ticks}
     d, b = out["diagonal (reference Jacobi)"], out["block Jacobi (per loop)"]
     out["iteration_ratio_diagonal_over_block"] = d["pcg_iterations_per_tick"] / max(b["pcg_iterations_per_tick"], 1e-9)
-    out["iteration_ratio_pair_over_learned"] = (out["pair blocks"]["pcg_iterations_per_tick"] /
-                                                max(out["learned pair blocks"]["pcg_iterations_per_tick"], 1e-9))
+    if "learned pair blocks" in out:
+        out["iteration_ratio_pair_over_learned"] = (out["pair blocks"]["pcg_iterations_per_tick"] /
+                                                    max(out["learned pair blocks"]["pcg_iterations_per_tick"], 1e-9))
     return out
 
 
@@ -513,6 +526,12 @@ def main():
             import torch
             torch.cuda.set_device(local)
             print(json.dumps(measure_full_forms(local)), flush=True)
+        return
+    if args.long_loops:
+        if rank == 0:
+            import torch
+            torch.cuda.set_device(local)
+            print(json.dumps(measure_closure_forms(local, chains=400, links=16, closure_fraction=1.0)), flush=True)
         return
     scene = scenes.stack_grid(50, 40, 50, seed=args.seed)
 

@@ -34,7 +34,12 @@ constexpr uint32_t kMBlock = 256;
 constexpr uint32_t kClosureThreads = 1024;
 constexpr uint32_t kClosureSteps = 12;     // device.rs:974
 constexpr uint32_t kClosureRounds = 8;     // closure.wgsl:356
-constexpr uint32_t kMaxLoop = 8;           // coordinates of one per-loop preconditioner block
+constexpr uint32_t kMaxLoop = 8;           // coordinates of one per-loop preconditioner block (storage)
+// A closure constrains 5 directions (3 of position, 2 of its hinge axis), so a
+// loop's J^T J has rank at most 5: a block of more of its coordinates is
+// singular (its Cholesky then hangs on the ridge alone, and the preconditioned
+// iteration diverged on 16-body loops).  Loops are cut into pieces of 5.
+constexpr uint32_t kLoopPiece = 5;
 constexpr uint32_t kBearingCache = 9;     // float4 per bearing in the projection cache
 constexpr uint32_t kLongList = 256;        // slot runs longer than this are summed in chunks of this many
 
@@ -142,7 +147,7 @@ MechTopology derive_topology(const MkCreation* cr, MechParams& p) {
     p.closure_bodies = (uint32_t)t.cb_bodies.size();
     p.blocks = (p.closure_coords + 1) / 2;
     // per-loop blocks: each closure coordinate joins the block of the first closure that
-    // contains it; loops longer than kMaxLoop are cut into consecutive pieces
+    // contains it; loops longer than kLoopPiece are cut into consecutive pieces
     {
         std::map<uint32_t, uint32_t> position;
         for (uint32_t q = 0; q < t.cq_coords.size(); ++q) position[t.cq_coords[q]] = q;
@@ -158,8 +163,8 @@ MechTopology derive_topology(const MkCreation* cr, MechParams& p) {
                 qs.push_back(it->second);
             }
             std::sort(qs.begin(), qs.end());
-            for (size_t i = 0; i < qs.size(); i += kMaxLoop) {
-                for (size_t j = i; j < std::min(qs.size(), i + kMaxLoop); ++j) t.loop_q.push_back(qs[j]);
+            for (size_t i = 0; i < qs.size(); i += kLoopPiece) {
+                for (size_t j = i; j < std::min<size_t>(qs.size(), i + kLoopPiece); ++j) t.loop_q.push_back(qs[j]);
                 t.loop_off.push_back((uint32_t)t.loop_q.size());
             }
         }

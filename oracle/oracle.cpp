@@ -1587,8 +1587,8 @@ template <class T> struct World : WorldBase {
                 qs.push_back(it->second);
             }
             std::sort(qs.begin(), qs.end());
-            for (size_t i = 0; i < qs.size(); i += 8) {
-                for (size_t j = i; j < std::min<size_t>(qs.size(), i + 8); ++j) loop_q.push_back(qs[j]);
+            for (size_t i = 0; i < qs.size(); i += 5) {   // pieces of 5: a closure's J^T J has rank <= 5
+                for (size_t j = i; j < std::min<size_t>(qs.size(), i + 5); ++j) loop_q.push_back(qs[j]);
                 loop_off.push_back((uint32_t)loop_q.size());
             }
         }

@@ -67,6 +67,21 @@ def test_chains_pcg_loop_blocks_bitexact(cuda_lib):
     assert cs["max_relative_residual"] <= 1e-5
 
 
+@pytest.mark.parametrize("mode", [1, 2], ids=["block", "grid"])
+def test_long_loops_pcg_pieces_bitexact(cuda_lib, mode):
+    """Sixteen-body loops (15 closure coordinates each, more than one block holds): the
+    per-loop blocks are pieces of 5 coordinates, the rank of a closure's constraint rows, so
+    every piece is positive definite; one block and the whole grid match the oracle."""
+    cfg = learned.closure_config(max_iterations=64)
+    prev = _closure_grid(mode)
+    try:
+        gpu, orc = _run(scenes.bearing_chains(chains=24, links=16, seed=3, closure_fraction=1.0, height=0.5),
+                        cfg, 4)
+    finally:
+        _closure_grid(max(prev, 0))
+    assert orc.closure_stats()["max_relative_residual"] < 1.0   # the iteration does not blow up
+
+
 def test_chains_pcg_pair_blocks_bitexact(cuda_lib):
     cfg = learned.closure_config(max_iterations=64)
     cfg.preconditioner = abi.PRECOND_PAIR_BLOCKS
