@@ -537,7 +537,7 @@ MK_API int mk_set_tuning(uint32_t key, uint32_t value);
 typedef struct MkTuning {
     uint32_t sort_items;          /* keys per thread of the collider sort's 256-thread onesweep tile: 2, 4, 6,
                                      8, 11 or 16, or 32 for 512 threads x 16 (default by size: 8 up to 64k keys,
-                                     11 up to 2M, else 16) */
+                                     11 up to 2M, else 32) */
     uint32_t sort_ctas_per_sm;    /* onesweep CTAs per SM (default 1 for the 8,192-key tile, 2 for 11 or 16
                                      keys, 3 for 8, else 6) */
     uint32_t append_ctas_per_sm;  /* CTAs per SM of the ordered-append kernels (default 8) */
