@@ -377,6 +377,23 @@ def test_standalone_sort_every_tile_shape(cuda_lib, items):
     assert np.array_equal(v_out.cpu().numpy().view(np.uint32), vals[order])
 
 
+def test_standalone_sort_above_2m_keys_default_tile(cuda_lib):
+    """Above 2M keys the default tile is the 8,192-key one: still the stable order."""
+    import torch
+    from mechanic_b200 import ops
+    rng = np.random.default_rng(17)
+    n = 3_000_001
+    keys = rng.integers(0, 1 << 40, n, dtype=np.uint64)
+    keys[::11] = keys[5]                                 # ties across tiles
+    vals = np.arange(n, dtype=np.uint32)
+    k_out, v_out = ops.sort_keys(torch.from_numpy(keys.view(np.int64)).cuda(),
+                                 torch.from_numpy(vals.view(np.int32)).cuda(), key_bits=40)
+    torch.cuda.synchronize()
+    order = np.argsort(keys, kind="stable")
+    assert np.array_equal(k_out.cpu().numpy().view(np.uint64), keys[order])
+    assert np.array_equal(v_out.cpu().numpy().view(np.uint32), vals[order])
+
+
 def test_grid_above_one_sort_tile_bitexact(cuda_lib):
     """16,000 colliders: the collider sort takes the onesweep passes, not the one-CTA sort."""
     scene = scenes.stack_grid(20, 10, 20, seed=13)
